@@ -1,0 +1,505 @@
+"""CPU oracle of MBPTcode's space-time ISDF RPA/GW route -- TEST INFRASTRUCTURE.
+
+This module is the checker, never the product: only tests/, the smoke check
+and bench.py's CPU-baseline leg may import it. It restates, in FP64 NumPy,
+the reference's algorithm for the route, each function citing the reference
+file:line it follows (paths inside MBPTcode). Its results are pinned against
+golden vectors produced by the reference itself (tests/golden/, generated by
+tests/golden/make_golden.py, which imports the reference), so the GPU path is
+compared with numbers that the reference computes.
+
+The time/frequency axes come from mbptcode_b200.grids, whose tables and
+least-squares transform fits are pinned bitwise to the reference's in the
+same fixtures.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+# reference constants (src/Base/numerics/constants.py)
+ISDF_TILE_GB = 4.0                   # :292
+BYTES_PER_GB = 1e9                   # :17
+QP_GRAPHICAL_TOL = 1e-8              # :272
+QP_GRAPHICAL_N_OMEGA = 150           # :273
+QP_GRAPHICAL_MAX_BISECTION = 100     # :274
+QP_Z_DERIV_STEP = 1e-3               # :276
+QP_WINDOW_Z_MIN = 0.5                # :553
+QP_SEARCH_WINDOW_TIERS = ((0.0, 0.5), (1.5, 1.0), (4.0, 2.0))   # :1464
+QP_SCAN_SECANT_MIN = 0.5             # :1613
+QP_SCAN_SPLIT_DEPTH = 6              # :1614
+EVGW_MAX_CYCLE, EVGW_TOL = 30, 1e-5  # :187-188
+EVGW_DIIS_SIZE, EVGW_DIIS_START = 8, 2   # :197-198
+
+
+# ---------------------------------------------------------------------------
+# chi0 sweep (src/SingleReference/LinearResponse/space_time.py)
+# ---------------------------------------------------------------------------
+
+def particle_hole_window(eps, nocc):
+    """src/Base/orbital_spaces.py:12-20."""
+    eps = np.asarray(eps, float)
+    homo, lumo = eps[:nocc].max(), eps[nocc:].min()
+    return lumo - homo, eps[nocc:].max() - eps[:nocc].min(), 0.5 * (homo + lumo)
+
+
+def split_branches(X, eps, nocc, mu=None):
+    """space_time.py:448-475: contiguous X_o, X_v and mu-shifted energies."""
+    eps = np.asarray(eps, float)
+    if mu is None:
+        mu = particle_hole_window(eps, nocc)[2]
+    X_o = np.ascontiguousarray(X[:, :nocc])
+    X_v = np.ascontiguousarray(X[:, nocc:])
+    return X_o, X_v, eps[:nocc] - mu, eps[nocc:] - mu, mu
+
+
+def tile_rows(M, tile_gb, per_row_bytes):
+    """space_time.py:413-416."""
+    return max(1, min(M, int(tile_gb * BYTES_PER_GB / max(per_row_bytes, 1))))
+
+
+def polarizability_projected_tau(X_o, X_v, e_o, e_v, D, tau, tile_gb=ISDF_TILE_GB):
+    """space_time.py:478-530: proj(tau) = -2 D^T (Go o Gv) D, grid-row tiled."""
+    M = X_o.shape[0]
+    rows = tile_rows(M, tile_gb, 3 * M * 8)
+    out = np.zeros((D.shape[1], D.shape[1]))
+    eo_t, ev_t = np.exp(e_o * tau), np.exp(-e_v * tau)
+    for p0 in range(0, M, rows):
+        p1 = min(p0 + rows, M)
+        Go = (X_o[p0:p1] * eo_t) @ X_o.T
+        Gv = (X_v[p0:p1] * ev_t) @ X_v.T
+        Go *= Gv
+        out += D[p0:p1].T @ (Go @ D)
+    out *= -2.0
+    return out
+
+
+def polarizability_projected_sweep(X, D, eps, nocc, tau_points, mu=None,
+                                   tile_gb=ISDF_TILE_GB):
+    """space_time.py:533-560: proj(tau) for every tau, (ntau, naux, naux)."""
+    X_o, X_v, e_o, e_v, _ = split_branches(X, eps, nocc, mu)
+    return np.stack([polarizability_projected_tau(X_o, X_v, e_o, e_v, D, t, tile_gb)
+                     for t in np.asarray(tau_points, float)])
+
+
+def chi0_imaginary_frequency(X, D, eps, nocc, grid, mu=None, tile_gb=ISDF_TILE_GB):
+    """space_time.py:607-651: chi0(i w_f) = sum_tau cosft_wt[f, tau] proj(tau)."""
+    X_o, X_v, e_o, e_v, _ = split_branches(X, eps, nocc, mu)
+    chi0 = np.zeros((grid.nfreq, D.shape[1], D.shape[1]))
+    for k, tau in enumerate(grid.tau_points):
+        proj = polarizability_projected_tau(X_o, X_v, e_o, e_v, D, tau, tile_gb)
+        chi0 += grid.cosft_wt[:, k, None, None] * proj
+    return chi0
+
+
+def dyson_screening(chi0, correlation=False):
+    """space_time.py:956-968: W = [I - chi0]^-1 (minus I when correlation)."""
+    W = np.linalg.inv(np.eye(chi0.shape[-1]) - chi0)
+    if correlation:
+        W[np.diag_indices_from(W)] -= 1.0
+    return W
+
+
+def dielectric_log_determinant(one_minus_c, where, flags=None):
+    """space_time.py:1073-1097: log|det|, flagging a non-positive determinant."""
+    sign, logdet = np.linalg.slogdet(one_minus_c)
+    if not sign > 0 and flags is not None:
+        flags.setdefault('nonpositive_det', []).append(where)
+    return logdet
+
+
+def rpa_correlation_energy(X, D, eps, nocc, grid, mu=None, flags=None,
+                           want_proj=False):
+    """space_time.py:1100-1183 (serial, gas phase):
+    E_c = (1/2pi) sum_w w_w [log det(I - chi0_w) + tr chi0_w]."""
+    proj = polarizability_projected_sweep(X, D, eps, nocc, grid.tau_points, mu)
+    blk = np.tensordot(grid.cosft_wt, proj, axes=(1, 0))
+    e_c = 0.0
+    for k in range(grid.nfreq):
+        c = blk[k]
+        logdet = dielectric_log_determinant(np.eye(c.shape[0]) - c, k, flags)
+        e_c += grid.omega_weights[k] * (logdet + np.trace(c))
+    e_c /= 2.0 * np.pi
+    return (e_c, proj) if want_proj else e_c
+
+
+# ---------------------------------------------------------------------------
+# screened interaction and self-energy (src/SingleReference/GW/imaginary_time.py)
+# ---------------------------------------------------------------------------
+
+def transform_screened(Ctw, W_omega):
+    """imaginary_time.py:181-195: Wt(tau) = sum_w Ctw[tau, w] (W(i w) - I)."""
+    n = W_omega.shape[-1]
+    blk = W_omega.copy()
+    blk[(slice(None),) + np.diag_indices(n)] -= 1.0
+    return np.tensordot(Ctw, blk, axes=(1, 0))
+
+
+def sigma_branch_sums(X, D, Wt_tau, eps, nocc, tau_sigma, mu, states):
+    """imaginary_time.py:39-92 (SigmaPairs.add, one block pair) over every tau:
+    Sigma^<_pp(tau) = sum_PQ X_s[P,p] (Go o Zt)_PQ X_s[Q,p] and
+    Sigma^>_pp(tau) = -sum_PQ X_s[P,p] (Gv o Zt)_PQ X_s[Q,p], Zt = D Wt D^T.
+    Equal to the MO diagonal of the AO build of :403-533 taken with X_ao = X,
+    mo_coeff = I (`sigma_ao_to_mo_diagonal` :581-587). Returns (2, ntau, S)."""
+    X_o, X_v, e_o, e_v, _ = split_branches(X, eps, nocc, mu)
+    X_s = np.ascontiguousarray(X[:, np.atleast_1d(states)])
+    sig = np.zeros((2, len(tau_sigma), X_s.shape[1]))
+    for k, tau in enumerate(tau_sigma):
+        Zt = (D @ Wt_tau[k]) @ D.T
+        G = (X_o * np.exp(e_o * tau)) @ X_o.T
+        G *= Zt
+        sig[0, k] = np.einsum('Pp,Pp->p', X_s, G @ X_s)
+        G = (X_v * np.exp(-e_v * tau)) @ X_v.T
+        G *= Zt
+        sig[1, k] = -np.einsum('Pp,Pp->p', X_s, G @ X_s)
+    return sig
+
+
+def sigma_frequency(sig, C, S):
+    """imaginary_time.py:525-532 / :559-561: Sigma_c(i w_p) =
+    -1/2 [C (S> + S<) + i S (S> - S<)], returned as (nstates, npade)."""
+    sig_l, sig_g = sig
+    return -0.5 * ((sig_g + sig_l).T @ C.T + 1j * ((sig_g - sig_l).T @ S.T))
+
+
+# ---------------------------------------------------------------------------
+# Pade continuation (src/Base/utils/grids/analytic_continuation.py)
+# ---------------------------------------------------------------------------
+
+def thiele_coefficients(z, f):
+    """analytic_continuation.py:15-22."""
+    n = len(z)
+    g = np.zeros((n, n), dtype=complex)
+    g[:, 0] = f
+    for i in range(1, n):
+        g[i:, i] = (g[i - 1, i - 1] - g[i:, i - 1]) / ((z[i:] - z[i - 1]) * g[i:, i - 1])
+    return g.diagonal().copy()
+
+
+def pade_eval(zq, z, a):
+    """analytic_continuation.py:25-31."""
+    r = a[-1] * np.ones_like(np.asarray(zq, dtype=complex))
+    for i in range(len(a) - 2, -1, -1):
+        r = a[i] / (1.0 + (zq - z[i]) * r)
+    return r
+
+
+def greedy_pade_order(z, f):
+    """analytic_continuation.py:34-61."""
+    remaining = list(range(len(z)))
+    order = [int(np.argmin(np.abs(z)))]
+    remaining.remove(order[0])
+    while remaining:
+        best_j, best = None, np.inf
+        for j in remaining:
+            trial = order + [j]
+            score = abs(thiele_coefficients(z[trial], f[trial])[-1])
+            if np.isfinite(score) and score < best:
+                best, best_j = score, j
+        if best_j is None:
+            raise FloatingPointError('greedy Pade ordering: no finite next '
+                                     'coefficient')
+        order.append(best_j)
+        remaining.remove(best_j)
+    return np.array(order)
+
+
+class PadeFit:
+    """analytic_continuation.py:64-89 (greedy, all points)."""
+
+    def __init__(self, z, f, greedy=True):
+        if greedy:
+            o = greedy_pade_order(z, f)
+            z, f = z[o], f[o]
+        self.z, self.f = z, f
+        self.coefficients = thiele_coefficients(z, f)
+
+    def __call__(self, zq):
+        return pade_eval(zq, self.z, self.coefficients)
+
+
+# ---------------------------------------------------------------------------
+# QP root finder (src/Solvers/qp_equation.py, sampled equation, no fprime)
+# ---------------------------------------------------------------------------
+
+class _Counted:
+    def __init__(self, f):
+        self.f, self.n = f, 0
+
+    def __call__(self, w):
+        self.n += 1
+        return self.f(w)
+
+
+def _search_windows(a):
+    """qp_equation.py:1280-1288."""
+    tier = 0
+    for k, (depth, _) in enumerate(QP_SEARCH_WINDOW_TIERS):
+        if abs(a) > depth:
+            tier = k
+    return [(a - half, a + half) for _, half in QP_SEARCH_WINDOW_TIERS[tier:]]
+
+
+def _refine_root(func, a, b, tol, max_bisection):
+    """qp_equation.py:1319-1333."""
+    fa = func(a)
+    for _ in range(max_bisection):
+        c = 0.5 * (a + b)
+        fc = func(c)
+        if fa * fc <= 0.0:
+            b = c
+        else:
+            a, fa = c, fc
+        if abs(b - a) <= tol:
+            break
+    return 0.5 * (a + b)
+
+
+def pole_strength(func, w, h=QP_Z_DERIV_STEP):
+    """qp_equation.py:1336-1350."""
+    d = (func(w + h) - func(w - h)) / (2.0 * h)
+    if d == 0.0 or not np.isfinite(d):
+        return np.nan
+    return 1.0 / d
+
+
+def _cells(func, l, r, fl, fr, depth):
+    """qp_equation.py:1256-1271 (no refusals)."""
+    if fl * fr < 0.0:
+        return [(l, r, fl, fr)]
+    if depth == 0 or fl == 0.0 or fr == 0.0 or not (fr - fl < QP_SCAN_SECANT_MIN * (r - l)):
+        return []
+    m = 0.5 * (l + r)
+    fm = float(func(m))
+    return _cells(func, l, m, fl, fm, depth - 1) + _cells(func, m, r, fm, fr, depth - 1)
+
+
+def _solve_bracket(func, bracket):
+    """qp_equation.py:1138-1157 with fprime None and positive_weight False."""
+    l, r, fl, fr = bracket
+    if l == r:
+        return [(float(l), float(pole_strength(func, l)))]
+    w = _refine_root(func, r, l, QP_GRAPHICAL_TOL, QP_GRAPHICAL_MAX_BISECTION)
+    fw = float(func(w))
+    if not abs(fw) <= max(abs(fl), abs(fr)):
+        return []
+    return [(float(w), float(pole_strength(func, w)))]
+
+
+def _valid(z, z_min=0.0):
+    """qp_equation.py:85-94 (`quasiparticle_weight`)."""
+    z = float(z)
+    return bool(np.isfinite(z) and z_min < z <= 1.0)
+
+
+def _select(found):
+    """qp_equation.py:97-109 with z_min 0 and no `near`."""
+    ok = [i for i, (_, z) in enumerate(found) if _valid(z)]
+    if not ok:
+        return None
+    return max(ok, key=lambda i: found[i][1])
+
+
+def solve_qp_equation_pole_strength(func, a):
+    """qp_equation.py:1353-1393 -> find_qp_root :155-232 -> _largest_root
+    :236-268 -> _weighed_roots :277-305 on a SampledEquation :1029-1271
+    (every bracket of a window is refined: its Z bounds are all infinite).
+
+    Returns (root, Z, quasiparticle)."""
+    found, k = [], None
+    windows = _search_windows(a)
+    for lo, hi in windows:
+        grid = np.linspace(lo, hi, QP_GRAPHICAL_N_OMEGA)
+        f = np.array([func(w) for w in grid])
+        brackets = []
+        for i in range(1, grid.size):
+            brackets += _cells(func, grid[i - 1], grid[i], f[i - 1], f[i],
+                               QP_SCAN_SPLIT_DEPTH)
+        found = []
+        for br in brackets:
+            found += _solve_bracket(func, br)
+        k = _select(found)
+        if k is not None and _valid(found[k][1], QP_WINDOW_Z_MIN):
+            return found[k][0], found[k][1], True
+    if not found:
+        return np.nan, np.nan, False
+    if k is None:
+        k = min(range(len(found)), key=lambda i: abs(found[i][0] - a))
+    return found[k][0], found[k][1], False
+
+
+def imaginary_axis_sample_points(freq_points, nocc, p, mu):
+    """GW/qp_solve.py:698-703."""
+    sign = -1.0 if p < nocc else 1.0
+    return mu + 1j * sign * np.asarray(freq_points)
+
+
+def solve_qp_from_imaginary_axis(eps_p, xc, z_fit, sigma_iw, greedy=True,
+                                 counter=None):
+    """GW/qp_solve.py:529-558: Pade-continue Sigma_c and solve
+    w = eps_p + xc + Re Sigma_c(w) for the root of largest Z."""
+    fit = PadeFit(z_fit, sigma_iw, greedy=greedy)
+
+    def residual(w):
+        return w - eps_p - xc - fit(np.array([w], dtype=complex))[0].real
+    func = _Counted(residual)
+    root, z, qp = solve_qp_equation_pole_strength(func, eps_p)
+    if counter is not None:
+        counter.append(func.n)
+    return root, z, fit
+
+
+def finish_qp(sigma, eps, nocc, states, mu, pade_freq, xc_diag=None,
+              greedy=True, counts=None):
+    """GW/qp_solve.py:575-695 on a restricted gas-phase reference with the
+    static term handed in (xc_diagonal; 0 for an HF reference, :311).
+    sigma (nstates, npade) on the positive branch; occupied states take the
+    conjugate (:659). Returns (roots, Z)."""
+    states = np.atleast_1d(states)
+    xc = np.zeros(len(states)) if xc_diag is None else np.asarray(xc_diag, float)
+    roots, zs = np.empty(len(states)), np.empty(len(states))
+    for i, p in enumerate(states):
+        z_fit = imaginary_axis_sample_points(pade_freq, nocc, int(p), mu)
+        s_p = np.conj(sigma[i]) if p < nocc else sigma[i]
+        roots[i], zs[i], _ = solve_qp_from_imaginary_axis(
+            float(eps[p]), xc[i], z_fit, s_p, greedy=greedy, counter=counts)
+    return roots, zs
+
+
+# ---------------------------------------------------------------------------
+# the route (src/SingleReference/GW/space_time.py:768-863, serial restricted)
+# ---------------------------------------------------------------------------
+
+def gw_space_time(X, D, eps, nocc, states, axes, eps_anchor=None, xc_diag=None,
+                  timings=None, counts=None):
+    """chi0 -> Dyson -> Wt(tau) -> Sigma_c diagonal -> QP roots, on the axes
+    `axes` (mbptcode_b200.grids.space_time_axes). Returns a dict with chi0,
+    W_minus_I, Wt, sigma (nstates, npade), roots and Z."""
+    import time
+    eps = np.asarray(eps, float)
+    mu = axes.mu
+    t0 = time.perf_counter()
+    chi0 = chi0_imaginary_frequency(X, D, eps, nocc, axes.grid, mu)
+    t1 = time.perf_counter()
+    W = np.stack([dyson_screening(c, correlation=True) for c in chi0])
+    t2 = time.perf_counter()
+    Wt = np.tensordot(axes.Ctw, W, axes=(1, 0))
+    sig = sigma_branch_sums(X, D, Wt, eps, nocc, axes.tau_sigma, mu, states)
+    sigma = sigma_frequency(sig, axes.C, axes.S)
+    t3 = time.perf_counter()
+    anchor = eps if eps_anchor is None else np.asarray(eps_anchor, float)
+    roots, z = finish_qp(sigma, anchor, nocc, states, mu, axes.pade_freq,
+                         xc_diag, counts=counts)
+    t4 = time.perf_counter()
+    if timings is not None:
+        timings.update(t_chi0=t1 - t0, t_dyson=t2 - t1, t_sigma=t3 - t2,
+                       t_qp=t4 - t3)
+    return {'chi0': chi0, 'W_minus_I': W, 'Wt': Wt, 'branch': sig,
+            'sigma': sigma, 'roots': roots, 'z': z}
+
+
+# ---------------------------------------------------------------------------
+# dRPA adjoint (src/gradients/rpa/space_time_adjoint.py:136-218, 473-563)
+# ---------------------------------------------------------------------------
+
+def polarizability_backward(proj_bar, X, D, eps, nocc, tau_points, mu=None):
+    """space_time_adjoint.py:167-218 with one row tile: the reverse of the
+    chi0 sweep, G(tau) recomputed per tau."""
+    X_o, X_v, e_o, e_v, _ = split_branches(X, eps, nocc, mu)
+    eps_bar = np.zeros(len(eps))
+    X_bar = np.zeros_like(X)
+    D_bar = np.zeros_like(D)
+    for k, tau in enumerate(tau_points):
+        pb = 0.5 * (proj_bar[k] + proj_bar[k].T)
+        E = -2.0 * (D @ pb)
+        w, u = np.exp(e_o * tau), np.exp(-e_v * tau)
+        Go = (X_o * w) @ X_o.T
+        Gv = (X_v * u) @ X_v.T
+        Pi = Go * Gv
+        D_bar += 2.0 * (Pi @ E)
+        Pi_bar = E @ D.T
+        GoX = (Pi_bar * Gv) @ X_o
+        GvX = (Pi_bar * Go) @ X_v
+        X_bar[:, :nocc] += 2.0 * GoX * w
+        X_bar[:, nocc:] += 2.0 * GvX * u
+        eps_bar[:nocc] += tau * w * np.einsum('bi,bi->i', X_o, GoX)
+        eps_bar[nocc:] -= tau * u * np.einsum('ba,ba->a', X_v, GvX)
+    return eps_bar, X_bar, D_bar
+
+
+def rpa_energy_and_adjoint(X, D, eps, nocc, grid, mu=None):
+    """space_time_adjoint.py:473-563, gas phase: (E_c, eps_bar, X_bar, D_bar)."""
+    e_c, proj = rpa_correlation_energy(X, D, eps, nocc, grid, mu, want_proj=True)
+    blk = np.tensordot(grid.cosft_wt, proj, axes=(1, 0))
+    eye = np.eye(proj.shape[-1])
+    for k in range(grid.nfreq):
+        scale = grid.omega_weights[k] / (2.0 * np.pi)
+        blk[k] = scale * (eye - np.linalg.inv(eye - blk[k]).T)
+    proj_bar = np.tensordot(grid.cosft_wt, blk, axes=(0, 0))
+    eps_bar, X_bar, D_bar = polarizability_backward(proj_bar, X, D, eps, nocc,
+                                                    grid.tau_points, mu)
+    return e_c, eps_bar, X_bar, D_bar
+
+
+# ---------------------------------------------------------------------------
+# evGW (src/SingleReference/GW/evGW.py:78-229) with Pulay DIIS
+# ---------------------------------------------------------------------------
+
+class PulayDIIS:
+    """Pulay's direct inversion in the iterative subspace (Chem. Phys. Lett.
+    73, 393 (1980)): the iterate that minimises the norm of the linearly
+    combined residuals under sum c = 1. Before `start` updates it passes the
+    iterate through; it keeps the last `size` pairs. This follows the
+    schedule the reference's evGW loop drives (evGW.py:181, 209-210)."""
+
+    def __init__(self, size, start):
+        self.size, self.start, self.seen = size, start, 0
+        self.vecs, self.errs = [], []
+
+    def update(self, vec, err):
+        if self.seen < self.start:
+            self.seen += 1
+            return vec
+        self.seen += 1
+        self.vecs.append(np.array(vec, float))
+        self.errs.append(np.array(err, float))
+        if len(self.vecs) > self.size:
+            self.vecs.pop(0)
+            self.errs.pop(0)
+        n = len(self.vecs)
+        B = np.zeros((n + 1, n + 1))
+        B[:n, :n] = [[e1 @ e2 for e2 in self.errs] for e1 in self.errs]
+        B[n, :n] = B[:n, n] = -1.0
+        rhs = np.zeros(n + 1)
+        rhs[n] = -1.0
+        c = np.linalg.solve(B, rhs)[:n]
+        return sum(ci * v for ci, v in zip(c, self.vecs))
+
+
+def evgw(X, D, eps0, nocc, ntau, tol=EVGW_TOL, max_cycle=EVGW_MAX_CYCLE,
+         diis_size=EVGW_DIIS_SIZE, diis_start=EVGW_DIIS_START, counts=None):
+    """evGW.py:78-229 restricted, every orbital updated, screening 'updated':
+    each cycle builds G, chi0 and W from the iterate, anchors the equation on
+    eps0 (GW/space_time.py:706-712) and converges on HOMO/LUMO."""
+    from mbptcode_b200.grids import space_time_axes
+    eps0 = np.asarray(eps0, float)
+    n = len(eps0)
+    tested = [nocc - 1, nocc]
+    eps = eps0.copy()
+    acc = PulayDIIS(diis_size, diis_start) if diis_size else None
+    history = []
+    converged = False
+    for _ in range(max_cycle):
+        axes = space_time_axes(eps, nocc, ntau=ntau, anchor=eps0)
+        out = gw_space_time(X, D, eps, nocc, np.arange(n), axes,
+                            eps_anchor=eps0, counts=counts)
+        eps_new = out['roots']
+        res = eps_new - eps
+        delta = float(np.abs(res[tested]).max())
+        history.append(delta)
+        if delta < tol:
+            eps = eps_new
+            converged = True
+            break
+        eps = acc.update(eps_new, res) if acc is not None else eps_new
+    return eps, {'cycles': len(history), 'converged': converged,
+                 'history': history}

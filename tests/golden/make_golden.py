@@ -1,0 +1,175 @@
+"""Generate the golden fixtures of tests/golden/ by running MBPTcode itself.
+
+Run in a container that holds the reference at /root/reference (pure Python;
+the modules used here import without pyscf):
+
+    python tests/golden/make_golden.py [/root/reference]
+
+Each fixture stores the inputs (seeded) and the reference's outputs for them:
+
+* grids.npz          tabulated tau/omega axes and the four transform matrices
+                     (src/Base/utils/grids/grids.py, time_frequency.py);
+* shared_kernel.npz  the random-factor system of the reference's
+                     tests/test_space_time_shared_kernel.py (M=23, n=8, nocc=3,
+                     naux=6, ntau=8, nfreq=5, seed 11, five row tiles):
+                     proj(tau) and chi0(i w);
+* route_<name>.npz   a synthetic ISDF system (mbptcode_b200.synthetic) through
+                     the reference route: chi0, W - I, Wt(tau), the Sigma_c
+                     diagonal from the AO build, QP roots and Z for every
+                     state, E_c and its adjoint;
+* qp_kat.npz         the root finder on closed-form self-energies
+                     (tests/test_qp_refine_root.py's two-pole Sigma and others).
+"""
+import os
+import sys
+import warnings
+
+import numpy as np
+
+REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REF)
+sys.path.insert(0, os.path.abspath(os.path.join(HERE, '..', '..')))
+
+from src.Base.utils.grids.grids import (gauss_legendre_grid,            # noqa: E402
+                                        minimax_frequency_grid, minimax_time_grid)
+from src.Base.utils.grids.time_frequency import (TimeFrequencyGrid,     # noqa: E402
+                                                 sigma_fit_ranges,
+                                                 minimax_transform_weights,
+                                                 COSINE_TW, COSINE_WT, SINE_TW)
+from src.Base.utils.grids.analytic_continuation import (PadeFit,        # noqa: E402
+                                                        thiele_coefficients)
+from src.Base.orbital_spaces import particle_hole_window                # noqa: E402
+from src.SingleReference.LinearResponse.space_time import (             # noqa: E402
+    chi0_imaginary_frequency, dyson_screening, polarizability_projected_sweep,
+    rpa_correlation_energy_space_time)
+from src.SingleReference.GW.imaginary_time import (                     # noqa: E402
+    minimax_points_for_gw, screening_frequency_grid, _transform_screened,
+    self_energy_matrix_imaginary_time, sigma_ao_to_mo_diagonal)
+from src.Solvers.qp_equation import solve_qp_equation_pole_strength     # noqa: E402
+from src.gradients.rpa.space_time_adjoint import rpa_energy_and_adjoint  # noqa: E402
+
+from mbptcode_b200.synthetic import synthetic_system                    # noqa: E402
+
+
+def grids_fixture():
+    out = {}
+    cases = [(8, 1.0, 12.0), (12, 0.35, 6.5), (16, 0.3, 30.0), (18, 0.2, 40.0),
+             (20, 0.3, 30.0), (24, 0.1, 20.0), (30, 1.0, 100.0), (34, 1.0, 100.0)]
+    out['cases'] = np.array(cases)
+    for i, (n, a, b) in enumerate(cases):
+        n = int(n)
+        out[f'tau_{i}'], out[f'tauw_{i}'] = minimax_time_grid(n, a, b)
+        out[f'om_{i}'], out[f'omw_{i}'] = minimax_frequency_grid(n, a, b)
+        with warnings.catch_warnings():
+            warnings.simplefilter('ignore')
+            g = TimeFrequencyGrid.minimax(n, a, b)
+        for k in ('cosft_wt', 'cosft_tw', 'sinft_wt', 'sinft_tw'):
+            out[f'{k}_{i}'] = getattr(g, k)
+    out['gl16'], out['gl16w'] = gauss_legendre_grid(16, 1.0)
+    np.savez_compressed(os.path.join(HERE, 'grids.npz'), **out)
+
+
+def shared_kernel_fixture():
+    M, NORB, NOCC, NAUX, NTAU, NFREQ = 23, 8, 3, 6, 8, 5
+    tile_gb = 5 * 3 * M * 8 / 1e9
+    rng = np.random.default_rng(11)
+    eps = np.sort(rng.normal(size=NORB))
+    eps[NOCC:] += 2.0
+    X = 0.25 * rng.normal(size=(M, NORB))
+    D = 0.25 * rng.normal(size=(M, NAUX))
+    gap = eps[NOCC] - eps[NOCC - 1]
+    e_max = eps[-1] - eps[0]
+    nu, wt = gauss_legendre_grid(NFREQ, w0=gap)
+    grid = TimeFrequencyGrid.minimax_split(NTAU, gap, e_max, nu, wt,
+                                           with_sine=False, with_inverse=False)
+    proj = polarizability_projected_sweep(X, D, eps, NOCC, grid.tau_points,
+                                          tile_memory_gb=tile_gb)
+    chi0 = chi0_imaginary_frequency(X, D, eps, NOCC, grid, tile_memory_gb=tile_gb)
+    np.savez_compressed(os.path.join(HERE, 'shared_kernel.npz'), X=X, D=D,
+                        eps=eps, nocc=NOCC, tau=grid.tau_points,
+                        cosft_wt=grid.cosft_wt, omega=nu, omega_w=wt,
+                        proj=proj, chi0=chi0)
+
+
+def route_fixture(name, n_orb, nocc, M, seed, variant, ntau, full=False):
+    X, D, eps = synthetic_system(n_orb, nocc, M, seed, variant)
+    e_min, e_max, mu = particle_hole_window(eps, nocc)
+    ntau_auto, _ = minimax_points_for_gw(eps, nocc, mu=mu)
+    freq, fw = screening_frequency_grid(ntau, eps, nocc, mu=mu)
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        grid = TimeFrequencyGrid.minimax_split(ntau, e_min, e_max, freq, fw)
+    rW, rS = sigma_fit_ranges(eps, nocc, mu=mu)
+    tau_sigma = 0.5 * minimax_time_grid(ntau, *rS)[0]
+    pade = gauss_legendre_grid(16, w0=1.0)[0]
+    chi0 = chi0_imaginary_frequency(X, D, eps, nocc, grid, mu=mu)
+    W = np.stack([dyson_screening(c, correlation=True) for c in chi0])
+    Ctw = minimax_transform_weights(COSINE_WT, tau_sigma, freq, *rW, warn=False)[0]
+    C = minimax_transform_weights(COSINE_TW, tau_sigma, pade, *rS, warn=False)[0]
+    S = minimax_transform_weights(SINE_TW, tau_sigma, pade, *rS, warn=False)[0]
+    Wt = _transform_screened(Ctw, W + np.eye(W.shape[-1]))
+    sig_ao = self_energy_matrix_imaginary_time(
+        X, D, W + np.eye(W.shape[-1]), np.eye(n_orb), eps, nocc, tau_sigma,
+        freq, pade, mu=mu)
+    states = np.arange(n_orb)
+    sigma = sigma_ao_to_mo_diagonal(sig_ao, np.eye(n_orb), states=states).T
+    roots, zs = np.empty(n_orb), np.empty(n_orb)
+    for i, p in enumerate(states):
+        sign = -1.0 if p < nocc else 1.0
+        z_fit = mu + 1j * sign * pade
+        s_p = np.conj(sigma[i]) if p < nocc else sigma[i]
+        fit = PadeFit(z_fit, s_p, greedy=True)
+
+        def residual(w, fit=fit, p=p):
+            return w - eps[p] - fit(np.array([w], dtype=complex))[0].real
+        got = solve_qp_equation_pole_strength(residual, eps[p],
+                                              return_diagnostics=True)
+        roots[i] = got[0]
+        dz = [z for w, z in got[1] if w == got[0]]
+        zs[i] = dz[0] if dz else np.nan
+    e_c = rpa_correlation_energy_space_time(X, D, eps, nocc, grid, mu=mu)
+    e_c2, eps_bar, X_bar, D_bar, _ = rpa_energy_and_adjoint(X, D, eps, nocc,
+                                                            grid, mu=mu)
+    big = dict(chi0=chi0, W_minus_I=W, Wt=Wt) if full else {}
+    np.savez_compressed(
+        os.path.join(HERE, f'route_{name}.npz'), **big, X=X, D=D, eps=eps, nocc=nocc,
+        ntau=ntau, ntau_auto=ntau_auto, mu=mu, tau=grid.tau_points,
+        omega=freq, omega_w=fw, cosft_wt=grid.cosft_wt, tau_sigma=tau_sigma,
+        Ctw=Ctw, C=C, S=S, pade=pade, sigma=sigma, roots=roots, z=zs, e_c=e_c, e_c_adj=e_c2,
+        eps_bar=eps_bar, X_bar=X_bar, D_bar=D_bar)
+
+
+def qp_fixture():
+    cases = {  # poles placed off the scan grids, so no division hits one
+        'two_pole': (lambda w: 0.05 / (w + 0.8) + 0.01 / (w - 0.9), -0.2),
+        'one_pole': (lambda w: 0.02 / (w + 0.5), 0.3),
+        'satellite': (lambda w: 0.3 / (w + 0.4537) + 0.02 / (w + 1.1129), -0.6),
+        'deep': (lambda w: 0.4 / (w - 0.2113) + 0.1 / (w + 3.0171), -2.0),
+    }
+    out = {}
+    for k, (sig, a) in cases.items():
+        f = lambda w, sig=sig, a=a: w - a - sig(w)
+        got = solve_qp_equation_pole_strength(f, a, return_diagnostics=True,
+                                              full_output=True)
+        out[k] = np.array([got[0], float(got[2])])
+    # Thiele coefficients of a random complex sample (16 points)
+    rng = np.random.default_rng(5)
+    z = 0.1 + 1j * np.sort(rng.uniform(0.01, 10.0, 16))
+    f = rng.normal(size=16) + 1j * rng.normal(size=16)
+    out['thiele_z'], out['thiele_f'] = z, f
+    out['thiele_a'] = thiele_coefficients(z, f)
+    fit = PadeFit(z, f, greedy=True)
+    out['greedy_z'] = fit.z
+    out['greedy_eval'] = fit(np.linspace(-1, 1, 7) + 0j)
+    np.savez_compressed(os.path.join(HERE, 'qp_kat.npz'), **out)
+
+
+if __name__ == '__main__':
+    grids_fixture()
+    shared_kernel_fixture()
+    route_fixture('calibrated', 24, 4, 64, 7, 'calibrated', 12, full=True)
+    route_fixture('literal16', 20, 3, 48, 3, 'literal', 16)
+    route_fixture('calibrated16', 28, 5, 72, 9, 'calibrated', 16)
+    qp_fixture()
+    print('fixtures written to', HERE)

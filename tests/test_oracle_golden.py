@@ -1,0 +1,121 @@
+"""The CPU oracle and the host-side grid builder, pinned to golden vectors
+that MBPTcode itself produced (tests/golden/make_golden.py)."""
+import numpy as np
+import pytest
+
+from mbptcode_b200 import grids
+from oracle import st_oracle as orc
+
+
+def test_grids_match_reference_bitwise(golden):
+    g = golden('grids')
+    for i, (n, a, b) in enumerate(g['cases']):
+        n = int(n)
+        tau, tw = grids.minimax_time_grid(n, a, b)
+        om, ow = grids.minimax_frequency_grid(n, a, b)
+        assert np.array_equal(tau, g[f'tau_{i}']) and np.array_equal(tw, g[f'tauw_{i}'])
+        assert np.array_equal(om, g[f'om_{i}']) and np.array_equal(ow, g[f'omw_{i}'])
+        with _quiet():
+            tf = grids.TimeFrequencyGrid.minimax(n, a, b)
+        for k in ('cosft_wt', 'cosft_tw', 'sinft_wt', 'sinft_tw'):
+            assert np.array_equal(getattr(tf, k), g[f'{k}_{i}']), (n, k)
+    x, w = grids.gauss_legendre_grid(16, 1.0)
+    assert np.array_equal(x, g['gl16']) and np.array_equal(w, g['gl16w'])
+
+
+class _quiet:
+    def __enter__(self):
+        import warnings
+        self._c = warnings.catch_warnings()
+        self._c.__enter__()
+        warnings.simplefilter('ignore')
+
+    def __exit__(self, *a):
+        self._c.__exit__(*a)
+
+
+# Laplace-identity known answers of the reference's tests/test_minimax_tau_grid.py
+IN_TABLE = [(6, 1.0, 3.0, 1e-6), (8, 1.0, 12.0, 1e-5), (14, 0.3, 30.0, 1e-6),
+            (20, 0.3, 30.0, 1e-9), (30, 1.0, 4000.0, 1e-8)]
+STRETCHED = [(22, 1.0, 100.0, 1e-9), (24, 1.0, 100.0, 1e-9), (28, 1.0, 100.0, 1e-9),
+             (30, 1.0, 100.0, 1e-9), (34, 1.0, 100.0, 1e-9), (34, 0.3, 30.0, 1e-9),
+             (30, 2.0, 60.0, 1e-9)]
+
+
+@pytest.mark.parametrize('n,a,b,tol', IN_TABLE + STRETCHED)
+def test_laplace_identity_known_answers(n, a, b, tol):
+    tau, w = grids.minimax_time_grid(n, a, b)
+    x = np.geomspace(a, b, 2001)
+    assert float(np.abs(1.0 - x * (np.exp(-np.outer(x, tau)) @ w)).max()) < tol
+
+
+def test_refusals():
+    with pytest.raises(ValueError):
+        grids.minimax_time_grid(7, 1.0, 10.0)
+    with pytest.raises(ValueError):
+        grids.minimax_time_grid(16, 0.0, 10.0)
+    with pytest.raises(ValueError):
+        grids.minimax_frequency_grid(16, 1.0, 0.5)
+
+
+def test_shared_kernel_system(golden):
+    g = golden('shared_kernel')
+    nocc = int(g['nocc'])
+    # five row tiles with a short last one, as in the reference's test
+    tile_gb = 5 * 3 * 23 * 8 / 1e9
+    proj = orc.polarizability_projected_sweep(g['X'], g['D'], g['eps'], nocc,
+                                              g['tau'], tile_gb=tile_gb)
+    assert np.allclose(proj, g['proj'], rtol=1e-13, atol=1e-13 * np.abs(g['proj']).max())
+    chi0 = np.tensordot(g['cosft_wt'], proj, axes=(1, 0))
+    scale = np.abs(g['chi0']).max()
+    assert np.abs(chi0 - g['chi0']).max() <= 1e-13 * scale
+
+
+@pytest.mark.parametrize('name', ['calibrated', 'literal16', 'calibrated16'])
+def test_route_matches_reference(golden, name):
+    g = golden('route_' + name)
+    X, D, eps, nocc = g['X'], g['D'], g['eps'], int(g['nocc'])
+    with _quiet():
+        axes = grids.space_time_axes(eps, nocc, ntau=int(g['ntau']))
+    assert np.array_equal(axes.grid.tau_points, g['tau'])
+    assert np.array_equal(axes.grid.cosft_wt, g['cosft_wt'])
+    assert np.array_equal(axes.tau_sigma, g['tau_sigma'])
+    for k in ('Ctw', 'C', 'S'):
+        assert np.array_equal(getattr(axes, k), g[k]), k
+    out = orc.gw_space_time(X, D, eps, nocc, np.arange(len(eps)), axes)
+    if 'chi0' in g:
+        s = np.abs(g['chi0']).max()
+        assert np.abs(out['chi0'] - g['chi0']).max() <= 1e-12 * s
+        s = np.abs(g['W_minus_I']).max()
+        assert np.abs(out['W_minus_I'] - g['W_minus_I']).max() <= 1e-11 * s
+        s = np.abs(g['Wt']).max()
+        assert np.abs(out['Wt'] - g['Wt']).max() <= 1e-11 * s
+    s = np.abs(g['sigma']).max()
+    assert np.abs(out['sigma'] - g['sigma']).max() <= 1e-10 * s
+    # QP roots: the scan's bisection tolerance is 1e-8 Ha
+    ok = np.isfinite(g['roots'])
+    assert np.array_equal(ok, np.isfinite(out['roots']))
+    assert np.abs(out['roots'][ok] - g['roots'][ok]).max() < 2e-8
+    e_c = orc.rpa_correlation_energy(X, D, eps, nocc, axes.grid)
+    assert abs(e_c - float(g['e_c'])) <= 1e-12 * abs(float(g['e_c'])) + 1e-15
+    e2, eb, xb, db = orc.rpa_energy_and_adjoint(X, D, eps, nocc, axes.grid)
+    for a, b in ((eb, g['eps_bar']), (xb, g['X_bar']), (db, g['D_bar'])):
+        assert np.abs(a - b).max() <= 1e-10 * np.abs(b).max() + 1e-18
+
+
+def test_qp_known_answers(golden):
+    g = golden('qp_kat')
+    cases = {
+        'two_pole': (lambda w: 0.05 / (w + 0.8) + 0.01 / (w - 0.9), -0.2),
+        'one_pole': (lambda w: 0.02 / (w + 0.5), 0.3),
+        'satellite': (lambda w: 0.3 / (w + 0.4537) + 0.02 / (w + 1.1129), -0.6),
+        'deep': (lambda w: 0.4 / (w - 0.2113) + 0.1 / (w + 3.0171), -2.0),
+    }
+    for k, (sig, a) in cases.items():
+        root, z, qp = orc.solve_qp_equation_pole_strength(lambda w: w - a - sig(w), a)
+        assert root == g[k][0] and float(qp) == g[k][1], k
+    a = orc.thiele_coefficients(g['thiele_z'], g['thiele_f'])
+    assert np.allclose(a, g['thiele_a'], rtol=1e-12)
+    fit = orc.PadeFit(g['thiele_z'], g['thiele_f'])
+    assert np.array_equal(fit.z, g['greedy_z'])
+    assert np.allclose(fit(np.linspace(-1, 1, 7) + 0j), g['greedy_eval'], rtol=1e-10)
