@@ -1,0 +1,225 @@
+/*
+ * libmbpt_b200 -- C ABI of the B200 (sm_100a) space-time ISDF RPA/GW route.
+ *
+ * Conventions
+ *   - Every array argument named *_dev is a DEVICE pointer owned by the
+ *     caller; *_host arguments are small host arrays read during the call.
+ *   - Matrices are row-major FP64 unless stated; complex arrays are
+ *     interleaved (re, im) FP64.
+ *   - Calls are stream-ordered on `stream` (a cudaStream_t, NULL = legacy
+ *     default stream) and take their scratch from the caller's `workspace`
+ *     of `ws_bytes` bytes, sized by the matching *_workspace_bytes query.
+ *     The FP64 products and the Cholesky/LU factorisations go through
+ *     cuBLAS/cuSOLVER handles created on first use (per host thread);
+ *     mbpt_dyson (and mbpt_rpa_energy through it) synchronises `stream`
+ *     once to read the factorisations' info words.
+ *   - The return value is an mbpt_status. Errors found on the device (a
+ *     bounded wait that ran out) are written to the int at `err_dev`
+ *     (zeroed by the caller before the call, read after it); NULL skips.
+ *   - mode MBPT_MODE_FP64 runs every product in FP64 (cuBLAS DGEMM, the plain
+ *     GPU path); MBPT_MODE_MIXED runs the N^3 products on the tcgen05 tensor
+ *     cores as split-BF16 (3-term) products with FP32 accumulation. The
+ *     tau <-> omega transforms, the Cholesky/log-det, the quadrature sums and
+ *     the QP root search are FP64 in both modes.
+ *
+ * Symbols: X (M x norb) collocation of the MO basis on the interpolation
+ * points, columns [0, nocc) occupied; D (M x naux) Coulomb factor, Z = D D^T;
+ * eps (norb) orbital energies; mu the chemical potential inside the gap.
+ */
+#ifndef MBPT_B200_H
+#define MBPT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum mbpt_status {
+  MBPT_OK = 0,
+  MBPT_ERR_SHAPE = 1,       /* inconsistent or unsupported sizes */
+  MBPT_ERR_NOT_SPD = 2,     /* 1 - chi0 not positive definite at some frequency */
+  MBPT_ERR_NONFINITE = 3,   /* a non-finite value where a finite one is needed */
+  MBPT_ERR_NO_ROOT = 4,     /* a QP equation without a root (per-state flag) */
+  MBPT_ERR_TIMEOUT = 5,     /* a bounded device-side wait ran out */
+  MBPT_ERR_CUDA = 6,        /* a CUDA runtime / library call failed */
+  MBPT_ERR_WORKSPACE = 7,   /* workspace smaller than the query returned */
+  MBPT_ERR_UNSUPPORTED = 8  /* device or option not supported */
+};
+
+enum mbpt_mode { MBPT_MODE_FP64 = 0, MBPT_MODE_MIXED = 1 };
+
+int mbpt_abi_version(void);
+const char *mbpt_status_string(int status);
+/* 1 when `device` is an sm_100 part this library was built for, else 0 */
+int mbpt_device_supported(int device);
+
+/* Instrumentation (no counterpart in MBPTcode, which has no device code):
+ * the number of this library's kernels launched by the process so far, and
+ * CUDA-event timing of the tensor-core engine's launches. mbpt_gemm_timing
+ * with enable = 1 starts recording on the launching streams; a call with
+ * non-NULL total_ms/launches (8 entries, indexed by epilogue kind: 0 split
+ * store, 1 FP32 store, 2 Hadamard, 3 self-energy Hadamards, 4 row
+ * contraction, 5 FP32 accumulate) waits for the recorded launches, returns
+ * their summed milliseconds and counts, and resets them. */
+long long mbpt_launch_count(void);
+int mbpt_gemm_timing(int enable, double *total_ms, long long *launches);
+
+/* ---- chi0 sweep ---------------------------------------------------------
+ * Replaces LinearResponse/space_time.py:607-651 chi0_imaginary_frequency
+ * (with :478-530 polarizability_projected_tau per tau point and :533-560
+ * polarizability_projected_sweep when proj_dev is given):
+ *   proj(tau_k)  = -2 D^T [G_occ(tau_k) o G_virt(tau_k)] D
+ *   chi0(i w_f)  = sum_k cosft_wt[f, k] proj(tau_k)
+ * G_occ(tau) = X_o diag(e^{(eps_i - mu) tau}) X_o^T,
+ * G_virt(tau) = X_v diag(e^{-(eps_a - mu) tau}) X_v^T.
+ * chi0_dev: (nfreq, naux, naux) output; proj_dev: optional (ntau, naux, naux)
+ * FP64 copy of proj(tau) (NULL: not kept).
+ * tau_host (ntau), cosft_wt_host (nfreq x ntau). */
+size_t mbpt_chi0_workspace_bytes(int64_t M, int64_t norb, int64_t nocc, int64_t naux,
+                                 int ntau, int mode);
+int mbpt_chi0_sweep(const double *X_dev, int64_t M, int64_t norb, int64_t nocc,
+                    const double *eps_dev, double mu, const double *D_dev, int64_t naux,
+                    const double *tau_host, int ntau, const double *cosft_wt_host, int nfreq,
+                    int mode, double *chi0_dev, double *proj_dev, void *workspace,
+                    size_t ws_bytes, int *err_dev, void *stream);
+
+/* ---- Dyson step and dielectric log-determinant ---------------------------
+ * Replaces LinearResponse/space_time.py:956-968 dyson_screening (per
+ * frequency, correlation=True) and :1073-1097 dielectric_log_determinant,
+ * by a Cholesky factorisation of 1 - chi0 at each frequency (FP64).
+ * chi0_dev (nfreq, naux, naux): in chi0; out W - I = [1 - chi0]^-1 - 1 when
+ * want_w, else the Cholesky factors.
+ * logdet_dev, trace_dev (nfreq): log det(1 - chi0) and tr chi0.
+ * info_host (nfreq): 0, or i > 0 when 1 - chi0 is not positive definite (its
+ * log|det| and inverse then come from an LU factorisation and sign_host[f]
+ * is the determinant's sign); the call then returns MBPT_ERR_NOT_SPD after
+ * finishing every frequency. info_host/sign_host may be NULL. */
+size_t mbpt_dyson_workspace_bytes(int64_t naux, int nfreq);
+int mbpt_dyson(double *chi0_dev, int64_t naux, int nfreq, int want_w, double *logdet_dev,
+               double *trace_dev, int *info_host, int *sign_host, void *workspace,
+               size_t ws_bytes, void *stream);
+
+/* ---- dRPA correlation energy ----------------------------------------------
+ * Replaces LinearResponse/space_time.py:1100-1183
+ * rpa_correlation_energy_space_time (gas phase, serial):
+ *   E_c = (1/2pi) sum_f omega_weights[f] [log det(1 - chi0_f) + tr chi0_f].
+ * e_c_dev: one FP64 output. proj_dev optional as in mbpt_chi0_sweep.
+ * logdet/trace of each frequency are left in the workspace head. */
+size_t mbpt_rpa_energy_workspace_bytes(int64_t M, int64_t norb, int64_t nocc, int64_t naux,
+                                       int ntau, int nfreq, int mode);
+int mbpt_rpa_energy(const double *X_dev, int64_t M, int64_t norb, int64_t nocc,
+                    const double *eps_dev, double mu, const double *D_dev, int64_t naux,
+                    const double *tau_host, int ntau, const double *cosft_wt_host,
+                    const double *omega_weights_host, int nfreq, int mode, double *e_c_dev,
+                    double *proj_dev, int *info_host, void *workspace, size_t ws_bytes,
+                    int *err_dev, void *stream);
+
+/* E_c = (1/2pi) sum_f w_f [logdet_f + trace_f], summed in frequency order
+ * (LinearResponse/space_time.py:1158-1182), from mbpt_dyson's outputs;
+ * omega_weights_dev (nfreq), e_c_dev one FP64 output. */
+int mbpt_energy_sum(const double *logdet_dev, const double *trace_dev,
+                    const double *omega_weights_dev, int nfreq, double *e_c_dev, void *stream);
+
+/* ---- tau <-> omega transform (FP64) --------------------------------------
+ * Replaces GW/imaginary_time.py:181-195 _transform_screened and the
+ * frequency fold of LinearResponse/space_time.py:854-905 / the adjoint's
+ * gradients/rpa/space_time_adjoint.py:440-454:
+ *   out[j] = sum_k w[j, k] in[k],   in (K, n, n), out (J, n, n), w_dev (J x K). */
+int mbpt_transform(const double *in_dev, int K, int64_t n, const double *w_dev, int J,
+                   double *out_dev, void *stream);
+
+/* ---- self-energy branch sums --------------------------------------------
+ * Replaces GW/imaginary_time.py:403-533 self_energy_matrix_imaginary_time
+ * followed by :581-587 sigma_ao_to_mo_diagonal (X_ao = X, mo_coeff = I),
+ * in the diagonal form of :39-92 SigmaPairs.add: for each tau_k
+ *   Zt = D Wt(tau_k) D^T,
+ *   branch[0,k,s] = +sum_PQ X[P,p] (G_occ(tau_k) o Zt)_PQ X[Q,p]
+ *   branch[1,k,s] = -sum_PQ X[P,p] (G_virt(tau_k) o Zt)_PQ X[Q,p],
+ * p = states[s]. Wt_dev (ntau, naux, naux); states_dev (nstates) int64;
+ * branch_dev (2, ntau, nstates) output. */
+size_t mbpt_sigma_workspace_bytes(int64_t M, int64_t norb, int64_t nocc, int64_t naux,
+                                  int ntau, int nstates, int mode);
+int mbpt_sigma_branch_sums(const double *X_dev, int64_t M, int64_t norb, int64_t nocc,
+                           const double *eps_dev, double mu, const double *D_dev,
+                           int64_t naux, const double *Wt_dev, const double *tau_host,
+                           int ntau, const int64_t *states_dev, int nstates, int mode,
+                           double *branch_dev, void *workspace, size_t ws_bytes, int *err_dev,
+                           void *stream);
+
+/* Sigma_c(i w_p) = -1/2 [C (S^> + S^<) + i S (S^> - S^<)]
+ * (GW/imaginary_time.py:525-532), C_dev/S_dev (npade x ntau);
+ * sigma_dev (nstates, npade) complex interleaved. */
+int mbpt_sigma_frequency(const double *branch_dev, int ntau, int nstates, const double *C_dev,
+                         const double *S_dev, int npade, double *sigma_dev, void *stream);
+
+/* ---- Pade continuation and QP roots --------------------------------------
+ * Replaces GW/qp_solve.py:575-695 finish_qp (its per-state loop),
+ * :529-558 solve_qp_from_imaginary_axis, analytic_continuation.py:64-89
+ * PadeFit and Solvers/qp_equation.py:1353-1393
+ * solve_qp_equation_pole_strength, for all states at once:
+ *   root of w = eps_anchor[p] + xc[s] + Re Sigma_c(w), largest Z.
+ * sigma_dev (nstates, npade) complex on the positive branch;
+ * pade_freq_host (npade); eps_anchor_dev (norb); xc_dev (nstates) or NULL
+ * (zero static term); warm_dev (nstates) predicted roots or NULL.
+ * flags bits: 1 quasiparticle (Z > 1/2), 2 no root (root NaN),
+ * 4 Z outside (0, 1], 8 Pade ordering failed, 16 warm start accepted,
+ * 32 bracket list overflow. evals: Sigma evaluations per state. */
+int mbpt_qp_solve(const double *sigma_dev, const double *pade_freq_host, int npade,
+                  const double *eps_anchor_dev, const double *xc_dev,
+                  const int64_t *states_dev, int nstates, int64_t nocc, double mu, int greedy,
+                  const double *warm_dev, double *roots_dev, double *z_dev, int *flags_dev,
+                  int *evals_dev, void *workspace, size_t ws_bytes, void *stream);
+
+/* ---- reverse sweep of the polarizability ---------------------------------
+ * Replaces gradients/rpa/space_time_adjoint.py:136-218
+ * polarizability_backward: for an adjoint proj_bar (ntau, naux, naux) of
+ * proj(tau), accumulates eps_bar (norb), X_bar (M x norb), D_bar (M x naux),
+ * recomputing G_occ(tau), G_virt(tau) per tau point (nothing is stored
+ * across tau). The outputs are overwritten. */
+size_t mbpt_chi0_backward_workspace_bytes(int64_t M, int64_t norb, int64_t nocc, int64_t naux,
+                                          int mode);
+int mbpt_chi0_backward(const double *proj_bar_dev, const double *X_dev, int64_t M,
+                       int64_t norb, int64_t nocc, const double *eps_dev, double mu,
+                       const double *D_dev, int64_t naux, const double *tau_host, int ntau,
+                       int mode, double *eps_bar_dev, double *X_bar_dev, double *D_bar_dev,
+                       void *workspace, size_t ws_bytes, int *err_dev, void *stream);
+
+/* chi0_bar(f) = (w_f / 2pi) [I - (1 - chi0_f)^-T] from W - I (the Dyson
+ * output): gradients/rpa/space_time_adjoint.py:528-539 (gas phase).
+ * Overwrites w_minus_i_dev (nfreq, naux, naux) in place; omega_weights_dev
+ * (nfreq). */
+int mbpt_energy_adjoint_seed(double *w_minus_i_dev, int64_t naux, int nfreq,
+                             const double *omega_weights_dev, void *stream);
+
+/* ---- quasiparticle-shift network (learned warm start) --------------------
+ * A 4 -> H -> H -> 1 perceptron with SiLU, FP32, parameters packed as
+ * [W1 (H x 4), b1 (H), W2 (H x H), b2 (H), W3 (H), b3 (1)].
+ * forward: y (B) from x (B x 4); the activations needed by backward are
+ * written to act_dev (B x 4H floats). backward: grad (same packing) of
+ * 0.5/B sum (y - t)^2, loss_dev (1) the loss. adamw: one AdamW step. */
+int mbpt_mlp_param_count(int hidden);
+int mbpt_mlp_forward(const float *params_dev, int hidden, const float *x_dev, int batch,
+                     float *y_dev, float *act_dev, void *stream);
+int mbpt_mlp_backward(const float *params_dev, int hidden, const float *x_dev, int batch,
+                      const float *act_dev, const float *y_dev, const float *target_dev,
+                      float *grad_dev, float *loss_dev, void *stream);
+int mbpt_mlp_adamw(float *params_dev, const float *grad_dev, float *m_dev, float *v_dev,
+                   int count, float lr, float beta1, float beta2, float eps, float weight_decay,
+                   int step, void *stream);
+
+/* ---- split-precision GEMM (diagnostic entry of the tensor-core engine) ---
+ * C (m x n, FP32, ldc) = alpha * A B^T with A (m x k) and B (n x k) FP64,
+ * each rounded to a BF16 pair and multiplied with three tcgen05 products.
+ * m, n, k are padded internally to multiples of 128 / 128 / 64. */
+size_t mbpt_gemm_split_workspace_bytes(int64_t m, int64_t n, int64_t k);
+int mbpt_gemm_split(const double *A_dev, const double *B_dev, int64_t m, int64_t n, int64_t k,
+                    double alpha, float *C_dev, int64_t ldc, void *workspace, size_t ws_bytes,
+                    int *err_dev, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MBPT_B200_H */

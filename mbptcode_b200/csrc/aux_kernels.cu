@@ -1,0 +1,171 @@
+// Small FP64 kernels of the adjoint and of the Dyson fallback path.
+#include <cmath>
+
+#include "internal.h"
+
+namespace mbpt {
+namespace {
+
+inline int blocks(int64_t n) {
+  int64_t b = (n + 255) / 256;
+  return static_cast<int>(b > 148 * 32 ? 148 * 32 : (b < 1 ? 1 : b));
+}
+
+// a_f <- -(w_f / 2pi) a_f^T for each W - I slice: chi0_bar of the dRPA energy
+// (W - I is symmetric here, the mirrored output of the Dyson step).
+__global__ void chi0_bar_seed_kernel(double *a, int64_t n, const double *w) {
+  double *m = a + static_cast<int64_t>(blockIdx.y) * n * n;
+  const double s = -w[blockIdx.y] / (2.0 * 3.14159265358979323846);
+  const int64_t total = n * n;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    m[i] *= s;
+}
+
+// out = (in + in^T) / 2
+__global__ void sym_half_kernel(const double *in, double *out, int64_t n) {
+  const int64_t total = n * n;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = i / n, c = i % n;
+    out[i] = 0.5 * (in[i] + in[c * n + r]);
+  }
+}
+
+// X_bar[:, occ] += 2 GoX w, X_bar[:, virt] += 2 GvX u;
+// eps_bar[i] += tau w_i sum_b X[b,i] GoX[b,i], eps_bar[a] -= tau u_a sum_b X[b,a] GvX[b,a]
+__global__ void xbar_kernel(const double *GoX, const double *GvX, const double *X, int64_t M,
+                            int64_t n, int64_t nocc, const double *eps, double mu, double tau,
+                            double *X_bar, double *eps_bar) {
+  const int64_t c = static_cast<int64_t>(blockIdx.x) * 32 + threadIdx.x;
+  __shared__ double part[8][33];
+  const int64_t nv = n - nocc;
+  double s = 0.0;
+  double f = 0.0;
+  if (c < n) {
+    const bool occ = c < nocc;
+    f = occ ? exp((eps[c] - mu) * tau) : exp(-(eps[c] - mu) * tau);
+    const int64_t r0 = static_cast<int64_t>(blockIdx.y) * 256;
+    const int64_t r1 = min(r0 + 256, M);
+    for (int64_t r = r0 + threadIdx.y; r < r1; r += 8) {
+      const double g = occ ? GoX[r * nocc + c] : GvX[r * nv + (c - nocc)];
+      X_bar[r * n + c] += 2.0 * g * f;
+      s += X[r * n + c] * g;
+    }
+  }
+  part[threadIdx.y][threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.y == 0 && c < n) {
+    double t = 0.0;
+    for (int k = 0; k < 8; ++k) t += part[k][threadIdx.x];
+    const double sign = c < nocc ? 1.0 : -1.0;
+    atomicAdd(eps_bar + c, sign * tau * f * t);
+  }
+}
+
+// restore a symmetric matrix from its row-major lower triangle
+__global__ void mirror_kernel(double *a, int64_t n) {
+  const int64_t total = n * n;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = i / n, c = i % n;
+    if (r < c) a[i] = a[c * n + r];
+  }
+}
+
+// log|det| and sign from an LU factor with 1-based pivots (column-major view)
+__global__ void lu_logdet_kernel(const double *LU, const int *piv, int64_t n, double *logdet,
+                                 int *sign) {
+  __shared__ double part[256];
+  __shared__ int neg[256];
+  double s = 0.0;
+  int ng = 0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const double d = LU[i * n + i];
+    s += log(fabs(d));
+    if (d < 0.0) ng ^= 1;
+    if (piv[i] != i + 1) ng ^= 1;
+  }
+  part[threadIdx.x] = s;
+  neg[threadIdx.x] = ng;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) {
+      part[threadIdx.x] += part[threadIdx.x + w];
+      neg[threadIdx.x] ^= neg[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    *logdet = part[0];
+    *sign = neg[0] ? -1 : 1;
+  }
+}
+
+// diag[f * n + i] <-> a_f[i, i]
+__global__ void diag_kernel(double *a, int64_t n, double *diag, bool save) {
+  double *m = a + static_cast<int64_t>(blockIdx.y) * n * n;
+  double *d = diag + static_cast<int64_t>(blockIdx.y) * n;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (save)
+      d[i] = m[i * n + i];
+    else
+      m[i * n + i] = d[i];
+  }
+}
+
+__global__ void identity_kernel(double *a, int64_t n, double diag_shift, bool set) {
+  const int64_t total = n * n;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = i / n, c = i % n;
+    if (set)
+      a[i] = (r == c) ? 1.0 : 0.0;
+    else if (r == c)
+      a[i] += diag_shift;
+  }
+}
+
+}  // namespace
+
+void launch_chi0_bar_seed(double *a, int64_t n, int nfreq, const double *w, cudaStream_t st) {
+  dim3 grid(static_cast<unsigned>(blocks(n * n) / 8 + 1), nfreq);
+  count_launch(); chi0_bar_seed_kernel<<<grid, 256, 0, st>>>(a, n, w);
+}
+
+void launch_sym_half(const double *in, double *out, int64_t n, cudaStream_t st) {
+  count_launch(); sym_half_kernel<<<blocks(n * n), 256, 0, st>>>(in, out, n);
+}
+
+void launch_xbar_update(const double *GoX, const double *GvX, const double *X, int64_t M,
+                        int64_t n, int64_t nocc, const double *eps, double mu, double tau,
+                        double *X_bar, double *eps_bar, cudaStream_t st) {
+  dim3 grid(static_cast<unsigned>((n + 31) / 32), static_cast<unsigned>((M + 255) / 256));
+  count_launch(); xbar_kernel<<<grid, dim3(32, 8), 0, st>>>(GoX, GvX, X, M, n, nocc, eps, mu, tau, X_bar,
+                                            eps_bar);
+}
+
+void launch_mirror_lower_to_upper(double *a, int64_t n, cudaStream_t st) {
+  count_launch(); mirror_kernel<<<blocks(n * n), 256, 0, st>>>(a, n);
+}
+
+void launch_lu_logdet(const double *LU, const int *piv, int64_t n, double *logdet, int *sign,
+                      cudaStream_t st) {
+  count_launch(); lu_logdet_kernel<<<1, 256, 0, st>>>(LU, piv, n, logdet, sign);
+}
+
+void launch_diag(double *a, int64_t n, int nmat, double *diag, bool save, cudaStream_t st) {
+  dim3 grid(static_cast<unsigned>((n + 255) / 256), nmat);
+  count_launch(); diag_kernel<<<grid, 256, 0, st>>>(a, n, diag, save);
+}
+
+void launch_identity(double *a, int64_t n, cudaStream_t st) {
+  count_launch(); identity_kernel<<<blocks(n * n), 256, 0, st>>>(a, n, 0.0, true);
+}
+
+void launch_minus_identity(double *a, int64_t n, cudaStream_t st) {
+  count_launch(); identity_kernel<<<blocks(n * n), 256, 0, st>>>(a, n, -1.0, false);
+}
+
+}  // namespace mbpt

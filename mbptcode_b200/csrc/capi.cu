@@ -1,0 +1,752 @@
+// C entry points of libmbpt_b200: orchestration of the route on the caller's
+// stream over the caller's workspace. FP64 mode runs the N^3 products through
+// cuBLAS DGEMM (the plain GPU path); mixed mode through the tcgen05 split
+// engine (umma_gemm.cuh). The Cholesky factorisations use cuSOLVER in FP64.
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "internal.h"
+
+namespace mbpt {
+int launch_pade_qp(const double *sigma, const double *pade_freq, int npade,
+                   const double *eps_anchor, const double *xc, const int64_t *states,
+                   int nstates, int64_t nocc, double mu, int greedy, const double *warm,
+                   double *roots, double *z, int *flags, int *evals, cudaStream_t st);
+void launch_chi0_bar_seed(double *a, int64_t n, int nfreq, const double *scale,
+                          cudaStream_t st);
+void launch_sym_half(const double *in, double *out, int64_t n, cudaStream_t st);
+void launch_xbar_update(const double *GoX, const double *GvX, const double *X, int64_t M,
+                        int64_t n, int64_t nocc, const double *eps, double mu, double tau,
+                        double *X_bar, double *eps_bar, cudaStream_t st);
+void launch_mirror_lower_to_upper(double *a, int64_t n, cudaStream_t st);
+void launch_lu_logdet(const double *LU, const int *piv, int64_t n, double *logdet, int *sign,
+                      cudaStream_t st);
+void launch_identity(double *a, int64_t n, cudaStream_t st);
+void launch_minus_identity(double *a, int64_t n, cudaStream_t st);
+void launch_diag(double *a, int64_t n, int nmat, double *diag, bool save, cudaStream_t st);
+
+namespace {
+std::atomic<long long> g_launches{0};
+}  // namespace
+
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+namespace {
+
+constexpr int kAbiVersion = 1;
+
+struct Handles {
+  cublasHandle_t blas = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+};
+
+Handles &handles(cudaStream_t st) {
+  thread_local Handles h;
+  if (!h.blas) {
+    cublasCreate(&h.blas);
+    cusolverDnCreate(&h.solver);
+  }
+  cublasSetStream(h.blas, st);
+  cusolverDnSetStream(h.solver, st);
+  return h;
+}
+
+// row-major C (m x n) = alpha op(A) op(B) + beta C
+bool dgemm_rm(cublasHandle_t h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
+              double alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
+              double beta, double *C, int64_t ldc) {
+  return cublasDgemm(h, tb ? CUBLAS_OP_T : CUBLAS_OP_N, ta ? CUBLAS_OP_T : CUBLAS_OP_N,
+                     static_cast<int>(n), static_cast<int>(m), static_cast<int>(k), &alpha, B,
+                     static_cast<int>(ldb), A, static_cast<int>(lda), &beta, C,
+                     static_cast<int>(ldc)) == CUBLAS_STATUS_SUCCESS;
+}
+
+inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+double *copy_weights(Arena &ar, const double *host, size_t count, cudaStream_t st) {
+  double *d = ar.take<double>(count);
+  if (d && host) cudaMemcpyAsync(d, host, count * sizeof(double), cudaMemcpyHostToDevice, st);
+  return d;
+}
+
+struct Dims {
+  int64_t M, n, nocc, nv, naux, Mp, Ap, Ko, Kv;
+  Dims(int64_t M_, int64_t n_, int64_t nocc_, int64_t naux_)
+      : M(M_), n(n_), nocc(nocc_), nv(n_ - nocc_), naux(naux_) {
+    Mp = round_up(M, 128);
+    Ap = round_up(naux, 128);
+    Ko = round_up(nocc, 64);
+    Kv = round_up(nv, 64);
+  }
+  bool ok() const { return M > 0 && n > nocc && nocc > 0 && naux > 0; }
+};
+
+// ---------------------------------------------------------------- chi0 sweep
+struct Chi0Bufs {
+  double *w;  // cosft_wt on the device
+  // fp64
+  double *Xo_s, *Xv_s, *Go, *Gv, *Y, *proj;
+  // mixed
+  bf16 *Dt_hi, *Dt_lo, *Yo_hi, *Yo_lo, *Yv_hi, *Yv_lo, *Pi_hi, *Pi_lo, *Z_hi, *Z_lo;
+  float *proj32;
+  double *eye;  // ntau x ntau identity for the optional proj copy
+};
+
+Chi0Bufs carve_chi0(Arena &ar, const Dims &d, int ntau, int nfreq, int mode, bool own_proj) {
+  Chi0Bufs b{};
+  b.w = ar.take<double>(static_cast<size_t>(nfreq) * ntau);
+  if (mode == MBPT_MODE_FP64) {
+    b.Xo_s = ar.take<double>(d.M * d.nocc);
+    b.Xv_s = ar.take<double>(d.M * d.nv);
+    b.Go = ar.take<double>(d.M * d.M);
+    b.Gv = ar.take<double>(d.M * d.M);
+    b.Y = ar.take<double>(d.M * d.naux);
+    if (own_proj) b.proj = ar.take<double>(static_cast<size_t>(ntau) * d.naux * d.naux);
+  } else {
+    b.Dt_hi = ar.take<bf16>(d.Ap * d.Mp);
+    b.Dt_lo = ar.take<bf16>(d.Ap * d.Mp);
+    b.Yo_hi = ar.take<bf16>(d.Mp * d.Ko);
+    b.Yo_lo = ar.take<bf16>(d.Mp * d.Ko);
+    b.Yv_hi = ar.take<bf16>(d.Mp * d.Kv);
+    b.Yv_lo = ar.take<bf16>(d.Mp * d.Kv);
+    b.Pi_hi = ar.take<bf16>(d.Mp * d.Mp);
+    b.Pi_lo = ar.take<bf16>(d.Mp * d.Mp);
+    b.Z_hi = ar.take<bf16>(d.Ap * d.Mp);
+    b.Z_lo = ar.take<bf16>(d.Ap * d.Mp);
+    b.proj32 = ar.take<float>(static_cast<size_t>(ntau) * d.Ap * d.Ap);
+    b.eye = ar.take<double>(static_cast<size_t>(ntau) * ntau);
+  }
+  return b;
+}
+
+int chi0_run(const double *X, const Dims &d, const double *eps, double mu, const double *D,
+             const double *tau, int ntau, const double *cw, int nfreq, int mode, double *chi0,
+             double *proj_out, Arena &ar, int *err, cudaStream_t st) {
+  Chi0Bufs b = carve_chi0(ar, d, ntau, nfreq, mode, proj_out == nullptr);
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  cudaMemcpyAsync(b.w, cw, sizeof(double) * nfreq * ntau, cudaMemcpyHostToDevice, st);
+  const int64_t a2 = d.naux * d.naux;
+  if (mode == MBPT_MODE_FP64) {
+    double *proj = proj_out ? proj_out : b.proj;
+    cublasHandle_t h = handles(st).blas;
+    for (int k = 0; k < ntau; ++k) {
+      launch_scaled_branches(X, d.M, d.n, d.nocc, eps, mu, tau[k], 1.0, b.Xo_s, b.Xv_s, st);
+      // G_occ = (X_o e^{e_o tau}) X_o^T, G_virt likewise (MBPTcode space_time.py:525-526)
+      if (!dgemm_rm(h, false, true, d.M, d.M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0, b.Go,
+                    d.M) ||
+          !dgemm_rm(h, false, true, d.M, d.M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n, 0.0,
+                    b.Gv, d.M))
+        return MBPT_ERR_CUDA;
+      launch_hadamard(b.Go, b.Gv, d.M * d.M, st);
+      if (!dgemm_rm(h, false, false, d.M, d.naux, d.M, 1.0, b.Go, d.M, D, d.naux, 0.0, b.Y,
+                    d.naux) ||
+          !dgemm_rm(h, true, false, d.naux, d.naux, d.M, -2.0, D, d.naux, b.Y, d.naux, 0.0,
+                    proj + k * a2, d.naux))
+        return MBPT_ERR_CUDA;
+    }
+    launch_transform<double>(proj, a2, d.naux, d.naux, d.naux, b.w, nfreq, ntau, chi0, a2,
+                             d.naux, st);
+  } else {
+    launch_split_pad<double>(D, d.M, d.naux, d.naux, 1.f, b.Dt_hi, b.Dt_lo, d.Mp, d.Mp, d.Ap,
+                             true, st);
+    SplitMat Yo{b.Yo_hi, b.Yo_lo, d.Mp, d.Ko, d.Ko}, Yv{b.Yv_hi, b.Yv_lo, d.Mp, d.Kv, d.Kv};
+    SplitMat Dt{b.Dt_hi, b.Dt_lo, d.Ap, d.Mp, d.Mp};
+    SplitMat Pi{b.Pi_hi, b.Pi_lo, d.Mp, d.Mp, d.Mp};
+    SplitMat Z{b.Z_hi, b.Z_lo, d.Ap, d.Mp, d.Mp};
+    for (int k = 0; k < ntau; ++k) {
+      launch_prep_branches(X, d.M, d.n, d.nocc, eps, mu, tau[k], b.Yo_hi, b.Yo_lo, d.Ko,
+                           b.Yv_hi, b.Yv_lo, d.Kv, d.Mp, st);
+      umma::EpiArgs e;
+      // Pi = (Y_o Y_o^T) o (Y_v Y_v^T), split for the next product
+      e.out0_hi = b.Pi_hi;
+      e.out0_lo = b.Pi_lo;
+      e.ld_out = d.Mp;
+      SplitMat A2[2] = {Yo, Yv};
+      int rc = gemm_split(umma::EPI_HADAMARD_SPLIT, 2, A2, A2, d.Mp, d.Mp, e, err, st);
+      if (rc) return rc;
+      // Z = D^T Pi  (= (Pi D)^T, Pi symmetric)
+      e = umma::EpiArgs();
+      e.out0_hi = b.Z_hi;
+      e.out0_lo = b.Z_lo;
+      e.ld_out = d.Mp;
+      rc = gemm_split(umma::EPI_SPLIT, 1, &Dt, &Pi, d.Ap, d.Mp, e, err, st);
+      if (rc) return rc;
+      // proj = -2 D^T Z^T
+      e = umma::EpiArgs();
+      e.outf = b.proj32 + k * d.Ap * d.Ap;
+      e.ld_outf = d.Ap;
+      e.alpha = -2.f;
+      rc = gemm_split(umma::EPI_F32, 1, &Dt, &Z, d.Ap, d.Ap, e, err, st);
+      if (rc) return rc;
+    }
+    launch_transform<float>(b.proj32, d.Ap * d.Ap, d.Ap, d.naux, d.naux, b.w, nfreq, ntau,
+                            chi0, a2, d.naux, st);
+    if (proj_out) {
+      std::vector<double> eye(static_cast<size_t>(ntau) * ntau, 0.0);
+      for (int k = 0; k < ntau; ++k) eye[k * ntau + k] = 1.0;
+      cudaMemcpyAsync(b.eye, eye.data(), sizeof(double) * eye.size(), cudaMemcpyHostToDevice,
+                      st);
+      launch_transform<float>(b.proj32, d.Ap * d.Ap, d.Ap, d.naux, d.naux, b.eye, ntau, ntau,
+                              proj_out, a2, d.naux, st);
+    }
+  }
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+// --------------------------------------------------------------------- Dyson
+struct DysonBufs {
+  int *info;
+  int *piv;
+  double *work;
+  double *rhs;   // n x n right-hand side of the LU inverse of a failed frequency
+  double *diag;  // nfreq x n diagonals of 1 - chi0, which the factorisation overwrites
+  int lwork;
+};
+
+int dyson_lwork(int64_t n) {
+  cudaStream_t st = nullptr;
+  Handles &h = handles(st);
+  int l1 = 0, l2 = 0, l3 = 0;
+  cusolverDnDpotrf_bufferSize(h.solver, CUBLAS_FILL_MODE_LOWER, static_cast<int>(n), nullptr,
+                              static_cast<int>(n), &l1);
+  cusolverDnDpotri_bufferSize(h.solver, CUBLAS_FILL_MODE_LOWER, static_cast<int>(n), nullptr,
+                              static_cast<int>(n), &l2);
+  cusolverDnDgetrf_bufferSize(h.solver, static_cast<int>(n), static_cast<int>(n), nullptr,
+                              static_cast<int>(n), &l3);
+  int l = l1 > l2 ? l1 : l2;
+  return l > l3 ? l : l3;
+}
+
+DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq) {
+  DysonBufs b{};
+  b.lwork = dyson_lwork(n);
+  b.info = ar.take<int>(nfreq + 1);
+  b.piv = ar.take<int>(n);
+  b.work = ar.take<double>(b.lwork > 0 ? b.lwork : 1);
+  b.rhs = ar.take<double>(n * n);
+  b.diag = ar.take<double>(n * static_cast<int64_t>(nfreq));
+  return b;
+}
+
+int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, double *trace,
+              int *info_host, int *sign_host, Arena &ar, cudaStream_t st) {
+  DysonBufs b = carve_dyson(ar, n, nfreq);
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  Handles &h = handles(st);
+  const int ni = static_cast<int>(n);
+  launch_one_minus(chi0, n, nfreq, trace, st);
+  launch_diag(chi0, n, nfreq, b.diag, true, st);
+  for (int f = 0; f < nfreq; ++f) {
+    if (cusolverDnDpotrf(h.solver, CUBLAS_FILL_MODE_LOWER, ni, chi0 + f * n * n, ni, b.work,
+                         b.lwork, b.info + f) != CUSOLVER_STATUS_SUCCESS)
+      return MBPT_ERR_CUDA;
+  }
+  std::vector<int> info(nfreq);
+  cudaMemcpyAsync(info.data(), b.info, sizeof(int) * nfreq, cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return MBPT_ERR_CUDA;
+  bool bad = false;
+  for (int f = 0; f < nfreq; ++f) {
+    if (info_host) info_host[f] = info[f];
+    if (sign_host) sign_host[f] = 1;
+    bad |= info[f] != 0;
+  }
+  launch_logdet_diag(chi0, n, nfreq, logdet, st);  // overwritten below where bad
+  for (int f = 0; f < nfreq; ++f) {
+    double *m = chi0 + f * n * n;
+    if (info[f] == 0) {
+      if (want_w) {
+        if (cusolverDnDpotri(h.solver, CUBLAS_FILL_MODE_LOWER, ni, m, ni, b.work, b.lwork,
+                             b.info + nfreq) != CUSOLVER_STATUS_SUCCESS)
+          return MBPT_ERR_CUDA;
+        launch_symmetrize_minus_identity(m, n, 1, st);
+      }
+      continue;
+    }
+    // not positive definite: restore 1 - chi0 from its untouched triangle,
+    // then LU for log|det| (and the inverse), as the reference's slogdet/inv
+    launch_mirror_lower_to_upper(m, n, st);
+    launch_diag(m, n, 1, b.diag + static_cast<int64_t>(f) * n, false, st);
+    if (cusolverDnDgetrf(h.solver, ni, ni, m, ni, b.work, b.piv, b.info + nfreq) !=
+        CUSOLVER_STATUS_SUCCESS)
+      return MBPT_ERR_CUDA;
+    int sgn = 1;
+    int *sgn_dev = b.info + nfreq;
+    launch_lu_logdet(m, b.piv, n, logdet + f, sgn_dev, st);
+    cudaMemcpyAsync(&sgn, sgn_dev, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (want_w) {
+      // inverse from the LU factor: solve against the identity, minus I
+      launch_identity(b.rhs, n, st);
+      if (cusolverDnDgetrs(h.solver, CUBLAS_OP_N, ni, ni, m, ni, b.piv, b.rhs, ni,
+                           b.info + nfreq) != CUSOLVER_STATUS_SUCCESS)
+        return MBPT_ERR_CUDA;
+      cudaMemcpyAsync(m, b.rhs, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, st);
+      launch_minus_identity(m, n, st);
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) return MBPT_ERR_CUDA;
+    if (sign_host) sign_host[f] = sgn;
+  }
+  if (cudaGetLastError() != cudaSuccess) return MBPT_ERR_CUDA;
+  return bad ? MBPT_ERR_NOT_SPD : MBPT_OK;
+}
+
+// -------------------------------------------------------------------- Sigma
+struct SigmaBufs {
+  // fp64
+  double *U, *Zt, *G, *Xo_s, *Xv_s, *Xs, *R;
+  // mixed
+  bf16 *D_hi, *D_lo, *W_hi, *W_lo, *U_hi, *U_lo, *Yo_hi, *Yo_lo, *Yv_hi, *Yv_lo, *Hl_hi,
+      *Hl_lo, *Hg_hi, *Hg_lo, *XsT_hi, *XsT_lo;
+  float *xs;
+  double *sig;
+};
+
+int64_t pad_states(int nstates) { return round_up(nstates, 128); }
+
+SigmaBufs carve_sigma(Arena &ar, const Dims &d, int ntau, int nstates, int mode) {
+  SigmaBufs b{};
+  if (mode == MBPT_MODE_FP64) {
+    b.U = ar.take<double>(d.M * d.naux);
+    b.Zt = ar.take<double>(d.M * d.M);
+    b.G = ar.take<double>(d.M * d.M);
+    b.Xo_s = ar.take<double>(d.M * d.nocc);
+    b.Xv_s = ar.take<double>(d.M * d.nv);
+    b.Xs = ar.take<double>(d.M * static_cast<int64_t>(nstates));
+    b.R = ar.take<double>(d.M * static_cast<int64_t>(nstates));
+  } else {
+    const int64_t Sp = pad_states(nstates);
+    b.D_hi = ar.take<bf16>(d.Mp * d.Ap);
+    b.D_lo = ar.take<bf16>(d.Mp * d.Ap);
+    b.W_hi = ar.take<bf16>(d.Ap * d.Ap);
+    b.W_lo = ar.take<bf16>(d.Ap * d.Ap);
+    b.U_hi = ar.take<bf16>(d.Mp * d.Ap);
+    b.U_lo = ar.take<bf16>(d.Mp * d.Ap);
+    b.Yo_hi = ar.take<bf16>(d.Mp * d.Ko);
+    b.Yo_lo = ar.take<bf16>(d.Mp * d.Ko);
+    b.Yv_hi = ar.take<bf16>(d.Mp * d.Kv);
+    b.Yv_lo = ar.take<bf16>(d.Mp * d.Kv);
+    b.Hl_hi = ar.take<bf16>(d.Mp * d.Mp);
+    b.Hl_lo = ar.take<bf16>(d.Mp * d.Mp);
+    b.Hg_hi = ar.take<bf16>(d.Mp * d.Mp);
+    b.Hg_lo = ar.take<bf16>(d.Mp * d.Mp);
+    b.XsT_hi = ar.take<bf16>(Sp * d.Mp);
+    b.XsT_lo = ar.take<bf16>(Sp * d.Mp);
+    b.xs = ar.take<float>(d.Mp * Sp);
+    b.sig = ar.take<double>(2 * static_cast<int64_t>(ntau) * Sp);
+  }
+  return b;
+}
+
+int sigma_run(const double *X, const Dims &d, const double *eps, double mu, const double *D,
+              const double *Wt, const double *tau, int ntau, const int64_t *states,
+              int nstates, int mode, double *branch, Arena &ar, int *err, cudaStream_t st) {
+  SigmaBufs b = carve_sigma(ar, d, ntau, nstates, mode);
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  const int64_t a2 = d.naux * d.naux;
+  const int64_t S = nstates;
+  if (mode == MBPT_MODE_FP64) {
+    cublasHandle_t h = handles(st).blas;
+    launch_gather_cols_f64(X, d.M, d.n, states, S, b.Xs, st);
+    for (int k = 0; k < ntau; ++k) {
+      // Zt = D Wt D^T (MBPTcode imaginary_time.py:508, :513)
+      if (!dgemm_rm(h, false, false, d.M, d.naux, d.naux, 1.0, D, d.naux, Wt + k * a2, d.naux,
+                    0.0, b.U, d.naux) ||
+          !dgemm_rm(h, false, true, d.M, d.M, d.naux, 1.0, b.U, d.naux, D, d.naux, 0.0, b.Zt,
+                    d.M))
+        return MBPT_ERR_CUDA;
+      launch_scaled_branches(X, d.M, d.n, d.nocc, eps, mu, tau[k], 1.0, b.Xo_s, b.Xv_s, st);
+      double *out_l = branch + static_cast<int64_t>(k) * S;
+      double *out_g = branch + static_cast<int64_t>(ntau + k) * S;
+      // lesser branch: G_occ o Zt contracted with X_s on both sides
+      if (!dgemm_rm(h, false, true, d.M, d.M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0, b.G,
+                    d.M))
+        return MBPT_ERR_CUDA;
+      launch_hadamard(b.G, b.Zt, d.M * d.M, st);
+      if (!dgemm_rm(h, false, false, d.M, S, d.M, 1.0, b.G, d.M, b.Xs, S, 0.0, b.R, S))
+        return MBPT_ERR_CUDA;
+      cudaMemsetAsync(out_l, 0, sizeof(double) * S, st);
+      launch_rowdot(b.R, S, b.Xs, S, d.M, S, 1.0, out_l, st);
+      // greater branch, with its minus sign
+      if (!dgemm_rm(h, false, true, d.M, d.M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n, 0.0,
+                    b.G, d.M))
+        return MBPT_ERR_CUDA;
+      launch_hadamard(b.G, b.Zt, d.M * d.M, st);
+      if (!dgemm_rm(h, false, false, d.M, S, d.M, 1.0, b.G, d.M, b.Xs, S, 0.0, b.R, S))
+        return MBPT_ERR_CUDA;
+      cudaMemsetAsync(out_g, 0, sizeof(double) * S, st);
+      launch_rowdot(b.R, S, b.Xs, S, d.M, S, -1.0, out_g, st);
+    }
+  } else {
+    const int64_t Sp = pad_states(nstates);
+    launch_split_pad<double>(D, d.M, d.naux, d.naux, 1.f, b.D_hi, b.D_lo, d.Ap, d.Mp, d.Ap,
+                             false, st);
+    launch_gather_cols_f32(X, d.M, d.n, states, S, b.xs, Sp, d.Mp, st);
+    launch_gather_cols_split_t(X, d.M, d.n, states, S, b.XsT_hi, b.XsT_lo, d.Mp, Sp, d.Mp, st);
+    cudaMemsetAsync(b.sig, 0, sizeof(double) * 2 * ntau * Sp, st);
+    SplitMat Dm{b.D_hi, b.D_lo, d.Mp, d.Ap, d.Ap};
+    SplitMat Wm{b.W_hi, b.W_lo, d.Ap, d.Ap, d.Ap};
+    SplitMat Um{b.U_hi, b.U_lo, d.Mp, d.Ap, d.Ap};
+    SplitMat Yo{b.Yo_hi, b.Yo_lo, d.Mp, d.Ko, d.Ko}, Yv{b.Yv_hi, b.Yv_lo, d.Mp, d.Kv, d.Kv};
+    SplitMat Hl{b.Hl_hi, b.Hl_lo, d.Mp, d.Mp, d.Mp}, Hg{b.Hg_hi, b.Hg_lo, d.Mp, d.Mp, d.Mp};
+    SplitMat XsT{b.XsT_hi, b.XsT_lo, Sp, d.Mp, d.Mp};
+    for (int k = 0; k < ntau; ++k) {
+      launch_split_pad<double>(Wt + k * a2, d.naux, d.naux, d.naux, 1.f, b.W_hi, b.W_lo, d.Ap,
+                               d.Ap, d.Ap, false, st);
+      launch_prep_branches(X, d.M, d.n, d.nocc, eps, mu, tau[k], b.Yo_hi, b.Yo_lo, d.Ko,
+                           b.Yv_hi, b.Yv_lo, d.Kv, d.Mp, st);
+      umma::EpiArgs e;
+      // U = D Wt (Wt symmetric)
+      e.out0_hi = b.U_hi;
+      e.out0_lo = b.U_lo;
+      e.ld_out = d.Ap;
+      int rc = gemm_split(umma::EPI_SPLIT, 1, &Dm, &Wm, d.Mp, d.Ap, e, err, st);
+      if (rc) return rc;
+      // one tile pass: Zt = U D^T, G_occ, G_virt -> H< = G_occ o Zt, H> = G_virt o Zt
+      e = umma::EpiArgs();
+      e.out0_hi = b.Hl_hi;
+      e.out0_lo = b.Hl_lo;
+      e.out1_hi = b.Hg_hi;
+      e.out1_lo = b.Hg_lo;
+      e.ld_out = d.Mp;
+      SplitMat A3[3] = {Um, Yo, Yv}, B3[3] = {Dm, Yo, Yv};
+      rc = gemm_split(umma::EPI_SIGMA_H, 3, A3, B3, d.Mp, d.Mp, e, err, st);
+      if (rc) return rc;
+      // branch sums: sum_P X_s[P,p] (H X_s)[P,p]
+      e = umma::EpiArgs();
+      e.xs = b.xs;
+      e.ld_xs = Sp;
+      e.sig0 = b.sig + static_cast<int64_t>(k) * Sp;
+      e.sig1 = b.sig + static_cast<int64_t>(ntau + k) * Sp;
+      SplitMat A2[2] = {Hl, Hg}, B2[2] = {XsT, XsT};
+      rc = gemm_split(umma::EPI_ROWDOT2, 2, A2, B2, d.Mp, Sp, e, err, st);
+      if (rc) return rc;
+    }
+    cudaMemcpy2DAsync(branch, sizeof(double) * S, b.sig, sizeof(double) * Sp,
+                      sizeof(double) * S, 2 * ntau, cudaMemcpyDeviceToDevice, st);
+  }
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+// ------------------------------------------------------------- chi0 adjoint
+struct BackBufs {
+  double *pb, *E, *Xo_s, *Xv_s, *Go, *Gv, *P, *T, *GoX, *GvX;
+};
+
+BackBufs carve_back(Arena &ar, const Dims &d) {
+  BackBufs b{};
+  b.pb = ar.take<double>(d.naux * d.naux);
+  b.E = ar.take<double>(d.M * d.naux);
+  b.Xo_s = ar.take<double>(d.M * d.nocc);
+  b.Xv_s = ar.take<double>(d.M * d.nv);
+  b.Go = ar.take<double>(d.M * d.M);
+  b.Gv = ar.take<double>(d.M * d.M);
+  b.P = ar.take<double>(d.M * d.M);
+  b.T = ar.take<double>(d.M * d.M);
+  b.GoX = ar.take<double>(d.M * d.nocc);
+  b.GvX = ar.take<double>(d.M * d.nv);
+  return b;
+}
+
+int back_run(const double *pbar, const double *X, const Dims &d, const double *eps, double mu,
+             const double *D, const double *tau, int ntau, double *eps_bar, double *X_bar,
+             double *D_bar, Arena &ar, cudaStream_t st) {
+  BackBufs b = carve_back(ar, d);
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  cublasHandle_t h = handles(st).blas;
+  const int64_t a2 = d.naux * d.naux;
+  cudaMemsetAsync(eps_bar, 0, sizeof(double) * d.n, st);
+  cudaMemsetAsync(X_bar, 0, sizeof(double) * d.M * d.n, st);
+  cudaMemsetAsync(D_bar, 0, sizeof(double) * d.M * d.naux, st);
+  for (int k = 0; k < ntau; ++k) {
+    // MBPTcode gradients/rpa/space_time_adjoint.py:196-217, one row tile
+    launch_sym_half(pbar + k * a2, b.pb, d.naux, st);
+    if (!dgemm_rm(h, false, false, d.M, d.naux, d.naux, -2.0, D, d.naux, b.pb, d.naux, 0.0,
+                  b.E, d.naux))
+      return MBPT_ERR_CUDA;
+    launch_scaled_branches(X, d.M, d.n, d.nocc, eps, mu, tau[k], 1.0, b.Xo_s, b.Xv_s, st);
+    if (!dgemm_rm(h, false, true, d.M, d.M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0, b.Go,
+                  d.M) ||
+        !dgemm_rm(h, false, true, d.M, d.M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n, 0.0,
+                  b.Gv, d.M))
+      return MBPT_ERR_CUDA;
+    launch_hadamard3(b.P, b.Go, b.Gv, d.M * d.M, st);  // Pi
+    if (!dgemm_rm(h, false, false, d.M, d.naux, d.M, 2.0, b.P, d.M, b.E, d.naux, 1.0, D_bar,
+                  d.naux) ||
+        !dgemm_rm(h, false, true, d.M, d.M, d.naux, 1.0, b.E, d.naux, D, d.naux, 0.0, b.P,
+                  d.M))  // Pi_bar
+      return MBPT_ERR_CUDA;
+    launch_hadamard3(b.T, b.P, b.Gv, d.M * d.M, st);  // Go_bar
+    if (!dgemm_rm(h, false, false, d.M, d.nocc, d.M, 1.0, b.T, d.M, X, d.n, 0.0, b.GoX,
+                  d.nocc))
+      return MBPT_ERR_CUDA;
+    launch_hadamard3(b.T, b.P, b.Go, d.M * d.M, st);  // Gv_bar
+    if (!dgemm_rm(h, false, false, d.M, d.nv, d.M, 1.0, b.T, d.M, X + d.nocc, d.n, 0.0, b.GvX,
+                  d.nv))
+      return MBPT_ERR_CUDA;
+    launch_xbar_update(b.GoX, b.GvX, X, d.M, d.n, d.nocc, eps, mu, tau[k], X_bar, eps_bar, st);
+  }
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+size_t count(void (*f)(Arena &)) {
+  Arena ar;
+  ar.counting = true;
+  f(ar);
+  return ar.used + 1024;
+}
+
+Arena arena(void *ws, size_t bytes) {
+  Arena ar;
+  ar.base = reinterpret_cast<uint8_t *>(ws);
+  ar.size = bytes;
+  if (reinterpret_cast<uintptr_t>(ws) & 1023) {
+    const size_t skip = 1024 - (reinterpret_cast<uintptr_t>(ws) & 1023);
+    ar.base += skip;
+    ar.size = bytes > skip ? bytes - skip : 0;
+  }
+  return ar;
+}
+
+}  // namespace
+}  // namespace mbpt
+
+using namespace mbpt;
+
+extern "C" {
+
+int mbpt_abi_version(void) { return kAbiVersion; }
+
+const char *mbpt_status_string(int s) {
+  switch (s) {
+    case MBPT_OK: return "ok";
+    case MBPT_ERR_SHAPE: return "inconsistent or unsupported sizes";
+    case MBPT_ERR_NOT_SPD: return "1 - chi0 is not positive definite at some frequency";
+    case MBPT_ERR_NONFINITE: return "non-finite value";
+    case MBPT_ERR_NO_ROOT: return "quasiparticle equation without a root";
+    case MBPT_ERR_TIMEOUT: return "a bounded device-side wait ran out";
+    case MBPT_ERR_CUDA: return "CUDA runtime or library error";
+    case MBPT_ERR_WORKSPACE: return "workspace too small";
+    case MBPT_ERR_UNSUPPORTED: return "unsupported device or option";
+    default: return "unknown status";
+  }
+}
+
+long long mbpt_launch_count(void) { return g_launches.load(); }
+
+int mbpt_gemm_timing(int enable, double *total_ms, long long *launches) {
+  return gemm_timing(enable, total_ms, launches);
+}
+
+int mbpt_energy_sum(const double *logdet, const double *trace, const double *w, int nfreq,
+                    double *e_c, void *stream) {
+  if (nfreq < 1) return MBPT_ERR_SHAPE;
+  launch_energy_sum(logdet, trace, w, nfreq, e_c, S(stream));
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+int mbpt_device_supported(int device) {
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return 0;
+  return p.major == 10 && p.minor == 0 ? 1 : 0;
+}
+
+size_t mbpt_chi0_workspace_bytes(int64_t M, int64_t norb, int64_t nocc, int64_t naux, int ntau,
+                                 int mode) {
+  Dims d(M, norb, nocc, naux);
+  Arena ar;
+  ar.counting = true;
+  carve_chi0(ar, d, ntau, 34, mode, true);
+  return ar.used + 2048;
+}
+
+int mbpt_chi0_sweep(const double *X, int64_t M, int64_t norb, int64_t nocc, const double *eps,
+                    double mu, const double *D, int64_t naux, const double *tau, int ntau,
+                    const double *cw, int nfreq, int mode, double *chi0, double *proj,
+                    void *ws, size_t ws_bytes, int *err, void *stream) {
+  Dims d(M, norb, nocc, naux);
+  if (!d.ok() || ntau < 1 || nfreq < 1 || ntau > 34 || nfreq > 34) return MBPT_ERR_SHAPE;
+  if (mode != MBPT_MODE_FP64 && mode != MBPT_MODE_MIXED) return MBPT_ERR_UNSUPPORTED;
+  Arena ar = arena(ws, ws_bytes);
+  return chi0_run(X, d, eps, mu, D, tau, ntau, cw, nfreq, mode, chi0, proj, ar, err, S(stream));
+}
+
+size_t mbpt_dyson_workspace_bytes(int64_t naux, int nfreq) {
+  Arena ar;
+  ar.counting = true;
+  carve_dyson(ar, naux, nfreq);
+  return ar.used + 2048;
+}
+
+int mbpt_dyson(double *chi0, int64_t naux, int nfreq, int want_w, double *logdet,
+               double *trace, int *info_host, int *sign_host, void *ws, size_t ws_bytes,
+               void *stream) {
+  if (naux < 1 || nfreq < 1) return MBPT_ERR_SHAPE;
+  Arena ar = arena(ws, ws_bytes);
+  return dyson_run(chi0, naux, nfreq, want_w, logdet, trace, info_host, sign_host, ar,
+                   S(stream));
+}
+
+size_t mbpt_rpa_energy_workspace_bytes(int64_t M, int64_t norb, int64_t nocc, int64_t naux,
+                                       int ntau, int nfreq, int mode) {
+  Dims d(M, norb, nocc, naux);
+  Arena ar;
+  ar.counting = true;
+  ar.take<double>(static_cast<size_t>(nfreq) * naux * naux);  // chi0
+  ar.take<double>(34);                                         // logdet
+  ar.take<double>(34);                                         // trace
+  ar.take<double>(34);                                         // weights
+  Arena a2 = ar;
+  carve_chi0(ar, d, ntau, nfreq, mode, true);
+  carve_dyson(a2, naux, nfreq);
+  return (ar.used > a2.used ? ar.used : a2.used) + 4096;
+}
+
+int mbpt_rpa_energy(const double *X, int64_t M, int64_t norb, int64_t nocc, const double *eps,
+                    double mu, const double *D, int64_t naux, const double *tau, int ntau,
+                    const double *cw, const double *ow, int nfreq, int mode, double *e_c,
+                    double *proj, int *info_host, void *ws, size_t ws_bytes, int *err,
+                    void *stream) {
+  Dims d(M, norb, nocc, naux);
+  if (!d.ok() || ntau < 1 || nfreq < 1 || ntau > 34 || nfreq > 34) return MBPT_ERR_SHAPE;
+  cudaStream_t st = S(stream);
+  Arena ar = arena(ws, ws_bytes);
+  double *chi0 = ar.take<double>(static_cast<size_t>(nfreq) * naux * naux);
+  double *logdet = ar.take<double>(34);
+  double *trace = ar.take<double>(34);
+  double *w = ar.take<double>(34);
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  Arena rest = ar;
+  int rc = chi0_run(X, d, eps, mu, D, tau, ntau, cw, nfreq, mode, chi0, proj, rest, err, st);
+  if (rc) return rc;
+  rest = ar;
+  rc = dyson_run(chi0, naux, nfreq, 0, logdet, trace, info_host, nullptr, rest, st);
+  if (rc && rc != MBPT_ERR_NOT_SPD) return rc;
+  cudaMemcpyAsync(w, ow, sizeof(double) * nfreq, cudaMemcpyHostToDevice, st);
+  launch_energy_sum(logdet, trace, w, nfreq, e_c, st);
+  if (cudaGetLastError() != cudaSuccess) return MBPT_ERR_CUDA;
+  return rc;
+}
+
+int mbpt_transform(const double *in, int K, int64_t n, const double *w_dev, int J,
+                   double *out, void *stream) {
+  if (K < 1 || J < 1 || K > 34 || J > 34 || n < 1) return MBPT_ERR_SHAPE;
+  cudaStream_t st = S(stream);
+  launch_transform<double>(in, n * n, n, n, n, w_dev, J, K, out, n * n, n, st);
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+size_t mbpt_sigma_workspace_bytes(int64_t M, int64_t norb, int64_t nocc, int64_t naux, int ntau,
+                                  int nstates, int mode) {
+  Dims d(M, norb, nocc, naux);
+  Arena ar;
+  ar.counting = true;
+  carve_sigma(ar, d, ntau, nstates, mode);
+  return ar.used + 2048;
+}
+
+int mbpt_sigma_branch_sums(const double *X, int64_t M, int64_t norb, int64_t nocc,
+                           const double *eps, double mu, const double *D, int64_t naux,
+                           const double *Wt, const double *tau, int ntau,
+                           const int64_t *states, int nstates, int mode, double *branch,
+                           void *ws, size_t ws_bytes, int *err, void *stream) {
+  Dims d(M, norb, nocc, naux);
+  if (!d.ok() || ntau < 1 || nstates < 1) return MBPT_ERR_SHAPE;
+  if (mode != MBPT_MODE_FP64 && mode != MBPT_MODE_MIXED) return MBPT_ERR_UNSUPPORTED;
+  Arena ar = arena(ws, ws_bytes);
+  return sigma_run(X, d, eps, mu, D, Wt, tau, ntau, states, nstates, mode, branch, ar, err,
+                   S(stream));
+}
+
+int mbpt_sigma_frequency(const double *branch, int ntau, int nstates, const double *C_dev,
+                         const double *S_dev, int npade, double *sigma, void *stream) {
+  if (ntau < 1 || nstates < 1 || npade < 1) return MBPT_ERR_SHAPE;
+  launch_sigma_frequency(branch, ntau, nstates, C_dev, S_dev, npade, sigma, S(stream));
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+int mbpt_qp_solve(const double *sigma, const double *pade_freq_host, int npade,
+                  const double *eps_anchor, const double *xc, const int64_t *states,
+                  int nstates, int64_t nocc, double mu, int greedy, const double *warm,
+                  double *roots, double *z, int *flags, int *evals, void *ws, size_t ws_bytes,
+                  void *stream) {
+  if (npade < 2 || npade > 32) return MBPT_ERR_SHAPE;
+  cudaStream_t st = S(stream);
+  Arena ar = arena(ws, ws_bytes);
+  double *pf = ar.take<double>(npade);
+  if (!pf || ar.overflow()) return MBPT_ERR_WORKSPACE;
+  cudaMemcpyAsync(pf, pade_freq_host, sizeof(double) * npade, cudaMemcpyHostToDevice, st);
+  return launch_pade_qp(sigma, pf, npade, eps_anchor, xc, states, nstates, nocc, mu, greedy,
+                        warm, roots, z, flags, evals, st);
+}
+
+size_t mbpt_chi0_backward_workspace_bytes(int64_t M, int64_t norb, int64_t nocc, int64_t naux,
+                                          int mode) {
+  (void)mode;
+  Dims d(M, norb, nocc, naux);
+  Arena ar;
+  ar.counting = true;
+  carve_back(ar, d);
+  return ar.used + 2048;
+}
+
+int mbpt_chi0_backward(const double *pbar, const double *X, int64_t M, int64_t norb,
+                       int64_t nocc, const double *eps, double mu, const double *D,
+                       int64_t naux, const double *tau, int ntau, int mode, double *eps_bar,
+                       double *X_bar, double *D_bar, void *ws, size_t ws_bytes, int *err,
+                       void *stream) {
+  (void)err;
+  Dims d(M, norb, nocc, naux);
+  if (!d.ok() || ntau < 1) return MBPT_ERR_SHAPE;
+  if (mode != MBPT_MODE_FP64) return MBPT_ERR_UNSUPPORTED;
+  Arena ar = arena(ws, ws_bytes);
+  return back_run(pbar, X, d, eps, mu, D, tau, ntau, eps_bar, X_bar, D_bar, ar, S(stream));
+}
+
+int mbpt_energy_adjoint_seed(double *wmi, int64_t naux, int nfreq, const double *ow_dev,
+                             void *stream) {
+  if (naux < 1 || nfreq < 1) return MBPT_ERR_SHAPE;
+  launch_chi0_bar_seed(wmi, naux, nfreq, ow_dev, S(stream));
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+size_t mbpt_gemm_split_workspace_bytes(int64_t m, int64_t n, int64_t k) {
+  const int64_t mp = round_up(m, 128), np = round_up(n, 128), kp = round_up(k, 64);
+  Arena ar;
+  ar.counting = true;
+  ar.take<bf16>(2 * mp * kp);
+  ar.take<bf16>(2 * np * kp);
+  ar.take<float>(mp * np);
+  return ar.used + 8192;
+}
+
+int mbpt_gemm_split(const double *A, const double *B, int64_t m, int64_t n, int64_t k,
+                    double alpha, float *C, int64_t ldc, void *ws, size_t ws_bytes, int *err,
+                    void *stream) {
+  if (m < 1 || n < 1 || k < 1 || ldc < n) return MBPT_ERR_SHAPE;
+  cudaStream_t st = S(stream);
+  const int64_t mp = round_up(m, 128), np = round_up(n, 128), kp = round_up(k, 64);
+  Arena ar = arena(ws, ws_bytes);
+  bf16 *a_hi = ar.take<bf16>(mp * kp), *a_lo = ar.take<bf16>(mp * kp);
+  bf16 *b_hi = ar.take<bf16>(np * kp), *b_lo = ar.take<bf16>(np * kp);
+  float *c = ar.take<float>(mp * np);
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  launch_split_pad<double>(A, m, k, k, 1.f, a_hi, a_lo, kp, mp, kp, false, st);
+  launch_split_pad<double>(B, n, k, k, 1.f, b_hi, b_lo, kp, np, kp, false, st);
+  SplitMat Am{a_hi, a_lo, mp, kp, kp}, Bm{b_hi, b_lo, np, kp, kp};
+  umma::EpiArgs e;
+  e.outf = c;
+  e.ld_outf = np;
+  e.alpha = static_cast<float>(alpha);
+  int rc = gemm_split(umma::EPI_F32, 1, &Am, &Bm, mp, np, e, err, st);
+  if (rc) return rc;
+  cudaMemcpy2DAsync(C, sizeof(float) * ldc, c, sizeof(float) * np, sizeof(float) * n, m,
+                    cudaMemcpyDeviceToDevice, st);
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+}  // extern "C"

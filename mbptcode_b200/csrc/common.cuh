@@ -1,0 +1,59 @@
+// Shared definitions of the libmbpt_b200 kernels: status codes, bounded waits,
+// BF16 split helpers. sm_100a only.
+#pragma once
+#include <cstdint>
+#include <cstddef>
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+#include "../../include/mbpt_b200.h"
+
+namespace mbpt {
+
+using bf16 = __nv_bfloat16;
+
+// A device-side wait gives up after this many nanoseconds of wall time
+// (%globaltimer) and reports MBPT_ERR_TIMEOUT through the call's error word.
+constexpr uint64_t kWaitLimitNs = 4000000000ull;
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// x = hi + lo with hi = bf16(x), lo = bf16(x - hi): 16 significant bits.
+__device__ __forceinline__ void split_bf16(float x, bf16 &hi, bf16 &lo) {
+  hi = __float2bfloat16_rn(x);
+  lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+}
+
+__host__ __device__ __forceinline__ int64_t round_up(int64_t x, int64_t m) {
+  return (x + m - 1) / m * m;
+}
+
+// Error word written by kernels that detect a failure on the device (a wait
+// that ran out). Zeroed by the host before a call, read back after it.
+struct DevErr {
+  int *word;
+  __device__ __forceinline__ void set(int code) const {
+    if (word) atomicCAS(word, 0, code);
+  }
+};
+
+// Number of this library's kernels launched by the process (instrumentation).
+void count_launch(int n = 1);
+
+}  // namespace mbpt
+
+#define MBPT_CUDA(call)                                                    \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess) return MBPT_ERR_CUDA;                             \
+  } while (0)
+
+#define MBPT_LAUNCH_CHECK()                                                  \
+  do {                                                                       \
+    cudaError_t e_ = cudaGetLastError();                                     \
+    if (e_ != cudaSuccess) return MBPT_ERR_CUDA;                             \
+  } while (0)

@@ -1,0 +1,159 @@
+// Host side of the tcgen05 split GEMM engine: TMA tensor maps and launches.
+#include <cudaTypedefs.h>
+#include <mutex>
+#include <vector>
+
+#include "internal.h"
+
+namespace mbpt {
+bool timing_begin(cudaStream_t st, cudaEvent_t *a, cudaEvent_t *b);
+void timing_end(cudaStream_t st, int epi, cudaEvent_t a, cudaEvent_t b);
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void *p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// rows x cols BF16 matrix (cols contiguous), boxes of 64 columns x box_rows.
+bool make_tmap(CUtensorMap *m, const bf16 *base, int64_t rows, int64_t cols, int64_t ld,
+               int box_rows) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld * 2) % 16 || cols % umma::BK) return false;
+  cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+  cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld * 2)};
+  cuuint32_t box[2] = {static_cast<cuuint32_t>(umma::BK), static_cast<cuuint32_t>(box_rows)};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(base), dims,
+                  strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <int NACC, int BN, int EPI>
+int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
+           const umma::EpiArgs &e, int *err, cudaStream_t st) {
+  using L = umma::Layout<NACC, BN>;
+  if (m_rows % umma::BM || n_rows % BN || m_rows <= 0 || n_rows <= 0) return MBPT_ERR_SHAPE;
+  umma::Params<NACC> p;
+  for (int j = 0; j < NACC; ++j) {
+    if (A[j].cols != B[j].cols || A[j].cols <= 0 || A[j].rows < m_rows || B[j].rows < n_rows)
+      return MBPT_ERR_SHAPE;
+    if (!make_tmap(&p.tm[4 * j + 0], A[j].hi, A[j].rows, A[j].cols, A[j].ld, umma::BM) ||
+        !make_tmap(&p.tm[4 * j + 1], A[j].lo, A[j].rows, A[j].cols, A[j].ld, umma::BM) ||
+        !make_tmap(&p.tm[4 * j + 2], B[j].hi, B[j].rows, B[j].cols, B[j].ld, BN) ||
+        !make_tmap(&p.tm[4 * j + 3], B[j].lo, B[j].rows, B[j].cols, B[j].ld, BN))
+      return MBPT_ERR_SHAPE;
+    p.k_tiles[j] = static_cast<int>(A[j].cols / umma::BK);
+  }
+  p.tiles_m = static_cast<int>(m_rows / umma::BM);
+  p.tiles_n = static_cast<int>(n_rows / BN);
+  p.epi = e;
+  p.err = err;
+  auto kern = umma::gemm_split_kernel<NACC, BN, EPI>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kSmemBytes) !=
+        cudaSuccess)
+      return MBPT_ERR_CUDA;
+    attr_set = true;
+  }
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  const bool timed = timing_begin(st, &ev0, &ev1);
+  count_launch();
+  kern<<<p.tiles_m * p.tiles_n, 192, L::kSmemBytes, st>>>(p);
+  if (timed) timing_end(st, EPI, ev0, ev1);
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+}  // namespace
+
+// ---- optional per-launch timing of the engine (CUDA events on the stream) ----
+namespace {
+struct Timing {
+  std::mutex mu;
+  bool on = false;
+  struct Rec {
+    int epi;
+    cudaEvent_t a, b;
+  };
+  std::vector<Rec> pending;
+  double total_ms[8] = {0};
+  long long launches[8] = {0};
+};
+Timing &timing() {
+  static Timing t;
+  return t;
+}
+}  // namespace
+
+bool timing_begin(cudaStream_t st, cudaEvent_t *a, cudaEvent_t *b) {
+  Timing &t = timing();
+  std::lock_guard<std::mutex> g(t.mu);
+  if (!t.on) return false;
+  cudaEventCreate(a);
+  cudaEventCreate(b);
+  cudaEventRecord(*a, st);
+  return true;
+}
+
+void timing_end(cudaStream_t st, int epi, cudaEvent_t a, cudaEvent_t b) {
+  Timing &t = timing();
+  cudaEventRecord(b, st);
+  std::lock_guard<std::mutex> g(t.mu);
+  t.pending.push_back({epi, a, b});
+}
+
+int gemm_timing(int enable, double *total_ms, long long *launches) {
+  Timing &t = timing();
+  std::lock_guard<std::mutex> g(t.mu);
+  for (auto &r : t.pending) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(r.b) != cudaSuccess) return MBPT_ERR_CUDA;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    t.total_ms[r.epi & 7] += ms;
+    t.launches[r.epi & 7] += 1;
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  t.pending.clear();
+  if (total_ms && launches) {
+    for (int i = 0; i < 8; ++i) {
+      total_ms[i] = t.total_ms[i];
+      launches[i] = t.launches[i];
+      t.total_ms[i] = 0;
+      t.launches[i] = 0;
+    }
+  }
+  t.on = enable != 0;
+  return MBPT_OK;
+}
+
+int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t m_rows,
+               int64_t n_rows, const umma::EpiArgs &e, int *err, cudaStream_t st) {
+  using namespace umma;
+  if (nacc == 1 && epi == EPI_SPLIT) return launch<1, 128, EPI_SPLIT>(A, B, m_rows, n_rows, e, err, st);
+  if (nacc == 1 && epi == EPI_F32) return launch<1, 128, EPI_F32>(A, B, m_rows, n_rows, e, err, st);
+  if (nacc == 1 && epi == EPI_F32_ACC)
+    return launch<1, 128, EPI_F32_ACC>(A, B, m_rows, n_rows, e, err, st);
+  if (nacc == 2 && epi == EPI_HADAMARD_SPLIT)
+    return launch<2, 128, EPI_HADAMARD_SPLIT>(A, B, m_rows, n_rows, e, err, st);
+  if (nacc == 3 && epi == EPI_SIGMA_H)
+    return launch<3, 128, EPI_SIGMA_H>(A, B, m_rows, n_rows, e, err, st);
+  if (nacc == 2 && epi == EPI_ROWDOT2)
+    return launch<2, 128, EPI_ROWDOT2>(A, B, m_rows, n_rows, e, err, st);
+  return MBPT_ERR_UNSUPPORTED;
+}
+
+}  // namespace mbpt

@@ -1,0 +1,83 @@
+// Internal (C++) interface between the route orchestration and the kernels.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include "umma_gemm.cuh"
+
+namespace mbpt {
+
+// A BF16 split operand: rows x cols (cols = K, contiguous), leading dim ld.
+struct SplitMat {
+  const bf16 *hi = nullptr, *lo = nullptr;
+  int64_t rows = 0, cols = 0, ld = 0;
+};
+
+// C (m_rows x n_rows tile grid, both multiples of 128) from nacc problems
+// A[j] B[j]^T with the fused epilogue `epi`.
+int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t m_rows,
+               int64_t n_rows, const umma::EpiArgs &e, int *err, cudaStream_t st);
+
+// Per-epilogue totals of the engine's launch times (enable = 1 starts
+// recording; a call with non-null outputs drains, returns and resets them).
+int gemm_timing(int enable, double *total_ms, long long *launches);
+
+// Bump allocator over a caller's workspace (1024-byte aligned slices).
+struct Arena {
+  uint8_t *base = nullptr;
+  size_t size = 0, used = 0;
+  bool counting = false;  // size-query mode: hand out nothing, count bytes
+  template <typename T>
+  T *take(size_t count) {
+    size_t off = (used + 1023) & ~static_cast<size_t>(1023);
+    size_t bytes = count * sizeof(T);
+    used = off + bytes;
+    if (counting) return nullptr;
+    if (used > size) return nullptr;
+    return reinterpret_cast<T *>(base + off);
+  }
+  bool overflow() const { return !counting && used > size; }
+};
+
+// ---- elementwise / bandwidth kernels (kernels.cu) ----
+template <typename T>
+void launch_split_pad(const T *src, int64_t rows, int64_t cols, int64_t ld_src, float scale,
+                      bf16 *hi, bf16 *lo, int64_t ld_dst, int64_t rows_p, int64_t cols_p,
+                      bool transpose, cudaStream_t st);
+void launch_prep_branches(const double *X, int64_t M, int64_t n, int64_t nocc,
+                          const double *eps, double mu, double tau, bf16 *o_hi, bf16 *o_lo,
+                          int64_t ld_o, bf16 *v_hi, bf16 *v_lo, int64_t ld_v, int64_t Mp,
+                          cudaStream_t st);
+void launch_scaled_branches(const double *X, int64_t M, int64_t n, int64_t nocc,
+                            const double *eps, double mu, double tau, double power,
+                            double *Xo_s, double *Xv_s, cudaStream_t st);
+void launch_hadamard(double *a, const double *b, int64_t n, cudaStream_t st);
+void launch_hadamard3(double *out, const double *a, const double *b, int64_t n, cudaStream_t st);
+// out[j] = sum_k w[j,k] in[k] over a rows x cols block of each slice
+template <typename Tin>
+void launch_transform(const Tin *in, int64_t in_slice, int64_t ld_in, int64_t rows,
+                      int64_t cols, const double *w_dev, int J, int K, double *out,
+                      int64_t out_slice, int64_t ld_out, cudaStream_t st);
+void launch_transform_split(const double *in, int64_t in_slice, int64_t ld_in, int64_t rows,
+                            int64_t cols, const double *w_dev, int J, int K, bf16 *out_hi,
+                            bf16 *out_lo, int64_t out_slice, int64_t ld_out, cudaStream_t st);
+void launch_one_minus(double *a, int64_t n, int nmat, double *trace, cudaStream_t st);
+void launch_logdet_diag(const double *L, int64_t n, int nmat, double *logdet,
+                        cudaStream_t st);
+void launch_symmetrize_minus_identity(double *a, int64_t n, int nmat, cudaStream_t st);
+void launch_rowdot(const double *R, int64_t ld_r, const double *Xs, int64_t ld_x, int64_t M,
+                   int64_t S, double sign, double *out, cudaStream_t st);
+void launch_gather_cols_f32(const double *X, int64_t M, int64_t n, const int64_t *states,
+                            int64_t S, float *xs, int64_t ld_xs, int64_t Mp, cudaStream_t st);
+void launch_gather_cols_split_t(const double *X, int64_t M, int64_t n, const int64_t *states,
+                                int64_t S, bf16 *hi, bf16 *lo, int64_t ld, int64_t Sp,
+                                int64_t Mp, cudaStream_t st);
+void launch_gather_cols_f64(const double *X, int64_t M, int64_t n, const int64_t *states,
+                            int64_t S, double *xs, cudaStream_t st);
+void launch_sigma_frequency(const double *branch, int ntau, int nstates, const double *C,
+                            const double *S, int npade, double *sigma, cudaStream_t st);
+void launch_energy_sum(const double *logdet, const double *trace, const double *w, int nfreq,
+                       double *e_c, cudaStream_t st);
+void launch_fill(double *a, double v, int64_t n, cudaStream_t st);
+
+}  // namespace mbpt

@@ -1,0 +1,394 @@
+// Split-precision tensor-core GEMM engine for sm_100a (tcgen05 + TMA + TMEM).
+//
+// Every product of the route's N^3 sweeps is C = A B^T with A (m x K) and
+// B (n x K) both K-contiguous, each operand held as a BF16 pair x = hi + lo.
+// One CTA owns a 128 x BN output tile and up to three accumulators in TMEM
+// (each its own (A, B, K) problem, e.g. G_occ, G_virt and Zt of the same grid
+// tile). Per 64-wide K slab it issues three tcgen05.mma per 16-wide step,
+// hi*hi + hi*lo + lo*hi, all into the same FP32 accumulator (the lo*lo term,
+// 2^-18 relative, is dropped). Warp roles: warp 0 issues the TMA loads
+// (128B swizzle, no multicast), warp 1 owns TMEM and issues the MMAs, warps
+// 2-5 run the fused epilogue (Hadamard products, BF16 re-split, FP32 stores
+// or the self-energy row contraction). Every mbarrier wait is bounded: on
+// timeout the kernel records MBPT_ERR_TIMEOUT, drains and returns.
+#pragma once
+#include <cuda.h>
+#include "common.cuh"
+
+namespace mbpt {
+namespace umma {
+
+constexpr int BM = 128;
+constexpr int BK = 64;  // BF16 elements per 128-byte swizzle row
+constexpr int kGroupM = 8;
+
+enum Epi : int {
+  EPI_SPLIT = 0,           // out0 = alpha * acc0, BF16 hi/lo
+  EPI_F32 = 1,             // outf = alpha * acc0, FP32
+  EPI_HADAMARD_SPLIT = 2,  // out0 = acc0 o acc1, BF16 hi/lo   (Pi = Go o Gv)
+  EPI_SIGMA_H = 3,         // out0 = acc1 o acc0, out1 = acc2 o acc0 (Go o Zt, Gv o Zt)
+  EPI_ROWDOT2 = 4,         // sig0[c] += sum_r xs[r,c] acc0[r,c], sig1[c] -= ... acc1
+  EPI_F32_ACC = 5,         // outf += alpha * acc0, FP32 read-modify-write
+};
+
+struct EpiArgs {
+  bf16 *out0_hi = nullptr, *out0_lo = nullptr, *out1_hi = nullptr, *out1_lo = nullptr;
+  int64_t ld_out = 0;
+  float *outf = nullptr;
+  int64_t ld_outf = 0;
+  float alpha = 1.f;
+  const float *xs = nullptr;
+  int64_t ld_xs = 0;
+  double *sig0 = nullptr, *sig1 = nullptr;
+};
+
+template <int NACC>
+struct Params {
+  CUtensorMap tm[4 * NACC];  // per accumulator: A hi, A lo, B hi, B lo
+  int k_tiles[NACC];
+  int tiles_m, tiles_n;
+  EpiArgs epi;
+  int *err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: false once kWaitLimitNs have passed without the phase flipping.
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
+  if (mbar_try_wait(b, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (true) {
+#pragma unroll 1
+    for (int i = 0; i < 64; ++i)
+      if (mbar_try_wait(b, parity)) return true;
+    if (global_ns() - t0 > kWaitLimitNs) return false;
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *tm, int x, int y,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), Blackwell descriptor version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4);
+  d |= static_cast<uint64_t>(1) << 16;
+  d |= static_cast<uint64_t>(1024 >> 4) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  d |= static_cast<uint64_t>(2) << 61;
+  return d;
+}
+
+// Instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t idesc_bf16(int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(n >> 3) << 17) |
+         (static_cast<uint32_t>(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db,
+                                         uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+// 32 consecutive FP32 columns of this thread's TMEM lane, waited on in place.
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(addr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void store_split32(bf16 *hi, bf16 *lo, const float (&v)[32]) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    __align__(16) bf16 h[8];
+    __align__(16) bf16 l[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) split_bf16(v[8 * q + i], h[i], l[i]);
+    reinterpret_cast<uint4 *>(hi)[q] = *reinterpret_cast<const uint4 *>(h);
+    reinterpret_cast<uint4 *>(lo)[q] = *reinterpret_cast<const uint4 *>(l);
+  }
+}
+
+// Lane l ends with the warp sum of column l of the 32 x 32 block v (row = lane).
+__device__ __forceinline__ float warp_column_sum(float (&v)[32], int lane) {
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    const bool upper = (lane & s) != 0;
+#pragma unroll
+    for (int i = 0; i < s; ++i) {
+      const float send = upper ? v[i] : v[i + s];
+      const float keep = upper ? v[i + s] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+    }
+  }
+  return v[0];
+}
+
+template <int NACC, int BN>
+struct Layout {
+  static constexpr int kABytes = BM * BK * 2;
+  static constexpr int kBBytes = BN * BK * 2;
+  static constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
+  static constexpr int kStages = (kStageBytes <= 64 * 1024) ? 3 : 2;
+  static constexpr int kSmemBytes = kStages * kStageBytes + 1024 + 256;
+  static constexpr int kTmemCols = (NACC * BN <= 32) ? 32 : (NACC * BN <= 64) ? 64
+                                   : (NACC * BN <= 128) ? 128 : (NACC * BN <= 256) ? 256 : 512;
+  static_assert(NACC * BN <= 512, "accumulators exceed TMEM");
+};
+
+template <int NACC, int BN, int EPI>
+__global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constant__ Params<NACC> p) {
+  using L = Layout<NACC, BN>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + L::kStages * L::kStageBytes);
+  uint64_t *empty = full + L::kStages;
+  uint64_t *accum = empty + L::kStages;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(accum + 1);
+  int *fail = reinterpret_cast<int *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // grouped raster: kGroupM row tiles sweep the column tiles together (L2 reuse)
+  const int pid = blockIdx.x;
+  const int per_group = kGroupM * p.tiles_n;
+  const int first_m = (pid / per_group) * kGroupM;
+  const int gsize = min(p.tiles_m - first_m, kGroupM);
+  const int tm = first_m + (pid % per_group) % gsize;
+  const int tn = (pid % per_group) / gsize;
+  const int m0 = tm * BM, n0 = tn * BN;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < L::kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accum, 1);
+    *fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(L::kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int it = 0;
+      bool ok = true;
+      for (int j = 0; j < NACC && ok; ++j) {
+        for (int kt = 0; kt < p.k_tiles[j]; ++kt, ++it) {
+          const int s = it % L::kStages;
+          const uint32_t ph = (it / L::kStages) & 1;
+          if (!mbar_wait(&empty[s], ph ^ 1)) { ok = false; break; }
+          mbar_expect_tx(&full[s], L::kStageBytes);
+          uint8_t *st = smem + s * L::kStageBytes;
+          tma_load_2d(st, &p.tm[4 * j + 0], kt * BK, m0, &full[s]);
+          tma_load_2d(st + L::kABytes, &p.tm[4 * j + 1], kt * BK, m0, &full[s]);
+          tma_load_2d(st + 2 * L::kABytes, &p.tm[4 * j + 2], kt * BK, n0, &full[s]);
+          tma_load_2d(st + 2 * L::kABytes + L::kBBytes, &p.tm[4 * j + 3], kt * BK, n0,
+                      &full[s]);
+        }
+      }
+      if (!ok) {
+        atomicExch(fail, 1);
+        DevErr{p.err}.set(MBPT_ERR_TIMEOUT);
+      }
+      // drain: every load issued lands before the CTA may exit
+      const int issued = it;
+      for (int q = max(0, issued - L::kStages); q < issued; ++q)
+        mbar_wait(&full[q % L::kStages], (q / L::kStages) & 1);
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_bf16(BN);
+      int it = 0;
+      bool ok = true;
+      for (int j = 0; j < NACC && ok; ++j) {
+        const uint32_t d = tmem + static_cast<uint32_t>(j * BN);
+        for (int kt = 0; kt < p.k_tiles[j]; ++kt, ++it) {
+          const int s = it % L::kStages;
+          const uint32_t ph = (it / L::kStages) & 1;
+          if (!mbar_wait(&full[s], ph) || *reinterpret_cast<volatile int *>(fail)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          uint8_t *st = smem + s * L::kStageBytes;
+          const uint64_t a_hi = sw128_desc(smem_u32(st));
+          const uint64_t a_lo = sw128_desc(smem_u32(st + L::kABytes));
+          const uint64_t b_hi = sw128_desc(smem_u32(st + 2 * L::kABytes));
+          const uint64_t b_lo = sw128_desc(smem_u32(st + 2 * L::kABytes + L::kBBytes));
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+            const uint64_t adv = static_cast<uint64_t>(kk * 2);  // 32 bytes >> 4
+            mma_bf16(d, a_hi + adv, b_hi + adv, idesc, (kt > 0 || kk > 0) ? 1u : 0u);
+            mma_bf16(d, a_hi + adv, b_lo + adv, idesc, 1u);
+            mma_bf16(d, a_lo + adv, b_hi + adv, idesc, 1u);
+          }
+          mma_commit(&empty[s]);
+        }
+      }
+      if (!ok) {
+        atomicExch(fail, 1);
+        DevErr{p.err}.set(MBPT_ERR_TIMEOUT);
+      }
+      mma_commit(accum);
+      mbar_wait(accum, 0);  // no MMA may still write TMEM when it is freed
+    }
+    __syncwarp();
+  } else {
+    // epilogue: warps 2..5 own TMEM lane quarters (warp % 4)
+    const int sp = warp & 3;
+    const bool ok = mbar_wait(accum, 0) && !*reinterpret_cast<volatile int *>(fail);
+    __syncwarp();
+    if (!ok) {
+      if (lane == 0) DevErr{p.err}.set(MBPT_ERR_TIMEOUT);
+    } else {
+      tc_fence_after();
+      const int row = m0 + sp * 32 + lane;
+      const uint32_t taddr = tmem + (static_cast<uint32_t>(sp * 32) << 16);
+      const EpiArgs &e = p.epi;
+#pragma unroll 1
+      for (int c = 0; c < BN; c += 32) {
+        const int col = n0 + c;
+        float v0[32];
+        tmem_ld32(taddr + c, v0);
+        if constexpr (EPI == EPI_SPLIT) {
+#pragma unroll
+          for (int i = 0; i < 32; ++i) v0[i] *= e.alpha;
+          store_split32(e.out0_hi + row * e.ld_out + col, e.out0_lo + row * e.ld_out + col, v0);
+        } else if constexpr (EPI == EPI_F32 || EPI == EPI_F32_ACC) {
+          float4 *dst = reinterpret_cast<float4 *>(e.outf + row * e.ld_outf + col);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            float4 o = make_float4(e.alpha * v0[4 * q], e.alpha * v0[4 * q + 1],
+                                   e.alpha * v0[4 * q + 2], e.alpha * v0[4 * q + 3]);
+            if constexpr (EPI == EPI_F32_ACC) {
+              const float4 prev = dst[q];
+              o.x += prev.x; o.y += prev.y; o.z += prev.z; o.w += prev.w;
+            }
+            dst[q] = o;
+          }
+        } else if constexpr (EPI == EPI_HADAMARD_SPLIT) {
+          float v1[32];
+          tmem_ld32(taddr + BN + c, v1);
+#pragma unroll
+          for (int i = 0; i < 32; ++i) v0[i] *= v1[i];
+          store_split32(e.out0_hi + row * e.ld_out + col, e.out0_lo + row * e.ld_out + col, v0);
+        } else if constexpr (EPI == EPI_SIGMA_H) {
+          float v1[32];
+          tmem_ld32(taddr + BN + c, v1);
+#pragma unroll
+          for (int i = 0; i < 32; ++i) v1[i] *= v0[i];
+          store_split32(e.out0_hi + row * e.ld_out + col, e.out0_lo + row * e.ld_out + col, v1);
+          tmem_ld32(taddr + 2 * BN + c, v1);
+#pragma unroll
+          for (int i = 0; i < 32; ++i) v1[i] *= v0[i];
+          store_split32(e.out1_hi + row * e.ld_out + col, e.out1_lo + row * e.ld_out + col, v1);
+        } else if constexpr (EPI == EPI_ROWDOT2) {
+          float v1[32], xs[32];
+          tmem_ld32(taddr + BN + c, v1);
+          const float4 *src = reinterpret_cast<const float4 *>(e.xs + row * e.ld_xs + col);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const float4 t = src[q];
+            xs[4 * q] = t.x; xs[4 * q + 1] = t.y; xs[4 * q + 2] = t.z; xs[4 * q + 3] = t.w;
+          }
+#pragma unroll
+          for (int i = 0; i < 32; ++i) {
+            v0[i] *= xs[i];
+            v1[i] *= xs[i];
+          }
+          const float s0 = warp_column_sum(v0, lane);
+          const float s1 = warp_column_sum(v1, lane);
+          atomicAdd(e.sig0 + col + lane, static_cast<double>(s0));
+          atomicAdd(e.sig1 + col + lane, -static_cast<double>(s1));
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(L::kTmemCols)
+                 : "memory");
+  }
+}
+
+}  // namespace umma
+}  // namespace mbpt

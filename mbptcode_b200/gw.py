@@ -1,0 +1,273 @@
+"""Space-time G0W0 on the B200: W(tau), the correlation self-energy diagonal,
+the Pade continuation and the quasiparticle roots.
+
+Mirrors MBPTcode's route (``src/SingleReference/GW/space_time.py:631-863``,
+restricted, serial, in core) and its helpers
+``GW/imaginary_time.py:181-195, 403-587`` and ``GW/qp_solve.py:529-703``;
+all arithmetic runs in libmbpt_b200.
+"""
+from __future__ import annotations
+
+import time
+import warnings
+
+import numpy as np
+import torch
+
+from ._lib import WORKSPACE, check, host_array, lib, ptr, require_device, stream_ptr
+from .grids import space_time_axes
+from .space_time import (_Err, _eps_host, _mode, check_mixed_weights, chi0_sweep,
+                         dyson_batch, to_device, transform)
+
+QP_FLAG_QUASIPARTICLE, QP_FLAG_NO_ROOT, QP_FLAG_Z_OUTSIDE, QP_FLAG_PADE_FAILED, \
+    QP_FLAG_WARM, QP_FLAG_OVERFLOW = 1, 2, 4, 8, 16, 32
+
+
+class QPNoRoot(RuntimeWarning):
+    """A quasiparticle equation without a root in its widest scan window."""
+
+
+class QPWeightOutside(RuntimeWarning):
+    """A quasiparticle root kept with Z outside (0, 1]."""
+
+
+def screened_interaction_tau(W_minus_I, Ctw, stream=None):
+    """Wt(tau) = sum_w Ctw[tau, w] (W(i w) - I): ``imaginary_time.py:181-195``
+    (here from W - I as the Dyson step leaves it), FP64 on the device."""
+    return transform(W_minus_I, Ctw, stream)
+
+
+def sigma_branch_sums(X, D, Wt, eps, nocc, tau_points, states, mu, precision=None,
+                      stream=None):
+    """(2, ntau, nstates) device tensor: Sigma^<_pp(tau) and Sigma^>_pp(tau) of
+    the states, the diagonal form of ``imaginary_time.py:39-92``."""
+    dev = Wt.device
+    Xd, Dd = to_device(X, dev), to_device(D, dev)
+    eps_h = _eps_host(eps)
+    ed = to_device(eps_h, dev)
+    M, norb = Xd.shape
+    naux = Dd.shape[1]
+    st = torch.as_tensor(np.asarray(states, dtype=np.int64), device=dev)
+    S = st.numel()
+    tau_h, tp = host_array(tau_points)
+    ntau = len(tau_h)
+    if Wt.shape != (ntau, naux, naux):
+        raise ValueError(f'Wt is {tuple(Wt.shape)}, need ({ntau}, {naux}, {naux})')
+    mode = _mode(precision)
+    branch = torch.empty((2, ntau, S), dtype=torch.float64, device=dev)
+    ws = WORKSPACE.get(lib().mbpt_sigma_workspace_bytes(M, norb, nocc, naux, ntau, S, mode), dev)
+    err = _Err(dev)
+    check(lib().mbpt_sigma_branch_sums(ptr(Xd), M, norb, nocc, ptr(ed), float(mu), ptr(Dd),
+                                       naux, ptr(Wt.contiguous()), tp, ntau, ptr(st), S, mode,
+                                       ptr(branch), ptr(ws), ws.numel(), ptr(err.t),
+                                       stream_ptr(stream)), 'mbpt_sigma_branch_sums')
+    err.check('mbpt_sigma_branch_sums')
+    return branch
+
+
+def sigma_frequency(branch, C, S, stream=None):
+    """Sigma_c(i w_p) = -1/2 [C (S> + S<) + i S (S> - S<)] as a complex
+    (nstates, npade) device tensor: ``imaginary_time.py:525-532``."""
+    dev = branch.device
+    ntau, nstates = branch.shape[1], branch.shape[2]
+    Cd = torch.as_tensor(np.ascontiguousarray(C, dtype=np.float64), device=dev)
+    Sd = torch.as_tensor(np.ascontiguousarray(S, dtype=np.float64), device=dev)
+    npade = Cd.shape[0]
+    out = torch.empty((nstates, npade, 2), dtype=torch.float64, device=dev)
+    check(lib().mbpt_sigma_frequency(ptr(branch.contiguous()), ntau, nstates, ptr(Cd), ptr(Sd),
+                                     npade, ptr(out), stream_ptr(stream)),
+          'mbpt_sigma_frequency')
+    return torch.view_as_complex(out)
+
+
+def qp_solve(sigma, pade_freq, eps_anchor, states, nocc, mu, xc=None, greedy=True,
+             warm=None, stream=None):
+    """Roots, Z, flags and Sigma-evaluation counts of the QP equations of all
+    states at once (device tensors): ``qp_solve.py:575-695`` per-state loop
+    with ``:529-558`` and ``Solvers/qp_equation.py:1353-1393``. `warm`
+    (nstates) predicted roots warm-start a Newton solve, the scan remaining
+    the fallback."""
+    dev = sigma.device
+    sig = torch.view_as_real(sigma.contiguous()).contiguous()
+    S, npade = sigma.shape
+    pf_h, pp = host_array(pade_freq)
+    ea = to_device(eps_anchor, dev)
+    st = torch.as_tensor(np.asarray(states, dtype=np.int64), device=dev)
+    xcd = None if xc is None else to_device(np.broadcast_to(np.asarray(xc, float), (S,))
+                                            if not isinstance(xc, torch.Tensor) else xc, dev)
+    wd = None if warm is None else to_device(warm, dev)
+    roots = torch.empty(S, dtype=torch.float64, device=dev)
+    z = torch.empty(S, dtype=torch.float64, device=dev)
+    flags = torch.empty(S, dtype=torch.int32, device=dev)
+    evals = torch.empty(S, dtype=torch.int32, device=dev)
+    ws = WORKSPACE.get(1 << 16, dev)
+    check(lib().mbpt_qp_solve(ptr(sig), pp, npade, ptr(ea), ptr(xcd), ptr(st), S, int(nocc),
+                              float(mu), int(bool(greedy)), ptr(wd), ptr(roots), ptr(z),
+                              ptr(flags), ptr(evals), ptr(ws), ws.numel(), stream_ptr(stream)),
+          'mbpt_qp_solve')
+    return roots, z, flags, evals
+
+
+def _report_flags(flags_h, states):
+    for s, f in zip(np.atleast_1d(states), flags_h):
+        if f & QP_FLAG_NO_ROOT:
+            warnings.warn(f'orbital {int(s)}: the quasiparticle equation has no root in '
+                          f'the widest scan window', QPNoRoot, stacklevel=3)
+        elif f & QP_FLAG_Z_OUTSIDE:
+            warnings.warn(f'orbital {int(s)}: root kept with Z outside (0, 1]',
+                          QPWeightOutside, stacklevel=3)
+
+
+class SweepResult(dict):
+    """Outputs of one chi0 -> W -> Sigma -> QP sweep (device tensors and
+    host arrays), with `timings` in seconds per stage (CUDA events)."""
+
+
+def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=None,
+             eps_anchor=None, xc_diagonal=None, greedy=True, warm=None, keep=False,
+             stream=None, timings=None):
+    """The whole space-time G0W0 sweep on device-resident (or host) inputs.
+
+    Returns a SweepResult with 'roots', 'z', 'flags', 'evals' (device),
+    'sigma' (nstates, npade) complex, 'axes', and with `keep` also 'Wt' and
+    'W_minus_I'. eps_anchor: the spectrum the equation is anchored on (evGW);
+    None is eps. timings: a dict receiving per-stage device times.
+    """
+    dev = require_device()
+    eps_h = _eps_host(eps)
+    n = len(eps_h)
+    states = np.arange(n) if states is None else np.atleast_1d(np.asarray(states, int))
+    if axes is None:
+        axes = space_time_axes(eps_h, nocc, ntau=ntau,
+                               anchor=None if eps_anchor is None else _eps_host(eps_anchor))
+    mu = axes.mu
+    check_mixed_weights(precision, axes.grid.cosft_wt, axes.Ctw, axes.C, axes.S)
+    ev = None
+    if timings is not None:
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        ev[0].record()
+    chi0, _ = chi0_sweep(X, D, eps_h, nocc, axes.grid.tau_points, axes.grid.cosft_wt, mu=mu,
+                         precision=precision, stream=stream)
+    if ev:
+        ev[1].record()
+    logdet, trace, info, _ = dyson_batch(chi0, want_w=True, stream=stream)
+    # E_c from the same factorisations: the frequency axis is a minimax quadrature
+    e_c = torch.empty((), dtype=torch.float64, device=dev)
+    ow = torch.as_tensor(np.asarray(axes.grid.omega_weights, float), device=dev)
+    check(lib().mbpt_energy_sum(ptr(logdet), ptr(trace), ptr(ow), len(ow), ptr(e_c),
+                                stream_ptr(stream)), 'mbpt_energy_sum')
+    if ev:
+        ev[2].record()
+    Wt = screened_interaction_tau(chi0, axes.Ctw, stream)
+    W_minus_I = chi0 if keep else None
+    del chi0
+    branch = sigma_branch_sums(X, D, Wt, eps_h, nocc, axes.tau_sigma, states, mu, precision,
+                               stream)
+    sigma = sigma_frequency(branch, axes.C, axes.S, stream)
+    if ev:
+        ev[3].record()
+    anchor = eps_h if eps_anchor is None else _eps_host(eps_anchor)
+    roots, z, flags, evals = qp_solve(sigma, axes.pade_freq, anchor, states, nocc, mu,
+                                      xc=xc_diagonal, greedy=greedy, warm=warm, stream=stream)
+    if ev:
+        ev[4].record()
+        ev[4].synchronize()
+        for k, name in enumerate(('t_chi0', 't_dyson', 't_sigma', 't_qp')):
+            timings[name] = ev[k].elapsed_time(ev[k + 1]) / 1e3
+        timings['dyson_frequencies'] = axes.grid.nfreq
+        timings['ntau'] = axes.ntau
+    res = SweepResult(roots=roots, z=z, flags=flags, evals=evals, sigma=sigma, axes=axes,
+                      states=states, branch=branch, dyson_info=info, e_c=e_c)
+    if keep:
+        res['Wt'] = Wt
+        res['W_minus_I'] = W_minus_I
+    return res
+
+
+def gw_space_time(X, D, eps, nocc, states=None, ntau='auto', precision=None,
+                  eps_anchor=None, xc_diagonal=None, greedy=True, with_z=False,
+                  failures=None, timings=None):
+    """QP energies (Hartree, host array) of `states`, the equation
+    w = eps_p + xc_p + Re Sigma_c(w) solved for the root of largest Z, on the
+    synthetic or caller-built ISDF factors X (M x norb, MO collocation) and
+    D (M x naux)."""
+    t0 = time.perf_counter()
+    res = gw_sweep(X, D, eps, nocc, states=states, ntau=ntau, precision=precision,
+                   eps_anchor=eps_anchor, xc_diagonal=xc_diagonal, greedy=greedy,
+                   timings=timings)
+    roots = res['roots'].cpu().numpy()
+    z = res['z'].cpu().numpy()
+    flags = res['flags'].cpu().numpy()
+    _report_flags(flags, res['states'])
+    if failures is not None:
+        for s, f in zip(res['states'], flags):
+            if f & QP_FLAG_PADE_FAILED:
+                failures[int(s)] = 'FloatingPointError: greedy Pade ordering failed'
+    if timings is not None:
+        timings['t_total_host'] = time.perf_counter() - t0
+    return (roots, z) if with_z else roots
+
+
+def _factors(factors):
+    if factors is None:
+        raise NotImplementedError(
+            'building the ISDF factors needs pyscf (integrals and the fit); pass '
+            'factors=(X_mo, D) or (X_mo, D, X_ao, coords)')
+    if isinstance(factors, dict):
+        return factors['X_mo'], factors['D']
+    return factors[0], factors[1]
+
+
+def solve_qp_energy_space_time(mf, mol, nocc, p_state, numerics=None, auxbasis=None,
+                               radii=None, factors=None, greedy=True, dm_correction=None,
+                               timings=None, distribute=None, comm=None, freq_block=None,
+                               scratch_dir=None, extras=None, screen_r_cut=None,
+                               sigma_x='mf', eps_anchor=None, sigma_x_matrix=None,
+                               spin_channel='alpha', xc_diagonal=None, with_z=False,
+                               failures=None, counts=None, grid_accuracy=None,
+                               precision=None):
+    """Drop-in for ``GW/space_time.py:631-863`` on a restricted gas-phase
+    reference with pre-built factors: the mean field gives eps (mo_energy);
+    the static term <Sigma_x - v_xc> is `xc_diagonal` (0 on an HF reference,
+    ``qp_solve.py:311``). numerics.quadrature: ntau_st ('auto' or a size),
+    npade and w0_gl. Returns Hartree, a float for a scalar p_state."""
+    for name, val in (('distribute', distribute), ('freq_block', freq_block),
+                      ('scratch_dir', scratch_dir), ('screen_r_cut', screen_r_cut),
+                      ('sigma_x_matrix', sigma_x_matrix), ('extras', extras)):
+        if val:
+            raise NotImplementedError(f'{name} is outside the one-GPU device route')
+    X, D = _factors(factors)
+    eps = np.asarray(getattr(mf, 'mo_energy', mf), float)
+    if eps.ndim != 1:
+        raise NotImplementedError('an unrestricted reference is outside the device route')
+    ntau, pade = 'auto', None
+    if numerics is not None:
+        q = numerics.quadrature
+        ntau = q.ntau_st
+        from .grids import pade_nodes
+        pade = pade_nodes(q.npade, q.w0_gl)
+    states = np.atleast_1d(p_state)
+    axes = space_time_axes(eps, nocc, ntau=ntau, pade_freq=pade,
+                           anchor=None if eps_anchor is None else np.asarray(eps_anchor))
+    res = gw_sweep(X, D, eps, nocc, states=states, axes=axes, precision=precision,
+                   eps_anchor=eps_anchor, xc_diagonal=xc_diagonal, greedy=greedy,
+                   timings=timings)
+    if timings is not None:
+        timings['ntau_auto'] = axes.ntau
+        timings['tau_fit_error'] = axes.tau_fit_error
+    roots = res['roots'].cpu().numpy()
+    z = res['z'].cpu().numpy()
+    _report_flags(res['flags'].cpu().numpy(), states)
+    if counts is not None:
+        counts['sigma_evaluations'] = res['evals'].cpu().numpy()
+    scalar = np.ndim(p_state) == 0
+    if with_z:
+        return (roots[0], z[0]) if scalar else (roots, z)
+    return roots[0] if scalar else roots
+
+
+def solve_qp_diagonal_space_time(mf, mol, nocc, states=None, **kw):
+    """``GW/space_time.py:1091-1105``: (qp energies, states)."""
+    n = len(np.asarray(getattr(mf, 'mo_energy', mf)))
+    states = np.arange(n) if states is None else np.atleast_1d(states)
+    return solve_qp_energy_space_time(mf, mol, nocc, states, **kw), states
