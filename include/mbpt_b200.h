@@ -218,6 +218,30 @@ int mbpt_gemm_split(const double *A_dev, const double *B_dev, int64_t m, int64_t
                     double alpha, float *C_dev, int64_t ldc, void *workspace, size_t ws_bytes,
                     int *err_dev, void *stream);
 
+/* ---- split-precision GEMM without caller scratch -------------------------
+ * No counterpart in MBPTcode: an addition of this library for callers that
+ * cannot allocate device memory, typically hosts whose device memory is all
+ * owned by their own allocator (a framework's caching pool, a fixed memory
+ * budget) and which therefore can neither pass a workspace nor let the
+ * library call cudaMalloc. Same product as mbpt_gemm_split (C = alpha A B^T,
+ * A m x k, B n x k FP64, C FP32 with ldc), but its scratch is a 32 MiB
+ * file-scope device array inside the library, which every GPU that loads
+ * the library holds until the process exits; the call itself allocates
+ * nothing. Limit: the padded operands and product must fit,
+ * 4 (mp kp + np kp) + 4 mp np <= 32 MiB with mp, np = m, n rounded up to
+ * 128 and kp = k rounded up to 64 (each part 1024-byte aligned); larger sizes
+ * return MBPT_ERR_WORKSPACE and compute nothing.
+ * The first call on a device looks up that array's device address (with
+ * the device current) and keeps it; make that first call before any stream
+ * capture. All calls share the one array and each overwrites it: calls whose
+ * work overlaps on the GPU (other streams, other host threads) race and must
+ * be serialised by the caller. mbpt_gemm_split_static_capacity returns the
+ * array's size in bytes. */
+size_t mbpt_gemm_split_static_capacity(void);
+int mbpt_gemm_split_static(const double *A_dev, const double *B_dev, int64_t m, int64_t n,
+                           int64_t k, double alpha, float *C_dev, int64_t ldc, int *err_dev,
+                           void *stream);
+
 #ifdef __cplusplus
 }
 #endif

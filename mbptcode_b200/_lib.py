@@ -56,6 +56,8 @@ _SIGNATURES = {
     'mbpt_mlp_adamw': (_i, [_p, _p, _p, _p, _i, _f, _f, _f, _f, _f, _i, _p]),
     'mbpt_gemm_split_workspace_bytes': (_sz, [_i64, _i64, _i64]),
     'mbpt_gemm_split': (_i, [_p, _p, _i64, _i64, _i64, _d, _p, _i64, _p, _sz, _p, _p]),
+    'mbpt_gemm_split_static_capacity': (_sz, []),
+    'mbpt_gemm_split_static': (_i, [_p, _p, _i64, _i64, _i64, _d, _p, _i64, _p, _p]),
 }
 
 

@@ -16,7 +16,8 @@ CSRC = os.path.join(HERE, 'csrc')
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, 'libmbpt_b200.so')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
-SOURCES = ['gemm_host.cu', 'kernels.cu', 'aux_kernels.cu', 'capi.cu', 'qp.cu', 'mlp.cu']
+SOURCES = ['gemm_host.cu', 'kernels.cu', 'aux_kernels.cu', 'capi.cu', 'qp.cu', 'mlp.cu',
+           'noalloc.cu']
 # files whose arithmetic must round as written (no FMA contraction)
 NO_FMA = {'qp.cu'}
 
