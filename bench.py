@@ -240,8 +240,13 @@ def main():
     clk = clocks.stop() if clocks else None
     ms_step = max_over_ranks(e0.elapsed_time(e1) / args.steps)
 
+    # per-stage device times of one more mixed sweep (outside the timed region)
+    stages = {}
+    gw_sweep(X, D, eps, NOCC, states=states, axes=axes, precision='mixed', timings=stages)
+    stages_fp64 = {}
+
     # ---- the plain FP64 GPU sweep (the >= 5x denominator) ----
-    sweep('fp64')
+    gw_sweep(X, D, eps, NOCC, states=states, axes=axes, precision='fp64', timings=stages_fp64)
     torch.cuda.synchronize()
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     nf = max(1, min(2, args.steps))
@@ -328,6 +333,8 @@ def main():
         'sweeps_per_s': round(world / s_step, 4),
         'fp64_s_per_sweep': round(ms_fp64 / 1e3, 5),
         'speedup_vs_fp64': round(ms_fp64 / ms_step, 3),
+        'stages_s': {k: round(v, 4) for k, v in stages.items() if k.startswith('t_')},
+        'stages_fp64_s': {k: round(v, 4) for k, v in stages_fp64.items() if k.startswith('t_')},
         'accuracy': acc, 'accuracy_other_variant': other,
         'e2e': {'value': round(e2e_s, 5), 'unit': 's', 'h2d_bytes_per_step': int(h2d),
                 'd2h_bytes_per_step': int(d2h)},

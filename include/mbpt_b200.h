@@ -172,6 +172,16 @@ int mbpt_qp_solve(const double *sigma_dev, const double *pade_freq_host, int npa
                   const double *warm_dev, double *roots_dev, double *z_dev, int *flags_dev,
                   int *evals_dev, void *workspace, size_t ws_bytes, void *stream);
 
+/* Re Sigma_c at real frequencies from the same continuation
+ * (analytic_continuation.py:25-31 pade_eval on each state's PadeFit):
+ * out_dev[s, q] = Re Sigma_c(query_dev[s, q]) for the nstates x nq query
+ * frequencies (Hartree); NaN for a state whose greedy ordering failed.
+ * Used for the features of the learned QP warm start (Sigma_c at eps +- 0.1). */
+int mbpt_pade_eval(const double *sigma_dev, const double *pade_freq_host, int npade,
+                   const int64_t *states_dev, int nstates, int64_t nocc, double mu, int greedy,
+                   const double *query_dev, int nq, double *out_dev, void *workspace,
+                   size_t ws_bytes, void *stream);
+
 /* ---- reverse sweep of the polarizability ---------------------------------
  * Replaces gradients/rpa/space_time_adjoint.py:136-218
  * polarizability_backward: for an adjoint proj_bar (ntau, naux, naux) of
@@ -217,6 +227,13 @@ size_t mbpt_gemm_split_workspace_bytes(int64_t m, int64_t n, int64_t k);
 int mbpt_gemm_split(const double *A_dev, const double *B_dev, int64_t m, int64_t n, int64_t k,
                     double alpha, float *C_dev, int64_t ldc, void *workspace, size_t ws_bytes,
                     int *err_dev, void *stream);
+/* The same with TF32 hi/lo pairs (22 significant bits, tcgen05 kind::tf32):
+ * the product form of the chi0 sweep's G_occ / G_virt stage in mixed mode.
+ * k is padded to a multiple of 32. */
+size_t mbpt_gemm_split_tf32_workspace_bytes(int64_t m, int64_t n, int64_t k);
+int mbpt_gemm_split_tf32(const double *A_dev, const double *B_dev, int64_t m, int64_t n,
+                         int64_t k, double alpha, float *C_dev, int64_t ldc, void *workspace,
+                         size_t ws_bytes, int *err_dev, void *stream);
 
 /* ---- split-precision GEMM without caller scratch -------------------------
  * No counterpart in MBPTcode: an addition of this library for callers that

@@ -46,6 +46,7 @@ _SIGNATURES = {
     'mbpt_sigma_frequency': (_i, [_p, _i, _i, _p, _p, _i, _p, _p]),
     'mbpt_qp_solve': (_i, [_p, _p, _i, _p, _p, _p, _i, _i64, _d, _i, _p, _p, _p, _p, _p, _p,
                            _sz, _p]),
+    'mbpt_pade_eval': (_i, [_p, _p, _i, _p, _i, _i64, _d, _i, _p, _i, _p, _p, _sz, _p]),
     'mbpt_chi0_backward_workspace_bytes': (_sz, [_i64, _i64, _i64, _i64, _i]),
     'mbpt_chi0_backward': (_i, [_p, _p, _i64, _i64, _i64, _p, _d, _p, _i64, _p, _i, _i, _p,
                                 _p, _p, _p, _sz, _p, _p]),
@@ -56,6 +57,8 @@ _SIGNATURES = {
     'mbpt_mlp_adamw': (_i, [_p, _p, _p, _p, _i, _f, _f, _f, _f, _f, _i, _p]),
     'mbpt_gemm_split_workspace_bytes': (_sz, [_i64, _i64, _i64]),
     'mbpt_gemm_split': (_i, [_p, _p, _i64, _i64, _i64, _d, _p, _i64, _p, _sz, _p, _p]),
+    'mbpt_gemm_split_tf32_workspace_bytes': (_sz, [_i64, _i64, _i64]),
+    'mbpt_gemm_split_tf32': (_i, [_p, _p, _i64, _i64, _i64, _d, _p, _i64, _p, _sz, _p, _p]),
     'mbpt_gemm_split_static_capacity': (_sz, []),
     'mbpt_gemm_split_static': (_i, [_p, _p, _i64, _i64, _i64, _d, _p, _i64, _p, _p]),
 }

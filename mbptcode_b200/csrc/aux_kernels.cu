@@ -115,6 +115,28 @@ __global__ void diag_kernel(double *a, int64_t n, double *diag, bool save) {
   }
 }
 
+// T (ib x ib, column-major) = the lower triangle of the column-major block at
+// A (leading dimension lda), zeros above the diagonal
+__global__ void lower_copy_kernel(const double *A, int64_t lda, double *T, int ib) {
+  const int64_t total = static_cast<int64_t>(ib) * ib;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t c = i / ib, r = i % ib;
+    T[i] = r >= c ? A[c * lda + r] : 0.0;
+  }
+}
+
+// zero the strict upper triangle of a column-major n x n matrix (the
+// row-major strict lower triangle of the buffer)
+__global__ void zero_strict_upper_cm_kernel(double *a, int64_t n) {
+  const int64_t total = n * n;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t c = i / n, r = i % n;  // column-major (r, c) at c * n + r
+    if (r < c) a[i] = 0.0;
+  }
+}
+
 __global__ void identity_kernel(double *a, int64_t n, double diag_shift, bool set) {
   const int64_t total = n * n;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
@@ -158,6 +180,16 @@ void launch_lu_logdet(const double *LU, const int *piv, int64_t n, double *logde
 void launch_diag(double *a, int64_t n, int nmat, double *diag, bool save, cudaStream_t st) {
   dim3 grid(static_cast<unsigned>((n + 255) / 256), nmat);
   count_launch(); diag_kernel<<<grid, 256, 0, st>>>(a, n, diag, save);
+}
+
+void launch_lower_copy(const double *A, int64_t lda, double *T, int ib, cudaStream_t st) {
+  count_launch();
+  lower_copy_kernel<<<blocks(static_cast<int64_t>(ib) * ib), 256, 0, st>>>(A, lda, T, ib);
+}
+
+void launch_zero_strict_upper_cm(double *a, int64_t n, cudaStream_t st) {
+  count_launch();
+  zero_strict_upper_cm_kernel<<<blocks(n * n), 256, 0, st>>>(a, n);
 }
 
 void launch_identity(double *a, int64_t n, cudaStream_t st) {

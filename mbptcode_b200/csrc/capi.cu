@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <algorithm>
 #include <vector>
 
 #include "internal.h"
@@ -18,6 +19,9 @@ int launch_pade_qp(const double *sigma, const double *pade_freq, int npade,
                    const double *eps_anchor, const double *xc, const int64_t *states,
                    int nstates, int64_t nocc, double mu, int greedy, const double *warm,
                    double *roots, double *z, int *flags, int *evals, cudaStream_t st);
+int launch_pade_eval(const double *sigma, const double *pade_freq, int npade,
+                     const int64_t *states, int nstates, int64_t nocc, double mu, int greedy,
+                     const double *query, int nq, double *out, cudaStream_t st);
 void launch_chi0_bar_seed(double *a, int64_t n, int nfreq, const double *scale,
                           cudaStream_t st);
 void launch_sym_half(const double *in, double *out, int64_t n, cudaStream_t st);
@@ -30,6 +34,8 @@ void launch_lu_logdet(const double *LU, const int *piv, int64_t n, double *logde
 void launch_identity(double *a, int64_t n, cudaStream_t st);
 void launch_minus_identity(double *a, int64_t n, cudaStream_t st);
 void launch_diag(double *a, int64_t n, int nmat, double *diag, bool save, cudaStream_t st);
+void launch_lower_copy(const double *A, int64_t lda, double *T, int ib, cudaStream_t st);
+void launch_zero_strict_upper_cm(double *a, int64_t n, cudaStream_t st);
 
 namespace {
 std::atomic<long long> g_launches{0};
@@ -93,7 +99,8 @@ struct Chi0Bufs {
   // fp64
   double *Xo_s, *Xv_s, *Go, *Gv, *Y, *proj;
   // mixed
-  bf16 *Dt_hi, *Dt_lo, *Yo_hi, *Yo_lo, *Yv_hi, *Yv_lo, *Pi_hi, *Pi_lo, *Z_hi, *Z_lo;
+  bf16 *Dt_hi, *Dt_lo, *Pi_hi, *Pi_lo, *Z_hi, *Z_lo;
+  float *Yo_hi, *Yo_lo, *Yv_hi, *Yv_lo;  // TF32 pairs of the G products
   float *proj32;
   double *eye;  // ntau x ntau identity for the optional proj copy
 };
@@ -111,10 +118,10 @@ Chi0Bufs carve_chi0(Arena &ar, const Dims &d, int ntau, int nfreq, int mode, boo
   } else {
     b.Dt_hi = ar.take<bf16>(d.Ap * d.Mp);
     b.Dt_lo = ar.take<bf16>(d.Ap * d.Mp);
-    b.Yo_hi = ar.take<bf16>(d.Mp * d.Ko);
-    b.Yo_lo = ar.take<bf16>(d.Mp * d.Ko);
-    b.Yv_hi = ar.take<bf16>(d.Mp * d.Kv);
-    b.Yv_lo = ar.take<bf16>(d.Mp * d.Kv);
+    b.Yo_hi = ar.take<float>(d.Mp * d.Ko);
+    b.Yo_lo = ar.take<float>(d.Mp * d.Ko);
+    b.Yv_hi = ar.take<float>(d.Mp * d.Kv);
+    b.Yv_lo = ar.take<float>(d.Mp * d.Kv);
     b.Pi_hi = ar.take<bf16>(d.Mp * d.Mp);
     b.Pi_lo = ar.take<bf16>(d.Mp * d.Mp);
     b.Z_hi = ar.take<bf16>(d.Ap * d.Mp);
@@ -155,13 +162,17 @@ int chi0_run(const double *X, const Dims &d, const double *eps, double mu, const
   } else {
     launch_split_pad<double>(D, d.M, d.naux, d.naux, 1.f, b.Dt_hi, b.Dt_lo, d.Mp, d.Mp, d.Ap,
                              true, st);
-    SplitMat Yo{b.Yo_hi, b.Yo_lo, d.Mp, d.Ko, d.Ko}, Yv{b.Yv_hi, b.Yv_lo, d.Mp, d.Kv, d.Kv};
+    // G_occ and G_virt in TF32x3: their K sums cancel (off-diagonal entries
+    // are ~sqrt(K) below the summed terms), which the BF16 split would carry
+    // into chi0 at ~1e-4 relative; the D^T Pi D products stay BF16x3
+    SplitMat Yo{b.Yo_hi, b.Yo_lo, d.Mp, d.Ko, d.Ko, true};
+    SplitMat Yv{b.Yv_hi, b.Yv_lo, d.Mp, d.Kv, d.Kv, true};
     SplitMat Dt{b.Dt_hi, b.Dt_lo, d.Ap, d.Mp, d.Mp};
     SplitMat Pi{b.Pi_hi, b.Pi_lo, d.Mp, d.Mp, d.Mp};
     SplitMat Z{b.Z_hi, b.Z_lo, d.Ap, d.Mp, d.Mp};
     for (int k = 0; k < ntau; ++k) {
-      launch_prep_branches(X, d.M, d.n, d.nocc, eps, mu, tau[k], b.Yo_hi, b.Yo_lo, d.Ko,
-                           b.Yv_hi, b.Yv_lo, d.Kv, d.Mp, st);
+      launch_prep_branches_tf32(X, d.M, d.n, d.nocc, eps, mu, tau[k], b.Yo_hi, b.Yo_lo, d.Ko,
+                                b.Yv_hi, b.Yv_lo, d.Kv, d.Mp, st);
       umma::EpiArgs e;
       // Pi = (Y_o Y_o^T) o (Y_v Y_v^T), split for the next product
       e.out0_hi = b.Pi_hi;
@@ -200,25 +211,116 @@ int chi0_run(const double *X, const Dims &d, const double *eps, double mu, const
 }
 
 // --------------------------------------------------------------------- Dyson
+// Block size of the LAUUM below; its DGEMM/DSYRK updates carry the flops.
+constexpr int64_t kLauumBlock = 512;
+
+// In place over the column-major lower triangle of an n x n factor L (the
+// row-major upper triangle of the buffer): L <- L^-1 (cuSOLVER trtri), then
+// L^-1 <- (L^-1)^T L^-1 (a blocked LAUUM on cuBLAS level 3, LAPACK's
+// blocking), leaving A^-1 = L^-T L^-1 in the same triangle. `T` is ib x ib
+// scratch. Replaces potri, whose LAUUM half runs far below DGEMM speed.
+// Below this size the triangular inverse is cuSOLVER's trtri; above it the
+// recursion turns the work into dense DGEMMs.
+constexpr int64_t kTrtriLeaf = 512;
+
+// In place: the lower-triangular column-major block at A (n x n, leading
+// dimension lda, zeros above its diagonal) becomes its inverse, by
+// [[L11, 0], [L21, L22]]^-1 = [[L11^-1, 0], [-L22^-1 L21 L11^-1, L22^-1]]
+// with both halves inverted first; T holds (n - n/2) x (n/2) doubles.
+int trtri_rec(Handles &h, double *A, int64_t n, int64_t lda, double *T, double *tw,
+              size_t tw_bytes, std::vector<char> &host_ws, int *info) {
+  if (n <= kTrtriLeaf) {
+    size_t dbytes = 0, hbytes = 0;
+    if (cusolverDnXtrtri_bufferSize(h.solver, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, n,
+                                    CUDA_R_64F, A, lda, &dbytes, &hbytes) !=
+        CUSOLVER_STATUS_SUCCESS)
+      return MBPT_ERR_CUDA;
+    if (dbytes > tw_bytes) return MBPT_ERR_WORKSPACE;
+    if (host_ws.size() < hbytes) host_ws.resize(hbytes);
+    return cusolverDnXtrtri(h.solver, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, n,
+                            CUDA_R_64F, A, lda, tw, dbytes, host_ws.data(), hbytes, info) ==
+                   CUSOLVER_STATUS_SUCCESS
+               ? MBPT_OK
+               : MBPT_ERR_CUDA;
+  }
+  const int64_t n1 = round_up(n / 2, 64), n2 = n - n1;
+  double *L11 = A, *L21 = A + n1, *L22 = A + n1 + n1 * lda;
+  int rc = trtri_rec(h, L11, n1, lda, T, tw, tw_bytes, host_ws, info);
+  if (rc) return rc;
+  rc = trtri_rec(h, L22, n2, lda, T, tw, tw_bytes, host_ws, info);
+  if (rc) return rc;
+  const double one = 1.0, zero = 0.0, minus = -1.0;
+  const int i1 = static_cast<int>(n1), i2 = static_cast<int>(n2), il = static_cast<int>(lda);
+  // T = L21 L11^-1, then L21 <- -L22^-1 T
+  if (cublasDgemm(h.blas, CUBLAS_OP_N, CUBLAS_OP_N, i2, i1, i1, &one, L21, il, L11, il, &zero,
+                  T, i2) != CUBLAS_STATUS_SUCCESS ||
+      cublasDgemm(h.blas, CUBLAS_OP_N, CUBLAS_OP_N, i2, i1, i2, &minus, L22, il, T, i2, &zero,
+                  L21, il) != CUBLAS_STATUS_SUCCESS)
+    return MBPT_ERR_CUDA;
+  return MBPT_OK;
+}
+
+int spd_inverse_from_factor(Handles &h, double *L, int64_t n, double *tw, size_t tw_bytes,
+                            std::vector<char> &host_ws, int *info, double *T, double *Tr,
+                            cudaStream_t st) {
+  // the dense products of the recursion need zeros above the diagonal
+  launch_zero_strict_upper_cm(L, n, st);
+  int rc = trtri_rec(h, L, n, n, Tr, tw, tw_bytes, host_ws, info);
+  if (rc) return rc;
+  const double one = 1.0, zero = 0.0;
+  const int lda = static_cast<int>(n);
+  for (int64_t i = 0; i < n; i += kLauumBlock) {
+    const int ib = static_cast<int>(std::min(kLauumBlock, n - i));
+    const int ii = static_cast<int>(i);
+    double *Aii = L + i + i * n;
+    // A(i:i+ib, 0:i) = A(i:i+ib, i:i+ib)^T A(i:i+ib, 0:i)
+    if (ii > 0 &&
+        cublasDtrmm(h.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T,
+                    CUBLAS_DIAG_NON_UNIT, ib, ii, &one, Aii, lda, L + i, lda, L + i, lda) !=
+            CUBLAS_STATUS_SUCCESS)
+      return MBPT_ERR_CUDA;
+    // A(i:i+ib, i:i+ib) = L11^T L11 from a copy with its strict upper part cleared
+    launch_lower_copy(Aii, n, T, ib, st);
+    if (cublasDsyrk(h.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, ib, ib, &one, T, ib, &zero,
+                    Aii, lda) != CUBLAS_STATUS_SUCCESS)
+      return MBPT_ERR_CUDA;
+    if (i + ib < n) {
+      const int rest = static_cast<int>(n - i - ib);
+      double *Abelow = L + (i + ib) + i * n;  // A(i+ib:n, i:i+ib)
+      if (ii > 0 && cublasDgemm(h.blas, CUBLAS_OP_T, CUBLAS_OP_N, ib, ii, rest, &one, Abelow,
+                                lda, L + (i + ib), lda, &one, L + i, lda) !=
+                        CUBLAS_STATUS_SUCCESS)
+        return MBPT_ERR_CUDA;
+      if (cublasDsyrk(h.blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, ib, rest, &one, Abelow, lda,
+                      &one, Aii, lda) != CUBLAS_STATUS_SUCCESS)
+        return MBPT_ERR_CUDA;
+    }
+  }
+  return MBPT_OK;
+}
+
 struct DysonBufs {
   int *info;
   int *piv;
   double *work;
   double *rhs;   // n x n right-hand side of the LU inverse of a failed frequency
   double *diag;  // nfreq x n diagonals of 1 - chi0, which the factorisation overwrites
+  double *T;     // diagonal-block scratch of the LAUUM
   int lwork;
 };
 
 int dyson_lwork(int64_t n) {
   cudaStream_t st = nullptr;
   Handles &h = handles(st);
-  int l1 = 0, l2 = 0, l3 = 0;
+  int l1 = 0, l3 = 0;
   cusolverDnDpotrf_bufferSize(h.solver, CUBLAS_FILL_MODE_LOWER, static_cast<int>(n), nullptr,
                               static_cast<int>(n), &l1);
-  cusolverDnDpotri_bufferSize(h.solver, CUBLAS_FILL_MODE_LOWER, static_cast<int>(n), nullptr,
-                              static_cast<int>(n), &l2);
   cusolverDnDgetrf_bufferSize(h.solver, static_cast<int>(n), static_cast<int>(n), nullptr,
                               static_cast<int>(n), &l3);
+  size_t tb = 0, th = 0;
+  cusolverDnXtrtri_bufferSize(h.solver, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, n,
+                              CUDA_R_64F, nullptr, n, &tb, &th);
+  const int l2 = static_cast<int>((tb + 7) / 8);
   int l = l1 > l2 ? l1 : l2;
   return l > l3 ? l : l3;
 }
@@ -231,6 +333,7 @@ DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq) {
   b.work = ar.take<double>(b.lwork > 0 ? b.lwork : 1);
   b.rhs = ar.take<double>(n * n);
   b.diag = ar.take<double>(n * static_cast<int64_t>(nfreq));
+  b.T = ar.take<double>(kLauumBlock * kLauumBlock);
   return b;
 }
 
@@ -248,6 +351,7 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
       return MBPT_ERR_CUDA;
   }
   std::vector<int> info(nfreq);
+  std::vector<char> host_ws;
   cudaMemcpyAsync(info.data(), b.info, sizeof(int) * nfreq, cudaMemcpyDeviceToHost, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return MBPT_ERR_CUDA;
   bool bad = false;
@@ -261,9 +365,9 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
     double *m = chi0 + f * n * n;
     if (info[f] == 0) {
       if (want_w) {
-        if (cusolverDnDpotri(h.solver, CUBLAS_FILL_MODE_LOWER, ni, m, ni, b.work, b.lwork,
-                             b.info + nfreq) != CUSOLVER_STATUS_SUCCESS)
-          return MBPT_ERR_CUDA;
+        const int rc = spd_inverse_from_factor(h, m, n, b.work, sizeof(double) * b.lwork,
+                                               host_ws, b.info + nfreq, b.T, b.rhs, st);
+        if (rc) return rc;
         launch_symmetrize_minus_identity(m, n, 1, st);
       }
       continue;
@@ -413,7 +517,8 @@ int sigma_run(const double *X, const Dims &d, const double *eps, double mu, cons
       e.out1_hi = b.Hg_hi;
       e.out1_lo = b.Hg_lo;
       e.ld_out = d.Mp;
-      SplitMat A3[3] = {Um, Yo, Yv}, B3[3] = {Dm, Yo, Yv};
+      // Zt last: its K = naux sum is the long one, drained by the kernel
+      SplitMat A3[3] = {Yo, Yv, Um}, B3[3] = {Yo, Yv, Dm};
       rc = gemm_split(umma::EPI_SIGMA_H, 3, A3, B3, d.Mp, d.Mp, e, err, st);
       if (rc) return rc;
       // branch sums: sum_P X_s[P,p] (H X_s)[P,p]
@@ -684,6 +789,20 @@ int mbpt_qp_solve(const double *sigma, const double *pade_freq_host, int npade,
                         warm, roots, z, flags, evals, st);
 }
 
+int mbpt_pade_eval(const double *sigma, const double *pade_freq_host, int npade,
+                   const int64_t *states, int nstates, int64_t nocc, double mu, int greedy,
+                   const double *query, int nq, double *out, void *ws, size_t ws_bytes,
+                   void *stream) {
+  if (npade < 2 || npade > 32) return MBPT_ERR_SHAPE;
+  cudaStream_t st = S(stream);
+  Arena ar = arena(ws, ws_bytes);
+  double *pf = ar.take<double>(npade);
+  if (!pf || ar.overflow()) return MBPT_ERR_WORKSPACE;
+  cudaMemcpyAsync(pf, pade_freq_host, sizeof(double) * npade, cudaMemcpyHostToDevice, st);
+  return launch_pade_eval(sigma, pf, npade, states, nstates, nocc, mu, greedy, query, nq, out,
+                          st);
+}
+
 size_t mbpt_chi0_backward_workspace_bytes(int64_t M, int64_t norb, int64_t nocc, int64_t naux,
                                           int mode) {
   (void)mode;
@@ -711,6 +830,43 @@ int mbpt_energy_adjoint_seed(double *wmi, int64_t naux, int nfreq, const double 
                              void *stream) {
   if (naux < 1 || nfreq < 1) return MBPT_ERR_SHAPE;
   launch_chi0_bar_seed(wmi, naux, nfreq, ow_dev, S(stream));
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+size_t mbpt_gemm_split_tf32_workspace_bytes(int64_t m, int64_t n, int64_t k) {
+  const int64_t mp = round_up(m, 128), np = round_up(n, 128), kp = round_up(k, 32);
+  Arena ar;
+  ar.counting = true;
+  ar.take<float>(mp * kp);
+  ar.take<float>(mp * kp);
+  ar.take<float>(np * kp);
+  ar.take<float>(np * kp);
+  ar.take<float>(mp * np);
+  return ar.used + 8192;
+}
+
+int mbpt_gemm_split_tf32(const double *A, const double *B, int64_t m, int64_t n, int64_t k,
+                         double alpha, float *C, int64_t ldc, void *ws, size_t ws_bytes,
+                         int *err, void *stream) {
+  if (m < 1 || n < 1 || k < 1 || ldc < n) return MBPT_ERR_SHAPE;
+  cudaStream_t st = S(stream);
+  const int64_t mp = round_up(m, 128), np = round_up(n, 128), kp = round_up(k, 32);
+  Arena ar = arena(ws, ws_bytes);
+  float *a_hi = ar.take<float>(mp * kp), *a_lo = ar.take<float>(mp * kp);
+  float *b_hi = ar.take<float>(np * kp), *b_lo = ar.take<float>(np * kp);
+  float *c = ar.take<float>(mp * np);
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  launch_split_pad_tf32(A, m, k, k, a_hi, a_lo, kp, mp, kp, st);
+  launch_split_pad_tf32(B, n, k, k, b_hi, b_lo, kp, np, kp, st);
+  SplitMat Am{a_hi, a_lo, mp, kp, kp, true}, Bm{b_hi, b_lo, np, kp, kp, true};
+  umma::EpiArgs e;
+  e.outf = c;
+  e.ld_outf = np;
+  e.alpha = static_cast<float>(alpha);
+  int rc = gemm_split(umma::EPI_F32, 1, &Am, &Bm, mp, np, e, err, st);
+  if (rc) return rc;
+  cudaMemcpy2DAsync(C, sizeof(float) * ldc, c, sizeof(float) * np, sizeof(float) * n, m,
+                    cudaMemcpyDeviceToDevice, st);
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 

@@ -28,6 +28,18 @@ __device__ __forceinline__ void split_bf16(float x, bf16 &hi, bf16 &lo) {
   lo = __float2bfloat16_rn(x - __bfloat162float(hi));
 }
 
+// x rounded to TF32 (10 explicit mantissa bits, to nearest with ties away
+// from zero) as an FP32 word with the low 13 bits clear. Finite inputs only.
+__device__ __forceinline__ float to_tf32(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+
+// x = hi + lo with hi = tf32(x), lo = tf32(x - hi): 22 significant bits.
+__device__ __forceinline__ void split_tf32(float x, float &hi, float &lo) {
+  hi = to_tf32(x);
+  lo = to_tf32(x - hi);
+}
+
 __host__ __device__ __forceinline__ int64_t round_up(int64_t x, int64_t m) {
   return (x + m - 1) / m * m;
 }

@@ -7,10 +7,12 @@
 
 namespace mbpt {
 
-// A BF16 split operand: rows x cols (cols = K, contiguous), leading dim ld.
+// A split operand x = hi + lo: rows x cols (cols = K, contiguous), leading
+// dimension ld, elements BF16 (tf32 false) or TF32-rounded FP32 words.
 struct SplitMat {
-  const bf16 *hi = nullptr, *lo = nullptr;
+  const void *hi = nullptr, *lo = nullptr;
   int64_t rows = 0, cols = 0, ld = 0;
+  bool tf32 = false;
 };
 
 // C (m_rows x n_rows tile grid, both multiples of 128) from nacc problems
@@ -48,6 +50,13 @@ void launch_prep_branches(const double *X, int64_t M, int64_t n, int64_t nocc,
                           const double *eps, double mu, double tau, bf16 *o_hi, bf16 *o_lo,
                           int64_t ld_o, bf16 *v_hi, bf16 *v_lo, int64_t ld_v, int64_t Mp,
                           cudaStream_t st);
+void launch_prep_branches_tf32(const double *X, int64_t M, int64_t n, int64_t nocc,
+                               const double *eps, double mu, double tau, float *o_hi,
+                               float *o_lo, int64_t ld_o, float *v_hi, float *v_lo,
+                               int64_t ld_v, int64_t Mp, cudaStream_t st);
+void launch_split_pad_tf32(const double *src, int64_t rows, int64_t cols, int64_t ld_src,
+                           float *hi, float *lo, int64_t ld_dst, int64_t rows_p, int64_t cols_p,
+                           cudaStream_t st);
 void launch_scaled_branches(const double *X, int64_t M, int64_t n, int64_t nocc,
                             const double *eps, double mu, double tau, double power,
                             double *Xo_s, double *Xv_s, cudaStream_t st);

@@ -93,6 +93,50 @@ __global__ void prep_branches_kernel(const double *__restrict__ X, int64_t M, in
   }
 }
 
+// The same Y_o, Y_v as TF32 hi/lo pairs in FP32 words (for the TF32x3 products).
+__global__ void prep_branches_tf32_kernel(const double *__restrict__ X, int64_t M, int64_t n,
+                                          int64_t nocc, const double *__restrict__ eps,
+                                          double mu, double tau, float *o_hi, float *o_lo,
+                                          int64_t ld_o, float *v_hi, float *v_lo, int64_t ld_v,
+                                          int64_t Mp) {
+  const int64_t width = ld_o + ld_v;
+  const int64_t total = Mp * width;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = i / width, c = i % width;
+    float x = 0.f, h, l;
+    if (c < ld_o) {
+      if (r < M && c < nocc) x = static_cast<float>(X[r * n + c] * exp(0.5 * (eps[c] - mu) * tau));
+      split_tf32(x, h, l);
+      o_hi[r * ld_o + c] = h;
+      o_lo[r * ld_o + c] = l;
+    } else {
+      const int64_t a = c - ld_o;
+      if (r < M && a < n - nocc)
+        x = static_cast<float>(X[r * n + nocc + a] * exp(-0.5 * (eps[nocc + a] - mu) * tau));
+      split_tf32(x, h, l);
+      v_hi[r * ld_v + a] = h;
+      v_lo[r * ld_v + a] = l;
+    }
+  }
+}
+
+// rows x cols (ld_src) FP64 -> TF32 hi/lo pairs, zero padded to rows_p x cols_p
+__global__ void split_pad_tf32_kernel(const double *__restrict__ src, int64_t rows,
+                                      int64_t cols, int64_t ld_src, float *hi, float *lo,
+                                      int64_t ld_dst, int64_t rows_p, int64_t cols_p) {
+  const int64_t n = rows_p * cols_p;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = i / cols_p, c = i % cols_p;
+    const float x = (r < rows && c < cols) ? static_cast<float>(src[r * ld_src + c]) : 0.f;
+    float h, l;
+    split_tf32(x, h, l);
+    hi[r * ld_dst + c] = h;
+    lo[r * ld_dst + c] = l;
+  }
+}
+
 // FP64 reference form: Xo_s[P,i] = X[P,i] e^{power (eps_i-mu) tau},
 // Xv_s[P,a] = X[P,nocc+a] e^{-power (eps_a-mu) tau}
 __global__ void scaled_branches_kernel(const double *__restrict__ X, int64_t M, int64_t n,
@@ -345,6 +389,23 @@ void launch_prep_branches(const double *X, int64_t M, int64_t n, int64_t nocc,
                           cudaStream_t st) {
   count_launch(); prep_branches_kernel<<<grid_cap(Mp * (ld_o + ld_v)), kThreads, 0, st>>>(
       X, M, n, nocc, eps, mu, tau, o_hi, o_lo, ld_o, v_hi, v_lo, ld_v, Mp);
+}
+
+void launch_prep_branches_tf32(const double *X, int64_t M, int64_t n, int64_t nocc,
+                               const double *eps, double mu, double tau, float *o_hi,
+                               float *o_lo, int64_t ld_o, float *v_hi, float *v_lo,
+                               int64_t ld_v, int64_t Mp, cudaStream_t st) {
+  count_launch();
+  prep_branches_tf32_kernel<<<grid_cap(Mp * (ld_o + ld_v)), kThreads, 0, st>>>(
+      X, M, n, nocc, eps, mu, tau, o_hi, o_lo, ld_o, v_hi, v_lo, ld_v, Mp);
+}
+
+void launch_split_pad_tf32(const double *src, int64_t rows, int64_t cols, int64_t ld_src,
+                           float *hi, float *lo, int64_t ld_dst, int64_t rows_p, int64_t cols_p,
+                           cudaStream_t st) {
+  count_launch();
+  split_pad_tf32_kernel<<<grid_cap(rows_p * cols_p), kThreads, 0, st>>>(
+      src, rows, cols, ld_src, hi, lo, ld_dst, rows_p, cols_p);
 }
 
 void launch_scaled_branches(const double *X, int64_t M, int64_t n, int64_t nocc,

@@ -191,21 +191,14 @@ __device__ int select_largest(const Found &fd) {
 
 // flags: 1 quasiparticle, 2 no root, 4 Z outside (0,1], 8 Pade failed,
 //        16 warm start accepted, 32 bracket list overflow
-__global__ void pade_qp_kernel(const double *sigma, const double *pade_freq, int npade,
-                               const double *eps_anchor, const double *xc,
-                               const int64_t *states, int nstates, int64_t nocc, double mu,
-                               int greedy, const double *warm, double *roots, double *zout,
-                               int *flags, int *evals) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nstates) return;
-  State s;
-  const int64_t p = states[i];
+// Thiele coefficients of state i (sample points mu +/- i w, Sigma conjugated
+// on the occupied branch) into s.z / s.a, greedily ordered unless greedy is 0;
+// false when the greedy ordering finds no finite next coefficient.
+__device__ bool build_fit(State &s, const double *sigma, const double *pade_freq, int npade,
+                          int i, int64_t p, int64_t nocc, double mu, int greedy) {
   const double sign = p < nocc ? -1.0 : 1.0;
   const bool conj = p < nocc;
   s.n = npade;
-  s.eps = eps_anchor[p];
-  s.xc = xc ? xc[i] : 0.0;
-  s.evals = 0;
   cplx zz[kMaxPade], ff[kMaxPade];
   for (int k = 0; k < npade; ++k) {
     zz[k] = {mu, sign * pade_freq[k]};
@@ -213,7 +206,6 @@ __global__ void pade_qp_kernel(const double *sigma, const double *pade_freq, int
     const double im = sigma[2 * (static_cast<int64_t>(i) * npade + k) + 1];
     ff[k] = {re, conj ? -im : im};
   }
-  int fl = 0;
   // ---- Thiele coefficients, greedy order ----
   if (greedy) {
     bool used[kMaxPade];
@@ -250,8 +242,7 @@ __global__ void pade_qp_kernel(const double *sigma, const double *pade_freq, int
         }
       }
       if (best_j < 0) {
-        fl |= 8;
-        break;
+        return false;
       }
       used[best_j] = true;
       s.z[m] = zz[best_j];
@@ -270,6 +261,23 @@ __global__ void pade_qp_kernel(const double *sigma, const double *pade_freq, int
       s.a[m] = g;
     }
   }
+  return true;
+}
+
+__global__ void pade_qp_kernel(const double *sigma, const double *pade_freq, int npade,
+                               const double *eps_anchor, const double *xc,
+                               const int64_t *states, int nstates, int64_t nocc, double mu,
+                               int greedy, const double *warm, double *roots, double *zout,
+                               int *flags, int *evals) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nstates) return;
+  State s;
+  const int64_t p = states[i];
+  s.eps = eps_anchor[p];
+  s.xc = xc ? xc[i] : 0.0;
+  s.evals = 0;
+  int fl = 0;
+  if (!build_fit(s, sigma, pade_freq, npade, i, p, nocc, mu, greedy)) fl |= 8;
   if (fl & 8) {
     roots[i] = NAN;
     zout[i] = NAN;
@@ -364,7 +372,37 @@ __global__ void pade_qp_kernel(const double *sigma, const double *pade_freq, int
   evals[i] = s.evals;
 }
 
+// out[i, q] = Re Sigma_c(query[i, q]) of state i's continuation (NaN when its
+// Pade construction failed)
+__global__ void pade_eval_kernel(const double *sigma, const double *pade_freq, int npade,
+                                 const int64_t *states, int nstates, int64_t nocc, double mu,
+                                 int greedy, const double *query, int nq, double *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nstates) return;
+  State s;
+  s.eps = 0.0;
+  s.xc = 0.0;
+  s.evals = 0;
+  const bool ok = build_fit(s, sigma, pade_freq, npade, i, states[i], nocc, mu, greedy);
+  for (int q = 0; q < nq; ++q) {
+    const int64_t o = static_cast<int64_t>(i) * nq + q;
+    out[o] = ok ? pade_re(s, query[o]) : NAN;
+  }
+}
+
 }  // namespace
+
+int launch_pade_eval(const double *sigma, const double *pade_freq, int npade,
+                     const int64_t *states, int nstates, int64_t nocc, double mu, int greedy,
+                     const double *query, int nq, double *out, cudaStream_t st) {
+  if (npade < 2 || npade > kMaxPade || nstates < 0 || nq < 1) return MBPT_ERR_SHAPE;
+  if (nstates == 0) return MBPT_OK;
+  count_launch();
+  pade_eval_kernel<<<(nstates + 63) / 64, 64, 0, st>>>(sigma, pade_freq, npade, states,
+                                                       nstates, nocc, mu, greedy, query, nq,
+                                                       out);
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
 
 int launch_pade_qp(const double *sigma, const double *pade_freq, int npade,
                    const double *eps_anchor, const double *xc, const int64_t *states,

@@ -26,7 +26,7 @@ enum Epi : int {
   EPI_SPLIT = 0,           // out0 = alpha * acc0, BF16 hi/lo
   EPI_F32 = 1,             // outf = alpha * acc0, FP32
   EPI_HADAMARD_SPLIT = 2,  // out0 = acc0 o acc1, BF16 hi/lo   (Pi = Go o Gv)
-  EPI_SIGMA_H = 3,         // out0 = acc1 o acc0, out1 = acc2 o acc0 (Go o Zt, Gv o Zt)
+  EPI_SIGMA_H = 3,         // out0 = acc0 o acc2, out1 = acc1 o acc2 (Go o Zt, Gv o Zt)
   EPI_ROWDOT2 = 4,         // sig0[c] += sum_r xs[r,c] acc0[r,c], sig1[c] -= ... acc1
   EPI_F32_ACC = 5,         // outf += alpha * acc0, FP32 read-modify-write
 };
@@ -123,6 +123,12 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int n) {
          (static_cast<uint32_t>(128 >> 4) << 24);
 }
 
+// Instruction descriptor: TF32 x TF32 -> FP32, both K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t idesc_tf32(int n) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(n >> 3) << 17) |
+         (static_cast<uint32_t>(128 >> 4) << 24);
+}
+
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db,
                                          uint32_t idesc, uint32_t accumulate) {
   asm volatile(
@@ -130,6 +136,31 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t 
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
       "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db,
+                                         uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+
+// One 32-byte K step (8 TF32 or 16 BF16 elements) of the three split
+// products hi*hi + hi*lo + lo*hi into accumulator d; `first` overwrites it.
+template <bool TF32>
+__device__ __forceinline__ void mma3(uint32_t d, uint64_t a_hi, uint64_t a_lo, uint64_t b_hi,
+                                     uint64_t b_lo, uint32_t idesc, uint32_t first) {
+  if constexpr (TF32) {
+    mma_tf32(d, a_hi, b_hi, idesc, first ? 0u : 1u);
+    mma_tf32(d, a_hi, b_lo, idesc, 1u);
+    mma_tf32(d, a_lo, b_hi, idesc, 1u);
+  } else {
+    mma_bf16(d, a_hi, b_hi, idesc, first ? 0u : 1u);
+    mma_bf16(d, a_hi, b_lo, idesc, 1u);
+    mma_bf16(d, a_lo, b_hi, idesc, 1u);
+  }
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
@@ -186,28 +217,43 @@ __device__ __forceinline__ float warp_column_sum(float (&v)[32], int lane) {
   return v[0];
 }
 
-template <int NACC, int BN>
+
+template <int NACC, int BN, bool DRAIN = false>
 struct Layout {
   static constexpr int kABytes = BM * BK * 2;
   static constexpr int kBBytes = BN * BK * 2;
   static constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
   static constexpr int kStages = (kStageBytes <= 64 * 1024) ? 3 : 2;
   static constexpr int kSmemBytes = kStages * kStageBytes + 1024 + 256;
-  static constexpr int kTmemCols = (NACC * BN <= 32) ? 32 : (NACC * BN <= 64) ? 64
-                                   : (NACC * BN <= 128) ? 128 : (NACC * BN <= 256) ? 256 : 512;
-  static_assert(NACC * BN <= 512, "accumulators exceed TMEM");
+  // a drained last accumulator takes two buffers
+  static constexpr int kCols = (NACC + (DRAIN ? 1 : 0)) * BN;
+  static constexpr int kTmemCols = (kCols <= 32) ? 32 : (kCols <= 64) ? 64
+                                   : (kCols <= 128) ? 128 : (kCols <= 256) ? 256 : 512;
+  static_assert(kCols <= 512, "accumulators exceed TMEM");
 };
 
-template <int NACC, int BN, int EPI>
+// TF32: operands are FP32 words holding TF32-rounded hi/lo parts (32 per
+// 128-byte row, K step 8); otherwise BF16 pairs (64 per row, K step 16).
+// Either way a stage holds 128-byte rows and a K step advances 32 bytes.
+//
+// DRAIN > 0: the tensor core's FP32 accumulation truncates, which biases a
+// long K sum towards zero by about half an ulp per accumulation step (~4e-5
+// relative at K = 7296 with three split products). The last accumulator is
+// therefore restarted every DRAIN K slabs in one of two TMEM buffers, and the
+// epilogue warps add each finished chunk into round-to-nearest FP32 sums in
+// registers while the MMAs fill the other buffer.
+template <int NACC, int BN, int EPI, bool TF32 = false, int DRAIN = 0>
 __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constant__ Params<NACC> p) {
-  using L = Layout<NACC, BN>;
+  using L = Layout<NACC, BN, (DRAIN > 0)>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
   uint64_t *full = reinterpret_cast<uint64_t *>(smem + L::kStages * L::kStageBytes);
   uint64_t *empty = full + L::kStages;
   uint64_t *accum = empty + L::kStages;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(accum + 1);
+  uint64_t *dfull = accum + 1;   // [2] a drained chunk is complete in buffer b
+  uint64_t *dempty = dfull + 2;  // [2] the epilogue has read buffer b
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(dempty + 2);
   int *fail = reinterpret_cast<int *>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -219,6 +265,7 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
   const int tm = first_m + (pid % per_group) % gsize;
   const int tn = (pid % per_group) / gsize;
   const int m0 = tm * BM, n0 = tn * BN;
+  constexpr int kLast = NACC - 1;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < L::kStages; ++s) {
@@ -226,6 +273,10 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
       mbar_init(&empty[s], 1);
     }
     mbar_init(accum, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&dfull[b], 1);
+      mbar_init(&dempty[b], 4);
+    }
     *fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -253,11 +304,12 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
           if (!mbar_wait(&empty[s], ph ^ 1)) { ok = false; break; }
           mbar_expect_tx(&full[s], L::kStageBytes);
           uint8_t *st = smem + s * L::kStageBytes;
-          tma_load_2d(st, &p.tm[4 * j + 0], kt * BK, m0, &full[s]);
-          tma_load_2d(st + L::kABytes, &p.tm[4 * j + 1], kt * BK, m0, &full[s]);
-          tma_load_2d(st + 2 * L::kABytes, &p.tm[4 * j + 2], kt * BK, n0, &full[s]);
-          tma_load_2d(st + 2 * L::kABytes + L::kBBytes, &p.tm[4 * j + 3], kt * BK, n0,
-                      &full[s]);
+          // K coordinate in elements: one 128-byte row per slab
+          const int kx = kt * (TF32 ? 32 : BK);
+          tma_load_2d(st, &p.tm[4 * j + 0], kx, m0, &full[s]);
+          tma_load_2d(st + L::kABytes, &p.tm[4 * j + 1], kx, m0, &full[s]);
+          tma_load_2d(st + 2 * L::kABytes, &p.tm[4 * j + 2], kx, n0, &full[s]);
+          tma_load_2d(st + 2 * L::kABytes + L::kBBytes, &p.tm[4 * j + 3], kx, n0, &full[s]);
         }
       }
       if (!ok) {
@@ -272,12 +324,22 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
     __syncwarp();
   } else if (warp == 1) {
     if (lane == 0) {
-      constexpr uint32_t idesc = idesc_bf16(BN);
+      constexpr uint32_t idesc = TF32 ? idesc_tf32(BN) : idesc_bf16(BN);
       int it = 0;
       bool ok = true;
       for (int j = 0; j < NACC && ok; ++j) {
-        const uint32_t d = tmem + static_cast<uint32_t>(j * BN);
+        const bool drained = DRAIN > 0 && j == kLast;
+        uint32_t d = tmem + static_cast<uint32_t>(j * BN);
+        int buf = 0;
         for (int kt = 0; kt < p.k_tiles[j]; ++kt, ++it) {
+          const bool chunk_start = drained && (kt % (DRAIN > 0 ? DRAIN : 1)) == 0;
+          if (chunk_start) {
+            const int c = kt / (DRAIN > 0 ? DRAIN : 1);
+            buf = c & 1;
+            if (!mbar_wait(&dempty[buf], ((c >> 1) & 1) ^ 1)) { ok = false; break; }
+            tc_fence_after();
+            d = tmem + static_cast<uint32_t>((kLast + buf) * BN);
+          }
           const int s = it % L::kStages;
           const uint32_t ph = (it / L::kStages) & 1;
           if (!mbar_wait(&full[s], ph) || *reinterpret_cast<volatile int *>(fail)) {
@@ -290,14 +352,16 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
           const uint64_t a_lo = sw128_desc(smem_u32(st + L::kABytes));
           const uint64_t b_hi = sw128_desc(smem_u32(st + 2 * L::kABytes));
           const uint64_t b_lo = sw128_desc(smem_u32(st + 2 * L::kABytes + L::kBBytes));
+          const bool restart = drained ? chunk_start : kt == 0;
 #pragma unroll
-          for (int kk = 0; kk < BK / 16; ++kk) {
+          for (int kk = 0; kk < 4; ++kk) {
             const uint64_t adv = static_cast<uint64_t>(kk * 2);  // 32 bytes >> 4
-            mma_bf16(d, a_hi + adv, b_hi + adv, idesc, (kt > 0 || kk > 0) ? 1u : 0u);
-            mma_bf16(d, a_hi + adv, b_lo + adv, idesc, 1u);
-            mma_bf16(d, a_lo + adv, b_hi + adv, idesc, 1u);
+            mma3<TF32>(d, a_hi + adv, a_lo + adv, b_hi + adv, b_lo + adv, idesc,
+                       (restart && kk == 0) ? 1u : 0u);
           }
           mma_commit(&empty[s]);
+          if (drained && ((kt + 1) % (DRAIN > 0 ? DRAIN : 1) == 0 || kt + 1 == p.k_tiles[j]))
+            mma_commit(&dfull[buf]);
         }
       }
       if (!ok) {
@@ -311,20 +375,58 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
   } else {
     // epilogue: warps 2..5 own TMEM lane quarters (warp % 4)
     const int sp = warp & 3;
-    const bool ok = mbar_wait(accum, 0) && !*reinterpret_cast<volatile int *>(fail);
+    const uint32_t taddr = tmem + (static_cast<uint32_t>(sp * 32) << 16);
+    bool ok = true;
+    float acc[DRAIN > 0 ? BN : 1];
+    if constexpr (DRAIN > 0) {
+#pragma unroll
+      for (int i = 0; i < BN; ++i) acc[i] = 0.f;
+      const int nchunks = (p.k_tiles[kLast] + DRAIN - 1) / DRAIN;
+      for (int c = 0; c < nchunks; ++c) {
+        const int b = c & 1;
+        if (!mbar_wait(&dfull[b], (c >> 1) & 1) || *reinterpret_cast<volatile int *>(fail)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+#pragma unroll
+        for (int q = 0; q < BN / 32; ++q) {
+          float t[32];
+          tmem_ld32(taddr + static_cast<uint32_t>((kLast + b) * BN + 32 * q), t);
+#pragma unroll
+          for (int i = 0; i < 32; ++i) acc[32 * q + i] += t[i];
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
+                                        smem_u32(&dempty[b]))
+                                    : "memory");
+      }
+    }
+    ok = ok && mbar_wait(accum, 0) && !*reinterpret_cast<volatile int *>(fail);
     __syncwarp();
     if (!ok) {
       if (lane == 0) DevErr{p.err}.set(MBPT_ERR_TIMEOUT);
     } else {
       tc_fence_after();
       const int row = m0 + sp * 32 + lane;
-      const uint32_t taddr = tmem + (static_cast<uint32_t>(sp * 32) << 16);
       const EpiArgs &e = p.epi;
-#pragma unroll 1
+      // 32 columns starting at c of accumulator j (the drained one from registers)
+      auto load = [&](int j, int c, float (&v)[32]) {
+        if constexpr (DRAIN > 0) {
+          if (j == kLast) {
+#pragma unroll
+            for (int i = 0; i < 32; ++i) v[i] = acc[c + i];
+            return;
+          }
+        }
+        tmem_ld32(taddr + static_cast<uint32_t>(j * BN + c), v);
+      };
+#pragma unroll
       for (int c = 0; c < BN; c += 32) {
         const int col = n0 + c;
         float v0[32];
-        tmem_ld32(taddr + c, v0);
+        load(0, c, v0);
         if constexpr (EPI == EPI_SPLIT) {
 #pragma unroll
           for (int i = 0; i < 32; ++i) v0[i] *= e.alpha;
@@ -343,23 +445,24 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
           }
         } else if constexpr (EPI == EPI_HADAMARD_SPLIT) {
           float v1[32];
-          tmem_ld32(taddr + BN + c, v1);
+          load(1, c, v1);
 #pragma unroll
           for (int i = 0; i < 32; ++i) v0[i] *= v1[i];
           store_split32(e.out0_hi + row * e.ld_out + col, e.out0_lo + row * e.ld_out + col, v0);
         } else if constexpr (EPI == EPI_SIGMA_H) {
-          float v1[32];
-          tmem_ld32(taddr + BN + c, v1);
+          // acc0 = G_occ, acc1 = G_virt, acc2 = Zt
+          float z[32], v1[32];
+          load(2, c, z);
 #pragma unroll
-          for (int i = 0; i < 32; ++i) v1[i] *= v0[i];
-          store_split32(e.out0_hi + row * e.ld_out + col, e.out0_lo + row * e.ld_out + col, v1);
-          tmem_ld32(taddr + 2 * BN + c, v1);
+          for (int i = 0; i < 32; ++i) v0[i] *= z[i];
+          store_split32(e.out0_hi + row * e.ld_out + col, e.out0_lo + row * e.ld_out + col, v0);
+          load(1, c, v1);
 #pragma unroll
-          for (int i = 0; i < 32; ++i) v1[i] *= v0[i];
+          for (int i = 0; i < 32; ++i) v1[i] *= z[i];
           store_split32(e.out1_hi + row * e.ld_out + col, e.out1_lo + row * e.ld_out + col, v1);
         } else if constexpr (EPI == EPI_ROWDOT2) {
           float v1[32], xs[32];
-          tmem_ld32(taddr + BN + c, v1);
+          load(1, c, v1);
           const float4 *src = reinterpret_cast<const float4 *>(e.xs + row * e.ld_xs + col);
 #pragma unroll
           for (int q = 0; q < 8; ++q) {

@@ -167,6 +167,9 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
     if ev:
         ev[3].record()
     anchor = eps_h if eps_anchor is None else _eps_host(eps_anchor)
+    if callable(warm):
+        # a predictor that reads this sweep's Sigma (the learned warm start)
+        warm = warm(SweepResult(sigma=sigma, axes=axes, states=states))
     roots, z, flags, evals = qp_solve(sigma, axes.pade_freq, anchor, states, nocc, mu,
                                       xc=xc_diagonal, greedy=greedy, warm=warm, stream=stream)
     if ev:

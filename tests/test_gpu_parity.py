@@ -31,27 +31,31 @@ def dev():
     return _lib.require_device()
 
 
+@pytest.mark.parametrize('kind,tol', [('bf16', 3e-5), ('tf32', 2e-6)])
 @pytest.mark.parametrize('m,n,k', [(300, 260, 200), (128, 128, 64), (1000, 700, 1100),
                                    (17, 5, 3)])
-def test_split_gemm_matches_fp64(dev, m, n, k):
+def test_split_gemm_matches_fp64(dev, m, n, k, kind, tol):
     rng = np.random.default_rng(m + n + k)
     A = rng.standard_normal((m, k))
     B = rng.standard_normal((n, k))
     Ad = torch.as_tensor(A, device=dev)
     Bd = torch.as_tensor(B, device=dev)
     C = torch.empty((m, n), dtype=torch.float32, device=dev)
-    ws = torch.empty(_lib.lib().mbpt_gemm_split_workspace_bytes(m, n, k), dtype=torch.uint8,
-                     device=dev)
+    lib = _lib.lib()
+    size = (lib.mbpt_gemm_split_workspace_bytes if kind == 'bf16'
+            else lib.mbpt_gemm_split_tf32_workspace_bytes)(m, n, k)
+    fn = lib.mbpt_gemm_split if kind == 'bf16' else lib.mbpt_gemm_split_tf32
+    ws = torch.empty(size, dtype=torch.uint8, device=dev)
     err = torch.zeros(1, dtype=torch.int32, device=dev)
-    _lib.check(_lib.lib().mbpt_gemm_split(_lib.ptr(Ad), _lib.ptr(Bd), m, n, k, 1.0,
-                                          _lib.ptr(C), n, _lib.ptr(ws), ws.numel(),
-                                          _lib.ptr(err), _lib.stream_ptr()), 'gemm')
+    _lib.check(fn(_lib.ptr(Ad), _lib.ptr(Bd), m, n, k, 1.0, _lib.ptr(C), n, _lib.ptr(ws),
+                  ws.numel(), _lib.ptr(err), _lib.stream_ptr()), 'gemm')
     torch.cuda.synchronize()
     assert int(err.item()) == 0
     ref = A @ B.T
-    # per-entry error against the scale of the products that were summed
+    # per-entry error against the scale of the products that were summed:
+    # 2^-18 per BF16x3 product, 2^-22 per TF32x3 product, FP32 accumulation
     scale = np.sqrt(k) * np.abs(A).max() * np.abs(B).max()
-    assert np.abs(C.cpu().numpy() - ref).max() <= 3e-5 * scale
+    assert np.abs(C.cpu().numpy() - ref).max() <= tol * scale
 
 
 @pytest.mark.parametrize('precision,tol', [('fp64', FP64_REL), ('mixed', MIXED_REL)])
