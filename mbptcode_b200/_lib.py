@@ -111,7 +111,14 @@ def require_device(device=None):
 
 
 def ptr(t):
-    return None if t is None else C.c_void_p(t.data_ptr())
+    """Device address of a CUDA tensor (None for None). A tensor anywhere
+    else is refused here, before any kernel could dereference it."""
+    if t is None:
+        return None
+    if not isinstance(t, torch.Tensor) or t.device.type != 'cuda':
+        raise ValueError(f'a device pointer is needed, got {type(t).__name__} on '
+                         f'{getattr(t, "device", "host")}')
+    return C.c_void_p(t.data_ptr())
 
 
 def launch_count():

@@ -41,7 +41,8 @@ def sigma_branch_sums(X, D, Wt, eps, nocc, tau_points, states, mu, precision=Non
                       stream=None):
     """(2, ntau, nstates) device tensor: Sigma^<_pp(tau) and Sigma^>_pp(tau) of
     the states, the diagonal form of ``imaginary_time.py:39-92``."""
-    dev = Wt.device
+    dev = require_device()
+    Wt = to_device(Wt, dev)
     Xd, Dd = to_device(X, dev), to_device(D, dev)
     eps_h = _eps_host(eps)
     ed = to_device(eps_h, dev)

@@ -21,16 +21,17 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from ._lib import WORKSPACE, check, host_array, lib, ptr, stream_ptr
+from ._lib import WORKSPACE, check, host_array, lib, ptr, require_device, stream_ptr
 from .gw import gw_sweep, sigma_branch_sums
-from .space_time import _eps_host
+from .space_time import _eps_host, to_device
 
 FEATURE_OFFSET = 0.1  # Ha, the two real frequencies Sigma_c is read at
 
 
 def exchange_diagonal(X, D, eps, nocc, states, mu):
     """Sigma_x,ii of `states` (device FP64)."""
-    dev = X.device
+    dev = require_device()
+    X, D = to_device(X, dev), to_device(D, dev)
     naux = D.shape[1]
     eye = torch.eye(naux, dtype=torch.float64, device=dev)[None]
     br = sigma_branch_sums(X, D, eye, eps, nocc, [0.0], states, mu, precision='fp64')

@@ -43,3 +43,14 @@ def test_product_path_refuses_without_gpu():
     from mbptcode_b200 import _lib
     with pytest.raises(RuntimeError):
         _lib.require_device()
+
+
+def test_host_tensors_are_refused_before_any_kernel():
+    import numpy as np
+    import torch
+    from mbptcode_b200 import _lib
+    with pytest.raises(ValueError):
+        _lib.ptr(torch.zeros(3))
+    with pytest.raises(ValueError):
+        _lib.ptr(np.zeros(3))
+    assert _lib.ptr(None) is None

@@ -42,8 +42,8 @@ def test_adjoint_matches_central_differences():
     axes = grids.space_time_axes(eps, nocc, ntau=20)
     dev = torch.device('cuda')
     V = torch.as_tensor(D @ D.T, device=dev)
-    Xt = torch.as_tensor(X, device=dev, requires_grad=True)
-    et = torch.as_tensor(eps, device=dev, requires_grad=True)
+    Xt = torch.tensor(X, device=dev, requires_grad=True)
+    et = torch.tensor(eps, device=dev, requires_grad=True)
     Vt = V.clone().requires_grad_(True)
     E = adjoint.rpa_energy(et, Xt, nocc=nocc, grid=axes.grid, V=Vt)
     E.backward()
