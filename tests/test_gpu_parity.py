@@ -184,3 +184,24 @@ def test_synthetic_literal_is_weak_and_calibrated_is_not():
             assert abs(e_ref) < 1e-8      # nearly non-interacting
         else:
             assert abs(e_ref) > 1e-2
+
+
+def test_planted_nonpositive_dielectric_is_flagged():
+    # the reference's planted-input test (tests/test_rpa_log_determinant.py):
+    # one eigenvalue of chi0 at 1.5 makes det(1 - chi0) negative; the
+    # Cholesky fails, the LU fallback gives log|det| and the inverse, and the
+    # frequency is flagged
+    rng = np.random.default_rng(1)
+    n = 40
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    lam = -rng.uniform(0.1, 2.0, n)
+    lam[0] = 1.5
+    c = (Q * lam) @ Q.T
+    flags = {}
+    with pytest.warns(st.NonPositiveDielectric):
+        ld = st.dielectric_log_determinant(np.eye(n) - c, 3, flags)
+    sign, ref = np.linalg.slogdet(np.eye(n) - c)
+    assert sign < 0 and abs(ld - ref) < 1e-10
+    assert flags['nonpositive_det'] == [3]
+    W = st.dyson_screening(c, correlation=True)
+    assert rel(W, np.linalg.inv(np.eye(n) - c) - np.eye(n)) < 1e-10

@@ -92,3 +92,27 @@ def test_replicas_over_two_gloo_ranks():
     assert m0 == [0, 2, 4, 6] and m1 == [1, 3, 5]
     assert t0 == t1 == 2.5
     assert g0 == g1 == [[0, 2, 4, 6], [1, 3, 5]]
+
+
+def test_plugin_rebinds_and_restores_reference_names():
+    ref = os.environ.get('MBPTCODE_ROOT', '/root/reference')
+    if not os.path.isdir(os.path.join(ref, 'src')):
+        pytest.skip('no MBPTcode checkout here')
+    import sys
+    sys.path.insert(0, ref)
+    try:
+        import importlib
+        from mbptcode_b200 import plugin, space_time
+        lr = importlib.import_module(plugin.LR)
+        orig = lr.chi0_imaginary_frequency
+        bound, skipped = plugin.install()
+        assert lr.chi0_imaginary_frequency is space_time.chi0_imaginary_frequency
+        assert 'dyson_screening' in bound[plugin.IT]
+        assert plugin.ST in skipped      # the driver imports pyscf, absent here
+        adj = importlib.import_module(plugin.ADJ)
+        assert adj.rpa_correlation_energy_space_time is \
+            space_time.rpa_correlation_energy_space_time
+        plugin.uninstall()
+        assert lr.chi0_imaginary_frequency is orig
+    finally:
+        sys.path.remove(ref)
