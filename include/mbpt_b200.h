@@ -18,9 +18,11 @@
  *     (zeroed by the caller before the call, read after it); NULL skips.
  *   - mode MBPT_MODE_FP64 runs every product in FP64 (cuBLAS DGEMM, the plain
  *     GPU path); MBPT_MODE_MIXED runs the N^3 products on the tcgen05 tensor
- *     cores as split-BF16 (3-term) products with FP32 accumulation. The
- *     tau <-> omega transforms, the Cholesky/log-det, the quadrature sums and
- *     the QP root search are FP64 in both modes.
+ *     cores as split (3-term) products with FP32 accumulation: BF16 pairs for
+ *     the Coulomb-side products, TF32 pairs for G_occ / G_virt and for the
+ *     inverse of the Dyson step. The tau <-> omega transforms, the
+ *     Cholesky/log-det, the quadrature sums and the QP root search are FP64
+ *     in both modes.
  *
  * Symbols: X (M x norb) collocation of the MO basis on the interpolation
  * points, columns [0, nocc) occupied; D (M x naux) Coulomb factor, Z = D D^T;
@@ -61,7 +63,8 @@ int mbpt_device_supported(int device);
  * with enable = 1 starts recording on the launching streams; a call with
  * non-NULL total_ms/launches (8 entries, indexed by epilogue kind: 0 split
  * store, 1 FP32 store, 2 Hadamard, 3 self-energy Hadamards, 4 row
- * contraction, 5 FP32 accumulate) waits for the recorded launches, returns
+ * contraction, 5 FP32 accumulate; 6 collects the TF32 products of
+ * mbpt_dyson's inverse whatever their epilogue) waits for the recorded launches, returns
  * their summed milliseconds and counts, and resets them. */
 long long mbpt_launch_count(void);
 int mbpt_gemm_timing(int enable, double *total_ms, long long *launches);
@@ -95,11 +98,16 @@ int mbpt_chi0_sweep(const double *X_dev, int64_t M, int64_t norb, int64_t nocc,
  * info_host (nfreq): 0, or i > 0 when 1 - chi0 is not positive definite (its
  * log|det| and inverse then come from an LU factorisation and sign_host[f]
  * is the determinant's sign); the call then returns MBPT_ERR_NOT_SPD after
- * finishing every frequency. info_host/sign_host may be NULL. */
-size_t mbpt_dyson_workspace_bytes(int64_t naux, int nfreq);
-int mbpt_dyson(double *chi0_dev, int64_t naux, int nfreq, int want_w, double *logdet_dev,
-               double *trace_dev, int *info_host, int *sign_host, void *workspace,
-               size_t ws_bytes, void *stream);
+ * finishing every frequency. info_host/sign_host may be NULL.
+ * mode: the factorisation and log-determinant are FP64 either way; the inverse
+ * W = L^-T L^-1 is formed from the FP64 factor by cuBLAS level-3 products
+ * (MBPT_MODE_FP64) or, with MBPT_MODE_MIXED, by TF32x3 tensor-core products
+ * (the triangular inverse's off-diagonal blocks and L^-T L^-1): a few 2^-22
+ * absolute on W - I, whose entries are bounded by 1. */
+size_t mbpt_dyson_workspace_bytes(int64_t naux, int nfreq, int mode);
+int mbpt_dyson(double *chi0_dev, int64_t naux, int nfreq, int want_w, int mode,
+               double *logdet_dev, double *trace_dev, int *info_host, int *sign_host,
+               void *workspace, size_t ws_bytes, int *err_dev, void *stream);
 
 /* ---- dRPA correlation energy ----------------------------------------------
  * Replaces LinearResponse/space_time.py:1100-1183

@@ -34,8 +34,8 @@ _SIGNATURES = {
     'mbpt_chi0_workspace_bytes': (_sz, [_i64, _i64, _i64, _i64, _i, _i]),
     'mbpt_chi0_sweep': (_i, [_p, _i64, _i64, _i64, _p, _d, _p, _i64, _p, _i, _p, _i, _i, _p,
                              _p, _p, _sz, _p, _p]),
-    'mbpt_dyson_workspace_bytes': (_sz, [_i64, _i]),
-    'mbpt_dyson': (_i, [_p, _i64, _i, _i, _p, _p, _p, _p, _p, _sz, _p]),
+    'mbpt_dyson_workspace_bytes': (_sz, [_i64, _i, _i]),
+    'mbpt_dyson': (_i, [_p, _i64, _i, _i, _i, _p, _p, _p, _p, _p, _sz, _p, _p]),
     'mbpt_rpa_energy_workspace_bytes': (_sz, [_i64, _i64, _i64, _i64, _i, _i, _i]),
     'mbpt_rpa_energy': (_i, [_p, _i64, _i64, _i64, _p, _d, _p, _i64, _p, _i, _p, _p, _i, _i,
                              _p, _p, _p, _p, _sz, _p, _p]),
@@ -126,7 +126,8 @@ def launch_count():
     return int(lib().mbpt_launch_count())
 
 
-EPILOGUES = ('split', 'f32', 'hadamard', 'sigma_hadamard', 'row_contraction', 'f32_acc')
+EPILOGUES = ('split', 'f32', 'hadamard', 'sigma_hadamard', 'row_contraction', 'f32_acc',
+             'dyson_tf32')
 
 
 def gemm_timing(enable=True, read=False):

@@ -1,4 +1,5 @@
-// Small FP64 kernels of the adjoint and of the Dyson fallback path.
+// Small FP64 kernels of the adjoint and of the Dyson step (its triangular
+// inverse and the FP64 <-> TF32-pair conversions of its tensor-core products).
 #include <cmath>
 
 #include "internal.h"
@@ -137,6 +138,88 @@ __global__ void zero_strict_upper_cm_kernel(double *a, int64_t n) {
   }
 }
 
+// Inverts the nb x nb diagonal blocks of a column-major lower-triangular
+// matrix in place, one CTA per block: the block is staged row-major in shared
+// memory and inverted row by row (forward substitution against the rows
+// already inverted), so the block never leaves the SM until it is done.
+__global__ void trtri_diag_blocks_kernel(double *A, int64_t n, int64_t lda, int nb) {
+  extern __shared__ double s[];  // m x m row-major block, then one row of L
+  const int64_t off = static_cast<int64_t>(blockIdx.x) * nb;
+  const int m = static_cast<int>(min(static_cast<int64_t>(nb), n - off));
+  double *row = s + m * m;
+  for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
+    const int r = idx / m, c = idx % m;
+    s[idx] = r >= c ? A[(off + c) * lda + off + r] : 0.0;
+  }
+  __syncthreads();
+  for (int i = 0; i < m; ++i) {
+    for (int k = threadIdx.x; k <= i; k += blockDim.x) row[k] = s[i * m + k];
+    __syncthreads();
+    const double inv = 1.0 / row[i];
+    // row i of L^-1: (L^-1)_ij = -(sum_{j<=k<i} L_ik (L^-1)_kj) / L_ii
+    for (int j = threadIdx.x; j <= i; j += blockDim.x) {
+      double acc = 0.0;
+      for (int k = j; k < i; ++k) acc = fma(row[k], s[k * m + j], acc);
+      s[i * m + j] = j == i ? inv : -acc * inv;
+    }
+    __syncthreads();
+  }
+  for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
+    const int r = idx / m, c = idx % m;
+    if (r >= c) A[(off + c) * lda + off + r] = s[idx];
+  }
+}
+
+// dst (rows_p x k_p row-major TF32 hi/lo pairs, zero padded) of the logical
+// rows x k FP64 matrix X(r, c) = src[r * rs + c * cs], through a 32 x 33
+// shared tile so that the global reads run along whichever stride is 1.
+// The pair is split from the FP64 value: hi = tf32(x), lo = tf32(x - hi).
+__global__ void strided_to_tf32_kernel(const double *__restrict__ src, int64_t rows, int64_t k,
+                                       int64_t rs, int64_t cs, float *hi, float *lo,
+                                       int64_t rows_p, int64_t k_p) {
+  __shared__ double tile[32][33];
+  const int64_t r0 = static_cast<int64_t>(blockIdx.y) * 32;
+  const int64_t c0 = static_cast<int64_t>(blockIdx.x) * 32;
+  const bool col_unit = cs == 1;
+  for (int a = threadIdx.y; a < 32; a += blockDim.y) {
+    const int64_t r = col_unit ? r0 + a : r0 + threadIdx.x;
+    const int64_t c = col_unit ? c0 + threadIdx.x : c0 + a;
+    const double v = (r < rows && c < k) ? src[r * rs + c * cs] : 0.0;
+    if (col_unit)
+      tile[a][threadIdx.x] = v;
+    else
+      tile[threadIdx.x][a] = v;
+  }
+  __syncthreads();
+  for (int a = threadIdx.y; a < 32; a += blockDim.y) {
+    const int64_t r = r0 + a, c = c0 + threadIdx.x;
+    if (r < rows_p && c < k_p) {
+      const double x = tile[a][threadIdx.x];
+      const float h = to_tf32(static_cast<float>(x));
+      hi[r * k_p + c] = h;
+      lo[r * k_p + c] = to_tf32(static_cast<float>(x - static_cast<double>(h)));
+    }
+  }
+}
+
+// C(i, j) (column-major, ldc) = alpha P[j * ldp + i] + beta C(i, j) - shift [i == j]
+// for i < m, j < n: the FP64 store of an engine product P = C^T (row-major FP32).
+// upper: P is symmetric and only its 128 x 128 tiles on and above the
+// diagonal were formed; entries below are read from their mirror.
+__global__ void combine_kernel(const float *P, int64_t ldp, double *C, int64_t ldc, int64_t m,
+                               int64_t n, double alpha, double beta, double shift, bool upper) {
+  const int64_t total = m * n;
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t j = t / m, i = t % m;
+    const bool mirror = upper && (j >> 7) > (i >> 7);
+    double v = alpha * static_cast<double>(mirror ? P[i * ldp + j] : P[j * ldp + i]);
+    if (beta != 0.0) v += beta * C[j * ldc + i];
+    if (i == j) v -= shift;
+    C[j * ldc + i] = v;
+  }
+}
+
 __global__ void identity_kernel(double *a, int64_t n, double diag_shift, bool set) {
   const int64_t total = n * n;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
@@ -190,6 +273,33 @@ void launch_lower_copy(const double *A, int64_t lda, double *T, int ib, cudaStre
 void launch_zero_strict_upper_cm(double *a, int64_t n, cudaStream_t st) {
   count_launch();
   zero_strict_upper_cm_kernel<<<blocks(n * n), 256, 0, st>>>(a, n);
+}
+
+int launch_trtri_diag_blocks(double *A, int64_t n, int64_t lda, int nb, cudaStream_t st) {
+  const size_t smem = sizeof(double) * (static_cast<size_t>(nb) * nb + nb);
+  // the attribute is per device, so it is set on every call (a host-side write)
+  if (cudaFuncSetAttribute(trtri_diag_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem)) != cudaSuccess)
+    return MBPT_ERR_CUDA;
+  count_launch();
+  trtri_diag_blocks_kernel<<<static_cast<unsigned>((n + nb - 1) / nb), 128, smem, st>>>(A, n, lda,
+                                                                                      nb);
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+void launch_strided_to_tf32(const double *src, int64_t rows, int64_t k, int64_t rs, int64_t cs,
+                            float *hi, float *lo, int64_t rows_p, int64_t k_p, cudaStream_t st) {
+  count_launch();
+  dim3 grid(static_cast<unsigned>((k_p + 31) / 32), static_cast<unsigned>((rows_p + 31) / 32));
+  strided_to_tf32_kernel<<<grid, dim3(32, 8), 0, st>>>(src, rows, k, rs, cs, hi, lo, rows_p,
+                                                       k_p);
+}
+
+void launch_combine(const float *P, int64_t ldp, double *C, int64_t ldc, int64_t m, int64_t n,
+                    double alpha, double beta, double shift, bool upper, cudaStream_t st) {
+  count_launch();
+  combine_kernel<<<blocks(m * n), 256, 0, st>>>(P, ldp, C, ldc, m, n, alpha, beta, shift,
+                                                upper);
 }
 
 void launch_identity(double *a, int64_t n, cudaStream_t st) {

@@ -36,6 +36,11 @@ void launch_minus_identity(double *a, int64_t n, cudaStream_t st);
 void launch_diag(double *a, int64_t n, int nmat, double *diag, bool save, cudaStream_t st);
 void launch_lower_copy(const double *A, int64_t lda, double *T, int ib, cudaStream_t st);
 void launch_zero_strict_upper_cm(double *a, int64_t n, cudaStream_t st);
+int launch_trtri_diag_blocks(double *A, int64_t n, int64_t lda, int nb, cudaStream_t st);
+void launch_strided_to_tf32(const double *src, int64_t rows, int64_t k, int64_t rs, int64_t cs,
+                            float *hi, float *lo, int64_t rows_p, int64_t k_p, cudaStream_t st);
+void launch_combine(const float *P, int64_t ldp, double *C, int64_t ldc, int64_t m, int64_t n,
+                    double alpha, double beta, double shift, bool upper, cudaStream_t st);
 
 namespace {
 std::atomic<long long> g_launches{0};
@@ -214,44 +219,72 @@ int chi0_run(const double *X, const Dims &d, const double *eps, double mu, const
 // Block size of the LAUUM below; its DGEMM/DSYRK updates carry the flops.
 constexpr int64_t kLauumBlock = 512;
 
-// In place over the column-major lower triangle of an n x n factor L (the
-// row-major upper triangle of the buffer): L <- L^-1 (cuSOLVER trtri), then
-// L^-1 <- (L^-1)^T L^-1 (a blocked LAUUM on cuBLAS level 3, LAPACK's
-// blocking), leaving A^-1 = L^-T L^-1 in the same triangle. `T` is ib x ib
-// scratch. Replaces potri, whose LAUUM half runs far below DGEMM speed.
-// Below this size the triangular inverse is cuSOLVER's trtri; above it the
-// recursion turns the work into dense DGEMMs.
-constexpr int64_t kTrtriLeaf = 512;
+// Diagonal blocks of the triangular inverse, inverted all at once in shared
+// memory (one CTA per block); the recursion above them turns the rest into
+// dense products.
+constexpr int64_t kTrtriLeaf = 128;
+
+// Scratch of the FP64 products routed through the TF32x3 engine.
+struct SplitScratch {
+  float *a_hi = nullptr, *a_lo = nullptr, *b_hi = nullptr, *b_lo = nullptr, *p = nullptr;
+  int64_t cap = 0;  // floats per buffer
+};
+
+// Column-major C (m x n, ldc) = alpha op(A) op(B) + beta C - shift I in FP64
+// storage, the product on the tensor cores as TF32 hi/lo pairs (three
+// products, FP32 drained accumulation, ~2^-22 relative). The engine forms
+// P = C^T row-major = op(B)^T op(A)^T, i.e. its operands are A_e = op(B)^T and
+// B_e = op(A), both K-contiguous after the conversion.
+// band: umma::Band flags of the engine operands A_e, B_e (the engine's M
+// rows are C's columns).
+int gemm_f64_split(const double *A, int64_t lda, bool ta, const double *B, int64_t ldb, bool tb,
+                   double *C, int64_t ldc, int64_t m, int64_t n, int64_t k, double alpha,
+                   double beta, double shift, const SplitScratch &s, int *err, cudaStream_t st,
+                   int band = 0) {
+  const int64_t mp = round_up(m, 128), np = round_up(n, 128), kp = round_up(k, 32);
+  if (np * kp > s.cap || mp * kp > s.cap || np * mp > s.cap) return MBPT_ERR_WORKSPACE;
+  // A_e(j, kk) = op(B)(kk, j);  B_e(i, kk) = op(A)(i, kk)
+  launch_strided_to_tf32(B, n, k, tb ? 1 : ldb, tb ? ldb : 1, s.a_hi, s.a_lo, np, kp, st);
+  launch_strided_to_tf32(A, m, k, ta ? lda : 1, ta ? 1 : lda, s.b_hi, s.b_lo, mp, kp, st);
+  SplitMat Ae{s.a_hi, s.a_lo, np, kp, kp, true}, Be{s.b_hi, s.b_lo, mp, kp, kp, true};
+  umma::EpiArgs e;
+  e.outf = s.p;
+  e.ld_outf = mp;
+  e.alpha = 1.f;
+  const int rc = gemm_split(umma::EPI_F32, 1, &Ae, &Be, np, mp, e, err, st, band);
+  if (rc) return rc;
+  launch_combine(s.p, mp, C, ldc, m, n, alpha, beta, shift, false, st);
+  return MBPT_OK;
+}
 
 // In place: the lower-triangular column-major block at A (n x n, leading
-// dimension lda, zeros above its diagonal) becomes its inverse, by
+// dimension lda, zeros above its diagonal, its kTrtriLeaf diagonal blocks
+// already inverted) becomes its inverse, by
 // [[L11, 0], [L21, L22]]^-1 = [[L11^-1, 0], [-L22^-1 L21 L11^-1, L22^-1]]
-// with both halves inverted first; T holds (n - n/2) x (n/2) doubles.
-int trtri_rec(Handles &h, double *A, int64_t n, int64_t lda, double *T, double *tw,
-              size_t tw_bytes, std::vector<char> &host_ws, int *info) {
-  if (n <= kTrtriLeaf) {
-    size_t dbytes = 0, hbytes = 0;
-    if (cusolverDnXtrtri_bufferSize(h.solver, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, n,
-                                    CUDA_R_64F, A, lda, &dbytes, &hbytes) !=
-        CUSOLVER_STATUS_SUCCESS)
-      return MBPT_ERR_CUDA;
-    if (dbytes > tw_bytes) return MBPT_ERR_WORKSPACE;
-    if (host_ws.size() < hbytes) host_ws.resize(hbytes);
-    return cusolverDnXtrtri(h.solver, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, n,
-                            CUDA_R_64F, A, lda, tw, dbytes, host_ws.data(), hbytes, info) ==
-                   CUSOLVER_STATUS_SUCCESS
-               ? MBPT_OK
-               : MBPT_ERR_CUDA;
-  }
-  const int64_t n1 = round_up(n / 2, 64), n2 = n - n1;
+// with both halves inverted first (n1 a multiple of kTrtriLeaf keeps the
+// leaves on the diagonal blocks). T holds (n - n1) x n1 doubles. The two
+// products run in FP64 (cuBLAS) or, with `split`, on the tensor cores.
+int trtri_rec(Handles &h, double *A, int64_t n, int64_t lda, double *T, const SplitScratch *split,
+              int *err, cudaStream_t st) {
+  if (n <= kTrtriLeaf) return MBPT_OK;
+  const int64_t n1 = round_up(n / 2, kTrtriLeaf), n2 = n - n1;
   double *L11 = A, *L21 = A + n1, *L22 = A + n1 + n1 * lda;
-  int rc = trtri_rec(h, L11, n1, lda, T, tw, tw_bytes, host_ws, info);
+  int rc = trtri_rec(h, L11, n1, lda, T, split, err, st);
   if (rc) return rc;
-  rc = trtri_rec(h, L22, n2, lda, T, tw, tw_bytes, host_ws, info);
+  rc = trtri_rec(h, L22, n2, lda, T, split, err, st);
   if (rc) return rc;
+  // T = L21 L11^-1, then L21 <- -L22^-1 T
+  if (split) {
+    // engine rows j of A_e = (L11^-1)^T vanish for k < j; rows i of
+    // B_e = L22^-1 vanish for k > i
+    rc = gemm_f64_split(L21, lda, false, L11, lda, false, T, n2, n2, n1, n1, 1.0, 0.0, 0.0,
+                        *split, err, st, umma::BAND_K_FROM_M);
+    if (rc) return rc;
+    return gemm_f64_split(L22, lda, false, T, n2, false, L21, lda, n2, n1, n2, -1.0, 0.0, 0.0,
+                          *split, err, st, umma::BAND_K_TO_N);
+  }
   const double one = 1.0, zero = 0.0, minus = -1.0;
   const int i1 = static_cast<int>(n1), i2 = static_cast<int>(n2), il = static_cast<int>(lda);
-  // T = L21 L11^-1, then L21 <- -L22^-1 T
   if (cublasDgemm(h.blas, CUBLAS_OP_N, CUBLAS_OP_N, i2, i1, i1, &one, L21, il, L11, il, &zero,
                   T, i2) != CUBLAS_STATUS_SUCCESS ||
       cublasDgemm(h.blas, CUBLAS_OP_N, CUBLAS_OP_N, i2, i1, i2, &minus, L22, il, T, i2, &zero,
@@ -260,13 +293,48 @@ int trtri_rec(Handles &h, double *A, int64_t n, int64_t lda, double *T, double *
   return MBPT_OK;
 }
 
-int spd_inverse_from_factor(Handles &h, double *L, int64_t n, double *tw, size_t tw_bytes,
-                            std::vector<char> &host_ws, int *info, double *T, double *Tr,
-                            cudaStream_t st) {
+// W - I from the Cholesky factor L of 1 - chi0 (column-major lower, in place;
+// the row-major upper triangle of the buffer). Both modes: diagonal blocks of
+// L^-1 in shared memory, the rest by the recursion above. FP64 mode: the
+// recursion on DGEMMs, then (L^-1)^T L^-1 by a blocked LAUUM on cuBLAS level 3
+// (LAPACK's blocking) into the same triangle, which the caller mirrors and
+// shifts by -I; this replaces potri, whose LAUUM half runs far below DGEMM
+// speed. Mixed mode: the recursion's products and W = (L^-1)^T L^-1 itself on
+// the tensor cores, W - I written whole (returns with *full = true).
+struct TimingTag {
+  explicit TimingTag(int tag) { timing_tag(tag); }
+  ~TimingTag() { timing_tag(-1); }
+};
+
+int spd_inverse_from_factor(Handles &h, double *L, int64_t n, double *T, double *Tr,
+                            const SplitScratch *split, int *err, bool *full, cudaStream_t st) {
+  *full = false;
+  TimingTag tag(kTimingDyson);
   // the dense products of the recursion need zeros above the diagonal
   launch_zero_strict_upper_cm(L, n, st);
-  int rc = trtri_rec(h, L, n, n, Tr, tw, tw_bytes, host_ws, info);
+  int rc = launch_trtri_diag_blocks(L, n, n, static_cast<int>(kTrtriLeaf), st);
   if (rc) return rc;
+  rc = trtri_rec(h, L, n, n, Tr, split, err, st);
+  if (rc) return rc;
+  if (split) {
+    // A_e = B_e = (L^-1)^T: row r is column r of L^-1, contiguous in the buffer
+    const int64_t np = round_up(n, 128), kp = round_up(n, 32);
+    if (np * kp > split->cap || np * np > split->cap) return MBPT_ERR_WORKSPACE;
+    launch_strided_to_tf32(L, n, n, n, 1, split->a_hi, split->a_lo, np, kp, st);
+    SplitMat Ae{split->a_hi, split->a_lo, np, kp, kp, true};
+    umma::EpiArgs e;
+    e.outf = split->p;
+    e.ld_outf = np;
+    e.alpha = 1.f;
+    // rows r of (L^-1)^T vanish for k < r, and W is symmetric: the tiles on
+    // and above the diagonal, each over K >= its column start, then mirrored
+    rc = gemm_split(umma::EPI_F32, 1, &Ae, &Ae, np, np, e, err, st,
+                    umma::BAND_K_FROM_M | umma::BAND_K_FROM_N | umma::BAND_UPPER);
+    if (rc) return rc;
+    launch_combine(split->p, np, L, n, n, n, 1.0, 0.0, 1.0, true, st);
+    *full = true;
+    return MBPT_OK;
+  }
   const double one = 1.0, zero = 0.0;
   const int lda = static_cast<int>(n);
   for (int64_t i = 0; i < n; i += kLauumBlock) {
@@ -306,6 +374,7 @@ struct DysonBufs {
   double *rhs;   // n x n right-hand side of the LU inverse of a failed frequency
   double *diag;  // nfreq x n diagonals of 1 - chi0, which the factorisation overwrites
   double *T;     // diagonal-block scratch of the LAUUM
+  SplitScratch split;  // mixed mode: tensor-core products of the inverse
   int lwork;
 };
 
@@ -317,15 +386,10 @@ int dyson_lwork(int64_t n) {
                               static_cast<int>(n), &l1);
   cusolverDnDgetrf_bufferSize(h.solver, static_cast<int>(n), static_cast<int>(n), nullptr,
                               static_cast<int>(n), &l3);
-  size_t tb = 0, th = 0;
-  cusolverDnXtrtri_bufferSize(h.solver, CUBLAS_FILL_MODE_LOWER, CUBLAS_DIAG_NON_UNIT, n,
-                              CUDA_R_64F, nullptr, n, &tb, &th);
-  const int l2 = static_cast<int>((tb + 7) / 8);
-  int l = l1 > l2 ? l1 : l2;
-  return l > l3 ? l : l3;
+  return l1 > l3 ? l1 : l3;
 }
 
-DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq) {
+DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq, int mode = MBPT_MODE_FP64) {
   DysonBufs b{};
   b.lwork = dyson_lwork(n);
   b.info = ar.take<int>(nfreq + 1);
@@ -334,12 +398,22 @@ DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq) {
   b.rhs = ar.take<double>(n * n);
   b.diag = ar.take<double>(n * static_cast<int64_t>(nfreq));
   b.T = ar.take<double>(kLauumBlock * kLauumBlock);
+  if (mode == MBPT_MODE_MIXED) {
+    const int64_t cap = round_up(n, 128) * round_up(n, 128);
+    b.split.cap = cap;
+    b.split.a_hi = ar.take<float>(cap);
+    b.split.a_lo = ar.take<float>(cap);
+    b.split.b_hi = ar.take<float>(cap);
+    b.split.b_lo = ar.take<float>(cap);
+    b.split.p = ar.take<float>(cap);
+  }
   return b;
 }
 
 int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, double *trace,
-              int *info_host, int *sign_host, Arena &ar, cudaStream_t st) {
-  DysonBufs b = carve_dyson(ar, n, nfreq);
+              int *info_host, int *sign_host, Arena &ar, cudaStream_t st,
+              int mode = MBPT_MODE_FP64, int *err = nullptr) {
+  DysonBufs b = carve_dyson(ar, n, nfreq, mode);
   if (ar.overflow()) return MBPT_ERR_WORKSPACE;
   Handles &h = handles(st);
   const int ni = static_cast<int>(n);
@@ -351,7 +425,6 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
       return MBPT_ERR_CUDA;
   }
   std::vector<int> info(nfreq);
-  std::vector<char> host_ws;
   cudaMemcpyAsync(info.data(), b.info, sizeof(int) * nfreq, cudaMemcpyDeviceToHost, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return MBPT_ERR_CUDA;
   bool bad = false;
@@ -365,10 +438,12 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
     double *m = chi0 + f * n * n;
     if (info[f] == 0) {
       if (want_w) {
-        const int rc = spd_inverse_from_factor(h, m, n, b.work, sizeof(double) * b.lwork,
-                                               host_ws, b.info + nfreq, b.T, b.rhs, st);
+        bool full = false;
+        const int rc = spd_inverse_from_factor(h, m, n, b.T, b.rhs,
+                                               mode == MBPT_MODE_MIXED ? &b.split : nullptr,
+                                               err, &full, st);
         if (rc) return rc;
-        launch_symmetrize_minus_identity(m, n, 1, st);
+        if (!full) launch_symmetrize_minus_identity(m, n, 1, st);
       }
       continue;
     }
@@ -680,20 +755,21 @@ int mbpt_chi0_sweep(const double *X, int64_t M, int64_t norb, int64_t nocc, cons
   return chi0_run(X, d, eps, mu, D, tau, ntau, cw, nfreq, mode, chi0, proj, ar, err, S(stream));
 }
 
-size_t mbpt_dyson_workspace_bytes(int64_t naux, int nfreq) {
+size_t mbpt_dyson_workspace_bytes(int64_t naux, int nfreq, int mode) {
   Arena ar;
   ar.counting = true;
-  carve_dyson(ar, naux, nfreq);
+  carve_dyson(ar, naux, nfreq, mode);
   return ar.used + 2048;
 }
 
-int mbpt_dyson(double *chi0, int64_t naux, int nfreq, int want_w, double *logdet,
+int mbpt_dyson(double *chi0, int64_t naux, int nfreq, int want_w, int mode, double *logdet,
                double *trace, int *info_host, int *sign_host, void *ws, size_t ws_bytes,
-               void *stream) {
+               int *err, void *stream) {
   if (naux < 1 || nfreq < 1) return MBPT_ERR_SHAPE;
+  if (mode != MBPT_MODE_FP64 && mode != MBPT_MODE_MIXED) return MBPT_ERR_UNSUPPORTED;
   Arena ar = arena(ws, ws_bytes);
   return dyson_run(chi0, naux, nfreq, want_w, logdet, trace, info_host, sign_host, ar,
-                   S(stream));
+                   S(stream), mode, err);
 }
 
 size_t mbpt_rpa_energy_workspace_bytes(int64_t M, int64_t norb, int64_t nocc, int64_t naux,

@@ -47,7 +47,7 @@ bool make_tmap(CUtensorMap *m, const void *base, int64_t rows, int64_t cols, int
 
 template <int NACC, int BN, int EPI, bool TF32, int DRAIN>
 int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
-           const umma::EpiArgs &e, int *err, cudaStream_t st) {
+           const umma::EpiArgs &e, int *err, cudaStream_t st, int band = 0) {
   using L = umma::Layout<NACC, BN, (DRAIN > 0)>;
   if (m_rows % umma::BM || n_rows % BN || m_rows <= 0 || n_rows <= 0) return MBPT_ERR_SHAPE;
   const int64_t bk = TF32 ? 32 : 64;
@@ -65,6 +65,7 @@ int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
   }
   p.tiles_m = static_cast<int>(m_rows / umma::BM);
   p.tiles_n = static_cast<int>(n_rows / BN);
+  p.band = band;
   p.epi = e;
   p.err = err;
   auto kern = umma::gemm_split_kernel<NACC, BN, EPI, TF32, DRAIN>;
@@ -95,21 +96,35 @@ struct Timing {
     cudaEvent_t a, b;
   };
   std::vector<Rec> pending;
+  std::vector<cudaEvent_t> pool;  // events of drained records, reused
   double total_ms[8] = {0};
   long long launches[8] = {0};
+  cudaEvent_t take() {
+    cudaEvent_t e = nullptr;
+    if (!pool.empty()) {
+      e = pool.back();
+      pool.pop_back();
+    } else {
+      cudaEventCreate(&e);
+    }
+    return e;
+  }
 };
 Timing &timing() {
   static Timing t;
   return t;
 }
+thread_local int g_timing_tag = -1;
 }  // namespace
+
+void timing_tag(int tag) { g_timing_tag = tag; }
 
 bool timing_begin(cudaStream_t st, cudaEvent_t *a, cudaEvent_t *b) {
   Timing &t = timing();
   std::lock_guard<std::mutex> g(t.mu);
   if (!t.on) return false;
-  cudaEventCreate(a);
-  cudaEventCreate(b);
+  *a = t.take();
+  *b = t.take();
   cudaEventRecord(*a, st);
   return true;
 }
@@ -118,7 +133,7 @@ void timing_end(cudaStream_t st, int epi, cudaEvent_t a, cudaEvent_t b) {
   Timing &t = timing();
   cudaEventRecord(b, st);
   std::lock_guard<std::mutex> g(t.mu);
-  t.pending.push_back({epi, a, b});
+  t.pending.push_back({g_timing_tag >= 0 ? g_timing_tag : epi, a, b});
 }
 
 int gemm_timing(int enable, double *total_ms, long long *launches) {
@@ -130,8 +145,8 @@ int gemm_timing(int enable, double *total_ms, long long *launches) {
     cudaEventElapsedTime(&ms, r.a, r.b);
     t.total_ms[r.epi & 7] += ms;
     t.launches[r.epi & 7] += 1;
-    cudaEventDestroy(r.a);
-    cudaEventDestroy(r.b);
+    t.pool.push_back(r.a);
+    t.pool.push_back(r.b);
   }
   t.pending.clear();
   if (total_ms && launches) {
@@ -147,12 +162,19 @@ int gemm_timing(int enable, double *total_ms, long long *launches) {
 }
 
 int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t m_rows,
-               int64_t n_rows, const umma::EpiArgs &e, int *err, cudaStream_t st) {
+               int64_t n_rows, const umma::EpiArgs &e, int *err, cudaStream_t st, int band) {
   using namespace umma;
   // K slabs per drained chunk of the last accumulator: 24 accumulation steps
   // (~1e-6 relative truncation bias, against ~4e-5 for an undrained K = 7296)
   constexpr int kDrain = 2;
   const bool tf = nacc > 0 && A[0].tf32;
+  if (band) {
+    // triangular K spans: the single drained FP32-store TF32 product only (its
+    // spans are never empty for the operand shapes the flags describe)
+    if (!tf || nacc != 1 || epi != EPI_F32) return MBPT_ERR_UNSUPPORTED;
+    if ((band & BAND_UPPER) && m_rows != n_rows) return MBPT_ERR_SHAPE;
+    return launch<1, 128, EPI_F32, true, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
+  }
   if (tf) {
     if (nacc == 2 && epi == EPI_HADAMARD_SPLIT)
       return launch<2, 128, EPI_HADAMARD_SPLIT, true, kDrain>(A, B, m_rows, n_rows, e, err, st);

@@ -16,13 +16,19 @@ struct SplitMat {
 };
 
 // C (m_rows x n_rows tile grid, both multiples of 128) from nacc problems
-// A[j] B[j]^T with the fused epilogue `epi`.
+// A[j] B[j]^T with the fused epilogue `epi`. band: umma::Band flags of
+// triangular operands (the TF32 single-product FP32 store only).
 int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t m_rows,
-               int64_t n_rows, const umma::EpiArgs &e, int *err, cudaStream_t st);
+               int64_t n_rows, const umma::EpiArgs &e, int *err, cudaStream_t st,
+               int band = 0);
 
 // Per-epilogue totals of the engine's launch times (enable = 1 starts
 // recording; a call with non-null outputs drains, returns and resets them).
 int gemm_timing(int enable, double *total_ms, long long *launches);
+// Records the calling thread's next engine launches under category `tag`
+// instead of their epilogue kind (-1: back to the epilogue kind).
+void timing_tag(int tag);
+constexpr int kTimingDyson = 6;  // TF32 products of the Dyson step's inverse
 
 // Bump allocator over a caller's workspace (1024-byte aligned slices).
 struct Arena {

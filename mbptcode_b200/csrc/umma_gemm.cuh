@@ -42,11 +42,25 @@ struct EpiArgs {
   double *sig0 = nullptr, *sig1 = nullptr;
 };
 
+// Structure of triangular operands, for products whose rows vanish on one
+// side of the diagonal in K: each output tile then runs only the K slabs that
+// can be nonzero (and, for a symmetric product, only tiles on or above the
+// diagonal). A row r of A (rows = the M dimension) that is zero for k < r
+// gives BAND_K_FROM_M: the tile starting at row m0 starts its K loop at m0.
+enum Band : int {
+  BAND_K_FROM_M = 1,  // A(r, k) = 0 for k < r
+  BAND_K_FROM_N = 2,  // B(r, k) = 0 for k < r
+  BAND_K_TO_M = 4,    // A(r, k) = 0 for k > r
+  BAND_K_TO_N = 8,    // B(r, k) = 0 for k > r
+  BAND_UPPER = 16,    // symmetric output: tiles below the diagonal are not formed
+};
+
 template <int NACC>
 struct Params {
   CUtensorMap tm[4 * NACC];  // per accumulator: A hi, A lo, B hi, B lo
   int k_tiles[NACC];
   int tiles_m, tiles_n;
+  int band;  // Band flags (0: dense)
   EpiArgs epi;
   int *err;
 };
@@ -266,6 +280,19 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
   const int tn = (pid % per_group) / gsize;
   const int m0 = tm * BM, n0 = tn * BN;
   constexpr int kLast = NACC - 1;
+  // uniform across the CTA, before any barrier or TMEM exists
+  if ((p.band & BAND_UPPER) && tn < tm) return;
+  // K slabs [kb, ke) of accumulator j that can hold nonzeros for this tile
+  constexpr int kSlab = TF32 ? 32 : BK;
+  auto k_span = [&](int j, int &kb, int &ke) {
+    kb = 0;
+    ke = p.k_tiles[j];
+    if (p.band & BAND_K_FROM_M) kb = max(kb, m0 / kSlab);
+    if (p.band & BAND_K_FROM_N) kb = max(kb, n0 / kSlab);
+    if (p.band & BAND_K_TO_M) ke = min(ke, (m0 + BM) / kSlab);
+    if (p.band & BAND_K_TO_N) ke = min(ke, (n0 + BN) / kSlab);
+    ke = max(ke, kb);
+  };
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < L::kStages; ++s) {
@@ -298,14 +325,16 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
       int it = 0;
       bool ok = true;
       for (int j = 0; j < NACC && ok; ++j) {
-        for (int kt = 0; kt < p.k_tiles[j]; ++kt, ++it) {
+        int kb, ke;
+        k_span(j, kb, ke);
+        for (int kt = kb; kt < ke; ++kt, ++it) {
           const int s = it % L::kStages;
           const uint32_t ph = (it / L::kStages) & 1;
           if (!mbar_wait(&empty[s], ph ^ 1)) { ok = false; break; }
           mbar_expect_tx(&full[s], L::kStageBytes);
           uint8_t *st = smem + s * L::kStageBytes;
           // K coordinate in elements: one 128-byte row per slab
-          const int kx = kt * (TF32 ? 32 : BK);
+          const int kx = kt * kSlab;
           tma_load_2d(st, &p.tm[4 * j + 0], kx, m0, &full[s]);
           tma_load_2d(st + L::kABytes, &p.tm[4 * j + 1], kx, m0, &full[s]);
           tma_load_2d(st + 2 * L::kABytes, &p.tm[4 * j + 2], kx, n0, &full[s]);
@@ -331,10 +360,13 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
         const bool drained = DRAIN > 0 && j == kLast;
         uint32_t d = tmem + static_cast<uint32_t>(j * BN);
         int buf = 0;
-        for (int kt = 0; kt < p.k_tiles[j]; ++kt, ++it) {
-          const bool chunk_start = drained && (kt % (DRAIN > 0 ? DRAIN : 1)) == 0;
+        int kb, ke;
+        k_span(j, kb, ke);
+        for (int kt = kb; kt < ke; ++kt, ++it) {
+          const int q = kt - kb;  // slab index within this tile's K span
+          const bool chunk_start = drained && (q % (DRAIN > 0 ? DRAIN : 1)) == 0;
           if (chunk_start) {
-            const int c = kt / (DRAIN > 0 ? DRAIN : 1);
+            const int c = q / (DRAIN > 0 ? DRAIN : 1);
             buf = c & 1;
             if (!mbar_wait(&dempty[buf], ((c >> 1) & 1) ^ 1)) { ok = false; break; }
             tc_fence_after();
@@ -352,7 +384,7 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
           const uint64_t a_lo = sw128_desc(smem_u32(st + L::kABytes));
           const uint64_t b_hi = sw128_desc(smem_u32(st + 2 * L::kABytes));
           const uint64_t b_lo = sw128_desc(smem_u32(st + 2 * L::kABytes + L::kBBytes));
-          const bool restart = drained ? chunk_start : kt == 0;
+          const bool restart = drained ? chunk_start : q == 0;
 #pragma unroll
           for (int kk = 0; kk < 4; ++kk) {
             const uint64_t adv = static_cast<uint64_t>(kk * 2);  // 32 bytes >> 4
@@ -360,7 +392,7 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
                        (restart && kk == 0) ? 1u : 0u);
           }
           mma_commit(&empty[s]);
-          if (drained && ((kt + 1) % (DRAIN > 0 ? DRAIN : 1) == 0 || kt + 1 == p.k_tiles[j]))
+          if (drained && ((q + 1) % (DRAIN > 0 ? DRAIN : 1) == 0 || kt + 1 == ke))
             mma_commit(&dfull[buf]);
         }
       }
@@ -381,7 +413,9 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
     if constexpr (DRAIN > 0) {
 #pragma unroll
       for (int i = 0; i < BN; ++i) acc[i] = 0.f;
-      const int nchunks = (p.k_tiles[kLast] + DRAIN - 1) / DRAIN;
+      int kb, ke;
+      k_span(kLast, kb, ke);
+      const int nchunks = (ke - kb + DRAIN - 1) / DRAIN;
       for (int c = 0; c < nchunks; ++c) {
         const int b = c & 1;
         if (!mbar_wait(&dfull[b], (c >> 1) & 1) || *reinterpret_cast<volatile int *>(fail)) {

@@ -151,7 +151,8 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
                          precision=precision, stream=stream)
     if ev:
         ev[1].record()
-    logdet, trace, info, _ = dyson_batch(chi0, want_w=True, stream=stream)
+    logdet, trace, info, _ = dyson_batch(chi0, want_w=True, stream=stream,
+                                         precision=precision)
     # E_c from the same factorisations: the frequency axis is a minimax quadrature
     e_c = torch.empty((), dtype=torch.float64, device=dev)
     ow = torch.as_tensor(np.asarray(axes.grid.omega_weights, float), device=dev)

@@ -195,24 +195,29 @@ class NonPositiveDielectric(RuntimeWarning):
     """det(1 - chi0) is not positive at an imaginary frequency."""
 
 
-def dyson_batch(chi0, want_w=True, stream=None):
+def dyson_batch(chi0, want_w=True, stream=None, precision='fp64'):
     """In place over a device tensor (nfreq, naux, naux): chi0 -> W - I (or
     the Cholesky factors). Returns (logdet, trace, info, sign) with logdet and
-    trace on the device and info/sign as host int arrays."""
+    trace on the device and info/sign as host int arrays. The factorisation
+    and log-determinant are FP64 in both precisions; 'mixed' forms the
+    inverse from the FP64 factor by TF32x3 tensor-core products."""
     dev = chi0.device
+    mode = _mode(precision)
     nfreq, naux = chi0.shape[0], chi0.shape[-1]
     logdet = torch.empty(nfreq, dtype=torch.float64, device=dev)
     trace = torch.empty(nfreq, dtype=torch.float64, device=dev)
     info = np.zeros(nfreq, dtype=np.int32)
     sign = np.ones(nfreq, dtype=np.int32)
-    ws = WORKSPACE.get(lib().mbpt_dyson_workspace_bytes(naux, nfreq), dev)
+    err = _Err(dev)
+    ws = WORKSPACE.get(lib().mbpt_dyson_workspace_bytes(naux, nfreq, mode), dev)
     import ctypes
-    rc = lib().mbpt_dyson(ptr(chi0), naux, nfreq, int(bool(want_w)), ptr(logdet), ptr(trace),
-                          info.ctypes.data_as(ctypes.c_void_p),
+    rc = lib().mbpt_dyson(ptr(chi0), naux, nfreq, int(bool(want_w)), mode, ptr(logdet),
+                          ptr(trace), info.ctypes.data_as(ctypes.c_void_p),
                           sign.ctypes.data_as(ctypes.c_void_p), ptr(ws), ws.numel(),
-                          stream_ptr(stream))
+                          ptr(err.t), stream_ptr(stream))
     if rc not in (_lib.OK, _lib.ERR_NOT_SPD):
         check(rc, 'mbpt_dyson')
+    err.check('mbpt_dyson')
     return logdet, trace, info, sign
 
 

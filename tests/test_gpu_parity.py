@@ -83,6 +83,37 @@ def test_dyson_and_transform_match_oracle(golden):
     assert rel(Wt.cpu().numpy(), g['Wt']) < 1e-12
 
 
+@pytest.mark.parametrize('n', [96, 300, 1000])
+def test_dyson_inverse_both_modes(n):
+    """W - I from the Cholesky factor (shared-memory diagonal blocks, the
+    recursive triangular inverse, L^-T L^-1) against torch's FP64 inverse:
+    FP64 mode to rounding; mixed mode to 5e-6 absolute. 1 - chi0 >= I puts
+    every eigenvalue of W in (0, 1], so each entry of L^-T L^-1 is a sum
+    bounded by 1, which TF32 pairs (2^-22 per factor) and FP32 accumulation
+    (drained every 64 terms) reproduce to a few 2^-22."""
+    g = torch.Generator(device='cpu').manual_seed(n)
+    A = torch.randn(n, n // 2 + 7, generator=g, dtype=torch.float64)
+    chi0 = -(A @ A.T) / n * 3.0
+    chi0 = torch.stack([chi0, 0.25 * chi0]).cuda()
+    eye = torch.eye(n, dtype=torch.float64, device='cuda')
+    ref = torch.linalg.inv(eye - chi0)
+    ref.diagonal(dim1=-2, dim2=-1).sub_(1.0)
+    out = {}
+    for prec in ('fp64', 'mixed'):
+        c = chi0.clone()
+        logdet, trace, info, _ = st.dyson_batch(c, want_w=True, precision=prec)
+        assert not np.any(info)
+        out[prec] = (c, logdet)
+    assert float((out['fp64'][0] - ref).abs().max()) < 1e-12
+    err_mixed = float((out['mixed'][0] - ref).abs().max())
+    print(f'n={n}: mixed max |W - W_ref| {err_mixed:.3e}')
+    assert err_mixed < 5e-6
+    # the factorisation and log-determinant are FP64 in both modes
+    assert torch.equal(out['fp64'][1], out['mixed'][1])
+    want = torch.linalg.slogdet(eye - chi0)[1]
+    assert float((out['fp64'][1] - want).abs().max()) < 1e-10 * n
+
+
 def frontier(nocc, n, width=4):
     return np.arange(max(0, nocc - width), min(n, nocc + width))
 
