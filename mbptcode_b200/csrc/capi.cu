@@ -410,50 +410,123 @@ DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq, int mode = MBPT_MODE_FP64
   return b;
 }
 
+// Per host thread and device: a side stream on which the inverse of one
+// frequency runs while the next frequency factorises on the caller's stream,
+// one event per frequency (its factor, log-determinant and info word are
+// done) and a pinned host copy of the info words.
+struct DysonPipe {
+  cudaStream_t side = nullptr;
+  cudaEvent_t join = nullptr;
+  std::vector<cudaEvent_t> ev;
+  int *info = nullptr;  // pinned host, `cap` ints
+  int cap = 0;
+  bool ok = false;
+};
+
+DysonPipe *dyson_pipe(int nfreq) {
+  thread_local std::vector<std::pair<int, DysonPipe>> pipes;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  DysonPipe *p = nullptr;
+  for (auto &e : pipes)
+    if (e.first == dev) p = &e.second;
+  if (!p) {
+    pipes.emplace_back(dev, DysonPipe{});
+    p = &pipes.back().second;
+    p->ok = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming) == cudaSuccess;
+  }
+  while (p->ok && static_cast<int>(p->ev.size()) < nfreq) {
+    cudaEvent_t e = nullptr;
+    p->ok = cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
+    if (p->ok) p->ev.push_back(e);
+  }
+  if (p->ok && p->cap < nfreq) {
+    if (p->info) cudaFreeHost(p->info);
+    p->info = nullptr;
+    p->ok = cudaHostAlloc(reinterpret_cast<void **>(&p->info), sizeof(int) * nfreq,
+                          cudaHostAllocPortable) == cudaSuccess;
+    p->cap = p->ok ? nfreq : 0;
+  }
+  return p->ok ? p : nullptr;
+}
+
+// Factorise every frequency on `st`; as soon as frequency f's info word is on
+// the host, its inverse goes to the side stream, so that the tensor-core (or
+// DGEMM) inverse of f overlaps the FP64 Cholesky factorisation of f + 1. A
+// frequency that is not positive definite falls back to LU with both streams
+// drained first. The caller's stream waits for the side stream at the end.
 int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, double *trace,
               int *info_host, int *sign_host, Arena &ar, cudaStream_t st,
               int mode = MBPT_MODE_FP64, int *err = nullptr) {
   DysonBufs b = carve_dyson(ar, n, nfreq, mode);
   if (ar.overflow()) return MBPT_ERR_WORKSPACE;
   Handles &h = handles(st);
+  DysonPipe *pp = dyson_pipe(nfreq);
+  if (!pp) return MBPT_ERR_CUDA;
   const int ni = static_cast<int>(n);
   launch_one_minus(chi0, n, nfreq, trace, st);
   launch_diag(chi0, n, nfreq, b.diag, true, st);
-  for (int f = 0; f < nfreq; ++f) {
-    if (cusolverDnDpotrf(h.solver, CUBLAS_FILL_MODE_LOWER, ni, chi0 + f * n * n, ni, b.work,
-                         b.lwork, b.info + f) != CUSOLVER_STATUS_SUCCESS)
-      return MBPT_ERR_CUDA;
-  }
-  std::vector<int> info(nfreq);
-  cudaMemcpyAsync(info.data(), b.info, sizeof(int) * nfreq, cudaMemcpyDeviceToHost, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess) return MBPT_ERR_CUDA;
-  bool bad = false;
-  for (int f = 0; f < nfreq; ++f) {
-    if (info_host) info_host[f] = info[f];
-    if (sign_host) sign_host[f] = 1;
-    bad |= info[f] != 0;
-  }
-  launch_logdet_diag(chi0, n, nfreq, logdet, st);  // overwritten below where bad
-  for (int f = 0; f < nfreq; ++f) {
+  auto factor = [&](int f) -> int {
     double *m = chi0 + f * n * n;
-    if (info[f] == 0) {
+    if (cusolverDnDpotrf(h.solver, CUBLAS_FILL_MODE_LOWER, ni, m, ni, b.work, b.lwork,
+                         b.info + f) != CUSOLVER_STATUS_SUCCESS)
+      return MBPT_ERR_CUDA;
+    // log det from the factor's diagonal before the inverse overwrites it
+    // (replaced below where the factorisation failed)
+    launch_logdet_diag(m, n, 1, logdet + f, st);
+    if (cudaMemcpyAsync(pp->info + f, b.info + f, sizeof(int), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaEventRecord(pp->ev[f], st) != cudaSuccess)
+      return MBPT_ERR_CUDA;
+    return MBPT_OK;
+  };
+  bool bad = false, side_used = false;
+  int rc = factor(0);
+  for (int f = 0; f < nfreq && rc == MBPT_OK; ++f) {
+    if (f + 1 < nfreq && (rc = factor(f + 1)) != MBPT_OK) break;
+    if (cudaEventSynchronize(pp->ev[f]) != cudaSuccess) {
+      rc = MBPT_ERR_CUDA;
+      break;
+    }
+    const int inf = pp->info[f];
+    if (info_host) info_host[f] = inf;
+    if (sign_host) sign_host[f] = 1;
+    double *m = chi0 + f * n * n;
+    if (inf == 0) {
       if (want_w) {
+        side_used = true;
+        if (cudaStreamWaitEvent(pp->side, pp->ev[f], 0) != cudaSuccess) {
+          rc = MBPT_ERR_CUDA;
+          break;
+        }
+        cublasSetStream(h.blas, pp->side);
         bool full = false;
-        const int rc = spd_inverse_from_factor(h, m, n, b.T, b.rhs,
-                                               mode == MBPT_MODE_MIXED ? &b.split : nullptr,
-                                               err, &full, st);
-        if (rc) return rc;
-        if (!full) launch_symmetrize_minus_identity(m, n, 1, st);
+        rc = spd_inverse_from_factor(h, m, n, b.T, b.rhs,
+                                     mode == MBPT_MODE_MIXED ? &b.split : nullptr, err, &full,
+                                     pp->side);
+        cublasSetStream(h.blas, st);
+        if (rc) break;
+        if (!full) launch_symmetrize_minus_identity(m, n, 1, pp->side);
       }
       continue;
     }
-    // not positive definite: restore 1 - chi0 from its untouched triangle,
-    // then LU for log|det| (and the inverse), as the reference's slogdet/inv
+    // not positive definite: drain both streams (the LU shares the scratch),
+    // restore 1 - chi0 from its untouched triangle, then LU for log|det| (and
+    // the inverse), as the reference's slogdet/inv
+    bad = true;
+    if (cudaStreamSynchronize(pp->side) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+      rc = MBPT_ERR_CUDA;
+      break;
+    }
     launch_mirror_lower_to_upper(m, n, st);
     launch_diag(m, n, 1, b.diag + static_cast<int64_t>(f) * n, false, st);
     if (cusolverDnDgetrf(h.solver, ni, ni, m, ni, b.work, b.piv, b.info + nfreq) !=
-        CUSOLVER_STATUS_SUCCESS)
-      return MBPT_ERR_CUDA;
+        CUSOLVER_STATUS_SUCCESS) {
+      rc = MBPT_ERR_CUDA;
+      break;
+    }
     int sgn = 1;
     int *sgn_dev = b.info + nfreq;
     launch_lu_logdet(m, b.piv, n, logdet + f, sgn_dev, st);
@@ -462,14 +535,24 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
       // inverse from the LU factor: solve against the identity, minus I
       launch_identity(b.rhs, n, st);
       if (cusolverDnDgetrs(h.solver, CUBLAS_OP_N, ni, ni, m, ni, b.piv, b.rhs, ni,
-                           b.info + nfreq) != CUSOLVER_STATUS_SUCCESS)
-        return MBPT_ERR_CUDA;
+                           b.info + nfreq) != CUSOLVER_STATUS_SUCCESS) {
+        rc = MBPT_ERR_CUDA;
+        break;
+      }
       cudaMemcpyAsync(m, b.rhs, sizeof(double) * n * n, cudaMemcpyDeviceToDevice, st);
       launch_minus_identity(m, n, st);
     }
-    if (cudaStreamSynchronize(st) != cudaSuccess) return MBPT_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+      rc = MBPT_ERR_CUDA;
+      break;
+    }
     if (sign_host) sign_host[f] = sgn;
   }
+  if (side_used) {
+    cudaEventRecord(pp->join, pp->side);
+    cudaStreamWaitEvent(st, pp->join, 0);
+  }
+  if (rc) return rc;
   if (cudaGetLastError() != cudaSuccess) return MBPT_ERR_CUDA;
   return bad ? MBPT_ERR_NOT_SPD : MBPT_OK;
 }

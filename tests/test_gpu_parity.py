@@ -236,3 +236,34 @@ def test_planted_nonpositive_dielectric_is_flagged():
     assert flags['nonpositive_det'] == [3]
     W = st.dyson_screening(c, correlation=True)
     assert rel(W, np.linalg.inv(np.eye(n) - c) - np.eye(n)) < 1e-10
+
+
+@pytest.mark.parametrize('prec', ['fp64', 'mixed'])
+def test_dyson_batch_with_failed_frequency_inside(prec):
+    """Four frequencies, the second not positive definite: the inverses of the
+    others run on the side stream while the next one factorises, the failed
+    one takes the LU fallback after both streams drain; every output must
+    match the dense FP64 answer and only the failed frequency is flagged."""
+    rng = np.random.default_rng(7)
+    n = 300
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    mats = []
+    for f in range(4):
+        lam = -rng.uniform(0.05, 3.0, n)
+        if f == 1:
+            lam[5] = 1.4
+        mats.append((Q * lam) @ Q.T)
+    chi0 = torch.as_tensor(np.stack(mats), device='cuda')
+    logdet, trace, info, sign = st.dyson_batch(chi0, want_w=True, precision=prec)
+    assert list(info != 0) == [False, True, False, False]
+    assert list(sign) == [1, -1, 1, 1]
+    tol = 1e-10 if prec == 'fp64' else 5e-6
+    for f, c in enumerate(mats):
+        one_minus = np.eye(n) - c
+        s_ref, ld_ref = np.linalg.slogdet(one_minus)
+        assert abs(float(logdet[f]) - ld_ref) < 1e-9 * n
+        assert abs(float(trace[f]) - np.trace(c)) < 1e-9 * n
+        W_ref = np.linalg.inv(one_minus) - np.eye(n)
+        # the LU frequency is FP64 in both modes
+        err = np.abs(chi0[f].cpu().numpy() - W_ref).max()
+        assert err < (1e-10 if f == 1 else tol) * max(1.0, np.abs(W_ref).max()), (f, err)
