@@ -63,8 +63,9 @@ int mbpt_device_supported(int device);
  * with enable = 1 starts recording on the launching streams; a call with
  * non-NULL total_ms/launches (8 entries, indexed by epilogue kind: 0 split
  * store, 1 FP32 store, 2 Hadamard, 3 self-energy Hadamards, 4 row
- * contraction, 5 FP32 accumulate; 6 collects the TF32 products of
- * mbpt_dyson's inverse whatever their epilogue) waits for the recorded launches, returns
+ * contraction, 5 FP32 accumulate, 6 TF32-pair store; 7 collects the TF32
+ * products of mbpt_dyson's inverse whatever their epilogue) waits for the
+ * recorded launches, returns
  * their summed milliseconds and counts, and resets them. */
 long long mbpt_launch_count(void);
 int mbpt_gemm_timing(int enable, double *total_ms, long long *launches);

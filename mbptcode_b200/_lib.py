@@ -127,7 +127,7 @@ def launch_count():
 
 
 EPILOGUES = ('split', 'f32', 'hadamard', 'sigma_hadamard', 'row_contraction', 'f32_acc',
-             'dyson_tf32')
+             'tf32_pair', 'dyson_tf32')
 
 
 def gemm_timing(enable=True, read=False):

@@ -142,7 +142,11 @@ __global__ void zero_strict_upper_cm_kernel(double *a, int64_t n) {
 // matrix in place, one CTA per block: the block is staged row-major in shared
 // memory and inverted row by row (forward substitution against the rows
 // already inverted), so the block never leaves the SM until it is done.
-__global__ void trtri_diag_blocks_kernel(double *A, int64_t n, int64_t lda, int nb) {
+// With c_hi set, the inverted blocks go out as TF32 pairs instead, in two
+// layouts of the padded (ldp) pair arrays: rows of L^-1 (r_*) and columns of
+// L^-1 as rows (c_*), zeros above the diagonal included; A keeps the factor.
+__global__ void trtri_diag_blocks_kernel(double *A, int64_t n, int64_t lda, int nb, float *c_hi,
+                                         float *c_lo, float *r_hi, float *r_lo, int64_t ldp) {
   extern __shared__ double s[];  // m x m row-major block, then one row of L
   const int64_t off = static_cast<int64_t>(blockIdx.x) * nb;
   const int m = static_cast<int>(min(static_cast<int64_t>(nb), n - off));
@@ -163,6 +167,18 @@ __global__ void trtri_diag_blocks_kernel(double *A, int64_t n, int64_t lda, int 
       s[i * m + j] = j == i ? inv : -acc * inv;
     }
     __syncthreads();
+  }
+  if (c_hi) {
+    for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
+      const int r = idx / m, c = idx % m;
+      const float h = to_tf32(static_cast<float>(s[idx]));
+      const float l = to_tf32(static_cast<float>(s[idx] - static_cast<double>(h)));
+      r_hi[(off + r) * ldp + off + c] = h;
+      r_lo[(off + r) * ldp + off + c] = l;
+      c_hi[(off + c) * ldp + off + r] = h;
+      c_lo[(off + c) * ldp + off + r] = l;
+    }
+    return;
   }
   for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
     const int r = idx / m, c = idx % m;
@@ -275,15 +291,16 @@ void launch_zero_strict_upper_cm(double *a, int64_t n, cudaStream_t st) {
   zero_strict_upper_cm_kernel<<<blocks(n * n), 256, 0, st>>>(a, n);
 }
 
-int launch_trtri_diag_blocks(double *A, int64_t n, int64_t lda, int nb, cudaStream_t st) {
+int launch_trtri_diag_blocks(double *A, int64_t n, int64_t lda, int nb, cudaStream_t st,
+                             float *c_hi, float *c_lo, float *r_hi, float *r_lo, int64_t ldp) {
   const size_t smem = sizeof(double) * (static_cast<size_t>(nb) * nb + nb);
   // the attribute is per device, so it is set on every call (a host-side write)
   if (cudaFuncSetAttribute(trtri_diag_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(smem)) != cudaSuccess)
     return MBPT_ERR_CUDA;
   count_launch();
-  trtri_diag_blocks_kernel<<<static_cast<unsigned>((n + nb - 1) / nb), 128, smem, st>>>(A, n, lda,
-                                                                                      nb);
+  trtri_diag_blocks_kernel<<<static_cast<unsigned>((n + nb - 1) / nb), 128, smem, st>>>(
+      A, n, lda, nb, c_hi, c_lo, r_hi, r_lo, ldp);
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 

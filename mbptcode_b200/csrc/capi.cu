@@ -36,7 +36,9 @@ void launch_minus_identity(double *a, int64_t n, cudaStream_t st);
 void launch_diag(double *a, int64_t n, int nmat, double *diag, bool save, cudaStream_t st);
 void launch_lower_copy(const double *A, int64_t lda, double *T, int ib, cudaStream_t st);
 void launch_zero_strict_upper_cm(double *a, int64_t n, cudaStream_t st);
-int launch_trtri_diag_blocks(double *A, int64_t n, int64_t lda, int nb, cudaStream_t st);
+int launch_trtri_diag_blocks(double *A, int64_t n, int64_t lda, int nb, cudaStream_t st,
+                             float *c_hi = nullptr, float *c_lo = nullptr, float *r_hi = nullptr,
+                             float *r_lo = nullptr, int64_t ldp = 0);
 void launch_strided_to_tf32(const double *src, int64_t rows, int64_t k, int64_t rs, int64_t cs,
                             float *hi, float *lo, int64_t rows_p, int64_t k_p, cudaStream_t st);
 void launch_combine(const float *P, int64_t ldp, double *C, int64_t ldc, int64_t m, int64_t n,
@@ -224,67 +226,36 @@ constexpr int64_t kLauumBlock = 512;
 // dense products.
 constexpr int64_t kTrtriLeaf = 128;
 
-// Scratch of the FP64 products routed through the TF32x3 engine.
-struct SplitScratch {
-  float *a_hi = nullptr, *a_lo = nullptr, *b_hi = nullptr, *b_lo = nullptr, *p = nullptr;
-  int64_t cap = 0;  // floats per buffer
+// Mixed-mode scratch of the inverse: TF32 hi/lo pair arrays, np x np each
+// (np = n rounded up to 128), zero outside what the recursion writes.
+//   LR: rows of the factor L (row i along k);
+//   IC: columns of L^-1 as rows, IC(j, k) = L^-1(k, j);
+//   IR: rows of L^-1, IR(i, k) = L^-1(i, k);
+//   TT: one product's T^T between the two products of a recursion node;
+//   P:  FP32 W = L^-T L^-1 before its FP64 store.
+struct PairScratch {
+  float *lr_hi = nullptr, *lr_lo = nullptr, *ic_hi = nullptr, *ic_lo = nullptr;
+  float *ir_hi = nullptr, *ir_lo = nullptr, *tt_hi = nullptr, *tt_lo = nullptr, *p = nullptr;
+  int64_t np = 0;
 };
-
-// Column-major C (m x n, ldc) = alpha op(A) op(B) + beta C - shift I in FP64
-// storage, the product on the tensor cores as TF32 hi/lo pairs (three
-// products, FP32 drained accumulation, ~2^-22 relative). The engine forms
-// P = C^T row-major = op(B)^T op(A)^T, i.e. its operands are A_e = op(B)^T and
-// B_e = op(A), both K-contiguous after the conversion.
-// band: umma::Band flags of the engine operands A_e, B_e (the engine's M
-// rows are C's columns).
-int gemm_f64_split(const double *A, int64_t lda, bool ta, const double *B, int64_t ldb, bool tb,
-                   double *C, int64_t ldc, int64_t m, int64_t n, int64_t k, double alpha,
-                   double beta, double shift, const SplitScratch &s, int *err, cudaStream_t st,
-                   int band = 0) {
-  const int64_t mp = round_up(m, 128), np = round_up(n, 128), kp = round_up(k, 32);
-  if (np * kp > s.cap || mp * kp > s.cap || np * mp > s.cap) return MBPT_ERR_WORKSPACE;
-  // A_e(j, kk) = op(B)(kk, j);  B_e(i, kk) = op(A)(i, kk)
-  launch_strided_to_tf32(B, n, k, tb ? 1 : ldb, tb ? ldb : 1, s.a_hi, s.a_lo, np, kp, st);
-  launch_strided_to_tf32(A, m, k, ta ? lda : 1, ta ? 1 : lda, s.b_hi, s.b_lo, mp, kp, st);
-  SplitMat Ae{s.a_hi, s.a_lo, np, kp, kp, true}, Be{s.b_hi, s.b_lo, mp, kp, kp, true};
-  umma::EpiArgs e;
-  e.outf = s.p;
-  e.ld_outf = mp;
-  e.alpha = 1.f;
-  const int rc = gemm_split(umma::EPI_F32, 1, &Ae, &Be, np, mp, e, err, st, band);
-  if (rc) return rc;
-  launch_combine(s.p, mp, C, ldc, m, n, alpha, beta, shift, false, st);
-  return MBPT_OK;
-}
 
 // In place: the lower-triangular column-major block at A (n x n, leading
 // dimension lda, zeros above its diagonal, its kTrtriLeaf diagonal blocks
 // already inverted) becomes its inverse, by
 // [[L11, 0], [L21, L22]]^-1 = [[L11^-1, 0], [-L22^-1 L21 L11^-1, L22^-1]]
 // with both halves inverted first (n1 a multiple of kTrtriLeaf keeps the
-// leaves on the diagonal blocks). T holds (n - n1) x n1 doubles. The two
-// products run in FP64 (cuBLAS) or, with `split`, on the tensor cores.
-int trtri_rec(Handles &h, double *A, int64_t n, int64_t lda, double *T, const SplitScratch *split,
-              int *err, cudaStream_t st) {
+// leaves on the diagonal blocks). T holds (n - n1) x n1 doubles. FP64 DGEMMs.
+int trtri_rec(Handles &h, double *A, int64_t n, int64_t lda, double *T) {
   if (n <= kTrtriLeaf) return MBPT_OK;
   const int64_t n1 = round_up(n / 2, kTrtriLeaf), n2 = n - n1;
   double *L11 = A, *L21 = A + n1, *L22 = A + n1 + n1 * lda;
-  int rc = trtri_rec(h, L11, n1, lda, T, split, err, st);
+  int rc = trtri_rec(h, L11, n1, lda, T);
   if (rc) return rc;
-  rc = trtri_rec(h, L22, n2, lda, T, split, err, st);
+  rc = trtri_rec(h, L22, n2, lda, T);
   if (rc) return rc;
-  // T = L21 L11^-1, then L21 <- -L22^-1 T
-  if (split) {
-    // engine rows j of A_e = (L11^-1)^T vanish for k < j; rows i of
-    // B_e = L22^-1 vanish for k > i
-    rc = gemm_f64_split(L21, lda, false, L11, lda, false, T, n2, n2, n1, n1, 1.0, 0.0, 0.0,
-                        *split, err, st, umma::BAND_K_FROM_M);
-    if (rc) return rc;
-    return gemm_f64_split(L22, lda, false, T, n2, false, L21, lda, n2, n1, n2, -1.0, 0.0, 0.0,
-                          *split, err, st, umma::BAND_K_TO_N);
-  }
   const double one = 1.0, zero = 0.0, minus = -1.0;
   const int i1 = static_cast<int>(n1), i2 = static_cast<int>(n2), il = static_cast<int>(lda);
+  // T = L21 L11^-1, then L21 <- -L22^-1 T
   if (cublasDgemm(h.blas, CUBLAS_OP_N, CUBLAS_OP_N, i2, i1, i1, &one, L21, il, L11, il, &zero,
                   T, i2) != CUBLAS_STATUS_SUCCESS ||
       cublasDgemm(h.blas, CUBLAS_OP_N, CUBLAS_OP_N, i2, i1, i2, &minus, L22, il, T, i2, &zero,
@@ -293,48 +264,94 @@ int trtri_rec(Handles &h, double *A, int64_t n, int64_t lda, double *T, const Sp
   return MBPT_OK;
 }
 
-// W - I from the Cholesky factor L of 1 - chi0 (column-major lower, in place;
-// the row-major upper triangle of the buffer). Both modes: diagonal blocks of
-// L^-1 in shared memory, the rest by the recursion above. FP64 mode: the
-// recursion on DGEMMs, then (L^-1)^T L^-1 by a blocked LAUUM on cuBLAS level 3
-// (LAPACK's blocking) into the same triangle, which the caller mirrors and
-// shifts by -I; this replaces potri, whose LAUUM half runs far below DGEMM
-// speed. Mixed mode: the recursion's products and W = (L^-1)^T L^-1 itself on
-// the tensor cores, W - I written whole (returns with *full = true).
+// The same recursion on TF32 pairs, for the diagonal block [o, o + n) of L^-1
+// (diagonal kTrtriLeaf blocks already in IC/IR, the factor's rows in LR).
+// Each node is two tensor-core products whose epilogues write pairs straight
+// into the layouts the next products read, so nothing is converted between
+// them. With the engine forming P = A_e B_e^T row by row of A_e:
+//   P1 = T^T = (L11^-1)^T L21^T:  A_e = IC rows (zero for k < row: K from m0),
+//        B_e = LR rows of L21; stored as pairs in TT;
+//   P2 = L21'^T = -(T^T) (L22^-1)^T: A_e = TT, B_e = IR rows of L22^-1 (zero
+//        for k > row: K up to the tile's end); stored into IC and, transposed,
+//        into IR.
+int trtri_pairs(const PairScratch &s, int64_t o, int64_t n, int *err, cudaStream_t st) {
+  if (n <= kTrtriLeaf) return MBPT_OK;
+  const int64_t n1 = round_up(n / 2, kTrtriLeaf), n2 = n - n1, n2p = round_up(n2, 128);
+  int rc = trtri_pairs(s, o, n1, err, st);
+  if (rc) return rc;
+  rc = trtri_pairs(s, o + n1, n2, err, st);
+  if (rc) return rc;
+  const int64_t ld = s.np;
+  auto at = [ld](float *b, int64_t r, int64_t c) { return b + r * ld + c; };
+  SplitMat A1{at(s.ic_hi, o, o), at(s.ic_lo, o, o), n1, n1, ld, true};
+  SplitMat B1{at(s.lr_hi, o + n1, o), at(s.lr_lo, o + n1, o), n2p, n1, ld, true};
+  umma::EpiArgs e1;
+  e1.p_hi = s.tt_hi;
+  e1.p_lo = s.tt_lo;
+  e1.ld_p = ld;
+  e1.alpha = 1.f;
+  rc = gemm_split(umma::EPI_TF32_PAIR, 1, &A1, &B1, n1, n2p, e1, err, st, umma::BAND_K_FROM_M);
+  if (rc) return rc;
+  const int64_t k2 = round_up(n2, 32);
+  SplitMat A2{s.tt_hi, s.tt_lo, n1, k2, ld, true};
+  SplitMat B2{at(s.ir_hi, o + n1, o + n1), at(s.ir_lo, o + n1, o + n1), n2p, k2, ld, true};
+  umma::EpiArgs e2;
+  e2.p_hi = at(s.ic_hi, o, o + n1);
+  e2.p_lo = at(s.ic_lo, o, o + n1);
+  e2.ld_p = ld;
+  e2.t_hi = at(s.ir_hi, o + n1, o);
+  e2.t_lo = at(s.ir_lo, o + n1, o);
+  e2.ld_t = ld;
+  e2.alpha = -1.f;
+  return gemm_split(umma::EPI_TF32_PAIR, 1, &A2, &B2, n1, n2p, e2, err, st, umma::BAND_K_TO_N);
+}
+
 struct TimingTag {
   explicit TimingTag(int tag) { timing_tag(tag); }
   ~TimingTag() { timing_tag(-1); }
 };
 
+// W - I from the Cholesky factor L of 1 - chi0 (column-major lower, in place;
+// the row-major upper triangle of the buffer). FP64 mode: the diagonal blocks
+// of L^-1 in shared memory, the recursion above on DGEMMs, then (L^-1)^T L^-1
+// by a blocked LAUUM on cuBLAS level 3 (LAPACK's blocking) into the same
+// triangle, which the caller mirrors and shifts by -I; this replaces potri,
+// whose LAUUM half runs far below DGEMM speed. Mixed mode (`pairs`): L^-1 as
+// TF32 pairs by the tensor-core recursion, then W = (L^-1)^T L^-1 on the
+// tensor cores over the tiles on and above the diagonal (rows of (L^-1)^T
+// vanish for k < row), W - I written whole (returns with *full = true).
 int spd_inverse_from_factor(Handles &h, double *L, int64_t n, double *T, double *Tr,
-                            const SplitScratch *split, int *err, bool *full, cudaStream_t st) {
+                            const PairScratch *pairs, int *err, bool *full, cudaStream_t st) {
   *full = false;
   TimingTag tag(kTimingDyson);
+  if (pairs) {
+    const PairScratch &s = *pairs;
+    const int64_t np = s.np, kp = round_up(n, 32);
+    // rows of L (its upper triangle is never read)
+    launch_strided_to_tf32(L, n, n, 1, n, s.lr_hi, s.lr_lo, np, np, st);
+    int rc = launch_trtri_diag_blocks(L, n, n, static_cast<int>(kTrtriLeaf), st, s.ic_hi,
+                                      s.ic_lo, s.ir_hi, s.ir_lo, np);
+    if (rc) return rc;
+    rc = trtri_pairs(s, 0, n, err, st);
+    if (rc) return rc;
+    SplitMat Ae{s.ic_hi, s.ic_lo, np, kp, np, true};
+    umma::EpiArgs e;
+    e.outf = s.p;
+    e.ld_outf = np;
+    e.alpha = 1.f;
+    rc = gemm_split(umma::EPI_F32, 1, &Ae, &Ae, np, np, e, err, st,
+                    umma::BAND_K_FROM_M | umma::BAND_K_FROM_N | umma::BAND_UPPER);
+    if (rc) return rc;
+    launch_combine(s.p, np, L, n, n, n, 1.0, 0.0, 1.0, true, st);
+    *full = true;
+    return MBPT_OK;
+  }
   // the dense products of the recursion need zeros above the diagonal
   launch_zero_strict_upper_cm(L, n, st);
   int rc = launch_trtri_diag_blocks(L, n, n, static_cast<int>(kTrtriLeaf), st);
   if (rc) return rc;
-  rc = trtri_rec(h, L, n, n, Tr, split, err, st);
+  rc = trtri_rec(h, L, n, n, Tr);
   if (rc) return rc;
-  if (split) {
-    // A_e = B_e = (L^-1)^T: row r is column r of L^-1, contiguous in the buffer
-    const int64_t np = round_up(n, 128), kp = round_up(n, 32);
-    if (np * kp > split->cap || np * np > split->cap) return MBPT_ERR_WORKSPACE;
-    launch_strided_to_tf32(L, n, n, n, 1, split->a_hi, split->a_lo, np, kp, st);
-    SplitMat Ae{split->a_hi, split->a_lo, np, kp, kp, true};
-    umma::EpiArgs e;
-    e.outf = split->p;
-    e.ld_outf = np;
-    e.alpha = 1.f;
-    // rows r of (L^-1)^T vanish for k < r, and W is symmetric: the tiles on
-    // and above the diagonal, each over K >= its column start, then mirrored
-    rc = gemm_split(umma::EPI_F32, 1, &Ae, &Ae, np, np, e, err, st,
-                    umma::BAND_K_FROM_M | umma::BAND_K_FROM_N | umma::BAND_UPPER);
-    if (rc) return rc;
-    launch_combine(split->p, np, L, n, n, n, 1.0, 0.0, 1.0, true, st);
-    *full = true;
-    return MBPT_OK;
-  }
   const double one = 1.0, zero = 0.0;
   const int lda = static_cast<int>(n);
   for (int64_t i = 0; i < n; i += kLauumBlock) {
@@ -374,7 +391,7 @@ struct DysonBufs {
   double *rhs;   // n x n right-hand side of the LU inverse of a failed frequency
   double *diag;  // nfreq x n diagonals of 1 - chi0, which the factorisation overwrites
   double *T;     // diagonal-block scratch of the LAUUM
-  SplitScratch split;  // mixed mode: tensor-core products of the inverse
+  PairScratch pairs;  // mixed mode: TF32 pairs of the tensor-core inverse
   int lwork;
 };
 
@@ -399,13 +416,12 @@ DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq, int mode = MBPT_MODE_FP64
   b.diag = ar.take<double>(n * static_cast<int64_t>(nfreq));
   b.T = ar.take<double>(kLauumBlock * kLauumBlock);
   if (mode == MBPT_MODE_MIXED) {
-    const int64_t cap = round_up(n, 128) * round_up(n, 128);
-    b.split.cap = cap;
-    b.split.a_hi = ar.take<float>(cap);
-    b.split.a_lo = ar.take<float>(cap);
-    b.split.b_hi = ar.take<float>(cap);
-    b.split.b_lo = ar.take<float>(cap);
-    b.split.p = ar.take<float>(cap);
+    const int64_t np = round_up(n, 128), cap = np * np;
+    PairScratch &q = b.pairs;
+    q.np = np;
+    for (float **f : {&q.lr_hi, &q.lr_lo, &q.ic_hi, &q.ic_lo, &q.ir_hi, &q.ir_lo, &q.tt_hi,
+                      &q.tt_lo, &q.p})
+      *f = ar.take<float>(cap);
   }
   return b;
 }
@@ -467,6 +483,14 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
   const int ni = static_cast<int>(n);
   launch_one_minus(chi0, n, nfreq, trace, st);
   launch_diag(chi0, n, nfreq, b.diag, true, st);
+  if (mode == MBPT_MODE_MIXED && want_w) {
+    // the pair arrays are read as zeros wherever the recursion does not write
+    // (padding, above the diagonal blocks); every frequency writes the rest
+    const size_t bytes = sizeof(float) * b.pairs.np * b.pairs.np;
+    for (float *f : {b.pairs.lr_hi, b.pairs.lr_lo, b.pairs.ic_hi, b.pairs.ic_lo, b.pairs.ir_hi,
+                     b.pairs.ir_lo, b.pairs.tt_hi, b.pairs.tt_lo})
+      if (cudaMemsetAsync(f, 0, bytes, st) != cudaSuccess) return MBPT_ERR_CUDA;
+  }
   auto factor = [&](int f) -> int {
     double *m = chi0 + f * n * n;
     if (cusolverDnDpotrf(h.solver, CUBLAS_FILL_MODE_LOWER, ni, m, ni, b.work, b.lwork,
@@ -503,7 +527,7 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
         cublasSetStream(h.blas, pp->side);
         bool full = false;
         rc = spd_inverse_from_factor(h, m, n, b.T, b.rhs,
-                                     mode == MBPT_MODE_MIXED ? &b.split : nullptr, err, &full,
+                                     mode == MBPT_MODE_MIXED ? &b.pairs : nullptr, err, &full,
                                      pp->side);
         cublasSetStream(h.blas, st);
         if (rc) break;

@@ -28,7 +28,7 @@ int gemm_timing(int enable, double *total_ms, long long *launches);
 // Records the calling thread's next engine launches under category `tag`
 // instead of their epilogue kind (-1: back to the epilogue kind).
 void timing_tag(int tag);
-constexpr int kTimingDyson = 6;  // TF32 products of the Dyson step's inverse
+constexpr int kTimingDyson = 7;  // TF32 products of the Dyson step's inverse
 
 // Bump allocator over a caller's workspace (1024-byte aligned slices).
 struct Arena {

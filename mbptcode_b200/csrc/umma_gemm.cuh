@@ -29,6 +29,7 @@ enum Epi : int {
   EPI_SIGMA_H = 3,         // out0 = acc0 o acc2, out1 = acc1 o acc2 (Go o Zt, Gv o Zt)
   EPI_ROWDOT2 = 4,         // sig0[c] += sum_r xs[r,c] acc0[r,c], sig1[c] -= ... acc1
   EPI_F32_ACC = 5,         // outf += alpha * acc0, FP32 read-modify-write
+  EPI_TF32_PAIR = 6,       // alpha * acc0 as a TF32 hi/lo pair at p (and transposed at t)
 };
 
 struct EpiArgs {
@@ -40,6 +41,10 @@ struct EpiArgs {
   const float *xs = nullptr;
   int64_t ld_xs = 0;
   double *sig0 = nullptr, *sig1 = nullptr;
+  // EPI_TF32_PAIR: row-major pair p (ld_p) and, when t_hi is set, the
+  // transposed pair t (element (r, c) of the tile grid at t[c * ld_t + r])
+  float *p_hi = nullptr, *p_lo = nullptr, *t_hi = nullptr, *t_lo = nullptr;
+  int64_t ld_p = 0, ld_t = 0;
 };
 
 // Structure of triangular operands, for products whose rows vanish on one
@@ -476,6 +481,30 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
               o.x += prev.x; o.y += prev.y; o.z += prev.z; o.w += prev.w;
             }
             dst[q] = o;
+          }
+        } else if constexpr (EPI == EPI_TF32_PAIR) {
+          float hi[32], lo[32];
+#pragma unroll
+          for (int i = 0; i < 32; ++i) {
+            const float v = e.alpha * v0[i];
+            hi[i] = to_tf32(v);
+            lo[i] = to_tf32(v - hi[i]);
+          }
+          float4 *dh = reinterpret_cast<float4 *>(e.p_hi + row * e.ld_p + col);
+          float4 *dl = reinterpret_cast<float4 *>(e.p_lo + row * e.ld_p + col);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            dh[q] = make_float4(hi[4 * q], hi[4 * q + 1], hi[4 * q + 2], hi[4 * q + 3]);
+            dl[q] = make_float4(lo[4 * q], lo[4 * q + 1], lo[4 * q + 2], lo[4 * q + 3]);
+          }
+          if (e.t_hi) {
+            // column col + i of the tile is row col + i of t: the warp's 32
+            // consecutive rows land on 32 consecutive floats
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+              e.t_hi[static_cast<int64_t>(col + i) * e.ld_t + row] = hi[i];
+              e.t_lo[static_cast<int64_t>(col + i) * e.ld_t + row] = lo[i];
+            }
           }
         } else if constexpr (EPI == EPI_HADAMARD_SPLIT) {
           float v1[32];
