@@ -60,7 +60,9 @@ int mbpt_device_supported(int device);
 /* Instrumentation (no counterpart in MBPTcode, which has no device code):
  * the number of this library's kernels launched by the process so far, and
  * CUDA-event timing of the tensor-core engine's launches. mbpt_gemm_timing
- * with enable = 1 starts recording on the launching streams; a call with
+ * with enable = 1 starts recording on the launching streams (enable = 2: all
+ * but category 7, whose many small launches the event pairs would slow down);
+ * a call with
  * non-NULL total_ms/launches (8 entries, indexed by epilogue kind: 0 split
  * store, 1 FP32 store, 2 Hadamard, 3 self-energy Hadamards, 4 row
  * contraction, 5 FP32 accumulate, 6 TF32-pair store; 7 collects the TF32

@@ -130,16 +130,19 @@ EPILOGUES = ('split', 'f32', 'hadamard', 'sigma_hadamard', 'row_contraction', 'f
              'tf32_pair', 'dyson_tf32')
 
 
-def gemm_timing(enable=True, read=False):
+def gemm_timing(enable=True, read=False, families=True):
     """Start/stop CUDA-event timing of the tensor-core engine; with read,
-    return {epilogue: (total ms, launches)} of what was recorded."""
+    return {epilogue: (total ms, launches)} of what was recorded. families
+    False leaves out the Dyson inverse's products (about a hundred small
+    launches per frequency, which per-launch events would slow down)."""
     import numpy as np
+    code = 0 if not enable else (1 if families else 2)
     if not read:
-        check(lib().mbpt_gemm_timing(int(enable), None, None), 'mbpt_gemm_timing')
+        check(lib().mbpt_gemm_timing(code, None, None), 'mbpt_gemm_timing')
         return None
     ms = np.zeros(8)
     n = np.zeros(8, dtype=np.int64)
-    check(lib().mbpt_gemm_timing(int(enable), ms.ctypes.data_as(C.c_void_p),
+    check(lib().mbpt_gemm_timing(code, ms.ctypes.data_as(C.c_void_p),
                                  n.ctypes.data_as(C.c_void_p)), 'mbpt_gemm_timing')
     return {name: (float(ms[i]), int(n[i])) for i, name in enumerate(EPILOGUES) if n[i]}
 

@@ -91,6 +91,7 @@ namespace {
 struct Timing {
   std::mutex mu;
   bool on = false;
+  bool tagged = true;  // also time launches made under a timing_tag
   struct Rec {
     int epi;
     cudaEvent_t a, b;
@@ -122,7 +123,7 @@ void timing_tag(int tag) { g_timing_tag = tag; }
 bool timing_begin(cudaStream_t st, cudaEvent_t *a, cudaEvent_t *b) {
   Timing &t = timing();
   std::lock_guard<std::mutex> g(t.mu);
-  if (!t.on) return false;
+  if (!t.on || (!t.tagged && g_timing_tag >= 0)) return false;
   *a = t.take();
   *b = t.take();
   cudaEventRecord(*a, st);
@@ -158,6 +159,7 @@ int gemm_timing(int enable, double *total_ms, long long *launches) {
     }
   }
   t.on = enable != 0;
+  t.tagged = enable != 2;
   return MBPT_OK;
 }
 

@@ -22,15 +22,50 @@ The coefficient tables are the GreenX ones (Apache-2.0, see data/NOTICE).
 """
 from __future__ import annotations
 
+import contextlib
 import json
 import os
+import threading
 import warnings
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
 
+try:
+    from threadpoolctl import ThreadpoolController
+except ImportError:  # pragma: no cover -- the fits then run on the BLAS's own threads
+    ThreadpoolController = None
+
 _DATA = os.path.join(os.path.dirname(__file__), 'data')
 _TABLES: dict = {}
+
+# The transform fits are many small independent SVDs (~1000 x 24): they run on
+# a shared pool of host threads, each with a single-threaded BLAS.
+_FIT_POOL = ThreadPoolExecutor(max_workers=max(1, min(32, os.cpu_count() or 1)),
+                               thread_name_prefix='mbpt-fit')
+_BLAS = {'ctrl': None, 'depth': 0, 'limit': None, 'lock': threading.Lock()}
+
+
+@contextlib.contextmanager
+def _single_threaded_blas():
+    """One BLAS thread per call while any fit is running (the limit is
+    process-wide, so only the outermost entry sets and restores it)."""
+    b = _BLAS
+    with b['lock']:
+        if b['depth'] == 0 and ThreadpoolController is not None:
+            if b['ctrl'] is None:
+                b['ctrl'] = ThreadpoolController()
+            b['limit'] = b['ctrl'].limit(limits=1)
+        b['depth'] += 1
+    try:
+        yield
+    finally:
+        with b['lock']:
+            b['depth'] -= 1
+            if b['depth'] == 0 and b['limit'] is not None:
+                b['limit'].restore_original_limits()
+                b['limit'] = None
 
 # transform kinds, numbered as GreenX numbers them
 COSINE_TW, COSINE_WT, SINE_TW, SINE_WT = 1, 2, 3, 4
@@ -218,15 +253,22 @@ def transform_weights(kind, tau, omega, e_min, e_max, regularization=None,
     nx = max((int(np.log10(e_max / e_min)) + 1) * nodes_factor, n_in)
     x = e_min * (e_max / e_min) ** (np.arange(nx) / (nx - 1.0))
     W = np.zeros((n_out, n_in))
-    worst = 0.0
-    for i in range(n_out):
+
+    def fit(i):
         psi, A = _fit_problem(kind, tau, omega, i, x)
         U, S, Vt = np.linalg.svd(A, full_matrices=False)
         keep = S > FIT_RCOND * S[0]
         filt = np.zeros_like(S)
         np.divide(S, reg ** 2 + S ** 2, out=filt, where=keep)
         W[i] = Vt.T @ (filt * (U.T @ psi))
-        err = float(np.abs(A @ W[i] - psi).max())
+        return float(np.abs(A @ W[i] - psi).max())
+
+    # the rows are independent: spread over the host's cores, each row's
+    # arithmetic unchanged
+    with _single_threaded_blas():
+        errs = [f.result() for f in [_FIT_POOL.submit(fit, i) for i in range(n_out)]]
+    worst = 0.0
+    for i, err in enumerate(errs):
         if not (np.isfinite(err) and np.isfinite(W[i]).all()):
             raise FloatingPointError(
                 f'transform kind {kind}: row {i} of {n_out} is not finite '
@@ -284,9 +326,13 @@ class TimeFrequencyGrid:
             if with_inverse:
                 kinds.append(('sinft_tw', SINE_WT))
         mats, errs = {}, {}
-        for name, kind in kinds:
-            mats[name], errs[name] = transform_weights(
-                kind, tau, omega_points, e_min, e_max, regularization)
+        # the transforms' rows all go to the fit pool at once
+        with _single_threaded_blas(), ThreadPoolExecutor(max_workers=len(kinds)) as outer:
+            futs = {name: outer.submit(transform_weights, kind, tau, omega_points, e_min,
+                                       e_max, regularization)
+                    for name, kind in kinds}
+            for name, f in futs.items():
+                mats[name], errs[name] = f.result()
         return cls(tau, tw, omega_points, np.asarray(omega_weights, float),
                    fit_errors=errs,
                    meta={'e_min': e_min, 'e_max': e_max, 'ntau': ntau,
@@ -374,11 +420,15 @@ def space_time_axes(eps, nocc, ntau='auto', pade_freq=None, anchor=None,
     ntau = int(ntau)
     freq, fw = screening_frequency_grid(ntau, eps, nocc, mu=mu)
     rW, rS = sigma_fit_ranges(eps, nocc, mu=mu)
-    grid = TimeFrequencyGrid.minimax_split(ntau, e_min, e_max, freq, fw)
     tau_sigma = 0.5 * minimax_time_grid(ntau, *rS)[0]
     pade = pade_nodes() if pade_freq is None else np.asarray(pade_freq, float)
-    Ctw, _ = transform_weights(COSINE_WT, tau_sigma, freq, *rW, warn=False)
-    C, _ = transform_weights(COSINE_TW, tau_sigma, pade, *rS, warn=False)
-    S, _ = transform_weights(SINE_TW, tau_sigma, pade, *rS, warn=False)
+    # the seven transform fits are independent: all in flight at once
+    with _single_threaded_blas(), ThreadPoolExecutor(max_workers=4) as outer:
+        f_grid = outer.submit(TimeFrequencyGrid.minimax_split, ntau, e_min, e_max, freq, fw)
+        f_ctw = outer.submit(transform_weights, COSINE_WT, tau_sigma, freq, *rW, warn=False)
+        f_c = outer.submit(transform_weights, COSINE_TW, tau_sigma, pade, *rS, warn=False)
+        f_s = outer.submit(transform_weights, SINE_TW, tau_sigma, pade, *rS, warn=False)
+        grid, (Ctw, _), (C, _), (S, _) = (f_grid.result(), f_ctw.result(), f_c.result(),
+                                          f_s.result())
     return SpaceTimeAxes(ntau, mu, grid, tau_sigma, Ctw, C, S, pade,
                          (rW, rS), tau_err)
