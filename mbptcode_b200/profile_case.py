@@ -1,13 +1,24 @@
-"""One tau point of the chi0 sweep and one of the self-energy sweep, mixed
-precision, for profiling the tensor-core engine under ncu.
+"""Small, self-contained invocations of the route for profiling under ncu.
 
     python -m mbptcode_b200.profile_case [--M 4096] [--n 682] [--nocc 68] [--states 682]
+    python -m mbptcode_b200.profile_case --dyson 4096 [--nfreq 1]
+    python -m mbptcode_b200.profile_case --sweep [--M 7200] [--n 1200] [--nocc 120]
 
-Launches, in order: the branch preparation, the TF32x3 G_occ/G_virt/Pi
-kernel, Z = D^T Pi, proj = -2 D^T Z^T, the FP64 transform, then on the
-self-energy side U = D W, the G_occ/G_virt/Zt kernel with the H epilogue and
-the row-contraction kernel -- one launch of each engine kernel. Device
-memory stays at a few GB (M = 4096: about 1 GB).
+Default: one tau point of the chi0 sweep and one of the self-energy sweep,
+mixed precision. Launches, in order: the branch preparation, the TF32x3
+G_occ/G_virt/Pi kernel, Z = D^T Pi, proj = -2 D^T Z^T, the FP64 transform,
+then on the self-energy side U = D W, the G_occ/G_virt/Zt kernel with the H
+epilogue and the row-contraction kernel -- one launch of each engine kernel.
+Device memory stays at a few GB (M = 4096: about 1 GB).
+
+--dyson N: the mixed Dyson step of `nfreq` frequencies of an N x N chi0
+(negative definite, seeded): cuSOLVER's Cholesky, the shared-memory diagonal
+blocks, the TF32-pair recursion (2 engine launches per node; with leaves of
+128 the last three engine launches of a frequency are the top node's two
+products and W = L^-T L^-1) and the mirrored FP64 store.
+
+--sweep: one whole mixed chi0 -> W -> Sigma -> QP sweep (24 points) of a
+synthetic system, for the launch list of the benchmark's workload.
 """
 from __future__ import annotations
 
@@ -17,19 +28,12 @@ import numpy as np
 import torch
 
 from . import grids
-from .gw import sigma_branch_sums
-from .space_time import chi0_sweep
+from .gw import gw_sweep, sigma_branch_sums
+from .space_time import chi0_sweep, dyson_batch
 from .synthetic import synthetic_system_torch
 
 
-def main():
-    p = argparse.ArgumentParser()
-    p.add_argument('--M', type=int, default=4096)
-    p.add_argument('--n', type=int, default=682)
-    p.add_argument('--nocc', type=int, default=68)
-    p.add_argument('--states', type=int, default=682)
-    a = p.parse_args()
-    torch.cuda.set_device(0)
+def tau_point(a):
     X, D, eps_t = synthetic_system_torch(a.n, a.nocc, a.M, seed=3, variant='calibrated')
     eps = eps_t.cpu().numpy()
     axes = grids.space_time_axes(eps, a.nocc, ntau=24)
@@ -43,6 +47,47 @@ def main():
     torch.cuda.synchronize()
     print(f'profile case M={a.M} n={a.n}: |chi0| {float(chi0.abs().max()):.3e}, '
           f'|branch| {float(br.abs().max()):.3e}')
+
+
+def dyson(a):
+    n = a.dyson
+    g = torch.Generator(device='cuda').manual_seed(1)
+    A = torch.randn(n, n // 2, generator=g, device='cuda', dtype=torch.float64)
+    chi0 = (-(A @ A.T) / n * 3.0)[None].repeat(a.nfreq, 1, 1).contiguous()
+    del A
+    logdet, _, info, _ = dyson_batch(chi0, want_w=True, precision='mixed')
+    torch.cuda.synchronize()
+    print(f'dyson case n={n} nfreq={a.nfreq}: info {info.tolist()}, '
+          f'logdet[0] {float(logdet[0]):.6e}')
+
+
+def sweep(a):
+    X, D, eps_t = synthetic_system_torch(a.n, a.nocc, a.M, seed=2024, variant='literal')
+    eps = eps_t.cpu().numpy()
+    axes = grids.space_time_axes(eps, a.nocc, ntau=24)
+    res = gw_sweep(X, D, eps, a.nocc, axes=axes, precision='mixed')
+    torch.cuda.synchronize()
+    print(f'sweep case M={a.M} n={a.n}: E_c {float(res["e_c"]):.6e}')
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument('--M', type=int, default=None)
+    p.add_argument('--n', type=int, default=None)
+    p.add_argument('--nocc', type=int, default=None)
+    p.add_argument('--states', type=int, default=682)
+    p.add_argument('--dyson', type=int, default=0)
+    p.add_argument('--nfreq', type=int, default=1)
+    p.add_argument('--sweep', action='store_true')
+    a = p.parse_args()
+    torch.cuda.set_device(0)
+    if a.dyson:
+        return dyson(a)
+    big = a.sweep
+    a.M = a.M or (7200 if big else 4096)
+    a.n = a.n or (1200 if big else 682)
+    a.nocc = a.nocc or (120 if big else 68)
+    return sweep(a) if a.sweep else tau_point(a)
 
 
 if __name__ == '__main__':
