@@ -64,10 +64,17 @@ class DIIS:
 
 def evgw_eigenvalues(X, D, eps0, nocc, ntau='auto', tol=EVGW_TOL, max_cycle=EVGW_MAX_CYCLE,
                      diis_size=EVGW_DIIS_SIZE, diis_start=EVGW_DIIS_START, precision=None,
-                     warm=None, eps_init=None, verbose=False):
+                     warm=None, eps_init=None, verbose=False, judge=False):
     """(eps, info): the evGW spectrum (Hartree, host array) of the system
     (X, D, eps0). info: cycles, converged, history (max |d eps| over HOMO and
-    LUMO per cycle), sigma_evaluations per cycle, warm_accepted per cycle."""
+    LUMO per cycle), sigma_evaluations per cycle, warm_accepted per cycle.
+
+    warm: 'previous' (the last cycle's roots) or a model with predict_roots
+    (the learned warm start; the states' exchange diagonal, independent of
+    the orbital energies, is computed once). judge: with a warm start, also
+    solve every cycle's equations plainly (the graphical scan, on the same
+    Sigma) and record in info['judge_max_diff'] the largest root difference
+    per cycle; those plain solves are not counted in sigma_evaluations."""
     eps0 = _eps_host(eps0)
     n = len(eps0)
     dev = torch.device('cuda', torch.cuda.current_device())
@@ -76,22 +83,34 @@ def evgw_eigenvalues(X, D, eps0, nocc, ntau='auto', tol=EVGW_TOL, max_cycle=EVGW
     tested = [nocc - 1, nocc]
     eps = eps0.copy() if eps_init is None else np.asarray(eps_init, float).copy()
     acc = DIIS(diis_size, diis_start) if diis_size else None
-    history, evals, accepted = [], [], []
+    history, evals, accepted, judged = [], [], [], []
     converged = False
     prev = None
+    sx = None
     for cycle in range(int(max_cycle)):
         axes = space_time_axes(eps, nocc, ntau=ntau, anchor=eps0)
         if warm == 'previous':
             w = prev
         elif warm is not None and hasattr(warm, 'predict_roots'):
+            if sx is None:
+                from .qp_mlp import exchange_diagonal
+                sx = exchange_diagonal(X, D, eps0, nocc, np.arange(n), axes.mu,
+                                       precision=precision)
+
             def w(partial, model=warm, ax=axes):
-                return model.predict_roots(X, D, eps0, nocc, ax, sweep=partial)
+                return model.predict_roots(X, D, eps0, nocc, ax, sweep=partial, sx=sx)
         else:
             w = None
         res = gw_sweep(X, D, eps, nocc, states=np.arange(n), axes=axes, precision=precision,
                        eps_anchor=eps0, warm=w)
         eps_new = res['roots'].cpu().numpy()
         flags = res['flags'].cpu().numpy()
+        if judge and w is not None:
+            from .gw import qp_solve
+            r_plain = qp_solve(res['sigma'], axes.pade_freq, eps0, res['states'], nocc,
+                               axes.mu)[0].cpu().numpy()
+            ok = np.isfinite(r_plain) & np.isfinite(eps_new)
+            judged.append(float(np.abs(r_plain - eps_new)[ok].max()) if ok.any() else 0.0)
         evals.append(int(res['evals'].sum().item()))
         accepted.append(int(((flags & 16) != 0).sum()))
         prev = res['roots']
@@ -111,4 +130,5 @@ def evgw_eigenvalues(X, D, eps0, nocc, ntau='auto', tol=EVGW_TOL, max_cycle=EVGW
                       stacklevel=2)
     return eps, {'cycles': len(history), 'converged': converged, 'history': history,
                  'sigma_evaluations': evals, 'warm_accepted': accepted,
+                 'judge_max_diff': judged,
                  'eps_mean_field': eps0, 'shift': eps - eps0}

@@ -28,13 +28,15 @@ from .space_time import _eps_host, to_device
 FEATURE_OFFSET = 0.1  # Ha, the two real frequencies Sigma_c is read at
 
 
-def exchange_diagonal(X, D, eps, nocc, states, mu):
-    """Sigma_x,ii of `states` (device FP64)."""
+def exchange_diagonal(X, D, eps, nocc, states, mu, precision='fp64'):
+    """Sigma_x,ii of `states` (device FP64). It depends on X, D and nocc only
+    (G_occ(0) = X_o X_o^T carries no orbital energy), so an evGW loop
+    computes it once."""
     dev = require_device()
     X, D = to_device(X, dev), to_device(D, dev)
     naux = D.shape[1]
     eye = torch.eye(naux, dtype=torch.float64, device=dev)[None]
-    br = sigma_branch_sums(X, D, eye, eps, nocc, [0.0], states, mu, precision='fp64')
+    br = sigma_branch_sums(X, D, eye, eps, nocc, [0.0], states, mu, precision=precision)
     return -br[0, 0]
 
 
@@ -54,13 +56,15 @@ def sigma_at(sigma, pade_freq, states, nocc, mu, query):
     return out
 
 
-def features(X, D, eps_anchor, nocc, sweep):
-    """(S, 4) FP32 device features of the states of a finished sweep."""
+def features(X, D, eps_anchor, nocc, sweep, sx=None):
+    """(S, 4) FP32 device features of the states of a finished sweep; `sx`,
+    the exchange diagonal of those states, is computed when not given."""
     states = sweep['states']
     axes = sweep['axes']
     dev = sweep['sigma'].device
     e = torch.as_tensor(np.asarray(_eps_host(eps_anchor), float)[states], device=dev)
-    sx = exchange_diagonal(X, D, sweep.get('eps_sweep', eps_anchor), nocc, states, axes.mu)
+    if sx is None:
+        sx = exchange_diagonal(X, D, sweep.get('eps_sweep', eps_anchor), nocc, states, axes.mu)
     q = torch.stack([e - FEATURE_OFFSET, e + FEATURE_OFFSET], dim=1)
     sc = sigma_at(sweep['sigma'], axes.pade_freq, states, nocc, axes.mu, q)
     return torch.stack([e, sx, sc[:, 0], sc[:, 1]], dim=1).to(torch.float32).contiguous()
@@ -142,13 +146,15 @@ class QPShiftModel:
     def predict_shift(self, x):
         return self._forward(self.standardise(x.to(self.device, torch.float32))) * self.y_scale
 
-    def predict_roots(self, X, D, eps, nocc, axes, eps_anchor=None, precision=None, sweep=None):
-        """Predicted QP roots of every orbital for the warm start: from the
-        finished sweep `sweep` when given, else after computing one."""
+    def predict_roots(self, X, D, eps, nocc, axes, eps_anchor=None, precision=None, sweep=None,
+                      sx=None):
+        """Predicted QP roots of the sweep's states for the warm start, from
+        the finished sweep `sweep` (whose Sigma the features read) and, when
+        given, the states' exchange diagonal `sx`."""
         anchor = eps if eps_anchor is None else eps_anchor
         if sweep is None:
             raise ValueError('predict_roots needs the sweep whose Sigma it reads')
-        x = features(X, D, anchor, nocc, sweep)
+        x = features(X, D, anchor, nocc, sweep, sx=sx)
         e = x[:, 0].double()
         return e + self.predict_shift(x).double()
 
