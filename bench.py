@@ -58,6 +58,12 @@ FLOPS = {
     'sigma_hadamard': 2.0 * M * M * M + 2.0 * M * M * N_ORB,   # Zt, G_occ, G_virt
     'row_contraction': 2.0 * 2.0 * M * M * N_ORB,       # (G o Zt) X_s, both branches
 }
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# engine kernels at this workload, from one ncu capture of a tau point at full
+# size (python -m mbptcode_b200.profile_case --M 7200 --n 1200 --nocc 120
+# --states 1200, the six engine launches of one tau point)
+TRAFFIC_BYTES = {'hadamard': 531.7e6, 'split': 2591.9e6, 'f32': 2581.6e6,
+                 'sigma_hadamard': 3318.6e6, 'row_contraction': 926.6e6}
 # algorithmic FLOPs of the Dyson step's inverse per frequency (triangular inverse
 # n^3/3 + L^-T L^-1 n^3/3, the classical SPD-inverse count), spread over launches
 # of many sizes: rated on their summed time
@@ -209,7 +215,8 @@ def main():
     import torch
     import torch.distributed as dist
     from mbptcode_b200 import _lib, grids
-    from mbptcode_b200.gw import gw_space_time, gw_sweep
+    from mbptcode_b200.gw import gw_space_time, gw_sweep, qp_solve
+    from mbptcode_b200.qp_mlp import MODEL_PATH, QPShiftModel
     from mbptcode_b200.synthetic import synthetic_system_torch
 
     torch.cuda.set_device(local)
@@ -236,8 +243,14 @@ def main():
     axes = grids.space_time_axes(eps, NOCC, ntau=NTAU)
     states = np.arange(N_ORB)
 
+    # the learned QP warm start (trained by mbptcode_b200.learned_warm_start on
+    # method-generated systems, shipped with the package): the mixed sweep's QP
+    # solve is warm-started, the plain FP64 path solves by the graphical scan
+    model = QPShiftModel.load(MODEL_PATH, device=dev)
+
     def sweep(precision):
-        return gw_sweep(X, D, eps, NOCC, states=states, axes=axes, precision=precision)
+        return gw_sweep(X, D, eps, NOCC, states=states, axes=axes, precision=precision,
+                        warm=model if precision == 'mixed' else None)
 
     clocks = Clocks(torch.cuda.current_device()) if rank == 0 else None
     for _ in range(args.warmup):
@@ -275,7 +288,8 @@ def main():
 
     # per-stage device times of one more mixed sweep (outside the timed region)
     stages = {}
-    gw_sweep(X, D, eps, NOCC, states=states, axes=axes, precision='mixed', timings=stages)
+    gw_sweep(X, D, eps, NOCC, states=states, axes=axes, precision='mixed', timings=stages,
+             warm=model)
     stages_fp64 = {}
 
     # ---- the plain FP64 GPU sweep (the >= 5x denominator) ----
@@ -290,6 +304,16 @@ def main():
     torch.cuda.synchronize()
     ms_fp64 = max_over_ranks(f0.elapsed_time(f1) / nf)
     acc = accuracy(res_mixed, res_fp64)
+    # the warm start judged by the plain scan on the same (mixed) Sigma
+    r_plain, _, _, e_plain = qp_solve(res_mixed['sigma'], axes.pade_freq, eps, states, NOCC,
+                                      axes.mu)
+    ok = torch.isfinite(r_plain) & torch.isfinite(res_mixed['roots'])
+    warm_info = {
+        'accepted': int(((res_mixed['flags'] & 16) != 0).sum().item()), 'states': N_ORB,
+        'sigma_evals_warm': int(res_mixed['evals'].sum().item()),
+        'sigma_evals_plain': int(e_plain.sum().item()),
+        'max_root_diff_meV': float((res_mixed['roots'] - r_plain)[ok].abs().max().item()
+                                   * HARTREE_EV * 1e3)}
 
     other = None
     if not args.no_accuracy_other:
@@ -298,7 +322,8 @@ def main():
                                             device=dev)
         eo_h = eo.cpu().numpy()
         ax_o = grids.space_time_axes(eo_h, NOCC, ntau=NTAU)
-        rm = gw_sweep(Xo, Do, eo_h, NOCC, states=states, axes=ax_o, precision='mixed')
+        rm = gw_sweep(Xo, Do, eo_h, NOCC, states=states, axes=ax_o, precision='mixed',
+                      warm=model)
         rf = gw_sweep(Xo, Do, eo_h, NOCC, states=states, axes=ax_o, precision='fp64')
         other = dict(variant=ov, **accuracy(rm, rf))
         del Xo, Do, rm, rf
@@ -307,12 +332,12 @@ def main():
     Xh = X.cpu().pin_memory()
     Dh = D.cpu().pin_memory()
     eh = eps_t.cpu().pin_memory()
-    gw_space_time(Xh, Dh, eh, NOCC, ntau=NTAU, precision='mixed')
+    gw_space_time(Xh, Dh, eh, NOCC, ntau=NTAU, precision='mixed', warm=model)
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        gw_space_time(Xh, Dh, eh, NOCC, ntau=NTAU, precision='mixed')
+        gw_space_time(Xh, Dh, eh, NOCC, ntau=NTAU, precision='mixed', warm=model)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
     h2d = Xh.numel() * 8 + Dh.numel() * 8 + eh.numel() * 8
@@ -340,13 +365,7 @@ def main():
             'launches': n, 'total_ms': round(ms, 3), 'avg_ms': round(ms / max(n, 1), 4),
             'tflops_alg': round(DYSON_INV_FLOPS * NTAU / (ms / 1e3) / 1e12, 1),
             'note': 'one sweep outside the timed region; summed over the family'}
-    traffic = None
-    tp = os.path.join(ROOT, 'profiles', 'traffic_per_launch.json')
-    if os.path.exists(tp):
-        try:
-            traffic = json.load(open(tp)).get(top)
-        except (OSError, ValueError):
-            traffic = None
+    traffic = TRAFFIC_BYTES.get(top)
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -381,7 +400,7 @@ def main():
         'speedup_vs_fp64': round(ms_fp64 / ms_step, 3),
         'stages_s': {k: round(v, 4) for k, v in stages.items() if k.startswith('t_')},
         'stages_fp64_s': {k: round(v, 4) for k, v in stages_fp64.items() if k.startswith('t_')},
-        'accuracy': acc, 'accuracy_other_variant': other,
+        'accuracy': acc, 'accuracy_other_variant': other, 'qp_warm_start': warm_info,
         'e2e': {'value': round(e2e_s, 5), 'unit': 's', 'h2d_bytes_per_step': int(h2d),
                 'd2h_bytes_per_step': int(d2h)},
         'gpu_launches': int(launches),

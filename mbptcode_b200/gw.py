@@ -135,6 +135,8 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
     None is eps. timings: a dict receiving per-stage device times.
     """
     dev = require_device()
+    # host inputs cross to the device once, here (both halves of the sweep read them)
+    X, D = to_device(X, dev), to_device(D, dev)
     eps_h = _eps_host(eps)
     n = len(eps_h)
     states = np.arange(n) if states is None else np.atleast_1d(np.asarray(states, int))
@@ -169,8 +171,15 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
     if ev:
         ev[3].record()
     anchor = eps_h if eps_anchor is None else _eps_host(eps_anchor)
-    if callable(warm):
-        # a predictor that reads this sweep's Sigma (the learned warm start)
+    if warm is not None and hasattr(warm, 'predict_roots'):
+        # the learned warm start: features from this sweep's Sigma and the
+        # states' exchange diagonal, in the sweep's precision
+        from .qp_mlp import exchange_diagonal
+        sx = exchange_diagonal(X, D, eps_h, nocc, states, mu, precision=precision)
+        warm = warm.predict_roots(X, D, eps_h, nocc, axes, eps_anchor=anchor, sx=sx,
+                                  sweep=SweepResult(sigma=sigma, axes=axes, states=states))
+    elif callable(warm):
+        # a predictor that reads this sweep's Sigma
         warm = warm(SweepResult(sigma=sigma, axes=axes, states=states))
     roots, z, flags, evals = qp_solve(sigma, axes.pade_freq, anchor, states, nocc, mu,
                                       xc=xc_diagonal, greedy=greedy, warm=warm, stream=stream)
@@ -191,7 +200,7 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
 
 def gw_space_time(X, D, eps, nocc, states=None, ntau='auto', precision=None,
                   eps_anchor=None, xc_diagonal=None, greedy=True, with_z=False,
-                  failures=None, timings=None):
+                  failures=None, timings=None, warm=None):
     """QP energies (Hartree, host array) of `states`, the equation
     w = eps_p + xc_p + Re Sigma_c(w) solved for the root of largest Z, on the
     synthetic or caller-built ISDF factors X (M x norb, MO collocation) and
@@ -199,7 +208,7 @@ def gw_space_time(X, D, eps, nocc, states=None, ntau='auto', precision=None,
     t0 = time.perf_counter()
     res = gw_sweep(X, D, eps, nocc, states=states, ntau=ntau, precision=precision,
                    eps_anchor=eps_anchor, xc_diagonal=xc_diagonal, greedy=greedy,
-                   timings=timings)
+                   timings=timings, warm=warm)
     roots = res['roots'].cpu().numpy()
     z = res['z'].cpu().numpy()
     flags = res['flags'].cpu().numpy()

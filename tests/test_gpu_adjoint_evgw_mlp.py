@@ -141,3 +141,15 @@ def test_learned_warm_start_saves_sigma_evaluations():
     # the same roots (Newton converges below the scan's 1e-8 bisection width)
     assert worst < 1e-7
     assert np.mean(saved) > 0.3, saved
+
+
+def test_shipped_model_warm_starts_a_new_system():
+    """The network shipped with the package (trained on 512 method-generated
+    systems) warm-starts the QP solve of a system it never saw: the same
+    roots as the plain scan on the same Sigma, far fewer Sigma evaluations."""
+    model = qp_mlp.QPShiftModel.load(qp_mlp.MODEL_PATH)
+    X, D, eps = synthetic_system(150, 15, 900, seed=4242, variant='calibrated')
+    r = qp_mlp.warm_start_compare(model, X, D, eps, 15, ntau=24, precision='mixed')
+    assert r['accepted'] > 0.8 * r['states']
+    assert r['max_root_diff'] < 1e-7
+    assert r['evals_warm'] < 0.3 * r['evals_plain']

@@ -116,3 +116,15 @@ def test_plugin_rebinds_and_restores_reference_names():
         assert lr.chi0_imaginary_frequency is orig
     finally:
         sys.path.remove(ref)
+
+
+def test_shipped_qp_shift_model_file():
+    """The trained warm-start network ships with the package: a 4 -> 64 -> 64 -> 1
+    parameter vector plus its input standardisation and target scale."""
+    from mbptcode_b200.qp_mlp import MODEL_PATH
+    d = np.load(MODEL_PATH)
+    H = int(d['hidden'])
+    assert H == 64
+    assert d['params'].shape == (4 * H + H + H * H + H + H + 1,)
+    assert d['x_mean'].shape == (4,) and d['x_std'].shape == (4,)
+    assert np.all(np.isfinite(d['params'])) and float(d['y_scale']) > 0
