@@ -148,7 +148,9 @@ int mbpt_transform(const double *in_dev, int K, int64_t n, const double *w_dev, 
  *   Zt = D Wt(tau_k) D^T,
  *   branch[0,k,s] = +sum_PQ X[P,p] (G_occ(tau_k) o Zt)_PQ X[Q,p]
  *   branch[1,k,s] = -sum_PQ X[P,p] (G_virt(tau_k) o Zt)_PQ X[Q,p],
- * p = states[s]. Wt_dev (ntau, naux, naux); states_dev (nstates) int64;
+ * p = states[s]. Wt_dev (ntau, naux, naux), or NULL for W = I at every tau
+ * (Zt = D D^T, the bare Coulomb factor: with tau = 0 the lesser branch is
+ * then -Sigma_x,pp, the exchange diagonal); states_dev (nstates) int64;
  * branch_dev (2, ntau, nstates) output. */
 size_t mbpt_sigma_workspace_bytes(int64_t M, int64_t norb, int64_t nocc, int64_t naux,
                                   int ntau, int nstates, int mode);

@@ -179,3 +179,33 @@ class Workspace:
 
 
 WORKSPACE = Workspace()
+
+
+class Buffers:
+    """Grow-only named device arrays per device, reused across calls: the
+    sweep's large intermediates (chi0 / W - I and W(tau), 10 GB each at
+    naux = 7200 and 24 points), so that repeated sweeps neither allocate nor
+    free them. As with the workspace, calls on one device are stream-ordered
+    and a result that must outlive the next call is copied (or asked for with
+    the sweep's keep option, which allocates its own)."""
+
+    def __init__(self):
+        self._buf = {}
+
+    def take(self, name, shape, device, dtype=torch.float64):
+        n = 1
+        for d in shape:
+            n *= int(d)
+        key = (device.index, name)
+        buf = self._buf.get(key)
+        if buf is None or buf.numel() < n or buf.dtype != dtype:
+            self._buf.pop(key, None)
+            buf = torch.empty(max(n, 1), dtype=dtype, device=device)
+            self._buf[key] = buf
+        return buf[:n].view(*shape)
+
+    def release(self):
+        self._buf.clear()
+
+
+BUFFERS = Buffers()

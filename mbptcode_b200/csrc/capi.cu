@@ -639,11 +639,12 @@ int sigma_run(const double *X, const Dims &d, const double *eps, double mu, cons
     cublasHandle_t h = handles(st).blas;
     launch_gather_cols_f64(X, d.M, d.n, states, S, b.Xs, st);
     for (int k = 0; k < ntau; ++k) {
-      // Zt = D Wt D^T (MBPTcode imaginary_time.py:508, :513)
-      if (!dgemm_rm(h, false, false, d.M, d.naux, d.naux, 1.0, D, d.naux, Wt + k * a2, d.naux,
-                    0.0, b.U, d.naux) ||
-          !dgemm_rm(h, false, true, d.M, d.M, d.naux, 1.0, b.U, d.naux, D, d.naux, 0.0, b.Zt,
-                    d.M))
+      // Zt = D Wt D^T (MBPTcode imaginary_time.py:508, :513); Wt = I without Wt
+      if (Wt && !dgemm_rm(h, false, false, d.M, d.naux, d.naux, 1.0, D, d.naux, Wt + k * a2,
+                          d.naux, 0.0, b.U, d.naux))
+        return MBPT_ERR_CUDA;
+      if ((Wt || k == 0) && !dgemm_rm(h, false, true, d.M, d.M, d.naux, 1.0, Wt ? b.U : D,
+                                      d.naux, D, d.naux, 0.0, b.Zt, d.M))
         return MBPT_ERR_CUDA;
       launch_scaled_branches(X, d.M, d.n, d.nocc, eps, mu, tau[k], 1.0, b.Xo_s, b.Xv_s, st);
       double *out_l = branch + static_cast<int64_t>(k) * S;
@@ -681,17 +682,20 @@ int sigma_run(const double *X, const Dims &d, const double *eps, double mu, cons
     SplitMat Hl{b.Hl_hi, b.Hl_lo, d.Mp, d.Mp, d.Mp}, Hg{b.Hg_hi, b.Hg_lo, d.Mp, d.Mp, d.Mp};
     SplitMat XsT{b.XsT_hi, b.XsT_lo, Sp, d.Mp, d.Mp};
     for (int k = 0; k < ntau; ++k) {
-      launch_split_pad<double>(Wt + k * a2, d.naux, d.naux, d.naux, 1.f, b.W_hi, b.W_lo, d.Ap,
-                               d.Ap, d.Ap, false, st);
       launch_prep_branches(X, d.M, d.n, d.nocc, eps, mu, tau[k], b.Yo_hi, b.Yo_lo, d.Ko,
                            b.Yv_hi, b.Yv_lo, d.Kv, d.Mp, st);
       umma::EpiArgs e;
-      // U = D Wt (Wt symmetric)
-      e.out0_hi = b.U_hi;
-      e.out0_lo = b.U_lo;
-      e.ld_out = d.Ap;
-      int rc = gemm_split(umma::EPI_SPLIT, 1, &Dm, &Wm, d.Mp, d.Ap, e, err, st);
-      if (rc) return rc;
+      int rc = MBPT_OK;
+      if (Wt) {
+        // U = D Wt (Wt symmetric); without Wt, W = I and U = D
+        launch_split_pad<double>(Wt + k * a2, d.naux, d.naux, d.naux, 1.f, b.W_hi, b.W_lo,
+                                 d.Ap, d.Ap, d.Ap, false, st);
+        e.out0_hi = b.U_hi;
+        e.out0_lo = b.U_lo;
+        e.ld_out = d.Ap;
+        rc = gemm_split(umma::EPI_SPLIT, 1, &Dm, &Wm, d.Mp, d.Ap, e, err, st);
+        if (rc) return rc;
+      }
       // one tile pass: Zt = U D^T, G_occ, G_virt -> H< = G_occ o Zt, H> = G_virt o Zt
       e = umma::EpiArgs();
       e.out0_hi = b.Hl_hi;
@@ -700,7 +704,7 @@ int sigma_run(const double *X, const Dims &d, const double *eps, double mu, cons
       e.out1_lo = b.Hg_lo;
       e.ld_out = d.Mp;
       // Zt last: its K = naux sum is the long one, drained by the kernel
-      SplitMat A3[3] = {Yo, Yv, Um}, B3[3] = {Yo, Yv, Dm};
+      SplitMat A3[3] = {Yo, Yv, Wt ? Um : Dm}, B3[3] = {Yo, Yv, Dm};
       rc = gemm_split(umma::EPI_SIGMA_H, 3, A3, B3, d.Mp, d.Mp, e, err, st);
       if (rc) return rc;
       // branch sums: sum_P X_s[P,p] (H X_s)[P,p]

@@ -14,7 +14,7 @@ import warnings
 import numpy as np
 import torch
 
-from ._lib import WORKSPACE, check, host_array, lib, ptr, require_device, stream_ptr
+from ._lib import BUFFERS, WORKSPACE, check, host_array, lib, ptr, require_device, stream_ptr
 from .grids import space_time_axes
 from .space_time import (_Err, _eps_host, _mode, check_mixed_weights, chi0_sweep,
                          dyson_batch, to_device, transform)
@@ -31,18 +31,19 @@ class QPWeightOutside(RuntimeWarning):
     """A quasiparticle root kept with Z outside (0, 1]."""
 
 
-def screened_interaction_tau(W_minus_I, Ctw, stream=None):
+def screened_interaction_tau(W_minus_I, Ctw, stream=None, out=None):
     """Wt(tau) = sum_w Ctw[tau, w] (W(i w) - I): ``imaginary_time.py:181-195``
     (here from W - I as the Dyson step leaves it), FP64 on the device."""
-    return transform(W_minus_I, Ctw, stream)
+    return transform(W_minus_I, Ctw, stream, out=out)
 
 
 def sigma_branch_sums(X, D, Wt, eps, nocc, tau_points, states, mu, precision=None,
                       stream=None):
     """(2, ntau, nstates) device tensor: Sigma^<_pp(tau) and Sigma^>_pp(tau) of
-    the states, the diagonal form of ``imaginary_time.py:39-92``."""
+    the states, the diagonal form of ``imaginary_time.py:39-92``. Wt None
+    stands for W = I at every tau (the bare Coulomb factor)."""
     dev = require_device()
-    Wt = to_device(Wt, dev)
+    Wt = None if Wt is None else to_device(Wt, dev)
     Xd, Dd = to_device(X, dev), to_device(D, dev)
     eps_h = _eps_host(eps)
     ed = to_device(eps_h, dev)
@@ -52,14 +53,15 @@ def sigma_branch_sums(X, D, Wt, eps, nocc, tau_points, states, mu, precision=Non
     S = st.numel()
     tau_h, tp = host_array(tau_points)
     ntau = len(tau_h)
-    if Wt.shape != (ntau, naux, naux):
+    if Wt is not None and Wt.shape != (ntau, naux, naux):
         raise ValueError(f'Wt is {tuple(Wt.shape)}, need ({ntau}, {naux}, {naux})')
     mode = _mode(precision)
     branch = torch.empty((2, ntau, S), dtype=torch.float64, device=dev)
     ws = WORKSPACE.get(lib().mbpt_sigma_workspace_bytes(M, norb, nocc, naux, ntau, S, mode), dev)
     err = _Err(dev)
     check(lib().mbpt_sigma_branch_sums(ptr(Xd), M, norb, nocc, ptr(ed), float(mu), ptr(Dd),
-                                       naux, ptr(Wt.contiguous()), tp, ntau, ptr(st), S, mode,
+                                       naux, ptr(None if Wt is None else Wt.contiguous()), tp,
+                                       ntau, ptr(st), S, mode,
                                        ptr(branch), ptr(ws), ws.numel(), ptr(err.t),
                                        stream_ptr(stream)), 'mbpt_sigma_branch_sums')
     err.check('mbpt_sigma_branch_sums')
@@ -149,8 +151,13 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
     if timings is not None:
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         ev[0].record()
+    naux = D.shape[1]
+    # the two 10 GB-class intermediates come from the per-device buffer cache
+    # unless the caller keeps them
     chi0, _ = chi0_sweep(X, D, eps_h, nocc, axes.grid.tau_points, axes.grid.cosft_wt, mu=mu,
-                         precision=precision, stream=stream)
+                         precision=precision, stream=stream,
+                         out=None if keep else BUFFERS.take(
+                             'sweep_chi0', (axes.grid.nfreq, naux, naux), dev))
     if ev:
         ev[1].record()
     logdet, trace, info, _ = dyson_batch(chi0, want_w=True, stream=stream,
@@ -162,7 +169,9 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
                                 stream_ptr(stream)), 'mbpt_energy_sum')
     if ev:
         ev[2].record()
-    Wt = screened_interaction_tau(chi0, axes.Ctw, stream)
+    Wt = screened_interaction_tau(
+        chi0, axes.Ctw, stream,
+        out=None if keep else BUFFERS.take('sweep_wt', (len(axes.Ctw), naux, naux), dev))
     W_minus_I = chi0 if keep else None
     del chi0
     branch = sigma_branch_sums(X, D, Wt, eps_h, nocc, axes.tau_sigma, states, mu, precision,

@@ -40,9 +40,7 @@ def exchange_diagonal(X, D, eps, nocc, states, mu, precision='fp64'):
     computes it once."""
     dev = require_device()
     X, D = to_device(X, dev), to_device(D, dev)
-    naux = D.shape[1]
-    eye = torch.eye(naux, dtype=torch.float64, device=dev)[None]
-    br = sigma_branch_sums(X, D, eye, eps, nocc, [0.0], states, mu, precision=precision)
+    br = sigma_branch_sums(X, D, None, eps, nocc, [0.0], states, mu, precision=precision)
     return -br[0, 0]
 
 

@@ -99,9 +99,10 @@ def _taus(tau_points, tau_indices):
 
 
 def chi0_sweep(X, D, eps, nocc, tau_points, cosft_wt, mu=None, precision=None,
-               want_proj=False, stream=None):
+               want_proj=False, stream=None, out=None):
     """(chi0 (nfreq, naux, naux), proj (ntau, naux, naux) or None) as device
-    tensors: the whole N^3 sweep in one library call."""
+    tensors: the whole N^3 sweep in one library call. `out`: a contiguous
+    FP64 device array of chi0's shape to write into."""
     dev = require_device()
     Xd, Dd = to_device(X, dev), to_device(D, dev)
     eps_h = _eps_host(eps)
@@ -120,7 +121,14 @@ def chi0_sweep(X, D, eps, nocc, tau_points, cosft_wt, mu=None, precision=None,
         raise ValueError(f'cosft_wt is {cw_h.shape}, need (nfreq, {ntau})')
     mode = _mode(precision)
     check_mixed_weights(precision, cw_h)
-    chi0 = torch.empty((nfreq, naux, naux), dtype=torch.float64, device=dev)
+    if out is not None:
+        if tuple(out.shape) != (nfreq, naux, naux) or out.dtype != torch.float64 \
+                or not out.is_contiguous() or out.device != dev:
+            raise ValueError(f'out must be a contiguous FP64 ({nfreq}, {naux}, {naux}) array '
+                             f'on {dev}')
+        chi0 = out
+    else:
+        chi0 = torch.empty((nfreq, naux, naux), dtype=torch.float64, device=dev)
     proj = (torch.empty((ntau, naux, naux), dtype=torch.float64, device=dev)
             if want_proj else None)
     nbytes = lib().mbpt_chi0_workspace_bytes(M, norb, nocc, naux, ntau, mode)
@@ -322,13 +330,17 @@ def rpa_correlation_energy_space_time(X, D, eps, nocc, grid, mu=None, tile_gb=No
     return value, SimpleNamespace(proj_tau=back(proj, X), tau_indices=None, freq_indices=None)
 
 
-def transform(values, weights, stream=None):
-    """sum_k weights[j, k] values[k] over (K, n, n) device tensors, FP64."""
+def transform(values, weights, stream=None, out=None):
+    """sum_k weights[j, k] values[k] over (K, n, n) device tensors, FP64
+    (into `out`, a contiguous (J, n, n) FP64 array, when given)."""
     dev = values.device
     K, n = values.shape[0], values.shape[-1]
     w = torch.as_tensor(np.ascontiguousarray(weights, dtype=np.float64), device=dev)
     J = w.shape[0]
-    out = torch.empty((J, n, n), dtype=torch.float64, device=dev)
+    if out is None:
+        out = torch.empty((J, n, n), dtype=torch.float64, device=dev)
+    elif tuple(out.shape) != (J, n, n) or out.dtype != torch.float64 or not out.is_contiguous():
+        raise ValueError(f'out must be a contiguous FP64 ({J}, {n}, {n}) array')
     check(lib().mbpt_transform(ptr(values.contiguous()), K, n, ptr(w), J, ptr(out),
                                stream_ptr(stream)), 'mbpt_transform')
     return out

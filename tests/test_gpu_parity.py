@@ -267,3 +267,20 @@ def test_dyson_batch_with_failed_frequency_inside(prec):
         # the LU frequency is FP64 in both modes
         err = np.abs(chi0[f].cpu().numpy() - W_ref).max()
         assert err < (1e-10 if f == 1 else tol) * max(1.0, np.abs(W_ref).max()), (f, err)
+
+
+@pytest.mark.parametrize('prec', ['fp64', 'mixed'])
+def test_sigma_branch_sums_identity_w(prec):
+    """Wt omitted stands for W = I at every tau: the same branch sums as an
+    explicit identity stack (the exchange diagonal's path, which skips the
+    D W product and the W conversion)."""
+    n, nocc, M = 60, 8, 256
+    X, D, eps = synthetic_system(n, nocc, M, seed=31, variant='calibrated')
+    mu = st.particle_hole_window(eps, nocc)[2]
+    taus = [0.0, 0.7]
+    states = np.arange(n)
+    eye = np.broadcast_to(np.eye(M), (2, M, M)).copy()
+    a = gw.sigma_branch_sums(X, D, None, eps, nocc, taus, states, mu, precision=prec)
+    b = gw.sigma_branch_sums(X, D, eye, eps, nocc, taus, states, mu, precision=prec)
+    tol = 1e-12 if prec == 'fp64' else MIXED_REL
+    assert rel(a.cpu().numpy(), b.cpu().numpy()) < tol
