@@ -50,12 +50,16 @@ N_ORB, NOCC, M, NTAU = 1200, 120, 7200, 24
 SEED = 2024
 
 # algorithmic FLOPs of one launch of each engine kernel at this workload
-# (the split products' 3x and the padding are not counted)
+# (the split products' 3x and the padding are not counted). Pi, proj and H are
+# symmetric: those launches form the 128 x 128 tiles on and above the
+# diagonal only (T (T + 1) / 2 of T^2, T = 57 tile rows) and count that work.
+_T = -(-M // 128)
+SYM = (_T * (_T + 1) / 2) / (_T * _T)
 FLOPS = {
-    'hadamard': 2.0 * M * M * N_ORB,                    # G_occ and G_virt of one tau
+    'hadamard': SYM * 2.0 * M * M * N_ORB,              # G_occ and G_virt of one tau
     'split': 2.0 * M * M * M,                           # D^T Pi  /  D Wt
-    'f32': 2.0 * M * M * M,                             # D^T (Pi D)
-    'sigma_hadamard': 2.0 * M * M * M + 2.0 * M * M * N_ORB,   # Zt, G_occ, G_virt
+    'f32': SYM * 2.0 * M * M * M,                       # D^T (Pi D)
+    'sigma_hadamard': SYM * (2.0 * M * M * M + 2.0 * M * M * N_ORB),   # Zt, G_occ, G_virt
     'row_contraction': 2.0 * 2.0 * M * M * N_ORB,       # (G o Zt) X_s, both branches
 }
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the

@@ -186,7 +186,9 @@ int chi0_run(const double *X, const Dims &d, const double *eps, double mu, const
       e.out0_lo = b.Pi_lo;
       e.ld_out = d.Mp;
       SplitMat A2[2] = {Yo, Yv};
-      int rc = gemm_split(umma::EPI_HADAMARD_SPLIT, 2, A2, A2, d.Mp, d.Mp, e, err, st);
+      // Pi is symmetric: the tiles on and above the diagonal, mirrored by the epilogue
+      int rc = gemm_split(umma::EPI_HADAMARD_SPLIT, 2, A2, A2, d.Mp, d.Mp, e, err, st,
+                          umma::BAND_UPPER);
       if (rc) return rc;
       // Z = D^T Pi  (= (Pi D)^T, Pi symmetric)
       e = umma::EpiArgs();
@@ -200,7 +202,8 @@ int chi0_run(const double *X, const Dims &d, const double *eps, double mu, const
       e.outf = b.proj32 + k * d.Ap * d.Ap;
       e.ld_outf = d.Ap;
       e.alpha = -2.f;
-      rc = gemm_split(umma::EPI_F32, 1, &Dt, &Z, d.Ap, d.Ap, e, err, st);
+      // proj = -2 D^T Pi D is symmetric: upper tiles, mirrored
+      rc = gemm_split(umma::EPI_F32, 1, &Dt, &Z, d.Ap, d.Ap, e, err, st, umma::BAND_UPPER);
       if (rc) return rc;
     }
     launch_transform<float>(b.proj32, d.Ap * d.Ap, d.Ap, d.naux, d.naux, b.w, nfreq, ntau,
@@ -705,7 +708,9 @@ int sigma_run(const double *X, const Dims &d, const double *eps, double mu, cons
       e.ld_out = d.Mp;
       // Zt last: its K = naux sum is the long one, drained by the kernel
       SplitMat A3[3] = {Yo, Yv, Wt ? Um : Dm}, B3[3] = {Yo, Yv, Dm};
-      rc = gemm_split(umma::EPI_SIGMA_H, 3, A3, B3, d.Mp, d.Mp, e, err, st);
+      // G_occ, G_virt and Zt = D W D^T are symmetric, so are H< and H>: upper
+      // tiles, mirrored by the epilogue
+      rc = gemm_split(umma::EPI_SIGMA_H, 3, A3, B3, d.Mp, d.Mp, e, err, st, umma::BAND_UPPER);
       if (rc) return rc;
       // branch sums: sum_P X_s[P,p] (H X_s)[P,p]
       e = umma::EpiArgs();

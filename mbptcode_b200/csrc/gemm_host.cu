@@ -170,6 +170,18 @@ int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t 
   // (~1e-6 relative truncation bias, against ~4e-5 for an undrained K = 7296)
   constexpr int kDrain = 2;
   const bool tf = nacc > 0 && A[0].tf32;
+  if (band == BAND_UPPER && !(tf && nacc == 1)) {
+    // symmetric products of full K: the upper tiles, mirrored by the epilogue
+    if (m_rows != n_rows) return MBPT_ERR_SHAPE;
+    if (tf && nacc == 2 && epi == EPI_HADAMARD_SPLIT)
+      return launch<2, 128, EPI_HADAMARD_SPLIT, true, kDrain>(A, B, m_rows, n_rows, e, err, st,
+                                                              band);
+    if (!tf && nacc == 1 && epi == EPI_F32)
+      return launch<1, 128, EPI_F32, false, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
+    if (!tf && nacc == 3 && epi == EPI_SIGMA_H)
+      return launch<3, 128, EPI_SIGMA_H, false, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
+    return MBPT_ERR_UNSUPPORTED;
+  }
   if (band) {
     // triangular K spans: the single drained FP32-store TF32 product only (its
     // spans are never empty for the operand shapes the flags describe)

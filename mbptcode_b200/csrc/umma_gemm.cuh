@@ -58,6 +58,8 @@ enum Band : int {
   BAND_K_TO_M = 4,    // A(r, k) = 0 for k > r
   BAND_K_TO_N = 8,    // B(r, k) = 0 for k > r
   BAND_UPPER = 16,    // symmetric output: tiles below the diagonal are not formed
+                      // (the FP32 / pair / Hadamard epilogues store each tile above
+                      // the diagonal twice, the second time transposed)
 };
 
 template <int NACC>
@@ -218,6 +220,20 @@ __device__ __forceinline__ void store_split32(bf16 *hi, bf16 *lo, const float (&
     for (int i = 0; i < 8; ++i) split_bf16(v[8 * q + i], h[i], l[i]);
     reinterpret_cast<uint4 *>(hi)[q] = *reinterpret_cast<const uint4 *>(h);
     reinterpret_cast<uint4 *>(lo)[q] = *reinterpret_cast<const uint4 *>(l);
+  }
+}
+
+// The transposed store of store_split32: v[i] goes to hi/lo[i * ld] (base at
+// the mirrored position); across the warp, lanes (consecutive rows) write
+// consecutive elements of each mirrored row.
+__device__ __forceinline__ void store_split32_t(bf16 *hi, bf16 *lo, int64_t ld,
+                                                const float (&v)[32]) {
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    bf16 h, l;
+    split_bf16(v[i], h, l);
+    hi[i * ld] = h;
+    lo[i * ld] = l;
   }
 }
 
@@ -450,6 +466,8 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
       tc_fence_after();
       const int row = m0 + sp * 32 + lane;
       const EpiArgs &e = p.epi;
+      // symmetric output: a tile above the diagonal also fills its mirror
+      const bool mirror = (p.band & BAND_UPPER) && tn > tm;
       // 32 columns starting at c of accumulator j (the drained one from registers)
       auto load = [&](int j, int c, float (&v)[32]) {
         if constexpr (DRAIN > 0) {
@@ -482,6 +500,13 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
             }
             dst[q] = o;
           }
+          if constexpr (EPI == EPI_F32) {
+            if (mirror) {
+#pragma unroll
+              for (int i = 0; i < 32; ++i)
+                e.outf[static_cast<int64_t>(col + i) * e.ld_outf + row] = e.alpha * v0[i];
+            }
+          }
         } else if constexpr (EPI == EPI_TF32_PAIR) {
           float hi[32], lo[32];
 #pragma unroll
@@ -512,6 +537,9 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
 #pragma unroll
           for (int i = 0; i < 32; ++i) v0[i] *= v1[i];
           store_split32(e.out0_hi + row * e.ld_out + col, e.out0_lo + row * e.ld_out + col, v0);
+          if (mirror)
+            store_split32_t(e.out0_hi + static_cast<int64_t>(col) * e.ld_out + row,
+                            e.out0_lo + static_cast<int64_t>(col) * e.ld_out + row, e.ld_out, v0);
         } else if constexpr (EPI == EPI_SIGMA_H) {
           // acc0 = G_occ, acc1 = G_virt, acc2 = Zt
           float z[32], v1[32];
@@ -519,10 +547,16 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
 #pragma unroll
           for (int i = 0; i < 32; ++i) v0[i] *= z[i];
           store_split32(e.out0_hi + row * e.ld_out + col, e.out0_lo + row * e.ld_out + col, v0);
+          if (mirror)
+            store_split32_t(e.out0_hi + static_cast<int64_t>(col) * e.ld_out + row,
+                            e.out0_lo + static_cast<int64_t>(col) * e.ld_out + row, e.ld_out, v0);
           load(1, c, v1);
 #pragma unroll
           for (int i = 0; i < 32; ++i) v1[i] *= z[i];
           store_split32(e.out1_hi + row * e.ld_out + col, e.out1_lo + row * e.ld_out + col, v1);
+          if (mirror)
+            store_split32_t(e.out1_hi + static_cast<int64_t>(col) * e.ld_out + row,
+                            e.out1_lo + static_cast<int64_t>(col) * e.ld_out + row, e.ld_out, v1);
         } else if constexpr (EPI == EPI_ROWDOT2) {
           float v1[32], xs[32];
           load(1, c, v1);
