@@ -267,46 +267,66 @@ int trtri_rec(Handles &h, double *A, int64_t n, int64_t lda, double *T) {
   return MBPT_OK;
 }
 
-// The same recursion on TF32 pairs, for the diagonal block [o, o + n) of L^-1
-// (diagonal kTrtriLeaf blocks already in IC/IR, the factor's rows in LR).
-// Each node is two tensor-core products whose epilogues write pairs straight
-// into the layouts the next products read, so nothing is converted between
-// them. With the engine forming P = A_e B_e^T row by row of A_e:
+// The same recursion on TF32 pairs over the whole n x n factor (diagonal
+// kTrtriLeaf blocks already in IC/IR, the factor's rows in LR), level by
+// level: the nodes of one depth are independent, so each depth is two grouped
+// launches, deepest first. Each node's products have epilogues that write
+// pairs straight into the layouts the next products read, so nothing is
+// converted between them. With the engine forming P = A_e B_e^T row by row of
+// A_e, for the node [o, o + n) split at n1:
 //   P1 = T^T = (L11^-1)^T L21^T:  A_e = IC rows (zero for k < row: K from m0),
-//        B_e = LR rows of L21; stored as pairs in TT;
+//        B_e = LR rows of L21; stored as pairs in TT rows [o, o + n1);
 //   P2 = L21'^T = -(T^T) (L22^-1)^T: A_e = TT, B_e = IR rows of L22^-1 (zero
 //        for k > row: K up to the tile's end); stored into IC and, transposed,
 //        into IR.
-int trtri_pairs(const PairScratch &s, int64_t o, int64_t n, int *err, cudaStream_t st) {
-  if (n <= kTrtriLeaf) return MBPT_OK;
-  const int64_t n1 = round_up(n / 2, kTrtriLeaf), n2 = n - n1, n2p = round_up(n2, 128);
-  int rc = trtri_pairs(s, o, n1, err, st);
-  if (rc) return rc;
-  rc = trtri_pairs(s, o + n1, n2, err, st);
-  if (rc) return rc;
+// Nodes of one depth cover disjoint rows, so their TT blocks do not overlap.
+void collect_nodes(int64_t o, int64_t n, size_t depth,
+                   std::vector<std::vector<std::pair<int64_t, int64_t>>> &levels) {
+  if (n <= kTrtriLeaf) return;
+  if (levels.size() <= depth) levels.resize(depth + 1);
+  levels[depth].push_back({o, n});
+  const int64_t n1 = round_up(n / 2, kTrtriLeaf);
+  collect_nodes(o, n1, depth + 1, levels);
+  collect_nodes(o + n1, n - n1, depth + 1, levels);
+}
+
+int trtri_pairs(const PairScratch &s, int64_t n, int *err, cudaStream_t st) {
+  std::vector<std::vector<std::pair<int64_t, int64_t>>> levels;
+  collect_nodes(0, n, 0, levels);
   const int64_t ld = s.np;
-  auto at = [ld](float *b, int64_t r, int64_t c) { return b + r * ld + c; };
-  SplitMat A1{at(s.ic_hi, o, o), at(s.ic_lo, o, o), n1, n1, ld, true};
-  SplitMat B1{at(s.lr_hi, o + n1, o), at(s.lr_lo, o + n1, o), n2p, n1, ld, true};
-  umma::EpiArgs e1;
-  e1.p_hi = s.tt_hi;
-  e1.p_lo = s.tt_lo;
-  e1.ld_p = ld;
-  e1.alpha = 1.f;
-  rc = gemm_split(umma::EPI_TF32_PAIR, 1, &A1, &B1, n1, n2p, e1, err, st, umma::BAND_K_FROM_M);
-  if (rc) return rc;
-  const int64_t k2 = round_up(n2, 32);
-  SplitMat A2{s.tt_hi, s.tt_lo, n1, k2, ld, true};
-  SplitMat B2{at(s.ir_hi, o + n1, o + n1), at(s.ir_lo, o + n1, o + n1), n2p, k2, ld, true};
-  umma::EpiArgs e2;
-  e2.p_hi = at(s.ic_hi, o, o + n1);
-  e2.p_lo = at(s.ic_lo, o, o + n1);
-  e2.ld_p = ld;
-  e2.t_hi = at(s.ir_hi, o + n1, o);
-  e2.t_lo = at(s.ir_lo, o + n1, o);
-  e2.ld_t = ld;
-  e2.alpha = -1.f;
-  return gemm_split(umma::EPI_TF32_PAIR, 1, &A2, &B2, n1, n2p, e2, err, st, umma::BAND_K_TO_N);
+  const SplitMat IC{s.ic_hi, s.ic_lo, ld, ld, ld, true}, IR{s.ir_hi, s.ir_lo, ld, ld, ld, true};
+  const SplitMat LR{s.lr_hi, s.lr_lo, ld, ld, ld, true}, TT{s.tt_hi, s.tt_lo, ld, ld, ld, true};
+  std::vector<GemmGroup> g1, g2;
+  for (size_t d = levels.size(); d-- > 0;) {
+    g1.clear();
+    g2.clear();
+    for (const auto &node : levels[d]) {
+      const int64_t o = node.first, nn = node.second;
+      const int64_t n1 = round_up(nn / 2, kTrtriLeaf), n2 = nn - n1, n2p = round_up(n2, 128);
+      g1.push_back({n1, n2p, n1, o, o, o + n1, o, o * ld, 0});
+      g2.push_back({n1, n2p, n2, o, 0, o + n1, o + n1, o * ld + o + n1, (o + n1) * ld + o});
+    }
+    umma::EpiArgs e1;
+    e1.p_hi = s.tt_hi;
+    e1.p_lo = s.tt_lo;
+    e1.ld_p = ld;
+    e1.alpha = 1.f;
+    int rc = gemm_split_grouped(umma::EPI_TF32_PAIR, IC, LR, g1.data(),
+                                static_cast<int>(g1.size()), e1, err, st, umma::BAND_K_FROM_M);
+    if (rc) return rc;
+    umma::EpiArgs e2;
+    e2.p_hi = s.ic_hi;
+    e2.p_lo = s.ic_lo;
+    e2.ld_p = ld;
+    e2.t_hi = s.ir_hi;
+    e2.t_lo = s.ir_lo;
+    e2.ld_t = ld;
+    e2.alpha = -1.f;
+    rc = gemm_split_grouped(umma::EPI_TF32_PAIR, TT, IR, g2.data(), static_cast<int>(g2.size()),
+                            e2, err, st, umma::BAND_K_TO_N);
+    if (rc) return rc;
+  }
+  return MBPT_OK;
 }
 
 struct TimingTag {
@@ -335,7 +355,7 @@ int spd_inverse_from_factor(Handles &h, double *L, int64_t n, double *T, double 
     int rc = launch_trtri_diag_blocks(L, n, n, static_cast<int>(kTrtriLeaf), st, s.ic_hi,
                                       s.ic_lo, s.ir_hi, s.ir_lo, np);
     if (rc) return rc;
-    rc = trtri_pairs(s, 0, n, err, st);
+    rc = trtri_pairs(s, n, err, st);
     if (rc) return rc;
     SplitMat Ae{s.ic_hi, s.ic_lo, np, kp, np, true};
     umma::EpiArgs e;

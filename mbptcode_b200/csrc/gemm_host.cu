@@ -3,6 +3,8 @@
 #include <mutex>
 #include <vector>
 
+#include <algorithm>
+
 #include "internal.h"
 
 namespace mbpt {
@@ -66,6 +68,7 @@ int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
   p.tiles_m = static_cast<int>(m_rows / umma::BM);
   p.tiles_n = static_cast<int>(n_rows / BN);
   p.band = band;
+  p.ngroups = 0;
   p.epi = e;
   p.err = err;
   auto kern = umma::gemm_split_kernel<NACC, BN, EPI, TF32, DRAIN>;
@@ -84,7 +87,80 @@ int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 
+constexpr int kMaxGroups = 32;
+
+// One grouped launch of up to kMaxGroups single-accumulator TF32 products.
+template <int EPI, int DRAIN>
+int launch_grouped(const SplitMat &A, const SplitMat &B, const GemmGroup *g, int ng,
+                   const umma::EpiArgs &e, int *err, cudaStream_t st, int band) {
+  using L = umma::Layout<1, 128, (DRAIN > 0)>;
+  if (!A.tf32 || !B.tf32 || ng < 1 || ng > kMaxGroups) return MBPT_ERR_SHAPE;
+  umma::Params<1, kMaxGroups> p;
+  if (!make_tmap(&p.tm[0], A.hi, A.rows, A.cols, A.ld, umma::BM, true) ||
+      !make_tmap(&p.tm[1], A.lo, A.rows, A.cols, A.ld, umma::BM, true) ||
+      !make_tmap(&p.tm[2], B.hi, B.rows, B.cols, B.ld, 128, true) ||
+      !make_tmap(&p.tm[3], B.lo, B.rows, B.cols, B.ld, 128, true))
+    return MBPT_ERR_SHAPE;
+  int tiles = 0;
+  for (int i = 0; i < ng; ++i) {
+    const GemmGroup &q = g[i];
+    const int64_t kp = (q.k + 31) / 32 * 32;
+    // every block inside its array, K origins on 32-element slabs
+    if (q.m_rows <= 0 || q.n_rows <= 0 || q.m_rows % umma::BM || q.n_rows % 128 || q.k <= 0 ||
+        q.a_k0 % 32 || q.b_k0 % 32 || q.a_row0 < 0 || q.b_row0 < 0 ||
+        q.a_row0 + q.m_rows > A.rows || q.b_row0 + q.n_rows > B.rows ||
+        q.a_k0 + kp > A.cols || q.b_k0 + kp > B.cols)
+      return MBPT_ERR_SHAPE;
+    umma::Group &G = p.grp[i];
+    G.tile_base = tiles;
+    G.tiles_m = static_cast<int>(q.m_rows / umma::BM);
+    G.tiles_n = static_cast<int>(q.n_rows / 128);
+    G.a_row0 = static_cast<int>(q.a_row0);
+    G.a_k0 = static_cast<int>(q.a_k0);
+    G.b_row0 = static_cast<int>(q.b_row0);
+    G.b_k0 = static_cast<int>(q.b_k0);
+    G.k_tiles = static_cast<int>(kp / 32);
+    G.p_off = q.p_off;
+    G.t_off = q.t_off;
+    tiles += G.tiles_m * G.tiles_n;
+  }
+  p.ngroups = ng;
+  p.k_tiles[0] = 0;
+  p.tiles_m = p.tiles_n = 0;
+  p.band = band;
+  p.epi = e;
+  p.err = err;
+  auto kern = umma::gemm_split_kernel<1, 128, EPI, true, DRAIN, kMaxGroups>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kSmemBytes) !=
+        cudaSuccess)
+      return MBPT_ERR_CUDA;
+    attr_set = true;
+  }
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  const bool timed = timing_begin(st, &ev0, &ev1);
+  count_launch();
+  kern<<<tiles, 192, L::kSmemBytes, st>>>(p);
+  if (timed) timing_end(st, EPI, ev0, ev1);
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
 }  // namespace
+
+int gemm_split_grouped(int epi, const SplitMat &A, const SplitMat &B, const GemmGroup *groups,
+                       int ngroups, const umma::EpiArgs &e, int *err, cudaStream_t st,
+                       int band) {
+  constexpr int kDrain = 2;
+  for (int first = 0; first < ngroups; first += kMaxGroups) {
+    const int ng = std::min(kMaxGroups, ngroups - first);
+    int rc = MBPT_ERR_UNSUPPORTED;
+    if (epi == umma::EPI_TF32_PAIR)
+      rc = launch_grouped<umma::EPI_TF32_PAIR, kDrain>(A, B, groups + first, ng, e, err, st, band);
+    if (rc) return rc;
+  }
+  return MBPT_OK;
+}
 
 // ---- optional per-launch timing of the engine (CUDA events on the stream) ----
 namespace {

@@ -22,6 +22,21 @@ int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t 
                int64_t n_rows, const umma::EpiArgs &e, int *err, cudaStream_t st,
                int band = 0);
 
+// One product of a grouped launch: an m_rows x n_rows output block (multiples
+// of 128) from the A rows [a_row0, +m_rows) and B rows [b_row0, +n_rows), K
+// elements from a_k0 / b_k0 (multiples of 32), output origins at element
+// offsets p_off / t_off of the epilogue's arrays.
+struct GemmGroup {
+  int64_t m_rows, n_rows, k;
+  int64_t a_row0, a_k0, b_row0, b_k0;
+  int64_t p_off, t_off;
+};
+// Independent single-accumulator TF32 products of the same A and B arrays in
+// as few launches as possible (up to 32 per launch); EPI_TF32_PAIR only.
+int gemm_split_grouped(int epi, const SplitMat &A, const SplitMat &B, const GemmGroup *groups,
+                       int ngroups, const umma::EpiArgs &e, int *err, cudaStream_t st,
+                       int band = 0);
+
 // Per-epilogue totals of the engine's launch times (enable = 1 starts
 // recording; a call with non-null outputs drains, returns and resets them).
 int gemm_timing(int enable, double *total_ms, long long *launches);

@@ -62,12 +62,26 @@ enum Band : int {
                       // the diagonal twice, the second time transposed)
 };
 
-template <int NACC>
+// Grouped launch (one accumulator): independent products of one launch, each
+// a block of the same A and B arrays. Coordinates are elements of those
+// arrays; the Band spans apply within each product.
+struct Group {
+  int tile_base;       // first linear tile of this product in the launch
+  int tiles_m, tiles_n;
+  int a_row0, a_k0;    // origin of the product's A block (row, K)
+  int b_row0, b_k0;    // origin of its B block
+  int k_tiles;         // K slabs from the origin
+  int64_t p_off, t_off;  // element offsets of its output (and transposed output)
+};
+
+template <int NACC, int NGRP = 0>
 struct Params {
   CUtensorMap tm[4 * NACC];  // per accumulator: A hi, A lo, B hi, B lo
   int k_tiles[NACC];
   int tiles_m, tiles_n;
   int band;  // Band flags (0: dense)
+  int ngroups;
+  Group grp[NGRP > 0 ? NGRP : 1];
   EpiArgs epi;
   int *err;
 };
@@ -277,8 +291,9 @@ struct Layout {
 // therefore restarted every DRAIN K slabs in one of two TMEM buffers, and the
 // epilogue warps add each finished chunk into round-to-nearest FP32 sums in
 // registers while the MMAs fill the other buffer.
-template <int NACC, int BN, int EPI, bool TF32 = false, int DRAIN = 0>
-__global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constant__ Params<NACC> p) {
+template <int NACC, int BN, int EPI, bool TF32 = false, int DRAIN = 0, int NGRP = 0>
+__global__ void __launch_bounds__(192, 1)
+    gemm_split_kernel(const __grid_constant__ Params<NACC, NGRP> p) {
   using L = Layout<NACC, BN, (DRAIN > 0)>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -292,11 +307,29 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
   int *fail = reinterpret_cast<int *>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // this CTA's product (grouped launches) and its origins
+  int pid = blockIdx.x, tiles_m = p.tiles_m, tiles_n = p.tiles_n;
+  int a_row0 = 0, a_k0 = 0, b_row0 = 0, b_k0 = 0, grp_k_tiles = 0;
+  int64_t p_off = 0, t_off = 0;
+  if constexpr (NGRP > 0) {
+    int g = 0;
+    while (g + 1 < p.ngroups && pid >= p.grp[g + 1].tile_base) ++g;
+    const Group &G = p.grp[g];
+    pid -= G.tile_base;
+    tiles_m = G.tiles_m;
+    tiles_n = G.tiles_n;
+    a_row0 = G.a_row0;
+    a_k0 = G.a_k0;
+    b_row0 = G.b_row0;
+    b_k0 = G.b_k0;
+    grp_k_tiles = G.k_tiles;
+    p_off = G.p_off;
+    t_off = G.t_off;
+  }
   // grouped raster: kGroupM row tiles sweep the column tiles together (L2 reuse)
-  const int pid = blockIdx.x;
-  const int per_group = kGroupM * p.tiles_n;
+  const int per_group = kGroupM * tiles_n;
   const int first_m = (pid / per_group) * kGroupM;
-  const int gsize = min(p.tiles_m - first_m, kGroupM);
+  const int gsize = min(tiles_m - first_m, kGroupM);
   const int tm = first_m + (pid % per_group) % gsize;
   const int tn = (pid % per_group) / gsize;
   const int m0 = tm * BM, n0 = tn * BN;
@@ -307,7 +340,7 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
   constexpr int kSlab = TF32 ? 32 : BK;
   auto k_span = [&](int j, int &kb, int &ke) {
     kb = 0;
-    ke = p.k_tiles[j];
+    ke = NGRP > 0 ? grp_k_tiles : p.k_tiles[j];
     if (p.band & BAND_K_FROM_M) kb = max(kb, m0 / kSlab);
     if (p.band & BAND_K_FROM_N) kb = max(kb, n0 / kSlab);
     if (p.band & BAND_K_TO_M) ke = min(ke, (m0 + BM) / kSlab);
@@ -356,10 +389,11 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
           uint8_t *st = smem + s * L::kStageBytes;
           // K coordinate in elements: one 128-byte row per slab
           const int kx = kt * kSlab;
-          tma_load_2d(st, &p.tm[4 * j + 0], kx, m0, &full[s]);
-          tma_load_2d(st + L::kABytes, &p.tm[4 * j + 1], kx, m0, &full[s]);
-          tma_load_2d(st + 2 * L::kABytes, &p.tm[4 * j + 2], kx, n0, &full[s]);
-          tma_load_2d(st + 2 * L::kABytes + L::kBBytes, &p.tm[4 * j + 3], kx, n0, &full[s]);
+          tma_load_2d(st, &p.tm[4 * j + 0], a_k0 + kx, a_row0 + m0, &full[s]);
+          tma_load_2d(st + L::kABytes, &p.tm[4 * j + 1], a_k0 + kx, a_row0 + m0, &full[s]);
+          tma_load_2d(st + 2 * L::kABytes, &p.tm[4 * j + 2], b_k0 + kx, b_row0 + n0, &full[s]);
+          tma_load_2d(st + 2 * L::kABytes + L::kBBytes, &p.tm[4 * j + 3], b_k0 + kx,
+                      b_row0 + n0, &full[s]);
         }
       }
       if (!ok) {
@@ -515,8 +549,8 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
             hi[i] = to_tf32(v);
             lo[i] = to_tf32(v - hi[i]);
           }
-          float4 *dh = reinterpret_cast<float4 *>(e.p_hi + row * e.ld_p + col);
-          float4 *dl = reinterpret_cast<float4 *>(e.p_lo + row * e.ld_p + col);
+          float4 *dh = reinterpret_cast<float4 *>(e.p_hi + p_off + row * e.ld_p + col);
+          float4 *dl = reinterpret_cast<float4 *>(e.p_lo + p_off + row * e.ld_p + col);
 #pragma unroll
           for (int q = 0; q < 8; ++q) {
             dh[q] = make_float4(hi[4 * q], hi[4 * q + 1], hi[4 * q + 2], hi[4 * q + 3]);
@@ -527,8 +561,8 @@ __global__ void __launch_bounds__(192, 1) gemm_split_kernel(const __grid_constan
             // consecutive rows land on 32 consecutive floats
 #pragma unroll
             for (int i = 0; i < 32; ++i) {
-              e.t_hi[static_cast<int64_t>(col + i) * e.ld_t + row] = hi[i];
-              e.t_lo[static_cast<int64_t>(col + i) * e.ld_t + row] = lo[i];
+              e.t_hi[t_off + static_cast<int64_t>(col + i) * e.ld_t + row] = hi[i];
+              e.t_lo[t_off + static_cast<int64_t>(col + i) * e.ld_t + row] = lo[i];
             }
           }
         } else if constexpr (EPI == EPI_HADAMARD_SPLIT) {
