@@ -211,6 +211,47 @@ __global__ void __launch_bounds__(256) transform_kernel(
   }
 }
 
+// The same transform for J = K = N (every transform of the route: the minimax
+// grids pair N tau with N omega points), N a compile-time constant: all N
+// inputs of an element are loaded before any arithmetic (N loads in flight
+// per element), each thread takes two neighbouring columns so that every
+// weight read from shared memory feeds two FMAs, and no loop is predicated.
+template <typename Tin, int N>
+__global__ void __launch_bounds__(256) transform_n_kernel(
+    const Tin *__restrict__ in, int64_t in_slice, int64_t ld_in, int64_t rows, int64_t cols,
+    const double *__restrict__ w, double *__restrict__ out, int64_t out_slice, int64_t ld_out) {
+  __shared__ double ws[N * N];
+  for (int i = threadIdx.x; i < N * N; i += blockDim.x) ws[i] = w[i];
+  __syncthreads();
+  // one pair of columns per thread and no grid-stride loop, so that nothing
+  // invites the compiler to keep the N^2 weights in registers across elements
+  const int64_t half = (cols + 1) / 2;
+  const int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (e >= rows * half) return;
+  const int64_t r = e / half, c = 2 * (e % half);
+  const bool two = c + 1 < cols;
+  const Tin *src = in + r * ld_in + c;
+  double x0[N], x1[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    x0[k] = static_cast<double>(src[k * in_slice]);
+    x1[k] = two ? static_cast<double>(src[k * in_slice + 1]) : 0.0;
+  }
+  double *dst = out + r * ld_out + c;
+#pragma unroll
+  for (int j = 0; j < N; ++j) {
+    double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      const double wv = ws[j * N + k];
+      a0 = fma(wv, x0[k], a0);
+      a1 = fma(wv, x1[k], a1);
+    }
+    dst[j * out_slice] = a0;
+    if (two) dst[j * out_slice + 1] = a1;
+  }
+}
+
 // a <- I - a for each n x n slice; trace[f] = tr(a) before the update.
 __global__ void one_minus_kernel(double *a, int64_t n, double *trace) {
   double *m = a + static_cast<int64_t>(blockIdx.y) * n * n;
@@ -428,6 +469,24 @@ template <typename Tin>
 void launch_transform(const Tin *in, int64_t in_slice, int64_t ld_in, int64_t rows,
                       int64_t cols, const double *w_dev, int J, int K, double *out,
                       int64_t out_slice, int64_t ld_out, cudaStream_t st) {
+  if (J == K) {
+    const int64_t elems = rows * ((cols + 1) / 2);
+#define MBPT_TRANSFORM_N(NN)                                                                  \
+  case NN:                                                                                    \
+    count_launch();                                                                           \
+    transform_n_kernel<Tin, NN><<<static_cast<unsigned>((elems + 255) / 256), 256, 0, st>>>( \
+        in, in_slice, ld_in, rows, cols, w_dev, out, out_slice, ld_out);                      \
+    return;
+    switch (J) {
+      MBPT_TRANSFORM_N(6) MBPT_TRANSFORM_N(8) MBPT_TRANSFORM_N(10) MBPT_TRANSFORM_N(12)
+      MBPT_TRANSFORM_N(14) MBPT_TRANSFORM_N(16) MBPT_TRANSFORM_N(18) MBPT_TRANSFORM_N(20)
+      MBPT_TRANSFORM_N(22) MBPT_TRANSFORM_N(24) MBPT_TRANSFORM_N(26) MBPT_TRANSFORM_N(28)
+      MBPT_TRANSFORM_N(30) MBPT_TRANSFORM_N(32) MBPT_TRANSFORM_N(34)
+      default:
+        break;
+    }
+#undef MBPT_TRANSFORM_N
+  }
   count_launch(); transform_kernel<Tin, false><<<grid_cap(rows * cols), 256, 0, st>>>(
       in, in_slice, ld_in, rows, cols, w_dev, J, K, out, nullptr, nullptr, out_slice, ld_out);
 }
