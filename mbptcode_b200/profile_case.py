@@ -19,6 +19,9 @@ products and W = L^-T L^-1) and the mirrored FP64 store.
 
 --sweep: one whole mixed chi0 -> W -> Sigma -> QP sweep (24 points) of a
 synthetic system, for the launch list of the benchmark's workload.
+
+--transform N: one FP64 tau <-> omega transform of 24 N x N matrices with a
+24 x 24 weight matrix (mbpt_transform, the W(i w) -> W(tau) step).
 """
 from __future__ import annotations
 
@@ -70,6 +73,17 @@ def sweep(a):
     print(f'sweep case M={a.M} n={a.n}: E_c {float(res["e_c"]):.6e}')
 
 
+def transform_case(a):
+    from .space_time import transform
+    n, k = a.transform, 24
+    g = torch.Generator(device='cuda').manual_seed(2)
+    x = torch.randn(k, n, n, generator=g, device='cuda', dtype=torch.float64)
+    w = np.random.default_rng(2).standard_normal((k, k))
+    out = transform(x, w)
+    torch.cuda.synchronize()
+    print(f'transform case n={n} K=J={k}: |out| {float(out.abs().max()):.3e}')
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument('--M', type=int, default=None)
@@ -79,10 +93,13 @@ def main():
     p.add_argument('--dyson', type=int, default=0)
     p.add_argument('--nfreq', type=int, default=1)
     p.add_argument('--sweep', action='store_true')
+    p.add_argument('--transform', type=int, default=0)
     a = p.parse_args()
     torch.cuda.set_device(0)
     if a.dyson:
         return dyson(a)
+    if a.transform:
+        return transform_case(a)
     big = a.sweep
     a.M = a.M or (7200 if big else 4096)
     a.n = a.n or (1200 if big else 682)
