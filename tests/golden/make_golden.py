@@ -18,7 +18,15 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      diagonal from the AO build, QP roots and Z for every
                      state, E_c and its adjoint;
 * qp_kat.npz         the root finder on closed-form self-energies
-                     (tests/test_qp_refine_root.py's two-pole Sigma and others).
+                     (tests/test_qp_refine_root.py's two-pole Sigma and others);
+* c1_<variant>.npz   the synthetic FP64 configuration at full size (n_orb = 400,
+                     nocc = 40, N_mu = 2400, 16 points, seed 400): the Sigma_c
+                     diagonal, every QP root and Z, E_c, and the adjoint
+                     projected on 32 seeded directions. X and D (46 MB) are not
+                     stored: the tests regenerate them from the seed and check
+                     the regeneration against the stored eps and checksums.
+
+    python tests/golden/make_golden.py [/root/reference] [--only c1]
 """
 import os
 import sys
@@ -26,7 +34,11 @@ import warnings
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+ARGS = [a for a in sys.argv[1:] if not a.startswith('--')]
+ONLY = sys.argv[sys.argv.index('--only') + 1] if '--only' in sys.argv else None
+if ONLY:
+    ARGS = [a for a in ARGS if a != ONLY]
+REF = ARGS[0] if ARGS else '/root/reference'
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REF)
 sys.path.insert(0, os.path.abspath(os.path.join(HERE, '..', '..')))
@@ -50,6 +62,9 @@ from src.Solvers.qp_equation import solve_qp_equation_pole_strength     # noqa: 
 from src.gradients.rpa.space_time_adjoint import rpa_energy_and_adjoint  # noqa: E402
 
 from mbptcode_b200.synthetic import synthetic_system                    # noqa: E402
+
+sys.path.insert(0, HERE)
+from c1_common import C1, c1_directions                                  # noqa: E402
 
 
 def grids_fixture():
@@ -140,6 +155,48 @@ def route_fixture(name, n_orb, nocc, M, seed, variant, ntau, full=False):
         eps_bar=eps_bar, X_bar=X_bar, D_bar=D_bar)
 
 
+def c1_fixture(variant):
+    n_orb, nocc, M, ntau, seed = (C1[k] for k in ('n_orb', 'nocc', 'M', 'ntau', 'seed'))
+    X, D, eps = synthetic_system(n_orb, nocc, M, seed, variant)
+    e_min, e_max, mu = particle_hole_window(eps, nocc)
+    freq, fw = screening_frequency_grid(ntau, eps, nocc, mu=mu)
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        grid = TimeFrequencyGrid.minimax_split(ntau, e_min, e_max, freq, fw)
+    rW, rS = sigma_fit_ranges(eps, nocc, mu=mu)
+    tau_sigma = 0.5 * minimax_time_grid(ntau, *rS)[0]
+    pade = gauss_legendre_grid(16, w0=1.0)[0]
+    chi0 = chi0_imaginary_frequency(X, D, eps, nocc, grid, mu=mu)
+    W = np.stack([dyson_screening(c, correlation=True) for c in chi0])
+    del chi0
+    sig_ao = self_energy_matrix_imaginary_time(
+        X, D, W + np.eye(W.shape[-1]), np.eye(n_orb), eps, nocc, tau_sigma,
+        freq, pade, mu=mu)
+    del W
+    states = np.arange(n_orb)
+    sigma = sigma_ao_to_mo_diagonal(sig_ao, np.eye(n_orb), states=states).T
+    roots, zs = np.empty(n_orb), np.empty(n_orb)
+    for i, p in enumerate(states):
+        sign = -1.0 if p < nocc else 1.0
+        s_p = np.conj(sigma[i]) if p < nocc else sigma[i]
+        fit = PadeFit(mu + 1j * sign * pade, s_p, greedy=True)
+
+        def residual(w, fit=fit, p=p):
+            return w - eps[p] - fit(np.array([w], dtype=complex))[0].real
+        got = solve_qp_equation_pole_strength(residual, eps[p], return_diagnostics=True)
+        roots[i] = got[0]
+        dz = [z for w, z in got[1] if w == got[0]]
+        zs[i] = dz[0] if dz else np.nan
+    e_c, eps_bar, X_bar, D_bar, _ = rpa_energy_and_adjoint(X, D, eps, nocc, grid, mu=mu)
+    proj = np.array([float(eps_bar @ de + (X_bar * dX).sum() + (D_bar * dD).sum())
+                     for de, dX, dD in c1_directions(n_orb, M, seed + 1)])
+    np.savez_compressed(
+        os.path.join(HERE, f'c1_{variant}.npz'), eps=eps, nocc=nocc, ntau=ntau, mu=mu,
+        seed=seed, M=M, X_sum=X.sum(), X_abs_sum=np.abs(X).sum(), D_sum=D.sum(),
+        D_diag=np.diag(D).copy(), sigma=sigma, roots=roots, z=zs, e_c=e_c,
+        adjoint_projections=proj)
+
+
 def qp_fixture():
     cases = {  # poles placed off the scan grids, so no division hits one
         'two_pole': (lambda w: 0.05 / (w + 0.8) + 0.01 / (w - 0.9), -0.2),
@@ -166,6 +223,11 @@ def qp_fixture():
 
 
 if __name__ == '__main__':
+    if ONLY == 'c1':
+        c1_fixture('literal')
+        c1_fixture('calibrated')
+        print('C1 fixtures written to', HERE)
+        sys.exit(0)
     grids_fixture()
     shared_kernel_fixture()
     route_fixture('calibrated', 24, 4, 64, 7, 'calibrated', 12, full=True)

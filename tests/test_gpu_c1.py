@@ -1,0 +1,93 @@
+"""Parity at the synthetic FP64 configuration's full size (n_orb = 400,
+nocc = 40, N_mu = 2400, 16 points; literal and calibrated generators) against
+outputs of the reference itself (tests/golden/c1_*.npz, made by
+tests/golden/make_golden.py --only c1), and the adjoint against central
+differences at the same size.
+
+X and D are regenerated from the seed; the regeneration is checked first
+against the stored eps and checksums. Tolerances as for the small routes:
+the 16-point transforms carry ~1e9 weights, which turn FP64 summation-order
+differences into ~1e-10 relative on Sigma and E_c and ~1e-6 on the adjoint."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip('torch')
+pytestmark = pytest.mark.gpu
+
+from mbptcode_b200 import adjoint, grids, gw, space_time as st     # noqa: E402
+from mbptcode_b200.synthetic import synthetic_system                # noqa: E402
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), 'golden'))
+from c1_common import C1, c1_directions                             # noqa: E402
+
+N, NOCC, M, NTAU, SEED = (C1[k] for k in ('n_orb', 'nocc', 'M', 'ntau', 'seed'))
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.fixture(scope='module', params=['literal', 'calibrated'])
+def c1(request):
+    g = np.load(os.path.join(os.path.dirname(__file__), 'golden', f'c1_{request.param}.npz'))
+    X, D, eps = synthetic_system(N, NOCC, M, SEED, request.param)
+    assert np.array_equal(eps, g['eps'])
+    assert abs(X.sum() - float(g['X_sum'])) < 1e-9 * float(g['X_abs_sum'])
+    assert rel(np.diag(D), g['D_diag']) < 1e-12
+    X_d = torch.as_tensor(X, device='cuda')
+    D_d = torch.as_tensor(D, device='cuda')
+    return request.param, g, X_d, D_d, eps
+
+
+def test_c1_route_fp64_matches_reference(c1):
+    variant, g, X, D, eps = c1
+    res = gw.gw_sweep(X, D, eps, NOCC, ntau=NTAU, precision='fp64')
+    assert rel(res['sigma'].cpu().numpy(), g['sigma']) < 1e-9
+    roots = res['roots'].cpu().numpy()
+    ok = np.isfinite(g['roots'])
+    assert np.array_equal(ok, np.isfinite(roots))
+    f = np.arange(NOCC - 10, NOCC + 10)
+    assert np.abs(roots[f] - g['roots'][f]).max() < 5e-8
+    assert np.abs(roots[ok] - g['roots'][ok]).max() < 2e-6
+    e_ref = float(g['e_c'])
+    assert abs(float(res['e_c']) - e_ref) <= 1e-9 * abs(e_ref) + 1e-15
+
+
+def test_c1_adjoint_matches_reference(c1):
+    variant, g, X, D, eps = c1
+    axes = grids.space_time_axes(eps, NOCC, ntau=NTAU)
+    e, eb, xb, db, _ = adjoint.rpa_energy_and_adjoint(X, D, eps, NOCC, axes.grid)
+    eb, xb, db = (np.asarray(t.cpu().numpy() if torch.is_tensor(t) else t) for t in (eb, xb, db))
+    proj = np.array([float(eb @ de + (xb * dX).sum() + (db * dD).sum())
+                     for de, dX, dD in c1_directions(N, M, SEED + 1)])
+    ref = g['adjoint_projections']
+    assert rel(proj, ref) < 1e-5
+
+
+def test_c1_adjoint_central_differences():
+    """32 seeded directions, h = 1e-5, on the calibrated C1 tensors with the
+    regularised 20-point grid (at 16 points the ~1e9 transform weights put
+    the difference quotient's noise near 1e-3, for the reference's adjoint as
+    for this one); grid and mu frozen, as the adjoint assumes."""
+    X, D, eps = synthetic_system(N, NOCC, M, SEED, 'calibrated')
+    axes = grids.space_time_axes(eps, NOCC, ntau=20)
+    mu = axes.mu
+    Xd, Dd = torch.as_tensor(X, device='cuda'), torch.as_tensor(D, device='cuda')
+    e, eb, xb, db, _ = adjoint.rpa_energy_and_adjoint(Xd, Dd, eps, NOCC, axes.grid, mu=mu)
+    eb, xb, db = (np.asarray(t.cpu().numpy() if torch.is_tensor(t) else t) for t in (eb, xb, db))
+    h = 1e-5
+    errs = []
+    for de, dX, dD in c1_directions(N, M, SEED + 7):
+        def energy(s):
+            Xs = Xd + s * h * torch.as_tensor(dX, device='cuda')
+            Ds = Dd + s * h * torch.as_tensor(dD, device='cuda')
+            return st.rpa_correlation_energy_space_time(Xs, Ds, eps + s * h * de, NOCC,
+                                                        axes.grid, mu=mu, precision='fp64')
+        fd = (energy(1) - energy(-1)) / (2 * h)
+        ad = float(eb @ de + (xb * dX).sum() + (db * dD).sum())
+        errs.append(abs(fd - ad) / max(abs(ad), 1e-300))
+    assert max(errs) < 1e-6, max(errs)
