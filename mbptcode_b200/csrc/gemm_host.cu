@@ -51,7 +51,9 @@ template <int NACC, int BN, int EPI, bool TF32, int DRAIN>
 int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
            const umma::EpiArgs &e, int *err, cudaStream_t st, int band = 0) {
   using L = umma::Layout<NACC, BN, (DRAIN > 0)>;
-  if (m_rows % umma::BM || n_rows % BN || m_rows <= 0 || n_rows <= 0) return MBPT_ERR_SHAPE;
+  // the last column tile may overhang a multiple of 128 (BN = 256): its
+  // B rows read as zeros and its dead columns are not stored
+  if (m_rows % umma::BM || n_rows % 128 || m_rows <= 0 || n_rows <= 0) return MBPT_ERR_SHAPE;
   const int64_t bk = TF32 ? 32 : 64;
   umma::Params<NACC> p;
   for (int j = 0; j < NACC; ++j) {
@@ -66,7 +68,8 @@ int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
     p.k_tiles[j] = static_cast<int>(A[j].cols / bk);
   }
   p.tiles_m = static_cast<int>(m_rows / umma::BM);
-  p.tiles_n = static_cast<int>(n_rows / BN);
+  p.tiles_n = static_cast<int>((n_rows + BN - 1) / BN);
+  p.n_valid = static_cast<int>(n_rows);
   p.band = band;
   p.ngroups = 0;
   p.epi = e;
@@ -82,7 +85,7 @@ int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   const bool timed = timing_begin(st, &ev0, &ev1);
   count_launch();
-  kern<<<p.tiles_m * p.tiles_n, 192, L::kSmemBytes, st>>>(p);
+  kern<<<p.tiles_m * p.tiles_n, 64 + BN, L::kSmemBytes, st>>>(p);
   if (timed) timing_end(st, EPI, ev0, ev1);
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
@@ -127,6 +130,7 @@ int launch_grouped(const SplitMat &A, const SplitMat &B, const GemmGroup *g, int
   p.ngroups = ng;
   p.k_tiles[0] = 0;
   p.tiles_m = p.tiles_n = 0;
+  p.n_valid = 1 << 30;
   p.band = band;
   p.epi = e;
   p.err = err;
@@ -278,8 +282,10 @@ int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t 
       return launch<1, 128, EPI_TF32_PAIR, true, kDrain>(A, B, m_rows, n_rows, e, err, st);
     return MBPT_ERR_UNSUPPORTED;
   }
+  // the non-symmetric N^3 products: 128 x 256 tiles (a quarter fewer operand
+  // bytes per flop through the shared-memory ring than 128 x 128)
   if (nacc == 1 && epi == EPI_SPLIT)
-    return launch<1, 128, EPI_SPLIT, false, kDrain>(A, B, m_rows, n_rows, e, err, st);
+    return launch<1, 256, EPI_SPLIT, false, kDrain>(A, B, m_rows, n_rows, e, err, st);
   if (nacc == 1 && epi == EPI_F32)
     return launch<1, 128, EPI_F32, false, kDrain>(A, B, m_rows, n_rows, e, err, st);
   if (nacc == 1 && epi == EPI_F32_ACC)

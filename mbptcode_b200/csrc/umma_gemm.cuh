@@ -79,6 +79,7 @@ struct Params {
   CUtensorMap tm[4 * NACC];  // per accumulator: A hi, A lo, B hi, B lo
   int k_tiles[NACC];
   int tiles_m, tiles_n;
+  int n_valid;  // output columns to store (tiles_n * BN unless the last tile overhangs)
   int band;  // Band flags (0: dense)
   int ngroups;
   Group grp[NGRP > 0 ? NGRP : 1];
@@ -291,8 +292,10 @@ struct Layout {
 // therefore restarted every DRAIN K slabs in one of two TMEM buffers, and the
 // epilogue warps add each finished chunk into round-to-nearest FP32 sums in
 // registers while the MMAs fill the other buffer.
+// BN = 128: 6 warps (producer, MMA, 4 epilogue); BN = 256: 10 warps, the 8
+// epilogue warps covering the TMEM lane quarters twice, 128 columns each.
 template <int NACC, int BN, int EPI, bool TF32 = false, int DRAIN = 0, int NGRP = 0>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(64 + BN, 1)
     gemm_split_kernel(const __grid_constant__ Params<NACC, NGRP> p) {
   using L = Layout<NACC, BN, (DRAIN > 0)>;
   extern __shared__ uint8_t smem_raw[];
@@ -356,7 +359,7 @@ __global__ void __launch_bounds__(192, 1)
     mbar_init(accum, 1);
     for (int b = 0; b < 2; ++b) {
       mbar_init(&dfull[b], 1);
-      mbar_init(&dempty[b], 4);
+      mbar_init(&dempty[b], BN / 32);
     }
     *fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -460,14 +463,16 @@ __global__ void __launch_bounds__(192, 1)
     }
     __syncwarp();
   } else {
-    // epilogue: warps 2..5 own TMEM lane quarters (warp % 4)
+    // epilogue: a warp owns TMEM lane quarter warp % 4 (the hardware's rule)
+    // and the 128 columns starting at cb
     const int sp = warp & 3;
+    const int cb = ((warp - 2) >> 2) * 128;
     const uint32_t taddr = tmem + (static_cast<uint32_t>(sp * 32) << 16);
     bool ok = true;
-    float acc[DRAIN > 0 ? BN : 1];
+    float acc[DRAIN > 0 ? 128 : 1];
     if constexpr (DRAIN > 0) {
 #pragma unroll
-      for (int i = 0; i < BN; ++i) acc[i] = 0.f;
+      for (int i = 0; i < 128; ++i) acc[i] = 0.f;
       int kb, ke;
       k_span(kLast, kb, ke);
       const int nchunks = (ke - kb + DRAIN - 1) / DRAIN;
@@ -479,9 +484,9 @@ __global__ void __launch_bounds__(192, 1)
         }
         tc_fence_after();
 #pragma unroll
-        for (int q = 0; q < BN / 32; ++q) {
+        for (int q = 0; q < 4; ++q) {
           float t[32];
-          tmem_ld32(taddr + static_cast<uint32_t>((kLast + b) * BN + 32 * q), t);
+          tmem_ld32(taddr + static_cast<uint32_t>((kLast + b) * BN + cb + 32 * q), t);
 #pragma unroll
           for (int i = 0; i < 32; ++i) acc[32 * q + i] += t[i];
         }
@@ -502,7 +507,8 @@ __global__ void __launch_bounds__(192, 1)
       const EpiArgs &e = p.epi;
       // symmetric output: a tile above the diagonal also fills its mirror
       const bool mirror = (p.band & BAND_UPPER) && tn > tm;
-      // 32 columns starting at c of accumulator j (the drained one from registers)
+      // 32 columns starting at the warp's column c of accumulator j (the
+      // drained one from registers)
       auto load = [&](int j, int c, float (&v)[32]) {
         if constexpr (DRAIN > 0) {
           if (j == kLast) {
@@ -511,11 +517,14 @@ __global__ void __launch_bounds__(192, 1)
             return;
           }
         }
-        tmem_ld32(taddr + static_cast<uint32_t>(j * BN + c), v);
+        tmem_ld32(taddr + static_cast<uint32_t>(j * BN + cb + c), v);
       };
+      // columns past n_valid (a 256-wide tile over a 128-multiple edge) are not stored
+      const bool live = n0 + cb < p.n_valid;
 #pragma unroll
-      for (int c = 0; c < BN; c += 32) {
-        const int col = n0 + c;
+      for (int c = 0; c < 128; c += 32) {
+        if (!live) break;
+        const int col = n0 + cb + c;
         float v0[32];
         load(0, c, v0);
         if constexpr (EPI == EPI_SPLIT) {
