@@ -337,8 +337,9 @@ __global__ void __launch_bounds__(64 + BN, 1)
   const int tn = (pid % per_group) / gsize;
   const int m0 = tm * BM, n0 = tn * BN;
   constexpr int kLast = NACC - 1;
-  // uniform across the CTA, before any barrier or TMEM exists
-  if ((p.band & BAND_UPPER) && tn < tm) return;
+  // uniform across the CTA, before any barrier or TMEM exists: a symmetric
+  // product skips tiles whose last 128-column block lies below the diagonal
+  if ((p.band & BAND_UPPER) && (n0 + BN) / 128 - 1 < tm) return;
   // K slabs [kb, ke) of accumulator j that can hold nonzeros for this tile
   constexpr int kSlab = TF32 ? 32 : BK;
   auto k_span = [&](int j, int &kb, int &ke) {
@@ -505,8 +506,11 @@ __global__ void __launch_bounds__(64 + BN, 1)
       tc_fence_after();
       const int row = m0 + sp * 32 + lane;
       const EpiArgs &e = p.epi;
-      // symmetric output: a tile above the diagonal also fills its mirror
-      const bool mirror = (p.band & BAND_UPPER) && tn > tm;
+      // symmetric output, per 128-column block tb of this warp: a block below
+      // the diagonal is not stored, one above it also fills its mirror
+      const int tb = (n0 + cb) / 128;
+      const bool upper = (p.band & BAND_UPPER) != 0;
+      const bool mirror = upper && tb > tm;
       // 32 columns starting at the warp's column c of accumulator j (the
       // drained one from registers)
       auto load = [&](int j, int c, float (&v)[32]) {
@@ -520,7 +524,7 @@ __global__ void __launch_bounds__(64 + BN, 1)
         tmem_ld32(taddr + static_cast<uint32_t>(j * BN + cb + c), v);
       };
       // columns past n_valid (a 256-wide tile over a 128-multiple edge) are not stored
-      const bool live = n0 + cb < p.n_valid;
+      const bool live = n0 + cb < p.n_valid && !(upper && tb < tm);
 #pragma unroll
       for (int c = 0; c < 128; c += 32) {
         if (!live) break;
