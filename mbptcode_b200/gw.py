@@ -38,7 +38,7 @@ def screened_interaction_tau(W_minus_I, Ctw, stream=None, out=None):
 
 
 def sigma_branch_sums(X, D, Wt, eps, nocc, tau_points, states, mu, precision=None,
-                      stream=None):
+                      stream=None, err=None):
     """(2, ntau, nstates) device tensor: Sigma^<_pp(tau) and Sigma^>_pp(tau) of
     the states, the diagonal form of ``imaginary_time.py:39-92``. Wt None
     stands for W = I at every tau (the bare Coulomb factor)."""
@@ -58,13 +58,15 @@ def sigma_branch_sums(X, D, Wt, eps, nocc, tau_points, states, mu, precision=Non
     mode = _mode(precision)
     branch = torch.empty((2, ntau, S), dtype=torch.float64, device=dev)
     ws = WORKSPACE.get(lib().mbpt_sigma_workspace_bytes(M, norb, nocc, naux, ntau, S, mode), dev)
-    err = _Err(dev)
+    own = err is None
+    err = _Err(dev) if own else err
     check(lib().mbpt_sigma_branch_sums(ptr(Xd), M, norb, nocc, ptr(ed), float(mu), ptr(Dd),
                                        naux, ptr(None if Wt is None else Wt.contiguous()), tp,
                                        ntau, ptr(st), S, mode,
                                        ptr(branch), ptr(ws), ws.numel(), ptr(err.t),
                                        stream_ptr(stream)), 'mbpt_sigma_branch_sums')
-    err.check('mbpt_sigma_branch_sums')
+    if own:
+        err.check('mbpt_sigma_branch_sums')
     return branch
 
 
@@ -147,6 +149,9 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
                                anchor=None if eps_anchor is None else _eps_host(eps_anchor))
     mu = axes.mu
     check_mixed_weights(precision, axes.grid.cosft_wt, axes.Ctw, axes.C, axes.S)
+    # one device error word for the sweep, read once at its end: no host sync
+    # between the stages (the Dyson step waits only for its info words)
+    err = _Err(dev)
     ev = None
     if timings is not None:
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
@@ -157,11 +162,11 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
     chi0, _ = chi0_sweep(X, D, eps_h, nocc, axes.grid.tau_points, axes.grid.cosft_wt, mu=mu,
                          precision=precision, stream=stream,
                          out=None if keep else BUFFERS.take(
-                             'sweep_chi0', (axes.grid.nfreq, naux, naux), dev))
+                             'sweep_chi0', (axes.grid.nfreq, naux, naux), dev), err=err)
     if ev:
         ev[1].record()
     logdet, trace, info, _ = dyson_batch(chi0, want_w=True, stream=stream,
-                                         precision=precision)
+                                         precision=precision, err=err)
     # E_c from the same factorisations: the frequency axis is a minimax quadrature
     e_c = torch.empty((), dtype=torch.float64, device=dev)
     ow = torch.as_tensor(np.asarray(axes.grid.omega_weights, float), device=dev)
@@ -175,7 +180,7 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
     W_minus_I = chi0 if keep else None
     del chi0
     branch = sigma_branch_sums(X, D, Wt, eps_h, nocc, axes.tau_sigma, states, mu, precision,
-                               stream)
+                               stream, err=err)
     sigma = sigma_frequency(branch, axes.C, axes.S, stream)
     if ev:
         ev[3].record()
@@ -184,7 +189,7 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
         # the learned warm start: features from this sweep's Sigma and the
         # states' exchange diagonal, in the sweep's precision
         from .qp_mlp import exchange_diagonal
-        sx = exchange_diagonal(X, D, eps_h, nocc, states, mu, precision=precision)
+        sx = exchange_diagonal(X, D, eps_h, nocc, states, mu, precision=precision, err=err)
         warm = warm.predict_roots(X, D, eps_h, nocc, axes, eps_anchor=anchor, sx=sx,
                                   sweep=SweepResult(sigma=sigma, axes=axes, states=states))
     elif callable(warm):
@@ -199,6 +204,7 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
             timings[name] = ev[k].elapsed_time(ev[k + 1]) / 1e3
         timings['dyson_frequencies'] = axes.grid.nfreq
         timings['ntau'] = axes.ntau
+    err.check('gw_sweep')
     res = SweepResult(roots=roots, z=z, flags=flags, evals=evals, sigma=sigma, axes=axes,
                       states=states, branch=branch, dyson_info=info, e_c=e_c)
     if keep:

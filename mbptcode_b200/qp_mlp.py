@@ -34,13 +34,14 @@ MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'data',
                           'qp_shift_model.npz')
 
 
-def exchange_diagonal(X, D, eps, nocc, states, mu, precision='fp64'):
+def exchange_diagonal(X, D, eps, nocc, states, mu, precision='fp64', err=None):
     """Sigma_x,ii of `states` (device FP64). It depends on X, D and nocc only
     (G_occ(0) = X_o X_o^T carries no orbital energy), so an evGW loop
     computes it once."""
     dev = require_device()
     X, D = to_device(X, dev), to_device(D, dev)
-    br = sigma_branch_sums(X, D, None, eps, nocc, [0.0], states, mu, precision=precision)
+    br = sigma_branch_sums(X, D, None, eps, nocc, [0.0], states, mu, precision=precision,
+                           err=err)
     return -br[0, 0]
 
 

@@ -99,10 +99,11 @@ def _taus(tau_points, tau_indices):
 
 
 def chi0_sweep(X, D, eps, nocc, tau_points, cosft_wt, mu=None, precision=None,
-               want_proj=False, stream=None, out=None):
+               want_proj=False, stream=None, out=None, err=None):
     """(chi0 (nfreq, naux, naux), proj (ntau, naux, naux) or None) as device
     tensors: the whole N^3 sweep in one library call. `out`: a contiguous
-    FP64 device array of chi0's shape to write into."""
+    FP64 device array of chi0's shape to write into. `err`: a device error
+    word the caller checks later (no host sync here); None checks now."""
     dev = require_device()
     Xd, Dd = to_device(X, dev), to_device(D, dev)
     eps_h = _eps_host(eps)
@@ -133,12 +134,14 @@ def chi0_sweep(X, D, eps, nocc, tau_points, cosft_wt, mu=None, precision=None,
             if want_proj else None)
     nbytes = lib().mbpt_chi0_workspace_bytes(M, norb, nocc, naux, ntau, mode)
     ws = WORKSPACE.get(nbytes, dev)
-    err = _Err(dev)
+    own = err is None
+    err = _Err(dev) if own else err
     check(lib().mbpt_chi0_sweep(ptr(Xd), M, norb, nocc, ptr(ed), float(mu), ptr(Dd), naux,
                                 tp, ntau, cp, nfreq, mode, ptr(chi0), ptr(proj), ptr(ws),
                                 ws.numel(), ptr(err.t), stream_ptr(stream)),
           'mbpt_chi0_sweep')
-    err.check('mbpt_chi0_sweep')
+    if own:
+        err.check('mbpt_chi0_sweep')
     return chi0, proj
 
 
@@ -203,7 +206,7 @@ class NonPositiveDielectric(RuntimeWarning):
     """det(1 - chi0) is not positive at an imaginary frequency."""
 
 
-def dyson_batch(chi0, want_w=True, stream=None, precision='fp64'):
+def dyson_batch(chi0, want_w=True, stream=None, precision='fp64', err=None):
     """In place over a device tensor (nfreq, naux, naux): chi0 -> W - I (or
     the Cholesky factors). Returns (logdet, trace, info, sign) with logdet and
     trace on the device and info/sign as host int arrays. The factorisation
@@ -216,7 +219,8 @@ def dyson_batch(chi0, want_w=True, stream=None, precision='fp64'):
     trace = torch.empty(nfreq, dtype=torch.float64, device=dev)
     info = np.zeros(nfreq, dtype=np.int32)
     sign = np.ones(nfreq, dtype=np.int32)
-    err = _Err(dev)
+    own = err is None
+    err = _Err(dev) if own else err
     ws = WORKSPACE.get(lib().mbpt_dyson_workspace_bytes(naux, nfreq, mode), dev)
     import ctypes
     rc = lib().mbpt_dyson(ptr(chi0), naux, nfreq, int(bool(want_w)), mode, ptr(logdet),
@@ -225,7 +229,8 @@ def dyson_batch(chi0, want_w=True, stream=None, precision='fp64'):
                           ptr(err.t), stream_ptr(stream))
     if rc not in (_lib.OK, _lib.ERR_NOT_SPD):
         check(rc, 'mbpt_dyson')
-    err.check('mbpt_dyson')
+    if own:
+        err.check('mbpt_dyson')
     return logdet, trace, info, sign
 
 
