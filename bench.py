@@ -418,7 +418,7 @@ def main():
         'stages_s': {k: round(v, 4) for k, v in stages.items() if k.startswith('t_')},
         'stages_fp64_s': {k: round(v, 4) for k, v in stages_fp64.items() if k.startswith('t_')},
         'accuracy': acc, 'accuracy_other_variant': other, 'qp_warm_start': warm_info,
-        'e2e': {'value': round(e2e_s, 5), 'unit': 's', 'h2d_bytes_per_step': int(h2d),
+        'e2e': {'value': round(e2e_s / world, 5), 'unit': 's', 'h2d_bytes_per_step': int(h2d),
                 'd2h_bytes_per_step': int(d2h)},
         'gpu_launches': int(launches),
         'kernels': kernels,
