@@ -1,5 +1,6 @@
 // Host side of the tcgen05 split GEMM engine: TMA tensor maps and launches.
 #include <cudaTypedefs.h>
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -47,6 +48,20 @@ bool make_tmap(CUtensorMap *m, const void *base, int64_t rows, int64_t cols, int
   return r == CUDA_SUCCESS;
 }
 
+// The dynamic shared-memory opt-in of a kernel, once per device (the
+// attribute belongs to the function on the current device).
+bool allow_smem(const void *kern, int bytes, std::atomic<uint64_t> &done) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  const uint64_t bit = dev < 64 ? (uint64_t{1} << dev) : 0;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return true;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+      cudaSuccess)
+    return false;
+  done.fetch_or(bit, std::memory_order_release);
+  return true;
+}
+
 template <int NACC, int BN, int EPI, bool TF32, int DRAIN>
 int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
            const umma::EpiArgs &e, int *err, cudaStream_t st, int band = 0) {
@@ -75,13 +90,9 @@ int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
   p.epi = e;
   p.err = err;
   auto kern = umma::gemm_split_kernel<NACC, BN, EPI, TF32, DRAIN>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kSmemBytes) !=
-        cudaSuccess)
-      return MBPT_ERR_CUDA;
-    attr_set = true;
-  }
+  static std::atomic<uint64_t> attr_set{0};  // one bit per device
+  if (!allow_smem(reinterpret_cast<const void *>(kern), L::kSmemBytes, attr_set))
+    return MBPT_ERR_CUDA;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   const bool timed = timing_begin(st, &ev0, &ev1);
   count_launch();
@@ -135,13 +146,9 @@ int launch_grouped(const SplitMat &A, const SplitMat &B, const GemmGroup *g, int
   p.epi = e;
   p.err = err;
   auto kern = umma::gemm_split_kernel<1, 128, EPI, true, DRAIN, kMaxGroups>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::kSmemBytes) !=
-        cudaSuccess)
-      return MBPT_ERR_CUDA;
-    attr_set = true;
-  }
+  static std::atomic<uint64_t> attr_set{0};  // one bit per device
+  if (!allow_smem(reinterpret_cast<const void *>(kern), L::kSmemBytes, attr_set))
+    return MBPT_ERR_CUDA;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   const bool timed = timing_begin(st, &ev0, &ev1);
   count_launch();

@@ -22,6 +22,10 @@ synthetic system, for the launch list of the benchmark's workload.
 
 --transform N: one FP64 tau <-> omega transform of 24 N x N matrices with a
 24 x 24 weight matrix (mbpt_transform, the W(i w) -> W(tau) step).
+
+--fp64-peak N: the FP64 reference rates of this GPU, timed with CUDA events
+(best of 5 after a warm-up): cuBLAS DGEMM at N^3 and cuSOLVER's Cholesky of
+an N x N SPD matrix (the FP64 factorisation of the Dyson step).
 """
 from __future__ import annotations
 
@@ -84,6 +88,33 @@ def transform_case(a):
     print(f'transform case n={n} K=J={k}: |out| {float(out.abs().max()):.3e}')
 
 
+def fp64_peak(a):
+    n = a.fp64_peak
+    g = torch.Generator(device='cuda').manual_seed(4)
+    A = torch.randn(n, n, generator=g, device='cuda', dtype=torch.float64)
+    B = torch.randn(n, n, generator=g, device='cuda', dtype=torch.float64)
+    S = A @ A.T / n
+    S.diagonal().add_(1.0)
+
+    def best(fn):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        return min(ts)
+    t_gemm = best(lambda: A @ B)
+    t_chol = best(lambda: torch.linalg.cholesky(S))
+    print(f'fp64 peak case n={n}: DGEMM {2 * n ** 3 / t_gemm / 1e12:.2f} TFLOP/s '
+          f'({t_gemm * 1e3:.3f} ms), Cholesky {n ** 3 / 3 / t_chol / 1e12:.2f} TFLOP/s '
+          f'({t_chol * 1e3:.3f} ms)')
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument('--M', type=int, default=None)
@@ -94,8 +125,11 @@ def main():
     p.add_argument('--nfreq', type=int, default=1)
     p.add_argument('--sweep', action='store_true')
     p.add_argument('--transform', type=int, default=0)
+    p.add_argument('--fp64-peak', type=int, default=0)
     a = p.parse_args()
     torch.cuda.set_device(0)
+    if a.fp64_peak:
+        return fp64_peak(a)
     if a.dyson:
         return dyson(a)
     if a.transform:
