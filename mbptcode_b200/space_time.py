@@ -57,8 +57,12 @@ def check_mixed_weights(precision, *weights):
 
 
 def to_device(a, device, dtype=torch.float64):
+    """`a` on `device` as a contiguous `dtype` tensor. A pinned host tensor is
+    copied asynchronously (stream-ordered before the kernels that read it),
+    so that the host work that follows overlaps the transfer."""
     if isinstance(a, torch.Tensor):
-        return a.to(device=device, dtype=dtype).contiguous()
+        pinned = a.device.type == 'cpu' and a.is_pinned() and a.dtype == dtype
+        return a.to(device=device, dtype=dtype, non_blocking=pinned).contiguous()
     return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=device)
 
 
