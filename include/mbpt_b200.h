@@ -72,6 +72,15 @@ int mbpt_device_supported(int device);
 long long mbpt_launch_count(void);
 int mbpt_gemm_timing(int enable, double *total_ms, long long *launches);
 
+/* Self-test of failure detection (no counterpart in MBPTcode): one thread
+ * waits, with the tensor-core engine's barrier-wait routine, on a
+ * shared-memory mbarrier that it completes first (arrive = 1) or that nothing
+ * completes (arrive = 0). The wait gives up after limit_us microseconds
+ * (1 ... 1e6) and writes MBPT_ERR_TIMEOUT to *err_dev; the kernel then returns
+ * normally, so the context stays usable. The engine's own waits give up the
+ * same way after 4 s. */
+int mbpt_wait_selftest(int arrive, int limit_us, int *err_dev, void *stream);
+
 /* ---- chi0 sweep ---------------------------------------------------------
  * Replaces LinearResponse/space_time.py:607-651 chi0_imaginary_frequency
  * (with :478-530 polarizability_projected_tau per tau point and :533-560

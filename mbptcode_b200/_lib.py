@@ -30,6 +30,7 @@ _SIGNATURES = {
     'mbpt_device_supported': (_i, [_i]),
     'mbpt_launch_count': (C.c_longlong, []),
     'mbpt_gemm_timing': (_i, [_i, _p, _p]),
+    'mbpt_wait_selftest': (_i, [_i, _i, _p, _p]),
     'mbpt_energy_sum': (_i, [_p, _p, _p, _i, _p, _p]),
     'mbpt_chi0_workspace_bytes': (_sz, [_i64, _i64, _i64, _i64, _i, _i]),
     'mbpt_chi0_sweep': (_i, [_p, _i64, _i64, _i64, _p, _d, _p, _i64, _p, _i, _p, _i, _i, _p,

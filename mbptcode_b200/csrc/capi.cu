@@ -854,6 +854,10 @@ const char *mbpt_status_string(int s) {
 
 long long mbpt_launch_count(void) { return g_launches.load(); }
 
+int mbpt_wait_selftest(int arrive, int limit_us, int *err_dev, void *stream) {
+  return wait_selftest(arrive, limit_us, err_dev, S(stream));
+}
+
 int mbpt_gemm_timing(int enable, double *total_ms, long long *launches) {
   return gemm_timing(enable, total_ms, launches);
 }

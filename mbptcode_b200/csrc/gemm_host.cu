@@ -173,6 +173,34 @@ int gemm_split_grouped(int epi, const SplitMat &A, const SplitMat &B, const Gemm
   return MBPT_OK;
 }
 
+// ---- self-test of the engine's bounded barrier wait ----
+namespace {
+// One thread waits, with the engine's wait routine, on a shared-memory
+// mbarrier of arrival count 1 that it first completes itself (arrive) or
+// that nothing completes; a wait that gives up writes MBPT_ERR_TIMEOUT.
+__global__ void wait_selftest_kernel(int arrive, uint64_t limit_ns, int *err) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    umma::mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (arrive)
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(umma::smem_u32(&bar))
+                   : "memory");
+    if (!umma::mbar_wait(&bar, 0, limit_ns)) DevErr{err}.set(MBPT_ERR_TIMEOUT);
+  }
+}
+}  // namespace
+
+int wait_selftest(int arrive, int64_t limit_us, int *err, cudaStream_t st) {
+  if (limit_us < 1 || limit_us > 1000000) return MBPT_ERR_SHAPE;
+  count_launch();
+  wait_selftest_kernel<<<1, 32, 0, st>>>(arrive, static_cast<uint64_t>(limit_us) * 1000u, err);
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
 // ---- optional per-launch timing of the engine (CUDA events on the stream) ----
 namespace {
 struct Timing {

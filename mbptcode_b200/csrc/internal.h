@@ -37,6 +37,10 @@ int gemm_split_grouped(int epi, const SplitMat &A, const SplitMat &B, const Gemm
                        int ngroups, const umma::EpiArgs &e, int *err, cudaStream_t st,
                        int band = 0);
 
+// The engine's bounded barrier wait on a barrier that is (arrive = 1) or is
+// never (arrive = 0) completed, giving up after limit_us microseconds.
+int wait_selftest(int arrive, int64_t limit_us, int *err, cudaStream_t st);
+
 // Per-epilogue totals of the engine's launch times (enable = 1 starts
 // recording; a call with non-null outputs drains, returns and resets them).
 int gemm_timing(int enable, double *total_ms, long long *launches);

@@ -114,14 +114,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *b, uint32_t parity) {
 }
 
 // Bounded wait: false once kWaitLimitNs have passed without the phase flipping.
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity,
+                                          uint64_t limit_ns = kWaitLimitNs) {
   if (mbar_try_wait(b, parity)) return true;
   const uint64_t t0 = global_ns();
   while (true) {
 #pragma unroll 1
     for (int i = 0; i < 64; ++i)
       if (mbar_try_wait(b, parity)) return true;
-    if (global_ns() - t0 > kWaitLimitNs) return false;
+    if (global_ns() - t0 > limit_ns) return false;
   }
 }
 

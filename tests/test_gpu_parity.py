@@ -284,3 +284,33 @@ def test_sigma_branch_sums_identity_w(prec):
     b = gw.sigma_branch_sums(X, D, eye, eps, nocc, taus, states, mu, precision=prec)
     tol = 1e-12 if prec == 'fp64' else MIXED_REL
     assert rel(a.cpu().numpy(), b.cpu().numpy()) < tol
+
+
+def test_bounded_wait_gives_up_and_context_survives(dev):
+    """Failure detection without a fault: a barrier that nothing completes
+    makes the engine's wait routine give up after its limit (20 ms here) and
+    report MBPT_ERR_TIMEOUT through the error word; the kernel returns, and
+    the same context then runs a tensor-core product correctly."""
+    lib = _lib.lib()
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.check(lib.mbpt_wait_selftest(0, 20000, _lib.ptr(err), _lib.stream_ptr()), 'selftest')
+    torch.cuda.synchronize()
+    assert int(err.item()) == _lib.ERR_TIMEOUT
+    err.zero_()
+    _lib.check(lib.mbpt_wait_selftest(1, 20000, _lib.ptr(err), _lib.stream_ptr()), 'selftest')
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert lib.mbpt_wait_selftest(0, 0, _lib.ptr(err), _lib.stream_ptr()) == _lib.ERR_SHAPE
+    # the context still works
+    rng = np.random.default_rng(3)
+    A, B = rng.standard_normal((200, 96)), rng.standard_normal((150, 96))
+    C = torch.empty((200, 150), dtype=torch.float32, device=dev)
+    ws = torch.empty(lib.mbpt_gemm_split_workspace_bytes(200, 150, 96), dtype=torch.uint8,
+                     device=dev)
+    _lib.check(lib.mbpt_gemm_split(_lib.ptr(torch.as_tensor(A, device=dev)),
+                                   _lib.ptr(torch.as_tensor(B, device=dev)), 200, 150, 96, 1.0,
+                                   _lib.ptr(C), 150, _lib.ptr(ws), ws.numel(), _lib.ptr(err),
+                                   _lib.stream_ptr()), 'gemm')
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert np.abs(C.cpu().numpy() - A @ B.T).max() < 3e-5 * np.sqrt(96) * 16
