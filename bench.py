@@ -36,6 +36,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -141,8 +142,10 @@ class Clocks:
     `window` marking the timed region; only samples inside it are kept."""
 
     def __init__(self, index):
-        self.path = os.path.join(ROOT, 'gpurun_out', f'clocks_{index}.csv')
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        # the samples go to a temporary file unless MBPT_CLOCKS_CSV names one
+        self.path = os.environ.get('MBPT_CLOCKS_CSV') or os.path.join(
+            tempfile.mkdtemp(prefix='mbpt_clocks_'), f'clocks_{index}.csv')
+        os.makedirs(os.path.dirname(os.path.abspath(self.path)), exist_ok=True)
         self.t0 = self.t1 = None
         q = ('timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
@@ -318,7 +321,7 @@ def main():
     torch.cuda.synchronize()
     ms_fp64 = max_over_ranks(f0.elapsed_time(f1) / nf)
     acc = accuracy(res_mixed, res_fp64)
-    # the warm start judged by the plain scan on the same (mixed) Sigma
+    # the warm start checked against the plain scan on the same (mixed) Sigma
     r_plain, _, _, e_plain = qp_solve(res_mixed['sigma'], axes.pade_freq, eps, states, NOCC,
                                       axes.mu)
     ok = torch.isfinite(r_plain) & torch.isfinite(res_mixed['roots'])

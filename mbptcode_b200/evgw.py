@@ -64,16 +64,16 @@ class DIIS:
 
 def evgw_eigenvalues(X, D, eps0, nocc, ntau='auto', tol=EVGW_TOL, max_cycle=EVGW_MAX_CYCLE,
                      diis_size=EVGW_DIIS_SIZE, diis_start=EVGW_DIIS_START, precision=None,
-                     warm=None, eps_init=None, verbose=False, judge=False):
+                     warm=None, eps_init=None, verbose=False, verify=False):
     """(eps, info): the evGW spectrum (Hartree, host array) of the system
     (X, D, eps0). info: cycles, converged, history (max |d eps| over HOMO and
     LUMO per cycle), sigma_evaluations per cycle, warm_accepted per cycle.
 
     warm: 'previous' (the last cycle's roots) or a model with predict_roots
     (the learned warm start; the states' exchange diagonal, independent of
-    the orbital energies, is computed once). judge: with a warm start, also
+    the orbital energies, is computed once). verify: with a warm start, also
     solve every cycle's equations plainly (the graphical scan, on the same
-    Sigma) and record in info['judge_max_diff'] the largest root difference
+    Sigma) and record in info['verify_max_diff'] the largest root difference
     per cycle; those plain solves are not counted in sigma_evaluations."""
     eps0 = _eps_host(eps0)
     n = len(eps0)
@@ -83,7 +83,7 @@ def evgw_eigenvalues(X, D, eps0, nocc, ntau='auto', tol=EVGW_TOL, max_cycle=EVGW
     tested = [nocc - 1, nocc]
     eps = eps0.copy() if eps_init is None else np.asarray(eps_init, float).copy()
     acc = DIIS(diis_size, diis_start) if diis_size else None
-    history, evals, accepted, judged = [], [], [], []
+    history, evals, accepted, verified = [], [], [], []
     converged = False
     prev = None
     sx = None
@@ -105,12 +105,12 @@ def evgw_eigenvalues(X, D, eps0, nocc, ntau='auto', tol=EVGW_TOL, max_cycle=EVGW
                        eps_anchor=eps0, warm=w)
         eps_new = res['roots'].cpu().numpy()
         flags = res['flags'].cpu().numpy()
-        if judge and w is not None:
+        if verify and w is not None:
             from .gw import qp_solve
             r_plain = qp_solve(res['sigma'], axes.pade_freq, eps0, res['states'], nocc,
                                axes.mu)[0].cpu().numpy()
             ok = np.isfinite(r_plain) & np.isfinite(eps_new)
-            judged.append(float(np.abs(r_plain - eps_new)[ok].max()) if ok.any() else 0.0)
+            verified.append(float(np.abs(r_plain - eps_new)[ok].max()) if ok.any() else 0.0)
         evals.append(int(res['evals'].sum().item()))
         accepted.append(int(((flags & 16) != 0).sum()))
         prev = res['roots']
@@ -130,5 +130,5 @@ def evgw_eigenvalues(X, D, eps0, nocc, ntau='auto', tol=EVGW_TOL, max_cycle=EVGW
                       stacklevel=2)
     return eps, {'cycles': len(history), 'converged': converged, 'history': history,
                  'sigma_evaluations': evals, 'warm_accepted': accepted,
-                 'judge_max_diff': judged,
+                 'verify_max_diff': verified,
                  'eps_mean_field': eps0, 'shift': eps - eps0}

@@ -14,8 +14,8 @@ Evaluation: `--eval` further systems, each solved by the evGW loop
 every state) and warm-started (the network's roots seed the kernel's Newton
 solve; the scan stays the fallback for any state whose Newton solve is not
 accepted). Reported: Sigma evaluations of both runs and the fraction of warm
-starts accepted; the QP error of the warm start, judged every cycle by the
-plain scan on the same Sigma (meV); and a G0W0 comparison of the same
+starts accepted; the QP error of the warm start, checked every cycle against
+the plain scan on the same Sigma (meV); and a G0W0 comparison of the same
 systems. The two runs' final spectra are reported too, next to the spread
 that a 1e-11 Ha change of the mean-field energies alone causes in the plain
 loop: far from the gap the evGW fixed point selects between near-equal QP
@@ -112,7 +112,7 @@ def main(argv=None):
         e_p, info_p = evgw_eigenvalues(X, D, eps, nocc, ntau=a.ntau, precision=a.precision)
         tw = time.perf_counter()
         e_w, info_w = evgw_eigenvalues(X, D, eps, nocc, ntau=a.ntau, precision=a.precision,
-                                       warm=model, judge=True)
+                                       warm=model, verify=True)
         te = time.perf_counter()
         e_q, _ = evgw_eigenvalues(X, D, eps + 1e-11, nocc, ntau=a.ntau, precision=a.precision)
         ok = np.isfinite(e_p) & np.isfinite(e_w)
@@ -127,7 +127,7 @@ def main(argv=None):
             'states_solved': int(n) * info_w['cycles'],
             'max_diff_meV': float(np.abs(e_w - e_p)[ok].max() * HARTREE_MEV),
             'frontier_max_diff_meV': float(np.abs(e_w - e_p)[f].max() * HARTREE_MEV),
-            'judge_max_diff_meV': max(info_w['judge_max_diff'], default=0.0) * HARTREE_MEV,
+            'verified_max_diff_meV': max(info_w['verify_max_diff'], default=0.0) * HARTREE_MEV,
             'perturbed_max_diff_meV': float(np.abs(e_q - e_p)[okq].max() * HARTREE_MEV),
             'perturbed_frontier_max_diff_meV': float(np.abs(e_q - e_p)[f].max() * HARTREE_MEV),
             's_plain': tw - tp, 's_warm': te - tw})
@@ -154,7 +154,7 @@ def main(argv=None):
         'evgw': {'evals_plain': tot(evgw, 'evals_plain'), 'evals_warm': tot(evgw, 'evals_warm'),
                  'saved_frac': 1 - tot(evgw, 'evals_warm') / max(1, tot(evgw, 'evals_plain')),
                  'accepted_frac': tot(evgw, 'warm_accepted') / max(1, tot(evgw, 'states_solved')),
-                 'judge_max_diff_meV': max(r['judge_max_diff_meV'] for r in evgw),
+                 'verified_max_diff_meV': max(r['verified_max_diff_meV'] for r in evgw),
                  'final_max_diff_meV': max(r['max_diff_meV'] for r in evgw),
                  'final_frontier_max_diff_meV': max(r['frontier_max_diff_meV'] for r in evgw),
                  'perturbed_final_max_diff_meV': max(r['perturbed_max_diff_meV'] for r in evgw),

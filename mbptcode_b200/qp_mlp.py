@@ -4,7 +4,7 @@ A 4 -> H -> H -> 1 perceptron (SiLU, FP32) predicts each orbital's QP shift
 w - eps_i from (eps_i, Sigma_x,ii, Re Sigma_c,ii(eps_i - 0.1), Re Sigma_c,ii(eps_i + 0.1))
 (Hartree). The prediction seeds a safeguarded Newton solve in the QP kernel;
 the plain graphical scan (MBPTcode ``Solvers/qp_equation.py:1353-1393``)
-remains the fallback and the judge of the prediction.
+remains the fallback and the check of the prediction.
 
 Features: Sigma_x,ii = -sum_PQ X_Pi (G_occ(0) o V)_PQ X_Qi with
 G_occ(0) = X_o X_o^T and V = D D^T, the exchange of the ISDF factors (the

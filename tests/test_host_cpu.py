@@ -108,7 +108,7 @@ def test_plugin_rebinds_and_restores_reference_names():
         bound, skipped = plugin.install()
         assert lr.chi0_imaginary_frequency is space_time.chi0_imaginary_frequency
         assert 'dyson_screening' in bound[plugin.IT]
-        assert plugin.ST in skipped      # the driver imports pyscf, absent here
+        assert plugin.ST in skipped      # MBPTcode's GW module imports pyscf, absent here
         adj = importlib.import_module(plugin.ADJ)
         assert adj.rpa_correlation_energy_space_time is \
             space_time.rpa_correlation_energy_space_time
