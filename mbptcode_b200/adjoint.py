@@ -37,7 +37,8 @@ def chi0_backward(proj_bar, X, D, eps, nocc, tau_points, mu, precision='fp64', s
     D_bar = torch.empty((M, naux), dtype=torch.float64, device=dev)
     ws = WORKSPACE.get(lib().mbpt_chi0_backward_workspace_bytes(M, norb, nocc, naux, mode), dev)
     err = _Err(dev)
-    check(lib().mbpt_chi0_backward(ptr(proj_bar.contiguous()), ptr(Xd), M, norb, nocc, ptr(ed),
+    pb = proj_bar.contiguous()  # held until the call has launched its kernels
+    check(lib().mbpt_chi0_backward(ptr(pb), ptr(Xd), M, norb, nocc, ptr(ed),
                                    float(mu), ptr(Dd), naux, tp, len(tau_h), mode,
                                    ptr(eps_bar), ptr(X_bar), ptr(D_bar), ptr(ws), ws.numel(),
                                    ptr(err.t), stream_ptr(stream)), 'mbpt_chi0_backward')

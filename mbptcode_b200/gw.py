@@ -60,8 +60,9 @@ def sigma_branch_sums(X, D, Wt, eps, nocc, tau_points, states, mu, precision=Non
     ws = WORKSPACE.get(lib().mbpt_sigma_workspace_bytes(M, norb, nocc, naux, ntau, S, mode), dev)
     own = err is None
     err = _Err(dev) if own else err
+    Wc = None if Wt is None else Wt.contiguous()  # held until the kernels are launched
     check(lib().mbpt_sigma_branch_sums(ptr(Xd), M, norb, nocc, ptr(ed), float(mu), ptr(Dd),
-                                       naux, ptr(None if Wt is None else Wt.contiguous()), tp,
+                                       naux, ptr(Wc), tp,
                                        ntau, ptr(st), S, mode,
                                        ptr(branch), ptr(ws), ws.numel(), ptr(err.t),
                                        stream_ptr(stream)), 'mbpt_sigma_branch_sums')
@@ -79,7 +80,8 @@ def sigma_frequency(branch, C, S, stream=None):
     Sd = torch.as_tensor(np.ascontiguousarray(S, dtype=np.float64), device=dev)
     npade = Cd.shape[0]
     out = torch.empty((nstates, npade, 2), dtype=torch.float64, device=dev)
-    check(lib().mbpt_sigma_frequency(ptr(branch.contiguous()), ntau, nstates, ptr(Cd), ptr(Sd),
+    bc = branch.contiguous()  # held until the call has launched its kernel
+    check(lib().mbpt_sigma_frequency(ptr(bc), ntau, nstates, ptr(Cd), ptr(Sd),
                                      npade, ptr(out), stream_ptr(stream)),
           'mbpt_sigma_frequency')
     return torch.view_as_complex(out)

@@ -350,7 +350,8 @@ def transform(values, weights, stream=None, out=None):
         out = torch.empty((J, n, n), dtype=torch.float64, device=dev)
     elif tuple(out.shape) != (J, n, n) or out.dtype != torch.float64 or not out.is_contiguous():
         raise ValueError(f'out must be a contiguous FP64 ({J}, {n}, {n}) array')
-    check(lib().mbpt_transform(ptr(values.contiguous()), K, n, ptr(w), J, ptr(out),
+    vc = values.contiguous()  # held until the call has launched its kernel
+    check(lib().mbpt_transform(ptr(vc), K, n, ptr(w), J, ptr(out),
                                stream_ptr(stream)), 'mbpt_transform')
     return out
 

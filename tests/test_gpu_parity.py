@@ -307,8 +307,8 @@ def test_bounded_wait_gives_up_and_context_survives(dev):
     C = torch.empty((200, 150), dtype=torch.float32, device=dev)
     ws = torch.empty(lib.mbpt_gemm_split_workspace_bytes(200, 150, 96), dtype=torch.uint8,
                      device=dev)
-    _lib.check(lib.mbpt_gemm_split(_lib.ptr(torch.as_tensor(A, device=dev)),
-                                   _lib.ptr(torch.as_tensor(B, device=dev)), 200, 150, 96, 1.0,
+    Ad, Bd = torch.as_tensor(A, device=dev), torch.as_tensor(B, device=dev)  # kept alive
+    _lib.check(lib.mbpt_gemm_split(_lib.ptr(Ad), _lib.ptr(Bd), 200, 150, 96, 1.0,
                                    _lib.ptr(C), 150, _lib.ptr(ws), ws.numel(), _lib.ptr(err),
                                    _lib.stream_ptr()), 'gemm')
     torch.cuda.synchronize()
