@@ -107,3 +107,21 @@ def test_c1_adjoint_central_differences():
         rich.append(abs(r - ad) / abs(ad))
     assert max(plain) < 1e-4, plain
     assert max(rich) < 1e-6, rich
+
+
+def test_c1_mixed_within_the_precision_bars():
+    """Mixed precision against FP64 on the calibrated C1 tensors with the
+    regularised 20-point grid (mixed refuses the 16-point weights): the 20
+    HOMO/LUMO-region QP energies within 10 meV and E_c within 1 uHa per
+    electron. At N_mu = 2400 this runs the 128 x 256 products over an
+    overhanging last column tile (2432 = 9.5 x 256), the upper-tile products
+    over 19 x 19 tiles and a four-level grouped Dyson recursion."""
+    X, D, eps = synthetic_system(N, NOCC, M, SEED, 'calibrated')
+    Xd, Dd = torch.as_tensor(X, device='cuda'), torch.as_tensor(D, device='cuda')
+    axes = grids.space_time_axes(eps, NOCC, ntau=20)
+    res = {p: gw.gw_sweep(Xd, Dd, eps, NOCC, axes=axes, precision=p) for p in ('fp64', 'mixed')}
+    f = np.arange(NOCC - 10, NOCC + 10)
+    r64, rmx = (res[p]['roots'].cpu().numpy() for p in ('fp64', 'mixed'))
+    assert np.abs(rmx[f] - r64[f]).max() < 10e-3 / 27.211386
+    e64, emx = (float(res[p]['e_c']) for p in ('fp64', 'mixed'))
+    assert abs(emx - e64) < 1e-6 * 2 * NOCC
