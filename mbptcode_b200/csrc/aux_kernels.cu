@@ -145,34 +145,43 @@ __global__ void zero_strict_upper_cm_kernel(double *a, int64_t n) {
 // With c_hi set, the inverted blocks go out as TF32 pairs instead, in two
 // layouts of the padded (ldp) pair arrays: rows of L^-1 (r_*) and columns of
 // L^-1 as rows (c_*), zeros above the diagonal included; A keeps the factor.
+// The row recursion's dot products are split over kDiagParts threads per
+// column (partial sums combined by warp shuffles), and the block is stored
+// with a padded row stride so the parts' reads fall in different banks.
+constexpr int kDiagParts = 4;
+
 __global__ void trtri_diag_blocks_kernel(double *A, int64_t n, int64_t lda, int nb, float *c_hi,
                                          float *c_lo, float *r_hi, float *r_lo, int64_t ldp) {
-  extern __shared__ double s[];  // m x m row-major block, then one row of L
+  extern __shared__ double s[];  // m x m row-major block (stride m + 1), then one row of L
   const int64_t off = static_cast<int64_t>(blockIdx.x) * nb;
   const int m = static_cast<int>(min(static_cast<int64_t>(nb), n - off));
-  double *row = s + m * m;
+  const int ls = m + 1;
+  double *row = s + m * ls;
   for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
     const int r = idx / m, c = idx % m;
-    s[idx] = r >= c ? A[(off + c) * lda + off + r] : 0.0;
+    s[r * ls + c] = r >= c ? A[(off + c) * lda + off + r] : 0.0;
   }
   __syncthreads();
+  const int j = threadIdx.x / kDiagParts, part = threadIdx.x % kDiagParts;
   for (int i = 0; i < m; ++i) {
-    for (int k = threadIdx.x; k <= i; k += blockDim.x) row[k] = s[i * m + k];
+    for (int k = threadIdx.x; k <= i; k += blockDim.x) row[k] = s[i * ls + k];
     __syncthreads();
     const double inv = 1.0 / row[i];
     // row i of L^-1: (L^-1)_ij = -(sum_{j<=k<i} L_ik (L^-1)_kj) / L_ii
-    for (int j = threadIdx.x; j <= i; j += blockDim.x) {
-      double acc = 0.0;
-      for (int k = j; k < i; ++k) acc = fma(row[k], s[k * m + j], acc);
-      s[i * m + j] = j == i ? inv : -acc * inv;
-    }
+    double acc = 0.0;
+    if (j < i)
+      for (int k = j + part; k < i; k += kDiagParts) acc = fma(row[k], s[k * ls + j], acc);
+#pragma unroll
+    for (int d = 1; d < kDiagParts; d <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, d);
+    if (part == 0 && j <= i) s[i * ls + j] = j == i ? inv : -acc * inv;
     __syncthreads();
   }
   if (c_hi) {
     for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
       const int r = idx / m, c = idx % m;
-      const float h = to_tf32(static_cast<float>(s[idx]));
-      const float l = to_tf32(static_cast<float>(s[idx] - static_cast<double>(h)));
+      const double x = s[r * ls + c];
+      const float h = to_tf32(static_cast<float>(x));
+      const float l = to_tf32(static_cast<float>(x - static_cast<double>(h)));
       r_hi[(off + r) * ldp + off + c] = h;
       r_lo[(off + r) * ldp + off + c] = l;
       c_hi[(off + c) * ldp + off + r] = h;
@@ -182,7 +191,7 @@ __global__ void trtri_diag_blocks_kernel(double *A, int64_t n, int64_t lda, int 
   }
   for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
     const int r = idx / m, c = idx % m;
-    if (r >= c) A[(off + c) * lda + off + r] = s[idx];
+    if (r >= c) A[(off + c) * lda + off + r] = s[r * ls + c];
   }
 }
 
@@ -215,24 +224,6 @@ __global__ void strided_to_tf32_kernel(const double *__restrict__ src, int64_t r
       hi[r * k_p + c] = h;
       lo[r * k_p + c] = to_tf32(static_cast<float>(x - static_cast<double>(h)));
     }
-  }
-}
-
-// C(i, j) (column-major, ldc) = alpha P[j * ldp + i] + beta C(i, j) - shift [i == j]
-// for i < m, j < n: the FP64 store of an engine product P = C^T (row-major FP32).
-// upper: P is symmetric and only its 128 x 128 tiles on and above the
-// diagonal were formed; entries below are read from their mirror.
-__global__ void combine_kernel(const float *P, int64_t ldp, double *C, int64_t ldc, int64_t m,
-                               int64_t n, double alpha, double beta, double shift, bool upper) {
-  const int64_t total = m * n;
-  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
-       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t j = t / m, i = t % m;
-    const bool mirror = upper && (j >> 7) > (i >> 7);
-    double v = alpha * static_cast<double>(mirror ? P[i * ldp + j] : P[j * ldp + i]);
-    if (beta != 0.0) v += beta * C[j * ldc + i];
-    if (i == j) v -= shift;
-    C[j * ldc + i] = v;
   }
 }
 
@@ -293,14 +284,15 @@ void launch_zero_strict_upper_cm(double *a, int64_t n, cudaStream_t st) {
 
 int launch_trtri_diag_blocks(double *A, int64_t n, int64_t lda, int nb, cudaStream_t st,
                              float *c_hi, float *c_lo, float *r_hi, float *r_lo, int64_t ldp) {
-  const size_t smem = sizeof(double) * (static_cast<size_t>(nb) * nb + nb);
+  if (nb < 1 || nb > 128) return MBPT_ERR_SHAPE;  // one thread group of kDiagParts per column
+  const size_t smem = sizeof(double) * (static_cast<size_t>(nb) * (nb + 1) + nb);
   // the attribute is per device, so it is set on every call (a host-side write)
   if (cudaFuncSetAttribute(trtri_diag_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(smem)) != cudaSuccess)
     return MBPT_ERR_CUDA;
   count_launch();
-  trtri_diag_blocks_kernel<<<static_cast<unsigned>((n + nb - 1) / nb), 128, smem, st>>>(
-      A, n, lda, nb, c_hi, c_lo, r_hi, r_lo, ldp);
+  trtri_diag_blocks_kernel<<<static_cast<unsigned>((n + nb - 1) / nb), nb * kDiagParts, smem,
+                             st>>>(A, n, lda, nb, c_hi, c_lo, r_hi, r_lo, ldp);
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 
@@ -310,13 +302,6 @@ void launch_strided_to_tf32(const double *src, int64_t rows, int64_t k, int64_t 
   dim3 grid(static_cast<unsigned>((k_p + 31) / 32), static_cast<unsigned>((rows_p + 31) / 32));
   strided_to_tf32_kernel<<<grid, dim3(32, 8), 0, st>>>(src, rows, k, rs, cs, hi, lo, rows_p,
                                                        k_p);
-}
-
-void launch_combine(const float *P, int64_t ldp, double *C, int64_t ldc, int64_t m, int64_t n,
-                    double alpha, double beta, double shift, bool upper, cudaStream_t st) {
-  count_launch();
-  combine_kernel<<<blocks(m * n), 256, 0, st>>>(P, ldp, C, ldc, m, n, alpha, beta, shift,
-                                                upper);
 }
 
 void launch_identity(double *a, int64_t n, cudaStream_t st) {

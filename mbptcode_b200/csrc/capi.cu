@@ -41,8 +41,6 @@ int launch_trtri_diag_blocks(double *A, int64_t n, int64_t lda, int nb, cudaStre
                              float *r_lo = nullptr, int64_t ldp = 0);
 void launch_strided_to_tf32(const double *src, int64_t rows, int64_t k, int64_t rs, int64_t cs,
                             float *hi, float *lo, int64_t rows_p, int64_t k_p, cudaStream_t st);
-void launch_combine(const float *P, int64_t ldp, double *C, int64_t ldc, int64_t m, int64_t n,
-                    double alpha, double beta, double shift, bool upper, cudaStream_t st);
 
 namespace {
 std::atomic<long long> g_launches{0};
@@ -234,11 +232,10 @@ constexpr int64_t kTrtriLeaf = 128;
 //   LR: rows of the factor L (row i along k);
 //   IC: columns of L^-1 as rows, IC(j, k) = L^-1(k, j);
 //   IR: rows of L^-1, IR(i, k) = L^-1(i, k);
-//   TT: one product's T^T between the two products of a recursion node;
-//   P:  FP32 W = L^-T L^-1 before its FP64 store.
+//   TT: one product's T^T between the two products of a recursion node.
 struct PairScratch {
   float *lr_hi = nullptr, *lr_lo = nullptr, *ic_hi = nullptr, *ic_lo = nullptr;
-  float *ir_hi = nullptr, *ir_lo = nullptr, *tt_hi = nullptr, *tt_lo = nullptr, *p = nullptr;
+  float *ir_hi = nullptr, *ir_lo = nullptr, *tt_hi = nullptr, *tt_lo = nullptr;
   int64_t np = 0;
 };
 
@@ -357,15 +354,19 @@ int spd_inverse_from_factor(Handles &h, double *L, int64_t n, double *T, double 
     if (rc) return rc;
     rc = trtri_pairs(s, n, err, st);
     if (rc) return rc;
+    // W - I straight into the factor's buffer as FP64 (row-major W(j, i) is
+    // the column-major W(i, j) the caller expects; W is symmetric anyway),
+    // tiles above the diagonal mirrored by the epilogue
     SplitMat Ae{s.ic_hi, s.ic_lo, np, kp, np, true};
     umma::EpiArgs e;
-    e.outf = s.p;
-    e.ld_outf = np;
+    e.outd = L;
+    e.ld_outd = n;
+    e.nd = static_cast<int>(n);
+    e.shift = 1.0;
     e.alpha = 1.f;
-    rc = gemm_split(umma::EPI_F32, 1, &Ae, &Ae, np, np, e, err, st,
+    rc = gemm_split(umma::EPI_F64_SYM, 1, &Ae, &Ae, np, np, e, err, st,
                     umma::BAND_K_FROM_M | umma::BAND_K_FROM_N | umma::BAND_UPPER);
     if (rc) return rc;
-    launch_combine(s.p, np, L, n, n, n, 1.0, 0.0, 1.0, true, st);
     *full = true;
     return MBPT_OK;
   }
@@ -443,7 +444,7 @@ DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq, int mode = MBPT_MODE_FP64
     PairScratch &q = b.pairs;
     q.np = np;
     for (float **f : {&q.lr_hi, &q.lr_lo, &q.ic_hi, &q.ic_lo, &q.ir_hi, &q.ir_lo, &q.tt_hi,
-                      &q.tt_lo, &q.p})
+                      &q.tt_lo})
       *f = ar.take<float>(cap);
   }
   return b;

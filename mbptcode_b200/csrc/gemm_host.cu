@@ -300,12 +300,14 @@ int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t 
   if (band) {
     // triangular K spans: the single drained FP32-store TF32 product only (its
     // spans are never empty for the operand shapes the flags describe)
-    if (!tf || nacc != 1 || (epi != EPI_F32 && epi != EPI_TF32_PAIR))
+    if (!tf || nacc != 1 || (epi != EPI_F32 && epi != EPI_TF32_PAIR && epi != EPI_F64_SYM))
       return MBPT_ERR_UNSUPPORTED;
     if ((band & BAND_UPPER) && m_rows != n_rows) return MBPT_ERR_SHAPE;
     if (epi == EPI_TF32_PAIR)
       return launch<1, 128, EPI_TF32_PAIR, true, kDrain>(A, B, m_rows, n_rows, e, err, st,
                                                          band);
+    if (epi == EPI_F64_SYM)
+      return launch<1, 128, EPI_F64_SYM, true, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
     return launch<1, 128, EPI_F32, true, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
   }
   if (tf) {

@@ -30,6 +30,8 @@ enum Epi : int {
   EPI_ROWDOT2 = 4,         // sig0[c] += sum_r xs[r,c] acc0[r,c], sig1[c] -= ... acc1
   EPI_F32_ACC = 5,         // outf += alpha * acc0, FP32 read-modify-write
   EPI_TF32_PAIR = 6,       // alpha * acc0 as a TF32 hi/lo pair at p (and transposed at t)
+  EPI_F64_SYM = 7,         // outd = alpha * acc0 - shift [row == col], FP64, rows and
+                           // columns below nd, mirrored (with BAND_UPPER)
 };
 
 struct EpiArgs {
@@ -45,6 +47,11 @@ struct EpiArgs {
   // transposed pair t (element (r, c) of the tile grid at t[c * ld_t + r])
   float *p_hi = nullptr, *p_lo = nullptr, *t_hi = nullptr, *t_lo = nullptr;
   int64_t ld_p = 0, ld_t = 0;
+  // EPI_F64_SYM: the nd x nd FP64 output (leading dimension ld_outd)
+  double *outd = nullptr;
+  int64_t ld_outd = 0;
+  int nd = 0;
+  double shift = 0.0;
 };
 
 // Structure of triangular operands, for products whose rows vanish on one
@@ -553,6 +560,19 @@ __global__ void __launch_bounds__(64 + BN, 1)
 #pragma unroll
               for (int i = 0; i < 32; ++i)
                 e.outf[static_cast<int64_t>(col + i) * e.ld_outf + row] = e.alpha * v0[i];
+            }
+          }
+        } else if constexpr (EPI == EPI_F64_SYM) {
+          if (row < e.nd) {
+            double *dst = e.outd + static_cast<int64_t>(row) * e.ld_outd + col;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+              if (col + i < e.nd) {
+                const double v = static_cast<double>(e.alpha * v0[i]) -
+                                 (row == col + i ? e.shift : 0.0);
+                dst[i] = v;
+                if (mirror) e.outd[static_cast<int64_t>(col + i) * e.ld_outd + row] = v;
+              }
             }
           }
         } else if constexpr (EPI == EPI_TF32_PAIR) {
