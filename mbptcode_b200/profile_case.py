@@ -23,6 +23,12 @@ synthetic system, for the launch list of the benchmark's workload.
 --transform N: one FP64 tau <-> omega transform of 24 N x N matrices with a
 24 x 24 weight matrix (mbpt_transform, the W(i w) -> W(tau) step).
 
+--qp-mlp: the latency-bound kernels of the QP solve and the learned warm
+start on a C1-sized system (n_orb = 400, N_mu = 2400, 20 points, mixed): one
+sweep, the plain and the warm-started Pade + QP kernels and the Pade
+evaluation of the features, then 5 training steps of the 4 -> 64 -> 64 -> 1
+network on 65536 samples (forward, backward, AdamW).
+
 --fp64-peak N: the FP64 reference rates of this GPU, timed with CUDA events
 (best of 5 after a warm-up): cuBLAS DGEMM at N^3 and cuSOLVER's Cholesky of
 an N x N SPD matrix (the FP64 factorisation of the Dyson step).
@@ -115,6 +121,24 @@ def fp64_peak(a):
           f'({t_chol * 1e3:.3f} ms)')
 
 
+def qp_mlp_case(a):
+    from .gw import qp_solve
+    from .qp_mlp import MODEL_PATH, QPShiftModel, features
+    X, D, eps_t = synthetic_system_torch(400, 40, 2400, seed=5, variant='calibrated')
+    eps = eps_t.cpu().numpy()
+    axes = grids.space_time_axes(eps, 40, ntau=20)
+    res = gw_sweep(X, D, eps, 40, axes=axes, precision='mixed')
+    model = QPShiftModel.load(MODEL_PATH)
+    warm = model.predict_roots(X, D, eps, 40, axes, sweep=res)
+    r = qp_solve(res['sigma'], axes.pade_freq, eps, res['states'], 40, axes.mu, warm=warm)
+    x = features(X, D, eps, 40, res)
+    xs = x.repeat(int(np.ceil(65536 / x.shape[0])), 1)[:65536].contiguous()
+    ys = torch.zeros(65536, dtype=torch.float32, device=xs.device)
+    model.fit(xs, ys, steps=5, batch=65536)
+    torch.cuda.synchronize()
+    print(f'qp/mlp case: warm accepted {int(((r[2] & 16) != 0).sum().item())} of 400')
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument('--M', type=int, default=None)
@@ -126,8 +150,11 @@ def main():
     p.add_argument('--sweep', action='store_true')
     p.add_argument('--transform', type=int, default=0)
     p.add_argument('--fp64-peak', type=int, default=0)
+    p.add_argument('--qp-mlp', action='store_true')
     a = p.parse_args()
     torch.cuda.set_device(0)
+    if a.qp_mlp:
+        return qp_mlp_case(a)
     if a.fp64_peak:
         return fp64_peak(a)
     if a.dyson:
