@@ -100,14 +100,19 @@ def check(status, where):
     return status
 
 
+_SUPPORTED = set()  # device indices already checked
+
+
 def require_device(device=None):
     """The CUDA device the route runs on: an sm_100 part, else an error."""
     if not torch.cuda.is_available():
         raise RuntimeError('mbptcode_b200 needs a CUDA device (sm_100a); none is visible')
     dev = torch.device('cuda', torch.cuda.current_device() if device is None else device)
-    if not lib().mbpt_device_supported(dev.index):
-        raise RuntimeError(f'{torch.cuda.get_device_name(dev)} is not an sm_100 device; '
-                           f'libmbpt_b200 is built for sm_100a only')
+    if dev.index not in _SUPPORTED:
+        if not lib().mbpt_device_supported(dev.index):
+            raise RuntimeError(f'{torch.cuda.get_device_name(dev)} is not an sm_100 device; '
+                               f'libmbpt_b200 is built for sm_100a only')
+        _SUPPORTED.add(dev.index)
     return dev
 
 

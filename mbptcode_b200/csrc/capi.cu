@@ -871,9 +871,12 @@ int mbpt_energy_sum(const double *logdet, const double *trace, const double *w, 
 }
 
 int mbpt_device_supported(int device) {
-  cudaDeviceProp p;
-  if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return 0;
-  return p.major == 10 && p.minor == 0 ? 1 : 0;
+  // two attributes, not cudaGetDeviceProperties (which takes milliseconds)
+  int major = 0, minor = 0;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess ||
+      cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device) != cudaSuccess)
+    return 0;
+  return major == 10 && minor == 0 ? 1 : 0;
 }
 
 size_t mbpt_chi0_workspace_bytes(int64_t M, int64_t norb, int64_t nocc, int64_t naux, int ntau,
