@@ -7,6 +7,7 @@
 
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <algorithm>
@@ -412,6 +413,7 @@ struct DysonBufs {
   int *info;
   int *piv;
   double *work;
+  double *work2;  // the second factor stream's cuSOLVER workspace
   double *rhs;   // n x n right-hand side of the LU inverse of a failed frequency
   double *diag;  // nfreq x n diagonals of 1 - chi0, which the factorisation overwrites
   double *T;     // diagonal-block scratch of the LAUUM
@@ -436,6 +438,7 @@ DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq, int mode = MBPT_MODE_FP64
   b.info = ar.take<int>(nfreq + 1);
   b.piv = ar.take<int>(n);
   b.work = ar.take<double>(b.lwork > 0 ? b.lwork : 1);
+  b.work2 = ar.take<double>(b.lwork > 0 ? b.lwork : 1);
   b.rhs = ar.take<double>(n * n);
   b.diag = ar.take<double>(n * static_cast<int64_t>(nfreq));
   b.T = ar.take<double>(kLauumBlock * kLauumBlock);
@@ -457,6 +460,13 @@ DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq, int mode = MBPT_MODE_FP64
 struct DysonPipe {
   cudaStream_t side = nullptr;
   cudaEvent_t join = nullptr;
+  // second factor stream: odd frequencies factorise there with their own
+  // cuSOLVER handle, so that two Cholesky factorisations (latency-bound
+  // panels between DGEMM-bound updates) share the GPU
+  cudaStream_t fac2 = nullptr;
+  cusolverDnHandle_t solver2 = nullptr;
+  cudaEvent_t fork = nullptr, join2 = nullptr;
+  int nfac = 1;
   std::vector<cudaEvent_t> ev;
   int *info = nullptr;  // pinned host, `cap` ints
   int cap = 0;
@@ -475,6 +485,15 @@ DysonPipe *dyson_pipe(int nfreq) {
     p = &pipes.back().second;
     p->ok = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) == cudaSuccess &&
             cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming) == cudaSuccess;
+    // MBPT_DYSON_FACTOR_STREAMS=1 keeps every factorisation on the caller's stream
+    const char *env = std::getenv("MBPT_DYSON_FACTOR_STREAMS");
+    p->nfac = (env && std::atoi(env) == 1) ? 1 : 2;
+    if (p->ok && p->nfac == 2)
+      p->ok = cudaStreamCreateWithFlags(&p->fac2, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&p->join2, cudaEventDisableTiming) == cudaSuccess &&
+              cusolverDnCreate(&p->solver2) == CUSOLVER_STATUS_SUCCESS &&
+              cusolverDnSetStream(p->solver2, p->fac2) == CUSOLVER_STATUS_SUCCESS;
   }
   while (p->ok && static_cast<int>(p->ev.size()) < nfreq) {
     cudaEvent_t e = nullptr;
@@ -491,11 +510,13 @@ DysonPipe *dyson_pipe(int nfreq) {
   return p->ok ? p : nullptr;
 }
 
-// Factorise every frequency on `st`; as soon as frequency f's info word is on
-// the host, its inverse goes to the side stream, so that the tensor-core (or
-// DGEMM) inverse of f overlaps the FP64 Cholesky factorisation of f + 1. A
-// frequency that is not positive definite falls back to LU with both streams
-// drained first. The caller's stream waits for the side stream at the end.
+// Factorise the frequencies on two streams (even ones on `st`, odd ones on the
+// pipe's second factor stream, two ahead of the host); as soon as frequency
+// f's info word is on the host, its inverse goes to the side stream, so that
+// the tensor-core (or DGEMM) inverse of f overlaps the FP64 Cholesky
+// factorisations of f + 1 and f + 2. A frequency that is not positive definite
+// falls back to LU with every stream drained first. The caller's stream waits
+// for the other two at the end.
 int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, double *trace,
               int *info_host, int *sign_host, Arena &ar, cudaStream_t st,
               int mode = MBPT_MODE_FP64, int *err = nullptr) {
@@ -515,24 +536,32 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
                      b.pairs.ir_lo, b.pairs.tt_hi, b.pairs.tt_lo})
       if (cudaMemsetAsync(f, 0, bytes, st) != cudaSuccess) return MBPT_ERR_CUDA;
   }
+  const int nfac = nfreq > 1 ? pp->nfac : 1;
+  if (nfac == 2 && (cudaEventRecord(pp->fork, st) != cudaSuccess ||
+                    cudaStreamWaitEvent(pp->fac2, pp->fork, 0) != cudaSuccess))
+    return MBPT_ERR_CUDA;
   auto factor = [&](int f) -> int {
     double *m = chi0 + f * n * n;
-    if (cusolverDnDpotrf(h.solver, CUBLAS_FILL_MODE_LOWER, ni, m, ni, b.work, b.lwork,
+    const bool second = nfac == 2 && (f & 1);
+    cudaStream_t fs = second ? pp->fac2 : st;
+    if (cusolverDnDpotrf(second ? pp->solver2 : h.solver, CUBLAS_FILL_MODE_LOWER, ni, m, ni,
+                         second ? b.work2 : b.work, b.lwork,
                          b.info + f) != CUSOLVER_STATUS_SUCCESS)
       return MBPT_ERR_CUDA;
     // log det from the factor's diagonal before the inverse overwrites it
     // (replaced below where the factorisation failed)
-    launch_logdet_diag(m, n, 1, logdet + f, st);
-    if (cudaMemcpyAsync(pp->info + f, b.info + f, sizeof(int), cudaMemcpyDeviceToHost, st) !=
+    launch_logdet_diag(m, n, 1, logdet + f, fs);
+    if (cudaMemcpyAsync(pp->info + f, b.info + f, sizeof(int), cudaMemcpyDeviceToHost, fs) !=
             cudaSuccess ||
-        cudaEventRecord(pp->ev[f], st) != cudaSuccess)
+        cudaEventRecord(pp->ev[f], fs) != cudaSuccess)
       return MBPT_ERR_CUDA;
     return MBPT_OK;
   };
   bool bad = false, side_used = false;
-  int rc = factor(0);
+  int rc = MBPT_OK;
+  for (int f = 0; f < nfac && f < nfreq && rc == MBPT_OK; ++f) rc = factor(f);
   for (int f = 0; f < nfreq && rc == MBPT_OK; ++f) {
-    if (f + 1 < nfreq && (rc = factor(f + 1)) != MBPT_OK) break;
+    if (f + nfac < nfreq && (rc = factor(f + nfac)) != MBPT_OK) break;
     if (cudaEventSynchronize(pp->ev[f]) != cudaSuccess) {
       rc = MBPT_ERR_CUDA;
       break;
@@ -564,6 +593,7 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
     // the inverse), as the reference's slogdet/inv
     bad = true;
     if (cudaStreamSynchronize(pp->side) != cudaSuccess ||
+        (nfac == 2 && cudaStreamSynchronize(pp->fac2) != cudaSuccess) ||
         cudaStreamSynchronize(st) != cudaSuccess) {
       rc = MBPT_ERR_CUDA;
       break;
@@ -599,6 +629,10 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
   if (side_used) {
     cudaEventRecord(pp->join, pp->side);
     cudaStreamWaitEvent(st, pp->join, 0);
+  }
+  if (nfac == 2) {
+    cudaEventRecord(pp->join2, pp->fac2);
+    cudaStreamWaitEvent(st, pp->join2, 0);
   }
   if (rc) return rc;
   if (cudaGetLastError() != cudaSuccess) return MBPT_ERR_CUDA;
