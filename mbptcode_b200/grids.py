@@ -380,6 +380,33 @@ def minimax_points_for_gw(eps, nocc, mu=None, target=DEFAULT_TAU_TARGET,
                                      target=target, npoints_max=npoints_max)
 
 
+def transition_range(spectra, noccs):
+    """(smallest, largest) particle-hole energy over every spin channel
+    (``src/Base/orbital_spaces.py:23-29``)."""
+    windows = [particle_hole_window(e, n) for e, n in zip(spectra, noccs)]
+    return min(w[0] for w in windows), max(w[1] for w in windows)
+
+
+def minimax_points_for_bse(eps, nocc, tau_target=DEFAULT_TAU_TARGET):
+    """(ntau, residual) of the static screening's time grid: only chi0 is
+    transformed, so the chi0 transition range alone sizes it
+    (``LinearResponse/space_time.py:971-981``)."""
+    gap, span, _ = particle_hole_window(eps, nocc)
+    return minimax_points_for_accuracy(gap, span, target=tau_target)
+
+
+def static_screening_grid(eps, nocc, ntau=None, tau_target=DEFAULT_TAU_TARGET):
+    """The one-frequency (omega = 0, weight 1) minimax split on which the
+    static screening is built, cosine tau -> omega weights only
+    (``LinearResponse/space_time.py:984-1000``). ntau None or 'auto' sizes
+    it by `minimax_points_for_bse`."""
+    e_min, e_max, _ = particle_hole_window(eps, nocc)
+    if ntau is None or (isinstance(ntau, str) and ntau.lower() == 'auto'):
+        ntau, _ = minimax_points_for_bse(eps, nocc, tau_target=tau_target)
+    return TimeFrequencyGrid.minimax_split(ntau, e_min, e_max, [0.0], [1.0],
+                                           with_sine=False, with_inverse=False)
+
+
 @dataclass
 class SpaceTimeAxes:
     """The axes of one restricted space-time GW solve.

@@ -2,7 +2,9 @@
 
 MBPTcode has no plugin registry: its kernels are module-level functions that
 importing modules bind by name (``GW/space_time.py:66-79``,
-``GW/imaginary_time.py:33-36``, ``gradients/rpa/space_time_adjoint.py:84-87``),
+``GW/imaginary_time.py:33-36``, ``gradients/rpa/space_time_adjoint.py:84-87``;
+the static screening in ``BSE/solve.py:70``, ``GW/contour_deformation.py:104``,
+``gradients/gwbse/reaction_field_adjoint.py:33``),
 and its own tests substitute them with ``monkeypatch.setattr(module, name,
 ...)`` (``tests/test_rpa_log_determinant.py:57-72``). `install()` does the
 same for every module that holds one of the names, so every caller --
@@ -23,6 +25,10 @@ LR = 'src.SingleReference.LinearResponse.space_time'
 IT = 'src.SingleReference.GW.imaginary_time'
 ST = 'src.SingleReference.GW.space_time'
 ADJ = 'src.gradients.rpa.space_time_adjoint'
+# importers of the static screening W(omega = 0)
+BSE = 'src.SingleReference.BSE.solve'
+CD = 'src.SingleReference.GW.contour_deformation'
+RF = 'src.gradients.gwbse.reaction_field_adjoint'
 
 _SAVED: dict = {}
 
@@ -64,7 +70,11 @@ def replacements():
         'dyson_screening': space_time.dyson_screening,
         'dielectric_log_determinant': space_time.dielectric_log_determinant,
         'rpa_correlation_energy_space_time': space_time.rpa_correlation_energy_space_time,
+        'static_screening_matrix': space_time.static_screening_matrix,
+        'static_screening_matrix_unrestricted': space_time.static_screening_matrix_unrestricted,
     }
+    static = {k: seams[k] for k in ('static_screening_matrix',
+                                    'static_screening_matrix_unrestricted')}
     return {
         LR: dict(seams),
         IT: {k: v for k, v in seams.items()
@@ -72,7 +82,10 @@ def replacements():
                       'polarizability_projected_tau')},
         ST: {'chi0_imaginary_frequency': space_time.chi0_imaginary_frequency,
              'dyson_screening': space_time.dyson_screening,
-             '_sigma_mo_diagonal': _sigma_mo_diagonal},
+             '_sigma_mo_diagonal': _sigma_mo_diagonal, **static},
+        BSE: dict(static),
+        CD: dict(static),
+        RF: dict(static),
         ADJ: {'rpa_energy_and_adjoint': adjoint.rpa_energy_and_adjoint,
               'rpa_correlation_energy_space_time':
                   space_time.rpa_correlation_energy_space_time,

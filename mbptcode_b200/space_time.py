@@ -255,6 +255,80 @@ def dyson_screening(chi0, transform=None, correlation=False):
     return back(out, chi0)
 
 
+def _one_rank(comm, who):
+    if comm is not None and comm.Get_size() > 1:
+        raise NotImplementedError(f'{who}: rank splits are outside the one-GPU route')
+
+
+def static_screening_matrix(X, D, eps, nocc, grid=None, mu=None, comm=None,
+                            tile_memory_gb=None, branches=None, precision=None):
+    """W = [1 - chi0(i omega = 0)]^-1 in the auxiliary basis
+    (``space_time.py:1003-1050``): the BSE kernel's and the reaction field's
+    static screened interaction. The grid's tau points form chi0 on its one
+    frequency in a single device sweep (the reference's ordered sum of the
+    tau addends is the transform's FP64 sum over tau), then the Dyson step
+    (FP64 Cholesky; the inverse on the tensor cores in mixed precision).
+    `branches` = (X_o, X_v) already split takes the place of X's columns;
+    tile_memory_gb is accepted for signature compatibility."""
+    _one_rank(comm, 'static_screening_matrix')
+    from .grids import static_screening_grid
+    eps_h = _eps_host(eps)
+    if branches is not None:
+        X_o, X_v = branches
+        if X_o.shape[1] != nocc:
+            raise ValueError(f'branches: X_o has {X_o.shape[1]} columns, nocc is {nocc}')
+        cat = torch.cat if isinstance(X_o, torch.Tensor) else np.concatenate
+        X = cat([X_o, X_v], 1)
+    grid = static_screening_grid(eps_h, nocc) if grid is None else grid
+    chi0, _ = chi0_sweep(X, D, eps_h, nocc, grid.tau_points, grid.cosft_wt, mu=mu,
+                         precision=precision)
+    return _static_w(chi0, precision, X)
+
+
+def _static_w(chi0, precision, like):
+    """W = [1 - chi0]^-1 of a (1, naux, naux) device chi0, in place."""
+    dyson_batch(chi0, want_w=True,
+                precision='mixed' if _mode(precision) == MODES['mixed'] else 'fp64')
+    chi0.diagonal(dim1=-2, dim2=-1).add_(1.0)
+    return back(chi0[0], like)
+
+
+def spin_summed(kernel, X_mos, D, spectra, noccs, *args, **kwargs):
+    """chi0_alpha + chi0_beta of an unrestricted reference from a kernel's
+    restricted form (``space_time.py:774-796``): every kernel carries the
+    closed-shell factor 2, so each spin contributes half the kernel on its own
+    collocation, spectrum and occupation, at its own mid-gap."""
+    out = None
+    for X, eps, nocc in zip(X_mos, spectra, noccs):
+        part = kernel(X, D, eps, nocc, *args,
+                      mu=particle_hole_window(_eps_host(eps), nocc)[2], **kwargs)
+        out = part if out is None else out + part
+    return out * 0.5
+
+
+def static_screening_matrix_unrestricted(X_mos, D, spectra, noccs, tau_target=None,
+                                         precision=None):
+    """`static_screening_matrix` of an unrestricted reference
+    (``space_time.py:1053-1066``): one W from chi0_alpha + chi0_beta on a grid
+    spanning both spins' transitions, with as many points as the harder spin
+    needs. Both spins' chi0 sweeps accumulate on the device."""
+    from .grids import (DEFAULT_TAU_TARGET, TimeFrequencyGrid, minimax_points_for_bse,
+                        transition_range)
+    target = DEFAULT_TAU_TARGET if tau_target is None else tau_target
+    spectra = [_eps_host(e) for e in spectra]
+    e_min, e_max = transition_range(spectra, noccs)
+    ntau = max(minimax_points_for_bse(e, n, tau_target=target)[0]
+               for e, n in zip(spectra, noccs))
+    grid = TimeFrequencyGrid.minimax_split(ntau, e_min, e_max, [0.0], [1.0],
+                                           with_sine=False, with_inverse=False)
+
+    def sweep(X, D, eps, nocc, mu=None):
+        return chi0_sweep(X, D, eps, nocc, grid.tau_points, grid.cosft_wt, mu=mu,
+                          precision=precision)[0]
+    chi0 = spin_summed(sweep, X_mos, D, spectra, noccs)
+    return _static_w(chi0, precision, X_mos[0])
+
+
 def dielectric_log_determinant(one_minus_c, where, flags=None):
     """log|det(1 - c)| with a NonPositiveDielectric warning and the
     'nonpositive_det' flag when the determinant is not positive:

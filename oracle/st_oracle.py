@@ -99,6 +99,22 @@ def dyson_screening(chi0, correlation=False):
     return W
 
 
+def static_screening_matrix(X, D, eps, nocc, grid, mu=None):
+    """space_time.py:1003-1050 on one rank: chi0 on the one-frequency static
+    grid (tau addends summed in tau order), then W = [1 - chi0]^-1."""
+    return dyson_screening(chi0_imaginary_frequency(X, D, eps, nocc, grid, mu=mu)[0])
+
+
+def static_screening_matrix_unrestricted(X_mos, D, spectra, noccs, grid):
+    """space_time.py:1053-1066 and spin_summed :774-796: half the restricted
+    chi0 of each spin (at its own mid-gap) summed, then the Dyson inverse.
+    `grid` is the two-spin static grid (transition range of both spins)."""
+    chi0 = sum(chi0_imaginary_frequency(X, D, e, n, grid,
+                                        mu=particle_hole_window(e, n)[2])[0]
+               for X, e, n in zip(X_mos, spectra, noccs))
+    return dyson_screening(0.5 * chi0)
+
+
 def dielectric_log_determinant(one_minus_c, where, flags=None):
     """space_time.py:1073-1097: log|det|, flagging a non-positive determinant."""
     sign, logdet = np.linalg.slogdet(one_minus_c)

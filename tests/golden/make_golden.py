@@ -17,6 +17,10 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      the reference route: chi0, W - I, Wt(tau), the Sigma_c
                      diagonal from the AO build, QP roots and Z for every
                      state, E_c and its adjoint;
+* static.npz         the static screening W(omega = 0) of the BSE kernel: the
+                     auto-sized one-frequency grid, W of a restricted system
+                     (auto and 12 points) and the spin-summed W of an
+                     unrestricted one;
 * qp_kat.npz         the root finder on closed-form self-energies
                      (tests/test_qp_refine_root.py's two-pole Sigma and others);
 * c1_<variant>.npz   the synthetic FP64 configuration at full size (n_orb = 400,
@@ -26,7 +30,7 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      stored: the tests regenerate them from the seed and check
                      the regeneration against the stored eps and checksums.
 
-    python tests/golden/make_golden.py [/root/reference] [--only c1]
+    python tests/golden/make_golden.py [/root/reference] [--only c1|static]
 """
 import os
 import sys
@@ -53,8 +57,9 @@ from src.Base.utils.grids.analytic_continuation import (PadeFit,        # noqa: 
                                                         thiele_coefficients)
 from src.Base.orbital_spaces import particle_hole_window                # noqa: E402
 from src.SingleReference.LinearResponse.space_time import (             # noqa: E402
-    chi0_imaginary_frequency, dyson_screening, polarizability_projected_sweep,
-    rpa_correlation_energy_space_time)
+    chi0_imaginary_frequency, dyson_screening, minimax_points_for_bse,
+    polarizability_projected_sweep, rpa_correlation_energy_space_time,
+    static_screening_grid, static_screening_matrix, static_screening_matrix_unrestricted)
 from src.SingleReference.GW.imaginary_time import (                     # noqa: E402
     minimax_points_for_gw, screening_frequency_grid, _transform_screened,
     self_energy_matrix_imaginary_time, sigma_ao_to_mo_diagonal)
@@ -197,6 +202,25 @@ def c1_fixture(variant):
         adjoint_projections=proj)
 
 
+def static_fixture():
+    """The static screening W(omega = 0) of the BSE kernel: the auto-sized
+    one-frequency grid and W of a restricted system, and the spin-summed W of
+    an unrestricted one (alpha: the restricted system; beta: its own
+    collocation and spectrum from another seed, one electron fewer)."""
+    X, D, eps = synthetic_system(24, 4, 64, 7, 'calibrated')
+    ntau, resid = minimax_points_for_bse(eps, 4)
+    grid = static_screening_grid(eps, 4)
+    W = static_screening_matrix(X, D, eps, 4, grid)
+    grid12 = static_screening_grid(eps, 4, ntau=12)
+    W12 = static_screening_matrix(X, D, eps, 4, grid12)
+    Xb, _, eps_b = synthetic_system(24, 3, 64, 8, 'calibrated')
+    Wu = static_screening_matrix_unrestricted([X, Xb], D, [eps, eps_b], [4, 3])
+    np.savez_compressed(
+        os.path.join(HERE, 'static.npz'), X=X, D=D, eps=eps, nocc=4, ntau=ntau,
+        resid=resid, tau=grid.tau_points, cosft_wt=grid.cosft_wt, W=W, tau12=grid12.tau_points,
+        cosft_wt12=grid12.cosft_wt, W12=W12, Xb=Xb, eps_b=eps_b, nocc_b=3, W_u=Wu)
+
+
 def qp_fixture():
     cases = {  # poles placed off the scan grids, so no division hits one
         'two_pole': (lambda w: 0.05 / (w + 0.8) + 0.01 / (w - 0.9), -0.2),
@@ -228,10 +252,15 @@ if __name__ == '__main__':
         c1_fixture('calibrated')
         print('C1 fixtures written to', HERE)
         sys.exit(0)
+    if ONLY == 'static':
+        static_fixture()
+        print('static screening fixture written to', HERE)
+        sys.exit(0)
     grids_fixture()
     shared_kernel_fixture()
     route_fixture('calibrated', 24, 4, 64, 7, 'calibrated', 12, full=True)
     route_fixture('literal16', 20, 3, 48, 3, 'literal', 16)
     route_fixture('calibrated16', 28, 5, 72, 9, 'calibrated', 16)
     qp_fixture()
+    static_fixture()
     print('fixtures written to', HERE)

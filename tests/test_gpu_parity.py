@@ -314,3 +314,31 @@ def test_bounded_wait_gives_up_and_context_survives(dev):
     torch.cuda.synchronize()
     assert int(err.item()) == 0
     assert np.abs(C.cpu().numpy() - A @ B.T).max() < 3e-5 * np.sqrt(96) * 16
+
+
+@pytest.mark.parametrize('precision,tol', [('fp64', 1e-11), ('mixed', 5e-5)])
+def test_static_screening_matches_reference_golden(golden, precision, tol):
+    """W(omega = 0) = [1 - chi0(0)]^-1 of the BSE kernel on the auto-sized
+    one-frequency grid and on 12 points, restricted and spin-summed
+    unrestricted, against the reference's W (entries bounded by 1, so the
+    bars are absolute: FP64 to rounding, mixed within the split products'
+    error on chi0)."""
+    g = golden('static')
+    X, D, eps, nocc = g['X'], g['D'], g['eps'], int(g['nocc'])
+    W = st.static_screening_matrix(X, D, eps, nocc, precision=precision)
+    assert isinstance(W, np.ndarray) and W.shape == g['W'].shape
+    assert np.abs(W - g['W']).max() < tol
+    W12 = st.static_screening_matrix(X, D, eps, nocc, grids.static_screening_grid(eps, nocc, 12),
+                                     precision=precision)
+    assert np.abs(W12 - g['W12']).max() < tol
+    Wb = st.static_screening_matrix(None, D, eps, nocc, precision=precision,
+                                    branches=(X[:, :nocc], X[:, nocc:]))
+    assert np.array_equal(Wb, W)
+    Wu = st.static_screening_matrix_unrestricted([X, g['Xb']], D, [eps, g['eps_b']],
+                                                 [nocc, int(g['nocc_b'])], precision=precision)
+    assert np.abs(Wu - g['W_u']).max() < tol
+    if precision == 'fp64':
+        grid = grids.static_screening_grid(eps, nocc)
+        chi0 = st.spin_summed(st.chi0_imaginary_frequency, [X, X], D, [eps, eps],
+                              [nocc, nocc], grid)
+        assert rel(chi0, orc.chi0_imaginary_frequency(X, D, eps, nocc, grid)) < FP64_REL

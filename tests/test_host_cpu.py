@@ -107,6 +107,9 @@ def test_plugin_rebinds_and_restores_reference_names():
         orig = lr.chi0_imaginary_frequency
         bound, skipped = plugin.install()
         assert lr.chi0_imaginary_frequency is space_time.chi0_imaginary_frequency
+        assert lr.static_screening_matrix is space_time.static_screening_matrix
+        # the static screening's other importers need pyscf, absent here
+        assert {plugin.BSE, plugin.CD, plugin.RF} <= set(skipped)
         assert 'dyson_screening' in bound[plugin.IT]
         assert plugin.ST in skipped      # MBPTcode's GW module imports pyscf, absent here
         adj = importlib.import_module(plugin.ADJ)

@@ -119,3 +119,32 @@ def test_qp_known_answers(golden):
     fit = orc.PadeFit(g['thiele_z'], g['thiele_f'])
     assert np.array_equal(fit.z, g['greedy_z'])
     assert np.allclose(fit(np.linspace(-1, 1, 7) + 0j), g['greedy_eval'], rtol=1e-10)
+
+
+def test_static_screening_grid_and_oracle(golden):
+    """The static screening W(omega = 0): the auto-sized one-frequency grid is
+    the reference's bit for bit, and the oracle's W (restricted, and the
+    spin-summed unrestricted form) matches the reference's."""
+    g = golden('static')
+    X, D, eps, nocc = g['X'], g['D'], g['eps'], int(g['nocc'])
+    n, resid = grids.minimax_points_for_bse(eps, nocc)
+    assert n == int(g['ntau']) and resid == float(g['resid'])
+    grid = grids.static_screening_grid(eps, nocc)
+    assert np.array_equal(grid.tau_points, g['tau'])
+    assert np.array_equal(grid.cosft_wt, g['cosft_wt'])
+    assert np.array_equal(grid.omega_points, [0.0]) and grid.cosft_tw is None
+    g12 = grids.static_screening_grid(eps, nocc, ntau=12)
+    assert np.array_equal(g12.tau_points, g['tau12'])
+    assert np.array_equal(g12.cosft_wt, g['cosft_wt12'])
+    W = orc.static_screening_matrix(X, D, eps, nocc, grid)
+    assert np.abs(W - g['W']).max() <= 1e-12
+    W12 = orc.static_screening_matrix(X, D, eps, nocc, g12)
+    assert np.abs(W12 - g['W12']).max() <= 1e-12
+    spectra, noccs = [eps, g['eps_b']], [nocc, int(g['nocc_b'])]
+    e_min, e_max = grids.transition_range(spectra, noccs)
+    nu = max(grids.minimax_points_for_bse(e, k)[0] for e, k in zip(spectra, noccs))
+    with _quiet():
+        gu = grids.TimeFrequencyGrid.minimax_split(nu, e_min, e_max, [0.0], [1.0],
+                                                   with_sine=False, with_inverse=False)
+    Wu = orc.static_screening_matrix_unrestricted([X, g['Xb']], D, spectra, noccs, gu)
+    assert np.abs(Wu - g['W_u']).max() <= 1e-12
