@@ -409,8 +409,9 @@ def static_screening_grid(eps, nocc, ntau=None, tau_target=DEFAULT_TAU_TARGET):
 
 @dataclass
 class SpaceTimeAxes:
-    """The axes of one restricted space-time GW solve.
+    """The axes of one space-time GW solve.
 
+    mu: the mid-gap (restricted), or one per spin channel (unrestricted);
     grid: chi0's tau axis onto the screening frequencies (cosft_wt);
     tau_sigma: the self-energy's own tau axis (half the rS minimax points);
     Ctw (ntau, nfreq): omega -> tau cosine weights of W - I over rW;
@@ -418,7 +419,7 @@ class SpaceTimeAxes:
     pade_freq: the Pade sample frequencies.
     """
     ntau: int
-    mu: float
+    mu: float | tuple
     grid: TimeFrequencyGrid
     tau_sigma: np.ndarray
     Ctw: np.ndarray
@@ -459,3 +460,64 @@ def space_time_axes(eps, nocc, ntau='auto', pade_freq=None, anchor=None,
                                           f_s.result())
     return SpaceTimeAxes(ntau, mu, grid, tau_sigma, Ctw, C, S, pade,
                          (rW, rS), tau_err)
+
+
+def unrestricted_fit_ranges(spectra, noccs):
+    """(rW, rS) of an unrestricted reference (``GW/imaginary_time.py:141-155``):
+    the restricted rule on both spin channels together, each channel at its
+    own mid-gap, rW from the union of the transitions and rS the hull of the
+    channels' self-energy ranges."""
+    w_lo, w_hi = transition_range(spectra, noccs)
+    parts = [self_energy_fit_ranges_from_window(e, 0.5 * (e[n - 1] + e[n]), w_lo, w_hi)
+             for e, n in ((np.asarray(e, float), n) for e, n in zip(spectra, noccs))]
+    rW = parts[0][0]
+    return rW, (min(rS[0] for _, rS in parts), max(rS[1] for _, rS in parts))
+
+
+def unrestricted_screening_frequency_grid(ntau, spectra, noccs):
+    """Minimax frequencies over the two-spin rW (``GW/imaginary_time.py:158-163``)."""
+    rW, _ = unrestricted_fit_ranges(spectra, noccs)
+    return minimax_frequency_grid(ntau, *rW)
+
+
+def minimax_points_for_gw_unrestricted(spectra, noccs, target=DEFAULT_TAU_TARGET,
+                                       npoints_max=34):
+    """`minimax_points_for_gw` over both spin channels' ranges together
+    (``GW/imaginary_time.py:166-173``)."""
+    w_lo, w_hi = transition_range(spectra, noccs)
+    rW, rS = unrestricted_fit_ranges(spectra, noccs)
+    return minimax_points_for_ranges((w_hi / w_lo, rW[1] / rW[0], rS[1] / rS[0]),
+                                     target=target, npoints_max=npoints_max)
+
+
+def space_time_axes_unrestricted(spectra, noccs, ntau='auto', pade_freq=None, anchors=None,
+                                 tau_target=DEFAULT_TAU_TARGET):
+    """The axes of the unrestricted route (``GW/space_time.py:559-618`` with two
+    channels): chi0's time grid over both spins' transitions, W's frequencies
+    and the self-energy's fit ranges over both channels, so that one W serves
+    either channel. `mu` is the tuple of the channels' own mid-gaps, on which
+    each channel samples its self-energy. `anchors` (one spectrum per spin)
+    size an automatic ntau."""
+    spectra = [np.asarray(e, float) for e in spectra]
+    noccs = [int(n) for n in noccs]
+    e_min, e_max = transition_range(spectra, noccs)
+    tau_err = None
+    if ntau is None or (isinstance(ntau, str) and ntau.lower() == 'auto'):
+        a = spectra if anchors is None else [np.asarray(x, float) for x in anchors]
+        ntau, tau_err = minimax_points_for_gw_unrestricted(a, noccs, target=tau_target)
+    if int(ntau) not in supported_sizes('omega'):
+        raise ValueError(f'ntau = {ntau} has no tabulated frequency grid')
+    ntau = int(ntau)
+    freq, fw = unrestricted_screening_frequency_grid(ntau, spectra, noccs)
+    rW, rS = unrestricted_fit_ranges(spectra, noccs)
+    tau_sigma = 0.5 * minimax_time_grid(ntau, *rS)[0]
+    pade = pade_nodes() if pade_freq is None else np.asarray(pade_freq, float)
+    with _single_threaded_blas(), ThreadPoolExecutor(max_workers=4) as outer:
+        f_grid = outer.submit(TimeFrequencyGrid.minimax_split, ntau, e_min, e_max, freq, fw)
+        f_ctw = outer.submit(transform_weights, COSINE_WT, tau_sigma, freq, *rW, warn=False)
+        f_c = outer.submit(transform_weights, COSINE_TW, tau_sigma, pade, *rS, warn=False)
+        f_s = outer.submit(transform_weights, SINE_TW, tau_sigma, pade, *rS, warn=False)
+        grid, (Ctw, _), (C, _), (S, _) = (f_grid.result(), f_ctw.result(), f_c.result(),
+                                          f_s.result())
+    mus = tuple(particle_hole_window(e, n)[2] for e, n in zip(spectra, noccs))
+    return SpaceTimeAxes(ntau, mus, grid, tau_sigma, Ctw, C, S, pade, (rW, rS), tau_err)

@@ -8,6 +8,7 @@ all arithmetic runs in libmbpt_b200.
 """
 from __future__ import annotations
 
+import contextlib
 import time
 import warnings
 
@@ -15,7 +16,7 @@ import numpy as np
 import torch
 
 from ._lib import BUFFERS, WORKSPACE, check, host_array, lib, ptr, require_device, stream_ptr
-from .grids import space_time_axes
+from .grids import space_time_axes, space_time_axes_unrestricted
 from .space_time import (_Err, _eps_host, _mode, check_mixed_weights, chi0_sweep,
                          dyson_batch, to_device, transform)
 
@@ -239,6 +240,75 @@ def gw_space_time(X, D, eps, nocc, states=None, ntau='auto', precision=None,
     return (roots, z) if with_z else roots
 
 
+def gw_sweep_unrestricted(X_mos, D, spectra, noccs, states=None, ntau='auto', axes=None,
+                          precision=None, eps_anchors=None, xc_diagonals=None, greedy=True,
+                          channels=(0, 1), stream=None):
+    """The space-time G0W0 sweep of an unrestricted reference
+    (``GW/space_time.py:866-1009``, serial, in core): one W from
+    chi0_alpha + chi0_beta (each half the restricted chi0 of that spin's
+    collocation X_mos[s], spectrum and occupation, at its own mid-gap), then
+    for each channel in `channels` the restricted self-energy sweep on that
+    channel's orbitals (Sigma_s = -G_s W has no spin factor) and its QP roots,
+    Sigma sampled through the channel's own mid-gap.
+
+    states: per channel, None (all) or the orbitals; eps_anchors and
+    xc_diagonals: per channel or None. Returns {'channels': {s: SweepResult},
+    'axes', 'e_c' (the spin-summed RPA energy from the same factorisations),
+    'dyson_info'}.
+    """
+    dev = require_device()
+    X_mos = [to_device(X, dev) for X in X_mos]
+    D = to_device(D, dev)
+    spectra = [_eps_host(e) for e in spectra]
+    noccs = [int(n) for n in noccs]
+    if len(X_mos) != 2 or len(spectra) != 2 or len(noccs) != 2:
+        raise ValueError('an unrestricted sweep takes two spin channels')
+    if axes is None:
+        axes = space_time_axes_unrestricted(
+            spectra, noccs, ntau=ntau,
+            anchors=None if eps_anchors is None else [_eps_host(a) for a in eps_anchors])
+    check_mixed_weights(precision, axes.grid.cosft_wt, axes.Ctw, axes.C, axes.S)
+    err = _Err(dev)
+    naux = D.shape[1]
+    shape = (axes.grid.nfreq, naux, naux)
+    chi0, _ = chi0_sweep(X_mos[0], D, spectra[0], noccs[0], axes.grid.tau_points,
+                         axes.grid.cosft_wt, mu=axes.mu[0], precision=precision,
+                         stream=stream, out=BUFFERS.take('sweep_chi0', shape, dev), err=err)
+    beta, _ = chi0_sweep(X_mos[1], D, spectra[1], noccs[1], axes.grid.tau_points,
+                         axes.grid.cosft_wt, mu=axes.mu[1], precision=precision,
+                         stream=stream, err=err)
+    # spin_summed: half of each spin's restricted chi0
+    with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
+        chi0.add_(beta).mul_(0.5)
+    del beta
+    logdet, trace, info, _ = dyson_batch(chi0, want_w=True, stream=stream,
+                                         precision=precision, err=err)
+    e_c = torch.empty((), dtype=torch.float64, device=dev)
+    ow = torch.as_tensor(np.asarray(axes.grid.omega_weights, float), device=dev)
+    check(lib().mbpt_energy_sum(ptr(logdet), ptr(trace), ptr(ow), len(ow), ptr(e_c),
+                                stream_ptr(stream)), 'mbpt_energy_sum')
+    Wt = screened_interaction_tau(
+        chi0, axes.Ctw, stream,
+        out=BUFFERS.take('sweep_wt', (len(axes.Ctw), naux, naux), dev))
+    del chi0
+    out = {}
+    for s in channels:
+        eps_s, n_s, mu_s = spectra[s], noccs[s], axes.mu[s]
+        st = states[s] if states is not None else None
+        st = np.arange(len(eps_s)) if st is None else np.atleast_1d(np.asarray(st, int))
+        branch = sigma_branch_sums(X_mos[s], D, Wt, eps_s, n_s, axes.tau_sigma, st, mu_s,
+                                   precision, stream, err=err)
+        sigma = sigma_frequency(branch, axes.C, axes.S, stream)
+        anchor = eps_s if eps_anchors is None else _eps_host(eps_anchors[s])
+        xc = None if xc_diagonals is None else xc_diagonals[s]
+        roots, z, flags, evals = qp_solve(sigma, axes.pade_freq, anchor, st, n_s, mu_s,
+                                          xc=xc, greedy=greedy, stream=stream)
+        out[s] = SweepResult(roots=roots, z=z, flags=flags, evals=evals, sigma=sigma,
+                             states=st, branch=branch)
+    err.check('gw_sweep_unrestricted')
+    return {'channels': out, 'axes': axes, 'e_c': e_c, 'dyson_info': info}
+
+
 def _factors(factors):
     if factors is None:
         raise NotImplementedError(
@@ -257,8 +327,11 @@ def solve_qp_energy_space_time(mf, mol, nocc, p_state, numerics=None, auxbasis=N
                                spin_channel='alpha', xc_diagonal=None, with_z=False,
                                failures=None, counts=None, grid_accuracy=None,
                                precision=None):
-    """Drop-in for ``GW/space_time.py:631-863`` on a restricted gas-phase
-    reference with pre-built factors: the mean field gives eps (mo_energy);
+    """Drop-in for ``GW/space_time.py:631-863`` on a gas-phase reference with
+    pre-built factors. Restricted: the mean field gives eps (mo_energy).
+    Unrestricted (mo_energy of shape (2, nmo), nocc = (nalpha, nbeta)): channel
+    `spin_channel`, from the factors' AO collocation (X_mo, D, X_ao[, coords])
+    and mf.mo_coeff per spin (``GW/space_time.py:866-1009``);
     the static term <Sigma_x - v_xc> is `xc_diagonal` (0 on an HF reference,
     ``qp_solve.py:311``). numerics.quadrature: ntau_st ('auto' or a size),
     npade and w0_gl. Returns Hartree, a float for a scalar p_state."""
@@ -269,8 +342,6 @@ def solve_qp_energy_space_time(mf, mol, nocc, p_state, numerics=None, auxbasis=N
             raise NotImplementedError(f'{name} is outside the one-GPU device route')
     X, D = _factors(factors)
     eps = np.asarray(getattr(mf, 'mo_energy', mf), float)
-    if eps.ndim != 1:
-        raise NotImplementedError('an unrestricted reference is outside the device route')
     ntau, pade = 'auto', None
     if numerics is not None:
         q = numerics.quadrature
@@ -278,6 +349,16 @@ def solve_qp_energy_space_time(mf, mol, nocc, p_state, numerics=None, auxbasis=N
         from .grids import pade_nodes
         pade = pade_nodes(q.npade, q.w0_gl)
     states = np.atleast_1d(p_state)
+    if eps.ndim == 2:
+        roots, z, evals = _unrestricted_channel(mf, nocc, states, factors, D, eps, ntau, pade,
+                                                spin_channel, eps_anchor, xc_diagonal,
+                                                greedy, precision, timings)
+        if counts is not None:
+            counts['sigma_evaluations'] = evals
+        scalar = np.ndim(p_state) == 0
+        if with_z:
+            return (roots[0], z[0]) if scalar else (roots, z)
+        return roots[0] if scalar else roots
     axes = space_time_axes(eps, nocc, ntau=ntau, pade_freq=pade,
                            anchor=None if eps_anchor is None else np.asarray(eps_anchor))
     res = gw_sweep(X, D, eps, nocc, states=states, axes=axes, precision=precision,
@@ -297,8 +378,52 @@ def solve_qp_energy_space_time(mf, mol, nocc, p_state, numerics=None, auxbasis=N
     return roots[0] if scalar else roots
 
 
+def _unrestricted_channel(mf, nocc, states, factors, D, eps, ntau, pade, spin_channel,
+                          eps_anchor, xc_diagonal, greedy, precision, timings):
+    """One channel of an unrestricted reference (``GW/space_time.py:866-1009``):
+    each spin's collocation X_ao C_s off the one factorization, one W from both
+    spins, the channel's Sigma and roots. Returns host (roots, z, evals)."""
+    if spin_channel not in ('alpha', 'beta'):
+        raise ValueError(f"spin_channel must be 'alpha' or 'beta', got {spin_channel!r}")
+    spin = 0 if spin_channel == 'alpha' else 1
+    X_ao = factors.get('X_ao') if isinstance(factors, dict) else (
+        tuple(factors) + (None,) * 4)[2]
+    if X_ao is None:
+        raise ValueError(
+            'an unrestricted reference needs the AO collocation of the factors, '
+            '(X_mo, D, X_ao[, coords]): each spin projects it on its own orbitals')
+    dev = require_device()
+    Xa = to_device(X_ao, dev)
+    X_mos = [Xa @ to_device(c, dev) for c in mf.mo_coeff]
+    noccs = tuple(int(n) for n in nocc)
+    anchors = None
+    if eps_anchor is not None:
+        anchors = np.asarray(eps_anchor, float)
+        if anchors.shape != (2, eps.shape[1]):
+            raise ValueError(f'an unrestricted eps_anchor is one spectrum per spin, shape '
+                             f'(2, {eps.shape[1]}); got {anchors.shape}')
+    axes = space_time_axes_unrestricted(list(eps), noccs, ntau=ntau, pade_freq=pade,
+                                        anchors=anchors)
+    per = [None, None]
+    per[spin] = states
+    xcs = None
+    if xc_diagonal is not None:
+        xcs = [None, None]
+        xcs[spin] = xc_diagonal
+    res = gw_sweep_unrestricted(X_mos, D, list(eps), noccs, states=per, axes=axes,
+                                precision=precision,
+                                eps_anchors=None if anchors is None else list(anchors),
+                                xc_diagonals=xcs, greedy=greedy, channels=(spin,))
+    if timings is not None:
+        timings['ntau_auto'] = axes.ntau
+        timings['tau_fit_error'] = axes.tau_fit_error
+    ch = res['channels'][spin]
+    _report_flags(ch['flags'].cpu().numpy(), states)
+    return ch['roots'].cpu().numpy(), ch['z'].cpu().numpy(), ch['evals'].cpu().numpy()
+
+
 def solve_qp_diagonal_space_time(mf, mol, nocc, states=None, **kw):
     """``GW/space_time.py:1091-1105``: (qp energies, states)."""
-    n = len(np.asarray(getattr(mf, 'mo_energy', mf)))
+    n = np.asarray(getattr(mf, 'mo_energy', mf)).shape[-1]
     states = np.arange(n) if states is None else np.atleast_1d(states)
     return solve_qp_energy_space_time(mf, mol, nocc, states, **kw), states

@@ -413,6 +413,29 @@ def gw_space_time(X, D, eps, nocc, states, axes, eps_anchor=None, xc_diag=None,
             'sigma': sigma, 'roots': roots, 'z': z}
 
 
+def gw_space_time_unrestricted(X_mos, D, spectra, noccs, states, axes):
+    """GW/space_time.py:866-1009 (serial): chi0 = half of each spin's
+    restricted chi0 at its own mid-gap (space_time.py:774-796), one W, then
+    per channel the restricted Sigma sweep on that channel's orbitals and its
+    QP roots sampled through the channel's mid-gap. `axes`: the two-spin axes
+    (mbptcode_b200.grids.space_time_axes_unrestricted; axes.mu per channel).
+    states: per channel. Returns {'W_minus_I', 'sigma': [..], 'roots': [..],
+    'z': [..]}."""
+    chi0 = 0.5 * sum(chi0_imaginary_frequency(X, D, np.asarray(e, float), n, axes.grid, m)
+                     for X, e, n, m in zip(X_mos, spectra, noccs, axes.mu))
+    W = np.stack([dyson_screening(c, correlation=True) for c in chi0])
+    Wt = np.tensordot(axes.Ctw, W, axes=(1, 0))
+    out = {'W_minus_I': W, 'sigma': [], 'roots': [], 'z': []}
+    for X, e, n, m, st in zip(X_mos, spectra, noccs, axes.mu, states):
+        e = np.asarray(e, float)
+        sig = sigma_branch_sums(X, D, Wt, e, n, axes.tau_sigma, m, st)
+        sigma = sigma_frequency(sig, axes.C, axes.S)
+        roots, z = finish_qp(sigma, e, n, st, m, axes.pade_freq)
+        for k, v in (('sigma', sigma), ('roots', roots), ('z', z)):
+            out[k].append(v)
+    return out
+
+
 # ---------------------------------------------------------------------------
 # dRPA adjoint (src/gradients/rpa/space_time_adjoint.py:136-218, 473-563)
 # ---------------------------------------------------------------------------

@@ -21,6 +21,9 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      auto-sized one-frequency grid, W of a restricted system
                      (auto and 12 points) and the spin-summed W of an
                      unrestricted one;
+* unrestricted.npz   the unrestricted route (two spin channels, one W from the
+                     spin-summed chi0): grids, W - I, each channel's Sigma_c
+                     diagonal, QP roots and Z;
 * qp_kat.npz         the root finder on closed-form self-energies
                      (tests/test_qp_refine_root.py's two-pole Sigma and others);
 * c1_<variant>.npz   the synthetic FP64 configuration at full size (n_orb = 400,
@@ -30,7 +33,7 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      stored: the tests regenerate them from the seed and check
                      the regeneration against the stored eps and checksums.
 
-    python tests/golden/make_golden.py [/root/reference] [--only c1|static]
+    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted]
 """
 import os
 import sys
@@ -59,10 +62,14 @@ from src.Base.orbital_spaces import particle_hole_window                # noqa: 
 from src.SingleReference.LinearResponse.space_time import (             # noqa: E402
     chi0_imaginary_frequency, dyson_screening, minimax_points_for_bse,
     polarizability_projected_sweep, rpa_correlation_energy_space_time,
-    static_screening_grid, static_screening_matrix, static_screening_matrix_unrestricted)
+    spin_summed, static_screening_grid, static_screening_matrix,
+    static_screening_matrix_unrestricted)
 from src.SingleReference.GW.imaginary_time import (                     # noqa: E402
     minimax_points_for_gw, screening_frequency_grid, _transform_screened,
-    self_energy_matrix_imaginary_time, sigma_ao_to_mo_diagonal)
+    self_energy_matrix_imaginary_time, sigma_ao_to_mo_diagonal,
+    minimax_points_for_gw_unrestricted, unrestricted_fit_ranges,
+    unrestricted_screening_frequency_grid)
+from src.Base.orbital_spaces import transition_range                    # noqa: E402
 from src.Solvers.qp_equation import solve_qp_equation_pole_strength     # noqa: E402
 from src.gradients.rpa.space_time_adjoint import rpa_energy_and_adjoint  # noqa: E402
 
@@ -221,6 +228,58 @@ def static_fixture():
         cosft_wt12=grid12.cosft_wt, W12=W12, Xb=Xb, eps_b=eps_b, nocc_b=3, W_u=Wu)
 
 
+def _qp_roots(sigma, eps, nocc, mu, pade, states):
+    """Roots and Z of every state, as GW/qp_solve.py:529-558 per state."""
+    roots, zs = np.empty(len(states)), np.empty(len(states))
+    for i, p in enumerate(states):
+        sign = -1.0 if p < nocc else 1.0
+        s_p = np.conj(sigma[i]) if p < nocc else sigma[i]
+        fit = PadeFit(mu + 1j * sign * pade, s_p, greedy=True)
+
+        def residual(w, fit=fit, p=p):
+            return w - eps[p] - fit(np.array([w], dtype=complex))[0].real
+        got = solve_qp_equation_pole_strength(residual, eps[p], return_diagnostics=True)
+        roots[i] = got[0]
+        dz = [z for w, z in got[1] if w == got[0]]
+        zs[i] = dz[0] if dz else np.nan
+    return roots, zs
+
+
+def unrestricted_fixture(ntau=12):
+    """The unrestricted route of GW/space_time.py:866-1009 composed from the
+    reference's kernels (the driver module itself needs pyscf): both spins'
+    chi0 by `spin_summed`, one W, then each channel's self-energy on the
+    two-spin fit ranges and its QP roots through its own mid-gap. Spin alpha:
+    5 of 24 orbitals occupied; spin beta: its own collocation and spectrum
+    (another seed), 4 occupied."""
+    X_a, D, eps_a = synthetic_system(24, 5, 72, 11, 'calibrated')
+    X_b, _, eps_b = synthetic_system(24, 4, 72, 12, 'calibrated')
+    X_mos, spectra, noccs = [X_a, X_b], [eps_a, eps_b], [5, 4]
+    e_min, e_max = transition_range(spectra, noccs)
+    ntau_auto, _ = minimax_points_for_gw_unrestricted(spectra, noccs)
+    freq, fw = unrestricted_screening_frequency_grid(ntau, spectra, noccs)
+    ranges = unrestricted_fit_ranges(spectra, noccs)
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        grid = TimeFrequencyGrid.minimax_split(ntau, e_min, e_max, freq, fw)
+    tau_sigma = 0.5 * minimax_time_grid(ntau, *ranges[1])[0]
+    pade = gauss_legendre_grid(16, w0=1.0)[0]
+    chi0 = spin_summed(chi0_imaginary_frequency, X_mos, D, spectra, noccs, grid)
+    W = np.stack([dyson_screening(c) for c in chi0])
+    out = dict(X_a=X_a, X_b=X_b, D=D, eps_a=eps_a, eps_b=eps_b, nocc_a=5, nocc_b=4, ntau=ntau,
+               ntau_auto=ntau_auto, tau=grid.tau_points, omega=freq, cosft_wt=grid.cosft_wt,
+               tau_sigma=tau_sigma, rW=ranges[0], rS=ranges[1], W_minus_I=W - np.eye(72))
+    for s, (X, e, n) in enumerate(zip(X_mos, spectra, noccs)):
+        mu = particle_hole_window(e, n)[2]
+        sig_ao = self_energy_matrix_imaginary_time(X, D, W, np.eye(24), e, n, tau_sigma, freq,
+                                                   pade, mu=mu, ranges=ranges)
+        states = np.arange(24)
+        sigma = sigma_ao_to_mo_diagonal(sig_ao, np.eye(24), states=states).T
+        roots, zs = _qp_roots(sigma, e, n, mu, pade, states)
+        out.update({f'sigma_{s}': sigma, f'roots_{s}': roots, f'z_{s}': zs, f'mu_{s}': mu})
+    np.savez_compressed(os.path.join(HERE, 'unrestricted.npz'), **out)
+
+
 def qp_fixture():
     cases = {  # poles placed off the scan grids, so no division hits one
         'two_pole': (lambda w: 0.05 / (w + 0.8) + 0.01 / (w - 0.9), -0.2),
@@ -256,6 +315,12 @@ if __name__ == '__main__':
         static_fixture()
         print('static screening fixture written to', HERE)
         sys.exit(0)
+    if ONLY == 'unrestricted':
+        unrestricted_fixture()
+        print('unrestricted fixture written to', HERE)
+        sys.exit(0)
+    if ONLY:
+        sys.exit(f'--only {ONLY}: choose c1, static or unrestricted')
     grids_fixture()
     shared_kernel_fixture()
     route_fixture('calibrated', 24, 4, 64, 7, 'calibrated', 12, full=True)
@@ -263,4 +328,5 @@ if __name__ == '__main__':
     route_fixture('calibrated16', 28, 5, 72, 9, 'calibrated', 16)
     qp_fixture()
     static_fixture()
+    unrestricted_fixture()
     print('fixtures written to', HERE)

@@ -342,3 +342,63 @@ def test_static_screening_matches_reference_golden(golden, precision, tol):
         chi0 = st.spin_summed(st.chi0_imaginary_frequency, [X, X], D, [eps, eps],
                               [nocc, nocc], grid)
         assert rel(chi0, orc.chi0_imaginary_frequency(X, D, eps, nocc, grid)) < FP64_REL
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'mixed'])
+def test_unrestricted_route_matches_reference_golden(golden, precision):
+    """Two spin channels, one W from the spin-summed chi0, each channel's
+    Sigma_c diagonal and QP roots against the reference's composition: FP64
+    to rounding (frontier roots to the scan's tolerance), mixed within the
+    QP bar (10 meV) on the frontier states."""
+    g = golden('unrestricted')
+    X_mos = [g['X_a'], g['X_b']]
+    spectra, noccs = [g['eps_a'], g['eps_b']], [int(g['nocc_a']), int(g['nocc_b'])]
+    res = gw.gw_sweep_unrestricted(X_mos, g['D'], spectra, noccs, ntau=int(g['ntau']),
+                                   precision=precision)
+    assert res['axes'].ntau == int(g['ntau'])
+    for s in range(2):
+        sigma = res['channels'][s]['sigma'].cpu().numpy()
+        roots = res['channels'][s]['roots'].cpu().numpy()
+        ref = g[f'roots_{s}']
+        f = frontier(noccs[s], len(spectra[s]))
+        if precision == 'fp64':
+            assert rel(sigma, g[f'sigma_{s}']) < 1e-9
+            assert np.abs(roots[f] - ref[f]).max() < 5e-8
+            assert np.abs(roots - ref).max() < 2e-6
+        else:
+            assert rel(sigma, g[f'sigma_{s}']) < 1e-4
+            assert np.abs(roots[f] - ref[f]).max() * 27.211386 < 10e-3
+
+
+def test_unrestricted_closed_shell_equals_restricted(golden):
+    """A closed shell run unrestricted reads every grid the restricted route
+    reads and halves twice its own chi0: the roots are the restricted ones."""
+    g = golden('route_calibrated')
+    X, D, eps, nocc = g['X'], g['D'], g['eps'], int(g['nocc'])
+    r = gw.gw_sweep(X, D, eps, nocc, ntau=int(g['ntau']), precision='fp64')
+    u = gw.gw_sweep_unrestricted([X, X], D, [eps, eps], [nocc, nocc], ntau=int(g['ntau']),
+                                 precision='fp64')
+    for s in range(2):
+        assert torch.equal(u['channels'][s]['roots'], r['roots'])
+    assert float(u['e_c']) == float(r['e_c'])
+
+
+def test_unrestricted_driver_channel(golden):
+    """solve_qp_energy_space_time on an unrestricted mean field: the channel's
+    collocation is X_ao C_s (here C_s = I, X_ao the alpha collocation for both
+    spins with the beta spectrum), nocc = (nalpha, nbeta)."""
+    g = golden('unrestricted')
+    X, D = g['X_a'], g['D']
+    eps2 = np.stack([g['eps_a'], g['eps_a']])
+
+    class MF:
+        mo_energy = eps2
+        mo_coeff = [np.eye(24), np.eye(24)]
+    n = int(g['nocc_a'])
+    got = gw.solve_qp_energy_space_time(MF, None, (n, n), np.arange(n - 2, n + 2),
+                                        factors=(X, D, X), spin_channel='beta')
+    ref = gw.gw_sweep_unrestricted([X, X], D, [g['eps_a']] * 2, [n, n],
+                                   states=[None, np.arange(n - 2, n + 2)], channels=(1,))
+    assert np.array_equal(got, ref['channels'][1]['roots'].cpu().numpy())
+    with pytest.raises(ValueError):
+        gw.solve_qp_energy_space_time(MF, None, (n, n), 0, factors=(X, D))

@@ -148,3 +148,31 @@ def test_static_screening_grid_and_oracle(golden):
                                                    with_sine=False, with_inverse=False)
     Wu = orc.static_screening_matrix_unrestricted([X, g['Xb']], D, spectra, noccs, gu)
     assert np.abs(Wu - g['W_u']).max() <= 1e-12
+
+
+def test_unrestricted_axes_and_oracle(golden):
+    """The unrestricted route: the two-spin axes (chi0's time grid over both
+    spins' transitions, W's frequencies and the self-energy's fit ranges
+    over both channels) are the reference's bit for bit, and the oracle's
+    W - I, Sigma_c diagonals and QP roots of both channels match it."""
+    g = golden('unrestricted')
+    spectra, noccs = [g['eps_a'], g['eps_b']], [int(g['nocc_a']), int(g['nocc_b'])]
+    assert grids.minimax_points_for_gw_unrestricted(spectra, noccs)[0] == int(g['ntau_auto'])
+    rW, rS = grids.unrestricted_fit_ranges(spectra, noccs)
+    assert rW == tuple(g['rW']) and rS == tuple(g['rS'])
+    with _quiet():
+        axes = grids.space_time_axes_unrestricted(spectra, noccs, ntau=int(g['ntau']))
+    assert np.array_equal(axes.grid.omega_points, g['omega'])
+    assert np.array_equal(axes.grid.tau_points, g['tau'])
+    assert np.array_equal(axes.grid.cosft_wt, g['cosft_wt'])
+    assert np.array_equal(axes.tau_sigma, g['tau_sigma'])
+    assert axes.mu == (g['mu_0'], g['mu_1'])
+    states = [np.arange(24)] * 2
+    out = orc.gw_space_time_unrestricted([g['X_a'], g['X_b']], g['D'], spectra, noccs, states,
+                                         axes)
+    W = g['W_minus_I']
+    assert np.abs(out['W_minus_I'] - W).max() <= 1e-12 * np.abs(W).max()
+    for s in range(2):
+        sig = g[f'sigma_{s}']
+        assert np.abs(out['sigma'][s] - sig).max() <= 1e-10 * np.abs(sig).max()
+        assert np.abs(out['roots'][s] - g[f'roots_{s}']).max() < 2e-6
