@@ -225,6 +225,33 @@ int mbpt_chi0_backward(const double *proj_bar_dev, const double *X_dev, int64_t 
 int mbpt_energy_adjoint_seed(double *w_minus_i_dev, int64_t naux, int nfreq,
                              const double *omega_weights_dev, void *stream);
 
+/* The self-energy adjoint: gradients/rpa/space_time_adjoint.py:795-875
+ * (`selfenergy_diag_backward`), its per-tau part :836-856 and the bra
+ * slices' share :866-871. For the branch adjoints sl_bar, sg_bar (ntau x
+ * nstates, device; the reverse of the tau -> omega weights :830-833, formed
+ * by the caller) of Sigma^<, Sigma^> at the time points tau_host, on W(tau)
+ * = Wt_dev (ntau, naux, naux; symmetric), it overwrites eps_bar (norb),
+ * X_bar (M x norb), D_bar (M x naux) with the self-energy sweep's share and
+ * writes Wt_bar_dev (ntau, naux, naux), which the Dyson and chi0 reverses
+ * (mbpt_dyson_backward, mbpt_transform, mbpt_chi0_backward) take on.
+ * states_dev: nstates int64 orbital indices. FP64. */
+size_t mbpt_sigma_backward_workspace_bytes(int64_t M, int64_t norb, int64_t nocc,
+                                           int64_t naux, int nstates);
+int mbpt_sigma_backward(const double *X_dev, int64_t M, int64_t norb, int64_t nocc,
+                        const double *eps_dev, double mu, const double *D_dev, int64_t naux,
+                        const double *tau_host, int ntau, const double *Wt_dev,
+                        const int64_t *states_dev, int nstates, const double *sl_bar_dev,
+                        const double *sg_bar_dev, double *eps_bar_dev, double *X_bar_dev,
+                        double *D_bar_dev, double *Wt_bar_dev, void *workspace,
+                        size_t ws_bytes, int *err_dev, void *stream);
+
+/* The reverse of the Dyson step W = [1 - chi0]^-1: chi0_bar_f = W_f W_bar_f W_f
+ * (gradients/rpa/space_time_adjoint.py:679-685), in place over wbar_dev
+ * (nfreq, naux, naux), from W - I (w_minus_i_dev, the Dyson output). FP64. */
+size_t mbpt_dyson_backward_workspace_bytes(int64_t naux);
+int mbpt_dyson_backward(const double *w_minus_i_dev, double *wbar_dev, int64_t naux, int nfreq,
+                        void *workspace, size_t ws_bytes, void *stream);
+
 /* ---- quasiparticle-shift network (learned warm start) --------------------
  * A 4 -> H -> H -> 1 perceptron with SiLU, FP32, parameters packed as
  * [W1 (H x 4), b1 (H), W2 (H x H), b2 (H), W3 (H), b3 (1)].

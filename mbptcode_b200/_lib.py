@@ -52,6 +52,11 @@ _SIGNATURES = {
     'mbpt_chi0_backward': (_i, [_p, _p, _i64, _i64, _i64, _p, _d, _p, _i64, _p, _i, _i, _p,
                                 _p, _p, _p, _sz, _p, _p]),
     'mbpt_energy_adjoint_seed': (_i, [_p, _i64, _i, _p, _p]),
+    'mbpt_sigma_backward_workspace_bytes': (_sz, [_i64, _i64, _i64, _i64, _i]),
+    'mbpt_sigma_backward': (_i, [_p, _i64, _i64, _i64, _p, _d, _p, _i64, _p, _i, _p, _p, _i,
+                                 _p, _p, _p, _p, _p, _p, _p, _sz, _p, _p]),
+    'mbpt_dyson_backward_workspace_bytes': (_sz, [_i64]),
+    'mbpt_dyson_backward': (_i, [_p, _p, _i64, _i, _p, _sz, _p]),
     'mbpt_mlp_param_count': (_i, [_i]),
     'mbpt_mlp_forward': (_i, [_p, _i, _p, _i, _p, _p, _p]),
     'mbpt_mlp_backward': (_i, [_p, _i, _p, _i, _p, _p, _p, _p, _p, _p]),

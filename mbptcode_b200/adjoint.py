@@ -1,4 +1,5 @@
-"""dRPA correlation energy and its adjoint on the B200.
+"""dRPA correlation energy, the self-energy diagonal, and their adjoints on
+the B200.
 
 Mirrors ``src/gradients/rpa/space_time_adjoint.py:473-563``
 (`rpa_energy_and_adjoint`, gas phase, one GPU): one forward sweep keeps
@@ -10,6 +11,14 @@ nothing of G is stored across tau -- to accumulate eps_bar, X_bar, D_bar.
 `RPAEnergy` wraps it as a torch.autograd.Function of (eps, X, D); the
 Coulomb factor's own dependence on V (D = chol(V)) is left to torch's
 Cholesky backward, so `rpa_energy(eps, X, V=V)` differentiates in V too.
+
+The self-energy diagonal Sigma^c_pp(i omega) and its reverse
+(``space_time_adjoint.py:652-691, 795-875``, the QP-gradient building
+blocks): `selfenergy_diag` keeps proj(tau) and W(tau) as its cache;
+`selfenergy_diag_backward` runs the self-energy sweep backwards
+(mbpt_sigma_backward), then the Dyson step (mbpt_dyson_backward, W rebuilt
+from proj(tau)) and the chi0 sweep (mbpt_chi0_backward). `SelfEnergyDiag`
+wraps them as a torch.autograd.Function of (eps, X, D).
 """
 from __future__ import annotations
 
@@ -119,3 +128,166 @@ def rpa_energy(eps, X, D=None, nocc=None, grid=None, V=None, mu=None, precision=
     if mu is None:
         mu = particle_hole_window(eps.detach().cpu().numpy(), nocc)[2]
     return RPAEnergy.apply(eps, X, D, nocc, grid, mu, precision)
+
+
+# ---------------------------------------------------------------- self-energy
+
+def _one_rank(comm, who):
+    if comm is not None and comm.Get_size() > 1:
+        raise NotImplementedError(f'{who}: rank splits are outside the one-GPU route')
+
+
+def _back(t, like):
+    return t if isinstance(like, torch.Tensor) else t.cpu().numpy()
+
+
+def selfenergy_diag(X, D, eps, nocc, grid, states, transforms, mu, tile_gb=None, comm=None,
+                    precision='fp64'):
+    """Sigma^c_pp(i omega_out) of `states` on the grid's own tau points, and
+    the cache its reverse needs (``GW/imaginary_time.py:731-768``): chi0 and
+    proj(tau) in one sweep, W - I by the Dyson step, Wt(tau) = Ctw (W - I),
+    the branch sums and the tau -> omega transform with (C, S). Returns
+    (sigma (nstates, nfreq_out) complex, (proj_tau, Wt_tau, None)); the
+    cache's tensors stay on the device."""
+    from .gw import screened_interaction_tau, sigma_branch_sums, sigma_frequency
+    _one_rank(comm, 'selfenergy_diag')
+    dev = require_device()
+    Xd, Dd = to_device(X, dev), to_device(D, dev)
+    eps_h = _eps_host(eps)
+    Ctw, C, S = transforms
+    chi0, proj = chi0_sweep(Xd, Dd, eps_h, nocc, grid.tau_points, grid.cosft_wt, mu=mu,
+                            precision=precision, want_proj=True)
+    dyson_batch(chi0, want_w=True, precision=precision)
+    Wt = screened_interaction_tau(chi0, Ctw)
+    del chi0
+    branch = sigma_branch_sums(Xd, Dd, Wt, eps_h, nocc, grid.tau_points,
+                               np.atleast_1d(states), mu, precision)
+    sigma = sigma_frequency(branch, C, S)
+    return _back(sigma, X), (proj, Wt, None)
+
+
+def screened_interaction_tau_backward(Wt_bar, proj_tau, grid, Ctw, tile_gb=None, comm=None):
+    """proj_bar (ntau, naux, naux) for an adjoint Wt_bar on
+    Wt(tau) = sum_w Ctw[tau, w] (W_w - I) (``space_time_adjoint.py:652-691``):
+    chi0 rebuilt from proj(tau), W by the Dyson step, chi0_bar = W W_bar W per
+    frequency, and the two transforms turned round. FP64."""
+    _one_rank(comm, 'screened_interaction_tau_backward')
+    dev = require_device()
+    Wb, P = to_device(Wt_bar, dev), to_device(proj_tau, dev)
+    cw = np.asarray(grid.cosft_wt, float)
+    chi0 = transform(P, cw)
+    dyson_batch(chi0, want_w=True, precision='fp64')
+    wbar = transform(Wb, np.ascontiguousarray(np.asarray(Ctw, float).T))
+    naux, nfreq = chi0.shape[-1], chi0.shape[0]
+    ws = WORKSPACE.get(lib().mbpt_dyson_backward_workspace_bytes(naux), dev)
+    check(lib().mbpt_dyson_backward(ptr(chi0), ptr(wbar), naux, nfreq, ptr(ws), ws.numel(),
+                                    stream_ptr()), 'mbpt_dyson_backward')
+    proj_bar = transform(wbar, np.ascontiguousarray(cw.T))
+    return _back(proj_bar, Wt_bar)
+
+
+def sigma_backward(branch_bar, X, D, eps, nocc, tau_points, states, mu, Wt):
+    """(eps_bar, X_bar, D_bar, Wt_bar) device tensors of the self-energy sweep
+    alone for branch adjoints (2, ntau, nstates) on (Sigma^<, Sigma^>)."""
+    dev = require_device()
+    Xd, Dd = to_device(X, dev), to_device(D, dev)
+    eps_h = _eps_host(eps)
+    ed = to_device(eps_h, dev)
+    M, norb = Xd.shape
+    naux = Dd.shape[1]
+    tau_h, tp = host_array(tau_points)
+    st_h = np.asarray(states, dtype=np.int64)
+    if st_h.size == 0 or st_h.min() < 0 or st_h.max() >= norb:
+        raise ValueError(f'states must be orbital indices in [0, {norb}), got {st_h}')
+    st = torch.as_tensor(st_h, device=dev)
+    S = st.numel()
+    bb = to_device(branch_bar, dev)
+    sl, sg = bb[0].contiguous(), bb[1].contiguous()
+    Wc = to_device(Wt, dev)
+    if Wc.shape != (len(tau_h), naux, naux) or sl.shape != (len(tau_h), S):
+        raise ValueError(f'Wt {tuple(Wc.shape)} and branch adjoints {tuple(bb.shape)} do not '
+                         f'match {len(tau_h)} tau points, {S} states, naux {naux}')
+    eps_bar = torch.empty(norb, dtype=torch.float64, device=dev)
+    X_bar = torch.empty((M, norb), dtype=torch.float64, device=dev)
+    D_bar = torch.empty((M, naux), dtype=torch.float64, device=dev)
+    Wt_bar = torch.empty_like(Wc)
+    ws = WORKSPACE.get(lib().mbpt_sigma_backward_workspace_bytes(M, norb, nocc, naux, S), dev)
+    err = _Err(dev)
+    check(lib().mbpt_sigma_backward(ptr(Xd), M, norb, nocc, ptr(ed), float(mu), ptr(Dd), naux,
+                                    tp, len(tau_h), ptr(Wc), ptr(st), S, ptr(sl), ptr(sg),
+                                    ptr(eps_bar), ptr(X_bar), ptr(D_bar), ptr(Wt_bar),
+                                    ptr(ws), ws.numel(), ptr(err.t), stream_ptr()),
+          'mbpt_sigma_backward')
+    err.check('mbpt_sigma_backward')
+    return eps_bar, X_bar, D_bar, Wt_bar
+
+
+def _branch_bar(a_re, a_im, C, S):
+    """Adjoints on (Sigma^<, Sigma^>)(tau) of Sigma = -1/2 [(S> + S<)^T C^T
+    + i (S> - S<)^T S^T] (``space_time_adjoint.py:830-833``)."""
+    a_re = a_re.detach().cpu().numpy() if isinstance(a_re, torch.Tensor) else np.asarray(a_re)
+    a_im = a_im.detach().cpu().numpy() if isinstance(a_im, torch.Tensor) else np.asarray(a_im)
+    ac = np.atleast_2d(a_re) @ np.asarray(C, float)
+    bs = np.atleast_2d(a_im) @ np.asarray(S, float)
+    return np.stack([-0.5 * (ac - bs).T, -0.5 * (ac + bs).T])
+
+
+def selfenergy_diag_backward(a_re, a_im, X, D, eps, nocc, grid, states, transforms, mu,
+                             cache, tile_gb=None, comm=None):
+    """(eps_bar, X_bar, D_bar) for the real functional
+    sum a_re Re Sigma + a_im Im Sigma of `selfenergy_diag`'s output
+    (``space_time_adjoint.py:795-875``): the self-energy sweep backwards, then
+    W_bar through the Dyson step and the chi0 sweep backwards. `cache` is
+    `selfenergy_diag`'s (proj_tau, Wt_tau, ...). FP64; arrays come back as X
+    is held."""
+    _one_rank(comm, 'selfenergy_diag_backward')
+    Ctw, C, S = transforms
+    proj, Wt = cache[0], cache[1]
+    eps_h = _eps_host(eps)
+    bb = _branch_bar(a_re, a_im, C, S)
+    e1, x1, d1, Wt_bar = sigma_backward(bb, X, D, eps_h, nocc, grid.tau_points,
+                                        np.atleast_1d(states), mu, Wt)
+    proj_bar = screened_interaction_tau_backward(Wt_bar, to_device(proj, Wt_bar.device), grid,
+                                                 Ctw)
+    e2, x2, d2 = chi0_backward(proj_bar, X, D, eps_h, nocc, grid.tau_points, mu)
+    out = (e1 + e2, x1 + x2, d1 + d2)
+    return tuple(_back(t, X) for t in out)
+
+
+class SelfEnergyDiag(torch.autograd.Function):
+    """Sigma^c_pp(i omega_out) (complex, nstates x nfreq_out) of (eps, X, D)
+    with `selfenergy_diag_backward` as backward; the grid, transforms and mu
+    are frozen. torch hands a real loss's gradient on a complex output as
+    dL/dRe + i dL/dIm, which are the adjoints a_re, a_im."""
+
+    @staticmethod
+    def forward(ctx, eps, X, D, nocc, grid, states, transforms, mu):
+        sigma, cache = selfenergy_diag(X.detach(), D.detach(), eps.detach(), nocc, grid,
+                                       states, transforms, mu)
+        ctx.args = (nocc, grid, states, transforms, mu, cache)
+        ctx.save_for_backward(eps, X, D)
+        return sigma
+
+    @staticmethod
+    def backward(ctx, g):
+        eps, X, D = ctx.saved_tensors
+        nocc, grid, states, transforms, mu, cache = ctx.args
+        eb, xb, db = selfenergy_diag_backward(g.real, g.imag, X.detach(), D.detach(),
+                                              eps.detach(), nocc, grid, states, transforms,
+                                              mu, cache)
+        return eb, xb, db, None, None, None, None, None
+
+
+def selfenergy_diag_t(eps, X, D, nocc, grid, states, transforms=None, mu=None, omega_out=None):
+    """Differentiable Sigma^c_pp(i omega_out) of device tensors (eps, X, D).
+    transforms default to `grids.sigma_transforms` on the grid's own axes
+    (omega_out: the grid's frequencies unless given)."""
+    eps_h = eps.detach().cpu().numpy()
+    if mu is None:
+        mu = particle_hole_window(eps_h, nocc)[2]
+    if transforms is None:
+        from .grids import sigma_transforms
+        out = grid.omega_points if omega_out is None else omega_out
+        transforms = sigma_transforms(eps_h, nocc, grid.tau_points, grid.omega_points, out,
+                                      mu=mu)
+    return SelfEnergyDiag.apply(eps, X, D, nocc, grid, np.atleast_1d(states), transforms, mu)

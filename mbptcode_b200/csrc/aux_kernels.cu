@@ -239,6 +239,56 @@ __global__ void identity_kernel(double *a, int64_t n, double diag_shift, bool se
   }
 }
 
+// ---------------------------------------------------------- self-energy adjoint
+// Xs[r, s] = X[r, states[s]] scaled by the branch adjoints of one tau point:
+// Xl = Xs diag(sl), Xg = Xs diag(sg) (MBPTcode gradients/rpa/space_time_adjoint.py:846-853,
+// there as the weights c of the bra slice)
+__global__ void sigma_back_gather_kernel(const double *__restrict__ X, int64_t M, int64_t n,
+                                         const int64_t *__restrict__ states, int64_t S,
+                                         const double *__restrict__ sl,
+                                         const double *__restrict__ sg, double *Xs, double *Xl,
+                                         double *Xg) {
+  const int64_t total = M * S;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = i / S, c = i % S;
+    const double x = X[r * n + states[c]];
+    Xs[i] = x;
+    Xl[i] = x * sl[c];
+    Xg[i] = x * sg[c];
+  }
+}
+
+// The elementwise reverse of Sigma^<_s = x_s^T (Go o Zt) x_s and
+// Sigma^>_s = -x_s^T (Gv o Zt) x_s with Al = sum_s sl_s x_s x_s^T and
+// Ag = sum_s sg_s x_s x_s^T, in place:
+//   zt <- Zt_bar = go al - gv ag,  al <- Go_bar = zt al,  ag <- Gv_bar = -zt ag,
+//   go <- L = go zt,               gv <- H = gv zt
+__global__ void sigma_back_hadamard_kernel(double *go, double *gv, double *zt, double *al,
+                                           double *ag, int64_t total) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double o = go[i], v = gv[i], z = zt[i], a = al[i], g = ag[i];
+    zt[i] = o * a - v * g;
+    al[i] = z * a;
+    ag[i] = -z * g;
+    go[i] = o * z;
+    gv[i] = v * z;
+  }
+}
+
+// X_bar[r, states[s]] += scale * T[r, s] (a state listed twice adds twice)
+__global__ void scatter_cols_kernel(const double *__restrict__ T, int64_t M, int64_t S,
+                                    const int64_t *__restrict__ states, double scale,
+                                    double *X_bar, int64_t n) {
+  const int64_t total = M * S;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = i / S, c = i % S;
+    atomicAdd(X_bar + r * n + states[c], scale * T[i]);
+  }
+}
+
 }  // namespace
 
 void launch_chi0_bar_seed(double *a, int64_t n, int nfreq, const double *w, cudaStream_t st) {
@@ -310,6 +360,26 @@ void launch_identity(double *a, int64_t n, cudaStream_t st) {
 
 void launch_minus_identity(double *a, int64_t n, cudaStream_t st) {
   count_launch(); identity_kernel<<<blocks(n * n), 256, 0, st>>>(a, n, -1.0, false);
+}
+
+void launch_sigma_back_gather(const double *X, int64_t M, int64_t n, const int64_t *states,
+                              int64_t S, const double *sl, const double *sg, double *Xs,
+                              double *Xl, double *Xg, cudaStream_t st) {
+  count_launch();
+  sigma_back_gather_kernel<<<blocks(M * S), 256, 0, st>>>(X, M, n, states, S, sl, sg, Xs, Xl,
+                                                          Xg);
+}
+
+void launch_sigma_back_hadamard(double *go, double *gv, double *zt, double *al, double *ag,
+                                int64_t total, cudaStream_t st) {
+  count_launch();
+  sigma_back_hadamard_kernel<<<blocks(total), 256, 0, st>>>(go, gv, zt, al, ag, total);
+}
+
+void launch_scatter_cols(const double *T, int64_t M, int64_t S, const int64_t *states,
+                         double scale, double *X_bar, int64_t n, cudaStream_t st) {
+  count_launch();
+  scatter_cols_kernel<<<blocks(M * S), 256, 0, st>>>(T, M, S, states, scale, X_bar, n);
 }
 
 }  // namespace mbpt

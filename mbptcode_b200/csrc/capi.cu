@@ -42,6 +42,13 @@ int launch_trtri_diag_blocks(double *A, int64_t n, int64_t lda, int nb, cudaStre
                              float *r_lo = nullptr, int64_t ldp = 0);
 void launch_strided_to_tf32(const double *src, int64_t rows, int64_t k, int64_t rs, int64_t cs,
                             float *hi, float *lo, int64_t rows_p, int64_t k_p, cudaStream_t st);
+void launch_sigma_back_gather(const double *X, int64_t M, int64_t n, const int64_t *states,
+                              int64_t S, const double *sl, const double *sg, double *Xs,
+                              double *Xl, double *Xg, cudaStream_t st);
+void launch_sigma_back_hadamard(double *go, double *gv, double *zt, double *al, double *ag,
+                                int64_t total, cudaStream_t st);
+void launch_scatter_cols(const double *T, int64_t M, int64_t S, const int64_t *states,
+                         double scale, double *X_bar, int64_t n, cudaStream_t st);
 
 namespace {
 std::atomic<long long> g_launches{0};
@@ -844,6 +851,102 @@ int back_run(const double *pbar, const double *X, const Dims &d, const double *e
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 
+// ------------------------------------------------------- self-energy adjoint
+struct SigBackBufs {
+  double *Xo_s, *Xv_s, *Go, *Gv, *Zt, *Al, *Ag, *U, *Xs, *Xl, *Xg, *T1, *GoX, *GvX;
+};
+
+SigBackBufs carve_sigma_back(Arena &ar, const Dims &d, int64_t S) {
+  SigBackBufs b{};
+  b.Xo_s = ar.take<double>(d.M * d.nocc);
+  b.Xv_s = ar.take<double>(d.M * d.nv);
+  for (double **m : {&b.Go, &b.Gv, &b.Zt, &b.Al, &b.Ag}) *m = ar.take<double>(d.M * d.M);
+  b.U = ar.take<double>(d.M * d.naux);
+  for (double **m : {&b.Xs, &b.Xl, &b.Xg, &b.T1}) *m = ar.take<double>(d.M * S);
+  b.GoX = ar.take<double>(d.M * d.nocc);
+  b.GvX = ar.take<double>(d.M * d.nv);
+  return b;
+}
+
+// The reverse of the states' self-energy branch sums over every tau point,
+// in the grid-space form of the forward: Sigma^<_s(tau) = x_s^T (Go o Zt) x_s,
+// Sigma^>_s(tau) = -x_s^T (Gv o Zt) x_s with Zt = D Wt(tau) D^T and x_s the
+// state's column of X. For the branch adjoints sl, sg of one tau point, with
+// Al = sum_s sl_s x_s x_s^T and Ag = sum_s sg_s x_s x_s^T:
+//   x_s_bar  = 2 [(Go o Zt) x_s sl_s - (Gv o Zt) x_s sg_s],
+//   Go_bar   = Zt o Al,   Gv_bar = -Zt o Ag    (then the G branches' reverse),
+//   Zt_bar   = Go o Al - Gv o Ag,
+//   Wt_bar   = D^T Zt_bar D,   D_bar += 2 Zt_bar D Wt.
+// It is the same derivative as MBPTcode gradients/rpa/space_time_adjoint.py:836-856
+// (written there on the three-index slices B_p = D^T diag(x_p) X), and
+// :866-871 for the bra slices' share of X_bar and D_bar.
+int sigma_back_run(const double *X, const Dims &d, const double *eps, double mu,
+                   const double *D, const double *tau, int ntau, const double *Wt,
+                   const int64_t *states, int64_t S, const double *sl_bar,
+                   const double *sg_bar, double *eps_bar, double *X_bar, double *D_bar,
+                   double *Wt_bar, Arena &ar, cudaStream_t st) {
+  SigBackBufs b = carve_sigma_back(ar, d, S);
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  cublasHandle_t h = handles(st).blas;
+  const int64_t a2 = d.naux * d.naux, M = d.M, A = d.naux;
+  cudaMemsetAsync(eps_bar, 0, sizeof(double) * d.n, st);
+  cudaMemsetAsync(X_bar, 0, sizeof(double) * M * d.n, st);
+  cudaMemsetAsync(D_bar, 0, sizeof(double) * M * A, st);
+  for (int k = 0; k < ntau; ++k) {
+    const double *Wk = Wt + k * a2;
+    launch_scaled_branches(X, M, d.n, d.nocc, eps, mu, tau[k], 1.0, b.Xo_s, b.Xv_s, st);
+    launch_sigma_back_gather(X, M, d.n, states, S, sl_bar + k * S, sg_bar + k * S, b.Xs, b.Xl,
+                             b.Xg, st);
+    if (!dgemm_rm(h, false, true, M, M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0, b.Go, M) ||
+        !dgemm_rm(h, false, true, M, M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n, 0.0, b.Gv,
+                  M) ||
+        !dgemm_rm(h, false, false, M, A, A, 1.0, D, A, Wk, A, 0.0, b.U, A) ||
+        !dgemm_rm(h, false, true, M, M, A, 1.0, b.U, A, D, A, 0.0, b.Zt, M) ||
+        !dgemm_rm(h, false, true, M, M, S, 1.0, b.Xl, S, b.Xs, S, 0.0, b.Al, M) ||
+        !dgemm_rm(h, false, true, M, M, S, 1.0, b.Xg, S, b.Xs, S, 0.0, b.Ag, M))
+      return MBPT_ERR_CUDA;
+    // Go -> L = Go o Zt, Gv -> H = Gv o Zt, Zt -> Zt_bar, Al -> Go_bar, Ag -> Gv_bar
+    launch_sigma_back_hadamard(b.Go, b.Gv, b.Zt, b.Al, b.Ag, M * M, st);
+    if (!dgemm_rm(h, false, false, M, S, M, 1.0, b.Go, M, b.Xl, S, 0.0, b.T1, S) ||
+        !dgemm_rm(h, false, false, M, S, M, -1.0, b.Gv, M, b.Xg, S, 1.0, b.T1, S))
+      return MBPT_ERR_CUDA;
+    launch_scatter_cols(b.T1, M, S, states, 2.0, X_bar, d.n, st);
+    if (!dgemm_rm(h, false, false, M, d.nocc, M, 1.0, b.Al, M, X, d.n, 0.0, b.GoX, d.nocc) ||
+        !dgemm_rm(h, false, false, M, d.nv, M, 1.0, b.Ag, M, X + d.nocc, d.n, 0.0, b.GvX,
+                  d.nv))
+      return MBPT_ERR_CUDA;
+    launch_xbar_update(b.GoX, b.GvX, X, M, d.n, d.nocc, eps, mu, tau[k], X_bar, eps_bar, st);
+    // U <- Zt_bar D, then Wt_bar = D^T U and D_bar += 2 U Wt (Zt_bar and Wt symmetric)
+    if (!dgemm_rm(h, false, false, M, A, M, 1.0, b.Zt, M, D, A, 0.0, b.U, A) ||
+        !dgemm_rm(h, true, false, A, A, M, 1.0, D, A, b.U, A, 0.0, Wt_bar + k * a2, A) ||
+        !dgemm_rm(h, false, false, M, A, A, 2.0, b.U, A, Wk, A, 1.0, D_bar, A))
+      return MBPT_ERR_CUDA;
+  }
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+// chi0_bar_f = W_f W_bar_f W_f in place over W_bar, W_f = I + (W - I)_f:
+// the reverse of the Dyson step W = [1 - chi0]^-1 (W symmetric), as MBPTcode
+// gradients/rpa/space_time_adjoint.py:679-685
+int dyson_back_run(const double *wmi, double *wbar, int64_t n, int nfreq, Arena &ar,
+                   cudaStream_t st) {
+  double *T = ar.take<double>(n * n);
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  cublasHandle_t h = handles(st).blas;
+  const size_t bytes = sizeof(double) * n * n;
+  for (int f = 0; f < nfreq; ++f) {
+    const double *Wm = wmi + f * n * n;
+    double *B = wbar + f * n * n;
+    // T = B + Wm B; B <- T + T Wm
+    if (cudaMemcpyAsync(T, B, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+        !dgemm_rm(h, false, false, n, n, n, 1.0, Wm, n, B, n, 1.0, T, n) ||
+        cudaMemcpyAsync(B, T, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+        !dgemm_rm(h, false, false, n, n, n, 1.0, T, n, Wm, n, 1.0, B, n))
+      return MBPT_ERR_CUDA;
+  }
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
 size_t count(void (*f)(Arena &)) {
   Arena ar;
   ar.counting = true;
@@ -1078,6 +1181,40 @@ int mbpt_chi0_backward(const double *pbar, const double *X, int64_t M, int64_t n
   if (mode != MBPT_MODE_FP64) return MBPT_ERR_UNSUPPORTED;
   Arena ar = arena(ws, ws_bytes);
   return back_run(pbar, X, d, eps, mu, D, tau, ntau, eps_bar, X_bar, D_bar, ar, S(stream));
+}
+
+size_t mbpt_sigma_backward_workspace_bytes(int64_t M, int64_t norb, int64_t nocc,
+                                           int64_t naux, int nstates) {
+  Dims d(M, norb, nocc, naux);
+  Arena ar;
+  ar.counting = true;
+  carve_sigma_back(ar, d, nstates > 0 ? nstates : 1);
+  return ar.used + 2048;
+}
+
+int mbpt_sigma_backward(const double *X, int64_t M, int64_t norb, int64_t nocc,
+                        const double *eps, double mu, const double *D, int64_t naux,
+                        const double *tau, int ntau, const double *Wt, const int64_t *states,
+                        int nstates, const double *sl_bar, const double *sg_bar,
+                        double *eps_bar, double *X_bar, double *D_bar, double *Wt_bar,
+                        void *ws, size_t ws_bytes, int *err, void *stream) {
+  (void)err;
+  Dims d(M, norb, nocc, naux);
+  if (!d.ok() || ntau < 1 || nstates < 1) return MBPT_ERR_SHAPE;
+  Arena ar = arena(ws, ws_bytes);
+  return sigma_back_run(X, d, eps, mu, D, tau, ntau, Wt, states, nstates, sl_bar, sg_bar,
+                        eps_bar, X_bar, D_bar, Wt_bar, ar, S(stream));
+}
+
+size_t mbpt_dyson_backward_workspace_bytes(int64_t naux) {
+  return sizeof(double) * static_cast<size_t>(naux) * naux + 2048;
+}
+
+int mbpt_dyson_backward(const double *w_minus_i, double *wbar, int64_t naux, int nfreq,
+                        void *ws, size_t ws_bytes, void *stream) {
+  if (naux < 1 || nfreq < 1) return MBPT_ERR_SHAPE;
+  Arena ar = arena(ws, ws_bytes);
+  return dyson_back_run(w_minus_i, wbar, naux, nfreq, ar, S(stream));
 }
 
 int mbpt_energy_adjoint_seed(double *wmi, int64_t naux, int nfreq, const double *ow_dev,

@@ -380,6 +380,20 @@ def minimax_points_for_gw(eps, nocc, mu=None, target=DEFAULT_TAU_TARGET,
                                      target=target, npoints_max=npoints_max)
 
 
+def sigma_transforms(eps, nocc, tau_points, omega_in, omega_out, mu=None, intermediate=None):
+    """(Ctw, C, S): the omega -> tau weights of W - I over rW and the tau ->
+    omega cosine and sine weights of Sigma over rS, on the caller's axes
+    (``Base/utils/grids/time_frequency.py:430-448``). Frozen per geometry, as
+    the reference treats them: not differentiated."""
+    if intermediate is not None:
+        raise NotImplementedError('an intermediate-orbital mask is outside the device route')
+    rW, rS = sigma_fit_ranges(eps, nocc, mu=mu)
+    Ctw = transform_weights(COSINE_WT, tau_points, omega_in, *rW)[0]
+    C = transform_weights(COSINE_TW, tau_points, omega_out, *rS)[0]
+    S = transform_weights(SINE_TW, tau_points, omega_out, *rS)[0]
+    return Ctw, C, S
+
+
 def transition_range(spectra, noccs):
     """(smallest, largest) particle-hole energy over every spin channel
     (``src/Base/orbital_spaces.py:23-29``)."""

@@ -77,16 +77,19 @@ def replacements():
                                     'static_screening_matrix_unrestricted')}
     return {
         LR: dict(seams),
-        IT: {k: v for k, v in seams.items()
-             if k in ('dyson_screening', 'polarizability_projected_sweep',
-                      'polarizability_projected_tau')},
+        IT: {**{k: v for k, v in seams.items()
+                if k in ('dyson_screening', 'polarizability_projected_sweep',
+                         'polarizability_projected_tau')},
+             'selfenergy_diag': adjoint.selfenergy_diag},
         ST: {'chi0_imaginary_frequency': space_time.chi0_imaginary_frequency,
              'dyson_screening': space_time.dyson_screening,
              '_sigma_mo_diagonal': _sigma_mo_diagonal, **static},
         BSE: dict(static),
         CD: dict(static),
         RF: dict(static),
-        ADJ: {'rpa_energy_and_adjoint': adjoint.rpa_energy_and_adjoint,
+        ADJ: {'selfenergy_diag_backward': adjoint.selfenergy_diag_backward,
+              'screened_interaction_tau_backward': adjoint.screened_interaction_tau_backward,
+              'rpa_energy_and_adjoint': adjoint.rpa_energy_and_adjoint,
               'rpa_correlation_energy_space_time':
                   space_time.rpa_correlation_energy_space_time,
               'chi0_imaginary_frequency': space_time.chi0_imaginary_frequency},

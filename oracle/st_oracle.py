@@ -465,6 +465,103 @@ def polarizability_backward(proj_bar, X, D, eps, nocc, tau_points, mu=None):
     return eps_bar, X_bar, D_bar
 
 
+# ---------------------------------------------------------------------------
+# self-energy diagonal in the auxiliary basis and its reverse
+# (GW/imaginary_time.py:632-661, 731-768; space_time_adjoint.py:593-691, 795-875)
+# ---------------------------------------------------------------------------
+
+def three_index_slice(X, D, p):
+    """LinearResponse/space_time.py:804-815: B_p[P, q] = sum_k D[k,P] X[k,p] X[k,q]."""
+    return D.T @ (X[:, p:p + 1] * X)
+
+
+def screened_interaction_tau(proj_tau, grid, Ctw):
+    """Wt(tau) = sum_w Ctw[tau, w] ([1 - chi0_w]^-1 - I), chi0 from proj(tau)."""
+    chi0 = np.tensordot(grid.cosft_wt, proj_tau, axes=(1, 0))
+    W = np.stack([dyson_screening(c, correlation=True) for c in chi0])
+    return np.tensordot(Ctw, W, axes=(1, 0))
+
+
+def selfenergy_diag(X, D, eps, nocc, grid, states, transforms, mu):
+    """GW/imaginary_time.py:731-768 (serial): Sigma^c_pp(i omega_out) and the
+    cache (proj_tau, Wt_tau, Bs), from the states' three-index slices."""
+    Ctw, C, S = transforms
+    eps = np.asarray(eps, float)
+    _, _, e_o, e_v, _ = split_branches(X, eps, nocc, mu)
+    proj = polarizability_projected_sweep(X, D, eps, nocc, grid.tau_points, mu)
+    Wt = screened_interaction_tau(proj, grid, Ctw)
+    states = np.atleast_1d(states)
+    Bs = np.stack([three_index_slice(X, D, int(p)) for p in states])
+    sig_l = np.zeros((len(grid.tau_points), len(states)))
+    sig_g = np.zeros_like(sig_l)
+    for k, tau in enumerate(grid.tau_points):
+        w, u = np.exp(e_o * tau), np.exp(-e_v * tau)
+        for s in range(len(states)):
+            bYb = np.einsum('Pq,Pq->q', Bs[s], Wt[k] @ Bs[s])
+            sig_l[k, s] = bYb[:nocc] @ w
+            sig_g[k, s] = -(bYb[nocc:] @ u)
+    sigma = -0.5 * ((sig_g + sig_l).T @ C.T + 1j * ((sig_g - sig_l).T @ S.T))
+    return sigma, (proj, Wt, Bs)
+
+
+def screened_interaction_tau_backward(Wt_bar, proj_tau, grid, Ctw):
+    """space_time_adjoint.py:652-691 (serial): chi0_bar = W W_bar W per
+    frequency, W rebuilt from proj(tau), folded back onto tau."""
+    chi0 = np.tensordot(grid.cosft_wt, proj_tau, axes=(1, 0))
+    Wbar = np.tensordot(Ctw, Wt_bar, axes=(0, 0))
+    eye = np.eye(chi0.shape[-1])
+    for f in range(len(chi0)):
+        Wf = np.linalg.inv(eye - chi0[f])
+        Wbar[f] = Wf @ Wbar[f] @ Wf
+    return np.tensordot(grid.cosft_wt.T, Wbar, axes=(1, 0))
+
+
+def three_index_slice_backward(X, D, p, Bp_bar, X_bar, D_bar):
+    """space_time_adjoint.py:593-624 with one row tile, accumulating."""
+    xp = X[:, p, None]
+    G = D @ Bp_bar
+    term = xp * G
+    term[:, p] += np.einsum('kq,kq->k', G, X)
+    X_bar += term
+    D_bar += xp * (X @ Bp_bar.T)
+
+
+def selfenergy_diag_backward(a_re, a_im, X, D, eps, nocc, grid, states, transforms, mu,
+                             cache):
+    """space_time_adjoint.py:795-875 (serial): (eps_bar, X_bar, D_bar) of
+    sum a_re Re Sigma + a_im Im Sigma."""
+    Ctw, C, S = transforms
+    eps = np.asarray(eps, float)
+    _, _, e_o, e_v, _ = split_branches(X, eps, nocc, mu)
+    proj, Wt, Bs = cache
+    states = np.atleast_1d(states)
+    ac, bs = a_re @ C, a_im @ S
+    sg_bar = -0.5 * (ac + bs).T
+    sl_bar = -0.5 * (ac - bs).T
+    eps_bar = np.zeros_like(eps)
+    Bs_bar = np.zeros_like(Bs)
+    Wt_bar = np.zeros_like(Wt)
+    c = np.empty(X.shape[1])
+    for k, tau in enumerate(grid.tau_points):
+        w, u = np.exp(e_o * tau), np.exp(-e_v * tau)
+        for s in range(len(states)):
+            b = Bs[s]
+            Y = Wt[k] @ b
+            c[:nocc] = sl_bar[k, s] * w
+            c[nocc:] = -sg_bar[k, s] * u
+            Bs_bar[s] += 2.0 * Y * c
+            Wt_bar[k] += (b * c) @ b.T
+            bYb = np.einsum('Pq,Pq->q', b, Y)
+            eps_bar[:nocc] += sl_bar[k, s] * tau * w * bYb[:nocc]
+            eps_bar[nocc:] += sg_bar[k, s] * tau * u * bYb[nocc:]
+    proj_bar = screened_interaction_tau_backward(Wt_bar, proj, grid, Ctw)
+    eps2, X_bar, D_bar = polarizability_backward(proj_bar, X, D, eps, nocc, grid.tau_points,
+                                                 mu)
+    for s, p in enumerate(states):
+        three_index_slice_backward(X, D, int(p), Bs_bar[s], X_bar, D_bar)
+    return eps_bar + eps2, X_bar, D_bar
+
+
 def rpa_energy_and_adjoint(X, D, eps, nocc, grid, mu=None):
     """space_time_adjoint.py:473-563, gas phase: (E_c, eps_bar, X_bar, D_bar)."""
     e_c, proj = rpa_correlation_energy(X, D, eps, nocc, grid, mu, want_proj=True)

@@ -24,6 +24,9 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
 * unrestricted.npz   the unrestricted route (two spin channels, one W from the
                      spin-summed chi0): grids, W - I, each channel's Sigma_c
                      diagonal, QP roots and Z;
+* sigma_adjoint.npz  the self-energy diagonal of three states and its adjoint
+                     (eps_bar, X_bar, D_bar) for seeded adjoints on Re and
+                     Im Sigma;
 * qp_kat.npz         the root finder on closed-form self-energies
                      (tests/test_qp_refine_root.py's two-pole Sigma and others);
 * c1_<variant>.npz   the synthetic FP64 configuration at full size (n_orb = 400,
@@ -33,7 +36,7 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      stored: the tests regenerate them from the seed and check
                      the regeneration against the stored eps and checksums.
 
-    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted]
+    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint]
 """
 import os
 import sys
@@ -71,7 +74,10 @@ from src.SingleReference.GW.imaginary_time import (                     # noqa: 
     unrestricted_screening_frequency_grid)
 from src.Base.orbital_spaces import transition_range                    # noqa: E402
 from src.Solvers.qp_equation import solve_qp_equation_pole_strength     # noqa: E402
-from src.gradients.rpa.space_time_adjoint import rpa_energy_and_adjoint  # noqa: E402
+from src.gradients.rpa.space_time_adjoint import (                      # noqa: E402
+    rpa_energy_and_adjoint, selfenergy_diag_backward)
+from src.SingleReference.GW.imaginary_time import selfenergy_diag        # noqa: E402
+from src.Base.utils.grids.time_frequency import sigma_transforms        # noqa: E402
 
 from mbptcode_b200.synthetic import synthetic_system                    # noqa: E402
 
@@ -280,6 +286,36 @@ def unrestricted_fixture(ntau=12):
     np.savez_compressed(os.path.join(HERE, 'unrestricted.npz'), **out)
 
 
+def sigma_adjoint_fixture(ntau=12, nfreq=10):
+    """The self-energy diagonal and its adjoint (GW/imaginary_time.py:731-768,
+    gradients/rpa/space_time_adjoint.py:795-875) on a small synthetic
+    system, set up as the reference's tests/test_kernel_lockstep.py sets them
+    up: Gauss-Legendre frequencies on the gap, the minimax tau axis over
+    (gap / 2, span), `sigma_transforms` on those axes; three states around
+    the gap and seeded adjoints on Re and Im Sigma."""
+    X, D, eps = synthetic_system(20, 4, 48, 21, 'calibrated')
+    nocc = 4
+    gap = eps[nocc] - eps[nocc - 1]
+    nu, wt = gauss_legendre_grid(nfreq, w0=gap)
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        grid = TimeFrequencyGrid.minimax_split(ntau, 0.5 * gap, eps[-1] - eps[0], nu, wt,
+                                               with_sine=False, with_inverse=False)
+        mu = 0.5 * (eps[nocc - 1] + eps[nocc])
+        transforms = sigma_transforms(eps, nocc, grid.tau_points, grid.omega_points,
+                                      grid.omega_points, mu=mu)
+    states = np.array([nocc - 1, nocc, nocc + 2])
+    a_re, a_im = np.random.default_rng(4).normal(size=(2, len(states), nfreq))
+    sigma, cache = selfenergy_diag(X, D, eps, nocc, grid, states, transforms, mu)
+    eps_bar, X_bar, D_bar = selfenergy_diag_backward(a_re, a_im, X, D, eps, nocc, grid, states,
+                                                     transforms, mu, cache)
+    np.savez_compressed(
+        os.path.join(HERE, 'sigma_adjoint.npz'), X=X, D=D, eps=eps, nocc=nocc, mu=mu,
+        states=states, tau=grid.tau_points, cosft_wt=grid.cosft_wt, omega=nu, omega_w=wt,
+        Ctw=transforms[0], C=transforms[1], S=transforms[2], a_re=a_re, a_im=a_im,
+        sigma=sigma, eps_bar=eps_bar, X_bar=X_bar, D_bar=D_bar)
+
+
 def qp_fixture():
     cases = {  # poles placed off the scan grids, so no division hits one
         'two_pole': (lambda w: 0.05 / (w + 0.8) + 0.01 / (w - 0.9), -0.2),
@@ -319,8 +355,12 @@ if __name__ == '__main__':
         unrestricted_fixture()
         print('unrestricted fixture written to', HERE)
         sys.exit(0)
+    if ONLY == 'sigma_adjoint':
+        sigma_adjoint_fixture()
+        print('self-energy adjoint fixture written to', HERE)
+        sys.exit(0)
     if ONLY:
-        sys.exit(f'--only {ONLY}: choose c1, static or unrestricted')
+        sys.exit(f'--only {ONLY}: choose c1, static, unrestricted or sigma_adjoint')
     grids_fixture()
     shared_kernel_fixture()
     route_fixture('calibrated', 24, 4, 64, 7, 'calibrated', 12, full=True)
@@ -329,4 +369,5 @@ if __name__ == '__main__':
     qp_fixture()
     static_fixture()
     unrestricted_fixture()
+    sigma_adjoint_fixture()
     print('fixtures written to', HERE)

@@ -108,6 +108,9 @@ def test_plugin_rebinds_and_restores_reference_names():
         bound, skipped = plugin.install()
         assert lr.chi0_imaginary_frequency is space_time.chi0_imaginary_frequency
         assert lr.static_screening_matrix is space_time.static_screening_matrix
+        it = importlib.import_module(plugin.IT)
+        from mbptcode_b200 import adjoint as adj_mod
+        assert it.selfenergy_diag is adj_mod.selfenergy_diag
         # the static screening's other importers need pyscf, absent here
         assert {plugin.BSE, plugin.CD, plugin.RF} <= set(skipped)
         assert 'dyson_screening' in bound[plugin.IT]

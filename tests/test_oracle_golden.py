@@ -176,3 +176,66 @@ def test_unrestricted_axes_and_oracle(golden):
         sig = g[f'sigma_{s}']
         assert np.abs(out['sigma'][s] - sig).max() <= 1e-10 * np.abs(sig).max()
         assert np.abs(out['roots'][s] - g[f'roots_{s}']).max() < 2e-6
+
+
+def _sigma_adjoint_case(g):
+    nu, wt = g['omega'], g['omega_w']
+    eps, nocc = g['eps'], int(g['nocc'])
+    gap = eps[nocc] - eps[nocc - 1]
+    with _quiet():
+        grid = grids.TimeFrequencyGrid.minimax_split(len(g['tau']), 0.5 * gap,
+                                                     eps[-1] - eps[0], nu, wt,
+                                                     with_sine=False, with_inverse=False)
+        tr = grids.sigma_transforms(eps, nocc, grid.tau_points, nu, nu, mu=float(g['mu']))
+    return grid, tr
+
+
+def test_sigma_adjoint_oracle_and_grid_space_form(golden):
+    """The self-energy diagonal and its adjoint: the axes and transforms are
+    the reference's bit for bit, the oracle (three-index form, as the
+    reference writes it) reproduces the reference's Sigma and
+    (eps_bar, X_bar, D_bar), and so does the grid-space form that
+    mbpt_sigma_backward evaluates on the device (restated here in NumPy:
+    Zt = D Wt D^T, the Hadamard reverse, Wt_bar = D^T Zt_bar D)."""
+    g = golden('sigma_adjoint')
+    X, D, eps, nocc, mu = g['X'], g['D'], g['eps'], int(g['nocc']), float(g['mu'])
+    grid, tr = _sigma_adjoint_case(g)
+    assert np.array_equal(grid.tau_points, g['tau'])
+    assert np.array_equal(grid.cosft_wt, g['cosft_wt'])
+    for a, k in zip(tr, ('Ctw', 'C', 'S')):
+        assert np.array_equal(a, g[k]), k
+    states = g['states']
+    sigma, cache = orc.selfenergy_diag(X, D, eps, nocc, grid, states, tr, mu)
+    assert np.abs(sigma - g['sigma']).max() <= 1e-12 * np.abs(g['sigma']).max()
+    out = orc.selfenergy_diag_backward(g['a_re'], g['a_im'], X, D, eps, nocc, grid, states,
+                                       tr, mu, cache)
+    for a, k in zip(out, ('eps_bar', 'X_bar', 'D_bar')):
+        assert np.abs(a - g[k]).max() <= 1e-10 * np.abs(g[k]).max(), k
+    # the grid-space reverse of the self-energy sweep, step for step as on the device
+    proj, Wt, _ = cache
+    ac, bs = g['a_re'] @ tr[1], g['a_im'] @ tr[2]
+    sl, sg = -0.5 * (ac - bs).T, -0.5 * (ac + bs).T
+    Xo, Xv = X[:, :nocc], X[:, nocc:]
+    eb, xb, db, wtb = np.zeros_like(eps), np.zeros_like(X), np.zeros_like(D), np.zeros_like(Wt)
+    Xs = X[:, states]
+    for k, tau in enumerate(grid.tau_points):
+        w, u = np.exp((eps[:nocc] - mu) * tau), np.exp(-(eps[nocc:] - mu) * tau)
+        Go, Gv = (Xo * w) @ Xo.T, (Xv * u) @ Xv.T
+        U = D @ Wt[k]
+        Zt = U @ D.T
+        Xl, Xg = Xs * sl[k], Xs * sg[k]
+        Al, Ag = Xl @ Xs.T, Xg @ Xs.T
+        Zb, Gob, Gvb, L, H = Go * Al - Gv * Ag, Zt * Al, -Zt * Ag, Go * Zt, Gv * Zt
+        np.add.at(xb.T, states, 2.0 * (L @ Xl - H @ Xg).T)
+        GoX, GvX = Gob @ Xo, Gvb @ Xv
+        xb[:, :nocc] += 2.0 * GoX * w
+        xb[:, nocc:] += 2.0 * GvX * u
+        eb[:nocc] += tau * w * np.einsum('ri,ri->i', Xo, GoX)
+        eb[nocc:] -= tau * u * np.einsum('ra,ra->a', Xv, GvX)
+        T = Zb @ D
+        wtb[k] = D.T @ T
+        db += 2.0 * T @ Wt[k]
+    pb = orc.screened_interaction_tau_backward(wtb, proj, grid, tr[0])
+    e2, x2, d2 = orc.polarizability_backward(pb, X, D, eps, nocc, grid.tau_points, mu)
+    for a, k in zip((eb + e2, xb + x2, db + d2), ('eps_bar', 'X_bar', 'D_bar')):
+        assert np.abs(a - g[k]).max() <= 1e-10 * np.abs(g[k]).max(), k
