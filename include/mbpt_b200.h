@@ -149,6 +149,12 @@ int mbpt_energy_sum(const double *logdet_dev, const double *trace_dev,
  *   out[j] = sum_k w[j, k] in[k],   in (K, n, n), out (J, n, n), w_dev (J x K). */
 int mbpt_transform(const double *in_dev, int K, int64_t n, const double *w_dev, int J,
                    double *out_dev, void *stream);
+/* The same transform added onto out: out[j] += sum_k w[j, k] in[k]. One
+ * frequency block's share of W(tau) in the blocked screening of
+ * GW/imaginary_time.py:230-348 (`screened_interaction_tau_blocked`,
+ * freq_block), which holds chi0 for a block of frequencies only. */
+int mbpt_transform_acc(const double *in_dev, int K, int64_t n, const double *w_dev, int J,
+                       double *out_dev, void *stream);
 
 /* ---- self-energy branch sums --------------------------------------------
  * Replaces GW/imaginary_time.py:403-533 self_energy_matrix_imaginary_time

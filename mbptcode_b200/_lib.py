@@ -41,6 +41,7 @@ _SIGNATURES = {
     'mbpt_rpa_energy': (_i, [_p, _i64, _i64, _i64, _p, _d, _p, _i64, _p, _i, _p, _p, _i, _i,
                              _p, _p, _p, _p, _sz, _p, _p]),
     'mbpt_transform': (_i, [_p, _i, _i64, _p, _i, _p, _p]),
+    'mbpt_transform_acc': (_i, [_p, _i, _i64, _p, _i, _p, _p]),
     'mbpt_sigma_workspace_bytes': (_sz, [_i64, _i64, _i64, _i64, _i, _i, _i]),
     'mbpt_sigma_branch_sums': (_i, [_p, _i64, _i64, _i64, _p, _d, _p, _i64, _p, _p, _i, _p,
                                     _i, _i, _p, _p, _sz, _p, _p]),

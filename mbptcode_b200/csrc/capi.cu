@@ -1102,6 +1102,14 @@ int mbpt_transform(const double *in, int K, int64_t n, const double *w_dev, int 
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 
+int mbpt_transform_acc(const double *in, int K, int64_t n, const double *w_dev, int J,
+                       double *out, void *stream) {
+  if (K < 1 || J < 1 || K > 34 || J > 34 || n < 1) return MBPT_ERR_SHAPE;
+  cudaStream_t st = S(stream);
+  launch_transform_acc(in, n * n, n, n, n, w_dev, J, K, out, n * n, n, st);
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
 size_t mbpt_sigma_workspace_bytes(int64_t M, int64_t norb, int64_t nocc, int64_t naux, int ntau,
                                   int nstates, int mode) {
   Dims d(M, norb, nocc, naux);

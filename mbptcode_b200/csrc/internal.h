@@ -92,6 +92,10 @@ template <typename Tin>
 void launch_transform(const Tin *in, int64_t in_slice, int64_t ld_in, int64_t rows,
                       int64_t cols, const double *w_dev, int J, int K, double *out,
                       int64_t out_slice, int64_t ld_out, cudaStream_t st);
+// out[j] += sum_k w[j,k] in[k] (FP64)
+void launch_transform_acc(const double *in, int64_t in_slice, int64_t ld_in, int64_t rows,
+                          int64_t cols, const double *w_dev, int J, int K, double *out,
+                          int64_t out_slice, int64_t ld_out, cudaStream_t st);
 void launch_transform_split(const double *in, int64_t in_slice, int64_t ld_in, int64_t rows,
                             int64_t cols, const double *w_dev, int J, int K, bf16 *out_hi,
                             bf16 *out_lo, int64_t out_slice, int64_t ld_out, cudaStream_t st);

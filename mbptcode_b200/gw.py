@@ -131,15 +131,57 @@ class SweepResult(dict):
     host arrays), with `timings` in seconds per stage (CUDA events)."""
 
 
+def screened_tau_blocked(X, D, eps, nocc, axes, freq_block, precision=None, stream=None,
+                         err=None, out=None):
+    """W(tau) = sum_w Ctw[tau, w] (W(i w) - I) with chi0 held for `freq_block`
+    frequencies at a time (``GW/imaginary_time.py:230-348``,
+    `screened_interaction_tau_blocked`): per block the chi0 sweep onto the
+    block's frequencies (the tau sweep recomputed, a factor nfreq/freq_block
+    in its time), the Dyson step, and the block's share added onto W(tau).
+    Returns (Wt, logdet, trace, info) over all frequencies."""
+    dev = require_device()
+    grid = axes.grid
+    nfreq, nb = grid.nfreq, int(freq_block)
+    if nb < 1:
+        raise ValueError(f'freq_block must be positive, got {freq_block}')
+    naux = D.shape[1]
+    cw, Ctw = np.asarray(grid.cosft_wt, float), np.asarray(axes.Ctw, float)
+    Wt = out if out is not None else torch.empty((len(Ctw), naux, naux), dtype=torch.float64,
+                                                 device=dev)
+    logdet = torch.empty(nfreq, dtype=torch.float64, device=dev)
+    trace = torch.empty(nfreq, dtype=torch.float64, device=dev)
+    info = np.zeros(nfreq, dtype=np.int32)
+    blk = BUFFERS.take('sweep_chi0', (min(nb, nfreq), naux, naux), dev)
+    ctx = torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext()
+    with ctx:
+        Wt.zero_()
+    for f0 in range(0, nfreq, nb):
+        f1 = min(f0 + nb, nfreq)
+        c = blk[:f1 - f0]
+        chi0_sweep(X, D, eps, nocc, grid.tau_points, cw[f0:f1], mu=axes.mu,
+                   precision=precision, stream=stream, out=c, err=err)
+        ld, tr, inf, _ = dyson_batch(c, want_w=True, stream=stream, precision=precision,
+                                     err=err)
+        with ctx:
+            logdet[f0:f1].copy_(ld)
+            trace[f0:f1].copy_(tr)
+        info[f0:f1] = inf
+        transform(c, np.ascontiguousarray(Ctw[:, f0:f1]), stream, out=Wt, accumulate=True)
+    return Wt, logdet, trace, info
+
+
 def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=None,
              eps_anchor=None, xc_diagonal=None, greedy=True, warm=None, keep=False,
-             stream=None, timings=None):
+             stream=None, timings=None, freq_block=None):
     """The whole space-time G0W0 sweep on device-resident (or host) inputs.
 
     Returns a SweepResult with 'roots', 'z', 'flags', 'evals' (device),
     'sigma' (nstates, npade) complex, 'axes', and with `keep` also 'Wt' and
     'W_minus_I'. eps_anchor: the spectrum the equation is anchored on (evGW);
     None is eps. timings: a dict receiving per-stage device times.
+    freq_block: hold chi0 for that many frequencies at a time
+    (`screened_tau_blocked`; 't_chi0' then times the whole blocked build of
+    W(tau) and 't_dyson' is zero); W - I is then not kept.
     """
     dev = require_device()
     # host inputs cross to the device once, here (both halves of the sweep read them)
@@ -160,6 +202,19 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
         ev[0].record()
     naux = D.shape[1]
+    if freq_block is not None and int(freq_block) < axes.grid.nfreq:
+        Wt, logdet, trace, info = screened_tau_blocked(
+            X, D, eps_h, nocc, axes, freq_block, precision, stream, err,
+            out=None if keep else BUFFERS.take('sweep_wt', (len(axes.Ctw), naux, naux), dev))
+        if ev:
+            ev[1].record()
+            ev[2].record()
+        e_c = torch.empty((), dtype=torch.float64, device=dev)
+        ow = torch.as_tensor(np.asarray(axes.grid.omega_weights, float), device=dev)
+        check(lib().mbpt_energy_sum(ptr(logdet), ptr(trace), ptr(ow), len(ow), ptr(e_c),
+                                    stream_ptr(stream)), 'mbpt_energy_sum')
+        return _sweep_tail(X, D, eps_h, nocc, states, axes, precision, eps_anchor, xc_diagonal,
+                           greedy, warm, keep, stream, timings, err, ev, Wt, None, info, e_c)
     # the two 10 GB-class intermediates come from the per-device buffer cache
     # unless the caller keeps them
     chi0, _ = chi0_sweep(X, D, eps_h, nocc, axes.grid.tau_points, axes.grid.cosft_wt, mu=mu,
@@ -182,6 +237,15 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
         out=None if keep else BUFFERS.take('sweep_wt', (len(axes.Ctw), naux, naux), dev))
     W_minus_I = chi0 if keep else None
     del chi0
+    return _sweep_tail(X, D, eps_h, nocc, states, axes, precision, eps_anchor, xc_diagonal,
+                       greedy, warm, keep, stream, timings, err, ev, Wt, W_minus_I, info, e_c)
+
+
+def _sweep_tail(X, D, eps_h, nocc, states, axes, precision, eps_anchor, xc_diagonal, greedy,
+                warm, keep, stream, timings, err, ev, Wt, W_minus_I, info, e_c):
+    """The self-energy half of `gw_sweep` from W(tau): branch sums, Sigma(i w),
+    the (warm-started) QP solve, and the result."""
+    mu = axes.mu
     branch = sigma_branch_sums(X, D, Wt, eps_h, nocc, axes.tau_sigma, states, mu, precision,
                                stream, err=err)
     sigma = sigma_frequency(branch, axes.C, axes.S, stream)
@@ -335,11 +399,14 @@ def solve_qp_energy_space_time(mf, mol, nocc, p_state, numerics=None, auxbasis=N
     the static term <Sigma_x - v_xc> is `xc_diagonal` (0 on an HF reference,
     ``qp_solve.py:311``). numerics.quadrature: ntau_st ('auto' or a size),
     npade and w0_gl. Returns Hartree, a float for a scalar p_state."""
-    for name, val in (('distribute', distribute), ('freq_block', freq_block),
-                      ('scratch_dir', scratch_dir), ('screen_r_cut', screen_r_cut),
+    for name, val in (('distribute', distribute), ('screen_r_cut', screen_r_cut),
                       ('sigma_x_matrix', sigma_x_matrix), ('extras', extras)):
         if val:
             raise NotImplementedError(f'{name} is outside the one-GPU device route')
+    if scratch_dir:
+        raise NotImplementedError(
+            'scratch_dir caches proj(tau) on disk between frequency blocks; the device '
+            'recomputes the tau sweep per block instead (freq_block alone)')
     X, D = _factors(factors)
     eps = np.asarray(getattr(mf, 'mo_energy', mf), float)
     ntau, pade = 'auto', None
@@ -350,6 +417,10 @@ def solve_qp_energy_space_time(mf, mol, nocc, p_state, numerics=None, auxbasis=N
         pade = pade_nodes(q.npade, q.w0_gl)
     states = np.atleast_1d(p_state)
     if eps.ndim == 2:
+        if freq_block:
+            raise NotImplementedError(
+                'freq_block on an unrestricted reference: the blocked path is built for one '
+                'spin; run it unblocked')
         roots, z, evals = _unrestricted_channel(mf, nocc, states, factors, D, eps, ntau, pade,
                                                 spin_channel, eps_anchor, xc_diagonal,
                                                 greedy, precision, timings)
@@ -363,7 +434,7 @@ def solve_qp_energy_space_time(mf, mol, nocc, p_state, numerics=None, auxbasis=N
                            anchor=None if eps_anchor is None else np.asarray(eps_anchor))
     res = gw_sweep(X, D, eps, nocc, states=states, axes=axes, precision=precision,
                    eps_anchor=eps_anchor, xc_diagonal=xc_diagonal, greedy=greedy,
-                   timings=timings)
+                   timings=timings, freq_block=freq_block)
     if timings is not None:
         timings['ntau_auto'] = axes.ntau
         timings['tau_fit_error'] = axes.tau_fit_error

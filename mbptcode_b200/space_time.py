@@ -413,20 +413,24 @@ def rpa_correlation_energy_space_time(X, D, eps, nocc, grid, mu=None, tile_gb=No
     return value, SimpleNamespace(proj_tau=back(proj, X), tau_indices=None, freq_indices=None)
 
 
-def transform(values, weights, stream=None, out=None):
+def transform(values, weights, stream=None, out=None, accumulate=False):
     """sum_k weights[j, k] values[k] over (K, n, n) device tensors, FP64
-    (into `out`, a contiguous (J, n, n) FP64 array, when given)."""
+    (into `out`, a contiguous (J, n, n) FP64 array, when given; added onto
+    `out` with `accumulate`)."""
     dev = values.device
     K, n = values.shape[0], values.shape[-1]
     w = torch.as_tensor(np.ascontiguousarray(weights, dtype=np.float64), device=dev)
     J = w.shape[0]
     if out is None:
+        if accumulate:
+            raise ValueError('accumulate needs out')
         out = torch.empty((J, n, n), dtype=torch.float64, device=dev)
     elif tuple(out.shape) != (J, n, n) or out.dtype != torch.float64 or not out.is_contiguous():
         raise ValueError(f'out must be a contiguous FP64 ({J}, {n}, {n}) array')
     vc = values.contiguous()  # held until the call has launched its kernel
-    check(lib().mbpt_transform(ptr(vc), K, n, ptr(w), J, ptr(out),
-                               stream_ptr(stream)), 'mbpt_transform')
+    fn = lib().mbpt_transform_acc if accumulate else lib().mbpt_transform
+    check(fn(ptr(vc), K, n, ptr(w), J, ptr(out), stream_ptr(stream)),
+          'mbpt_transform_acc' if accumulate else 'mbpt_transform')
     return out
 
 

@@ -402,3 +402,43 @@ def test_unrestricted_driver_channel(golden):
     assert np.array_equal(got, ref['channels'][1]['roots'].cpu().numpy())
     with pytest.raises(ValueError):
         gw.solve_qp_energy_space_time(MF, None, (n, n), 0, factors=(X, D))
+
+
+@pytest.mark.parametrize('precision', ['fp64', 'mixed'])
+def test_frequency_blocked_screening(golden, precision):
+    """freq_block: chi0 held for 5 of the 12 frequencies at a time (blocks of
+    5, 5, 2; the tau sweep recomputed per block) gives the unblocked sweep's
+    W(tau), E_c and roots up to the order of the W(tau) sums, and, in FP64,
+    the reference's Sigma_c diagonal."""
+    g = golden('route_calibrated')
+    X, D, eps, nocc = g['X'], g['D'], g['eps'], int(g['nocc'])
+    axes = grids.space_time_axes(eps, nocc, ntau=int(g['ntau']))
+    full = gw.gw_sweep(X, D, eps, nocc, axes=axes, precision=precision, keep=True)
+    blk = gw.gw_sweep(X, D, eps, nocc, axes=axes, precision=precision, keep=True, freq_block=5)
+    assert rel(blk['Wt'].cpu().numpy(), full['Wt'].cpu().numpy()) < 1e-12
+    assert abs(float(blk['e_c']) - float(full['e_c'])) <= 1e-12 * abs(float(full['e_c']))
+    assert np.array_equal(blk['dyson_info'], full['dyson_info'])
+    r_b, r_f = blk['roots'].cpu().numpy(), full['roots'].cpu().numpy()
+    f = frontier(nocc, len(eps))
+    assert np.abs(r_b[f] - r_f[f]).max() < 1e-9
+    if precision == 'fp64':
+        assert rel(blk['sigma'].cpu().numpy(), g['sigma']) < 1e-9
+
+
+def test_driver_freq_block_and_scratch_dir(golden):
+    g = golden('route_calibrated')
+    X, D, eps, nocc = g['X'], g['D'], g['eps'], int(g['nocc'])
+    states = np.arange(nocc - 2, nocc + 2)
+
+    class Quad:
+        ntau_st, npade, w0_gl = int(g['ntau']), 16, 1.0
+
+    class Num:
+        quadrature = Quad
+    a = gw.solve_qp_energy_space_time(eps, None, nocc, states, numerics=Num, factors=(X, D))
+    b = gw.solve_qp_energy_space_time(eps, None, nocc, states, numerics=Num, factors=(X, D),
+                                      freq_block=4)
+    assert np.abs(a - b).max() < 1e-9
+    with pytest.raises(NotImplementedError):
+        gw.solve_qp_energy_space_time(eps, None, nocc, states, numerics=Num, factors=(X, D),
+                                      freq_block=4, scratch_dir='/tmp/x')
