@@ -289,6 +289,120 @@ __global__ void scatter_cols_kernel(const double *__restrict__ T, int64_t M, int
   }
 }
 
+// ------------------------------------------------ batched blocked Cholesky
+// One 128-column step of the left-looking Cholesky of a batch of column-major
+// n x n matrices (the lower factor, as cuSOLVER's lower-fill potrf leaves it;
+// the strict upper triangle is never written).
+constexpr int kCholNb = 128;
+constexpr int kCholStride = kCholNb + 2;  // (stride + 1) odd: row c of lane c in its own bank
+
+// P_f (m x nbj, column-major, ld m) <- the block column A_f[j0:, j0:j0+nbj]
+__global__ void chol_copy_panel_kernel(const double *__restrict__ A, int64_t n, int64_t j0,
+                                       int64_t m, int nbj, double *__restrict__ P) {
+  const double *a = A + static_cast<int64_t>(blockIdx.y) * n * n;
+  double *p = P + static_cast<int64_t>(blockIdx.y) * m * nbj;
+  const int64_t total = m * nbj;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t c = i / m, r = i % m;
+    p[i] = a[(j0 + c) * n + j0 + r];
+  }
+}
+
+// One CTA (512 threads) per matrix: the updated diagonal block (the top nbj
+// rows of P_f) is factorised in shared memory, right-looking: per column c
+// the column is scaled by 1/sqrt of its pivot (and copied to a contiguous
+// vector), then the rank-1 update of the rest runs one row per warp with the
+// lanes on consecutive columns, so the shared-memory accesses are free of
+// bank conflicts. Its lower factor goes into A_f's diagonal block (lower
+// triangle and diagonal only). The inverse X = L^-1 is formed one thread per
+// column by forward substitution, X kept transposed (column c of X in row c
+// of the strict upper triangle; the row stride makes the lanes' rows fall in
+// different banks), four independent partial sums per thread, and written to
+// Linv_f (column-major, ld kCholNb, zeros above the diagonal). A pivot that
+// is not positive records info_f = its global column + 1 (the first one
+// only), as potrf does; the factor of that matrix is then not meaningful.
+__global__ void __launch_bounds__(512) chol_diag_block_kernel(
+    const double *__restrict__ P, int64_t m, int nbj, double *A, int64_t n, int64_t j0,
+    double *__restrict__ Linv, int *info) {
+  extern __shared__ double sm[];
+  double *s = sm;                                  // nbj x nbj, row stride kCholStride
+  double *diag = sm + kCholNb * kCholStride;       // L_cc
+  double *xdiag = diag + kCholNb;                  // (L^-1)_cc
+  double *colc = xdiag + kCholNb;                  // the scaled column c
+  __shared__ int bad;
+  const int f = blockIdx.x, tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
+  const double *p = P + static_cast<int64_t>(f) * m * nbj;
+  double *a = A + static_cast<int64_t>(f) * n * n;
+  if (tid == 0) bad = -1;
+  // the tile, eight independent loads in flight per thread before any store
+  const int tot = nbj * nbj;
+  for (int i0 = tid; i0 < tot; i0 += 8 * blockDim.x) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int i = i0 + u * blockDim.x;
+      const int c = i / nbj, r = i % nbj;
+      v[u] = (i < tot && r >= c) ? p[static_cast<int64_t>(c) * m + r] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i < tot) s[(i % nbj) * kCholStride + i / nbj] = v[u];
+    }
+  }
+  __syncthreads();
+  for (int c = 0; c < nbj; ++c) {
+    // the pivot's square root and reciprocal only where they are used
+    if (tid == 0) {
+      const double d = s[c * kCholStride + c];
+      diag[c] = sqrt(d);
+      if (!(d > 0.0) && bad < 0) bad = c;
+    }
+    if (tid > c && tid < nbj) {
+      const double v = s[tid * kCholStride + c] / sqrt(s[c * kCholStride + c]);
+      s[tid * kCholStride + c] = v;
+      colc[tid] = v;
+    }
+    __syncthreads();
+    for (int r = c + 1 + warp; r < nbj; r += nwarps) {
+      const double lr = colc[r];
+      double *row = s + r * kCholStride;
+      for (int k = c + 1 + lane; k <= r; k += 32) row[k] -= lr * colc[k];
+    }
+    __syncthreads();
+  }
+  if (tid < nbj) xdiag[tid] = 1.0 / diag[tid];
+  __syncthreads();
+  // x_c = 1 / L_cc, x_r = -(sum_{c <= i < r} L_ri x_i) / L_rr, x_i (i > c) at s[c][i]
+  if (tid < nbj) {
+    const int c = tid;
+    const double *xc = s + c * kCholStride;
+    for (int r = c + 1; r < nbj; ++r) {
+      const double *lr = s + r * kCholStride;
+      double a0 = lr[c] * xdiag[c], a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      int i = c + 1;
+      for (; i + 3 < r; i += 4) {
+        a0 = fma(lr[i], xc[i], a0);
+        a1 = fma(lr[i + 1], xc[i + 1], a1);
+        a2 = fma(lr[i + 2], xc[i + 2], a2);
+        a3 = fma(lr[i + 3], xc[i + 3], a3);
+      }
+      for (; i < r; ++i) a0 = fma(lr[i], xc[i], a0);
+      s[c * kCholStride + r] = -((a0 + a1) + (a2 + a3)) * xdiag[r];
+    }
+  }
+  __syncthreads();
+  double *ld = Linv + static_cast<int64_t>(f) * kCholNb * kCholNb;
+  for (int i = tid; i < nbj * nbj; i += blockDim.x) {
+    const int c = i / nbj, r = i % nbj;
+    if (r >= c) a[(j0 + c) * n + j0 + r] = r == c ? diag[c] : s[r * kCholStride + c];
+    ld[c * kCholNb + r] = r == c ? xdiag[c] : (r > c ? s[c * kCholStride + r] : 0.0);
+  }
+  if (tid == 0 && bad >= 0 && info[f] == 0) info[f] = static_cast<int>(j0) + bad + 1;
+}
+
 }  // namespace
 
 void launch_chi0_bar_seed(double *a, int64_t n, int nfreq, const double *w, cudaStream_t st) {
@@ -380,6 +494,25 @@ void launch_scatter_cols(const double *T, int64_t M, int64_t S, const int64_t *s
                          double scale, double *X_bar, int64_t n, cudaStream_t st) {
   count_launch();
   scatter_cols_kernel<<<blocks(M * S), 256, 0, st>>>(T, M, S, states, scale, X_bar, n);
+}
+
+void launch_chol_copy_panel(const double *A, int64_t n, int64_t j0, int64_t m, int nbj,
+                            int nmat, double *P, cudaStream_t st) {
+  dim3 grid(static_cast<unsigned>(blocks(m * nbj)), nmat);
+  count_launch();
+  chol_copy_panel_kernel<<<grid, 256, 0, st>>>(A, n, j0, m, nbj, P);
+}
+
+int launch_chol_diag_block(const double *P, int64_t m, int nbj, double *A, int64_t n,
+                           int64_t j0, int nmat, double *Linv, int *info, cudaStream_t st) {
+  if (nbj < 1 || nbj > kCholNb) return MBPT_ERR_SHAPE;
+  const size_t smem = sizeof(double) * (kCholNb * kCholStride + 3 * kCholNb);
+  if (cudaFuncSetAttribute(chol_diag_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem)) != cudaSuccess)
+    return MBPT_ERR_CUDA;
+  count_launch();
+  chol_diag_block_kernel<<<nmat, 512, smem, st>>>(P, m, nbj, A, n, j0, Linv, info);
+  return MBPT_OK;
 }
 
 }  // namespace mbpt

@@ -42,6 +42,10 @@ int launch_trtri_diag_blocks(double *A, int64_t n, int64_t lda, int nb, cudaStre
                              float *r_lo = nullptr, int64_t ldp = 0);
 void launch_strided_to_tf32(const double *src, int64_t rows, int64_t k, int64_t rs, int64_t cs,
                             float *hi, float *lo, int64_t rows_p, int64_t k_p, cudaStream_t st);
+void launch_chol_copy_panel(const double *A, int64_t n, int64_t j0, int64_t m, int nbj,
+                            int nmat, double *P, cudaStream_t st);
+int launch_chol_diag_block(const double *P, int64_t m, int nbj, double *A, int64_t n,
+                           int64_t j0, int nmat, double *Linv, int *info, cudaStream_t st);
 void launch_sigma_back_gather(const double *X, int64_t M, int64_t n, const int64_t *states,
                               int64_t S, const double *sl, const double *sg, double *Xs,
                               double *Xl, double *Xg, cudaStream_t st);
@@ -416,6 +420,59 @@ int spd_inverse_from_factor(Handles &h, double *L, int64_t n, double *T, double 
   return MBPT_OK;
 }
 
+constexpr int kCholNb = 128;     // block columns of the batched Cholesky
+constexpr int kBatchedCholMin = 4;  // frequencies from which the batch beats one potrf each
+
+// Left-looking blocked Cholesky of nmat column-major n x n SPD matrices at
+// once (A_f = L_f L_f^T, L_f in the lower triangle, the strict upper triangle
+// untouched, info_f as potrf reports it). Per 128-column step j0, for all
+// matrices in one launch each: the block column is copied to P, updated by
+// one strided-batched DGEMM P -= L[j0:, :j0] L[j0:j0+nb, :j0]^T (inner
+// dimension j0, so the FP64 GEMMs run long), its diagonal block factorised
+// and inverted in shared memory, and the panel below it formed by a second
+// batched DGEMM, L[j0+nb:, j0-block] = P_below L_jj^-T. Every launch carries
+// the whole batch, so the latency-bound diagonal blocks cost one launch per
+// step for all frequencies. P: nmat * n * kCholNb doubles; Linv: nmat *
+// kCholNb^2 doubles; info: nmat ints, zeroed by the caller.
+int chol_batched(double *A, int64_t n, int nmat, int *info, double *P, double *Linv,
+                 cublasHandle_t h, cudaStream_t st) {
+  const long long n2 = static_cast<long long>(n) * n;
+  const double one = 1.0, minus = -1.0, zero = 0.0;
+  for (int64_t j0 = 0; j0 < n; j0 += kCholNb) {
+    const int nbj = static_cast<int>(std::min<int64_t>(kCholNb, n - j0));
+    const int64_t m = n - j0;
+    launch_chol_copy_panel(A, n, j0, m, nbj, nmat, P, st);
+    if (j0 > 0 &&
+        cublasDgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_T, static_cast<int>(m), nbj,
+                                  static_cast<int>(j0), &minus, A + j0, static_cast<int>(n), n2,
+                                  A + j0, static_cast<int>(n), n2, &one, P,
+                                  static_cast<int>(m), static_cast<long long>(m) * nbj,
+                                  nmat) != CUBLAS_STATUS_SUCCESS)
+      return MBPT_ERR_CUDA;
+    int rc = launch_chol_diag_block(P, m, nbj, A, n, j0, nmat, Linv, info, st);
+    if (rc) return rc;
+    const int64_t mb = m - nbj;
+    if (mb > 0 &&
+        cublasDgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_T, static_cast<int>(mb), nbj, nbj,
+                                  &one, P + nbj, static_cast<int>(m),
+                                  static_cast<long long>(m) * nbj, Linv, kCholNb,
+                                  static_cast<long long>(kCholNb) * kCholNb, &zero,
+                                  A + j0 * n + j0 + nbj, static_cast<int>(n), n2,
+                                  nmat) != CUBLAS_STATUS_SUCCESS)
+      return MBPT_ERR_CUDA;
+  }
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+bool batched_chol_enabled(int nfreq) {
+  // MBPT_DYSON_BATCHED=0 keeps one cuSOLVER potrf per frequency
+  static const int env = [] {
+    const char *e = std::getenv("MBPT_DYSON_BATCHED");
+    return e ? std::atoi(e) : 1;
+  }();
+  return env != 0 && nfreq >= kBatchedCholMin;
+}
+
 struct DysonBufs {
   int *info;
   int *piv;
@@ -425,6 +482,7 @@ struct DysonBufs {
   double *diag;  // nfreq x n diagonals of 1 - chi0, which the factorisation overwrites
   double *T;     // diagonal-block scratch of the LAUUM
   PairScratch pairs;  // mixed mode: TF32 pairs of the tensor-core inverse
+  double *chol_P = nullptr, *chol_Linv = nullptr;  // batched Cholesky scratch
   int lwork;
 };
 
@@ -449,6 +507,10 @@ DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq, int mode = MBPT_MODE_FP64
   b.rhs = ar.take<double>(n * n);
   b.diag = ar.take<double>(n * static_cast<int64_t>(nfreq));
   b.T = ar.take<double>(kLauumBlock * kLauumBlock);
+  if (batched_chol_enabled(nfreq)) {
+    b.chol_P = ar.take<double>(static_cast<int64_t>(nfreq) * n * kCholNb);
+    b.chol_Linv = ar.take<double>(static_cast<int64_t>(nfreq) * kCholNb * kCholNb);
+  }
   if (mode == MBPT_MODE_MIXED) {
     const int64_t np = round_up(n, 128), cap = np * np;
     PairScratch &q = b.pairs;
@@ -472,6 +534,7 @@ struct DysonPipe {
   // panels between DGEMM-bound updates) share the GPU
   cudaStream_t fac2 = nullptr;
   cusolverDnHandle_t solver2 = nullptr;
+  cublasHandle_t blas2 = nullptr;  // the second half of a batched factorisation
   cudaEvent_t fork = nullptr, join2 = nullptr;
   int nfac = 1;
   std::vector<cudaEvent_t> ev;
@@ -500,7 +563,9 @@ DysonPipe *dyson_pipe(int nfreq) {
               cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreateWithFlags(&p->join2, cudaEventDisableTiming) == cudaSuccess &&
               cusolverDnCreate(&p->solver2) == CUSOLVER_STATUS_SUCCESS &&
-              cusolverDnSetStream(p->solver2, p->fac2) == CUSOLVER_STATUS_SUCCESS;
+              cusolverDnSetStream(p->solver2, p->fac2) == CUSOLVER_STATUS_SUCCESS &&
+              cublasCreate(&p->blas2) == CUBLAS_STATUS_SUCCESS &&
+              cublasSetStream(p->blas2, p->fac2) == CUBLAS_STATUS_SUCCESS;
   }
   while (p->ok && static_cast<int>(p->ev.size()) < nfreq) {
     cudaEvent_t e = nullptr;
@@ -543,11 +608,40 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
                      b.pairs.ir_lo, b.pairs.tt_hi, b.pairs.tt_lo})
       if (cudaMemsetAsync(f, 0, bytes, st) != cudaSuccess) return MBPT_ERR_CUDA;
   }
-  const int nfac = nfreq > 1 ? pp->nfac : 1;
+  // many frequencies: one batched factorisation of all of them, then the
+  // per-frequency loop below only reads their info words
+  const bool batched = b.chol_P != nullptr;
+  if (batched) {
+    if (cudaMemsetAsync(b.info, 0, sizeof(int) * nfreq, st) != cudaSuccess) return MBPT_ERR_CUDA;
+    // two halves on two streams: one half's DGEMMs fill the GPU while the
+    // other half's diagonal blocks (one CTA per matrix) are factorised
+    const int half = pp->nfac == 2 && nfreq >= 2 * kBatchedCholMin ? nfreq / 2 : nfreq;
+    if (half < nfreq && (cudaEventRecord(pp->fork, st) != cudaSuccess ||
+                         cudaStreamWaitEvent(pp->fac2, pp->fork, 0) != cudaSuccess))
+      return MBPT_ERR_CUDA;
+    int rc0 = chol_batched(chi0, n, half, b.info, b.chol_P, b.chol_Linv, h.blas, st);
+    if (!rc0 && half < nfreq)
+      rc0 = chol_batched(chi0 + half * n * n, n, nfreq - half, b.info + half,
+                         b.chol_P + static_cast<int64_t>(half) * n * kCholNb,
+                         b.chol_Linv + static_cast<int64_t>(half) * kCholNb * kCholNb,
+                         pp->blas2, pp->fac2);
+    if (half < nfreq && (cudaEventRecord(pp->join2, pp->fac2) != cudaSuccess ||
+                         cudaStreamWaitEvent(st, pp->join2, 0) != cudaSuccess))
+      return MBPT_ERR_CUDA;
+    if (rc0) return rc0;
+    launch_logdet_diag(chi0, n, nfreq, logdet, st);
+    if (cudaMemcpyAsync(pp->info, b.info, sizeof(int) * nfreq, cudaMemcpyDeviceToHost, st) !=
+        cudaSuccess)
+      return MBPT_ERR_CUDA;
+    for (int f = 0; f < nfreq; ++f)
+      if (cudaEventRecord(pp->ev[f], st) != cudaSuccess) return MBPT_ERR_CUDA;
+  }
+  const int nfac = nfreq > 1 && !batched ? pp->nfac : 1;
   if (nfac == 2 && (cudaEventRecord(pp->fork, st) != cudaSuccess ||
                     cudaStreamWaitEvent(pp->fac2, pp->fork, 0) != cudaSuccess))
     return MBPT_ERR_CUDA;
   auto factor = [&](int f) -> int {
+    if (batched) return MBPT_OK;
     double *m = chi0 + f * n * n;
     const bool second = nfac == 2 && (f & 1);
     cudaStream_t fs = second ? pp->fac2 : st;

@@ -11,11 +11,13 @@ then on the self-energy side U = D W, the G_occ/G_virt/Zt kernel with the H
 epilogue and the row-contraction kernel -- one launch of each engine kernel.
 Device memory stays at a few GB (M = 4096: about 1 GB).
 
---dyson N: the mixed Dyson step of `nfreq` frequencies of an N x N chi0
+--dyson N [--time]: the mixed Dyson step of `nfreq` frequencies of an N x N chi0
 (negative definite, seeded): cuSOLVER's Cholesky, the shared-memory diagonal
 blocks, the TF32-pair recursion (2 engine launches per node; with leaves of
 128 the last three engine launches of a frequency are the top node's two
-products and W = L^-T L^-1) and the mirrored FP64 store.
+products and W = L^-T L^-1) and the mirrored FP64 store. From 4 frequencies
+on, the factorisations are one batched Cholesky of all of them. --time
+prints CUDA-event times of the factorisations alone and of the whole step.
 
 --sweep: one whole mixed chi0 -> W -> Sigma -> QP sweep (24 points) of a
 synthetic system, for the launch list of the benchmark's workload.
@@ -68,6 +70,22 @@ def dyson(a):
     A = torch.randn(n, n // 2, generator=g, device='cuda', dtype=torch.float64)
     chi0 = (-(A @ A.T) / n * 3.0)[None].repeat(a.nfreq, 1, 1).contiguous()
     del A
+    if a.time:
+        # the factorisations alone (want_w False), then the whole step, each
+        # the best of 3 after a warm-up, on copies of the same chi0
+        for want_w in (False, True):
+            best = 1e9
+            for _ in range(4):
+                c = chi0.clone()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                dyson_batch(c, want_w=want_w, precision='mixed')
+                e1.record()
+                torch.cuda.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+            print(f'dyson n={n} nfreq={a.nfreq} want_w={want_w}: {best:.2f} ms '
+                  f'({best / a.nfreq:.3f} ms per frequency)', flush=True)
+        return
     logdet, _, info, _ = dyson_batch(chi0, want_w=True, precision='mixed')
     torch.cuda.synchronize()
     print(f'dyson case n={n} nfreq={a.nfreq}: info {info.tolist()}, '
@@ -147,6 +165,7 @@ def main():
     p.add_argument('--states', type=int, default=682)
     p.add_argument('--dyson', type=int, default=0)
     p.add_argument('--nfreq', type=int, default=1)
+    p.add_argument('--time', action='store_true')
     p.add_argument('--sweep', action='store_true')
     p.add_argument('--transform', type=int, default=0)
     p.add_argument('--fp64-peak', type=int, default=0)

@@ -240,10 +240,12 @@ def test_planted_nonpositive_dielectric_is_flagged():
 
 @pytest.mark.parametrize('prec', ['fp64', 'mixed'])
 def test_dyson_batch_with_failed_frequency_inside(prec):
-    """Four frequencies, the second not positive definite: the inverses of the
-    others run on the side stream while the next one factorises, the failed
-    one takes the LU fallback after both streams drain; every output must
-    match the dense FP64 answer and only the failed frequency is flagged."""
+    """Four frequencies, the second not positive definite: the batched
+    Cholesky of all four flags it (its other factors are unaffected), the
+    inverses of the others run on the side stream, the failed one takes the
+    LU fallback after the streams drain, restored from the triangle the
+    factorisation left untouched; every output must match the dense FP64
+    answer and only the failed frequency is flagged."""
     rng = np.random.default_rng(7)
     n = 300
     Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
@@ -442,3 +444,26 @@ def test_driver_freq_block_and_scratch_dir(golden):
     with pytest.raises(NotImplementedError):
         gw.solve_qp_energy_space_time(eps, None, nocc, states, numerics=Num, factors=(X, D),
                                       freq_block=4, scratch_dir='/tmp/x')
+
+
+@pytest.mark.parametrize('n', [96, 1000, 1200])
+def test_dyson_batched_cholesky(n):
+    """Five frequencies take the batched left-looking Cholesky (128-column
+    steps: one batched DGEMM update, the diagonal blocks factorised and
+    inverted in shared memory, one batched DGEMM panel; n = 1000 and 1200
+    end on a partial block): log-determinants against slogdet, W - I against
+    the FP64 inverse, FP64 mode to rounding and mixed mode to 5e-6."""
+    g = torch.Generator(device='cpu').manual_seed(n + 5)
+    A = torch.randn(5, n, n // 2 + 3, generator=g, dtype=torch.float64)
+    scale = torch.tensor([3.0, 0.5, 1.0, 2.0, 0.1], dtype=torch.float64)[:, None, None]
+    chi0 = (-(A @ A.transpose(1, 2)) / n * scale).cuda()
+    eye = torch.eye(n, dtype=torch.float64, device='cuda')
+    ref = torch.linalg.inv(eye - chi0) - eye
+    want = torch.linalg.slogdet(eye - chi0)[1]
+    for prec, tol in (('fp64', 1e-12), ('mixed', 5e-6)):
+        c = chi0.clone()
+        logdet, trace, info, _ = st.dyson_batch(c, want_w=True, precision=prec)
+        assert not np.any(info)
+        assert float((logdet - want).abs().max()) < 1e-10 * n
+        assert float((trace - chi0.diagonal(dim1=-2, dim2=-1).sum(-1)).abs().max()) < 1e-9 * n
+        assert float((c - ref).abs().max()) < tol, prec
