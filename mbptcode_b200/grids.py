@@ -40,10 +40,8 @@ except ImportError:  # pragma: no cover -- the fits then run on the BLAS's own t
 _DATA = os.path.join(os.path.dirname(__file__), 'data')
 _TABLES: dict = {}
 
-# The transform fits are many small independent SVDs (~1000 x 24): they run on
-# a shared pool of host threads, each with a single-threaded BLAS.
-_FIT_POOL = ThreadPoolExecutor(max_workers=max(1, min(32, os.cpu_count() or 1)),
-                               thread_name_prefix='mbpt-fit')
+# The transform fits are many small independent SVDs (~1000 x 24), one stacked
+# SVD per transform, with a single-threaded BLAS.
 _BLAS = {'ctrl': None, 'depth': 0, 'limit': None, 'lock': threading.Lock()}
 
 
@@ -253,20 +251,21 @@ def transform_weights(kind, tau, omega, e_min, e_max, regularization=None,
     nx = max((int(np.log10(e_max / e_min)) + 1) * nodes_factor, n_in)
     x = e_min * (e_max / e_min) ** (np.arange(nx) / (nx - 1.0))
     W = np.zeros((n_out, n_in))
-
-    def fit(i):
-        psi, A = _fit_problem(kind, tau, omega, i, x)
-        U, S, Vt = np.linalg.svd(A, full_matrices=False)
+    # every row's design matrix in one stack and one stacked SVD (LAPACK per
+    # matrix, outside the interpreter lock), then each row's filtered
+    # pseudo-inverse exactly as a single row's fit computes it
+    probs = [_fit_problem(kind, tau, omega, i, x) for i in range(n_out)]
+    A_all = np.stack([A for _, A in probs])
+    with _single_threaded_blas():
+        U_all, S_all, Vt_all = np.linalg.svd(A_all, full_matrices=False)
+    errs = []
+    for i, (psi, A) in enumerate(probs):
+        U, S, Vt = U_all[i], S_all[i], Vt_all[i]
         keep = S > FIT_RCOND * S[0]
         filt = np.zeros_like(S)
         np.divide(S, reg ** 2 + S ** 2, out=filt, where=keep)
         W[i] = Vt.T @ (filt * (U.T @ psi))
-        return float(np.abs(A @ W[i] - psi).max())
-
-    # the rows are independent: spread over the host's cores, each row's
-    # arithmetic unchanged
-    with _single_threaded_blas():
-        errs = [f.result() for f in [_FIT_POOL.submit(fit, i) for i in range(n_out)]]
+        errs.append(float(np.abs(A @ W[i] - psi).max()))
     worst = 0.0
     for i, err in enumerate(errs):
         if not (np.isfinite(err) and np.isfinite(W[i]).all()):
@@ -426,7 +425,10 @@ class SpaceTimeAxes:
     """The axes of one space-time GW solve.
 
     mu: the mid-gap (restricted), or one per spin channel (unrestricted);
-    grid: chi0's tau axis onto the screening frequencies (cosft_wt);
+    grid: chi0's tau axis onto the screening frequencies, with the cosine
+    tau -> omega weights cosft_wt only (the route's one use of the grid; the
+    full four-matrix grid is TimeFrequencyGrid.minimax_split on the same
+    arguments);
     tau_sigma: the self-energy's own tau axis (half the rS minimax points);
     Ctw (ntau, nfreq): omega -> tau cosine weights of W - I over rW;
     C, S (npade, ntau): tau -> i omega cosine / sine weights of Sigma over rS;
@@ -466,7 +468,8 @@ def space_time_axes(eps, nocc, ntau='auto', pade_freq=None, anchor=None,
     pade = pade_nodes() if pade_freq is None else np.asarray(pade_freq, float)
     # the seven transform fits are independent: all in flight at once
     with _single_threaded_blas(), ThreadPoolExecutor(max_workers=4) as outer:
-        f_grid = outer.submit(TimeFrequencyGrid.minimax_split, ntau, e_min, e_max, freq, fw)
+        f_grid = outer.submit(TimeFrequencyGrid.minimax_split, ntau, e_min, e_max, freq, fw,
+                              with_sine=False, with_inverse=False)
         f_ctw = outer.submit(transform_weights, COSINE_WT, tau_sigma, freq, *rW, warn=False)
         f_c = outer.submit(transform_weights, COSINE_TW, tau_sigma, pade, *rS, warn=False)
         f_s = outer.submit(transform_weights, SINE_TW, tau_sigma, pade, *rS, warn=False)
@@ -527,7 +530,8 @@ def space_time_axes_unrestricted(spectra, noccs, ntau='auto', pade_freq=None, an
     tau_sigma = 0.5 * minimax_time_grid(ntau, *rS)[0]
     pade = pade_nodes() if pade_freq is None else np.asarray(pade_freq, float)
     with _single_threaded_blas(), ThreadPoolExecutor(max_workers=4) as outer:
-        f_grid = outer.submit(TimeFrequencyGrid.minimax_split, ntau, e_min, e_max, freq, fw)
+        f_grid = outer.submit(TimeFrequencyGrid.minimax_split, ntau, e_min, e_max, freq, fw,
+                              with_sine=False, with_inverse=False)
         f_ctw = outer.submit(transform_weights, COSINE_WT, tau_sigma, freq, *rW, warn=False)
         f_c = outer.submit(transform_weights, COSINE_TW, tau_sigma, pade, *rS, warn=False)
         f_s = outer.submit(transform_weights, SINE_TW, tau_sigma, pade, *rS, warn=False)
