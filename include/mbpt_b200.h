@@ -251,6 +251,26 @@ int mbpt_sigma_backward(const double *X_dev, int64_t M, int64_t norb, int64_t no
                         double *D_bar_dev, double *Wt_bar_dev, void *workspace,
                         size_t ws_bytes, int *err_dev, void *stream);
 
+/* ---- contour deformation (GW/contour_deformation.py), FP64 ----------------
+ * Three-index slices B_s = D^T diag(X[:, p_s]) X of the states p_s
+ * (LinearResponse/space_time.py:804-815 `three_index_slice`), written to
+ * B_dev as (nstates, naux, norb) row-major; states_host: nstates int64. */
+size_t mbpt_three_index_slices_workspace_bytes(int64_t M, int64_t norb);
+int mbpt_three_index_slices(const double *X_dev, int64_t M, int64_t norb, const double *D_dev,
+                            int64_t naux, const int64_t *states_host, int nstates,
+                            double *B_dev, void *workspace, size_t ws_bytes, void *stream);
+
+/* The imaginary-axis screening contraction of the contour deformation:
+ * wc[k, c] = B[:, c]^T (W - I)_k B[:, c] for W - I (nfreq, naux, naux) from the
+ * Dyson step and B (naux x ncols, row-major; the states' slices side by side):
+ * GW/contour_deformation.py:229-237 `screening_contraction` and :248-290
+ * `cd_screening_contraction_multi` (one W per frequency serving every
+ * state). wc_dev: nfreq x ncols, overwritten. */
+size_t mbpt_screening_contraction_workspace_bytes(int64_t naux, int64_t ncols);
+int mbpt_screening_contraction(const double *w_minus_i_dev, int nfreq, int64_t naux,
+                               const double *B_dev, int64_t ncols, double *wc_dev,
+                               void *workspace, size_t ws_bytes, void *stream);
+
 /* The reverse of the Dyson step W = [1 - chi0]^-1: chi0_bar_f = W_f W_bar_f W_f
  * (gradients/rpa/space_time_adjoint.py:679-685), in place over wbar_dev
  * (nfreq, naux, naux), from W - I (w_minus_i_dev, the Dyson output). FP64. */

@@ -1,0 +1,314 @@
+"""Contour-deformation correlation self-energy on the B200.
+
+Mirrors the kernel seams of MBPTcode's ``src/SingleReference/GW/contour_deformation.py``
+and ``GW/real_screening.py`` with the same names and argument meaning:
+
+    Sigma^c_pp(omega) = Sigma^int + Sigma^res,
+    Sigma^int = -(1/pi) sum_kq c[k, q](omega) wc[k, q],
+    wc[k, q]  = B_p[:, q]^T (W(i nu_k) - I) B_p[:, q],
+    Sigma^res = sum_{q in residues} w_q (b_q^T W(|eps_q - omega|) b_q - b_q^T b_q),
+
+with B_p = D^T diag(X[:, p]) X the state's three-index slice, W = [1 - chi0]^-1
+on the contour's Gauss-Legendre frequencies nu_k, c the quadrature weights with
+the Lorentzian's singular part integrated in closed form
+(`cd_integral_weights`), and the residues' W at real frequencies below the gap
+from the cosh transform of proj(tau) (`LaplaceRealScreening`).
+
+On the device: proj(tau) on the contour's own time grid and chi0(i nu) by the
+chi0 sweep and the tau -> omega transform, W - I by the Dyson step (one
+batched FP64 Cholesky of every frequency), the slices and the screening
+contraction (mbpt_three_index_slices, mbpt_screening_contraction: one W per
+frequency serves every state) and each residue frequency's W. The quadrature
+weights, the residue sets and the sums over k and q are host arithmetic on
+nfreq x norb numbers. FP64 throughout.
+
+The reference's root finder for this route (`qp_energy_cd` on
+`Solvers/qp_equation.py` `solve_qp_equation_scan`) is not part of this module;
+the explicit O(N^4) particle-hole backends (`C_ov`) are not either.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from ._lib import WORKSPACE, check, lib, ptr, require_device, stream_ptr
+from .grids import TimeFrequencyGrid, gauss_legendre_grid, particle_hole_window
+from .space_time import _eps_host, chi0_sweep, dyson_batch, to_device, transform
+
+# MBPTcode src/Base/numerics/constants.py
+RESIDUE_ON_CONTOUR_TOL = 1e-10   # :461
+CD_NFREQ = 64                    # :478
+CD_NTAU = 24                     # :493
+LAPLACE_SCREENING_TOL = 1e-8     # :577
+
+_MAX_J = 32  # output rows per transform call (the transform kernel's limit is 34)
+
+
+class ResidueRefused(ValueError):
+    """A real frequency the imaginary-time representation does not carry
+    (``real_screening.py:49-54``)."""
+
+
+def gap_scaled_w0(eps, nocc, scale=0.5):
+    """w0 = scale (eps_LUMO - eps_HOMO) (``Base/utils/grids/grids.py:173-186``)."""
+    eps = np.asarray(eps, float)
+    w0 = scale * (eps[nocc] - eps[nocc - 1])
+    if not w0 > 0:
+        raise ValueError(f'gap_scaled_w0: the gap {eps[nocc] - eps[nocc - 1]:.6g} is not positive')
+    return w0
+
+
+def cd_grid_range(eps, nocc, e_min_below_gap=None):
+    """(e_min, e_max) of the contour's time grid: e_min reaches below the gap,
+    by default by half of it (``contour_deformation.py:439-468``)."""
+    eps = np.asarray(eps, float)
+    gap, e_max, _ = particle_hole_window(eps, nocc)
+    shift = gap_scaled_w0(eps, nocc) if e_min_below_gap is None else float(e_min_below_gap)
+    if gap - shift <= 0:
+        raise ValueError(f'e_min_below_gap {shift} exceeds the gap {gap:.4f}: the imaginary-'
+                         f'time grid would be asked to represent e^{{-y tau}} at y <= 0')
+    return gap - shift, e_max
+
+
+def cd_frequency_grid(eps, nocc, ntau=CD_NTAU, nfreq_cd=CD_NFREQ, w0_cd=None,
+                      e_min_below_gap=None):
+    """(nu, nu_weights, grid, w0): Gauss-Legendre nu on w0 (half the gap by
+    default) and the minimax time grid over `cd_grid_range` onto it, cosine
+    tau -> omega weights only (``contour_deformation.py:471-503``)."""
+    e_min, e_max = cd_grid_range(eps, nocc, e_min_below_gap)
+    w0 = float(w0_cd) if w0_cd is not None else gap_scaled_w0(eps, nocc)
+    nu, nu_weights = gauss_legendre_grid(int(nfreq_cd), w0=w0)
+    grid = TimeFrequencyGrid.minimax_split(int(ntau), e_min, e_max, nu, nu_weights,
+                                           with_sine=False, with_inverse=False)
+    return nu, nu_weights, grid, w0
+
+
+def cd_integral_weights(de, nu_points, nu_weights):
+    """(c, dc), (nfreq, norb): Sigma^int = -(1/pi) sum c wc for de = omega -
+    eps, and its derivative in de (``contour_deformation.py:150-202``). The
+    Lorentzian de/(de^2 + nu^2) times wc is integrated as wc(0) times a
+    closed-form integral of de/(de^2 + nu^2) a^2/(a^2 + nu^2) plus the
+    quadrature of the remainder, wc(0) extrapolated in nu^2 from the two
+    smallest nodes (a = four times the median node); at |de| below
+    RESIDUE_ON_CONTOUR_TOL the closed form takes sign 0, as the residue term
+    takes that pole at half weight."""
+    de = np.asarray(de, float)
+    nu = np.asarray(nu_points, float)
+    wt = np.asarray(nu_weights, float)
+    den = de[None, :] ** 2 + nu[:, None] ** 2
+    g = de[None, :] / den
+    dg = (nu[:, None] ** 2 - de[None, :] ** 2) / den ** 2
+    c = wt[:, None] * g
+    dc = wt[:, None] * dg
+    k1, k2 = np.argsort(nu)[:2]
+    n1, n2 = nu[k1] ** 2, nu[k2] ** 2
+    a = 4.0 * float(np.median(nu))
+    h = wt * a * a / (a * a + nu ** 2)
+    side = np.where(np.abs(de) < RESIDUE_ON_CONTOUR_TOL, 0.0, np.sign(de))
+    ad = a + np.abs(de)
+    err = 0.5 * np.pi * side * a / ad - h @ g
+    derr = -0.5 * np.pi * a / ad ** 2 - h @ dg
+    for k, coef in ((k1, n2 / (n2 - n1)), (k2, -n1 / (n2 - n1))):
+        c[k] += coef * err
+        dc[k] += coef * derr
+    return c, dc
+
+
+def residue_set(eps, nocc, omega, tol=RESIDUE_ON_CONTOUR_TOL):
+    """[(q, weight)]: the poles of G the deformation sweeps over
+    (``real_screening.py:157-168``): occupied levels above omega (-1),
+    virtual ones below it (+1), a level on the contour at half weight."""
+    eps = np.asarray(eps, float)
+    out = []
+    for q in range(len(eps)):
+        gap = eps[q] - omega
+        if abs(gap) < tol:
+            out.append((q, -0.5 if q < nocc else 0.5))
+        elif q < nocc and gap > 0.0:
+            out.append((q, -1.0))
+        elif q >= nocc and gap < 0.0:
+            out.append((q, 1.0))
+    return out
+
+
+def real_frequency_weights(grid, omega):
+    """(c, dc): chi0(omega) = sum_k c_k proj(tau_k) at a real omega below the
+    gap, c_k = 2 w_k cosh(omega tau_k) on the grid's bare Laplace quadrature,
+    and its omega derivative (``real_screening.py:184-209``)."""
+    t = np.asarray(grid.tau_points, float)
+    w = 2.0 * np.asarray(grid.tau_weights, float)
+    return w * np.cosh(omega * t), w * t * np.sinh(omega * t)
+
+
+def laplace_representation_error(grid, eps, nocc, freq):
+    """max over y = d -+ freq of |y sum_k w_k e^{-y tau_k} - 1| on the pair
+    energies d, inf where freq reaches the gap
+    (``LinearResponse/space_time.py:908-931``)."""
+    eps = np.asarray(eps, float)
+    d = (eps[nocc:][None, :] - eps[:nocc][:, None]).ravel()
+    y = np.concatenate([d - freq, d + freq])
+    if y.min() <= 0.0:
+        return np.inf
+    q = np.exp(-np.outer(y, grid.tau_points)) @ grid.tau_weights
+    return float(np.abs(q * y - 1.0).max())
+
+
+def _rows_transform(proj, weights):
+    """sum_k weights[j, k] proj[k] for any number of output rows (in chunks
+    of the transform kernel's limit)."""
+    weights = np.asarray(weights, float)
+    parts = [transform(proj, np.ascontiguousarray(weights[j:j + _MAX_J]))
+             for j in range(0, weights.shape[0], _MAX_J)]
+    return parts[0] if len(parts) == 1 else torch.cat(parts)
+
+
+def polarizability_tau(X, D, eps, nocc, grid, mu=None):
+    """proj(tau) on the grid's time points, (ntau, naux, naux) on the device,
+    FP64 (``gradients/rpa/space_time_adjoint.py:94-113``)."""
+    _, proj = chi0_sweep(X, D, eps, nocc, grid.tau_points,
+                         np.zeros((1, len(grid.tau_points))), mu=mu, precision='fp64',
+                         want_proj=True)
+    return proj
+
+
+def screening_minus_identity(proj_tau, cosft_wt):
+    """W(i nu) - I for every frequency of cosft_wt: chi0 = cosft_wt proj(tau),
+    then the Dyson step (FP64 Cholesky; ``contour_deformation.py:209-226``
+    factorises and solves per frequency). Returns (W - I, info)."""
+    dev = require_device()
+    chi0 = _rows_transform(to_device(proj_tau, dev), cosft_wt)
+    _, _, info, _ = dyson_batch(chi0, want_w=True, precision='fp64')
+    return chi0, info
+
+
+def three_index_slices(X, D, states):
+    """(nstates, naux, norb) device tensor of B_p = D^T diag(X[:, p]) X
+    (``LinearResponse/space_time.py:804-815``)."""
+    dev = require_device()
+    Xd, Dd = to_device(X, dev), to_device(D, dev)
+    M, norb = Xd.shape
+    naux = Dd.shape[1]
+    st = np.ascontiguousarray(np.atleast_1d(states), dtype=np.int64)
+    B = torch.empty((len(st), naux, norb), dtype=torch.float64, device=dev)
+    ws = WORKSPACE.get(lib().mbpt_three_index_slices_workspace_bytes(M, norb), dev)
+    import ctypes
+    check(lib().mbpt_three_index_slices(ptr(Xd), M, norb, ptr(Dd), naux,
+                                        st.ctypes.data_as(ctypes.c_void_p), len(st), ptr(B),
+                                        ptr(ws), ws.numel(), stream_ptr()),
+          'mbpt_three_index_slices')
+    return B
+
+
+def screening_contraction_device(w_minus_i, Bps):
+    """[wc_s (nfreq, norb)] for each slice: wc[k, q] = B[:, q]^T (W - I)_k
+    B[:, q], one product per frequency for all slices side by side."""
+    dev = w_minus_i.device
+    Bs = [to_device(b, dev) for b in Bps]
+    naux, norb = Bs[0].shape
+    B = torch.cat(Bs, dim=1).contiguous()
+    nfreq, ncols = w_minus_i.shape[0], B.shape[1]
+    wc = torch.empty((nfreq, ncols), dtype=torch.float64, device=dev)
+    ws = WORKSPACE.get(lib().mbpt_screening_contraction_workspace_bytes(naux, ncols), dev)
+    wm = w_minus_i.contiguous()
+    check(lib().mbpt_screening_contraction(ptr(wm), nfreq, naux, ptr(B), ncols, ptr(wc),
+                                           ptr(ws), ws.numel(), stream_ptr()),
+          'mbpt_screening_contraction')
+    return [wc[:, i * norb:(i + 1) * norb] for i in range(len(Bs))]
+
+
+def cd_screening_contraction_multi(proj_tau, cosft_wt, Bps, tile_gb=None, freq_indices=None):
+    """wc[nu, q] for a list of bra slices on one factorisation per frequency
+    (``contour_deformation.py:248-270``); arrays come back as Bps[0] is held."""
+    if freq_indices is not None:
+        raise NotImplementedError('frequency splits over ranks are outside the one-GPU route')
+    wmi, info = screening_minus_identity(proj_tau, cosft_wt)
+    if np.any(info):
+        import warnings
+        warnings.warn('1 - chi0(i nu) is not positive definite at frequencies '
+                      f'{np.nonzero(info)[0].tolist()}; solved by LU', RuntimeWarning)
+    out = screening_contraction_device(wmi, Bps)
+    if isinstance(Bps[0], torch.Tensor):
+        return out
+    return [w.cpu().numpy() for w in out]
+
+
+def screening_contraction(Bp, wbp):
+    """wc[k, q] = sum_P Bp[P, q] (W(i nu_k) Bp - Bp)[P, q] from W Bp given per
+    frequency (``contour_deformation.py:229-237``)."""
+    return np.einsum('Pq,kPq->kq', np.asarray(Bp), np.asarray(wbp) - np.asarray(Bp)[None],
+                     optimize=True)
+
+
+class LaplaceRealScreening:
+    """W at a real frequency below the particle-hole gap from proj(tau): one
+    (ntau, naux^2) transform and one Dyson step per frequency, the W - I of
+    each frequency kept for later calls (``real_screening.py:94-154``).
+    Refuses (ResidueRefused) a frequency the grid does not carry."""
+
+    def __init__(self, proj_tau, grid, eps, nocc, tol=LAPLACE_SCREENING_TOL):
+        self.proj_tau = to_device(proj_tau, require_device())
+        self.grid = grid
+        self.eps = np.asarray(eps, float)
+        self.nocc = nocc
+        self.tol = tol
+        self._w = {}
+
+    def representation_error(self, freq):
+        return laplace_representation_error(self.grid, self.eps, self.nocc, freq)
+
+    def _weights(self, freq):
+        err = self.representation_error(freq)
+        if not err < self.tol:
+            gap = particle_hole_window(self.eps, self.nocc)[0]
+            raise ResidueRefused(
+                f'real frequency {freq:.4f} Ha is not carried by the tau grid: bare-quadrature '
+                f'error {err:.1e} against tol {self.tol:.0e}; gap - freq = {gap - freq:.4f} '
+                f'Ha, the grid\'s e_min is {self.grid.meta.get("e_min", float("nan")):.4f}. '
+                f'Build the grid with e_min <= gap - freq, or use the explicit backend.')
+        return real_frequency_weights(self.grid, freq)
+
+    def w_minus_identity(self, freq):
+        key = float(freq)
+        if key not in self._w:
+            c, _ = self._weights(key)
+            chi0 = _rows_transform(self.proj_tau, c[None, :])
+            dyson_batch(chi0, want_w=True, precision='fp64')
+            self._w[key] = chi0[0]
+        return self._w[key]
+
+    def apply(self, freq, b):
+        """W(freq) b = b + (W - I) b."""
+        bd = to_device(b, self.proj_tau.device)
+        y = bd + self.w_minus_identity(freq) @ bd
+        return y if isinstance(b, torch.Tensor) else y.cpu().numpy()
+
+
+def sigma_cd(p, omega, Bp, eps, nocc, nu_points, nu_weights, residues=None, wbp=None,
+             eta=0.0, wc=None, C_ov=None, real_screening=None):
+    """Sigma^c_pp(omega) by contour deformation from the state's slice Bp and
+    its contracted screening wc (``contour_deformation.py:310-343``):
+    the imaginary-axis integral and, for the residue set (recomputed at omega
+    when not given), sum_q w_q (b_q^T W(|eps_q - omega|) b_q - b_q^T b_q) with
+    `real_screening`'s W (a LaplaceRealScreening)."""
+    if C_ov is not None or eta:
+        raise NotImplementedError('the explicit particle-hole backends are outside the '
+                                  'cubic device route')
+    eps = np.asarray(eps, float)
+    Bh = Bp.detach().cpu().numpy() if isinstance(Bp, torch.Tensor) else np.asarray(Bp)
+    if wc is None:
+        if wbp is None:
+            raise ValueError('sigma_cd needs wc or wbp on the device route')
+        wc = screening_contraction(Bh, wbp)
+    wc = wc.detach().cpu().numpy() if isinstance(wc, torch.Tensor) else np.asarray(wc)
+    c, _ = cd_integral_weights(omega - eps, nu_points, nu_weights)
+    s_int = -float(np.einsum('kq,kq->', c, wc)) / np.pi
+    res = residue_set(eps, nocc, omega) if residues is None else residues
+    s_res = 0.0
+    if res:
+        if real_screening is None:
+            raise ValueError('the residue term needs real_screening on the device route')
+        for q, weight in res:
+            b = Bh[:, q]
+            y = real_screening.apply(abs(eps[q] - omega), b)
+            s_res += weight * (float(b @ y) - float(b @ b))
+    return s_int + s_res

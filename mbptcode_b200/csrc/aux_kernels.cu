@@ -403,6 +403,18 @@ __global__ void __launch_bounds__(512) chol_diag_block_kernel(
   if (tid == 0 && bad >= 0 && info[f] == 0) info[f] = static_cast<int>(j0) + bad + 1;
 }
 
+// out[r, c] = X[r, p] X[r, c]: the collocation of state p times every
+// orbital's, the grid side of the three-index slice B_p = D^T out
+__global__ void row_scaled_copy_kernel(const double *__restrict__ X, int64_t M, int64_t n,
+                                       int64_t p, double *__restrict__ out) {
+  const int64_t total = M * n;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = i / n;
+    out[i] = X[r * n + p] * X[i];
+  }
+}
+
 }  // namespace
 
 void launch_chi0_bar_seed(double *a, int64_t n, int nfreq, const double *w, cudaStream_t st) {
@@ -513,6 +525,12 @@ int launch_chol_diag_block(const double *P, int64_t m, int nbj, double *A, int64
   count_launch();
   chol_diag_block_kernel<<<nmat, 512, smem, st>>>(P, m, nbj, A, n, j0, Linv, info);
   return MBPT_OK;
+}
+
+void launch_row_scaled_copy(const double *X, int64_t M, int64_t n, int64_t p, double *out,
+                            cudaStream_t st) {
+  count_launch();
+  row_scaled_copy_kernel<<<blocks(M * n), 256, 0, st>>>(X, M, n, p, out);
 }
 
 }  // namespace mbpt

@@ -42,6 +42,8 @@ int launch_trtri_diag_blocks(double *A, int64_t n, int64_t lda, int nb, cudaStre
                              float *r_lo = nullptr, int64_t ldp = 0);
 void launch_strided_to_tf32(const double *src, int64_t rows, int64_t k, int64_t rs, int64_t cs,
                             float *hi, float *lo, int64_t rows_p, int64_t k_p, cudaStream_t st);
+void launch_row_scaled_copy(const double *X, int64_t M, int64_t n, int64_t p, double *out,
+                            cudaStream_t st);
 void launch_chol_copy_panel(const double *A, int64_t n, int64_t j0, int64_t m, int nbj,
                             int nmat, double *P, cudaStream_t st);
 int launch_chol_diag_block(const double *P, int64_t m, int nbj, double *A, int64_t n,
@@ -1283,6 +1285,56 @@ int mbpt_chi0_backward(const double *pbar, const double *X, int64_t M, int64_t n
   if (mode != MBPT_MODE_FP64) return MBPT_ERR_UNSUPPORTED;
   Arena ar = arena(ws, ws_bytes);
   return back_run(pbar, X, d, eps, mu, D, tau, ntau, eps_bar, X_bar, D_bar, ar, S(stream));
+}
+
+size_t mbpt_three_index_slices_workspace_bytes(int64_t M, int64_t norb) {
+  return sizeof(double) * static_cast<size_t>(M) * norb + 2048;
+}
+
+int mbpt_three_index_slices(const double *X, int64_t M, int64_t norb, const double *D,
+                            int64_t naux, const int64_t *states_host, int nstates, double *B,
+                            void *ws, size_t ws_bytes, void *stream) {
+  if (M < 1 || norb < 1 || naux < 1 || nstates < 1) return MBPT_ERR_SHAPE;
+  cudaStream_t st = S(stream);
+  Arena ar = arena(ws, ws_bytes);
+  double *T = ar.take<double>(M * norb);
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  cublasHandle_t h = handles(st).blas;
+  for (int s = 0; s < nstates; ++s) {
+    const int64_t p = states_host[s];
+    if (p < 0 || p >= norb) return MBPT_ERR_SHAPE;
+    // B_p = D^T (x_p o X): LinearResponse/space_time.py:804-815
+    launch_row_scaled_copy(X, M, norb, p, T, st);
+    if (!dgemm_rm(h, true, false, naux, norb, M, 1.0, D, naux, T, norb, 0.0,
+                  B + static_cast<int64_t>(s) * naux * norb, norb))
+      return MBPT_ERR_CUDA;
+  }
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+size_t mbpt_screening_contraction_workspace_bytes(int64_t naux, int64_t ncols) {
+  return sizeof(double) * static_cast<size_t>(naux) * ncols + 2048;
+}
+
+int mbpt_screening_contraction(const double *w_minus_i, int nfreq, int64_t naux,
+                               const double *B, int64_t ncols, double *wc, void *ws,
+                               size_t ws_bytes, void *stream) {
+  if (nfreq < 1 || naux < 1 || ncols < 1) return MBPT_ERR_SHAPE;
+  cudaStream_t st = S(stream);
+  Arena ar = arena(ws, ws_bytes);
+  double *Y = ar.take<double>(naux * ncols);
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  cublasHandle_t h = handles(st).blas;
+  if (cudaMemsetAsync(wc, 0, sizeof(double) * nfreq * ncols, st) != cudaSuccess)
+    return MBPT_ERR_CUDA;
+  for (int k = 0; k < nfreq; ++k) {
+    // wc[k, c] = B[:, c]^T (W - I)_k B[:, c]: GW/contour_deformation.py:229-237, 273-290
+    if (!dgemm_rm(h, false, false, naux, ncols, naux, 1.0, w_minus_i + k * naux * naux, naux,
+                  B, ncols, 0.0, Y, ncols))
+      return MBPT_ERR_CUDA;
+    launch_rowdot(Y, ncols, B, ncols, naux, ncols, 1.0, wc + k * ncols, st);
+  }
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 
 size_t mbpt_sigma_backward_workspace_bytes(int64_t M, int64_t norb, int64_t nocc,

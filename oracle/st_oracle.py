@@ -639,3 +639,74 @@ def evgw(X, D, eps0, nocc, ntau, tol=EVGW_TOL, max_cycle=EVGW_MAX_CYCLE,
         eps = acc.update(eps_new, res) if acc is not None else eps_new
     return eps, {'cycles': len(history), 'converged': converged,
                  'history': history}
+
+
+# ---------------------------------------------------------------------------
+# contour deformation (src/SingleReference/GW/contour_deformation.py,
+# GW/real_screening.py): the imaginary-axis screening contraction, the
+# Laplace real-frequency screening and Sigma^c(omega)
+# ---------------------------------------------------------------------------
+
+def cd_integral_weights(de, nu, wt, on_contour_tol=1e-10):
+    """contour_deformation.py:150-202: quadrature weights of the Lorentzian
+    with its singular part (wc(0) times de/(de^2+nu^2) a^2/(a^2+nu^2))
+    integrated in closed form; wc(0) from the two smallest nodes."""
+    de, nu, wt = (np.asarray(a, float) for a in (de, nu, wt))
+    g = de[None, :] / (de[None, :] ** 2 + nu[:, None] ** 2)
+    c = wt[:, None] * g
+    order = np.argsort(nu)
+    k1, k2 = order[0], order[1]
+    n1, n2 = nu[k1] ** 2, nu[k2] ** 2
+    a = 4.0 * float(np.median(nu))
+    h = wt * a * a / (a * a + nu ** 2)
+    side = np.where(np.abs(de) < on_contour_tol, 0.0, np.sign(de))
+    err = 0.5 * np.pi * side * a / (a + np.abs(de)) - h @ g
+    c[k1] += n2 / (n2 - n1) * err
+    c[k2] += -n1 / (n2 - n1) * err
+    return c
+
+
+def cd_screening_contraction(proj_tau, cosft_wt, Bps):
+    """contour_deformation.py:248-290 (serial): per frequency chi0 =
+    cosft_wt proj(tau), W B - B by a solve, wc[k, q] = B[:,q].(W B - B)[:,q]."""
+    chi0 = np.tensordot(cosft_wt, proj_tau, axes=(1, 0))
+    eye = np.eye(chi0.shape[-1])
+    out = [np.zeros((len(chi0), B.shape[1])) for B in Bps]
+    for k in range(len(chi0)):
+        for wc, B in zip(out, Bps):
+            wc[k] = np.einsum('Pq,Pq->q', B, np.linalg.solve(eye - chi0[k], B) - B)
+    return out
+
+
+def residue_set(eps, nocc, omega, tol=1e-10):
+    """real_screening.py:157-168."""
+    out = []
+    for q, e in enumerate(eps):
+        gap = e - omega
+        if abs(gap) < tol:
+            out.append((q, -0.5 if q < nocc else 0.5))
+        elif q < nocc and gap > 0.0:
+            out.append((q, -1.0))
+        elif q >= nocc and gap < 0.0:
+            out.append((q, 1.0))
+    return out
+
+
+def laplace_screening_apply(proj_tau, tau, tau_w, freq, b):
+    """real_screening.py:147-150 with :184-209: W(freq) b, chi0(freq) =
+    sum_k 2 w_k cosh(freq tau_k) proj(tau_k), below the gap."""
+    c = 2.0 * np.asarray(tau_w) * np.cosh(freq * np.asarray(tau))
+    chi0 = np.tensordot(c, proj_tau, axes=(0, 0))
+    return np.linalg.solve(np.eye(chi0.shape[0]) - chi0, b)
+
+
+def sigma_cd(p, omega, Bp, eps, nocc, nu, nu_w, wc, proj_tau, tau, tau_w):
+    """contour_deformation.py:310-343 with the Laplace residue backend."""
+    eps = np.asarray(eps, float)
+    c = cd_integral_weights(omega - eps, nu, nu_w)
+    s = -float(np.einsum('kq,kq->', c, wc)) / np.pi
+    for q, weight in residue_set(eps, nocc, omega):
+        b = Bp[:, q]
+        y = laplace_screening_apply(proj_tau, tau, tau_w, abs(eps[q] - omega), b)
+        s += weight * (b @ y - b @ b)
+    return s

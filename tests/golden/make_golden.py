@@ -27,6 +27,12 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
 * sigma_adjoint.npz  the self-energy diagonal of three states and its adjoint
                      (eps_bar, X_bar, D_bar) for seeded adjoints on Re and
                      Im Sigma;
+* contour.npz        the contour-deformation self-energy's pieces: the contour
+                     grid, proj(tau) on it, the screening contraction of three
+                     states, Sigma^c at points around each state's level
+                     (residues through the Laplace backend) and the integral
+                     weights (the CD module loads pyscf for its driver; a
+                     stand-in that raises on use lets it import here);
 * qp_kat.npz         the root finder on closed-form self-energies
                      (tests/test_qp_refine_root.py's two-pole Sigma and others);
 * c1_<variant>.npz   the synthetic FP64 configuration at full size (n_orb = 400,
@@ -36,7 +42,7 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      stored: the tests regenerate them from the seed and check
                      the regeneration against the stored eps and checksums.
 
-    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint]
+    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour]
 """
 import os
 import sys
@@ -316,6 +322,93 @@ def sigma_adjoint_fixture(ntau=12, nfreq=10):
         sigma=sigma, eps_bar=eps_bar, X_bar=X_bar, D_bar=D_bar)
 
 
+def _import_contour_deformation():
+    """MBPTcode's GW/contour_deformation.py imports pyscf at module load for
+    its driver (mean field, integrals); the functions this fixture calls never
+    touch it. pyscf is absent here, so a stand-in package whose every
+    attribute raises when called lets the module load."""
+    import importlib.abc
+    import importlib.machinery
+    import types
+
+    class _Inert:
+        def __init__(self, name):
+            self._n = name
+
+        def __getattr__(self, name):
+            return _Inert(self._n + '.' + name)
+
+        def __call__(self, *a, **k):
+            raise RuntimeError(f'{self._n}: pyscf is not available here')
+
+        def __mro_entries__(self, bases):
+            return (object,)
+
+    class _Package(types.ModuleType):
+        def __init__(self, name):
+            super().__init__(name)
+            self.__path__ = []
+
+        def __getattr__(self, name):
+            if name.startswith('__'):
+                raise AttributeError(name)
+            return _Inert(self.__name__ + '.' + name)
+
+    class _Finder(importlib.abc.MetaPathFinder, importlib.abc.Loader):
+        def find_spec(self, fullname, path, target=None):
+            if fullname == 'pyscf' or fullname.startswith('pyscf.'):
+                return importlib.machinery.ModuleSpec(fullname, self, is_package=True)
+            return None
+
+        def create_module(self, spec):
+            return _Package(spec.name)
+
+        def exec_module(self, module):
+            pass
+
+    sys.meta_path.insert(0, _Finder())
+    import src.SingleReference.GW.contour_deformation as cd
+    import src.SingleReference.GW.real_screening as rs
+    return cd, rs
+
+
+def contour_fixture():
+    """The contour-deformation self-energy's pieces (GW/contour_deformation.py,
+    GW/real_screening.py) on a small synthetic system: the contour grid
+    (64 Gauss-Legendre frequencies on half the gap, 24 time points reaching
+    half a gap below it), proj(tau) on it, the screening contraction wc of
+    three states around the gap, Sigma^c at points on both sides of each
+    state's level and on it (residues through the Laplace backend), and the
+    integral weights at a set of de values."""
+    cd, rs = _import_contour_deformation()
+    from src.gradients.rpa.space_time_adjoint import polarizability_tau
+    from src.SingleReference.LinearResponse.space_time import three_index_slice
+    X, D, eps = synthetic_system(16, 3, 48, 31, 'calibrated')
+    nocc = 3
+    mu = particle_hole_window(eps, nocc)[2]
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        nu, nu_w, grid, w0 = cd.cd_frequency_grid(eps, nocc)
+    proj = polarizability_tau(X, D, eps, nocc, grid, mu=mu)
+    states = np.array([nocc - 1, nocc, nocc + 1])
+    Bps = [three_index_slice(X, D, int(p)) for p in states]
+    wcs = cd.cd_screening_contraction_multi(proj, grid.cosft_wt, Bps)
+    lap = rs.LaplaceRealScreening(proj, grid, eps, nocc)
+    shifts = np.array([-0.06, -0.02, 0.0, 0.02, 0.06])
+    sig = np.zeros((len(states), len(shifts)))
+    for i, p in enumerate(states):
+        for j, dw in enumerate(shifts):
+            sig[i, j] = cd.sigma_cd(int(p), eps[p] + dw, Bps[i], eps, nocc, nu, nu_w,
+                                    wc=wcs[i], real_screening=lap)
+    de = np.array([-0.3, -1e-3, 0.0, 1e-12, 2e-3, 0.05, 0.7])
+    c, dc = cd.cd_integral_weights(de, nu, nu_w)
+    np.savez_compressed(
+        os.path.join(HERE, 'contour.npz'), X=X, D=D, eps=eps, nocc=nocc, mu=mu, nu=nu,
+        nu_w=nu_w, w0=w0, tau=grid.tau_points, tau_w=grid.tau_weights, cosft_wt=grid.cosft_wt,
+        proj=proj, states=states, B=np.stack(Bps), wc=np.stack(wcs), shifts=shifts, sigma=sig,
+        de=de, c=c, dc=dc)
+
+
 def qp_fixture():
     cases = {  # poles placed off the scan grids, so no division hits one
         'two_pole': (lambda w: 0.05 / (w + 0.8) + 0.01 / (w - 0.9), -0.2),
@@ -359,8 +452,12 @@ if __name__ == '__main__':
         sigma_adjoint_fixture()
         print('self-energy adjoint fixture written to', HERE)
         sys.exit(0)
+    if ONLY == 'contour':
+        contour_fixture()
+        print('contour-deformation fixture written to', HERE)
+        sys.exit(0)
     if ONLY:
-        sys.exit(f'--only {ONLY}: choose c1, static, unrestricted or sigma_adjoint')
+        sys.exit(f'--only {ONLY}: choose c1, static, unrestricted, sigma_adjoint or contour')
     grids_fixture()
     shared_kernel_fixture()
     route_fixture('calibrated', 24, 4, 64, 7, 'calibrated', 12, full=True)
@@ -370,4 +467,5 @@ if __name__ == '__main__':
     static_fixture()
     unrestricted_fixture()
     sigma_adjoint_fixture()
+    contour_fixture()
     print('fixtures written to', HERE)

@@ -467,3 +467,37 @@ def test_dyson_batched_cholesky(n):
         assert float((logdet - want).abs().max()) < 1e-10 * n
         assert float((trace - chi0.diagonal(dim1=-2, dim2=-1).sum(-1)).abs().max()) < 1e-9 * n
         assert float((c - ref).abs().max()) < tol, prec
+
+
+def test_contour_deformation_device_matches_reference_golden(golden):
+    """The contour-deformation self-energy on the device against the
+    reference (GW/contour_deformation.py, GW/real_screening.py): proj(tau) on
+    the contour's time grid, the three-index slices of three states, their
+    screening contraction over 64 frequencies (one Dyson step per frequency
+    for all states), and Sigma^c at five points around each state's level with
+    the residues' W from the cosh transform of proj(tau); FP64 throughout."""
+    import warnings
+    from mbptcode_b200 import contour
+    g = golden('contour')
+    X, D, eps, nocc, mu = g['X'], g['D'], g['eps'], int(g['nocc']), float(g['mu'])
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        nu, nu_w, grid, _ = contour.cd_frequency_grid(eps, nocc)
+    proj = contour.polarizability_tau(X, D, eps, nocc, grid, mu=mu)
+    assert rel(proj.cpu().numpy(), g['proj']) < FP64_REL
+    B = contour.three_index_slices(X, D, g['states'])
+    assert rel(B.cpu().numpy(), g['B']) < FP64_REL
+    wcs = contour.cd_screening_contraction_multi(proj, grid.cosft_wt, list(B))
+    assert rel(torch.stack(wcs).cpu().numpy(), g['wc']) < 1e-10
+    wc_np = contour.cd_screening_contraction_multi(g['proj'], grid.cosft_wt, list(g['B']))
+    assert isinstance(wc_np[0], np.ndarray) and rel(np.stack(wc_np), g['wc']) < 1e-10
+    lap = contour.LaplaceRealScreening(proj, grid, eps, nocc)
+    for i, p in enumerate(g['states']):
+        for j, dw in enumerate(g['shifts']):
+            s = contour.sigma_cd(int(p), eps[p] + dw, B[i], eps, nocc, nu, nu_w, wc=wcs[i],
+                                 real_screening=lap)
+            assert abs(s - g['sigma'][i, j]) <= 1e-9 * abs(g['sigma'][i, j]), (p, dw)
+    # a residue frequency at the gap is refused, as the reference refuses it
+    gap = eps[nocc] - eps[nocc - 1]
+    with pytest.raises(contour.ResidueRefused):
+        lap.apply(gap, B[0][:, 0])

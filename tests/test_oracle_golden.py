@@ -239,3 +239,29 @@ def test_sigma_adjoint_oracle_and_grid_space_form(golden):
     e2, x2, d2 = orc.polarizability_backward(pb, X, D, eps, nocc, grid.tau_points, mu)
     for a, k in zip((eb + e2, xb + x2, db + d2), ('eps_bar', 'X_bar', 'D_bar')):
         assert np.abs(a - g[k]).max() <= 1e-10 * np.abs(g[k]).max(), k
+
+
+def test_contour_deformation_pieces(golden):
+    """The contour-deformation self-energy's host pieces and the oracle
+    against the reference (GW/contour_deformation.py, GW/real_screening.py):
+    the contour grid bit for bit, the integral weights, the screening
+    contraction of three states and Sigma^c around each state's level."""
+    from mbptcode_b200 import contour
+    g = golden('contour')
+    eps, nocc = g['eps'], int(g['nocc'])
+    with _quiet():
+        nu, nu_w, grid, w0 = contour.cd_frequency_grid(eps, nocc)
+    assert np.array_equal(nu, g['nu']) and np.array_equal(nu_w, g['nu_w']) and w0 == g['w0']
+    assert np.array_equal(grid.tau_points, g['tau']) and np.array_equal(grid.tau_weights, g['tau_w'])
+    assert np.array_equal(grid.cosft_wt, g['cosft_wt'])
+    c, dc = contour.cd_integral_weights(g['de'], nu, nu_w)
+    assert np.allclose(c, g['c'], rtol=1e-13, atol=0) and np.allclose(dc, g['dc'], rtol=1e-13, atol=0)
+    assert np.allclose(orc.cd_integral_weights(g['de'], nu, nu_w), g['c'], rtol=1e-13, atol=0)
+    wcs = orc.cd_screening_contraction(g['proj'], g['cosft_wt'], list(g['B']))
+    assert np.abs(np.stack(wcs) - g['wc']).max() <= 1e-12 * np.abs(g['wc']).max()
+    for i, p in enumerate(g['states']):
+        for j, dw in enumerate(g['shifts']):
+            s = orc.sigma_cd(int(p), eps[p] + dw, g['B'][i], eps, nocc, nu, nu_w, g['wc'][i],
+                             g['proj'], g['tau'], g['tau_w'])
+            assert abs(s - g['sigma'][i, j]) <= 1e-11 * abs(g['sigma'][i, j]), (p, dw)
+    assert contour.residue_set(eps, nocc, eps[nocc]) == orc.residue_set(eps, nocc, eps[nocc])
