@@ -19,7 +19,7 @@ import importlib
 
 import numpy as np
 
-from . import adjoint, gw, space_time
+from . import adjoint, contour, gw, space_time
 
 LR = 'src.SingleReference.LinearResponse.space_time'
 IT = 'src.SingleReference.GW.imaginary_time'
@@ -85,7 +85,8 @@ def replacements():
              'dyson_screening': space_time.dyson_screening,
              '_sigma_mo_diagonal': _sigma_mo_diagonal, **static},
         BSE: dict(static),
-        CD: dict(static),
+        CD: {**static,
+             'cd_screening_contraction_multi': contour.cd_screening_contraction_multi},
         RF: dict(static),
         ADJ: {'selfenergy_diag_backward': adjoint.selfenergy_diag_backward,
               'screened_interaction_tau_backward': adjoint.screened_interaction_tau_backward,
