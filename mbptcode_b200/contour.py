@@ -22,11 +22,19 @@ frequency serves every state) and each residue frequency's W. The quadrature
 weights, the residue sets and the sums over k and q are host arithmetic on
 nfreq x norb numbers. FP64 throughout.
 
-The reference's root finder for this route (`qp_energy_cd` on
-`Solvers/qp_equation.py` `solve_qp_equation_scan`) is not part of this module;
-the explicit O(N^4) particle-hole backends (`C_ov`) are not either.
+The quasiparticle equation of this route, w = eps_p + xc + Sigma^c(w), is
+solved as the reference solves it (`qp_energy_cd` on
+``Solvers/qp_equation.py`` `solve_qp_equation_scan`, without a followed root):
+a grid over the narrowest window about the bare level walked outward, cells
+halved where the secant slope hides a pole, each bracket refined by Newton on
+the closed-form slope (`sigma_cd_slope`) safeguarded by the bracket, the
+weights of a positive-weight self-energy summing to one ending the walk. The
+explicit O(N^4) particle-hole backends (`C_ov`) are not part of this module.
 """
 from __future__ import annotations
+
+import warnings
+from collections import OrderedDict
 
 import numpy as np
 import torch
@@ -40,6 +48,12 @@ RESIDUE_ON_CONTOUR_TOL = 1e-10   # :461
 CD_NFREQ = 64                    # :478
 CD_NTAU = 24                     # :493
 LAPLACE_SCREENING_TOL = 1e-8     # :577
+QP_GRAPHICAL_N_OMEGA = 150       # :273
+QP_ROOT_TOL, QP_ROOT_MAX_ITER = 1e-11, 100   # :501-502
+QP_WINDOW_Z_MIN = 0.5            # :553
+QP_SEARCH_WINDOW_TIERS = ((0.0, 0.5), (1.5, 1.0), (4.0, 2.0))   # :1464
+QP_SCAN_SECANT_MIN, QP_SCAN_SPLIT_DEPTH = 0.5, 6                # :1613-1614
+QP_WEIGHT_SUM_SLACK = 1e-3       # :1625
 
 _MAX_J = 32  # output rows per transform call (the transform kernel's limit is 34)
 
@@ -245,13 +259,18 @@ class LaplaceRealScreening:
     each frequency kept for later calls (``real_screening.py:94-154``).
     Refuses (ResidueRefused) a frequency the grid does not carry."""
 
-    def __init__(self, proj_tau, grid, eps, nocc, tol=LAPLACE_SCREENING_TOL):
+    def __init__(self, proj_tau, grid, eps, nocc, tol=LAPLACE_SCREENING_TOL,
+                 cache_bytes=4e9):
         self.proj_tau = to_device(proj_tau, require_device())
         self.grid = grid
         self.eps = np.asarray(eps, float)
         self.nocc = nocc
         self.tol = tol
-        self._w = {}
+        # the latest frequencies' W - I (the value and the slope of one point
+        # apply W at the same frequencies), bounded by memory
+        naux = self.proj_tau.shape[-1]
+        self._cap = max(2, min(2 * len(self.eps), int(cache_bytes // (8 * naux * naux))))
+        self._w = OrderedDict()
 
     def representation_error(self, freq):
         return laplace_representation_error(self.grid, self.eps, self.nocc, freq)
@@ -269,18 +288,31 @@ class LaplaceRealScreening:
 
     def w_minus_identity(self, freq):
         key = float(freq)
-        if key not in self._w:
+        w = self._w.get(key)
+        if w is None:
             c, _ = self._weights(key)
             chi0 = _rows_transform(self.proj_tau, c[None, :])
             dyson_batch(chi0, want_w=True, precision='fp64')
-            self._w[key] = chi0[0]
-        return self._w[key]
+            w = self._w[key] = chi0[0]
+            if len(self._w) > self._cap:
+                self._w.popitem(last=False)
+        else:
+            self._w.move_to_end(key)
+        return w
 
     def apply(self, freq, b):
         """W(freq) b = b + (W - I) b."""
         bd = to_device(b, self.proj_tau.device)
         y = bd + self.w_minus_identity(freq) @ bd
         return y if isinstance(b, torch.Tensor) else y.cpu().numpy()
+
+    def slope(self, freq, y):
+        """y^T [dchi0/dfreq] y, dchi0/dfreq = sum_k dc_k proj(tau_k)
+        (``real_screening.py:152-154``)."""
+        _, dc = self._weights(freq)
+        dchi0 = _rows_transform(self.proj_tau, dc[None, :])[0]
+        yd = to_device(y, self.proj_tau.device)
+        return float(yd @ (dchi0 @ yd))
 
 
 def sigma_cd(p, omega, Bp, eps, nocc, nu_points, nu_weights, residues=None, wbp=None,
@@ -312,3 +344,241 @@ def sigma_cd(p, omega, Bp, eps, nocc, nu_points, nu_weights, residues=None, wbp=
             y = real_screening.apply(abs(eps[q] - omega), b)
             s_res += weight * (float(b @ y) - float(b @ b))
     return s_int + s_res
+
+
+def sigma_cd_slope(p, omega, Bp, eps, nocc, nu_points, nu_weights, residues, wc, eta=0.0,
+                   C_ov=None, real_screening=None):
+    """dSigma^c_pp/domega in closed form at a frozen residue set
+    (``contour_deformation.py:346-373``): the integral weights' derivative
+    against wc, and per residue W [dchi0/dfreq] W contracted with b_q on both
+    sides, signed by the side of the pole."""
+    if C_ov is not None or eta:
+        raise NotImplementedError('the explicit particle-hole backends are outside the '
+                                  'cubic device route')
+    eps = np.asarray(eps, float)
+    Bh = Bp.detach().cpu().numpy() if isinstance(Bp, torch.Tensor) else np.asarray(Bp)
+    wc = wc.detach().cpu().numpy() if isinstance(wc, torch.Tensor) else np.asarray(wc)
+    _, dc = cd_integral_weights(omega - eps, nu_points, nu_weights)
+    slope = -float(np.einsum('kq,kq->', dc, wc)) / np.pi
+    for q, weight in residues or ():
+        gap = eps[q] - omega
+        freq = abs(gap)
+        y = real_screening.apply(freq, Bh[:, q])
+        slope -= weight * real_screening.slope(freq, y) * np.sign(gap)
+    return slope
+
+
+# ------------------------------------------------ the scan root finder
+# Solvers/qp_equation.py: `solve_qp_equation_scan` (:1396-1420) on a
+# `SampledEquation` (:1029-1278) through `find_qp_root` (:155-233) without a
+# followed root, as `qp_energy_cd` calls it.
+
+def _qp_search_windows(a):
+    """Windows about the bare level, narrowest first: the tier of the
+    state's depth, then every wider tier (:1280-1288)."""
+    tier = 0
+    for k, (depth, _) in enumerate(QP_SEARCH_WINDOW_TIERS):
+        if abs(a) > depth:
+            tier = k
+    return [(a - half, a + half) for _, half in QP_SEARCH_WINDOW_TIERS[tier:]]
+
+
+def _valid_weight(z, z_min=0.0):
+    """Z of a quasiparticle: finite and in (z_min, 1] (:95-102)."""
+    z = float(z)
+    return bool(np.isfinite(z) and z_min < z <= 1.0)
+
+
+def _bracketed_newton(fval, l, r, sl, tol, max_iter):
+    """The root of f in (l, r), f of sign sl at l, by Newton on the slope
+    safeguarded by the bracket: a step leaving it, or not under half the step
+    before the last, is a bisection; a step below tol that stays in the
+    closed bracket ends it (:376-426, for a costly f)."""
+    if sl == 0.0:
+        return float(l)
+    w = 0.5 * (l + r)
+    step = old = r - l
+    for _ in range(int(max_iter)):
+        f, fp = fval(w)
+        if f == 0.0:
+            return float(w)
+        if np.sign(f) == sl:
+            l = w
+        else:
+            r = w
+        dw = -f / fp
+        if abs(dw) < tol and l <= w + dw <= r:
+            return float(w + dw)
+        mid = 0.5 * (l + r)
+        if not l < mid < r:
+            break
+        newton = np.isfinite(dw) and l < w + dw < r and abs(dw) <= 0.5 * abs(old)
+        old, step = step, (dw if newton else mid - w)
+        w = w + dw if newton else mid
+    return float(w)
+
+
+class _Scan:
+    """f(w) = w - a - Sigma(w) known pointwise with a closed-form slope, for
+    a positive-weight Sigma; points a refusal type rejects are NaN, the first
+    refusal kept (:1071-1092, :1143-1166, :1250-1278)."""
+
+    def __init__(self, func, fprime, tol, max_iter, refusals):
+        self.tol, self.max_iter = tol, max_iter
+        self.refusals, self.refused = tuple(refusals), None
+        self.func, self.fprime = self._guarded(func), self._guarded(fprime)
+
+    def _guarded(self, g):
+        def call(w):
+            try:
+                return g(w)
+            except self.refusals as refusal:
+                if self.refused is None:
+                    self.refused = refusal
+                return np.nan
+        return call
+
+    def weight(self, w):
+        fp = float(self.fprime(w))
+        return 1.0 / fp if fp != 0.0 else np.nan
+
+    def solve(self, bracket):
+        """[(root, Z)] of a bracket (l, r, f(l), f(r)); empty for a pole."""
+        l, r, fl, fr = bracket
+        if l == r:
+            return [(float(l), self.weight(l))]
+        if fl > 0.0 > fr:
+            return []                   # f falls: a pole of a positive-weight Sigma
+        fval = lambda x: (float(self.func(x)), float(self.fprime(x)))  # noqa: E731
+        w = _bracketed_newton(fval, l, r, np.sign(fl), self.tol, self.max_iter)
+        fw = fval(w)[0]
+        if not abs(fw) <= max(abs(fl), abs(fr)):
+            return []                   # |f| grew (a pole) or the point was refused
+        return [(float(w), self.weight(w))]
+
+    def cells(self, l, r, fl, fr, depth):
+        """Brackets in [l, r]: the cell on a sign change; its halves while
+        its secant slope is below QP_SCAN_SECANT_MIN or one end is refused
+        and the other not, at most `depth` times (:1250-1266)."""
+        if fl * fr < 0.0:
+            return [(l, r, fl, fr)]
+        edge = np.isnan(fl) != np.isnan(fr)
+        if depth == 0 or fl == 0.0 or fr == 0.0 or not (
+                edge or fr - fl < QP_SCAN_SECANT_MIN * (r - l)):
+            return []
+        m = 0.5 * (l + r)
+        fm = float(self.func(m))
+        return self.cells(l, m, fl, fm, depth - 1) + self.cells(m, r, fm, fr, depth - 1)
+
+    def outward(self, lo, hi, a):
+        """The brackets of each grid cell, cells in increasing distance from
+        the one holding a, f evaluated as the cells reach a grid point
+        (:1110-1129)."""
+        grid = np.linspace(lo, hi, QP_GRAPHICAL_N_OMEGA)
+        f = {}
+
+        def value(j):
+            if j not in f:
+                f[j] = float(self.func(grid[j]))
+            return f[j]
+        c0 = min(max(int(np.searchsorted(grid, a)) - 1, 0), grid.size - 2)
+        for d in range(grid.size - 1):
+            for c in sorted({c0 - d, c0 + d}):
+                if 0 <= c < grid.size - 1:
+                    yield self.cells(grid[c], grid[c + 1], value(c), value(c + 1),
+                                     QP_SCAN_SPLIT_DEPTH)
+
+
+def _weighed_outward(scan, lo, hi, a, enough):
+    """[(root, Z)] of the cells walked outward from a, until the valid
+    weights found leave (plus QP_WEIGHT_SUM_SLACK) no more of their sum, one,
+    than the largest of them or `enough` (:312-339)."""
+    found, best, weighed = [], -np.inf, 0.0
+    for brackets in scan.outward(lo, hi, a):
+        for bracket in brackets:
+            got = scan.solve(bracket)
+            found.append((bracket[0], got))
+            for _, z in got:
+                if _valid_weight(z):
+                    weighed += z
+                    best = max(best, z)
+        if 1.0 - weighed + QP_WEIGHT_SUM_SLACK <= max(best, enough):
+            break
+    found.sort(key=lambda lr: lr[0])
+    return [rz for _, got in found for rz in got]
+
+
+def solve_qp_equation_scan(residual, fprime, a, tol=QP_ROOT_TOL, max_iter=QP_ROOT_MAX_ITER,
+                           label='', refusals=()):
+    """(w, Z) of residual(w) = 0 for a positive-weight self-energy: per
+    window, narrowest first, the root of largest valid weight; a weight above
+    QP_WINDOW_Z_MIN ends the search, the widest window keeps its largest
+    valid weight (the root nearest a if none is valid). No quasiparticle
+    where Sigma could be evaluated raises the first refusal; no root at all
+    is (NaN, NaN) with a QPNoRoot warning; a root with Z outside (0, 1] is
+    kept with a QPWeightOutside warning (:155-273, :1396-1420)."""
+    from .gw import QPNoRoot, QPWeightOutside
+    scan = _Scan(residual, fprime, tol, max_iter, refusals)
+    windows = _qp_search_windows(a)
+    found, w, z, quasi = [], np.nan, np.nan, False
+    for i, (lo, hi) in enumerate(windows):
+        enough = QP_WINDOW_Z_MIN if i + 1 < len(windows) else -np.inf
+        found = _weighed_outward(scan, lo, hi, a, enough)
+        ok = [k for k, (_, zk) in enumerate(found) if _valid_weight(zk)]
+        if ok:
+            k = max(ok, key=lambda j: found[j][1])
+            if _valid_weight(found[k][1], QP_WINDOW_Z_MIN):
+                w, z, quasi = found[k][0], found[k][1], True
+                break
+    if not quasi:
+        if scan.refused is not None:
+            raise scan.refused
+        if not found:
+            warnings.warn(f'{label or "the quasiparticle equation"} has no root in the widest '
+                          f'scan window [{windows[-1][0]:.6f}, {windows[-1][1]:.6f}] Ha about '
+                          f'{a:.6f} Ha.', QPNoRoot, stacklevel=2)
+            return np.nan, np.nan
+        ok = [k for k, (_, zk) in enumerate(found) if _valid_weight(zk)]
+        k = (max(ok, key=lambda j: found[j][1]) if ok
+             else min(range(len(found)), key=lambda j: abs(found[j][0] - a)))
+        w, z = found[k]
+    if np.isfinite(w) and not 0.0 < z <= 1.0:
+        warnings.warn(f'the quasiparticle root of {label or "the quasiparticle equation"} '
+                      f'{w!r} Ha has Z = {z!r}, outside (0, 1]: kept', QPWeightOutside,
+                      stacklevel=2)
+    return float(w), float(z)
+
+
+def qp_energy_cd(p, Bp, eps, nocc, nu_points, nu_weights, xc_correction=0.0, tol=QP_ROOT_TOL,
+                 max_iter=QP_ROOT_MAX_ITER, follow=None, wbp=None, wc=None, C_ov=None,
+                 eta=0.0, real_screening=None, branch=None, rescan=True):
+    """(eps^QP_p, Z_p, residues) of w = eps_p + xc_correction + Sigma^c(w) by
+    contour deformation (``contour_deformation.py:376-436``): the scan about
+    the bare level with Newton on the closed-form slope, the residue set
+    re-decided at every point and frozen at the root."""
+    if follow is not None or branch is not None:
+        raise NotImplementedError('following a root along a walk is outside the device route')
+    if C_ov is not None or eta:
+        raise NotImplementedError('the explicit particle-hole backends are outside the '
+                                  'cubic device route')
+    eps = np.asarray(eps, float)
+    Bh = Bp.detach().cpu().numpy() if isinstance(Bp, torch.Tensor) else np.asarray(Bp)
+    if wc is None:
+        if wbp is None:
+            raise ValueError('qp_energy_cd needs wc or wbp on the device route')
+        wc = screening_contraction(Bh, wbp)
+    wc = wc.detach().cpu().numpy() if isinstance(wc, torch.Tensor) else np.asarray(wc)
+
+    def residual(w):
+        return w - eps[p] - xc_correction - sigma_cd(
+            p, w, Bh, eps, nocc, nu_points, nu_weights, residues=residue_set(eps, nocc, w),
+            wc=wc, real_screening=real_screening)
+
+    def fprime(w):
+        return 1.0 - sigma_cd_slope(p, w, Bh, eps, nocc, nu_points, nu_weights,
+                                    residue_set(eps, nocc, w), wc,
+                                    real_screening=real_screening)
+    w, z = solve_qp_equation_scan(residual, fprime, float(eps[p] + xc_correction), tol=tol,
+                                  max_iter=max_iter, label=f'orbital {p}',
+                                  refusals=(ResidueRefused,))
+    return w, z, residue_set(eps, nocc, w)

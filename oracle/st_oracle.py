@@ -647,13 +647,16 @@ def evgw(X, D, eps0, nocc, ntau, tol=EVGW_TOL, max_cycle=EVGW_MAX_CYCLE,
 # Laplace real-frequency screening and Sigma^c(omega)
 # ---------------------------------------------------------------------------
 
-def cd_integral_weights(de, nu, wt, on_contour_tol=1e-10):
+def cd_integral_weights(de, nu, wt, on_contour_tol=1e-10, with_slope=False):
     """contour_deformation.py:150-202: quadrature weights of the Lorentzian
     with its singular part (wc(0) times de/(de^2+nu^2) a^2/(a^2+nu^2))
-    integrated in closed form; wc(0) from the two smallest nodes."""
+    integrated in closed form; wc(0) from the two smallest nodes. With
+    with_slope also their derivative in de."""
     de, nu, wt = (np.asarray(a, float) for a in (de, nu, wt))
-    g = de[None, :] / (de[None, :] ** 2 + nu[:, None] ** 2)
-    c = wt[:, None] * g
+    den = de[None, :] ** 2 + nu[:, None] ** 2
+    g = de[None, :] / den
+    dg = (nu[:, None] ** 2 - de[None, :] ** 2) / den ** 2
+    c, dc = wt[:, None] * g, wt[:, None] * dg
     order = np.argsort(nu)
     k1, k2 = order[0], order[1]
     n1, n2 = nu[k1] ** 2, nu[k2] ** 2
@@ -661,9 +664,11 @@ def cd_integral_weights(de, nu, wt, on_contour_tol=1e-10):
     h = wt * a * a / (a * a + nu ** 2)
     side = np.where(np.abs(de) < on_contour_tol, 0.0, np.sign(de))
     err = 0.5 * np.pi * side * a / (a + np.abs(de)) - h @ g
-    c[k1] += n2 / (n2 - n1) * err
-    c[k2] += -n1 / (n2 - n1) * err
-    return c
+    derr = -0.5 * np.pi * a / (a + np.abs(de)) ** 2 - h @ dg
+    for k, coef in ((k1, n2 / (n2 - n1)), (k2, -n1 / (n2 - n1))):
+        c[k] += coef * err
+        dc[k] += coef * derr
+    return (c, dc) if with_slope else c
 
 
 def cd_screening_contraction(proj_tau, cosft_wt, Bps):
@@ -692,6 +697,43 @@ def residue_set(eps, nocc, omega, tol=1e-10):
     return out
 
 
+class LaplaceRefused(ValueError):
+    """real_screening.py:128-146: a real frequency the time grid's bare
+    quadrature does not carry (error of y sum w e^{-y tau} = 1 above 1e-8
+    on y = d -+ freq, LinearResponse/space_time.py:908-931)."""
+
+
+def laplace_check(eps, nocc, tau, tau_w, freq, tol=1e-8):
+    eps = np.asarray(eps, float)
+    d = (eps[nocc:][None, :] - eps[:nocc][:, None]).ravel()
+    y = np.concatenate([d - freq, d + freq])
+    if y.min() <= 0.0 or not float(np.abs(
+            (np.exp(-np.outer(y, tau)) @ tau_w) * y - 1.0).max()) < tol:
+        raise LaplaceRefused(freq)
+
+
+def laplace_screening_slope(proj_tau, tau, tau_w, freq, y):
+    """real_screening.py:152-154: y^T [sum_k 2 w_k tau_k sinh(freq tau_k)
+    proj(tau_k)] y."""
+    dc = 2.0 * np.asarray(tau_w) * np.asarray(tau) * np.sinh(freq * np.asarray(tau))
+    return float(y @ np.tensordot(dc, proj_tau, axes=(0, 0)) @ y)
+
+
+def sigma_cd_slope(p, omega, Bp, eps, nocc, nu, nu_w, wc, proj_tau, tau, tau_w):
+    """contour_deformation.py:346-373 with the Laplace residue backend (the
+    representability check of real_screening.py:132-145 on each frequency)."""
+    eps = np.asarray(eps, float)
+    _, dc = cd_integral_weights(omega - eps, nu, nu_w, with_slope=True)
+    slope = -float(np.einsum('kq,kq->', dc, wc)) / np.pi
+    for q, weight in residue_set(eps, nocc, omega):
+        gap = eps[q] - omega
+        freq = abs(gap)
+        laplace_check(eps, nocc, tau, tau_w, freq)
+        y = laplace_screening_apply(proj_tau, tau, tau_w, freq, Bp[:, q])
+        slope -= weight * laplace_screening_slope(proj_tau, tau, tau_w, freq, y) * np.sign(gap)
+    return slope
+
+
 def laplace_screening_apply(proj_tau, tau, tau_w, freq, b):
     """real_screening.py:147-150 with :184-209: W(freq) b, chi0(freq) =
     sum_k 2 w_k cosh(freq tau_k) proj(tau_k), below the gap."""
@@ -707,6 +749,7 @@ def sigma_cd(p, omega, Bp, eps, nocc, nu, nu_w, wc, proj_tau, tau, tau_w):
     s = -float(np.einsum('kq,kq->', c, wc)) / np.pi
     for q, weight in residue_set(eps, nocc, omega):
         b = Bp[:, q]
+        laplace_check(eps, nocc, tau, tau_w, abs(eps[q] - omega))
         y = laplace_screening_apply(proj_tau, tau, tau_w, abs(eps[q] - omega), b)
         s += weight * (b @ y - b @ b)
     return s

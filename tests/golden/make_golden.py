@@ -378,8 +378,9 @@ def contour_fixture():
     (64 Gauss-Legendre frequencies on half the gap, 24 time points reaching
     half a gap below it), proj(tau) on it, the screening contraction wc of
     three states around the gap, Sigma^c at points on both sides of each
-    state's level and on it (residues through the Laplace backend), and the
-    integral weights at a set of de values."""
+    state's level and on it (residues through the Laplace backend), each
+    state's quasiparticle root and Z (`qp_energy_cd`), and the integral
+    weights at a set of de values."""
     cd, rs = _import_contour_deformation()
     from src.gradients.rpa.space_time_adjoint import polarizability_tau
     from src.SingleReference.LinearResponse.space_time import three_index_slice
@@ -400,13 +401,18 @@ def contour_fixture():
         for j, dw in enumerate(shifts):
             sig[i, j] = cd.sigma_cd(int(p), eps[p] + dw, Bps[i], eps, nocc, nu, nu_w,
                                     wc=wcs[i], real_screening=lap)
+    roots = np.zeros((len(states), 2))
+    for i, p in enumerate(states):
+        w, z, _ = cd.qp_energy_cd(int(p), Bps[i], eps, nocc, nu, nu_w, wc=wcs[i],
+                                  real_screening=rs.LaplaceRealScreening(proj, grid, eps, nocc))
+        roots[i] = w, z
     de = np.array([-0.3, -1e-3, 0.0, 1e-12, 2e-3, 0.05, 0.7])
     c, dc = cd.cd_integral_weights(de, nu, nu_w)
     np.savez_compressed(
         os.path.join(HERE, 'contour.npz'), X=X, D=D, eps=eps, nocc=nocc, mu=mu, nu=nu,
         nu_w=nu_w, w0=w0, tau=grid.tau_points, tau_w=grid.tau_weights, cosft_wt=grid.cosft_wt,
         proj=proj, states=states, B=np.stack(Bps), wc=np.stack(wcs), shifts=shifts, sigma=sig,
-        de=de, c=c, dc=dc)
+        roots=roots, de=de, c=c, dc=dc)
 
 
 def qp_fixture():

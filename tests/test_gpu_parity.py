@@ -501,3 +501,10 @@ def test_contour_deformation_device_matches_reference_golden(golden):
     gap = eps[nocc] - eps[nocc - 1]
     with pytest.raises(contour.ResidueRefused):
         lap.apply(gap, B[0][:, 0])
+    # the quasiparticle roots and Z of the three states (`qp_energy_cd`: the
+    # scan with Newton on the closed-form slope, the device's Sigma^c)
+    for i, p in enumerate(g['states']):
+        w, z, res = contour.qp_energy_cd(int(p), B[i], eps, nocc, nu, nu_w, wc=wcs[i],
+                                         real_screening=lap)
+        assert abs(w - g['roots'][i, 0]) < 1e-9 and abs(z - g['roots'][i, 1]) < 1e-8, p
+        assert res == contour.residue_set(eps, nocc, w)

@@ -265,3 +265,27 @@ def test_contour_deformation_pieces(golden):
                              g['proj'], g['tau'], g['tau_w'])
             assert abs(s - g['sigma'][i, j]) <= 1e-11 * abs(g['sigma'][i, j]), (p, dw)
     assert contour.residue_set(eps, nocc, eps[nocc]) == orc.residue_set(eps, nocc, eps[nocc])
+
+
+
+def test_contour_root_finder_on_the_oracle(golden):
+    """The contour deformation's scan root finder (restated in
+    mbptcode_b200.contour from Solvers/qp_equation.py) driven by the oracle's
+    Sigma^c and closed-form slope gives the reference's `qp_energy_cd` roots
+    and Z for three states around the gap."""
+    from mbptcode_b200 import contour
+    g = golden('contour')
+    eps, nocc = g['eps'], int(g['nocc'])
+    args = (g['proj'], g['tau'], g['tau_w'])
+    for i, p in enumerate(g['states']):
+        p = int(p)
+        B, wc = g['B'][i], g['wc'][i]
+
+        def residual(w, p=p, B=B, wc=wc):
+            return w - eps[p] - orc.sigma_cd(p, w, B, eps, nocc, g['nu'], g['nu_w'], wc, *args)
+
+        def fprime(w, p=p, B=B, wc=wc):
+            return 1.0 - orc.sigma_cd_slope(p, w, B, eps, nocc, g['nu'], g['nu_w'], wc, *args)
+        w, z = contour.solve_qp_equation_scan(residual, fprime, float(eps[p]),
+                                              refusals=(orc.LaplaceRefused,))
+        assert abs(w - g['roots'][i, 0]) < 1e-10 and abs(z - g['roots'][i, 1]) < 1e-9, p
