@@ -582,3 +582,81 @@ def qp_energy_cd(p, Bp, eps, nocc, nu_points, nu_weights, xc_correction=0.0, tol
                                   max_iter=max_iter, label=f'orbital {p}',
                                   refusals=(ResidueRefused,))
     return w, z, residue_set(eps, nocc, w)
+
+
+HARTREE_TO_EV = 27.211386245988  # MBPTcode constants.py:11 (CODATA 2018)
+
+
+def contour_roots(X, D, eps, nocc, states, ntau=CD_NTAU, nfreq_cd=CD_NFREQ, w0_cd=None,
+                  e_min_below_gap=None, xc_correction=0.0, mu=None):
+    """(roots in Hartree, Z, per-state records) of the states on one contour
+    grid with the residues from the cosh transform of proj(tau)
+    (``contour_deformation.py:558-598, 780-812``, continuation 'laplace'):
+    one proj(tau) and one W per frequency serve every state, each state's
+    root by `qp_energy_cd`. xc_correction: the static term, one per state or
+    one for all."""
+    eps = _eps_host(eps)
+    states = np.atleast_1d(np.asarray(states, int))
+    nu, nu_w, grid, w0 = cd_frequency_grid(eps, nocc, ntau=ntau, nfreq_cd=nfreq_cd,
+                                           w0_cd=w0_cd, e_min_below_gap=e_min_below_gap)
+    proj = polarizability_tau(X, D, eps, nocc, grid, mu=mu)
+    B = three_index_slices(X, D, states)
+    wcs = cd_screening_contraction_multi(proj, grid.cosft_wt, list(B))
+    lap = LaplaceRealScreening(proj, grid, eps, nocc)
+    roots, zs, records = np.zeros(len(states)), np.zeros(len(states)), []
+    for i, p in enumerate(states):
+        xc = (float(np.asarray(xc_correction).ravel()[i]) if np.ndim(xc_correction)
+              else float(xc_correction))
+        try:
+            w, z, res = qp_energy_cd(int(p), B[i], eps, nocc, nu, nu_w, xc_correction=xc,
+                                     wc=wcs[i], real_screening=lap)
+        except ResidueRefused as refusal:
+            raise ResidueRefused(
+                f"continuation='laplace' cannot serve orbital {int(p)}: its contour sweeps "
+                f'a residue the imaginary-time grid does not represent. {refusal}') from refusal
+        roots[i], zs[i] = w, z
+        records.append({'state': int(p), 'residues': len(res),
+                        'representation_error': (max(lap.representation_error(
+                            abs(eps[q] - w)) for q, _ in res) if res else None)})
+    info = {'continuation': 'laplace', 'ntau': int(ntau), 'nfreq_cd': int(nfreq_cd),
+            'w0_cd': float(w0), 'residue_route_taken': 'laplace', 'states': records}
+    return roots, zs, info
+
+
+def solve_qp_energy_contour(mf, mol, nocc, states, continuation='laplace', numerics=None,
+                            w0_cd=None, auxbasis=None, radii=None, counts=None, factors=None,
+                            grid_accuracy=None, sigma_x='mf', dm_correction=None,
+                            eps_anchor=None, spin_channel='alpha', xc_diagonal=None):
+    """Drop-in for ``GW/contour_deformation.py:601-820`` on a restricted
+    gas-phase reference with pre-built factors, continuation 'laplace':
+    (quasiparticle energies in eV, pole strengths, diagnostics). The mean
+    field gives eps (mo_energy); the static term <Sigma_x - v_xc> is
+    `xc_diagonal` (zero on a Hartree-Fock reference); numerics.quadrature:
+    ntau_cd and nfreq_cd where it has them. 'cd' (the explicit O(N^4)
+    residues, the reference's default) and 'sop' are outside the device
+    route and refused; 'laplace' solves the same contour wherever the time
+    grid carries the residue frequencies, and refuses a state by name
+    otherwise, as the reference does."""
+    if continuation != 'laplace':
+        raise NotImplementedError(f"continuation={continuation!r}: the device route runs "
+                                  "'laplace' (the cubic residues)")
+    if factors is None:
+        raise NotImplementedError('building the ISDF factors needs pyscf (integrals and the '
+                                  'fit); pass factors=(X_mo, D)')
+    eps = np.asarray(getattr(mf, 'mo_energy', mf), float)
+    if eps.ndim != 1:
+        raise NotImplementedError('an unrestricted reference is outside the contour route '
+                                  'on the device')
+    ntau, nfreq = CD_NTAU, CD_NFREQ
+    if numerics is not None:
+        q = numerics.quadrature
+        ntau = getattr(q, 'ntau_cd', ntau)
+        nfreq = getattr(q, 'nfreq_cd', nfreq)
+    states = np.atleast_1d(np.asarray(states, int))
+    xc = 0.0 if xc_diagonal is None else np.asarray(xc_diagonal, float)
+    if eps_anchor is not None:
+        xc = xc + (np.asarray(eps_anchor, float)[states] - eps[states])
+    X, D = (factors['X_mo'], factors['D']) if isinstance(factors, dict) else factors[:2]
+    roots, zs, info = contour_roots(X, D, eps, nocc, states, ntau=ntau, nfreq_cd=nfreq,
+                                    w0_cd=w0_cd, xc_correction=xc)
+    return roots * HARTREE_TO_EV, zs, info

@@ -508,3 +508,12 @@ def test_contour_deformation_device_matches_reference_golden(golden):
                                          real_screening=lap)
         assert abs(w - g['roots'][i, 0]) < 1e-9 and abs(z - g['roots'][i, 1]) < 1e-8, p
         assert res == contour.residue_set(eps, nocc, w)
+    # the drop-in driver on the same factors (default contour grid): eV roots
+    ev, zs, info = contour.solve_qp_energy_contour(eps, None, nocc, g['states'],
+                                                   factors=(X, D))
+    assert np.abs(ev / contour.HARTREE_TO_EV - g['roots'][:, 0]).max() < 1e-9
+    assert np.abs(zs - g['roots'][:, 1]).max() < 1e-8
+    assert info['continuation'] == 'laplace' and len(info['states']) == 3
+    with pytest.raises(NotImplementedError):
+        contour.solve_qp_energy_contour(eps, None, nocc, g['states'], continuation='cd',
+                                        factors=(X, D))
