@@ -251,6 +251,21 @@ int mbpt_sigma_backward(const double *X_dev, int64_t M, int64_t norb, int64_t no
                         double *D_bar_dev, double *Wt_bar_dev, void *workspace,
                         size_t ws_bytes, int *err_dev, void *stream);
 
+/* The self-energy's two branches as full AO matrices: per time point tau_k
+ *   Sigma^<(tau_k) = X_ao^T (G_occ(tau_k) o Zt_k) X_ao,
+ *   Sigma^>(tau_k) = -X_ao^T (G_virt(tau_k) o Zt_k) X_ao,
+ * G from the MO collocation X_ao mo_coeff (occupied/virtual split at nocc,
+ * eps - mu), Zt_k = D Wt_k D^T: GW/imaginary_time.py:403-533
+ * (`self_energy_matrix_imaginary_time`, before its tau -> omega fold).
+ * out_dev: (2, ntau, nao, nao), lesser branch first. FP64. */
+size_t mbpt_sigma_ao_workspace_bytes(int64_t M, int64_t nao, int64_t norb, int64_t nocc,
+                                     int64_t naux);
+int mbpt_sigma_ao(const double *X_ao_dev, int64_t M, int64_t nao, const double *mo_coeff_dev,
+                  int64_t norb, int64_t nocc, const double *eps_dev, double mu,
+                  const double *D_dev, int64_t naux, const double *Wt_dev,
+                  const double *tau_host, int ntau, double *out_dev, void *workspace,
+                  size_t ws_bytes, int *err_dev, void *stream);
+
 /* ---- contour deformation (GW/contour_deformation.py), FP64 ----------------
  * Three-index slices B_s = D^T diag(X[:, p_s]) X of the states p_s
  * (LinearResponse/space_time.py:804-815 `three_index_slice`), written to

@@ -55,6 +55,21 @@ def chi0_backward(proj_bar, X, D, eps, nocc, tau_points, mu, precision='fp64', s
     return eps_bar, X_bar, D_bar
 
 
+def polarizability_backward(proj_bar, X, D, eps, nocc, grid, mu=None, tile_gb=None,
+                            tau_indices=None):
+    """(eps_bar, X_bar, D_bar) for an adjoint proj_bar (ntau, naux, naux) on
+    proj(tau) (``space_time_adjoint.py:136-164``), the reverse chi0 sweep on
+    the device; arrays come back as proj_bar is held."""
+    if tau_indices is not None:
+        raise NotImplementedError('tau splits over ranks are outside the one-GPU route')
+    dev = require_device()
+    eps_h = _eps_host(eps)
+    if mu is None:
+        mu = particle_hole_window(eps_h, nocc)[2]
+    out = chi0_backward(to_device(proj_bar, dev), X, D, eps_h, nocc, grid.tau_points, mu)
+    return tuple(t if isinstance(proj_bar, torch.Tensor) else t.cpu().numpy() for t in out)
+
+
 def energy_and_adjoint_device(X, D, eps, nocc, grid, mu=None, want_grad=True,
                               precision='fp64', stream=None):
     """(E_c 0-d tensor, eps_bar, X_bar, D_bar) on the device."""
@@ -149,7 +164,7 @@ def selfenergy_diag(X, D, eps, nocc, grid, states, transforms, mu, tile_gb=None,
     the branch sums and the tau -> omega transform with (C, S). Returns
     (sigma (nstates, nfreq_out) complex, (proj_tau, Wt_tau, None)); the
     cache's tensors stay on the device."""
-    from .gw import screened_interaction_tau, sigma_branch_sums, sigma_frequency
+    from .gw import sigma_branch_sums, sigma_frequency, w_tau_from_frequencies
     _one_rank(comm, 'selfenergy_diag')
     dev = require_device()
     Xd, Dd = to_device(X, dev), to_device(D, dev)
@@ -158,7 +173,7 @@ def selfenergy_diag(X, D, eps, nocc, grid, states, transforms, mu, tile_gb=None,
     chi0, proj = chi0_sweep(Xd, Dd, eps_h, nocc, grid.tau_points, grid.cosft_wt, mu=mu,
                             precision=precision, want_proj=True)
     dyson_batch(chi0, want_w=True, precision=precision)
-    Wt = screened_interaction_tau(chi0, Ctw)
+    Wt = w_tau_from_frequencies(chi0, Ctw)
     del chi0
     branch = sigma_branch_sums(Xd, Dd, Wt, eps_h, nocc, grid.tau_points,
                                np.atleast_1d(states), mu, precision)

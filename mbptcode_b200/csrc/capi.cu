@@ -1287,6 +1287,61 @@ int mbpt_chi0_backward(const double *pbar, const double *X, int64_t M, int64_t n
   return back_run(pbar, X, d, eps, mu, D, tau, ntau, eps_bar, X_bar, D_bar, ar, S(stream));
 }
 
+size_t mbpt_sigma_ao_workspace_bytes(int64_t M, int64_t nao, int64_t norb, int64_t nocc,
+                                     int64_t naux) {
+  Arena ar;
+  ar.counting = true;
+  ar.take<double>(M * norb);                 // X_mo
+  ar.take<double>(M * norb);                 // the scaled branches
+  for (int i = 0; i < 3; ++i) ar.take<double>(M * M);
+  ar.take<double>(M * naux);
+  ar.take<double>(M * nao);
+  (void)nocc;
+  return ar.used + 2048;
+}
+
+int mbpt_sigma_ao(const double *X_ao, int64_t M, int64_t nao, const double *mo_coeff,
+                  int64_t norb, int64_t nocc, const double *eps, double mu, const double *D,
+                  int64_t naux, const double *Wt, const double *tau_host, int ntau, double *out,
+                  void *ws, size_t ws_bytes, int *err, void *stream) {
+  (void)err;
+  Dims d(M, norb, nocc, naux);
+  if (!d.ok() || nao < 1 || ntau < 1) return MBPT_ERR_SHAPE;
+  cudaStream_t st = S(stream);
+  Arena ar = arena(ws, ws_bytes);
+  double *Xmo = ar.take<double>(M * norb);
+  double *Xs = ar.take<double>(M * norb);
+  double *Xo_s = Xs, *Xv_s = Xs + M * nocc;
+  double *Go = ar.take<double>(M * M), *Gv = ar.take<double>(M * M), *Zt = ar.take<double>(M * M);
+  double *U = ar.take<double>(M * naux);
+  double *R = ar.take<double>(M * nao);
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  cublasHandle_t h = handles(st).blas;
+  const int64_t nv = norb - nocc, a2 = naux * naux, o2 = nao * nao;
+  // the occupied/virtual split needs the MO collocation; the outer indices
+  // stay AO (GW/imaginary_time.py:403-533)
+  if (!dgemm_rm(h, false, false, M, norb, nao, 1.0, X_ao, nao, mo_coeff, norb, 0.0, Xmo, norb))
+    return MBPT_ERR_CUDA;
+  for (int k = 0; k < ntau; ++k) {
+    launch_scaled_branches(Xmo, M, norb, nocc, eps, mu, tau_host[k], 1.0, Xo_s, Xv_s, st);
+    if (!dgemm_rm(h, false, true, M, M, nocc, 1.0, Xo_s, nocc, Xmo, norb, 0.0, Go, M) ||
+        !dgemm_rm(h, false, true, M, M, nv, 1.0, Xv_s, nv, Xmo + nocc, norb, 0.0, Gv, M) ||
+        !dgemm_rm(h, false, false, M, naux, naux, 1.0, D, naux, Wt + k * a2, naux, 0.0, U, naux) ||
+        !dgemm_rm(h, false, true, M, M, naux, 1.0, U, naux, D, naux, 0.0, Zt, M))
+      return MBPT_ERR_CUDA;
+    launch_hadamard(Go, Zt, M * M, st);
+    launch_hadamard(Gv, Zt, M * M, st);
+    // Sigma^<(tau) = X_ao^T (G_occ o Zt) X_ao, Sigma^>(tau) = -X_ao^T (G_virt o Zt) X_ao
+    if (!dgemm_rm(h, false, false, M, nao, M, 1.0, Go, M, X_ao, nao, 0.0, R, nao) ||
+        !dgemm_rm(h, true, false, nao, nao, M, 1.0, X_ao, nao, R, nao, 0.0, out + k * o2, nao) ||
+        !dgemm_rm(h, false, false, M, nao, M, 1.0, Gv, M, X_ao, nao, 0.0, R, nao) ||
+        !dgemm_rm(h, true, false, nao, nao, M, -1.0, X_ao, nao, R, nao, 0.0,
+                  out + (ntau + k) * o2, nao))
+      return MBPT_ERR_CUDA;
+  }
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
 size_t mbpt_three_index_slices_workspace_bytes(int64_t M, int64_t norb) {
   return sizeof(double) * static_cast<size_t>(M) * norb + 2048;
 }

@@ -283,6 +283,14 @@ def transform_weights(kind, tau, omega, e_min, e_max, regularization=None,
     return (W * phase if forward else W * phase.T), worst
 
 
+def minimax_transform_weights(kind, tau, omega, e_min, e_max, regularization=None,
+                              nodes_factor=200, warn=True):
+    """The reference's name for `transform_weights`
+    (``Base/utils/grids/time_frequency.py:282-380``)."""
+    return transform_weights(kind, tau, omega, e_min, e_max, regularization=regularization,
+                             nodes_factor=nodes_factor, warn=warn)
+
+
 @dataclass
 class TimeFrequencyGrid:
     """Both imaginary axes and the transforms between them (T = 0 minimax).

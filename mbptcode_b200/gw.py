@@ -32,10 +32,96 @@ class QPWeightOutside(RuntimeWarning):
     """A quasiparticle root kept with Z outside (0, 1]."""
 
 
-def screened_interaction_tau(W_minus_I, Ctw, stream=None, out=None):
+def w_tau_from_frequencies(W_minus_I, Ctw, stream=None, out=None):
     """Wt(tau) = sum_w Ctw[tau, w] (W(i w) - I): ``imaginary_time.py:181-195``
     (here from W - I as the Dyson step leaves it), FP64 on the device."""
     return transform(W_minus_I, Ctw, stream, out=out)
+
+
+def _transform_screened(Ctw, W_omega):
+    """sum_w Ctw[., w] (W(i w) - I) from W itself (``imaginary_time.py:181-195``):
+    NumPy in, NumPy out, as the reference."""
+    from .space_time import back
+    dev = require_device()
+    Wm = to_device(W_omega, dev).clone()
+    Wm.diagonal(dim1=-2, dim2=-1).sub_(1.0)
+    return back(transform(Wm, np.asarray(Ctw, float)), W_omega)
+
+
+def self_energy_matrix_imaginary_time(X_ao, D, W_omega, mo_coeff, eps, nocc, tau_points,
+                                      omega_in, omega_out, mu=None, ranges=None,
+                                      tau_indices=None, Wt_tau=None, block_memory_gb=None,
+                                      coords=None, screen_r_cut=None):
+    """Full Sigma^c_{mu nu}(i omega_out) in the AO basis, (nfreq_out, nao, nao)
+    complex (``imaginary_time.py:403-533``): W(tau) from W(i omega_in) (or
+    Wt_tau as given), per time point the two branches X_ao^T (G o Zt) X_ao
+    with G from the MO collocation X_ao mo_coeff (mbpt_sigma_ao, FP64), then
+    Sigma = -1/2 [C (S^> + S^<) + i S (S^> - S^<)]. tau_indices: that subset's
+    contribution. block_memory_gb and coords are accepted for signature
+    compatibility; distance screening (screen_r_cut) is refused. NumPy in,
+    NumPy out."""
+    from .grids import COSINE_TW, COSINE_WT, SINE_TW, sigma_fit_ranges, transform_weights
+    from .space_time import back
+    if screen_r_cut:
+        raise NotImplementedError('distance screening is outside the device route')
+    dev = require_device()
+    eps_h = _eps_host(eps)
+    if mu is None:
+        mu = float(0.5 * (eps_h[:nocc].max() + eps_h[nocc:].min()))
+    rW, rS = ranges or sigma_fit_ranges(eps_h, nocc, mu=mu)
+    tau = np.asarray(tau_points, float)
+    which = np.arange(len(tau)) if tau_indices is None else np.atleast_1d(tau_indices)
+    if Wt_tau is None:
+        Ctw, _ = transform_weights(COSINE_WT, tau, omega_in, *rW, warn=False)
+        Wm = to_device(W_omega, dev).clone()
+        Wm.diagonal(dim1=-2, dim2=-1).sub_(1.0)
+        Wt = transform(Wm, Ctw[which])
+        del Wm
+    else:
+        Wt = to_device(Wt_tau, dev)[torch.as_tensor(which, device=dev)].contiguous()
+    C, _ = transform_weights(COSINE_TW, tau, omega_out, *rS, warn=False)
+    S, _ = transform_weights(SINE_TW, tau, omega_out, *rS, warn=False)
+    Xa, Dd, Cm = to_device(X_ao, dev), to_device(D, dev), to_device(mo_coeff, dev)
+    ed = to_device(eps_h, dev)
+    M, nao = Xa.shape
+    norb, naux, nt = Cm.shape[1], Dd.shape[1], len(which)
+    tau_h, tp = host_array(tau[which])
+    br = torch.empty((2, nt, nao, nao), dtype=torch.float64, device=dev)
+    ws = WORKSPACE.get(lib().mbpt_sigma_ao_workspace_bytes(M, nao, norb, nocc, naux), dev)
+    err = _Err(dev)
+    check(lib().mbpt_sigma_ao(ptr(Xa), M, nao, ptr(Cm), norb, nocc, ptr(ed), float(mu),
+                              ptr(Dd), naux, ptr(Wt), tp, nt, ptr(br), ptr(ws), ws.numel(),
+                              ptr(err.t), stream_ptr()), 'mbpt_sigma_ao')
+    err.check('mbpt_sigma_ao')
+    re = transform((br[1] + br[0]).contiguous(), np.ascontiguousarray(C[:, which]))
+    im = transform((br[1] - br[0]).contiguous(), np.ascontiguousarray(S[:, which]))
+    return back(torch.complex(-0.5 * re, -0.5 * im), X_ao)
+
+
+def sigma_ao_to_mo_diagonal(sigma_ao, mo_coeff, states=None):
+    """MO-diagonal Sigma_pp, (nfreq, nstates), without the full MO matrix
+    (``imaginary_time.py:581-587``)."""
+    if isinstance(sigma_ao, torch.Tensor):
+        Cm = to_device(mo_coeff, sigma_ao.device).to(sigma_ao.dtype)
+        Cm = Cm if states is None else Cm[:, torch.as_tensor(np.atleast_1d(states),
+                                                            device=sigma_ao.device)]
+        return torch.einsum('mp,wmn,np->wp', Cm, sigma_ao, Cm)
+    Cm = np.asarray(mo_coeff) if states is None else np.asarray(mo_coeff)[:, states]
+    return np.einsum('mp,wmn,np->wp', Cm, sigma_ao, Cm, optimize=True)
+
+
+def screened_interaction_tau(proj_tau, grid, Ctw, tile_gb=None, comm=None):
+    """Wt(tau) = sum_w Ctw[t, w] ([I - chi0_w]^-1 - I) from proj(tau)
+    (``imaginary_time.py:590-629``): chi0 on the grid's frequencies by the
+    tau -> omega transform, the Dyson step, the omega -> tau transform; FP64
+    on the device, arrays back as proj_tau is held."""
+    from .space_time import back
+    if comm is not None and comm.Get_size() > 1:
+        raise NotImplementedError('rank splits are outside the one-GPU route')
+    dev = require_device()
+    chi0 = transform(to_device(proj_tau, dev), np.asarray(grid.cosft_wt, float))
+    dyson_batch(chi0, want_w=True, precision='fp64')
+    return back(transform(chi0, np.asarray(Ctw, float)), proj_tau)
 
 
 def sigma_branch_sums(X, D, Wt, eps, nocc, tau_points, states, mu, precision=None,
@@ -232,7 +318,7 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
                                 stream_ptr(stream)), 'mbpt_energy_sum')
     if ev:
         ev[2].record()
-    Wt = screened_interaction_tau(
+    Wt = w_tau_from_frequencies(
         chi0, axes.Ctw, stream,
         out=None if keep else BUFFERS.take('sweep_wt', (len(axes.Ctw), naux, naux), dev))
     W_minus_I = chi0 if keep else None
@@ -351,7 +437,7 @@ def gw_sweep_unrestricted(X_mos, D, spectra, noccs, states=None, ntau='auto', ax
     ow = torch.as_tensor(np.asarray(axes.grid.omega_weights, float), device=dev)
     check(lib().mbpt_energy_sum(ptr(logdet), ptr(trace), ptr(ow), len(ow), ptr(e_c),
                                 stream_ptr(stream)), 'mbpt_energy_sum')
-    Wt = screened_interaction_tau(
+    Wt = w_tau_from_frequencies(
         chi0, axes.Ctw, stream,
         out=BUFFERS.take('sweep_wt', (len(axes.Ctw), naux, naux), dev))
     del chi0

@@ -51,7 +51,7 @@ def _sigma_mo_diagonal(X_mo, D, W_omega, mf, eps, nocc, tau_points, freq_points,
         Ctw, _ = transform_weights(COSINE_WT, tau_points, freq_points, *rW, warn=False)
         Wm = space_time.to_device(W_omega, space_time.require_device()).clone()
         Wm.diagonal(dim1=-2, dim2=-1).sub_(1.0)
-        Wt = gw.screened_interaction_tau(Wm, Ctw)
+        Wt = gw.w_tau_from_frequencies(Wm, Ctw)
     else:
         Wt = Wt_tau
     C, _ = transform_weights(COSINE_TW, tau_points, pade_freq, *rS, warn=False)
@@ -80,7 +80,11 @@ def replacements():
         IT: {**{k: v for k, v in seams.items()
                 if k in ('dyson_screening', 'polarizability_projected_sweep',
                          'polarizability_projected_tau')},
-             'selfenergy_diag': adjoint.selfenergy_diag},
+             'selfenergy_diag': adjoint.selfenergy_diag,
+             'self_energy_matrix_imaginary_time': gw.self_energy_matrix_imaginary_time,
+             'sigma_ao_to_mo_diagonal': gw.sigma_ao_to_mo_diagonal,
+             'screened_interaction_tau': gw.screened_interaction_tau,
+             '_transform_screened': gw._transform_screened},
         ST: {'chi0_imaginary_frequency': space_time.chi0_imaginary_frequency,
              'dyson_screening': space_time.dyson_screening,
              '_sigma_mo_diagonal': _sigma_mo_diagonal, **static},
@@ -88,7 +92,8 @@ def replacements():
         CD: {**static,
              'cd_screening_contraction_multi': contour.cd_screening_contraction_multi},
         RF: dict(static),
-        ADJ: {'selfenergy_diag_backward': adjoint.selfenergy_diag_backward,
+        ADJ: {'polarizability_backward': adjoint.polarizability_backward,
+              'selfenergy_diag_backward': adjoint.selfenergy_diag_backward,
               'screened_interaction_tau_backward': adjoint.screened_interaction_tau_backward,
               'rpa_energy_and_adjoint': adjoint.rpa_energy_and_adjoint,
               'rpa_correlation_energy_space_time':

@@ -753,3 +753,32 @@ def sigma_cd(p, omega, Bp, eps, nocc, nu, nu_w, wc, proj_tau, tau, tau_w):
         y = laplace_screening_apply(proj_tau, tau, tau_w, abs(eps[q] - omega), b)
         s += weight * (b @ y - b @ b)
     return s
+
+
+def self_energy_matrix(X_ao, D, W_omega, mo_coeff, eps, nocc, tau_points, omega_in, omega_out,
+                       mu, tau_indices=None):
+    """GW/imaginary_time.py:403-533 in one block: the full AO Sigma^c(i w_out),
+    G from the MO collocation X_ao mo_coeff, the outer indices AO."""
+    from mbptcode_b200.grids import (COSINE_TW, COSINE_WT, SINE_TW, sigma_fit_ranges,
+                                     transform_weights)
+    eps = np.asarray(eps, float)
+    rW, rS = sigma_fit_ranges(eps, nocc, mu=mu)
+    Ctw = transform_weights(COSINE_WT, tau_points, omega_in, *rW, warn=False)[0]
+    C = transform_weights(COSINE_TW, tau_points, omega_out, *rS, warn=False)[0]
+    S = transform_weights(SINE_TW, tau_points, omega_out, *rS, warn=False)[0]
+    Wt = transform_screened(Ctw, W_omega)
+    X_mo = X_ao @ mo_coeff
+    X_o, X_v = X_mo[:, :nocc], X_mo[:, nocc:]
+    e_o, e_v = eps[:nocc] - mu, eps[nocc:] - mu
+    nao = X_ao.shape[1]
+    out = np.zeros((len(omega_out), nao, nao), dtype=complex)
+    which = range(len(tau_points)) if tau_indices is None else tau_indices
+    for k in which:
+        tau = tau_points[k]
+        Zt = (D @ Wt[k]) @ D.T
+        s_l = X_ao.T @ (((X_o * np.exp(e_o * tau)) @ X_o.T) * Zt) @ X_ao
+        s_g = -X_ao.T @ (((X_v * np.exp(-e_v * tau)) @ X_v.T) * Zt) @ X_ao
+        for w in range(len(omega_out)):
+            out.real[w] += C[w, k] * (s_g + s_l)
+            out.imag[w] += S[w, k] * (s_g - s_l)
+    return -0.5 * out

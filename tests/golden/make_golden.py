@@ -33,6 +33,9 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      (residues through the Laplace backend) and the integral
                      weights (the CD module loads pyscf for its driver; a
                      stand-in that raises on use lets it import here);
+* sigma_ao.npz       the full AO self-energy with an AO collocation that is not
+                     the MO one, a subset of its time points, its MO diagonal,
+                     and the chi0 sweep's reverse for a seeded proj_bar;
 * qp_kat.npz         the root finder on closed-form self-energies
                      (tests/test_qp_refine_root.py's two-pole Sigma and others);
 * c1_<variant>.npz   the synthetic FP64 configuration at full size (n_orb = 400,
@@ -42,7 +45,7 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      stored: the tests regenerate them from the seed and check
                      the regeneration against the stored eps and checksums.
 
-    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour]
+    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|sigma_ao]
 """
 import os
 import sys
@@ -415,6 +418,42 @@ def contour_fixture():
         roots=roots, de=de, c=c, dc=dc)
 
 
+def sigma_ao_fixture():
+    """The full AO self-energy of GW/imaginary_time.py:403-533 with an AO
+    collocation that is not the MO one (X_ao = X_mo C^T, C a seeded orthogonal
+    mo_coeff), its MO diagonal (:581-587), and proj_bar's reverse sweep
+    (gradients/rpa/space_time_adjoint.py:136-164) for a seeded proj_bar."""
+    from src.gradients.rpa.space_time_adjoint import polarizability_backward
+    X, D, eps = synthetic_system(20, 4, 48, 17, 'calibrated')
+    nocc, ntau = 4, 12
+    rng = np.random.default_rng(17)
+    Cmo = np.linalg.qr(rng.standard_normal((20, 20)))[0]
+    X_ao = X @ Cmo.T
+    e_min, e_max, mu = particle_hole_window(eps, nocc)
+    freq, fw = screening_frequency_grid(ntau, eps, nocc, mu=mu)
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        grid = TimeFrequencyGrid.minimax_split(ntau, e_min, e_max, freq, fw)
+    rW, rS = sigma_fit_ranges(eps, nocc, mu=mu)
+    tau_sigma = 0.5 * minimax_time_grid(ntau, *rS)[0]
+    pade = gauss_legendre_grid(16, w0=1.0)[0]
+    chi0 = chi0_imaginary_frequency(X, D, eps, nocc, grid, mu=mu)
+    W = np.stack([dyson_screening(c) for c in chi0])
+    sig = self_energy_matrix_imaginary_time(X_ao, D, W, Cmo, eps, nocc, tau_sigma, freq, pade,
+                                            mu=mu)
+    sig_sub = self_energy_matrix_imaginary_time(X_ao, D, W, Cmo, eps, nocc, tau_sigma, freq,
+                                                pade, mu=mu, tau_indices=[1, 4, 7])
+    states = np.array([nocc - 1, nocc, nocc + 3])
+    diag = sigma_ao_to_mo_diagonal(sig, Cmo, states=states)
+    proj_bar = rng.standard_normal((ntau, 48, 48))
+    eb, xb, db = polarizability_backward(proj_bar, X, D, eps, nocc, grid, mu=mu)
+    np.savez_compressed(
+        os.path.join(HERE, 'sigma_ao.npz'), X=X, X_ao=X_ao, D=D, eps=eps, nocc=nocc, mo=Cmo,
+        mu=mu, ntau=ntau, omega=freq, tau_sigma=tau_sigma, pade=pade, W=W, sigma=sig,
+        sigma_sub=sig_sub, states=states, diag=diag, proj_bar=proj_bar, eps_bar=eb, X_bar=xb,
+        D_bar=db)
+
+
 def qp_fixture():
     cases = {  # poles placed off the scan grids, so no division hits one
         'two_pole': (lambda w: 0.05 / (w + 0.8) + 0.01 / (w - 0.9), -0.2),
@@ -458,12 +497,17 @@ if __name__ == '__main__':
         sigma_adjoint_fixture()
         print('self-energy adjoint fixture written to', HERE)
         sys.exit(0)
+    if ONLY == 'sigma_ao':
+        sigma_ao_fixture()
+        print('AO self-energy fixture written to', HERE)
+        sys.exit(0)
     if ONLY == 'contour':
         contour_fixture()
         print('contour-deformation fixture written to', HERE)
         sys.exit(0)
     if ONLY:
-        sys.exit(f'--only {ONLY}: choose c1, static, unrestricted, sigma_adjoint or contour')
+        sys.exit(f'--only {ONLY}: choose c1, static, unrestricted, sigma_adjoint, contour or '
+                 'sigma_ao')
     grids_fixture()
     shared_kernel_fixture()
     route_fixture('calibrated', 24, 4, 64, 7, 'calibrated', 12, full=True)
@@ -474,4 +518,5 @@ if __name__ == '__main__':
     unrestricted_fixture()
     sigma_adjoint_fixture()
     contour_fixture()
+    sigma_ao_fixture()
     print('fixtures written to', HERE)

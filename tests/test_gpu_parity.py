@@ -79,7 +79,7 @@ def test_dyson_and_transform_match_oracle(golden):
     g = golden('route_calibrated')
     W = st.dyson_screening(g['chi0'], correlation=True)
     assert rel(W, g['W_minus_I']) < 1e-11
-    Wt = gw.screened_interaction_tau(torch.as_tensor(g['W_minus_I'], device='cuda'), g['Ctw'])
+    Wt = gw.w_tau_from_frequencies(torch.as_tensor(g['W_minus_I'], device='cuda'), g['Ctw'])
     assert rel(Wt.cpu().numpy(), g['Wt']) < 1e-12
 
 
@@ -517,3 +517,35 @@ def test_contour_deformation_device_matches_reference_golden(golden):
     with pytest.raises(NotImplementedError):
         contour.solve_qp_energy_contour(eps, None, nocc, g['states'], continuation='cd',
                                         factors=(X, D))
+
+
+def test_ao_self_energy_and_mirrors_match_reference_golden(golden):
+    """self_energy_matrix_imaginary_time (full AO matrix, an AO collocation
+    that is not the MO one; all time points and a subset), its MO diagonal,
+    screened_interaction_tau from proj(tau) and polarizability_backward,
+    under the reference's names and signatures, against the reference."""
+    g = golden('sigma_ao')
+    X, X_ao, D, eps, nocc, mo = g['X'], g['X_ao'], g['D'], g['eps'], int(g['nocc']), g['mo']
+    mu = float(g['mu'])
+    args = (X_ao, D, g['W'], mo, eps, nocc, g['tau_sigma'], g['omega'], g['pade'])
+    sig = gw.self_energy_matrix_imaginary_time(*args, mu=mu)
+    assert isinstance(sig, np.ndarray) and sig.dtype == complex
+    assert rel(sig, g['sigma']) < 1e-10
+    sub = gw.self_energy_matrix_imaginary_time(*args, mu=mu, tau_indices=[1, 4, 7])
+    assert rel(sub, g['sigma_sub']) < 1e-10
+    diag = gw.sigma_ao_to_mo_diagonal(sig, mo, states=g['states'])
+    assert rel(diag, g['diag']) < 1e-10
+    axes_grid = grids.TimeFrequencyGrid.minimax_split(
+        int(g['ntau']), *grids.particle_hole_window(eps, nocc)[:2], g['omega'],
+        grids.screening_frequency_grid(int(g['ntau']), eps, nocc, mu=mu)[1],
+        with_sine=False, with_inverse=False)
+    proj = orc.polarizability_projected_sweep(X, D, eps, nocc, axes_grid.tau_points, mu)
+    rW, _ = grids.sigma_fit_ranges(eps, nocc, mu=mu)
+    Ctw = grids.minimax_transform_weights(grids.COSINE_WT, g['tau_sigma'], g['omega'], *rW,
+                                          warn=False)[0]
+    Wt = gw.screened_interaction_tau(proj, axes_grid, Ctw)
+    assert rel(Wt, orc.screened_interaction_tau(proj, axes_grid, Ctw)) < 1e-11
+    from mbptcode_b200 import adjoint
+    out = adjoint.polarizability_backward(g['proj_bar'], X, D, eps, nocc, axes_grid, mu=mu)
+    for a, k in zip(out, ('eps_bar', 'X_bar', 'D_bar')):
+        assert rel(a, g[k]) < 1e-10, k

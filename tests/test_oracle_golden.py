@@ -289,3 +289,15 @@ def test_contour_root_finder_on_the_oracle(golden):
         w, z = contour.solve_qp_equation_scan(residual, fprime, float(eps[p]),
                                               refusals=(orc.LaplaceRefused,))
         assert abs(w - g['roots'][i, 0]) < 1e-10 and abs(z - g['roots'][i, 1]) < 1e-9, p
+
+
+def test_ao_self_energy_oracle(golden):
+    """The oracle's full AO self-energy (an AO collocation that is not the MO
+    one) and the chi0 sweep's reverse against the reference's."""
+    g = golden('sigma_ao')
+    args = (g['X_ao'], g['D'], g['W'], g['mo'], g['eps'], int(g['nocc']), g['tau_sigma'],
+            g['omega'], g['pade'], float(g['mu']))
+    sig = orc.self_energy_matrix(*args)
+    assert np.abs(sig - g['sigma']).max() <= 1e-10 * np.abs(g['sigma']).max()
+    sub = orc.self_energy_matrix(*args, tau_indices=[1, 4, 7])
+    assert np.abs(sub - g['sigma_sub']).max() <= 1e-10 * np.abs(g['sigma_sub']).max()
