@@ -202,6 +202,41 @@ def qp_solve(sigma, pade_freq, eps_anchor, states, nocc, mu, xc=None, greedy=Tru
     return roots, z, flags, evals
 
 
+def imaginary_axis_sample_points(freq_points, nocc, p, mu):
+    """z = mu -/+ i omega_p: the Pade sample points of state p, below mu for an
+    occupied state (``qp_solve.py:698-703``)."""
+    sign = -1.0 if p < nocc else 1.0
+    return mu + 1j * sign * np.asarray(freq_points, float)
+
+
+def solve_qp_from_imaginary_axis(eps, p_state, xc_correction, z_fit, sigma_iw, greedy=True,
+                                 max_order=None, with_z=False):
+    """One state's Pade continuation and QP root of largest Z on the device
+    (``qp_solve.py:529-558``): the sample points are mu -/+ i omega_p
+    (`imaginary_axis_sample_points`; the lower branch carries the conjugate
+    values), which the QP kernel takes as (omega_p, mu, branch)."""
+    if max_order is not None:
+        raise NotImplementedError('a cap on the Pade order is outside the device route')
+    z = np.asarray(z_fit, complex)
+    mu = float(z.real[0])
+    lower = bool(z.imag[0] < 0)
+    if not (np.allclose(z.real, mu, rtol=0, atol=0)
+            and np.all(np.sign(z.imag) == np.sign(z.imag[0]))):
+        raise NotImplementedError('the device QP solve takes sample points mu -/+ i omega')
+    freq = np.abs(z.imag)
+    sig = np.asarray(sigma_iw, complex)
+    sig = np.conj(sig) if lower else sig   # the kernel conjugates an occupied state itself
+    eps = np.asarray(eps, float)
+    p = int(p_state)
+    dev = require_device()
+    sigma = torch.as_tensor(sig[None, :], dtype=torch.complex128, device=dev)
+    roots, zz, flags, _ = qp_solve(sigma, freq, eps, [p], p + 1 if lower else p, mu,
+                                   xc=[float(xc_correction)], greedy=greedy)
+    _report_flags(flags.cpu().numpy(), [p])
+    root = float(roots[0])
+    return (root, float(zz[0])) if with_z else root
+
+
 def _report_flags(flags_h, states):
     for s, f in zip(np.atleast_1d(states), flags_h):
         if f & QP_FLAG_NO_ROOT:

@@ -25,6 +25,7 @@ LR = 'src.SingleReference.LinearResponse.space_time'
 IT = 'src.SingleReference.GW.imaginary_time'
 ST = 'src.SingleReference.GW.space_time'
 ADJ = 'src.gradients.rpa.space_time_adjoint'
+QS = 'src.SingleReference.GW.qp_solve'
 # importers of the static screening W(omega = 0)
 BSE = 'src.SingleReference.BSE.solve'
 CD = 'src.SingleReference.GW.contour_deformation'
@@ -88,6 +89,8 @@ def replacements():
         ST: {'chi0_imaginary_frequency': space_time.chi0_imaginary_frequency,
              'dyson_screening': space_time.dyson_screening,
              '_sigma_mo_diagonal': _sigma_mo_diagonal, **static},
+        QS: {'solve_qp_from_imaginary_axis': gw.solve_qp_from_imaginary_axis,
+             'imaginary_axis_sample_points': gw.imaginary_axis_sample_points},
         BSE: dict(static),
         CD: {**static,
              'cd_screening_contraction_multi': contour.cd_screening_contraction_multi},

@@ -549,3 +549,21 @@ def test_ao_self_energy_and_mirrors_match_reference_golden(golden):
     out = adjoint.polarizability_backward(g['proj_bar'], X, D, eps, nocc, axes_grid, mu=mu)
     for a, k in zip(out, ('eps_bar', 'X_bar', 'D_bar')):
         assert rel(a, g[k]) < 1e-10, k
+
+
+def test_per_state_qp_solve_matches_reference_golden(golden):
+    """solve_qp_from_imaginary_axis under the reference's signature (sample
+    points mu -/+ i omega, the lower branch conjugated), one state at a time
+    on the device, against the reference's roots and Z of every state."""
+    g = golden('route_calibrated')
+    eps, nocc = g['eps'], int(g['nocc'])
+    mu = float(grids.particle_hole_window(eps, nocc)[2])
+    for p in range(len(eps)):
+        z_fit = gw.imaginary_axis_sample_points(g['pade'], nocc, p, mu)
+        s_p = np.conj(g['sigma'][p]) if p < nocc else g['sigma'][p]
+        root, z = gw.solve_qp_from_imaginary_axis(eps, p, 0.0, z_fit, s_p, with_z=True)
+        if np.isfinite(g['roots'][p]):
+            tol = 5e-8 if abs(p - nocc) <= 4 else 2e-6
+            assert abs(root - g['roots'][p]) < tol, p
+    with pytest.raises(NotImplementedError):
+        gw.solve_qp_from_imaginary_axis(eps, 0, 0.0, z_fit, s_p, max_order=8)
