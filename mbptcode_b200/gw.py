@@ -521,7 +521,8 @@ def solve_qp_energy_space_time(mf, mol, nocc, p_state, numerics=None, auxbasis=N
     ``qp_solve.py:311``). numerics.quadrature: ntau_st ('auto' or a size),
     npade and w0_gl. Returns Hartree, a float for a scalar p_state."""
     for name, val in (('distribute', distribute), ('screen_r_cut', screen_r_cut),
-                      ('sigma_x_matrix', sigma_x_matrix), ('extras', extras)):
+                      ('sigma_x_matrix', sigma_x_matrix), ('extras', extras),
+                      ('dm_correction (the static term is xc_diagonal here)', dm_correction)):
         if val:
             raise NotImplementedError(f'{name} is outside the one-GPU device route')
     if scratch_dir:
@@ -619,3 +620,88 @@ def solve_qp_diagonal_space_time(mf, mol, nocc, states=None, **kw):
     n = np.asarray(getattr(mf, 'mo_energy', mf)).shape[-1]
     states = np.arange(n) if states is None else np.atleast_1d(states)
     return solve_qp_energy_space_time(mf, mol, nocc, states, **kw), states
+
+
+HARTREE_TO_EV = 27.211386245988  # MBPTcode constants.py:11 (CODATA 2018)
+
+
+def _resolve_states(state, nocc):
+    """'homo', an index or a list of them -> orbital indices
+    (``qp_energy.py:608-616``)."""
+    if state == 'homo':
+        return [nocc - 1]
+    if isinstance(state, list):
+        return state
+    if isinstance(state, (int, np.integer)):
+        return [int(state)]
+    raise ValueError(f'Invalid state parameter: {state}')
+
+
+def calc_qp_energy(mf, selfenergy='GW', polarizability='RPA', df=True, eta=None, state='homo',
+                   spin_channel='alpha', printSpectralFunction=False, dm_correction=None,
+                   tda=False, nroots=8, mode='casida', self_consistency='G0W0',
+                   eps_anchor=None, n_workers=None, continuation=None, return_z=False,
+                   solver='auto', equilibrium=False, out=None, **route_kwargs):
+    """Quasiparticle energies in eV (``GW/qp_energy.py:294-616``), mode
+    'space-time' on pre-built factors (route_kwargs['factors'] = (X_mo, D) or
+    (X_mo, D, X_ao)): G0W0 with continuation 'pade' (the default; no Z, as
+    the reference) or 'laplace' (the contour, Z from its slope), or
+    self_consistency 'evGW'. mf: an object with mo_energy and mo_occ (or
+    route_kwargs['nocc']). The reference's refusals are kept: GW@RPA on
+    density fitting only, no eta, no tda; the Casida and imaginary-frequency
+    modes and the 'cd'/'sop' continuations are other routes and refused."""
+    if mode != 'space-time':
+        raise NotImplementedError(f"mode={mode!r}: the device route is mode='space-time'")
+    if isinstance(selfenergy, list) or str(selfenergy).upper() != 'GW':
+        raise ValueError(f"mode='space-time' implements GW only, got selfenergy={selfenergy!r}")
+    if str(polarizability).upper() != 'RPA':
+        raise ValueError(f"mode='space-time' implements RPA screening only, got "
+                         f"polarizability={polarizability!r}")
+    if not df:
+        raise ValueError("mode='space-time' requires density fitting (df=True).")
+    if tda:
+        raise ValueError("tda has no meaning for mode='space-time'")
+    if eta is not None:
+        raise ValueError("eta broadens nothing on mode='space-time'")
+    continuation = 'pade' if continuation is None else continuation
+    if continuation not in ('pade', 'laplace'):
+        raise NotImplementedError(f'continuation={continuation!r} is outside the device route')
+    eps = np.asarray(getattr(mf, 'mo_energy', mf), float)
+    nocc = route_kwargs.pop('nocc', None)
+    if nocc is None:
+        occ = np.asarray(getattr(mf, 'mo_occ'))
+        nocc = (tuple(int((o > 0).sum()) for o in occ) if occ.ndim == 2
+                else int((occ > 0).sum()))
+    nocc_ch = nocc[0 if spin_channel == 'alpha' else 1] if isinstance(nocc, tuple) else nocc
+    states = _resolve_states(state, nocc_ch)
+    if self_consistency in ('evGW', 'evgw'):
+        if continuation != 'pade' or eps_anchor is not None or eps.ndim != 1:
+            raise NotImplementedError("self_consistency='evGW' runs the restricted Pade route "
+                                      "without eps_anchor")
+        from .evgw import evgw_eigenvalues
+        X, D = _factors(route_kwargs.get('factors'))
+        e, _ = evgw_eigenvalues(X, D, eps, nocc, precision=route_kwargs.get('precision'))
+        res = [float(e[p]) * HARTREE_TO_EV for p in states]
+        z = None
+    elif self_consistency != 'G0W0':
+        raise NotImplementedError(f'self_consistency={self_consistency!r} is outside the device '
+                                  'route')
+    elif continuation == 'laplace':
+        from .contour import solve_qp_energy_contour
+        ev, zs, _ = solve_qp_energy_contour(eps, None, nocc, np.asarray(states),
+                                            continuation='laplace', eps_anchor=eps_anchor,
+                                            **route_kwargs)
+        res, z = list(ev), list(zs)
+    else:
+        if return_z:
+            raise ValueError("continuation='pade' returns no Z: differentiating a Thiele "
+                             "recursion divides by vanishing inverse differences")
+        e = solve_qp_energy_space_time(mf, None, nocc, np.asarray(states),
+                                       dm_correction=dm_correction, eps_anchor=eps_anchor,
+                                       spin_channel=spin_channel, **route_kwargs)
+        res, z = [float(x) * HARTREE_TO_EV for x in np.atleast_1d(e)], None
+    if return_z and z is None:
+        raise ValueError('this route returns no Z')
+    if not isinstance(state, list):
+        return (res[0], z[0]) if return_z else res[0]
+    return (res, z) if return_z else res

@@ -567,3 +567,45 @@ def test_per_state_qp_solve_matches_reference_golden(golden):
             assert abs(root - g['roots'][p]) < tol, p
     with pytest.raises(NotImplementedError):
         gw.solve_qp_from_imaginary_axis(eps, 0, 0.0, z_fit, s_p, max_order=8)
+
+
+def test_calc_qp_energy_dispatch(golden):
+    """calc_qp_energy, mode='space-time', on pre-built factors: 'homo' and a
+    list of states by the Pade route against the reference's roots (eV), the
+    contour ('laplace') with Z against the reference's qp_energy_cd, and the
+    reference's refusals."""
+    from types import SimpleNamespace
+    g = golden('route_calibrated')
+    X, D, eps, nocc = g['X'], g['D'], g['eps'], int(g['nocc'])
+    occ = np.zeros(len(eps))
+    occ[:nocc] = 2.0
+    mf = SimpleNamespace(mo_energy=eps, mo_occ=occ)
+
+    class Quad:
+        ntau_st, npade, w0_gl = int(g['ntau']), 16, 1.0
+
+    class Num:
+        quadrature = Quad
+    ev = gw.HARTREE_TO_EV
+    homo = gw.calc_qp_energy(mf, mode='space-time', factors=(X, D), numerics=Num)
+    assert abs(homo / ev - g['roots'][nocc - 1]) < 5e-8
+    both = gw.calc_qp_energy(mf, mode='space-time', state=[nocc - 1, nocc], factors=(X, D),
+                             numerics=Num)
+    assert np.abs(np.array(both) / ev - g['roots'][nocc - 1:nocc + 1]).max() < 5e-8
+    c = golden('contour')
+    occ_c = np.zeros(len(c['eps']))
+    occ_c[:int(c['nocc'])] = 2.0
+    mf_c = SimpleNamespace(mo_energy=c['eps'], mo_occ=occ_c)
+    e, z = gw.calc_qp_energy(mf_c, mode='space-time', continuation='laplace',
+                             state=[int(p) for p in c['states']], factors=(c['X'], c['D']),
+                             return_z=True)
+    assert np.abs(np.array(e) / ev - c['roots'][:, 0]).max() < 1e-9
+    assert np.abs(np.array(z) - c['roots'][:, 1]).max() < 1e-8
+    with pytest.raises(NotImplementedError):
+        gw.calc_qp_energy(mf, mode='casida', factors=(X, D))
+    with pytest.raises(ValueError):
+        gw.calc_qp_energy(mf, mode='space-time', selfenergy='GWGammaInf', factors=(X, D))
+    with pytest.raises(ValueError):
+        gw.calc_qp_energy(mf, mode='space-time', eta=0.01, factors=(X, D))
+    with pytest.raises(ValueError):
+        gw.calc_qp_energy(mf, mode='space-time', return_z=True, factors=(X, D), numerics=Num)
