@@ -31,6 +31,11 @@ sweep, the plain and the warm-started Pade + QP kernels and the Pade
 evaluation of the features, then 5 training steps of the 4 -> 64 -> 64 -> 1
 network on 65536 samples (forward, backward, AdamW).
 
+--rows: device times at n_orb = 1200, N_mu = 7200 of the rows built beside the
+sweep: the static screening, the frequency-blocked and the unrestricted sweeps,
+the self-energy diagonal with its adjoint (20 states), the contour's
+screening contraction (64 frequencies, 20 states) and one Sigma^c evaluation.
+
 --fp64-peak N: the FP64 reference rates of this GPU, timed with CUDA events
 (best of 5 after a warm-up): cuBLAS DGEMM at N^3 and cuSOLVER's Cholesky of
 an N x N SPD matrix (the FP64 factorisation of the Dyson step).
@@ -112,6 +117,68 @@ def transform_case(a):
     print(f'transform case n={n} K=J={k}: |out| {float(out.abs().max()):.3e}')
 
 
+def rows(a):
+    """Device times (CUDA events, after a warm-up call) of the rows built
+    beside the sweep, at n_orb = 1200, N_mu = 7200 (the C2 shapes), one JSON
+    line each."""
+    import json
+    import time
+    from . import adjoint, contour, gw, space_time
+    n, nocc, M = 1200, 120, 7200
+    X, D, eps_t = synthetic_system_torch(n, nocc, M, seed=2024, variant='calibrated')
+    eps = eps_t.cpu().numpy()
+    states20 = np.arange(nocc - 10, nocc + 10)
+
+    def timed(name, fn, reps=1, **extra):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        print(json.dumps({'row': name, 's': round(e0.elapsed_time(e1) / 1e3 / reps, 4),
+                          'host_s': round((time.perf_counter() - t0) / reps, 4), **extra}),
+              flush=True)
+
+    sgrid = grids.static_screening_grid(eps, nocc)
+    for prec in ('mixed', 'fp64'):
+        timed(f'static W(0), {prec}', lambda prec=prec: space_time.static_screening_matrix(
+            X, D, eps, nocc, sgrid, precision=prec), ntau=sgrid.ntau)
+    axes = grids.space_time_axes(eps, nocc, ntau=24)
+    timed('sweep, freq_block=6, mixed', lambda: gw.gw_sweep(
+        X, D, eps, nocc, axes=axes, precision='mixed', freq_block=6))
+    Xb, _, eps_b = synthetic_system_torch(n, nocc - 1, M, seed=2025, variant='calibrated')
+    ua = grids.space_time_axes_unrestricted([eps, eps_b.cpu().numpy()], [nocc, nocc - 1], ntau=24)
+    timed('unrestricted sweep (both channels, 1200 states each), mixed',
+          lambda: gw.gw_sweep_unrestricted([X, Xb], D, [eps, eps_b.cpu().numpy()],
+                                           [nocc, nocc - 1], axes=ua, precision='mixed'))
+    del Xb
+    tr = grids.sigma_transforms(eps, nocc, axes.grid.tau_points, axes.grid.omega_points,
+                                axes.pade_freq, mu=axes.mu)
+
+    def sigma_adjoint():
+        sig, cache = adjoint.selfenergy_diag(X, D, eps_t, nocc, axes.grid, states20, tr, axes.mu)
+        a = torch.ones(sig.shape, dtype=torch.float64, device=sig.device)
+        adjoint.selfenergy_diag_backward(a, a, X, D, eps_t, nocc, axes.grid, states20, tr,
+                                         axes.mu, cache)
+    timed('self-energy diagonal + adjoint, 20 states, 24 points, FP64', sigma_adjoint)
+    nu, nu_w, cgrid, _ = contour.cd_frequency_grid(eps, nocc)
+    proj = contour.polarizability_tau(X, D, eps, nocc, cgrid)
+    B = contour.three_index_slices(X, D, states20)
+    timed('contour: W(i nu) at 64 frequencies + contraction of 20 states, FP64',
+          lambda: contour.cd_screening_contraction_multi(proj, cgrid.cosft_wt, list(B)))
+    wcs = contour.cd_screening_contraction_multi(proj, cgrid.cosft_wt, list(B))
+    lap = contour.LaplaceRealScreening(proj, cgrid, eps, nocc)
+    p = nocc - 1
+    timed('contour: Sigma^c(eps_HOMO - 0.05) of the HOMO (residues by the cosh transform)',
+          lambda: contour.sigma_cd(p, eps[p] - 0.05, B[9], eps, nocc, nu, nu_w, wc=wcs[9],
+                                   real_screening=contour.LaplaceRealScreening(
+                                       proj, cgrid, eps, nocc)))
+
+
 def fp64_peak(a):
     n = a.fp64_peak
     g = torch.Generator(device='cuda').manual_seed(4)
@@ -170,10 +237,13 @@ def main():
     p.add_argument('--transform', type=int, default=0)
     p.add_argument('--fp64-peak', type=int, default=0)
     p.add_argument('--qp-mlp', action='store_true')
+    p.add_argument('--rows', action='store_true')
     a = p.parse_args()
     torch.cuda.set_device(0)
     if a.qp_mlp:
         return qp_mlp_case(a)
+    if a.rows:
+        return rows(a)
     if a.fp64_peak:
         return fp64_peak(a)
     if a.dyson:
