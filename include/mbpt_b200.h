@@ -280,11 +280,13 @@ int mbpt_three_index_slices(const double *X_dev, int64_t M, int64_t norb, const 
  * Dyson step and B (naux x ncols, row-major; the states' slices side by side):
  * GW/contour_deformation.py:229-237 `screening_contraction` and :248-290
  * `cd_screening_contraction_multi` (one W per frequency serving every
- * state). wc_dev: nfreq x ncols, overwritten. */
-size_t mbpt_screening_contraction_workspace_bytes(int64_t naux, int64_t ncols);
+ * state). wc_dev: nfreq x ncols, overwritten. mode: FP64 (cuBLAS DGEMM per
+ * frequency) or MIXED ((W - I)_k B as a split-BF16 tensor-core product with
+ * FP32 output, the column dots in FP64). */
+size_t mbpt_screening_contraction_workspace_bytes(int64_t naux, int64_t ncols, int mode);
 int mbpt_screening_contraction(const double *w_minus_i_dev, int nfreq, int64_t naux,
-                               const double *B_dev, int64_t ncols, double *wc_dev,
-                               void *workspace, size_t ws_bytes, void *stream);
+                               const double *B_dev, int64_t ncols, int mode, double *wc_dev,
+                               void *workspace, size_t ws_bytes, int *err_dev, void *stream);
 
 /* The reverse of the Dyson step W = [1 - chi0]^-1: chi0_bar_f = W_f W_bar_f W_f
  * (gradients/rpa/space_time_adjoint.py:679-685), in place over wbar_dev

@@ -185,13 +185,14 @@ def polarizability_tau(X, D, eps, nocc, grid, mu=None):
     return proj
 
 
-def screening_minus_identity(proj_tau, cosft_wt):
+def screening_minus_identity(proj_tau, cosft_wt, precision='fp64'):
     """W(i nu) - I for every frequency of cosft_wt: chi0 = cosft_wt proj(tau),
     then the Dyson step (FP64 Cholesky; ``contour_deformation.py:209-226``
-    factorises and solves per frequency). Returns (W - I, info)."""
+    factorises and solves per frequency; 'mixed' forms the inverse from the
+    FP64 factor by TF32x3 tensor-core products). Returns (W - I, info)."""
     dev = require_device()
     chi0 = _rows_transform(to_device(proj_tau, dev), cosft_wt)
-    _, _, info, _ = dyson_batch(chi0, want_w=True, precision='fp64')
+    _, _, info, _ = dyson_batch(chi0, want_w=True, precision=precision)
     return chi0, info
 
 
@@ -213,34 +214,42 @@ def three_index_slices(X, D, states):
     return B
 
 
-def screening_contraction_device(w_minus_i, Bps):
+def screening_contraction_device(w_minus_i, Bps, precision='fp64'):
     """[wc_s (nfreq, norb)] for each slice: wc[k, q] = B[:, q]^T (W - I)_k
-    B[:, q], one product per frequency for all slices side by side."""
+    B[:, q], one product per frequency for all slices side by side; 'mixed'
+    forms the products as split-BF16 tensor-core products (FP32 out)."""
+    from .space_time import _Err, _mode
     dev = w_minus_i.device
     Bs = [to_device(b, dev) for b in Bps]
     naux, norb = Bs[0].shape
     B = torch.cat(Bs, dim=1).contiguous()
     nfreq, ncols = w_minus_i.shape[0], B.shape[1]
+    mode = _mode(precision)
     wc = torch.empty((nfreq, ncols), dtype=torch.float64, device=dev)
-    ws = WORKSPACE.get(lib().mbpt_screening_contraction_workspace_bytes(naux, ncols), dev)
+    ws = WORKSPACE.get(lib().mbpt_screening_contraction_workspace_bytes(naux, ncols, mode), dev)
     wm = w_minus_i.contiguous()
-    check(lib().mbpt_screening_contraction(ptr(wm), nfreq, naux, ptr(B), ncols, ptr(wc),
-                                           ptr(ws), ws.numel(), stream_ptr()),
+    err = _Err(dev)
+    check(lib().mbpt_screening_contraction(ptr(wm), nfreq, naux, ptr(B), ncols, mode, ptr(wc),
+                                           ptr(ws), ws.numel(), ptr(err.t), stream_ptr()),
           'mbpt_screening_contraction')
+    err.check('mbpt_screening_contraction')
     return [wc[:, i * norb:(i + 1) * norb] for i in range(len(Bs))]
 
 
-def cd_screening_contraction_multi(proj_tau, cosft_wt, Bps, tile_gb=None, freq_indices=None):
+def cd_screening_contraction_multi(proj_tau, cosft_wt, Bps, tile_gb=None, freq_indices=None,
+                                   precision='fp64'):
     """wc[nu, q] for a list of bra slices on one factorisation per frequency
-    (``contour_deformation.py:248-270``); arrays come back as Bps[0] is held."""
+    (``contour_deformation.py:248-270``); arrays come back as Bps[0] is held.
+    precision 'mixed': the Dyson inverses and the contraction's products on
+    the tensor cores (the factorisations stay FP64)."""
     if freq_indices is not None:
         raise NotImplementedError('frequency splits over ranks are outside the one-GPU route')
-    wmi, info = screening_minus_identity(proj_tau, cosft_wt)
+    wmi, info = screening_minus_identity(proj_tau, cosft_wt, precision=precision)
     if np.any(info):
         import warnings
         warnings.warn('1 - chi0(i nu) is not positive definite at frequencies '
                       f'{np.nonzero(info)[0].tolist()}; solved by LU', RuntimeWarning)
-    out = screening_contraction_device(wmi, Bps)
+    out = screening_contraction_device(wmi, Bps, precision=precision)
     if isinstance(Bps[0], torch.Tensor):
         return out
     return [w.cpu().numpy() for w in out]

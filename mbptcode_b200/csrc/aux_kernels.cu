@@ -415,6 +415,29 @@ __global__ void row_scaled_copy_kernel(const double *__restrict__ X, int64_t M, 
   }
 }
 
+// out[p] = sum_P X[P, p] R[P, p] with R in FP32 (a split product's output)
+// and X in FP64: the screening contraction's column dots
+__global__ void rowdot_f32_kernel(const float *__restrict__ R, int64_t ld_r,
+                                  const double *__restrict__ X, int64_t ld_x, int64_t M,
+                                  int64_t S, double *out) {
+  __shared__ double part[8][33];
+  const int64_t p = static_cast<int64_t>(blockIdx.x) * 32 + threadIdx.x;
+  const int64_t r0 = static_cast<int64_t>(blockIdx.y) * 256;
+  double s = 0.0;
+  if (p < S) {
+    const int64_t r1 = min(r0 + 256, M);
+    for (int64_t r = r0 + threadIdx.y; r < r1; r += 8)
+      s += X[r * ld_x + p] * static_cast<double>(R[r * ld_r + p]);
+  }
+  part[threadIdx.y][threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.y == 0 && p < S) {
+    double t = 0.0;
+    for (int k = 0; k < 8; ++k) t += part[k][threadIdx.x];
+    atomicAdd(out + p, t);
+  }
+}
+
 }  // namespace
 
 void launch_chi0_bar_seed(double *a, int64_t n, int nfreq, const double *w, cudaStream_t st) {
@@ -531,6 +554,13 @@ void launch_row_scaled_copy(const double *X, int64_t M, int64_t n, int64_t p, do
                             cudaStream_t st) {
   count_launch();
   row_scaled_copy_kernel<<<blocks(M * n), 256, 0, st>>>(X, M, n, p, out);
+}
+
+void launch_rowdot_f32(const float *R, int64_t ld_r, const double *X, int64_t ld_x, int64_t M,
+                       int64_t S, double *out, cudaStream_t st) {
+  dim3 grid(static_cast<unsigned>((S + 31) / 32), static_cast<unsigned>((M + 255) / 256));
+  count_launch();
+  rowdot_f32_kernel<<<grid, dim3(32, 8), 0, st>>>(R, ld_r, X, ld_x, M, S, out);
 }
 
 }  // namespace mbpt

@@ -44,6 +44,8 @@ void launch_strided_to_tf32(const double *src, int64_t rows, int64_t k, int64_t 
                             float *hi, float *lo, int64_t rows_p, int64_t k_p, cudaStream_t st);
 void launch_row_scaled_copy(const double *X, int64_t M, int64_t n, int64_t p, double *out,
                             cudaStream_t st);
+void launch_rowdot_f32(const float *R, int64_t ld_r, const double *X, int64_t ld_x, int64_t M,
+                       int64_t S, double *out, cudaStream_t st);
 void launch_chol_copy_panel(const double *A, int64_t n, int64_t j0, int64_t m, int nbj,
                             int nmat, double *P, cudaStream_t st);
 int launch_chol_diag_block(const double *P, int64_t m, int nbj, double *A, int64_t n,
@@ -1367,21 +1369,71 @@ int mbpt_three_index_slices(const double *X, int64_t M, int64_t norb, const doub
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 
-size_t mbpt_screening_contraction_workspace_bytes(int64_t naux, int64_t ncols) {
-  return sizeof(double) * static_cast<size_t>(naux) * ncols + 2048;
+struct ContractionBufs {
+  double *Y = nullptr;                                        // fp64
+  bf16 *w_hi = nullptr, *w_lo = nullptr, *b_hi = nullptr, *b_lo = nullptr;  // mixed
+  float *y = nullptr;
+  int64_t mp = 0, np = 0, kp = 0;
+};
+
+ContractionBufs carve_contraction(Arena &ar, int64_t naux, int64_t ncols, int mode) {
+  ContractionBufs b;
+  if (mode == MBPT_MODE_FP64) {
+    b.Y = ar.take<double>(naux * ncols);
+    return b;
+  }
+  b.mp = round_up(naux, 128);
+  b.np = round_up(ncols, 128);
+  b.kp = round_up(naux, 64);
+  b.w_hi = ar.take<bf16>(b.mp * b.kp);
+  b.w_lo = ar.take<bf16>(b.mp * b.kp);
+  b.b_hi = ar.take<bf16>(b.np * b.kp);
+  b.b_lo = ar.take<bf16>(b.np * b.kp);
+  b.y = ar.take<float>(b.mp * b.np);
+  return b;
+}
+
+size_t mbpt_screening_contraction_workspace_bytes(int64_t naux, int64_t ncols, int mode) {
+  Arena ar;
+  ar.counting = true;
+  carve_contraction(ar, naux, ncols, mode);
+  return ar.used + 8192;
 }
 
 int mbpt_screening_contraction(const double *w_minus_i, int nfreq, int64_t naux,
-                               const double *B, int64_t ncols, double *wc, void *ws,
-                               size_t ws_bytes, void *stream) {
+                               const double *B, int64_t ncols, int mode, double *wc, void *ws,
+                               size_t ws_bytes, int *err, void *stream) {
   if (nfreq < 1 || naux < 1 || ncols < 1) return MBPT_ERR_SHAPE;
+  if (mode != MBPT_MODE_FP64 && mode != MBPT_MODE_MIXED) return MBPT_ERR_UNSUPPORTED;
   cudaStream_t st = S(stream);
   Arena ar = arena(ws, ws_bytes);
-  double *Y = ar.take<double>(naux * ncols);
+  ContractionBufs c = carve_contraction(ar, naux, ncols, mode);
   if (ar.overflow()) return MBPT_ERR_WORKSPACE;
-  cublasHandle_t h = handles(st).blas;
   if (cudaMemsetAsync(wc, 0, sizeof(double) * nfreq * ncols, st) != cudaSuccess)
     return MBPT_ERR_CUDA;
+  if (mode == MBPT_MODE_MIXED) {
+    // Y_k = (W - I)_k B as one split-BF16 product per frequency (FP32 out):
+    // A = (W - I)_k (naux x naux), the second operand B^T (ncols x naux),
+    // split once; then the column dots against B in FP64
+    launch_split_pad<double>(B, naux, ncols, ncols, 1.f, c.b_hi, c.b_lo, c.kp, c.kp, c.np,
+                             true, st);
+    SplitMat Bm{c.b_hi, c.b_lo, c.np, c.kp, c.kp};
+    for (int k = 0; k < nfreq; ++k) {
+      launch_split_pad<double>(w_minus_i + k * naux * naux, naux, naux, naux, 1.f, c.w_hi,
+                               c.w_lo, c.kp, c.mp, c.kp, false, st);
+      SplitMat Am{c.w_hi, c.w_lo, c.mp, c.kp, c.kp};
+      umma::EpiArgs e;
+      e.outf = c.y;
+      e.ld_outf = c.np;
+      e.alpha = 1.f;
+      int rc = gemm_split(umma::EPI_F32, 1, &Am, &Bm, c.mp, c.np, e, err, st);
+      if (rc) return rc;
+      launch_rowdot_f32(c.y, c.np, B, ncols, naux, ncols, wc + k * ncols, st);
+    }
+    return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+  }
+  double *Y = c.Y;
+  cublasHandle_t h = handles(st).blas;
   for (int k = 0; k < nfreq; ++k) {
     // wc[k, c] = B[:, c]^T (W - I)_k B[:, c]: GW/contour_deformation.py:229-237, 273-290
     if (!dgemm_rm(h, false, false, naux, ncols, naux, 1.0, w_minus_i + k * naux * naux, naux,

@@ -170,6 +170,9 @@ def rows(a):
     B = contour.three_index_slices(X, D, states20)
     timed('contour: W(i nu) at 64 frequencies + contraction of 20 states, FP64',
           lambda: contour.cd_screening_contraction_multi(proj, cgrid.cosft_wt, list(B)))
+    timed('contour: the same in mixed precision (TF32x3 Dyson inverses, split-BF16 contraction)',
+          lambda: contour.cd_screening_contraction_multi(proj, cgrid.cosft_wt, list(B),
+                                                         precision='mixed'))
     wcs = contour.cd_screening_contraction_multi(proj, cgrid.cosft_wt, list(B))
     lap = contour.LaplaceRealScreening(proj, cgrid, eps, nocc)
     p = nocc - 1

@@ -491,6 +491,17 @@ def test_contour_deformation_device_matches_reference_golden(golden):
     assert rel(torch.stack(wcs).cpu().numpy(), g['wc']) < 1e-10
     wc_np = contour.cd_screening_contraction_multi(g['proj'], grid.cosft_wt, list(g['B']))
     assert isinstance(wc_np[0], np.ndarray) and rel(np.stack(wc_np), g['wc']) < 1e-10
+    # the contraction's products as split-BF16 tensor-core products (FP32
+    # out, 2^-16-level relative error per product term): wc to 1e-4 of its
+    # scale, Sigma^c to 1e-5 Ha
+    wc_mx = contour.cd_screening_contraction_multi(proj, grid.cosft_wt, list(B),
+                                                   precision='mixed')
+    assert rel(torch.stack(wc_mx).cpu().numpy(), g['wc']) < 1e-4
+    lap_mx = contour.LaplaceRealScreening(proj, grid, eps, nocc)
+    for i, p in enumerate(g['states']):
+        s = contour.sigma_cd(int(p), eps[p], B[i], eps, nocc, nu, nu_w, wc=wc_mx[i],
+                             real_screening=lap_mx)
+        assert abs(s - g['sigma'][i, 2]) < 1e-5, p
     lap = contour.LaplaceRealScreening(proj, grid, eps, nocc)
     for i, p in enumerate(g['states']):
         for j, dw in enumerate(g['shifts']):
@@ -601,6 +612,11 @@ def test_calc_qp_energy_dispatch(golden):
                              return_z=True)
     assert np.abs(np.array(e) / ev - c['roots'][:, 0]).max() < 1e-9
     assert np.abs(np.array(z) - c['roots'][:, 1]).max() < 1e-8
+    from mbptcode_b200 import evgw
+    e_ev = gw.calc_qp_energy(mf, mode='space-time', self_consistency='evGW',
+                             state=[nocc - 1, nocc], factors=(X, D))
+    e_direct, _ = evgw.evgw_eigenvalues(X, D, eps, nocc)
+    assert np.abs(np.array(e_ev) / ev - e_direct[nocc - 1:nocc + 1]).max() < 1e-12
     with pytest.raises(NotImplementedError):
         gw.calc_qp_energy(mf, mode='casida', factors=(X, D))
     with pytest.raises(ValueError):
