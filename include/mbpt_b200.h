@@ -288,6 +288,27 @@ int mbpt_screening_contraction(const double *w_minus_i_dev, int nfreq, int64_t n
                                const double *B_dev, int64_t ncols, int mode, double *wc_dev,
                                void *workspace, size_t ws_bytes, int *err_dev, void *stream);
 
+/* The contour deformation's reverse (gradients/gwbse/qp_space_time.py:328-361,
+ * the integral term's adjoint): for adjoints wc_bar (nfreq x norb) on
+ * wc[k, q] = b_q^T (W - I)_k b_q, accumulates B_bar += 2 (W - I)_k B
+ * diag(wc_bar[k]) over k and writes W_bar_k = B diag(wc_bar[k]) B^T
+ * (nfreq, naux, naux). B, B_bar: naux x norb. FP64. */
+size_t mbpt_cd_integral_backward_workspace_bytes(int64_t naux, int64_t norb);
+int mbpt_cd_integral_backward(const double *w_minus_i_dev, int nfreq, int64_t naux,
+                              const double *B_dev, int64_t norb, const double *wc_bar_dev,
+                              double *B_bar_dev, double *W_bar_dev, void *workspace,
+                              size_t ws_bytes, void *stream);
+
+/* The three-index slice's reverse (gradients/rpa/space_time_adjoint.py:593-624):
+ * for an adjoint B_bar (naux x norb) on B_p = D^T diag(X[:, p]) X, accumulates
+ * X_bar (M x norb) and D_bar (M x naux). FP64. */
+size_t mbpt_three_index_slice_backward_workspace_bytes(int64_t M, int64_t norb, int64_t naux);
+int mbpt_three_index_slice_backward(const double *X_dev, int64_t M, int64_t norb,
+                                    const double *D_dev, int64_t naux, int64_t p,
+                                    const double *B_bar_dev, double *X_bar_dev,
+                                    double *D_bar_dev, void *workspace, size_t ws_bytes,
+                                    void *stream);
+
 /* The reverse of the Dyson step W = [1 - chi0]^-1: chi0_bar_f = W_f W_bar_f W_f
  * (gradients/rpa/space_time_adjoint.py:679-685), in place over wbar_dev
  * (nfreq, naux, naux), from W - I (w_minus_i_dev, the Dyson output). FP64. */

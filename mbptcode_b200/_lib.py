@@ -63,6 +63,11 @@ _SIGNATURES = {
     'mbpt_three_index_slices': (_i, [_p, _i64, _i64, _p, _i64, _p, _i, _p, _p, _sz, _p]),
     'mbpt_screening_contraction_workspace_bytes': (_sz, [_i64, _i64, _i]),
     'mbpt_screening_contraction': (_i, [_p, _i, _i64, _p, _i64, _i, _p, _p, _sz, _p, _p]),
+    'mbpt_cd_integral_backward_workspace_bytes': (_sz, [_i64, _i64]),
+    'mbpt_cd_integral_backward': (_i, [_p, _i, _i64, _p, _i64, _p, _p, _p, _p, _sz, _p]),
+    'mbpt_three_index_slice_backward_workspace_bytes': (_sz, [_i64, _i64, _i64]),
+    'mbpt_three_index_slice_backward': (_i, [_p, _i64, _i64, _p, _i64, _i64, _p, _p, _p, _p,
+                                             _sz, _p]),
     'mbpt_dyson_backward_workspace_bytes': (_sz, [_i64]),
     'mbpt_dyson_backward': (_i, [_p, _p, _i64, _i, _p, _sz, _p]),
     'mbpt_mlp_param_count': (_i, [_i]),

@@ -669,3 +669,98 @@ def solve_qp_energy_contour(mf, mol, nocc, states, continuation='laplace', numer
     roots, zs, info = contour_roots(X, D, eps, nocc, states, ntau=ntau, nfreq_cd=nfreq,
                                     w0_cd=w0_cd, xc_correction=xc)
     return roots * HARTREE_TO_EV, zs, info
+
+
+def _slice_backward(X, D, p, B_bar, X_bar, D_bar):
+    Xd, Dd = to_device(X, B_bar.device), to_device(D, B_bar.device)
+    M, norb = Xd.shape
+    naux = Dd.shape[1]
+    ws = WORKSPACE.get(lib().mbpt_three_index_slice_backward_workspace_bytes(M, norb, naux),
+                       B_bar.device)
+    Bb = B_bar.contiguous()
+    check(lib().mbpt_three_index_slice_backward(ptr(Xd), M, norb, ptr(Dd), naux, int(p), ptr(Bb),
+                                                ptr(X_bar), ptr(D_bar), ptr(ws), ws.numel(),
+                                                stream_ptr()),
+          'mbpt_three_index_slice_backward')
+
+
+def qp_gradient_space_time(X, D, eps, nocc, grid, nu_points, nu_weights, p, *,
+                           residue_route='laplace', mu=None, xc_correction=0.0, w0=None,
+                           tol=QP_ROOT_TOL, laplace_tol=LAPLACE_SCREENING_TOL, want_grad=True,
+                           tile_gb=None, follow=None, route_out=None, n_poles=None,
+                           sop_stride=None, scissor=None, sop_poles=None, comm=None, z0=None):
+    """(eps^QP_p, Z, eps_bar, X_bar, D_bar), or (eps^QP_p, Z) with want_grad
+    False: the contour-deformation QP energy of state p and its gradient in
+    (eps, X, D) (``gradients/gwbse/qp_space_time.py:412-452``), residues by
+    the cosh transform of proj(tau) on `grid` (the contour's time grid, mu
+    frozen). The root is differentiated implicitly, d eps^QP = Z [d eps_p +
+    dSigma^c(w)|_w], the residue set frozen at the root: the integral term's
+    adjoint goes to the slice, to W(i nu) (then W W_bar W onto chi0 and
+    proj(tau)) and to eps through its weights; each residue's to the slice,
+    to chi0 at its real frequency (folded onto proj(tau) by the cosh weights)
+    and to eps through its frequency; then the chi0 sweep's and the slice's
+    reverses. FP64 on the device; arrays come back as X is held."""
+    if residue_route != 'laplace':
+        raise NotImplementedError(f'residue_route={residue_route!r}: the device route serves '
+                                  "'laplace' (the cubic residues)")
+    if any(v is not None for v in (follow, scissor, sop_poles, comm, z0, w0)):
+        raise NotImplementedError('walks, scissors, pole models and rank splits are outside '
+                                  'the device route')
+    dev = require_device()
+    eps_h = _eps_host(eps)
+    p = int(p)
+    if mu is None:
+        mu = particle_hole_window(eps_h, nocc)[2]
+    proj = polarizability_tau(X, D, eps_h, nocc, grid, mu=mu)
+    wmi, _ = screening_minus_identity(proj, grid.cosft_wt)
+    B = three_index_slices(X, D, [p])[0]
+    wc = screening_contraction_device(wmi, [B])[0]
+    lap = LaplaceRealScreening(proj, grid, eps_h, nocc, tol=laplace_tol)
+    w, z, res = qp_energy_cd(p, B, eps_h, nocc, nu_points, nu_weights,
+                             xc_correction=xc_correction, tol=tol, wc=wc, real_screening=lap)
+    if route_out is not None:
+        route_out.update(residue_route='laplace', residues=res)
+    if not want_grad:
+        return w, z
+    naux, norb = B.shape
+    eps_bar = np.zeros(norb)
+    eps_bar[p] += z
+    c, dc = cd_integral_weights(w - eps_h, nu_points, nu_weights)
+    coeff = -z / np.pi
+    wc_h = wc.cpu().numpy()
+    eps_bar += -coeff * np.einsum('kq,kq->q', wc_h, dc)
+    wc_bar = torch.as_tensor(coeff * c, dtype=torch.float64, device=dev)
+    B_bar = torch.zeros_like(B)
+    W_bar = torch.empty_like(wmi)
+    ws = WORKSPACE.get(lib().mbpt_cd_integral_backward_workspace_bytes(naux, norb), dev)
+    Bc = B.contiguous()
+    check(lib().mbpt_cd_integral_backward(ptr(wmi), wmi.shape[0], naux, ptr(Bc), norb,
+                                          ptr(wc_bar), ptr(B_bar), ptr(W_bar), ptr(ws),
+                                          ws.numel(), stream_ptr()),
+          'mbpt_cd_integral_backward')
+    wsd = WORKSPACE.get(lib().mbpt_dyson_backward_workspace_bytes(naux), dev)
+    check(lib().mbpt_dyson_backward(ptr(wmi), ptr(W_bar), naux, wmi.shape[0], ptr(wsd),
+                                    wsd.numel(), stream_ptr()), 'mbpt_dyson_backward')
+    cw_t = np.ascontiguousarray(np.asarray(grid.cosft_wt, float).T)   # (ntau, nfreq)
+    proj_bar = torch.zeros_like(proj)
+    for k0 in range(0, cw_t.shape[1], _MAX_J):
+        transform(W_bar[k0:k0 + _MAX_J].contiguous(), np.ascontiguousarray(cw_t[:, k0:k0 + _MAX_J]),
+                  out=proj_bar, accumulate=True)
+    del W_bar
+    tau = np.asarray(grid.tau_points, float)
+    for q, wt in res:
+        f = abs(eps_h[q] - w)
+        cf, _ = real_frequency_weights(grid, f)
+        b = B[:, q]
+        y = lap.apply(f, b)
+        B_bar[:, q] += (z * wt * 2.0) * (y - b)
+        proj_bar += torch.as_tensor(z * wt * cf, device=dev)[:, None, None] * torch.outer(y, y)[None]
+        eps_bar[q] += z * wt * lap.slope(f, y) * np.sign(eps_h[q] - w)
+    del tau
+    from .adjoint import chi0_backward
+    e2, X_bar, D_bar = chi0_backward(proj_bar, X, D, eps_h, nocc, grid.tau_points, mu)
+    _slice_backward(X, D, p, B_bar, X_bar, D_bar)
+    eps_bar = eps_bar + e2.cpu().numpy()
+    if isinstance(X, torch.Tensor):
+        return w, z, torch.as_tensor(eps_bar, device=dev), X_bar, D_bar
+    return w, z, eps_bar, X_bar.cpu().numpy(), D_bar.cpu().numpy()

@@ -438,6 +438,41 @@ __global__ void rowdot_f32_kernel(const float *__restrict__ R, int64_t ld_r,
   }
 }
 
+// out[P, q] (+)= factor Y[P, q] v[q] over an nr x nc row-major block
+__global__ void col_scale_kernel(const double *__restrict__ Y, const double *__restrict__ v,
+                                 int64_t nr, int64_t nc, double factor, double *out,
+                                 bool accumulate) {
+  const int64_t total = nr * nc;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double x = factor * Y[i] * v[i % nc];
+    out[i] = accumulate ? out[i] + x : x;
+  }
+}
+
+// out[r, c] += a[r * lda + p] b[r, c]: row r scaled by a's column p
+__global__ void row_scale_acc_kernel(const double *__restrict__ a, int64_t lda, int64_t p,
+                                     const double *__restrict__ b, int64_t nr, int64_t nc,
+                                     double *out) {
+  const int64_t total = nr * nc;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[i] += a[(i / nc) * lda + p] * b[i];
+}
+
+// out[r * ldo + p] += sum_c G[r, c] X[r, c]: one warp per row
+__global__ void row_dot_into_col_kernel(const double *__restrict__ G,
+                                        const double *__restrict__ X, int64_t nr, int64_t nc,
+                                        double *out, int64_t ldo, int64_t p) {
+  const int64_t r = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (r >= nr) return;
+  double s = 0.0;
+  for (int64_t c = lane; c < nc; c += 32) s += G[r * nc + c] * X[r * nc + c];
+  for (int d = 16; d; d >>= 1) s += __shfl_xor_sync(0xffffffffu, s, d);
+  if (lane == 0) out[r * ldo + p] += s;
+}
+
 }  // namespace
 
 void launch_chi0_bar_seed(double *a, int64_t n, int nfreq, const double *w, cudaStream_t st) {
@@ -561,6 +596,25 @@ void launch_rowdot_f32(const float *R, int64_t ld_r, const double *X, int64_t ld
   dim3 grid(static_cast<unsigned>((S + 31) / 32), static_cast<unsigned>((M + 255) / 256));
   count_launch();
   rowdot_f32_kernel<<<grid, dim3(32, 8), 0, st>>>(R, ld_r, X, ld_x, M, S, out);
+}
+
+void launch_col_scale(const double *Y, const double *v, int64_t nr, int64_t nc, double factor,
+                      double *out, bool accumulate, cudaStream_t st) {
+  count_launch();
+  col_scale_kernel<<<blocks(nr * nc), 256, 0, st>>>(Y, v, nr, nc, factor, out, accumulate);
+}
+
+void launch_row_scale_acc(const double *a, int64_t lda, int64_t p, const double *b, int64_t nr,
+                          int64_t nc, double *out, cudaStream_t st) {
+  count_launch();
+  row_scale_acc_kernel<<<blocks(nr * nc), 256, 0, st>>>(a, lda, p, b, nr, nc, out);
+}
+
+void launch_row_dot_into_col(const double *G, const double *X, int64_t nr, int64_t nc,
+                             double *out, int64_t ldo, int64_t p, cudaStream_t st) {
+  count_launch();
+  row_dot_into_col_kernel<<<static_cast<unsigned>((nr + 7) / 8), 256, 0, st>>>(G, X, nr, nc,
+                                                                              out, ldo, p);
 }
 
 }  // namespace mbpt

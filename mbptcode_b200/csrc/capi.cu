@@ -46,6 +46,12 @@ void launch_row_scaled_copy(const double *X, int64_t M, int64_t n, int64_t p, do
                             cudaStream_t st);
 void launch_rowdot_f32(const float *R, int64_t ld_r, const double *X, int64_t ld_x, int64_t M,
                        int64_t S, double *out, cudaStream_t st);
+void launch_col_scale(const double *Y, const double *v, int64_t nr, int64_t nc, double factor,
+                      double *out, bool accumulate, cudaStream_t st);
+void launch_row_scale_acc(const double *a, int64_t lda, int64_t p, const double *b, int64_t nr,
+                          int64_t nc, double *out, cudaStream_t st);
+void launch_row_dot_into_col(const double *G, const double *X, int64_t nr, int64_t nc,
+                             double *out, int64_t ldo, int64_t p, cudaStream_t st);
 void launch_chol_copy_panel(const double *A, int64_t n, int64_t j0, int64_t m, int nbj,
                             int nmat, double *P, cudaStream_t st);
 int launch_chol_diag_block(const double *P, int64_t m, int nbj, double *A, int64_t n,
@@ -1441,6 +1447,61 @@ int mbpt_screening_contraction(const double *w_minus_i, int nfreq, int64_t naux,
       return MBPT_ERR_CUDA;
     launch_rowdot(Y, ncols, B, ncols, naux, ncols, 1.0, wc + k * ncols, st);
   }
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+size_t mbpt_cd_integral_backward_workspace_bytes(int64_t naux, int64_t norb) {
+  return 2 * sizeof(double) * static_cast<size_t>(naux) * norb + 2048;
+}
+
+int mbpt_cd_integral_backward(const double *w_minus_i, int nfreq, int64_t naux, const double *B,
+                              int64_t norb, const double *wc_bar, double *B_bar, double *W_bar,
+                              void *ws, size_t ws_bytes, void *stream) {
+  if (nfreq < 1 || naux < 1 || norb < 1) return MBPT_ERR_SHAPE;
+  cudaStream_t st = S(stream);
+  Arena ar = arena(ws, ws_bytes);
+  double *Y = ar.take<double>(naux * norb), *T = ar.take<double>(naux * norb);
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  cublasHandle_t h = handles(st).blas;
+  for (int k = 0; k < nfreq; ++k) {
+    // wc[k, q] = b_q^T (W - I)_k b_q: B_bar += 2 ((W - I)_k B) diag(wc_bar[k]),
+    // W_bar_k = B diag(wc_bar[k]) B^T (gradients/gwbse/qp_space_time.py:328-350)
+    const double *v = wc_bar + k * norb;
+    if (!dgemm_rm(h, false, false, naux, norb, naux, 1.0, w_minus_i + k * naux * naux, naux, B,
+                  norb, 0.0, Y, norb))
+      return MBPT_ERR_CUDA;
+    launch_col_scale(Y, v, naux, norb, 2.0, B_bar, true, st);
+    launch_col_scale(B, v, naux, norb, 1.0, T, false, st);
+    if (!dgemm_rm(h, false, true, naux, naux, norb, 1.0, T, norb, B, norb, 0.0,
+                  W_bar + k * naux * naux, naux))
+      return MBPT_ERR_CUDA;
+  }
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+size_t mbpt_three_index_slice_backward_workspace_bytes(int64_t M, int64_t norb, int64_t naux) {
+  return sizeof(double) * static_cast<size_t>(M) * (norb > naux ? norb : naux) + 2048;
+}
+
+int mbpt_three_index_slice_backward(const double *X, int64_t M, int64_t norb, const double *D,
+                                    int64_t naux, int64_t p, const double *B_bar, double *X_bar,
+                                    double *D_bar, void *ws, size_t ws_bytes, void *stream) {
+  if (M < 1 || norb < 1 || naux < 1 || p < 0 || p >= norb) return MBPT_ERR_SHAPE;
+  cudaStream_t st = S(stream);
+  Arena ar = arena(ws, ws_bytes);
+  double *G = ar.take<double>(M * (norb > naux ? norb : naux));
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  cublasHandle_t h = handles(st).blas;
+  // B_p = D^T diag(x_p) X (LinearResponse/space_time.py:804-815), its reverse
+  // gradients/rpa/space_time_adjoint.py:593-624: G = D B_bar,
+  // X_bar += diag(x_p) G, X_bar[:, p] += rowsum(G o X), D_bar += diag(x_p) X B_bar^T
+  if (!dgemm_rm(h, false, false, M, norb, naux, 1.0, D, naux, B_bar, norb, 0.0, G, norb))
+    return MBPT_ERR_CUDA;
+  launch_row_dot_into_col(G, X, M, norb, X_bar, norb, p, st);
+  launch_row_scale_acc(X, norb, p, G, M, norb, X_bar, st);
+  if (!dgemm_rm(h, false, true, M, naux, norb, 1.0, X, norb, B_bar, norb, 0.0, G, naux))
+    return MBPT_ERR_CUDA;
+  launch_row_scale_acc(X, norb, p, G, M, naux, D_bar, st);
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 

@@ -26,6 +26,7 @@ IT = 'src.SingleReference.GW.imaginary_time'
 ST = 'src.SingleReference.GW.space_time'
 ADJ = 'src.gradients.rpa.space_time_adjoint'
 QS = 'src.SingleReference.GW.qp_solve'
+QG = 'src.gradients.gwbse.qp_space_time'
 # importers of the static screening W(omega = 0)
 BSE = 'src.SingleReference.BSE.solve'
 CD = 'src.SingleReference.GW.contour_deformation'
@@ -91,6 +92,7 @@ def replacements():
              '_sigma_mo_diagonal': _sigma_mo_diagonal, **static},
         QS: {'solve_qp_from_imaginary_axis': gw.solve_qp_from_imaginary_axis,
              'imaginary_axis_sample_points': gw.imaginary_axis_sample_points},
+        QG: {'qp_gradient_space_time': contour.qp_gradient_space_time},
         BSE: dict(static),
         CD: {**static,
              'cd_screening_contraction_multi': contour.cd_screening_contraction_multi},

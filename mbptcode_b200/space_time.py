@@ -63,7 +63,10 @@ def to_device(a, device, dtype=torch.float64):
     if isinstance(a, torch.Tensor):
         pinned = a.device.type == 'cpu' and a.is_pinned() and a.dtype == dtype
         return a.to(device=device, dtype=dtype, non_blocking=pinned).contiguous()
-    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=device)
+    a = np.ascontiguousarray(a)
+    if not a.flags.writeable:   # a broadcast view: torch wants memory it may own
+        a = a.copy()
+    return torch.as_tensor(a, dtype=dtype, device=device)
 
 
 def back(t, like):

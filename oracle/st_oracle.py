@@ -782,3 +782,53 @@ def self_energy_matrix(X_ao, D, W_omega, mo_coeff, eps, nocc, tau_points, omega_
             out.real[w] += C[w, k] * (s_g + s_l)
             out.imag[w] += S[w, k] * (s_g - s_l)
     return -0.5 * out
+
+
+def qp_gradient_laplace(X, D, eps, nocc, tau, tau_w, cosft_wt, nu, nu_w, p, mu, root, z):
+    """gradients/gwbse/qp_space_time.py:412-452 for one state on the Laplace
+    residue route, given its root and Z: (eps_bar, X_bar, D_bar) of
+    eps^QP_p = Z [d eps_p + dSigma^c(w)|_w] (implicit differentiation, the
+    residue set frozen at the root), with
+      the integral term's adjoint on wc (-Z/pi c) carried to B_p (2 (W-I) B
+      wc_bar), to W(i nu) (B diag(wc_bar) B^T, then W W_bar W onto chi0 and
+      proj(tau)) and to eps through the weights' de-derivative
+      (contour_deformation_adjoint.py, qp_space_time.py:328-361);
+      each residue's adjoint on b_q (2 w_q (y - b)), its rank-one adjoint
+      w_q y y^T on chi0 at the real frequency folded onto proj(tau) by the
+      cosh weights, and the frequency's eps dependence through the slope;
+      then the chi0 sweep's reverse and the slice's (:593-624)."""
+    eps = np.asarray(eps, float)
+    proj = polarizability_projected_sweep(X, D, eps, nocc, tau, mu)
+    chi0 = np.tensordot(cosft_wt, proj, axes=(1, 0))
+    naux = proj.shape[-1]
+    eye = np.eye(naux)
+    B = three_index_slice(X, D, p)
+    eps_bar = np.zeros_like(eps)
+    eps_bar[p] += z
+    c, dc = cd_integral_weights(root - eps, nu, nu_w, with_slope=True)
+    coeff = -z / np.pi
+    B_bar = np.zeros_like(B)
+    chi0_bar = np.zeros_like(chi0)
+    for k in range(len(chi0)):
+        Wm = np.linalg.inv(eye - chi0[k]) - eye
+        Y = Wm @ B
+        wck = np.einsum('Pq,Pq->q', B, Y)
+        wcb = coeff * c[k]
+        B_bar += 2.0 * Y * wcb
+        Wk = eye + Wm
+        chi0_bar[k] = Wk @ ((B * wcb) @ B.T) @ Wk
+        eps_bar += -coeff * wck * dc[k]
+    proj_bar = np.tensordot(cosft_wt.T, chi0_bar, axes=(1, 0))
+    for q, wt in residue_set(eps, nocc, root):
+        f = abs(eps[q] - root)
+        cf = 2.0 * np.asarray(tau_w) * np.cosh(f * np.asarray(tau))
+        dcf = 2.0 * np.asarray(tau_w) * np.asarray(tau) * np.sinh(f * np.asarray(tau))
+        b = B[:, q]
+        y = np.linalg.solve(eye - np.tensordot(cf, proj, axes=(0, 0)), b)
+        B_bar[:, q] += z * wt * 2.0 * (y - b)
+        proj_bar += (z * wt) * cf[:, None, None] * np.outer(y, y)[None]
+        slope = float(y @ np.tensordot(dcf, proj, axes=(0, 0)) @ y)
+        eps_bar[q] += z * wt * slope * np.sign(eps[q] - root)
+    e2, X_bar, D_bar = polarizability_backward(proj_bar, X, D, eps, nocc, tau, mu)
+    three_index_slice_backward(X, D, p, B_bar, X_bar, D_bar)
+    return eps_bar + e2, X_bar, D_bar

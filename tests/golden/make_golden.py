@@ -382,8 +382,10 @@ def contour_fixture():
     half a gap below it), proj(tau) on it, the screening contraction wc of
     three states around the gap, Sigma^c at points on both sides of each
     state's level and on it (residues through the Laplace backend), each
-    state's quasiparticle root and Z (`qp_energy_cd`), and the integral
-    weights at a set of de values."""
+    state's quasiparticle root and Z (`qp_energy_cd`), the gradient of each
+    root in (eps, X, D) (gradients/gwbse/qp_space_time.py:412-452, residues
+    by the cosh transform), and the integral weights at a set of de
+    values."""
     cd, rs = _import_contour_deformation()
     from src.gradients.rpa.space_time_adjoint import polarizability_tau
     from src.SingleReference.LinearResponse.space_time import three_index_slice
@@ -409,13 +411,19 @@ def contour_fixture():
         w, z, _ = cd.qp_energy_cd(int(p), Bps[i], eps, nocc, nu, nu_w, wc=wcs[i],
                                   real_screening=rs.LaplaceRealScreening(proj, grid, eps, nocc))
         roots[i] = w, z
+    from src.gradients.gwbse.qp_space_time import qp_gradient_space_time
+    grads = [qp_gradient_space_time(X, D, eps, nocc, grid, nu, nu_w, int(p),
+                                    residue_route='laplace', mu=mu) for p in states]
     de = np.array([-0.3, -1e-3, 0.0, 1e-12, 2e-3, 0.05, 0.7])
     c, dc = cd.cd_integral_weights(de, nu, nu_w)
     np.savez_compressed(
         os.path.join(HERE, 'contour.npz'), X=X, D=D, eps=eps, nocc=nocc, mu=mu, nu=nu,
         nu_w=nu_w, w0=w0, tau=grid.tau_points, tau_w=grid.tau_weights, cosft_wt=grid.cosft_wt,
         proj=proj, states=states, B=np.stack(Bps), wc=np.stack(wcs), shifts=shifts, sigma=sig,
-        roots=roots, de=de, c=c, dc=dc)
+        roots=roots, de=de, c=c, dc=dc,
+        grad_roots=np.array([[gr[0], gr[1]] for gr in grads]),
+        eps_bar=np.stack([gr[2] for gr in grads]), X_bar=np.stack([gr[3] for gr in grads]),
+        D_bar=np.stack([gr[4] for gr in grads]))
 
 
 def sigma_ao_fixture():

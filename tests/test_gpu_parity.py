@@ -625,3 +625,23 @@ def test_calc_qp_energy_dispatch(golden):
         gw.calc_qp_energy(mf, mode='space-time', eta=0.01, factors=(X, D))
     with pytest.raises(ValueError):
         gw.calc_qp_energy(mf, mode='space-time', return_z=True, factors=(X, D), numerics=Num)
+
+
+def test_contour_qp_gradient_matches_reference_golden(golden):
+    """The gradient of a contour-deformation QP energy in (eps, X, D) on the
+    device (Laplace residues) against the reference's qp_gradient_space_time
+    for three states around the gap: FP64 to 1e-9 of each adjoint's scale."""
+    import warnings
+    from mbptcode_b200 import contour
+    g = golden('contour')
+    eps, nocc, mu = g['eps'], int(g['nocc']), float(g['mu'])
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        nu, nu_w, grid, _ = contour.cd_frequency_grid(eps, nocc)
+    for i, p in enumerate(g['states']):
+        w, z, eb, xb, db = contour.qp_gradient_space_time(g['X'], g['D'], eps, nocc, grid, nu,
+                                                          nu_w, int(p), mu=mu)
+        assert abs(w - g['grad_roots'][i, 0]) < 1e-9 and abs(z - g['grad_roots'][i, 1]) < 1e-8
+        for a, k in ((eb, 'eps_bar'), (xb, 'X_bar'), (db, 'D_bar')):
+            ref = g[k][i]
+            assert np.abs(a - ref).max() <= 1e-8 * np.abs(ref).max(), (int(p), k)

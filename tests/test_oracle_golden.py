@@ -301,3 +301,18 @@ def test_ao_self_energy_oracle(golden):
     assert np.abs(sig - g['sigma']).max() <= 1e-10 * np.abs(g['sigma']).max()
     sub = orc.self_energy_matrix(*args, tau_indices=[1, 4, 7])
     assert np.abs(sub - g['sigma_sub']).max() <= 1e-10 * np.abs(g['sigma_sub']).max()
+
+
+def test_contour_qp_gradient_oracle(golden):
+    """The oracle's gradient of a contour-deformation QP energy (Laplace
+    residues) against the reference's qp_gradient_space_time for three
+    states around the gap."""
+    g = golden('contour')
+    eps, nocc, mu = g['eps'], int(g['nocc']), float(g['mu'])
+    for i, p in enumerate(g['states']):
+        w, z = g['grad_roots'][i]
+        eb, xb, db = orc.qp_gradient_laplace(g['X'], g['D'], eps, nocc, g['tau'], g['tau_w'],
+                                             g['cosft_wt'], g['nu'], g['nu_w'], int(p), mu, w, z)
+        for a, k in ((eb, 'eps_bar'), (xb, 'X_bar'), (db, 'D_bar')):
+            ref = g[k][i]
+            assert np.abs(a - ref).max() <= 1e-9 * np.abs(ref).max(), (int(p), k)
