@@ -547,6 +547,12 @@ struct DysonPipe {
   cublasHandle_t blas2 = nullptr;  // the second half of a batched factorisation
   cudaEvent_t fork = nullptr, join2 = nullptr;
   int nfac = 1;
+  // groups of the batched factorisation (MBPT_DYSON_CHOL_GROUPS, default 4):
+  // group 0 on the caller's stream, group 1 on fac2, the rest on these
+  int groups = 2;
+  std::vector<cudaStream_t> xs;
+  std::vector<cublasHandle_t> xb;
+  std::vector<cudaEvent_t> xj;
   std::vector<cudaEvent_t> ev;
   int *info = nullptr;  // pinned host, `cap` ints
   int cap = 0;
@@ -576,6 +582,21 @@ DysonPipe *dyson_pipe(int nfreq) {
               cusolverDnSetStream(p->solver2, p->fac2) == CUSOLVER_STATUS_SUCCESS &&
               cublasCreate(&p->blas2) == CUBLAS_STATUS_SUCCESS &&
               cublasSetStream(p->blas2, p->fac2) == CUBLAS_STATUS_SUCCESS;
+    const char *genv = std::getenv("MBPT_DYSON_CHOL_GROUPS");
+    const int g = genv ? std::atoi(genv) : 4;
+    p->groups = p->nfac == 2 ? std::max(1, std::min(6, g)) : 1;
+    for (int i = 2; p->ok && i < p->groups; ++i) {
+      cudaStream_t xs = nullptr;
+      cublasHandle_t xb = nullptr;
+      cudaEvent_t xj = nullptr;
+      p->ok = cudaStreamCreateWithFlags(&xs, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&xj, cudaEventDisableTiming) == cudaSuccess &&
+              cublasCreate(&xb) == CUBLAS_STATUS_SUCCESS &&
+              cublasSetStream(xb, xs) == CUBLAS_STATUS_SUCCESS;
+      p->xs.push_back(xs);
+      p->xb.push_back(xb);
+      p->xj.push_back(xj);
+    }
   }
   while (p->ok && static_cast<int>(p->ev.size()) < nfreq) {
     cudaEvent_t e = nullptr;
@@ -623,21 +644,30 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
   const bool batched = b.chol_P != nullptr;
   if (batched) {
     if (cudaMemsetAsync(b.info, 0, sizeof(int) * nfreq, st) != cudaSuccess) return MBPT_ERR_CUDA;
-    // two halves on two streams: one half's DGEMMs fill the GPU while the
-    // other half's diagonal blocks (one CTA per matrix) are factorised
-    const int half = pp->nfac == 2 && nfreq >= 2 * kBatchedCholMin ? nfreq / 2 : nfreq;
-    if (half < nfreq && (cudaEventRecord(pp->fork, st) != cudaSuccess ||
-                         cudaStreamWaitEvent(pp->fac2, pp->fork, 0) != cudaSuccess))
-      return MBPT_ERR_CUDA;
-    int rc0 = chol_batched(chi0, n, half, b.info, b.chol_P, b.chol_Linv, h.blas, st);
-    if (!rc0 && half < nfreq)
-      rc0 = chol_batched(chi0 + half * n * n, n, nfreq - half, b.info + half,
-                         b.chol_P + static_cast<int64_t>(half) * n * kCholNb,
-                         b.chol_Linv + static_cast<int64_t>(half) * kCholNb * kCholNb,
-                         pp->blas2, pp->fac2);
-    if (half < nfreq && (cudaEventRecord(pp->join2, pp->fac2) != cudaSuccess ||
-                         cudaStreamWaitEvent(st, pp->join2, 0) != cudaSuccess))
-      return MBPT_ERR_CUDA;
+    // groups of frequencies on their own streams (four by default, each of
+    // at least kBatchedCholMin frequencies): one
+    // group's DGEMMs fill the GPU while another's diagonal blocks (one CTA
+    // per matrix) are factorised
+    const int G = std::max(1, std::min(pp->groups, nfreq / kBatchedCholMin));
+    auto stream_of = [&](int g) { return g == 0 ? st : (g == 1 ? pp->fac2 : pp->xs[g - 2]); };
+    auto blas_of = [&](int g) { return g == 0 ? h.blas : (g == 1 ? pp->blas2 : pp->xb[g - 2]); };
+    auto join_of = [&](int g) { return g == 1 ? pp->join2 : pp->xj[g - 2]; };
+    if (G > 1 && cudaEventRecord(pp->fork, st) != cudaSuccess) return MBPT_ERR_CUDA;
+    for (int g = 1; g < G; ++g)
+      if (cudaStreamWaitEvent(stream_of(g), pp->fork, 0) != cudaSuccess) return MBPT_ERR_CUDA;
+    int rc0 = MBPT_OK;
+    for (int g = 0; g < G && !rc0; ++g) {
+      const int f0 = static_cast<int>(static_cast<int64_t>(nfreq) * g / G);
+      const int f1 = static_cast<int>(static_cast<int64_t>(nfreq) * (g + 1) / G);
+      rc0 = chol_batched(chi0 + f0 * n * n, n, f1 - f0, b.info + f0,
+                         b.chol_P + static_cast<int64_t>(f0) * n * kCholNb,
+                         b.chol_Linv + static_cast<int64_t>(f0) * kCholNb * kCholNb,
+                         blas_of(g), stream_of(g));
+    }
+    for (int g = 1; g < G; ++g)
+      if (cudaEventRecord(join_of(g), stream_of(g)) != cudaSuccess ||
+          cudaStreamWaitEvent(st, join_of(g), 0) != cudaSuccess)
+        return MBPT_ERR_CUDA;
     if (rc0) return rc0;
     launch_logdet_diag(chi0, n, nfreq, logdet, st);
     if (cudaMemcpyAsync(pp->info, b.info, sizeof(int) * nfreq, cudaMemcpyDeviceToHost, st) !=
