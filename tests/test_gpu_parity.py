@@ -645,3 +645,31 @@ def test_contour_qp_gradient_matches_reference_golden(golden):
         for a, k in ((eb, 'eps_bar'), (xb, 'X_bar'), (db, 'D_bar')):
             ref = g[k][i]
             assert np.abs(a - ref).max() <= 1e-8 * np.abs(ref).max(), (int(p), k)
+
+
+@pytest.mark.parametrize('prec', ['fp64', 'mixed'])
+def test_dyson_batched_groups_with_failed_frequency(prec):
+    """17 frequencies: the batched Cholesky in four stream groups (4-5
+    frequencies each), frequency 11 (third group) not positive definite.
+    It alone is flagged and takes the LU fallback; every other output matches
+    the dense FP64 answer."""
+    rng = np.random.default_rng(11)
+    n, nfreq = 200, 17
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    mats = []
+    for f in range(nfreq):
+        lam = -rng.uniform(0.05, 3.0, n)
+        if f == 11:
+            lam[3] = 1.7
+        mats.append((Q * lam) @ Q.T)
+    chi0 = torch.as_tensor(np.stack(mats), device='cuda')
+    logdet, trace, info, sign = st.dyson_batch(chi0, want_w=True, precision=prec)
+    assert [int(f) for f in np.nonzero(info)[0]] == [11]
+    assert sign[11] == -1 and np.all(np.delete(sign, 11) == 1)
+    tol = 1e-10 if prec == 'fp64' else 5e-6
+    for f, c in enumerate(mats):
+        one_minus = np.eye(n) - c
+        assert abs(float(logdet[f]) - np.linalg.slogdet(one_minus)[1]) < 1e-9 * n
+        W_ref = np.linalg.inv(one_minus) - np.eye(n)
+        err = np.abs(chi0[f].cpu().numpy() - W_ref).max()
+        assert err < (1e-10 if f == 11 else tol) * max(1.0, np.abs(W_ref).max()), (f, err)
