@@ -473,6 +473,29 @@ __global__ void row_dot_into_col_kernel(const double *__restrict__ G,
   if (lane == 0) out[r * ldo + p] += s;
 }
 
+// The batched Cholesky's inverted diagonal blocks of one matrix (block j at
+// Linv + j * step_stride, column-major, ld kCholNb) as TF32 pairs in the two
+// layouts of the triangular-inverse recursion: rows of L^-1 (r_*) and columns
+// of L^-1 as rows (c_*), zeros above the diagonal included, as
+// trtri_diag_blocks_kernel writes them. One CTA per block.
+__global__ void linv_blocks_to_pairs_kernel(const double *__restrict__ Linv,
+                                            int64_t step_stride, int64_t n, float *c_hi,
+                                            float *c_lo, float *r_hi, float *r_lo, int64_t ldp) {
+  const int64_t off = static_cast<int64_t>(blockIdx.x) * kCholNb;
+  const int m = static_cast<int>(min(static_cast<int64_t>(kCholNb), n - off));
+  const double *X = Linv + static_cast<int64_t>(blockIdx.x) * step_stride;
+  for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
+    const int c = idx / m, r = idx % m;
+    const double x = X[c * kCholNb + r];
+    const float h = to_tf32(static_cast<float>(x));
+    const float l = to_tf32(static_cast<float>(x - static_cast<double>(h)));
+    r_hi[(off + r) * ldp + off + c] = h;
+    r_lo[(off + r) * ldp + off + c] = l;
+    c_hi[(off + c) * ldp + off + r] = h;
+    c_lo[(off + c) * ldp + off + r] = l;
+  }
+}
+
 }  // namespace
 
 void launch_chi0_bar_seed(double *a, int64_t n, int nfreq, const double *w, cudaStream_t st) {
@@ -615,6 +638,14 @@ void launch_row_dot_into_col(const double *G, const double *X, int64_t nr, int64
   count_launch();
   row_dot_into_col_kernel<<<static_cast<unsigned>((nr + 7) / 8), 256, 0, st>>>(G, X, nr, nc,
                                                                               out, ldo, p);
+}
+
+void launch_linv_blocks_to_pairs(const double *Linv, int64_t step_stride, int64_t n,
+                                 float *c_hi, float *c_lo, float *r_hi, float *r_lo,
+                                 int64_t ldp, cudaStream_t st) {
+  count_launch();
+  linv_blocks_to_pairs_kernel<<<static_cast<unsigned>((n + kCholNb - 1) / kCholNb), 256, 0,
+                                st>>>(Linv, step_stride, n, c_hi, c_lo, r_hi, r_lo, ldp);
 }
 
 }  // namespace mbpt

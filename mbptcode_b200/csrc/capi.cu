@@ -44,6 +44,9 @@ void launch_strided_to_tf32(const double *src, int64_t rows, int64_t k, int64_t 
                             float *hi, float *lo, int64_t rows_p, int64_t k_p, cudaStream_t st);
 void launch_row_scaled_copy(const double *X, int64_t M, int64_t n, int64_t p, double *out,
                             cudaStream_t st);
+void launch_linv_blocks_to_pairs(const double *Linv, int64_t step_stride, int64_t n,
+                                 float *c_hi, float *c_lo, float *r_hi, float *r_lo,
+                                 int64_t ldp, cudaStream_t st);
 void launch_rowdot_f32(const float *R, int64_t ld_r, const double *X, int64_t ld_x, int64_t M,
                        int64_t S, double *out, cudaStream_t st);
 void launch_col_scale(const double *Y, const double *v, int64_t nr, int64_t nc, double factor,
@@ -363,7 +366,8 @@ struct TimingTag {
 // tensor cores over the tiles on and above the diagonal (rows of (L^-1)^T
 // vanish for k < row), W - I written whole (returns with *full = true).
 int spd_inverse_from_factor(Handles &h, double *L, int64_t n, double *T, double *Tr,
-                            const PairScratch *pairs, int *err, bool *full, cudaStream_t st) {
+                            const PairScratch *pairs, int *err, bool *full, cudaStream_t st,
+                            const double *diag_inv = nullptr, int64_t diag_inv_stride = 0) {
   *full = false;
   TimingTag tag(kTimingDyson);
   if (pairs) {
@@ -371,8 +375,14 @@ int spd_inverse_from_factor(Handles &h, double *L, int64_t n, double *T, double 
     const int64_t np = s.np, kp = round_up(n, 32);
     // rows of L (its upper triangle is never read)
     launch_strided_to_tf32(L, n, n, 1, n, s.lr_hi, s.lr_lo, np, np, st);
-    int rc = launch_trtri_diag_blocks(L, n, n, static_cast<int>(kTrtriLeaf), st, s.ic_hi,
-                                      s.ic_lo, s.ir_hi, s.ir_lo, np);
+    int rc = MBPT_OK;
+    if (diag_inv)
+      // the batched factorisation kept its inverted 128 x 128 diagonal blocks
+      launch_linv_blocks_to_pairs(diag_inv, diag_inv_stride, n, s.ic_hi, s.ic_lo, s.ir_hi,
+                                  s.ir_lo, np, st);
+    else
+      rc = launch_trtri_diag_blocks(L, n, n, static_cast<int>(kTrtriLeaf), st, s.ic_hi,
+                                    s.ic_lo, s.ir_hi, s.ir_lo, np);
     if (rc) return rc;
     rc = trtri_pairs(s, n, err, st);
     if (rc) return rc;
@@ -443,9 +453,10 @@ constexpr int kBatchedCholMin = 4;  // frequencies from which the batch beats on
 // batched DGEMM, L[j0+nb:, j0-block] = P_below L_jj^-T. Every launch carries
 // the whole batch, so the latency-bound diagonal blocks cost one launch per
 // step for all frequencies. P: nmat * n * kCholNb doubles; Linv: nmat *
-// kCholNb^2 doubles; info: nmat ints, zeroed by the caller.
+// kCholNb^2 doubles per step, step j at Linv + j * linv_step_stride (0: every
+// step in the same place); info: nmat ints, zeroed by the caller.
 int chol_batched(double *A, int64_t n, int nmat, int *info, double *P, double *Linv,
-                 cublasHandle_t h, cudaStream_t st) {
+                 cublasHandle_t h, cudaStream_t st, int64_t linv_step_stride = 0) {
   const long long n2 = static_cast<long long>(n) * n;
   const double one = 1.0, minus = -1.0, zero = 0.0;
   for (int64_t j0 = 0; j0 < n; j0 += kCholNb) {
@@ -459,13 +470,14 @@ int chol_batched(double *A, int64_t n, int nmat, int *info, double *P, double *L
                                   static_cast<int>(m), static_cast<long long>(m) * nbj,
                                   nmat) != CUBLAS_STATUS_SUCCESS)
       return MBPT_ERR_CUDA;
-    int rc = launch_chol_diag_block(P, m, nbj, A, n, j0, nmat, Linv, info, st);
+    double *Lj = Linv + (j0 / kCholNb) * linv_step_stride;
+    int rc = launch_chol_diag_block(P, m, nbj, A, n, j0, nmat, Lj, info, st);
     if (rc) return rc;
     const int64_t mb = m - nbj;
     if (mb > 0 &&
         cublasDgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_T, static_cast<int>(mb), nbj, nbj,
                                   &one, P + nbj, static_cast<int>(m),
-                                  static_cast<long long>(m) * nbj, Linv, kCholNb,
+                                  static_cast<long long>(m) * nbj, Lj, kCholNb,
                                   static_cast<long long>(kCholNb) * kCholNb, &zero,
                                   A + j0 * n + j0 + nbj, static_cast<int>(n), n2,
                                   nmat) != CUBLAS_STATUS_SUCCESS)
@@ -519,7 +531,9 @@ DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq, int mode = MBPT_MODE_FP64
   b.T = ar.take<double>(kLauumBlock * kLauumBlock);
   if (batched_chol_enabled(nfreq)) {
     b.chol_P = ar.take<double>(static_cast<int64_t>(nfreq) * n * kCholNb);
-    b.chol_Linv = ar.take<double>(static_cast<int64_t>(nfreq) * kCholNb * kCholNb);
+    // every step's inverted diagonal blocks are kept: the mixed inverse reads them
+    const int64_t steps = (n + kCholNb - 1) / kCholNb;
+    b.chol_Linv = ar.take<double>(steps * nfreq * kCholNb * kCholNb);
   }
   if (mode == MBPT_MODE_MIXED) {
     const int64_t np = round_up(n, 128), cap = np * np;
@@ -662,7 +676,8 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
       rc0 = chol_batched(chi0 + f0 * n * n, n, f1 - f0, b.info + f0,
                          b.chol_P + static_cast<int64_t>(f0) * n * kCholNb,
                          b.chol_Linv + static_cast<int64_t>(f0) * kCholNb * kCholNb,
-                         blas_of(g), stream_of(g));
+                         blas_of(g), stream_of(g),
+                         static_cast<int64_t>(nfreq) * kCholNb * kCholNb);
     }
     for (int g = 1; g < G; ++g)
       if (cudaEventRecord(join_of(g), stream_of(g)) != cudaSuccess ||
@@ -720,9 +735,11 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
         }
         cublasSetStream(h.blas, pp->side);
         bool full = false;
-        rc = spd_inverse_from_factor(h, m, n, b.T, b.rhs,
-                                     mode == MBPT_MODE_MIXED ? &b.pairs : nullptr, err, &full,
-                                     pp->side);
+        rc = spd_inverse_from_factor(
+            h, m, n, b.T, b.rhs, mode == MBPT_MODE_MIXED ? &b.pairs : nullptr, err, &full,
+            pp->side,
+            batched ? b.chol_Linv + static_cast<int64_t>(f) * kCholNb * kCholNb : nullptr,
+            static_cast<int64_t>(nfreq) * kCholNb * kCholNb);
         cublasSetStream(h.blas, st);
         if (rc) break;
         if (!full) launch_symmetrize_minus_identity(m, n, 1, pp->side);
