@@ -306,6 +306,10 @@ int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t 
     if (epi == EPI_TF32_PAIR)
       return launch<1, 128, EPI_TF32_PAIR, true, kDrain>(A, B, m_rows, n_rows, e, err, st,
                                                          band);
+    // the symmetric FP64 store (W = L^-T L^-1): 128 x 256 tiles, which halve
+    // the A reads through shared memory for the three TF32 products
+    if (epi == EPI_F64_SYM && (band & BAND_UPPER))
+      return launch<1, 256, EPI_F64_SYM, true, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
     if (epi == EPI_F64_SYM)
       return launch<1, 128, EPI_F64_SYM, true, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
     return launch<1, 128, EPI_F32, true, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
