@@ -28,8 +28,14 @@ solved as the reference solves it (`qp_energy_cd` on
 a grid over the narrowest window about the bare level walked outward, cells
 halved where the secant slope hides a pole, each bracket refined by Newton on
 the closed-form slope (`sigma_cd_slope`) safeguarded by the bracket, the
-weights of a positive-weight self-energy summing to one ending the walk. The
-explicit O(N^4) particle-hole backends (`C_ov`) are not part of this module.
+weights of a positive-weight self-energy summing to one ending the walk.
+
+Continuation 'cd' takes the residues' W from the explicit particle-hole
+response instead (`ExplicitRealScreening`, ``real_screening.py:57-91``):
+C_ov = B[:, occ, virt] from the occupied states' slices, chi0(freq) =
+2 (C_ov f) C_ov^T by mbpt_chi0_aux (a symmetric rank-k FP64 product over
+column chunks) and the Dyson step, which falls back from Cholesky to LU above
+the particle-hole gap where 1 - chi0 is indefinite.
 """
 from __future__ import annotations
 
@@ -41,7 +47,8 @@ import torch
 
 from ._lib import WORKSPACE, check, lib, ptr, require_device, stream_ptr
 from .grids import TimeFrequencyGrid, gauss_legendre_grid, particle_hole_window
-from .space_time import _eps_host, chi0_sweep, dyson_batch, to_device, transform
+from .space_time import (_eps_host, chi0_aux, chi0_sweep, dyson_batch, frequency_factor,
+                         to_device, transform)
 
 # MBPTcode src/Base/numerics/constants.py
 RESIDUE_ON_CONTOUR_TOL = 1e-10   # :461
@@ -324,33 +331,152 @@ class LaplaceRealScreening:
         return float(yd @ (dchi0 @ yd))
 
 
+def ov_energies(eps, nocc):
+    """d[(i, a)] = eps_a - eps_i on the pair index of C_ov, i major
+    (``Base/orbital_spaces.py:31-34``)."""
+    eps = np.asarray(eps, float)
+    return (eps[nocc:][None, :] - eps[:nocc][:, None]).ravel()
+
+
+def three_index_ov(X, D, eps, nocc, tile_gb=None):
+    """C_ov[P, (i, a)] = sum_k D[k, P] X[k, i] X[k, a], (naux, nocc * nvirt)
+    on the device (``LinearResponse/space_time.py:833-851``): the occupied
+    states' three-index slices (mbpt_three_index_slices), a block of
+    occupied states at a time, their virtual columns laid side by side.
+    tile_gb bounds a block's slices (default 2 GB)."""
+    dev = require_device()
+    Xd, Dd = to_device(X, dev), to_device(D, dev)
+    norb, naux = Xd.shape[1], Dd.shape[1]
+    nvirt = norb - nocc
+    C = torch.empty((naux, nocc, nvirt), dtype=torch.float64, device=dev)
+    per = 8 * naux * norb
+    step = max(1, min(nocc, int((tile_gb or 2.0) * 1e9 // per)))
+    for i0 in range(0, nocc, step):
+        i1 = min(nocc, i0 + step)
+        B = three_index_slices(Xd, Dd, np.arange(i0, i1))
+        C[:, i0:i1, :] = B[:, :, nocc:].permute(1, 0, 2)
+    return C.reshape(naux, nocc * nvirt)
+
+
+def require_three_index(C_ov, what):
+    """``contour_deformation.py:109-114``."""
+    if C_ov is None:
+        raise ResidueRefused(
+            f'{what} needs C_ov = B[:, occ, virt] as (naux, nocc*nvirt) and it was not '
+            f'supplied. A frontier state sweeps no residues and needs none once the '
+            f'imaginary-axis screening comes in as wbp or wc.')
+
+
+class ExplicitRealScreening:
+    """W at a real frequency from the particle-hole block C_ov, explicitly
+    (``real_screening.py:57-91``, continuation 'cd'): chi0 = 2 (C_ov f) C_ov^T
+    by mbpt_chi0_aux (a symmetric rank-k product over column chunks) and
+    W - I by the Dyson step (Cholesky below the gap, LU above it, where
+    1 - chi0 is indefinite), the W - I of the latest frequencies kept for
+    later calls. eta broadens the particle-hole poles (off by default).
+    pair_energies: the pair index of C_ov when it is not the one (eps, nocc)
+    spans. FP64; O(naux^2 nocc nvirt) per frequency, the route the cubic one
+    is checked against and the only one above the particle-hole gap."""
+
+    def __init__(self, C_ov, eps, nocc, eta=0.0, pair_energies=None, cache_bytes=4e9):
+        self.C_ov = to_device(C_ov, require_device())
+        self.eps = np.asarray(eps, float)
+        self.nocc = nocc
+        self.eta = float(eta)
+        self.d = (ov_energies(self.eps, nocc) if pair_energies is None
+                  else np.asarray(pair_energies, float))
+        if self.d.size != self.C_ov.shape[1]:
+            raise ValueError(f'C_ov has {self.C_ov.shape[1]} pairs, the pair energies '
+                             f'{self.d.size}')
+        naux = self.C_ov.shape[0]
+        self._cap = max(2, min(2 * len(self.eps), int(cache_bytes // (8 * naux * naux))))
+        self._w = OrderedDict()
+
+    def w_minus_identity(self, freq, imaginary=False):
+        key = (float(freq), bool(imaginary))
+        w = self._w.get(key)
+        if w is None:
+            f = frequency_factor(self.d, float(freq), imaginary, self.eta)
+            chi0 = chi0_aux([(self.C_ov, f)], 2.0)[None]
+            dyson_batch(chi0, want_w=True, precision='fp64')
+            w = self._w[key] = chi0[0]
+            if len(self._w) > self._cap:
+                self._w.popitem(last=False)
+        else:
+            self._w.move_to_end(key)
+        return w
+
+    def apply(self, freq, b):
+        """W(freq) b = b + (W - I) b."""
+        bd = to_device(b, self.C_ov.device)
+        y = bd + self.w_minus_identity(freq) @ bd
+        return y if isinstance(b, torch.Tensor) else y.cpu().numpy()
+
+    def slope(self, freq, y):
+        """y^T [dchi0/dfreq] y = 2 sum_(ia) df/dw (C_ov^T y)_(ia)^2
+        (``real_screening.py:87-91``)."""
+        z = (self.C_ov.T @ to_device(y, self.C_ov.device)).cpu().numpy()
+        return 2.0 * float(frequency_factor(self.d, float(freq), False, self.eta,
+                                            slopes=True)[2] @ z ** 2)
+
+
+def residue_backend(real_screening, C_ov, eps, nocc, eta):
+    """The backend the residue term uses: the one given, else the explicit one
+    from C_ov (``contour_deformation.py:117-122``)."""
+    if real_screening is not None:
+        return real_screening
+    require_three_index(C_ov, 'the residue term')
+    return ExplicitRealScreening(C_ov, eps, nocc, eta)
+
+
+def wc_explicit(Bp, C_ov, d, nu_points, block=8):
+    """wc[k, q] = Bp[:, q]^T (W(i nu_k) - I) Bp[:, q] from the explicit
+    imaginary-axis screening (``contour_deformation.py:240-245``): per block
+    of frequencies the explicit chi0 (mbpt_chi0_aux), the Dyson step and the
+    screening contraction. (nfreq, norb) on the host."""
+    dev = require_device()
+    Cd = to_device(C_ov, dev)
+    Bd = to_device(Bp, dev)
+    naux = Cd.shape[0]
+    nu = np.asarray(nu_points, float)
+    out = []
+    for k0 in range(0, len(nu), block):
+        ks = nu[k0:k0 + block]
+        stack = torch.empty((len(ks), naux, naux), dtype=torch.float64, device=dev)
+        for m, v in enumerate(ks):
+            chi0_aux([(Cd, frequency_factor(d, float(v), True))], 2.0, out=stack[m])
+        dyson_batch(stack, want_w=True, precision='fp64')
+        out.append(screening_contraction_device(stack, [Bd])[0].cpu().numpy())
+    return np.concatenate(out)
+
+
 def sigma_cd(p, omega, Bp, eps, nocc, nu_points, nu_weights, residues=None, wbp=None,
              eta=0.0, wc=None, C_ov=None, real_screening=None):
     """Sigma^c_pp(omega) by contour deformation from the state's slice Bp and
     its contracted screening wc (``contour_deformation.py:310-343``):
     the imaginary-axis integral and, for the residue set (recomputed at omega
     when not given), sum_q w_q (b_q^T W(|eps_q - omega|) b_q - b_q^T b_q) with
-    `real_screening`'s W (a LaplaceRealScreening)."""
-    if C_ov is not None or eta:
-        raise NotImplementedError('the explicit particle-hole backends are outside the '
-                                  'cubic device route')
+    `real_screening`'s W (a LaplaceRealScreening or ExplicitRealScreening;
+    with C_ov and no backend the explicit one). With neither wc nor wbp the
+    imaginary-axis screening is built explicitly from C_ov (`wc_explicit`)."""
     eps = np.asarray(eps, float)
     Bh = Bp.detach().cpu().numpy() if isinstance(Bp, torch.Tensor) else np.asarray(Bp)
     if wc is None:
         if wbp is None:
-            raise ValueError('sigma_cd needs wc or wbp on the device route')
-        wc = screening_contraction(Bh, wbp)
+            require_three_index(C_ov, 'the imaginary-axis screening without wbp or wc')
+            wc = wc_explicit(Bp, C_ov, ov_energies(eps, nocc), nu_points)
+        else:
+            wc = screening_contraction(Bh, wbp)
     wc = wc.detach().cpu().numpy() if isinstance(wc, torch.Tensor) else np.asarray(wc)
     c, _ = cd_integral_weights(omega - eps, nu_points, nu_weights)
     s_int = -float(np.einsum('kq,kq->', c, wc)) / np.pi
     res = residue_set(eps, nocc, omega) if residues is None else residues
     s_res = 0.0
     if res:
-        if real_screening is None:
-            raise ValueError('the residue term needs real_screening on the device route')
+        rs = residue_backend(real_screening, C_ov, eps, nocc, eta)
         for q, weight in res:
             b = Bh[:, q]
-            y = real_screening.apply(abs(eps[q] - omega), b)
+            y = rs.apply(abs(eps[q] - omega), b)
             s_res += weight * (float(b @ y) - float(b @ b))
     return s_int + s_res
 
@@ -361,19 +487,18 @@ def sigma_cd_slope(p, omega, Bp, eps, nocc, nu_points, nu_weights, residues, wc,
     (``contour_deformation.py:346-373``): the integral weights' derivative
     against wc, and per residue W [dchi0/dfreq] W contracted with b_q on both
     sides, signed by the side of the pole."""
-    if C_ov is not None or eta:
-        raise NotImplementedError('the explicit particle-hole backends are outside the '
-                                  'cubic device route')
     eps = np.asarray(eps, float)
     Bh = Bp.detach().cpu().numpy() if isinstance(Bp, torch.Tensor) else np.asarray(Bp)
     wc = wc.detach().cpu().numpy() if isinstance(wc, torch.Tensor) else np.asarray(wc)
     _, dc = cd_integral_weights(omega - eps, nu_points, nu_weights)
     slope = -float(np.einsum('kq,kq->', dc, wc)) / np.pi
-    for q, weight in residues or ():
-        gap = eps[q] - omega
-        freq = abs(gap)
-        y = real_screening.apply(freq, Bh[:, q])
-        slope -= weight * real_screening.slope(freq, y) * np.sign(gap)
+    if residues:
+        rs = residue_backend(real_screening, C_ov, eps, nocc, eta)
+        for q, weight in residues:
+            gap = eps[q] - omega
+            freq = abs(gap)
+            y = rs.apply(freq, Bh[:, q])
+            slope -= weight * rs.slope(freq, y) * np.sign(gap)
     return slope
 
 
@@ -564,29 +689,35 @@ def qp_energy_cd(p, Bp, eps, nocc, nu_points, nu_weights, xc_correction=0.0, tol
     """(eps^QP_p, Z_p, residues) of w = eps_p + xc_correction + Sigma^c(w) by
     contour deformation (``contour_deformation.py:376-436``): the scan about
     the bare level with Newton on the closed-form slope, the residue set
-    re-decided at every point and frozen at the root."""
+    re-decided at every point and frozen at the root. The imaginary-axis
+    screening comes in as wc, as wbp contracted once here, or -- with neither
+    -- explicitly from C_ov (`wc_explicit`, contracted once). The residues
+    read `real_screening`, else the explicit backend of C_ov (broadened by
+    eta), built once for the whole scan: its kept W - I serves the value and
+    the slope at one point, as the reference's `_PointApplies` does."""
     if follow is not None or branch is not None:
         raise NotImplementedError('following a root along a walk is outside the device route')
-    if C_ov is not None or eta:
-        raise NotImplementedError('the explicit particle-hole backends are outside the '
-                                  'cubic device route')
     eps = np.asarray(eps, float)
     Bh = Bp.detach().cpu().numpy() if isinstance(Bp, torch.Tensor) else np.asarray(Bp)
     if wc is None:
-        if wbp is None:
-            raise ValueError('qp_energy_cd needs wc or wbp on the device route')
-        wc = screening_contraction(Bh, wbp)
+        if wbp is not None:
+            wc = screening_contraction(Bh, wbp)
+        else:
+            require_three_index(C_ov, 'the imaginary-axis screening without wbp or wc')
+            wc = wc_explicit(Bp, C_ov, ov_energies(eps, nocc), nu_points)
     wc = wc.detach().cpu().numpy() if isinstance(wc, torch.Tensor) else np.asarray(wc)
+    if real_screening is not None or C_ov is not None:
+        real_screening = residue_backend(real_screening, C_ov, eps, nocc, eta)
+    common = dict(eta=eta, C_ov=C_ov, real_screening=real_screening)
 
     def residual(w):
         return w - eps[p] - xc_correction - sigma_cd(
             p, w, Bh, eps, nocc, nu_points, nu_weights, residues=residue_set(eps, nocc, w),
-            wc=wc, real_screening=real_screening)
+            wc=wc, **common)
 
     def fprime(w):
         return 1.0 - sigma_cd_slope(p, w, Bh, eps, nocc, nu_points, nu_weights,
-                                    residue_set(eps, nocc, w), wc,
-                                    real_screening=real_screening)
+                                    residue_set(eps, nocc, w), wc, **common)
     w, z = solve_qp_equation_scan(residual, fprime, float(eps[p] + xc_correction), tol=tol,
                                   max_iter=max_iter, label=f'orbital {p}',
                                   refusals=(ResidueRefused,))
@@ -597,58 +728,75 @@ HARTREE_TO_EV = 27.211386245988  # MBPTcode constants.py:11 (CODATA 2018)
 
 
 def contour_roots(X, D, eps, nocc, states, ntau=CD_NTAU, nfreq_cd=CD_NFREQ, w0_cd=None,
-                  e_min_below_gap=None, xc_correction=0.0, mu=None):
+                  e_min_below_gap=None, xc_correction=0.0, mu=None, continuation='laplace'):
     """(roots in Hartree, Z, per-state records) of the states on one contour
-    grid with the residues from the cosh transform of proj(tau)
-    (``contour_deformation.py:558-598, 780-812``, continuation 'laplace'):
-    one proj(tau) and one W per frequency serve every state, each state's
-    root by `qp_energy_cd`. xc_correction: the static term, one per state or
-    one for all."""
+    grid (``contour_deformation.py:558-598, 767-812``): one proj(tau) and one
+    W per frequency serve every state's imaginary-axis term, each state's
+    root by `qp_energy_cd`. The residues read W at real frequencies from the
+    cosh transform of the same proj(tau) (continuation 'laplace', which
+    refuses a state whose residues the time grid does not carry) or from the
+    explicit particle-hole response of C_ov (continuation 'cd', any state).
+    xc_correction: the static term, one per state or one for all."""
+    if continuation not in ('laplace', 'cd'):
+        raise ValueError(f"continuation={continuation!r}: choose 'cd' or 'laplace'")
     eps = _eps_host(eps)
     states = np.atleast_1d(np.asarray(states, int))
+    explicit = (ExplicitRealScreening(three_index_ov(X, D, eps, nocc), eps, nocc)
+                if continuation == 'cd' else None)
     nu, nu_w, grid, w0 = cd_frequency_grid(eps, nocc, ntau=ntau, nfreq_cd=nfreq_cd,
                                            w0_cd=w0_cd, e_min_below_gap=e_min_below_gap)
     proj = polarizability_tau(X, D, eps, nocc, grid, mu=mu)
     B = three_index_slices(X, D, states)
     wcs = cd_screening_contraction_multi(proj, grid.cosft_wt, list(B))
-    lap = LaplaceRealScreening(proj, grid, eps, nocc)
+    if explicit is None:
+        backend = LaplaceRealScreening(proj, grid, eps, nocc)
+    else:
+        backend = explicit
+        del proj
     roots, zs, records = np.zeros(len(states)), np.zeros(len(states)), []
     for i, p in enumerate(states):
         xc = (float(np.asarray(xc_correction).ravel()[i]) if np.ndim(xc_correction)
               else float(xc_correction))
         try:
             w, z, res = qp_energy_cd(int(p), B[i], eps, nocc, nu, nu_w, xc_correction=xc,
-                                     wc=wcs[i], real_screening=lap)
+                                     wc=wcs[i], real_screening=backend)
         except ResidueRefused as refusal:
+            if explicit is not None:
+                raise
             raise ResidueRefused(
                 f"continuation='laplace' cannot serve orbital {int(p)}: its contour sweeps "
                 f'a residue the imaginary-time grid does not represent. {refusal}') from refusal
         roots[i], zs[i] = w, z
+        error = None
+        if explicit is None and res:
+            error = max(backend.representation_error(abs(eps[q] - w)) for q, _ in res)
         records.append({'state': int(p), 'residues': len(res),
-                        'representation_error': (max(lap.representation_error(
-                            abs(eps[q] - w)) for q, _ in res) if res else None)})
-    info = {'continuation': 'laplace', 'ntau': int(ntau), 'nfreq_cd': int(nfreq_cd),
-            'w0_cd': float(w0), 'residue_route_taken': 'laplace', 'states': records}
+                        'representation_error': error})
+    info = {'continuation': continuation, 'ntau': int(ntau), 'nfreq_cd': int(nfreq_cd),
+            'w0_cd': float(w0),
+            'residue_route_taken': 'explicit' if explicit is not None else 'laplace',
+            'states': records}
     return roots, zs, info
 
 
-def solve_qp_energy_contour(mf, mol, nocc, states, continuation='laplace', numerics=None,
+def solve_qp_energy_contour(mf, mol, nocc, states, continuation='cd', numerics=None,
                             w0_cd=None, auxbasis=None, radii=None, counts=None, factors=None,
                             grid_accuracy=None, sigma_x='mf', dm_correction=None,
                             eps_anchor=None, spin_channel='alpha', xc_diagonal=None):
     """Drop-in for ``GW/contour_deformation.py:601-820`` on a restricted
-    gas-phase reference with pre-built factors, continuation 'laplace':
-    (quasiparticle energies in eV, pole strengths, diagnostics). The mean
-    field gives eps (mo_energy); the static term <Sigma_x - v_xc> is
-    `xc_diagonal` (zero on a Hartree-Fock reference); numerics.quadrature:
-    ntau_cd and nfreq_cd where it has them. 'cd' (the explicit O(N^4)
-    residues, the reference's default) and 'sop' are outside the device
-    route and refused; 'laplace' solves the same contour wherever the time
-    grid carries the residue frequencies, and refuses a state by name
-    otherwise, as the reference does."""
-    if continuation != 'laplace':
+    gas-phase reference with pre-built factors: (quasiparticle energies in eV,
+    pole strengths, diagnostics). The mean field gives eps (mo_energy); the
+    static term <Sigma_x - v_xc> is `xc_diagonal` (zero on a Hartree-Fock
+    reference); numerics.quadrature: ntau_cd and nfreq_cd where it has them.
+    'cd' (the default, as in the reference) reads the residues' W from the
+    explicit particle-hole response of C_ov, O(N^4) per residue frequency and
+    exact for any state; 'laplace' solves the same contour from the cubic
+    cosh transform wherever the time grid carries the residue frequencies,
+    and refuses a state by name otherwise, as the reference does. 'sop' (the
+    pole model) is outside the device route and refused."""
+    if continuation not in ('cd', 'laplace'):
         raise NotImplementedError(f"continuation={continuation!r}: the device route runs "
-                                  "'laplace' (the cubic residues)")
+                                  "'cd' (explicit residues) and 'laplace' (cubic residues)")
     if factors is None:
         raise NotImplementedError('building the ISDF factors needs pyscf (integrals and the '
                                   'fit); pass factors=(X_mo, D)')
@@ -667,7 +815,7 @@ def solve_qp_energy_contour(mf, mol, nocc, states, continuation='laplace', numer
         xc = xc + (np.asarray(eps_anchor, float)[states] - eps[states])
     X, D = (factors['X_mo'], factors['D']) if isinstance(factors, dict) else factors[:2]
     roots, zs, info = contour_roots(X, D, eps, nocc, states, ntau=ntau, nfreq_cd=nfreq,
-                                    w0_cd=w0_cd, xc_correction=xc)
+                                    w0_cd=w0_cd, xc_correction=xc, continuation=continuation)
     return roots * HARTREE_TO_EV, zs, info
 
 

@@ -438,6 +438,20 @@ __global__ void rowdot_f32_kernel(const float *__restrict__ R, int64_t ld_r,
   }
 }
 
+// out[P, j] = s (C[P, j0 + j] f[j0 + j]) for an nr x nc block of the
+// particle-hole columns of C (leading dimension ldc): the explicit response's
+// scaled factor, one column chunk at a time
+__global__ void cols_scaled_copy_kernel(const double *__restrict__ C, int64_t ldc, int64_t j0,
+                                        const double *__restrict__ f, double s, int64_t nr,
+                                        int64_t nc, double *__restrict__ out) {
+  const int64_t total = nr * nc;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = i / nc, j = i % nc;
+    out[i] = s * (C[r * ldc + j0 + j] * f[j0 + j]);
+  }
+}
+
 // out[P, q] (+)= factor Y[P, q] v[q] over an nr x nc row-major block
 __global__ void col_scale_kernel(const double *__restrict__ Y, const double *__restrict__ v,
                                  int64_t nr, int64_t nc, double factor, double *out,
@@ -619,6 +633,12 @@ void launch_rowdot_f32(const float *R, int64_t ld_r, const double *X, int64_t ld
   dim3 grid(static_cast<unsigned>((S + 31) / 32), static_cast<unsigned>((M + 255) / 256));
   count_launch();
   rowdot_f32_kernel<<<grid, dim3(32, 8), 0, st>>>(R, ld_r, X, ld_x, M, S, out);
+}
+
+void launch_cols_scaled_copy(const double *C, int64_t ldc, int64_t j0, const double *f,
+                             double s, int64_t nr, int64_t nc, double *out, cudaStream_t st) {
+  count_launch();
+  cols_scaled_copy_kernel<<<blocks(nr * nc), 256, 0, st>>>(C, ldc, j0, f, s, nr, nc, out);
 }
 
 void launch_col_scale(const double *Y, const double *v, int64_t nr, int64_t nc, double factor,

@@ -51,6 +51,8 @@ void launch_rowdot_f32(const float *R, int64_t ld_r, const double *X, int64_t ld
                        int64_t S, double *out, cudaStream_t st);
 void launch_col_scale(const double *Y, const double *v, int64_t nr, int64_t nc, double factor,
                       double *out, bool accumulate, cudaStream_t st);
+void launch_cols_scaled_copy(const double *C, int64_t ldc, int64_t j0, const double *f,
+                             double s, int64_t nr, int64_t nc, double *out, cudaStream_t st);
 void launch_row_scale_acc(const double *a, int64_t lda, int64_t p, const double *b, int64_t nr,
                           int64_t nc, double *out, cudaStream_t st);
 void launch_row_dot_into_col(const double *G, const double *X, int64_t nr, int64_t nc,
@@ -1419,6 +1421,44 @@ int mbpt_three_index_slices(const double *X, int64_t M, int64_t norb, const doub
                   B + static_cast<int64_t>(s) * naux * norb, norb))
       return MBPT_ERR_CUDA;
   }
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+// The explicit particle-hole response chi0 = s (C f) C^T: columns of C in
+// chunks of kChi0AuxChunk, each chunk scaled into the workspace and folded in
+// by a symmetric rank-k product (one triangle), the other triangle mirrored.
+constexpr int64_t kChi0AuxChunk = 4096;
+
+size_t mbpt_chi0_aux_workspace_bytes(int64_t naux, int64_t nov) {
+  if (naux < 1 || nov < 1) return 0;
+  return sizeof(double) * static_cast<size_t>(naux) * std::min(nov, kChi0AuxChunk) + 2048;
+}
+
+int mbpt_chi0_aux(const double *C, int64_t naux, int64_t nov, int64_t ldc, const double *f,
+                  double spin_factor, int accumulate, double *chi0, void *ws, size_t ws_bytes,
+                  void *stream) {
+  if (naux < 1 || nov < 1 || ldc < nov || naux > INT32_MAX || ldc > INT32_MAX)
+    return MBPT_ERR_SHAPE;
+  cudaStream_t st = S(stream);
+  const int64_t chunk = std::min(nov, kChi0AuxChunk);
+  Arena ar = arena(ws, ws_bytes);
+  double *T = ar.take<double>(naux * chunk);
+  if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+  cublasHandle_t h = handles(st).blas;
+  const double one = 1.0;
+  for (int64_t j0 = 0; j0 < nov; j0 += chunk) {
+    const int64_t nc = std::min(chunk, nov - j0);
+    launch_cols_scaled_copy(C, ldc, j0, f, spin_factor, naux, nc, T, st);
+    const double beta = (j0 == 0 && !accumulate) ? 0.0 : 1.0;
+    // column-major view: chi0 = T_cm^T C_cm over this chunk's rows of the
+    // transposed factors, its upper triangle (the row-major lower one)
+    if (cublasDsyrkx(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, static_cast<int>(naux),
+                     static_cast<int>(nc), &one, T, static_cast<int>(nc), C + j0,
+                     static_cast<int>(ldc), &beta, chi0,
+                     static_cast<int>(naux)) != CUBLAS_STATUS_SUCCESS)
+      return MBPT_ERR_CUDA;
+  }
+  launch_mirror_lower_to_upper(chi0, naux, st);
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 

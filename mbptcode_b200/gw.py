@@ -645,11 +645,12 @@ def calc_qp_energy(mf, selfenergy='GW', polarizability='RPA', df=True, eta=None,
     """Quasiparticle energies in eV (``GW/qp_energy.py:294-616``), mode
     'space-time' on pre-built factors (route_kwargs['factors'] = (X_mo, D) or
     (X_mo, D, X_ao)): G0W0 with continuation 'pade' (the default; no Z, as
-    the reference) or 'laplace' (the contour, Z from its slope), or
-    self_consistency 'evGW'. mf: an object with mo_energy and mo_occ (or
-    route_kwargs['nocc']). The reference's refusals are kept: GW@RPA on
-    density fitting only, no eta, no tda; the Casida and imaginary-frequency
-    modes and the 'cd'/'sop' continuations are other routes and refused."""
+    the reference), 'cd' or 'laplace' (the contour with explicit or cubic
+    residues, Z from its slope), or self_consistency 'evGW'. mf: an object
+    with mo_energy and mo_occ (or route_kwargs['nocc']). The reference's
+    refusals are kept: GW@RPA on density fitting only, no eta, no tda; the
+    Casida and imaginary-frequency modes and the 'sop' continuation are other
+    routes and refused."""
     if mode != 'space-time':
         raise NotImplementedError(f"mode={mode!r}: the device route is mode='space-time'")
     if isinstance(selfenergy, list) or str(selfenergy).upper() != 'GW':
@@ -664,7 +665,7 @@ def calc_qp_energy(mf, selfenergy='GW', polarizability='RPA', df=True, eta=None,
     if eta is not None:
         raise ValueError("eta broadens nothing on mode='space-time'")
     continuation = 'pade' if continuation is None else continuation
-    if continuation not in ('pade', 'laplace'):
+    if continuation not in ('pade', 'laplace', 'cd'):
         raise NotImplementedError(f'continuation={continuation!r} is outside the device route')
     eps = np.asarray(getattr(mf, 'mo_energy', mf), float)
     nocc = route_kwargs.pop('nocc', None)
@@ -686,10 +687,10 @@ def calc_qp_energy(mf, selfenergy='GW', polarizability='RPA', df=True, eta=None,
     elif self_consistency != 'G0W0':
         raise NotImplementedError(f'self_consistency={self_consistency!r} is outside the device '
                                   'route')
-    elif continuation == 'laplace':
+    elif continuation in ('laplace', 'cd'):
         from .contour import solve_qp_energy_contour
         ev, zs, _ = solve_qp_energy_contour(eps, None, nocc, np.asarray(states),
-                                            continuation='laplace', eps_anchor=eps_anchor,
+                                            continuation=continuation, eps_anchor=eps_anchor,
                                             **route_kwargs)
         res, z = list(ev), list(zs)
     else:

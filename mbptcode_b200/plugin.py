@@ -4,7 +4,9 @@ MBPTcode has no plugin registry: its kernels are module-level functions that
 importing modules bind by name (``GW/space_time.py:66-79``,
 ``GW/imaginary_time.py:33-36``, ``gradients/rpa/space_time_adjoint.py:84-87``;
 the static screening in ``BSE/solve.py:70``, ``GW/contour_deformation.py:104``,
-``gradients/gwbse/reaction_field_adjoint.py:33``),
+``gradients/gwbse/reaction_field_adjoint.py:33``; the contour's explicit
+residue backend in ``GW/real_screening.py:57`` and
+``GW/contour_deformation.py:96``),
 and its own tests substitute them with ``monkeypatch.setattr(module, name,
 ...)`` (``tests/test_rpa_log_determinant.py:57-72``). `install()` does the
 same for every module that holds one of the names, so every caller --
@@ -31,6 +33,7 @@ QG = 'src.gradients.gwbse.qp_space_time'
 BSE = 'src.SingleReference.BSE.solve'
 CD = 'src.SingleReference.GW.contour_deformation'
 RF = 'src.gradients.gwbse.reaction_field_adjoint'
+RS = 'src.SingleReference.GW.real_screening'
 
 _SAVED: dict = {}
 
@@ -95,7 +98,10 @@ def replacements():
         QG: {'qp_gradient_space_time': contour.qp_gradient_space_time},
         BSE: dict(static),
         CD: {**static,
-             'cd_screening_contraction_multi': contour.cd_screening_contraction_multi},
+             'cd_screening_contraction_multi': contour.cd_screening_contraction_multi,
+             'ExplicitRealScreening': contour.ExplicitRealScreening,
+             'wc_explicit': contour.wc_explicit},
+        RS: {'ExplicitRealScreening': contour.ExplicitRealScreening},
         RF: dict(static),
         ADJ: {'polarizability_backward': adjoint.polarizability_backward,
               'selfenergy_diag_backward': adjoint.selfenergy_diag_backward,

@@ -36,6 +36,10 @@ sweep: the static screening, the frequency-blocked and the unrestricted sweeps,
 the self-energy diagonal with its adjoint (20 states), the contour's
 screening contraction (64 frequencies, 20 states) and one Sigma^c evaluation.
 
+--rows-cd: the contour's explicit particle-hole backend (continuation 'cd') at
+the same size: C_ov, the explicit response at one real frequency and one
+W(freq) - I below and above the particle-hole gap.
+
 --fp64-peak N: the FP64 reference rates of this GPU, timed with CUDA events
 (best of 5 after a warm-up): cuBLAS DGEMM at N^3 and cuSOLVER's Cholesky of
 an N x N SPD matrix (the FP64 factorisation of the Dyson step).
@@ -182,6 +186,46 @@ def rows(a):
                                        proj, cgrid, eps, nocc)))
 
 
+def explicit_rows(a):
+    """Device times of the contour's explicit particle-hole backend
+    (continuation 'cd') at n_orb = 1200, nocc = 120, N_mu = 7200: C_ov
+    (7200 x 129600) from the occupied slices, the explicit response at one
+    real frequency (mbpt_chi0_aux: naux (naux + 1) nov useful flops of a
+    symmetric rank-k product) and one W(freq) - I below and above the gap
+    (the Dyson step: Cholesky below, LU above). One JSON line each."""
+    import json
+    from . import contour, space_time
+    n, nocc, M = 1200, 120, 7200
+    X, D, eps_t = synthetic_system_torch(n, nocc, M, seed=2024, variant='calibrated')
+    eps = eps_t.cpu().numpy()
+
+    def timed(name, fn, flops=None):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        extra = {'tflops': round(flops / t / 1e12, 1)} if flops else {}
+        print(json.dumps({'row': name, 's': round(t, 4), **extra}), flush=True)
+
+    C = contour.three_index_ov(X, D, eps, nocc)
+    timed('cd: C_ov (7200 x 129600) from the 120 occupied slices',
+          lambda: contour.three_index_ov(X, D, eps, nocc))
+    d = contour.ov_energies(eps, nocc)
+    gap = eps[nocc] - eps[nocc - 1]
+    f = space_time.frequency_factor(d, 0.5 * gap, False)
+    out = torch.empty((M, M), dtype=torch.float64, device='cuda')
+    naux, nov = C.shape
+    timed('cd: explicit chi0 at one real frequency (mbpt_chi0_aux, FP64)',
+          lambda: space_time.chi0_aux([(C, f)], 2.0, out=out), flops=naux * (naux + 1) * nov)
+    for label, w in (('below the gap (Cholesky)', 0.5 * gap), ('above the gap (LU)', 1.5 * gap)):
+        timed(f'cd: W(freq) - I {label}, chi0 + Dyson',
+              lambda w=w: contour.ExplicitRealScreening(C, eps, nocc).w_minus_identity(w))
+
+
 def fp64_peak(a):
     n = a.fp64_peak
     g = torch.Generator(device='cuda').manual_seed(4)
@@ -241,12 +285,15 @@ def main():
     p.add_argument('--fp64-peak', type=int, default=0)
     p.add_argument('--qp-mlp', action='store_true')
     p.add_argument('--rows', action='store_true')
+    p.add_argument('--rows-cd', action='store_true')
     a = p.parse_args()
     torch.cuda.set_device(0)
     if a.qp_mlp:
         return qp_mlp_case(a)
     if a.rows:
         return rows(a)
+    if a.rows_cd:
+        return explicit_rows(a)
     if a.fp64_peak:
         return fp64_peak(a)
     if a.dyson:

@@ -258,6 +258,60 @@ def dyson_screening(chi0, transform=None, correlation=False):
     return back(out, chi0)
 
 
+def frequency_factor(d, w, imaginary, eta=0.0, slopes=False):
+    """The bubble's frequency factor for pair energies d at frequency w
+    (``LinearResponse/imaginary_frequency.py:25-59``), host FP64 on nov
+    numbers: -2d/(d^2 + w^2) on the imaginary axis, 1/(w - d) - 1/(w + d) on
+    the real one, a/(a^2 + eta^2) - b/(b^2 + eta^2) broadened (a = w - d,
+    b = w + d). slopes=True returns (f, df/dd, df/dw), df/dw None on the
+    imaginary axis."""
+    d = np.asarray(d, float)
+    if imaginary:
+        den = d ** 2 + w ** 2
+        f = -2.0 * d / den
+        return (f, -2.0 * (w ** 2 - d ** 2) / den ** 2, None) if slopes else f
+    a, b = w - d, w + d
+    if eta == 0.0:
+        f = 1.0 / a - 1.0 / b
+        return (f, 1.0 / a ** 2 + 1.0 / b ** 2, -1.0 / a ** 2 + 1.0 / b ** 2) if slopes else f
+    da, db = a ** 2 + eta ** 2, b ** 2 + eta ** 2
+    f = a / da - b / db
+    if not slopes:
+        return f
+    return (f, -(eta ** 2 - a ** 2) / da ** 2 - (eta ** 2 - b ** 2) / db ** 2,
+            (eta ** 2 - a ** 2) / da ** 2 - (eta ** 2 - b ** 2) / db ** 2)
+
+
+def chi0_aux(blocks, spin_factor=1.0, scratch=None, out=None):
+    """chi0 = spin_factor sum_s (C_s f_s) C_s^T in the auxiliary basis, on the
+    device (``LinearResponse/space_time.py:934-953``): blocks = [(C_ov, f)],
+    C_ov (naux, n_ov) and f its pairs' frequency factor (`frequency_factor`).
+    One mbpt_chi0_aux call per block, accumulating into `out` (a device
+    (naux, naux) tensor, allocated when None), which is returned. scratch is
+    accepted for the reference's signature; the column chunks live in the
+    call's workspace. NumPy factors give a NumPy result unless `out` is
+    given; device factors keep it on the device."""
+    del scratch
+    dev = require_device()
+    blocks = list(blocks)
+    host = out is None and bool(blocks) and not isinstance(blocks[0][0], torch.Tensor)
+    for s, (C, f) in enumerate(blocks):
+        Cd = to_device(C, dev)
+        if Cd.dim() != 2 or Cd.stride(1) != 1:
+            Cd = Cd.contiguous()
+        naux, nov = Cd.shape
+        fd = to_device(np.ascontiguousarray(f, dtype=float), dev)
+        if fd.numel() != nov:
+            raise ValueError(f'chi0_aux: f has {fd.numel()} pairs, C_ov {nov}')
+        if out is None:
+            out = torch.empty((naux, naux), dtype=torch.float64, device=dev)
+        ws = WORKSPACE.get(lib().mbpt_chi0_aux_workspace_bytes(naux, nov), dev)
+        check(lib().mbpt_chi0_aux(ptr(Cd), naux, nov, Cd.stride(0), ptr(fd),
+                                  float(spin_factor), int(s > 0), ptr(out), ptr(ws), ws.numel(),
+                                  stream_ptr()), 'mbpt_chi0_aux')
+    return out.cpu().numpy() if host else out
+
+
 def _one_rank(comm, who):
     if comm is not None and comm.Get_size() > 1:
         raise NotImplementedError(f'{who}: rank splits are outside the one-GPU route')

@@ -755,6 +755,91 @@ def sigma_cd(p, omega, Bp, eps, nocc, nu, nu_w, wc, proj_tau, tau, tau_w):
     return s
 
 
+# the explicit particle-hole backend of continuation 'cd'
+
+def frequency_factor(d, w, imaginary, eta=0.0, slopes=False):
+    """LinearResponse/imaginary_frequency.py:25-59: the bubble's frequency
+    factor for pair energies d at w, (f, df/dd, df/dw) with slopes. Imaginary
+    axis -2d/(d^2 + w^2); real axis 1/(w - d) - 1/(w + d), broadened by eta."""
+    d = np.asarray(d, float)
+    if imaginary:
+        den = d * d + w * w
+        f = -2.0 * d / den
+        return (f, -2.0 * (w * w - d * d) / den ** 2, None) if slopes else f
+    a, b = w - d, w + d
+    if eta == 0.0:
+        f = 1.0 / a - 1.0 / b
+        return (f, 1.0 / a ** 2 + 1.0 / b ** 2, -1.0 / a ** 2 + 1.0 / b ** 2) if slopes else f
+    da, db = a * a + eta * eta, b * b + eta * eta
+    f = a / da - b / db
+    if not slopes:
+        return f
+    return (f, (a * a - eta * eta) / da ** 2 + (b * b - eta * eta) / db ** 2,
+            (eta * eta - a * a) / da ** 2 - (eta * eta - b * b) / db ** 2)
+
+
+def ov_energies(eps, nocc):
+    """Base/orbital_spaces.py:31-34: d[(i, a)] = eps_a - eps_i, i major."""
+    eps = np.asarray(eps, float)
+    return (eps[nocc:][None, :] - eps[:nocc][:, None]).ravel()
+
+
+def three_index_ov(X, D, eps, nocc):
+    """LinearResponse/space_time.py:833-851: C_ov[P, (i, a)] =
+    sum_k D[k, P] X[k, i] X[k, a], (naux, nocc * nvirt)."""
+    Xo, Xv = X[:, :nocc], X[:, nocc:]
+    return D.T @ (Xo[:, :, None] * Xv[:, None, :]).reshape(X.shape[0], -1)
+
+
+def explicit_screening_apply(C_ov, d, freq, b, eta=0.0, imaginary=False):
+    """real_screening.py:84-85 with :171-181: W(freq) b, W = [1 - chi0]^-1,
+    chi0 = 2 (C_ov f) C_ov^T -- by a solve (the reference inverts)."""
+    chi0 = 2.0 * (C_ov * frequency_factor(d, freq, imaginary, eta)) @ C_ov.T
+    return np.linalg.solve(np.eye(len(chi0)) - chi0, b)
+
+
+def explicit_screening_slope(C_ov, d, freq, y, eta=0.0):
+    """real_screening.py:87-91: y^T [dchi0/dfreq] y = 2 sum df/dw (C_ov^T y)^2."""
+    z = C_ov.T @ y
+    return 2.0 * float(frequency_factor(d, freq, False, eta, slopes=True)[2] @ z ** 2)
+
+
+def wc_explicit(Bp, C_ov, d, nu):
+    """contour_deformation.py:240-245: wc[k, q] = B[:, q]^T (W(i nu_k) - I)
+    B[:, q] from the explicit imaginary-axis screening."""
+    out = np.zeros((len(nu), Bp.shape[1]))
+    for k, v in enumerate(nu):
+        out[k] = np.einsum('Pq,Pq->q', Bp, explicit_screening_apply(C_ov, d, v, Bp,
+                                                                    imaginary=True) - Bp)
+    return out
+
+
+def sigma_cd_explicit(p, omega, Bp, eps, nocc, nu, nu_w, wc, C_ov, eta=0.0):
+    """contour_deformation.py:310-343 with the explicit residue backend."""
+    eps = np.asarray(eps, float)
+    d = ov_energies(eps, nocc)
+    c = cd_integral_weights(omega - eps, nu, nu_w)
+    s = -float(np.einsum('kq,kq->', c, wc)) / np.pi
+    for q, weight in residue_set(eps, nocc, omega):
+        b = Bp[:, q]
+        y = explicit_screening_apply(C_ov, d, abs(eps[q] - omega), b, eta)
+        s += weight * (b @ y - b @ b)
+    return s
+
+
+def sigma_cd_slope_explicit(p, omega, Bp, eps, nocc, nu, nu_w, wc, C_ov, eta=0.0):
+    """contour_deformation.py:346-373 with the explicit residue backend."""
+    eps = np.asarray(eps, float)
+    d = ov_energies(eps, nocc)
+    _, dc = cd_integral_weights(omega - eps, nu, nu_w, with_slope=True)
+    slope = -float(np.einsum('kq,kq->', dc, wc)) / np.pi
+    for q, weight in residue_set(eps, nocc, omega):
+        gap = eps[q] - omega
+        y = explicit_screening_apply(C_ov, d, abs(gap), Bp[:, q], eta)
+        slope -= weight * explicit_screening_slope(C_ov, d, abs(gap), y, eta) * np.sign(gap)
+    return slope
+
+
 def self_energy_matrix(X_ao, D, W_omega, mo_coeff, eps, nocc, tau_points, omega_in, omega_out,
                        mu, tau_indices=None):
     """GW/imaginary_time.py:403-533 in one block: the full AO Sigma^c(i w_out),

@@ -33,6 +33,10 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      (residues through the Laplace backend) and the integral
                      weights (the CD module loads pyscf for its driver; a
                      stand-in that raises on use lets it import here);
+* contour_explicit.npz  the explicit particle-hole backend of continuation
+                     'cd': C_ov, W(freq) b and its slope below and above the
+                     gap, the explicit imaginary-axis contraction, Sigma^c
+                     with explicit residues and five states' roots and Z;
 * sigma_ao.npz       the full AO self-energy with an AO collocation that is not
                      the MO one, a subset of its time points, its MO diagonal,
                      and the chi0 sweep's reverse for a seeded proj_bar;
@@ -45,7 +49,7 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      stored: the tests regenerate them from the seed and check
                      the regeneration against the stored eps and checksums.
 
-    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|sigma_ao]
+    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|contour_explicit|sigma_ao]
 """
 import os
 import sys
@@ -426,6 +430,65 @@ def contour_fixture():
         D_bar=np.stack([gr[4] for gr in grads]))
 
 
+def contour_explicit_fixture():
+    """The contour deformation's explicit particle-hole backend (continuation
+    'cd'; GW/real_screening.py:57-91, 171-181; GW/contour_deformation.py:240-245)
+    on the contour fixture's system: C_ov (LinearResponse/space_time.py:833-851),
+    W(freq) b and its slope at real frequencies below and above the gap (with
+    and without broadening), the explicit imaginary-axis contraction wc of
+    three states, Sigma^c with explicit residues around their levels, and the
+    quasiparticle roots and Z of five states from the deepest to the highest
+    (the cubic wc with explicit residues; one state with the explicit wc too)."""
+    cd, rs = _import_contour_deformation()
+    from src.gradients.rpa.space_time_adjoint import polarizability_tau
+    from src.SingleReference.LinearResponse.space_time import (three_index_ov,
+                                                               three_index_slice)
+    from src.Base.orbital_spaces import ov_energies
+    X, D, eps = synthetic_system(16, 3, 48, 31, 'calibrated')
+    nocc = 3
+    mu = particle_hole_window(eps, nocc)[2]
+    gap = particle_hole_window(eps, nocc)[0]
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        nu, nu_w, grid, w0 = cd.cd_frequency_grid(eps, nocc)
+    C_ov = three_index_ov(X, D, eps, nocc)
+    d = ov_energies(eps, nocc)
+    rng = np.random.default_rng(41)
+    b = rng.standard_normal(C_ov.shape[0])
+    freqs = np.array([0.2, 0.8, 1.3, 2.5]) * gap
+    etas = np.array([0.0, 0.01])
+    apply_ = np.zeros((len(etas), len(freqs), len(b)))
+    slope = np.zeros((len(etas), len(freqs)))
+    for a, eta in enumerate(etas):
+        ers = rs.ExplicitRealScreening(C_ov, eps, nocc, eta=float(eta))
+        for j, f in enumerate(freqs):
+            apply_[a, j] = ers.apply(float(f), b)
+            slope[a, j] = ers.slope(float(f), apply_[a, j])
+    proj = polarizability_tau(X, D, eps, nocc, grid, mu=mu)
+    states = np.array([0, nocc - 1, nocc, nocc + 1, len(eps) - 1])
+    Bps = [three_index_slice(X, D, int(p)) for p in states]
+    wcs = cd.cd_screening_contraction_multi(proj, grid.cosft_wt, Bps)
+    near = [1, 2, 3]                      # the three states around the gap
+    wcx = np.stack([cd.wc_explicit(Bps[i], C_ov, d, nu) for i in near])
+    shifts = np.array([-0.06, 0.0, 0.06])
+    sig = np.zeros((len(near), len(shifts)))
+    for r, i in enumerate(near):
+        p = int(states[i])
+        for j, dw in enumerate(shifts):
+            sig[r, j] = cd.sigma_cd(p, eps[p] + dw, Bps[i], eps, nocc, nu, nu_w, wc=wcs[i],
+                                    C_ov=C_ov)
+    roots = np.zeros((len(states), 2))
+    for i, p in enumerate(states):
+        w, z, _ = cd.qp_energy_cd(int(p), Bps[i], eps, nocc, nu, nu_w, wc=wcs[i], C_ov=C_ov)
+        roots[i] = w, z
+    w, z, _ = cd.qp_energy_cd(int(states[2]), Bps[2], eps, nocc, nu, nu_w, C_ov=C_ov)
+    np.savez_compressed(
+        os.path.join(HERE, 'contour_explicit.npz'), X=X, D=D, eps=eps, nocc=nocc, mu=mu, nu=nu,
+        nu_w=nu_w, C_ov=C_ov, b=b, freqs=freqs, etas=etas, apply=apply_, slope=slope,
+        states=states, wc=np.stack(wcs), near=np.array(near), wc_explicit=wcx, shifts=shifts,
+        sigma=sig, roots=roots, root_explicit_wc=np.array([w, z]))
+
+
 def sigma_ao_fixture():
     """The full AO self-energy of GW/imaginary_time.py:403-533 with an AO
     collocation that is not the MO one (X_ao = X_mo C^T, C a seeded orthogonal
@@ -513,9 +576,13 @@ if __name__ == '__main__':
         contour_fixture()
         print('contour-deformation fixture written to', HERE)
         sys.exit(0)
+    if ONLY == 'contour_explicit':
+        contour_explicit_fixture()
+        print('explicit contour backend fixture written to', HERE)
+        sys.exit(0)
     if ONLY:
-        sys.exit(f'--only {ONLY}: choose c1, static, unrestricted, sigma_adjoint, contour or '
-                 'sigma_ao')
+        sys.exit(f'--only {ONLY}: choose c1, static, unrestricted, sigma_adjoint, contour, '
+                 'contour_explicit or sigma_ao')
     grids_fixture()
     shared_kernel_fixture()
     route_fixture('calibrated', 24, 4, 64, 7, 'calibrated', 12, full=True)
@@ -526,5 +593,6 @@ if __name__ == '__main__':
     unrestricted_fixture()
     sigma_adjoint_fixture()
     contour_fixture()
+    contour_explicit_fixture()
     sigma_ao_fixture()
     print('fixtures written to', HERE)

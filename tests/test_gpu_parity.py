@@ -521,13 +521,77 @@ def test_contour_deformation_device_matches_reference_golden(golden):
         assert res == contour.residue_set(eps, nocc, w)
     # the drop-in driver on the same factors (default contour grid): eV roots
     ev, zs, info = contour.solve_qp_energy_contour(eps, None, nocc, g['states'],
-                                                   factors=(X, D))
+                                                   continuation='laplace', factors=(X, D))
     assert np.abs(ev / contour.HARTREE_TO_EV - g['roots'][:, 0]).max() < 1e-9
     assert np.abs(zs - g['roots'][:, 1]).max() < 1e-8
     assert info['continuation'] == 'laplace' and len(info['states']) == 3
     with pytest.raises(NotImplementedError):
-        contour.solve_qp_energy_contour(eps, None, nocc, g['states'], continuation='cd',
+        contour.solve_qp_energy_contour(eps, None, nocc, g['states'], continuation='sop',
                                         factors=(X, D))
+
+
+def test_contour_explicit_backend_matches_reference_golden(golden):
+    """Continuation 'cd' against the reference: C_ov from the occupied
+    states' slices, the explicit response (mbpt_chi0_aux) against its NumPy
+    composition, W(freq) b and its slope below and above the particle-hole
+    gap with and without broadening (the Dyson step's LU above the gap), the
+    explicit imaginary-axis contraction, Sigma^c with explicit residues, the
+    roots and Z of five states from the deepest to the highest (one with the
+    explicit contraction too), and the drop-in driver's default
+    continuation."""
+    from mbptcode_b200 import contour, gw, space_time
+    g = golden('contour_explicit')
+    eps, nocc, X, D = g['eps'], int(g['nocc']), g['X'], g['D']
+    nu, nu_w = g['nu'], g['nu_w']
+    C = contour.three_index_ov(X, D, eps, nocc)
+    assert np.abs(C.cpu().numpy() - g['C_ov']).max() <= 1e-12 * np.abs(g['C_ov']).max()
+    d = contour.ov_energies(eps, nocc)
+    # the response alone, one block and two accumulated blocks (host in, host out)
+    f = space_time.frequency_factor(d, float(g['freqs'][2]), False)
+    ref = 2.0 * (g['C_ov'] * f) @ g['C_ov'].T
+    chi = space_time.chi0_aux([(g['C_ov'], f)], 2.0)
+    assert np.abs(chi - ref).max() <= 1e-13 * np.abs(ref).max()
+    assert np.array_equal(chi, chi.T)
+    chi2 = space_time.chi0_aux([(g['C_ov'][:, :20], f[:20]), (g['C_ov'][:, 20:], f[20:])], 2.0)
+    assert np.abs(chi2 - ref).max() <= 1e-13 * np.abs(ref).max()
+    for a, eta in enumerate(g['etas']):
+        ers = contour.ExplicitRealScreening(C, eps, nocc, eta=float(eta))
+        for j, fr in enumerate(g['freqs']):
+            y = ers.apply(float(fr), g['b'])
+            want = g['apply'][a, j]
+            assert np.abs(y - want).max() <= 1e-10 * np.abs(want).max(), (eta, fr)
+            s = ers.slope(float(fr), y)
+            assert abs(s - g['slope'][a, j]) <= 1e-9 * abs(g['slope'][a, j]), (eta, fr)
+    B = contour.three_index_slices(X, D, g['states'])
+    for r, i in enumerate(g['near']):
+        wcx = contour.wc_explicit(B[i], C, d, nu)
+        assert np.abs(wcx - g['wc_explicit'][r]).max() <= 1e-10 * np.abs(wcx).max()
+        p = int(g['states'][i])
+        for j, dw in enumerate(g['shifts']):
+            s = contour.sigma_cd(p, eps[p] + dw, B[i], eps, nocc, nu, nu_w, wc=g['wc'][i],
+                                 C_ov=C)
+            assert abs(s - g['sigma'][r, j]) <= 1e-9 * abs(g['sigma'][r, j]), (p, dw)
+    for i, p in enumerate(g['states']):
+        w, z, res = contour.qp_energy_cd(int(p), B[i], eps, nocc, nu, nu_w, wc=g['wc'][i],
+                                         C_ov=C)
+        assert abs(w - g['roots'][i, 0]) < 1e-9 and abs(z - g['roots'][i, 1]) < 1e-8, p
+        assert res == contour.residue_set(eps, nocc, w)
+    w, z, _ = contour.qp_energy_cd(int(g['states'][2]), B[2], eps, nocc, nu, nu_w, C_ov=C)
+    assert abs(w - g['root_explicit_wc'][0]) < 1e-9 and abs(z - g['root_explicit_wc'][1]) < 1e-8
+    # the drop-in driver: 'cd' is its default, as in the reference
+    ev, zs, info = contour.solve_qp_energy_contour(eps, None, nocc, g['states'], factors=(X, D))
+    assert np.abs(ev / contour.HARTREE_TO_EV - g['roots'][:, 0]).max() < 1e-9
+    assert np.abs(zs - g['roots'][:, 1]).max() < 1e-8
+    assert info['continuation'] == 'cd' and info['residue_route_taken'] == 'explicit'
+    # and through calc_qp_energy(mode='space-time', continuation='cd')
+    from types import SimpleNamespace
+    occ = np.zeros(len(eps))
+    occ[:nocc] = 2.0
+    e, z = gw.calc_qp_energy(SimpleNamespace(mo_energy=eps, mo_occ=occ), mode='space-time',
+                             continuation='cd', state=[int(p) for p in g['states']],
+                             factors=(X, D), return_z=True)
+    assert np.abs(np.asarray(z) - g['roots'][:, 1]).max() < 1e-8
+    assert np.abs(np.asarray(e) / contour.HARTREE_TO_EV - g['roots'][:, 0]).max() < 1e-9
 
 
 def test_ao_self_energy_and_mirrors_match_reference_golden(golden):

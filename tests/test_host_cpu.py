@@ -114,6 +114,9 @@ def test_plugin_rebinds_and_restores_reference_names():
         # the static screening's other importers need pyscf, absent here
         assert {plugin.BSE, plugin.CD, plugin.RF} <= set(skipped)
         assert 'dyson_screening' in bound[plugin.IT]
+        from mbptcode_b200 import contour
+        rs = importlib.import_module(plugin.RS)
+        assert rs.ExplicitRealScreening is contour.ExplicitRealScreening
         assert plugin.ST in skipped      # MBPTcode's GW module imports pyscf, absent here
         adj = importlib.import_module(plugin.ADJ)
         assert adj.rpa_correlation_energy_space_time is \

@@ -291,6 +291,48 @@ def test_contour_root_finder_on_the_oracle(golden):
         assert abs(w - g['roots'][i, 0]) < 1e-10 and abs(z - g['roots'][i, 1]) < 1e-9, p
 
 
+def test_contour_explicit_backend_oracle(golden):
+    """The oracle's explicit particle-hole backend (continuation 'cd') against
+    the reference: C_ov, W(freq) b and its slope below and above the gap with
+    and without broadening, the explicit imaginary-axis contraction, Sigma^c
+    with explicit residues, and five states' roots and Z through the scan
+    root finder of mbptcode_b200.contour."""
+    from mbptcode_b200 import contour
+    g = golden('contour_explicit')
+    eps, nocc, X, D = g['eps'], int(g['nocc']), g['X'], g['D']
+    C = orc.three_index_ov(X, D, eps, nocc)
+    assert np.abs(C - g['C_ov']).max() <= 1e-13 * np.abs(g['C_ov']).max()
+    d = orc.ov_energies(eps, nocc)
+    for a, eta in enumerate(g['etas']):
+        for j, f in enumerate(g['freqs']):
+            y = orc.explicit_screening_apply(C, d, f, g['b'], eta)
+            ref = g['apply'][a, j]
+            assert np.abs(y - ref).max() <= 1e-11 * np.abs(ref).max(), (eta, f)
+            s = orc.explicit_screening_slope(C, d, f, y, eta)
+            assert abs(s - g['slope'][a, j]) <= 1e-10 * abs(g['slope'][a, j]), (eta, f)
+    B = [orc.three_index_slice(X, D, int(p)) for p in g['states']]
+    for r, i in enumerate(g['near']):
+        wcx = orc.wc_explicit(B[i], C, d, g['nu'])
+        assert np.abs(wcx - g['wc_explicit'][r]).max() <= 1e-11 * np.abs(wcx).max()
+        p = int(g['states'][i])
+        for j, dw in enumerate(g['shifts']):
+            s = orc.sigma_cd_explicit(p, eps[p] + dw, B[i], eps, nocc, g['nu'], g['nu_w'],
+                                      g['wc'][i], C)
+            assert abs(s - g['sigma'][r, j]) <= 1e-11 * abs(g['sigma'][r, j]), (p, dw)
+    for i, p in enumerate(g['states']):
+        p = int(p)
+
+        def residual(w, p=p, i=i):
+            return w - eps[p] - orc.sigma_cd_explicit(p, w, B[i], eps, nocc, g['nu'],
+                                                      g['nu_w'], g['wc'][i], C)
+
+        def fprime(w, p=p, i=i):
+            return 1.0 - orc.sigma_cd_slope_explicit(p, w, B[i], eps, nocc, g['nu'],
+                                                     g['nu_w'], g['wc'][i], C)
+        w, z = contour.solve_qp_equation_scan(residual, fprime, float(eps[p]))
+        assert abs(w - g['roots'][i, 0]) < 1e-10 and abs(z - g['roots'][i, 1]) < 1e-9, p
+
+
 def test_ao_self_energy_oracle(golden):
     """The oracle's full AO self-energy (an AO collocation that is not the MO
     one) and the chi0 sweep's reverse against the reference's."""
