@@ -278,14 +278,17 @@ int mbpt_three_index_slices(const double *X_dev, int64_t M, int64_t norb, const 
 /* The explicit particle-hole response of one block (continuation 'cd'),
  * LinearResponse/space_time.py:934-953 `chi0_aux` as GW/real_screening.py:
  * 171-181 `screening_aux` calls it:
- *   chi0 = spin_factor (C diag(f)) C^T   (+ chi0 when accumulate),
+ *   chi0 = spin_factor (C diag(f)) C^T   (+ chi0 when accumulate, FP64 only),
  * C_dev (naux, nov) row-major with leading dimension ldc, f_dev (nov) the
  * pairs' frequency factor (LinearResponse/imaginary_frequency.py:25-59),
- * chi0_dev (naux, naux), symmetric on return. FP64. */
-size_t mbpt_chi0_aux_workspace_bytes(int64_t naux, int64_t nov);
+ * chi0_dev (naux, naux) FP64, symmetric on return. mode MBPT_MODE_FP64: a
+ * symmetric rank-k DGEMM over column chunks; MBPT_MODE_MIXED: one split
+ * BF16x3 tensor-core product (FP32 accumulation, ~1e-5 relative). */
+size_t mbpt_chi0_aux_workspace_bytes(int64_t naux, int64_t nov, int mode);
 int mbpt_chi0_aux(const double *C_dev, int64_t naux, int64_t nov, int64_t ldc,
-                  const double *f_dev, double spin_factor, int accumulate, double *chi0_dev,
-                  void *workspace, size_t ws_bytes, void *stream);
+                  const double *f_dev, double spin_factor, int accumulate, int mode,
+                  double *chi0_dev, void *workspace, size_t ws_bytes, int *err_dev,
+                  void *stream);
 
 /* The imaginary-axis screening contraction of the contour deformation:
  * wc[k, c] = B[:, c]^T (W - I)_k B[:, c] for W - I (nfreq, naux, naux) from the

@@ -375,11 +375,15 @@ class ExplicitRealScreening:
     1 - chi0 is indefinite), the W - I of the latest frequencies kept for
     later calls. eta broadens the particle-hole poles (off by default).
     pair_energies: the pair index of C_ov when it is not the one (eps, nocc)
-    spans. FP64; O(naux^2 nocc nvirt) per frequency, the route the cubic one
-    is checked against and the only one above the particle-hole gap."""
+    spans. O(naux^2 nocc nvirt) per frequency, the route the cubic one is
+    checked against and the only one above the particle-hole gap. precision
+    'fp64' (default) or 'mixed' (the response as one split BF16x3
+    tensor-core product; the Dyson step stays FP64)."""
 
-    def __init__(self, C_ov, eps, nocc, eta=0.0, pair_energies=None, cache_bytes=4e9):
+    def __init__(self, C_ov, eps, nocc, eta=0.0, pair_energies=None, cache_bytes=4e9,
+                 precision='fp64'):
         self.C_ov = to_device(C_ov, require_device())
+        self.precision = precision
         self.eps = np.asarray(eps, float)
         self.nocc = nocc
         self.eta = float(eta)
@@ -397,7 +401,7 @@ class ExplicitRealScreening:
         w = self._w.get(key)
         if w is None:
             f = frequency_factor(self.d, float(freq), imaginary, self.eta)
-            chi0 = chi0_aux([(self.C_ov, f)], 2.0)[None]
+            chi0 = chi0_aux([(self.C_ov, f)], 2.0, precision=self.precision)[None]
             dyson_batch(chi0, want_w=True, precision='fp64')
             w = self._w[key] = chi0[0]
             if len(self._w) > self._cap:
@@ -728,7 +732,8 @@ HARTREE_TO_EV = 27.211386245988  # MBPTcode constants.py:11 (CODATA 2018)
 
 
 def contour_roots(X, D, eps, nocc, states, ntau=CD_NTAU, nfreq_cd=CD_NFREQ, w0_cd=None,
-                  e_min_below_gap=None, xc_correction=0.0, mu=None, continuation='laplace'):
+                  e_min_below_gap=None, xc_correction=0.0, mu=None, continuation='laplace',
+                  precision='fp64'):
     """(roots in Hartree, Z, per-state records) of the states on one contour
     grid (``contour_deformation.py:558-598, 767-812``): one proj(tau) and one
     W per frequency serve every state's imaginary-axis term, each state's
@@ -736,18 +741,22 @@ def contour_roots(X, D, eps, nocc, states, ntau=CD_NTAU, nfreq_cd=CD_NFREQ, w0_c
     cosh transform of the same proj(tau) (continuation 'laplace', which
     refuses a state whose residues the time grid does not carry) or from the
     explicit particle-hole response of C_ov (continuation 'cd', any state).
-    xc_correction: the static term, one per state or one for all."""
+    xc_correction: the static term, one per state or one for all. precision
+    'mixed' runs the screening contraction and the explicit response as
+    split tensor-core products (the Dyson steps and the Laplace residues stay
+    FP64)."""
     if continuation not in ('laplace', 'cd'):
         raise ValueError(f"continuation={continuation!r}: choose 'cd' or 'laplace'")
     eps = _eps_host(eps)
     states = np.atleast_1d(np.asarray(states, int))
-    explicit = (ExplicitRealScreening(three_index_ov(X, D, eps, nocc), eps, nocc)
+    explicit = (ExplicitRealScreening(three_index_ov(X, D, eps, nocc), eps, nocc,
+                                      precision=precision)
                 if continuation == 'cd' else None)
     nu, nu_w, grid, w0 = cd_frequency_grid(eps, nocc, ntau=ntau, nfreq_cd=nfreq_cd,
                                            w0_cd=w0_cd, e_min_below_gap=e_min_below_gap)
     proj = polarizability_tau(X, D, eps, nocc, grid, mu=mu)
     B = three_index_slices(X, D, states)
-    wcs = cd_screening_contraction_multi(proj, grid.cosft_wt, list(B))
+    wcs = cd_screening_contraction_multi(proj, grid.cosft_wt, list(B), precision=precision)
     if explicit is None:
         backend = LaplaceRealScreening(proj, grid, eps, nocc)
     else:
@@ -782,7 +791,8 @@ def contour_roots(X, D, eps, nocc, states, ntau=CD_NTAU, nfreq_cd=CD_NFREQ, w0_c
 def solve_qp_energy_contour(mf, mol, nocc, states, continuation='cd', numerics=None,
                             w0_cd=None, auxbasis=None, radii=None, counts=None, factors=None,
                             grid_accuracy=None, sigma_x='mf', dm_correction=None,
-                            eps_anchor=None, spin_channel='alpha', xc_diagonal=None):
+                            eps_anchor=None, spin_channel='alpha', xc_diagonal=None,
+                            precision='fp64'):
     """Drop-in for ``GW/contour_deformation.py:601-820`` on a restricted
     gas-phase reference with pre-built factors: (quasiparticle energies in eV,
     pole strengths, diagnostics). The mean field gives eps (mo_energy); the
@@ -793,7 +803,8 @@ def solve_qp_energy_contour(mf, mol, nocc, states, continuation='cd', numerics=N
     exact for any state; 'laplace' solves the same contour from the cubic
     cosh transform wherever the time grid carries the residue frequencies,
     and refuses a state by name otherwise, as the reference does. 'sop' (the
-    pole model) is outside the device route and refused."""
+    pole model) is outside the device route and refused. precision: as
+    `contour_roots`."""
     if continuation not in ('cd', 'laplace'):
         raise NotImplementedError(f"continuation={continuation!r}: the device route runs "
                                   "'cd' (explicit residues) and 'laplace' (cubic residues)")
@@ -815,7 +826,8 @@ def solve_qp_energy_contour(mf, mol, nocc, states, continuation='cd', numerics=N
         xc = xc + (np.asarray(eps_anchor, float)[states] - eps[states])
     X, D = (factors['X_mo'], factors['D']) if isinstance(factors, dict) else factors[:2]
     roots, zs, info = contour_roots(X, D, eps, nocc, states, ntau=ntau, nfreq_cd=nfreq,
-                                    w0_cd=w0_cd, xc_correction=xc, continuation=continuation)
+                                    w0_cd=w0_cd, xc_correction=xc, continuation=continuation,
+                                    precision=precision)
     return roots * HARTREE_TO_EV, zs, info
 
 

@@ -1424,24 +1424,53 @@ int mbpt_three_index_slices(const double *X, int64_t M, int64_t norb, const doub
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 
-// The explicit particle-hole response chi0 = s (C f) C^T: columns of C in
-// chunks of kChi0AuxChunk, each chunk scaled into the workspace and folded in
-// by a symmetric rank-k product (one triangle), the other triangle mirrored.
+// The explicit particle-hole response chi0 = s (C f) C^T. FP64: columns of C
+// in chunks of kChi0AuxChunk, each chunk scaled into the workspace and folded
+// in by a symmetric rank-k product (one triangle), the other triangle
+// mirrored. Mixed: C f and C as zero-padded BF16 pairs, one split product
+// over the whole K on the engine's upper 128 x 256 tiles, stored as FP64 and
+// mirrored by its epilogue.
 constexpr int64_t kChi0AuxChunk = 4096;
 
-size_t mbpt_chi0_aux_workspace_bytes(int64_t naux, int64_t nov) {
+size_t mbpt_chi0_aux_workspace_bytes(int64_t naux, int64_t nov, int mode) {
   if (naux < 1 || nov < 1) return 0;
+  if (mode == MBPT_MODE_MIXED)
+    return 4 * sizeof(bf16) * static_cast<size_t>(round_up(naux, 128)) * round_up(nov, 64) +
+           4096;
   return sizeof(double) * static_cast<size_t>(naux) * std::min(nov, kChi0AuxChunk) + 2048;
 }
 
 int mbpt_chi0_aux(const double *C, int64_t naux, int64_t nov, int64_t ldc, const double *f,
-                  double spin_factor, int accumulate, double *chi0, void *ws, size_t ws_bytes,
-                  void *stream) {
+                  double spin_factor, int accumulate, int mode, double *chi0, void *ws,
+                  size_t ws_bytes, int *err, void *stream) {
   if (naux < 1 || nov < 1 || ldc < nov || naux > INT32_MAX || ldc > INT32_MAX)
     return MBPT_ERR_SHAPE;
+  if (mode != MBPT_MODE_FP64 && mode != MBPT_MODE_MIXED) return MBPT_ERR_UNSUPPORTED;
   cudaStream_t st = S(stream);
-  const int64_t chunk = std::min(nov, kChi0AuxChunk);
   Arena ar = arena(ws, ws_bytes);
+  if (mode == MBPT_MODE_MIXED) {
+    // the epilogue stores, it does not add
+    if (accumulate) return MBPT_ERR_UNSUPPORTED;
+    const int64_t mp = round_up(naux, 128), kp = round_up(nov, 64);
+    bf16 *a_hi = ar.take<bf16>(mp * kp), *a_lo = ar.take<bf16>(mp * kp);
+    bf16 *b_hi = ar.take<bf16>(mp * kp), *b_lo = ar.take<bf16>(mp * kp);
+    if (ar.overflow()) return MBPT_ERR_WORKSPACE;
+    launch_split_pad_colscale(C, naux, nov, ldc, f, spin_factor, a_hi, a_lo, kp, mp, kp, st);
+    launch_split_pad<double>(C, naux, nov, ldc, 1.f, b_hi, b_lo, kp, mp, kp, false, st);
+    SplitMat A{a_hi, a_lo, mp, kp, kp, false};
+    SplitMat B{b_hi, b_lo, mp, kp, kp, false};
+    umma::EpiArgs e;
+    e.outd = chi0;
+    e.ld_outd = naux;
+    e.nd = static_cast<int>(naux);
+    e.shift = 0.0;
+    e.alpha = 1.f;
+    const int rc = gemm_split(umma::EPI_F64_SYM, 1, &A, &B, mp, mp, e, err, st,
+                              umma::BAND_UPPER);
+    if (rc) return rc;
+    return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+  }
+  const int64_t chunk = std::min(nov, kChi0AuxChunk);
   double *T = ar.take<double>(naux * chunk);
   if (ar.overflow()) return MBPT_ERR_WORKSPACE;
   cublasHandle_t h = handles(st).blas;

@@ -295,6 +295,8 @@ int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t 
       return launch<1, 256, EPI_F32, false, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
     if (!tf && nacc == 3 && epi == EPI_SIGMA_H)
       return launch<3, 128, EPI_SIGMA_H, false, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
+    if (!tf && nacc == 1 && epi == EPI_F64_SYM)
+      return launch<1, 256, EPI_F64_SYM, false, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
     return MBPT_ERR_UNSUPPORTED;
   }
   if (band) {

@@ -79,6 +79,9 @@ void launch_prep_branches_tf32(const double *X, int64_t M, int64_t n, int64_t no
                                const double *eps, double mu, double tau, float *o_hi,
                                float *o_lo, int64_t ld_o, float *v_hi, float *v_lo,
                                int64_t ld_v, int64_t Mp, cudaStream_t st);
+void launch_split_pad_colscale(const double *src, int64_t rows, int64_t cols, int64_t ld_src,
+                               const double *f, double s, bf16 *hi, bf16 *lo, int64_t ld_dst,
+                               int64_t rows_p, int64_t cols_p, cudaStream_t st);
 void launch_split_pad_tf32(const double *src, int64_t rows, int64_t cols, int64_t ld_src,
                            float *hi, float *lo, int64_t ld_dst, int64_t rows_p, int64_t cols_p,
                            cudaStream_t st);

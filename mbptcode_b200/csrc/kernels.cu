@@ -37,6 +37,27 @@ __global__ void split_pad_kernel(const T *__restrict__ src, int64_t rows, int64_
   }
 }
 
+// hi/lo[r, c] = the BF16 pair of s (src[r, c] f[c]), zero-padded to rows_p x
+// cols_p: the explicit response's particle-hole columns scaled by their
+// frequency factor on the way into the split engine
+__global__ void split_pad_colscale_kernel(const double *__restrict__ src, int64_t rows,
+                                          int64_t cols, int64_t ld_src,
+                                          const double *__restrict__ f, double s,
+                                          bf16 *__restrict__ hi, bf16 *__restrict__ lo,
+                                          int64_t ld_dst, int64_t rows_p, int64_t cols_p) {
+  const int64_t n = rows_p * cols_p;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t r = i / cols_p, c = i % cols_p;
+    float x = 0.f;
+    if (r < rows && c < cols) x = static_cast<float>(s * (src[r * ld_src + c] * f[c]));
+    bf16 h, l;
+    split_bf16(x, h, l);
+    hi[r * ld_dst + c] = h;
+    lo[r * ld_dst + c] = l;
+  }
+}
+
 // dst[c][r] = src[r][c] through a 32 x 33 shared tile
 template <typename T>
 __global__ void split_pad_transpose_kernel(const T *__restrict__ src, int64_t rows,
@@ -425,6 +446,14 @@ template void launch_split_pad<double>(const double *, int64_t, int64_t, int64_t
                                        bf16 *, int64_t, int64_t, int64_t, bool, cudaStream_t);
 template void launch_split_pad<float>(const float *, int64_t, int64_t, int64_t, float, bf16 *,
                                       bf16 *, int64_t, int64_t, int64_t, bool, cudaStream_t);
+
+void launch_split_pad_colscale(const double *src, int64_t rows, int64_t cols, int64_t ld_src,
+                               const double *f, double s, bf16 *hi, bf16 *lo, int64_t ld_dst,
+                               int64_t rows_p, int64_t cols_p, cudaStream_t st) {
+  count_launch();
+  split_pad_colscale_kernel<<<grid_cap(rows_p * cols_p), kThreads, 0, st>>>(
+      src, rows, cols, ld_src, f, s, hi, lo, ld_dst, rows_p, cols_p);
+}
 
 void launch_prep_branches(const double *X, int64_t M, int64_t n, int64_t nocc,
                           const double *eps, double mu, double tau, bf16 *o_hi, bf16 *o_lo,

@@ -221,9 +221,20 @@ def explicit_rows(a):
     naux, nov = C.shape
     timed('cd: explicit chi0 at one real frequency (mbpt_chi0_aux, FP64)',
           lambda: space_time.chi0_aux([(C, f)], 2.0, out=out), flops=naux * (naux + 1) * nov)
-    for label, w in (('below the gap (Cholesky)', 0.5 * gap), ('above the gap (LU)', 1.5 * gap)):
-        timed(f'cd: W(freq) - I {label}, chi0 + Dyson',
-              lambda w=w: contour.ExplicitRealScreening(C, eps, nocc).w_minus_identity(w))
+    ref = out.clone()
+    timed('cd: the same as one split BF16x3 product (mixed; TFLOP/s of the FP64-equivalent '
+          'useful flops)',
+          lambda: space_time.chi0_aux([(C, f)], 2.0, out=out, precision='mixed'),
+          flops=naux * (naux + 1) * nov)
+    print(json.dumps({'row': 'cd: mixed explicit chi0, max |error| / max |chi0|',
+                      'rel': float((out - ref).abs().max() / ref.abs().max())}), flush=True)
+    del ref
+    for prec in ('fp64', 'mixed'):
+        for label, w in (('below the gap (Cholesky)', 0.5 * gap),
+                         ('above the gap (LU)', 1.5 * gap)):
+            timed(f'cd: W(freq) - I {label}, chi0 + Dyson, {prec}',
+                  lambda w=w, prec=prec: contour.ExplicitRealScreening(
+                      C, eps, nocc, precision=prec).w_minus_identity(w))
 
 
 def fp64_peak(a):

@@ -282,33 +282,40 @@ def frequency_factor(d, w, imaginary, eta=0.0, slopes=False):
             (eta ** 2 - a ** 2) / da ** 2 - (eta ** 2 - b ** 2) / db ** 2)
 
 
-def chi0_aux(blocks, spin_factor=1.0, scratch=None, out=None):
+def chi0_aux(blocks, spin_factor=1.0, scratch=None, out=None, precision='fp64'):
     """chi0 = spin_factor sum_s (C_s f_s) C_s^T in the auxiliary basis, on the
     device (``LinearResponse/space_time.py:934-953``): blocks = [(C_ov, f)],
     C_ov (naux, n_ov) and f its pairs' frequency factor (`frequency_factor`).
     One mbpt_chi0_aux call per block, accumulating into `out` (a device
-    (naux, naux) tensor, allocated when None), which is returned. scratch is
-    accepted for the reference's signature; the column chunks live in the
-    call's workspace. NumPy factors give a NumPy result unless `out` is
-    given; device factors keep it on the device."""
+    (naux, naux) FP64 tensor, allocated when None), which is returned.
+    precision 'fp64' (default: a symmetric rank-k DGEMM over column chunks)
+    or 'mixed' (one split BF16x3 tensor-core product per block, ~1e-5
+    relative; one block only). scratch is accepted for the reference's
+    signature; the chunks live in the call's workspace. NumPy factors give
+    a NumPy result unless `out` is given; device factors keep it on the
+    device."""
     del scratch
     dev = require_device()
+    mode = _mode(precision)
     blocks = list(blocks)
+    if mode == MODES['mixed'] and len(blocks) > 1:
+        raise ValueError("chi0_aux: precision='mixed' takes one block (stack the pairs)")
     host = out is None and bool(blocks) and not isinstance(blocks[0][0], torch.Tensor)
+    err = _Err(dev)
     for s, (C, f) in enumerate(blocks):
         Cd = to_device(C, dev)
-        if Cd.dim() != 2 or Cd.stride(1) != 1:
-            Cd = Cd.contiguous()
         naux, nov = Cd.shape
         fd = to_device(np.ascontiguousarray(f, dtype=float), dev)
         if fd.numel() != nov:
             raise ValueError(f'chi0_aux: f has {fd.numel()} pairs, C_ov {nov}')
         if out is None:
             out = torch.empty((naux, naux), dtype=torch.float64, device=dev)
-        ws = WORKSPACE.get(lib().mbpt_chi0_aux_workspace_bytes(naux, nov), dev)
+        ws = WORKSPACE.get(lib().mbpt_chi0_aux_workspace_bytes(naux, nov, mode), dev)
         check(lib().mbpt_chi0_aux(ptr(Cd), naux, nov, Cd.stride(0), ptr(fd),
-                                  float(spin_factor), int(s > 0), ptr(out), ptr(ws), ws.numel(),
-                                  stream_ptr()), 'mbpt_chi0_aux')
+                                  float(spin_factor), int(s > 0), mode, ptr(out), ptr(ws),
+                                  ws.numel(), ptr(err.t), stream_ptr()), 'mbpt_chi0_aux')
+    if mode == MODES['mixed']:
+        err.check('mbpt_chi0_aux')
     return out.cpu().numpy() if host else out
 
 

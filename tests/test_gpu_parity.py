@@ -554,6 +554,10 @@ def test_contour_explicit_backend_matches_reference_golden(golden):
     assert np.array_equal(chi, chi.T)
     chi2 = space_time.chi0_aux([(g['C_ov'][:, :20], f[:20]), (g['C_ov'][:, 20:], f[20:])], 2.0)
     assert np.abs(chi2 - ref).max() <= 1e-13 * np.abs(ref).max()
+    # mixed: one split BF16x3 tensor-core product (FP32 accumulation)
+    chim = space_time.chi0_aux([(g['C_ov'], f)], 2.0, precision='mixed')
+    err_m = np.abs(chim - ref).max() / np.abs(ref).max()
+    assert err_m <= 5e-5, err_m
     for a, eta in enumerate(g['etas']):
         ers = contour.ExplicitRealScreening(C, eps, nocc, eta=float(eta))
         for j, fr in enumerate(g['freqs']):
@@ -583,6 +587,13 @@ def test_contour_explicit_backend_matches_reference_golden(golden):
     assert np.abs(ev / contour.HARTREE_TO_EV - g['roots'][:, 0]).max() < 1e-9
     assert np.abs(zs - g['roots'][:, 1]).max() < 1e-8
     assert info['continuation'] == 'cd' and info['residue_route_taken'] == 'explicit'
+    # the mixed route: the screening contraction and the explicit response as
+    # split products, the Dyson steps FP64 -- within 1e-5 Ha (0.27 meV) of the
+    # reference's roots
+    r_m, z_m, _ = contour.contour_roots(X, D, eps, nocc, g['states'], continuation='cd',
+                                        precision='mixed')
+    dr = np.abs(r_m - g['roots'][:, 0]).max()
+    assert dr < 1e-5 and np.abs(z_m - g['roots'][:, 1]).max() < 1e-4, (dr, z_m)
     # and through calc_qp_energy(mode='space-time', continuation='cd')
     from types import SimpleNamespace
     occ = np.zeros(len(eps))
