@@ -79,12 +79,21 @@ def gap_scaled_w0(eps, nocc, scale=0.5):
     return w0
 
 
-def cd_grid_range(eps, nocc, e_min_below_gap=None):
+def cd_grid_range(eps, nocc, e_min_below_gap=None, pair_energies=None):
     """(e_min, e_max) of the contour's time grid: e_min reaches below the gap,
-    by default by half of it (``contour_deformation.py:439-468``)."""
-    eps = np.asarray(eps, float)
-    gap, e_max, _ = particle_hole_window(eps, nocc)
-    shift = gap_scaled_w0(eps, nocc) if e_min_below_gap is None else float(e_min_below_gap)
+    by default by half of it (``contour_deformation.py:439-468``).
+    pair_energies: the screening's particle-hole energies when they are not
+    the ones (eps, nocc) spans (both spins of an unrestricted reference): the
+    range and the default shift then follow them."""
+    if pair_energies is not None:
+        d = np.asarray(pair_energies, float)
+        gap, e_max = float(d.min()), float(d.max())
+        shift = 0.5 * gap if e_min_below_gap is None else float(e_min_below_gap)
+    else:
+        eps = np.asarray(eps, float)
+        gap, e_max, _ = particle_hole_window(eps, nocc)
+        shift = (gap_scaled_w0(eps, nocc) if e_min_below_gap is None
+                 else float(e_min_below_gap))
     if gap - shift <= 0:
         raise ValueError(f'e_min_below_gap {shift} exceeds the gap {gap:.4f}: the imaginary-'
                          f'time grid would be asked to represent e^{{-y tau}} at y <= 0')
@@ -92,12 +101,18 @@ def cd_grid_range(eps, nocc, e_min_below_gap=None):
 
 
 def cd_frequency_grid(eps, nocc, ntau=CD_NTAU, nfreq_cd=CD_NFREQ, w0_cd=None,
-                      e_min_below_gap=None):
+                      e_min_below_gap=None, pair_energies=None):
     """(nu, nu_weights, grid, w0): Gauss-Legendre nu on w0 (half the gap by
-    default) and the minimax time grid over `cd_grid_range` onto it, cosine
-    tau -> omega weights only (``contour_deformation.py:471-503``)."""
-    e_min, e_max = cd_grid_range(eps, nocc, e_min_below_gap)
-    w0 = float(w0_cd) if w0_cd is not None else gap_scaled_w0(eps, nocc)
+    default; half the smallest pair energy with pair_energies) and the
+    minimax time grid over `cd_grid_range` onto it, cosine tau -> omega
+    weights only (``contour_deformation.py:471-503``)."""
+    e_min, e_max = cd_grid_range(eps, nocc, e_min_below_gap, pair_energies)
+    if w0_cd is not None:
+        w0 = float(w0_cd)
+    elif pair_energies is not None:
+        w0 = 0.5 * float(np.min(pair_energies))
+    else:
+        w0 = gap_scaled_w0(eps, nocc)
     nu, nu_weights = gauss_legendre_grid(int(nfreq_cd), w0=w0)
     grid = TimeFrequencyGrid.minimax_split(int(ntau), e_min, e_max, nu, nu_weights,
                                            with_sine=False, with_inverse=False)
@@ -161,12 +176,14 @@ def real_frequency_weights(grid, omega):
     return w * np.cosh(omega * t), w * t * np.sinh(omega * t)
 
 
-def laplace_representation_error(grid, eps, nocc, freq):
+def laplace_representation_error(grid, eps, nocc, freq, pair_energies=None):
     """max over y = d -+ freq of |y sum_k w_k e^{-y tau_k} - 1| on the pair
-    energies d, inf where freq reaches the gap
-    (``LinearResponse/space_time.py:908-931``)."""
-    eps = np.asarray(eps, float)
-    d = (eps[nocc:][None, :] - eps[:nocc][:, None]).ravel()
+    energies d (those of (eps, nocc), or pair_energies), inf where freq
+    reaches the gap (``LinearResponse/space_time.py:908-931``)."""
+    if pair_energies is None:
+        d = ov_energies(eps, nocc)
+    else:
+        d = np.asarray(pair_energies, float)
     y = np.concatenate([d - freq, d + freq])
     if y.min() <= 0.0:
         return np.inf
@@ -273,15 +290,20 @@ class LaplaceRealScreening:
     """W at a real frequency below the particle-hole gap from proj(tau): one
     (ntau, naux^2) transform and one Dyson step per frequency, the W - I of
     each frequency kept for later calls (``real_screening.py:94-154``).
-    Refuses (ResidueRefused) a frequency the grid does not carry."""
+    Refuses (ResidueRefused) a frequency the grid does not carry.
+    pair_energies: the particle-hole energies proj(tau) was summed over, when
+    they are not the ones (eps, nocc) spans (both spins of an unrestricted
+    reference)."""
 
     def __init__(self, proj_tau, grid, eps, nocc, tol=LAPLACE_SCREENING_TOL,
-                 cache_bytes=4e9):
+                 pair_energies=None, cache_bytes=4e9):
         self.proj_tau = to_device(proj_tau, require_device())
         self.grid = grid
         self.eps = np.asarray(eps, float)
         self.nocc = nocc
         self.tol = tol
+        self.pair_energies = (None if pair_energies is None
+                              else np.asarray(pair_energies, float))
         # the latest frequencies' W - I (the value and the slope of one point
         # apply W at the same frequencies), bounded by memory
         naux = self.proj_tau.shape[-1]
@@ -289,12 +311,14 @@ class LaplaceRealScreening:
         self._w = OrderedDict()
 
     def representation_error(self, freq):
-        return laplace_representation_error(self.grid, self.eps, self.nocc, freq)
+        return laplace_representation_error(self.grid, self.eps, self.nocc, freq,
+                                            pair_energies=self.pair_energies)
 
     def _weights(self, freq):
         err = self.representation_error(freq)
         if not err < self.tol:
-            gap = particle_hole_window(self.eps, self.nocc)[0]
+            gap = (particle_hole_window(self.eps, self.nocc)[0] if self.pair_energies is None
+                   else float(self.pair_energies.min()))
             raise ResidueRefused(
                 f'real frequency {freq:.4f} Ha is not carried by the tau grid: bare-quadrature '
                 f'error {err:.1e} against tol {self.tol:.0e}; gap - freq = {gap - freq:.4f} '
@@ -731,6 +755,36 @@ def qp_energy_cd(p, Bp, eps, nocc, nu_points, nu_weights, xc_correction=0.0, tol
 HARTREE_TO_EV = 27.211386245988  # MBPTcode constants.py:11 (CODATA 2018)
 
 
+def _roots_on_contour(continuation, states, B, wcs, eps, nocc, nu, nu_w, xc_correction,
+                      backend, w0, ntau, nfreq_cd):
+    """Each state's root and Z by `qp_energy_cd` on one contour grid, with
+    the per-state records (``contour_deformation.py:558-598``)."""
+    explicit = continuation == 'cd'
+    roots, zs, records = np.zeros(len(states)), np.zeros(len(states)), []
+    for i, p in enumerate(states):
+        xc = (float(np.asarray(xc_correction).ravel()[i]) if np.ndim(xc_correction)
+              else float(xc_correction))
+        try:
+            w, z, res = qp_energy_cd(int(p), B[i], eps, nocc, nu, nu_w, xc_correction=xc,
+                                     wc=wcs[i], real_screening=backend)
+        except ResidueRefused as refusal:
+            if explicit:
+                raise
+            raise ResidueRefused(
+                f"continuation='laplace' cannot serve orbital {int(p)}: its contour sweeps "
+                f'a residue the imaginary-time grid does not represent. {refusal}') from refusal
+        roots[i], zs[i] = w, z
+        error = None
+        if not explicit and res:
+            error = max(backend.representation_error(abs(eps[q] - w)) for q, _ in res)
+        records.append({'state': int(p), 'residues': len(res),
+                        'representation_error': error})
+    info = {'continuation': continuation, 'ntau': int(ntau), 'nfreq_cd': int(nfreq_cd),
+            'w0_cd': float(w0), 'residue_route_taken': 'explicit' if explicit else 'laplace',
+            'states': records}
+    return roots, zs, info
+
+
 def contour_roots(X, D, eps, nocc, states, ntau=CD_NTAU, nfreq_cd=CD_NFREQ, w0_cd=None,
                   e_min_below_gap=None, xc_correction=0.0, mu=None, continuation='laplace',
                   precision='fp64'):
@@ -757,35 +811,50 @@ def contour_roots(X, D, eps, nocc, states, ntau=CD_NTAU, nfreq_cd=CD_NFREQ, w0_c
     proj = polarizability_tau(X, D, eps, nocc, grid, mu=mu)
     B = three_index_slices(X, D, states)
     wcs = cd_screening_contraction_multi(proj, grid.cosft_wt, list(B), precision=precision)
-    if explicit is None:
-        backend = LaplaceRealScreening(proj, grid, eps, nocc)
-    else:
-        backend = explicit
-        del proj
-    roots, zs, records = np.zeros(len(states)), np.zeros(len(states)), []
-    for i, p in enumerate(states):
-        xc = (float(np.asarray(xc_correction).ravel()[i]) if np.ndim(xc_correction)
-              else float(xc_correction))
-        try:
-            w, z, res = qp_energy_cd(int(p), B[i], eps, nocc, nu, nu_w, xc_correction=xc,
-                                     wc=wcs[i], real_screening=backend)
-        except ResidueRefused as refusal:
-            if explicit is not None:
-                raise
-            raise ResidueRefused(
-                f"continuation='laplace' cannot serve orbital {int(p)}: its contour sweeps "
-                f'a residue the imaginary-time grid does not represent. {refusal}') from refusal
-        roots[i], zs[i] = w, z
-        error = None
-        if explicit is None and res:
-            error = max(backend.representation_error(abs(eps[q] - w)) for q, _ in res)
-        records.append({'state': int(p), 'residues': len(res),
-                        'representation_error': error})
-    info = {'continuation': continuation, 'ntau': int(ntau), 'nfreq_cd': int(nfreq_cd),
-            'w0_cd': float(w0),
-            'residue_route_taken': 'explicit' if explicit is not None else 'laplace',
-            'states': records}
-    return roots, zs, info
+    backend = LaplaceRealScreening(proj, grid, eps, nocc) if explicit is None else explicit
+    del proj
+    return _roots_on_contour(continuation, states, B, wcs, eps, nocc, nu, nu_w, xc_correction,
+                             backend, w0, ntau, nfreq_cd)
+
+
+def contour_roots_unrestricted(X_mos, D, spectra, noccs, spin, states, ntau=CD_NTAU,
+                               nfreq_cd=CD_NFREQ, w0_cd=None, e_min_below_gap=None,
+                               xc_correction=0.0, continuation='laplace', precision='fp64'):
+    """`contour_roots` for one spin channel of an unrestricted reference
+    (``contour_deformation.py:686-812``): both spins' pair energies side by
+    side set the contour grid, proj(tau) is the spin sum (half of each spin's
+    restricted sweep at its own mid-gap), the channel's slices and contraction
+    read it, and the residues come from its cosh transform on those pair
+    energies ('laplace') or from both spins' C_ov side by side at 1/sqrt(2),
+    so that the restricted factor 2 counts every pair once ('cd'). spin: 0
+    (alpha) or 1 (beta); states are the channel's orbitals."""
+    if continuation not in ('laplace', 'cd'):
+        raise ValueError(f"continuation={continuation!r}: choose 'cd' or 'laplace'")
+    if len(X_mos) != 2 or len(spectra) != 2 or len(noccs) != 2 or spin not in (0, 1):
+        raise ValueError('an unrestricted contour takes two spin channels and spin 0 or 1')
+    from .space_time import spin_summed
+    spectra = [_eps_host(e) for e in spectra]
+    noccs = [int(n) for n in noccs]
+    pairs = np.concatenate([ov_energies(e, n) for e, n in zip(spectra, noccs)])
+    eps, nocc = spectra[spin], noccs[spin]
+    states = np.atleast_1d(np.asarray(states, int))
+    explicit = None
+    if continuation == 'cd':
+        C = torch.cat([three_index_ov(X, D, e, n) for X, e, n in zip(X_mos, spectra, noccs)],
+                      dim=1)
+        C.mul_(1.0 / np.sqrt(2.0))
+        explicit = ExplicitRealScreening(C, eps, nocc, pair_energies=pairs, precision=precision)
+    nu, nu_w, grid, w0 = cd_frequency_grid(eps, nocc, ntau=ntau, nfreq_cd=nfreq_cd,
+                                           w0_cd=w0_cd, e_min_below_gap=e_min_below_gap,
+                                           pair_energies=pairs)
+    proj = spin_summed(polarizability_tau, X_mos, D, spectra, noccs, grid)
+    B = three_index_slices(X_mos[spin], D, states)
+    wcs = cd_screening_contraction_multi(proj, grid.cosft_wt, list(B), precision=precision)
+    backend = (LaplaceRealScreening(proj, grid, eps, nocc, pair_energies=pairs)
+               if explicit is None else explicit)
+    del proj
+    return _roots_on_contour(continuation, states, B, wcs, eps, nocc, nu, nu_w, xc_correction,
+                             backend, w0, ntau, nfreq_cd)
 
 
 def solve_qp_energy_contour(mf, mol, nocc, states, continuation='cd', numerics=None,
@@ -793,11 +862,14 @@ def solve_qp_energy_contour(mf, mol, nocc, states, continuation='cd', numerics=N
                             grid_accuracy=None, sigma_x='mf', dm_correction=None,
                             eps_anchor=None, spin_channel='alpha', xc_diagonal=None,
                             precision='fp64'):
-    """Drop-in for ``GW/contour_deformation.py:601-820`` on a restricted
-    gas-phase reference with pre-built factors: (quasiparticle energies in eV,
-    pole strengths, diagnostics). The mean field gives eps (mo_energy); the
+    """Drop-in for ``GW/contour_deformation.py:601-820`` on a gas-phase
+    reference with pre-built factors: (quasiparticle energies in eV, pole
+    strengths, diagnostics). The mean field gives eps (mo_energy); the
     static term <Sigma_x - v_xc> is `xc_diagonal` (zero on a Hartree-Fock
     reference); numerics.quadrature: ntau_cd and nfreq_cd where it has them.
+    An unrestricted mean field (mo_energy (2, nmo), nocc (nalpha, nbeta),
+    mo_coeff per spin) solves `spin_channel` by `contour_roots_unrestricted`
+    from the factors' AO collocation, (X_mo, D, X_ao[, coords]).
     'cd' (the default, as in the reference) reads the residues' W from the
     explicit particle-hole response of C_ov, O(N^4) per residue frequency and
     exact for any state; 'laplace' solves the same contour from the cubic
@@ -812,9 +884,6 @@ def solve_qp_energy_contour(mf, mol, nocc, states, continuation='cd', numerics=N
         raise NotImplementedError('building the ISDF factors needs pyscf (integrals and the '
                                   'fit); pass factors=(X_mo, D)')
     eps = np.asarray(getattr(mf, 'mo_energy', mf), float)
-    if eps.ndim != 1:
-        raise NotImplementedError('an unrestricted reference is outside the contour route '
-                                  'on the device')
     ntau, nfreq = CD_NTAU, CD_NFREQ
     if numerics is not None:
         q = numerics.quadrature
@@ -822,9 +891,33 @@ def solve_qp_energy_contour(mf, mol, nocc, states, continuation='cd', numerics=N
         nfreq = getattr(q, 'nfreq_cd', nfreq)
     states = np.atleast_1d(np.asarray(states, int))
     xc = 0.0 if xc_diagonal is None else np.asarray(xc_diagonal, float)
+    X, D = (factors['X_mo'], factors['D']) if isinstance(factors, dict) else factors[:2]
+    if eps.ndim == 2:
+        if spin_channel not in ('alpha', 'beta'):
+            raise ValueError(f"spin_channel must be 'alpha' or 'beta', got {spin_channel!r}")
+        spin = 0 if spin_channel == 'alpha' else 1
+        X_ao = factors.get('X_ao') if isinstance(factors, dict) else (
+            tuple(factors) + (None,) * 4)[2]
+        if X_ao is None:
+            raise ValueError(
+                'an unrestricted reference needs the AO collocation of the factors, '
+                '(X_mo, D, X_ao[, coords]): each spin projects it on its own orbitals')
+        dev = require_device()
+        Xa = to_device(X_ao, dev)
+        X_mos = [Xa @ to_device(c, dev) for c in mf.mo_coeff]
+        if eps_anchor is not None:
+            anchor = np.asarray(eps_anchor, float)
+            if anchor.shape != eps.shape:
+                raise ValueError(f'an unrestricted eps_anchor is one spectrum per spin, shape '
+                                 f'{eps.shape}; got {anchor.shape}')
+            xc = xc + (anchor[spin][states] - eps[spin][states])
+        roots, zs, info = contour_roots_unrestricted(
+            X_mos, D, list(eps), tuple(int(n) for n in nocc), spin, states, ntau=ntau,
+            nfreq_cd=nfreq, w0_cd=w0_cd, xc_correction=xc, continuation=continuation,
+            precision=precision)
+        return roots * HARTREE_TO_EV, zs, info
     if eps_anchor is not None:
         xc = xc + (np.asarray(eps_anchor, float)[states] - eps[states])
-    X, D = (factors['X_mo'], factors['D']) if isinstance(factors, dict) else factors[:2]
     roots, zs, info = contour_roots(X, D, eps, nocc, states, ntau=ntau, nfreq_cd=nfreq,
                                     w0_cd=w0_cd, xc_correction=xc, continuation=continuation,
                                     precision=precision)

@@ -689,8 +689,9 @@ def calc_qp_energy(mf, selfenergy='GW', polarizability='RPA', df=True, eta=None,
                                   'route')
     elif continuation in ('laplace', 'cd'):
         from .contour import solve_qp_energy_contour
-        ev, zs, _ = solve_qp_energy_contour(eps, None, nocc, np.asarray(states),
-                                            continuation=continuation, eps_anchor=eps_anchor,
+        ev, zs, _ = solve_qp_energy_contour(mf if eps.ndim == 2 else eps, None, nocc,
+                                            np.asarray(states), continuation=continuation,
+                                            eps_anchor=eps_anchor, spin_channel=spin_channel,
                                             **route_kwargs)
         res, z = list(ev), list(zs)
     else:

@@ -703,9 +703,10 @@ class LaplaceRefused(ValueError):
     on y = d -+ freq, LinearResponse/space_time.py:908-931)."""
 
 
-def laplace_check(eps, nocc, tau, tau_w, freq, tol=1e-8):
+def laplace_check(eps, nocc, tau, tau_w, freq, tol=1e-8, pair_energies=None):
     eps = np.asarray(eps, float)
-    d = (eps[nocc:][None, :] - eps[:nocc][:, None]).ravel()
+    d = (ov_energies(eps, nocc) if pair_energies is None
+         else np.asarray(pair_energies, float))
     y = np.concatenate([d - freq, d + freq])
     if y.min() <= 0.0 or not float(np.abs(
             (np.exp(-np.outer(y, tau)) @ tau_w) * y - 1.0).max()) < tol:
@@ -719,16 +720,18 @@ def laplace_screening_slope(proj_tau, tau, tau_w, freq, y):
     return float(y @ np.tensordot(dc, proj_tau, axes=(0, 0)) @ y)
 
 
-def sigma_cd_slope(p, omega, Bp, eps, nocc, nu, nu_w, wc, proj_tau, tau, tau_w):
+def sigma_cd_slope(p, omega, Bp, eps, nocc, nu, nu_w, wc, proj_tau, tau, tau_w,
+                   pair_energies=None):
     """contour_deformation.py:346-373 with the Laplace residue backend (the
-    representability check of real_screening.py:132-145 on each frequency)."""
+    representability check of real_screening.py:132-145 on each frequency;
+    pair_energies: both spins' of an unrestricted reference)."""
     eps = np.asarray(eps, float)
     _, dc = cd_integral_weights(omega - eps, nu, nu_w, with_slope=True)
     slope = -float(np.einsum('kq,kq->', dc, wc)) / np.pi
     for q, weight in residue_set(eps, nocc, omega):
         gap = eps[q] - omega
         freq = abs(gap)
-        laplace_check(eps, nocc, tau, tau_w, freq)
+        laplace_check(eps, nocc, tau, tau_w, freq, pair_energies=pair_energies)
         y = laplace_screening_apply(proj_tau, tau, tau_w, freq, Bp[:, q])
         slope -= weight * laplace_screening_slope(proj_tau, tau, tau_w, freq, y) * np.sign(gap)
     return slope
@@ -742,14 +745,14 @@ def laplace_screening_apply(proj_tau, tau, tau_w, freq, b):
     return np.linalg.solve(np.eye(chi0.shape[0]) - chi0, b)
 
 
-def sigma_cd(p, omega, Bp, eps, nocc, nu, nu_w, wc, proj_tau, tau, tau_w):
+def sigma_cd(p, omega, Bp, eps, nocc, nu, nu_w, wc, proj_tau, tau, tau_w, pair_energies=None):
     """contour_deformation.py:310-343 with the Laplace residue backend."""
     eps = np.asarray(eps, float)
     c = cd_integral_weights(omega - eps, nu, nu_w)
     s = -float(np.einsum('kq,kq->', c, wc)) / np.pi
     for q, weight in residue_set(eps, nocc, omega):
         b = Bp[:, q]
-        laplace_check(eps, nocc, tau, tau_w, abs(eps[q] - omega))
+        laplace_check(eps, nocc, tau, tau_w, abs(eps[q] - omega), pair_energies=pair_energies)
         y = laplace_screening_apply(proj_tau, tau, tau_w, abs(eps[q] - omega), b)
         s += weight * (b @ y - b @ b)
     return s
@@ -814,10 +817,11 @@ def wc_explicit(Bp, C_ov, d, nu):
     return out
 
 
-def sigma_cd_explicit(p, omega, Bp, eps, nocc, nu, nu_w, wc, C_ov, eta=0.0):
+def sigma_cd_explicit(p, omega, Bp, eps, nocc, nu, nu_w, wc, C_ov, eta=0.0,
+                      pair_energies=None):
     """contour_deformation.py:310-343 with the explicit residue backend."""
     eps = np.asarray(eps, float)
-    d = ov_energies(eps, nocc)
+    d = ov_energies(eps, nocc) if pair_energies is None else np.asarray(pair_energies, float)
     c = cd_integral_weights(omega - eps, nu, nu_w)
     s = -float(np.einsum('kq,kq->', c, wc)) / np.pi
     for q, weight in residue_set(eps, nocc, omega):
@@ -827,10 +831,11 @@ def sigma_cd_explicit(p, omega, Bp, eps, nocc, nu, nu_w, wc, C_ov, eta=0.0):
     return s
 
 
-def sigma_cd_slope_explicit(p, omega, Bp, eps, nocc, nu, nu_w, wc, C_ov, eta=0.0):
+def sigma_cd_slope_explicit(p, omega, Bp, eps, nocc, nu, nu_w, wc, C_ov, eta=0.0,
+                            pair_energies=None):
     """contour_deformation.py:346-373 with the explicit residue backend."""
     eps = np.asarray(eps, float)
-    d = ov_energies(eps, nocc)
+    d = ov_energies(eps, nocc) if pair_energies is None else np.asarray(pair_energies, float)
     _, dc = cd_integral_weights(omega - eps, nu, nu_w, with_slope=True)
     slope = -float(np.einsum('kq,kq->', dc, wc)) / np.pi
     for q, weight in residue_set(eps, nocc, omega):

@@ -37,6 +37,10 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      'cd': C_ov, W(freq) b and its slope below and above the
                      gap, the explicit imaginary-axis contraction, Sigma^c
                      with explicit residues and five states' roots and Z;
+* contour_unrestricted.npz  the contour of an unrestricted reference: the grid
+                     on both spins' pair energies, the spin-summed proj(tau),
+                     each channel's contraction and its roots and Z with the
+                     Laplace and the explicit residues;
 * sigma_ao.npz       the full AO self-energy with an AO collocation that is not
                      the MO one, a subset of its time points, its MO diagonal,
                      and the chi0 sweep's reverse for a seeded proj_bar;
@@ -49,7 +53,7 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      stored: the tests regenerate them from the seed and check
                      the regeneration against the stored eps and checksums.
 
-    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|contour_explicit|sigma_ao]
+    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|contour_explicit|contour_unrestricted|sigma_ao]
 """
 import os
 import sys
@@ -489,6 +493,55 @@ def contour_explicit_fixture():
         sigma=sig, roots=roots, root_explicit_wc=np.array([w, z]))
 
 
+def contour_unrestricted_fixture():
+    """The contour deformation of an unrestricted reference, composed from the
+    reference's pieces as GW/contour_deformation.py:686-812 composes them (the
+    driver itself needs pyscf): both spins' pair energies side by side set the
+    contour grid (cd_grid_range / cd_frequency_grid with pair_energies), the
+    spin-summed proj(tau), each channel's slices and screening contraction,
+    and each channel's roots and Z with the Laplace residues (pair energies
+    of both spins) and with the explicit ones (both spins' C_ov side by side
+    at 1/sqrt(2)). Spin alpha: 3 of 16 orbitals occupied; spin beta: its own
+    collocation and spectrum (another seed), 2 occupied."""
+    cd, rs = _import_contour_deformation()
+    from src.SingleReference.LinearResponse.space_time import (three_index_ov,
+                                                               three_index_slice)
+    from src.Base.orbital_spaces import ov_energies
+    X_a, D, eps_a = synthetic_system(16, 3, 48, 31, 'calibrated')
+    X_b, _, eps_b = synthetic_system(16, 2, 48, 33, 'calibrated')
+    X_mos, spectra, noccs = [X_a, X_b], [eps_a, eps_b], [3, 2]
+    pairs = np.concatenate([ov_energies(e, n) for e, n in zip(spectra, noccs)])
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        nu, nu_w, grid, w0 = cd.cd_frequency_grid(eps_a, 3, pair_energies=pairs)
+    proj = spin_summed(polarizability_projected_sweep, X_mos, D, spectra, noccs,
+                       grid.tau_points)
+    C_ov = np.hstack([three_index_ov(X, D, e, n) for X, e, n in zip(X_mos, spectra, noccs)])
+    out = dict(X_a=X_a, X_b=X_b, D=D, eps_a=eps_a, eps_b=eps_b, nocc_a=3, nocc_b=2, nu=nu,
+               nu_w=nu_w, w0=w0, tau=grid.tau_points, tau_w=grid.tau_weights,
+               cosft_wt=grid.cosft_wt, proj=proj, pairs=pairs)
+    for s, (X, e, n) in enumerate(zip(X_mos, spectra, noccs)):
+        states = np.array([n - 1, n, n + 1])
+        Bps = [three_index_slice(X, D, int(p)) for p in states]
+        wcs = cd.cd_screening_contraction_multi(proj, grid.cosft_wt, Bps)
+        lap, exp_ = np.full((3, 2), np.nan), np.zeros((3, 2))
+        for i, p in enumerate(states):
+            try:
+                w, z, _ = cd.qp_energy_cd(int(p), Bps[i], e, n, nu, nu_w, wc=wcs[i],
+                                          real_screening=rs.LaplaceRealScreening(
+                                              proj, grid, e, n, pair_energies=pairs))
+                lap[i] = w, z
+            except ValueError:
+                pass
+            w, z, _ = cd.qp_energy_cd(int(p), Bps[i], e, n, nu, nu_w, wc=wcs[i],
+                                      real_screening=rs.ExplicitRealScreening(
+                                          C_ov / np.sqrt(2.0), e, n, pair_energies=pairs))
+            exp_[i] = w, z
+        out.update({f'states_{s}': states, f'wc_{s}': np.stack(wcs), f'roots_laplace_{s}': lap,
+                    f'roots_cd_{s}': exp_})
+    np.savez_compressed(os.path.join(HERE, 'contour_unrestricted.npz'), **out)
+
+
 def sigma_ao_fixture():
     """The full AO self-energy of GW/imaginary_time.py:403-533 with an AO
     collocation that is not the MO one (X_ao = X_mo C^T, C a seeded orthogonal
@@ -580,9 +633,13 @@ if __name__ == '__main__':
         contour_explicit_fixture()
         print('explicit contour backend fixture written to', HERE)
         sys.exit(0)
+    if ONLY == 'contour_unrestricted':
+        contour_unrestricted_fixture()
+        print('unrestricted contour fixture written to', HERE)
+        sys.exit(0)
     if ONLY:
         sys.exit(f'--only {ONLY}: choose c1, static, unrestricted, sigma_adjoint, contour, '
-                 'contour_explicit or sigma_ao')
+                 'contour_explicit, contour_unrestricted or sigma_ao')
     grids_fixture()
     shared_kernel_fixture()
     route_fixture('calibrated', 24, 4, 64, 7, 'calibrated', 12, full=True)
@@ -594,5 +651,6 @@ if __name__ == '__main__':
     sigma_adjoint_fixture()
     contour_fixture()
     contour_explicit_fixture()
+    contour_unrestricted_fixture()
     sigma_ao_fixture()
     print('fixtures written to', HERE)

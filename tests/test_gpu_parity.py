@@ -605,6 +605,47 @@ def test_contour_explicit_backend_matches_reference_golden(golden):
     assert np.abs(np.asarray(e) / contour.HARTREE_TO_EV - g['roots'][:, 0]).max() < 1e-9
 
 
+def test_contour_unrestricted_matches_reference_golden(golden):
+    """The contour of an unrestricted reference on the device: each channel's
+    roots and Z with the Laplace residues (both spins' pair energies) and the
+    explicit ones (both spins' C_ov at 1/sqrt(2)) against the reference's
+    composition, directly and through the drop-in driver and calc_qp_energy
+    with an unrestricted mean field (X_ao = [X_alpha | X_beta], mo_coeff
+    selecting each half)."""
+    from types import SimpleNamespace
+    from mbptcode_b200 import contour, gw
+    g = golden('contour_unrestricted')
+    X_mos, D = [g['X_a'], g['X_b']], g['D']
+    spectra, noccs = [g['eps_a'], g['eps_b']], [int(g['nocc_a']), int(g['nocc_b'])]
+    for s in (0, 1):
+        for cont in ('laplace', 'cd'):
+            r, z, info = contour.contour_roots_unrestricted(X_mos, D, spectra, noccs, s,
+                                                            g[f'states_{s}'], continuation=cont)
+            want = g[f'roots_{cont}_{s}']
+            assert np.abs(r - want[:, 0]).max() < 1e-9 and np.abs(z - want[:, 1]).max() < 1e-8, \
+                (s, cont, r - want[:, 0])
+            assert info['continuation'] == cont
+    norb = len(spectra[0])
+    X_ao = np.hstack(X_mos)
+    mo = np.zeros((2, 2 * norb, norb))
+    mo[0, :norb] = np.eye(norb)
+    mo[1, norb:] = np.eye(norb)
+    occ = np.zeros((2, norb))
+    occ[0, :noccs[0]] = 1.0
+    occ[1, :noccs[1]] = 1.0
+    mf = SimpleNamespace(mo_energy=np.stack(spectra), mo_occ=occ, mo_coeff=mo)
+    ev, zs, info = contour.solve_qp_energy_contour(mf, None, tuple(noccs), g['states_1'],
+                                                   spin_channel='beta',
+                                                   factors=(X_mos[0], D, X_ao))
+    assert np.abs(ev / contour.HARTREE_TO_EV - g['roots_cd_1'][:, 0]).max() < 1e-9
+    assert info['residue_route_taken'] == 'explicit'
+    e, z = gw.calc_qp_energy(mf, mode='space-time', continuation='laplace', spin_channel='alpha',
+                             state=[int(p) for p in g['states_0']], factors=(X_mos[0], D, X_ao),
+                             return_z=True)
+    assert np.abs(np.asarray(e) / contour.HARTREE_TO_EV - g['roots_laplace_0'][:, 0]).max() < 1e-9
+    assert np.abs(np.asarray(z) - g['roots_laplace_0'][:, 1]).max() < 1e-8
+
+
 def test_ao_self_energy_and_mirrors_match_reference_golden(golden):
     """self_energy_matrix_imaginary_time (full AO matrix, an AO collocation
     that is not the MO one; all time points and a subset), its MO diagonal,

@@ -333,6 +333,54 @@ def test_contour_explicit_backend_oracle(golden):
         assert abs(w - g['roots'][i, 0]) < 1e-10 and abs(z - g['roots'][i, 1]) < 1e-9, p
 
 
+def test_contour_unrestricted_oracle(golden):
+    """The contour of an unrestricted reference against the reference's
+    composition: the grid on both spins' pair energies (host code, bit for
+    bit), the oracle's spin-summed proj(tau) and each channel's contraction,
+    and each channel's roots and Z through the scan root finder with the
+    Laplace residues (on both spins' pair energies) and the explicit ones
+    (both spins' C_ov side by side at 1/sqrt(2))."""
+    from mbptcode_b200 import contour
+    g = golden('contour_unrestricted')
+    X_mos, D = [g['X_a'], g['X_b']], g['D']
+    spectra, noccs = [g['eps_a'], g['eps_b']], [int(g['nocc_a']), int(g['nocc_b'])]
+    pairs = np.concatenate([orc.ov_energies(e, n) for e, n in zip(spectra, noccs)])
+    assert np.array_equal(pairs, g['pairs'])
+    with _quiet():
+        nu, nu_w, grid, w0 = contour.cd_frequency_grid(spectra[0], noccs[0], pair_energies=pairs)
+    assert np.array_equal(nu, g['nu']) and np.array_equal(nu_w, g['nu_w']) and w0 == g['w0']
+    assert np.array_equal(grid.tau_points, g['tau']) and np.array_equal(grid.cosft_wt,
+                                                                       g['cosft_wt'])
+    proj = 0.5 * sum(orc.polarizability_projected_sweep(X, D, e, n, g['tau'])
+                     for X, e, n in zip(X_mos, spectra, noccs))
+    assert np.abs(proj - g['proj']).max() <= 1e-12 * np.abs(g['proj']).max()
+    C = np.hstack([orc.three_index_ov(X, D, e, n)
+                   for X, e, n in zip(X_mos, spectra, noccs)]) / np.sqrt(2.0)
+    for s, (X, e, n) in enumerate(zip(X_mos, spectra, noccs)):
+        B = [orc.three_index_slice(X, D, int(p)) for p in g[f'states_{s}']]
+        wcs = orc.cd_screening_contraction(g['proj'], g['cosft_wt'], B)
+        assert np.abs(np.stack(wcs) - g[f'wc_{s}']).max() <= 1e-12 * np.abs(g[f'wc_{s}']).max()
+        for i, p in enumerate(g[f'states_{s}']):
+            p, wc = int(p), g[f'wc_{s}'][i]
+            lap = dict(pair_energies=pairs)
+            roots = {}
+            for name, sig, slope, extra in (
+                    ('laplace', orc.sigma_cd, orc.sigma_cd_slope,
+                     (g['proj'], g['tau'], g['tau_w'])),
+                    ('cd', orc.sigma_cd_explicit, orc.sigma_cd_slope_explicit, (C,))):
+                def residual(w, p=p, i=i, sig=sig, extra=extra):
+                    return w - e[p] - sig(p, w, B[i], e, n, nu, nu_w, wc, *extra, **lap)
+
+                def fprime(w, p=p, i=i, slope=slope, extra=extra):
+                    return 1.0 - slope(p, w, B[i], e, n, nu, nu_w, wc, *extra, **lap)
+                roots[name] = contour.solve_qp_equation_scan(residual, fprime, float(e[p]),
+                                                             refusals=(orc.LaplaceRefused,))
+            for name in ('laplace', 'cd'):
+                want = g[f'roots_{name}_{s}'][i]
+                w, z = roots[name]
+                assert abs(w - want[0]) < 1e-10 and abs(z - want[1]) < 1e-9, (s, p, name)
+
+
 def test_ao_self_energy_oracle(golden):
     """The oracle's full AO self-energy (an AO collocation that is not the MO
     one) and the chi0 sweep's reverse against the reference's."""
