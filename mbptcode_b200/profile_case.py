@@ -40,6 +40,9 @@ screening contraction (64 frequencies, 20 states) and one Sigma^c evaluation.
 the same size: C_ov, the explicit response at one real frequency and one
 W(freq) - I below and above the particle-hole gap.
 
+--chi0-aux NAUX NOV [--mixed]: the explicit response alone on a seeded factor,
+three calls (the capture case of its engine launch).
+
 --fp64-peak N: the FP64 reference rates of this GPU, timed with CUDA events
 (best of 5 after a warm-up): cuBLAS DGEMM at N^3 and cuSOLVER's Cholesky of
 an N x N SPD matrix (the FP64 factorisation of the Dyson step).
@@ -237,6 +240,23 @@ def explicit_rows(a):
                       C, eps, nocc, precision=prec).w_minus_identity(w))
 
 
+def chi0_aux_case(a):
+    """The explicit particle-hole response alone on a seeded (naux x nov)
+    factor, three calls in the requested precision (the capture case of the
+    mixed response's engine launch): --chi0-aux NAUX NOV [--mixed]."""
+    from . import space_time
+    naux, nov = a.chi0_aux
+    g = torch.Generator(device='cuda').manual_seed(7)
+    C = torch.randn(naux, nov, generator=g, device='cuda', dtype=torch.float64) / nov ** 0.5
+    f = -np.linspace(0.5, 2.0, nov)
+    out = torch.empty((naux, naux), dtype=torch.float64, device='cuda')
+    prec = 'mixed' if a.mixed else 'fp64'
+    for _ in range(3):
+        space_time.chi0_aux([(C, f)], 2.0, out=out, precision=prec)
+    torch.cuda.synchronize()
+    print(f'chi0_aux {prec} naux={naux} nov={nov}: ok', flush=True)
+
+
 def fp64_peak(a):
     n = a.fp64_peak
     g = torch.Generator(device='cuda').manual_seed(4)
@@ -297,6 +317,8 @@ def main():
     p.add_argument('--qp-mlp', action='store_true')
     p.add_argument('--rows', action='store_true')
     p.add_argument('--rows-cd', action='store_true')
+    p.add_argument('--chi0-aux', type=int, nargs=2, default=None)
+    p.add_argument('--mixed', action='store_true')
     a = p.parse_args()
     torch.cuda.set_device(0)
     if a.qp_mlp:
@@ -305,6 +327,8 @@ def main():
         return rows(a)
     if a.rows_cd:
         return explicit_rows(a)
+    if a.chi0_aux:
+        return chi0_aux_case(a)
     if a.fp64_peak:
         return fp64_peak(a)
     if a.dyson:
