@@ -1449,11 +1449,11 @@ int mbpt_three_index_slices(const double *X, int64_t M, int64_t norb, const doub
 
 // The explicit particle-hole response chi0 = s (C f) C^T. FP64: columns of C
 // in chunks of kChi0AuxChunk, each chunk scaled into the workspace and folded
-// in by a symmetric rank-k product (one triangle), the other triangle
-// mirrored. Mixed: C f and C as zero-padded BF16 pairs, one split product
+// into the lower triangle by row-panel DGEMMs, the other triangle mirrored. Mixed: C f and C as zero-padded BF16 pairs, one split product
 // over the whole K on the engine's upper 128 x 256 tiles, stored as FP64 and
 // mirrored by its epilogue.
 constexpr int64_t kChi0AuxChunk = 4096;
+constexpr int64_t kChi0AuxPanel = 1024;
 
 size_t mbpt_chi0_aux_workspace_bytes(int64_t naux, int64_t nov, int mode) {
   if (naux < 1 || nov < 1) return 0;
@@ -1497,18 +1497,19 @@ int mbpt_chi0_aux(const double *C, int64_t naux, int64_t nov, int64_t ldc, const
   double *T = ar.take<double>(naux * chunk);
   if (ar.overflow()) return MBPT_ERR_WORKSPACE;
   cublasHandle_t h = handles(st).blas;
-  const double one = 1.0;
   for (int64_t j0 = 0; j0 < nov; j0 += chunk) {
     const int64_t nc = std::min(chunk, nov - j0);
     launch_cols_scaled_copy(C, ldc, j0, f, spin_factor, naux, nc, T, st);
     const double beta = (j0 == 0 && !accumulate) ? 0.0 : 1.0;
-    // column-major view: chi0 = T_cm^T C_cm over this chunk's rows of the
-    // transposed factors, its upper triangle (the row-major lower one)
-    if (cublasDsyrkx(h, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, static_cast<int>(naux),
-                     static_cast<int>(nc), &one, T, static_cast<int>(nc), C + j0,
-                     static_cast<int>(ldc), &beta, chi0,
-                     static_cast<int>(naux)) != CUBLAS_STATUS_SUCCESS)
-      return MBPT_ERR_CUDA;
+    // the row-major lower triangle in row panels of kChi0AuxPanel: rows
+    // [q0, q1) against columns [0, q1), one DGEMM each (the diagonal block
+    // whole), the upper triangle mirrored once at the end
+    for (int64_t q0 = 0; q0 < naux; q0 += kChi0AuxPanel) {
+      const int64_t q1 = std::min(naux, q0 + kChi0AuxPanel);
+      if (!dgemm_rm(h, false, true, q1 - q0, q1, nc, 1.0, T + q0 * nc, nc, C + j0, ldc, beta,
+                    chi0 + q0 * naux, naux))
+        return MBPT_ERR_CUDA;
+    }
   }
   launch_mirror_lower_to_upper(chi0, naux, st);
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
