@@ -275,6 +275,13 @@ int mbpt_three_index_slices(const double *X_dev, int64_t M, int64_t norb, const 
                             int64_t naux, const int64_t *states_host, int nstates,
                             double *B_dev, void *workspace, size_t ws_bytes, void *stream);
 
+/* (1 - chi0) y = b from mbpt_dyson's Cholesky factor (want_w = 0: the
+ * column-major lower factor L of 1 - chi0 in the chi0 slice), in place on b
+ * (column-major n x nrhs): the contour residues' W(freq) b
+ * (GW/real_screening.py:147-150 `LaplaceRealScreening.apply`, which solves
+ * against 1 - chi0), without forming W. FP64. */
+int mbpt_chol_solve(const double *L_dev, int64_t n, double *b_dev, int nrhs, void *stream);
+
 /* The explicit particle-hole response of one block (continuation 'cd'),
  * LinearResponse/space_time.py:934-953 `chi0_aux` as GW/real_screening.py:
  * 171-181 `screening_aux` calls it:

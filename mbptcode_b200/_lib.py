@@ -61,6 +61,7 @@ _SIGNATURES = {
                            _p, _sz, _p, _p]),
     'mbpt_three_index_slices_workspace_bytes': (_sz, [_i64, _i64]),
     'mbpt_three_index_slices': (_i, [_p, _i64, _i64, _p, _i64, _p, _i, _p, _p, _sz, _p]),
+    'mbpt_chol_solve': (_i, [_p, _i64, _p, _i, _p]),
     'mbpt_chi0_aux_workspace_bytes': (_sz, [_i64, _i64, _i]),
     'mbpt_chi0_aux': (_i, [_p, _i64, _i64, _i64, _p, _d, _i, _i, _p, _p, _sz, _p, _p]),
     'mbpt_screening_contraction_workspace_bytes': (_sz, [_i64, _i64, _i]),

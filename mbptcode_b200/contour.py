@@ -286,10 +286,53 @@ def screening_contraction(Bp, wbp):
                      optimize=True)
 
 
+class _ResidueSolves:
+    """W(freq) b for the residues of one backend: 1 - chi0(freq) factorised
+    once per frequency by the Dyson step's FP64 Cholesky and kept for the
+    latest `cap` frequencies (the value and the slope of one scan point
+    apply W at the same frequencies), each b then solved against the factor
+    by two triangular solves (mbpt_chol_solve) without forming W. Where
+    1 - chi0 is not positive definite (the explicit response above the
+    gap) W - I comes from the LU inverse instead."""
+
+    def __init__(self, cap):
+        self.cap = cap
+        self._c = OrderedDict()
+
+    def entry(self, key, build):
+        ent = self._c.get(key)
+        if ent is not None:
+            self._c.move_to_end(key)
+            return ent
+        chi0 = build()
+        _, _, info, _ = dyson_batch(chi0, want_w=False, precision='fp64')
+        if info[0] == 0:
+            ent = ('factor', chi0[0])
+        else:
+            chi0 = build()
+            dyson_batch(chi0, want_w=True, precision='fp64')
+            ent = ('w', chi0[0])
+        self._c[key] = ent
+        if len(self._c) > self.cap:
+            self._c.popitem(last=False)
+        return ent
+
+    @staticmethod
+    def solve(ent, bd):
+        kind, m = ent
+        if kind == 'w':
+            return bd + m @ bd
+        y = bd.clone().contiguous()
+        check(lib().mbpt_chol_solve(ptr(m), m.shape[0], ptr(y), 1, stream_ptr()),
+              'mbpt_chol_solve')
+        return y
+
+
 class LaplaceRealScreening:
     """W at a real frequency below the particle-hole gap from proj(tau): one
-    (ntau, naux^2) transform and one Dyson step per frequency, the W - I of
-    each frequency kept for later calls (``real_screening.py:94-154``).
+    (ntau, naux^2) transform and one Cholesky factorisation per frequency,
+    the factor kept for later calls and W b solved against it
+    (``real_screening.py:94-154``).
     Refuses (ResidueRefused) a frequency the grid does not carry.
     pair_energies: the particle-hole energies proj(tau) was summed over, when
     they are not the ones (eps, nocc) spans (both spins of an unrestricted
@@ -309,10 +352,24 @@ class LaplaceRealScreening:
         naux = self.proj_tau.shape[-1]
         self._cap = max(2, min(2 * len(self.eps), int(cache_bytes // (8 * naux * naux))))
         self._w = OrderedDict()
+        self._solves = _ResidueSolves(self._cap)
+        # the representability check on the device: 2 nocc nvirt x ntau
+        # exponentials per new frequency
+        dev = self.proj_tau.device
+        d = (ov_energies(self.eps, nocc) if self.pair_energies is None
+             else self.pair_energies)
+        self._d = torch.as_tensor(d, dtype=torch.float64, device=dev)
+        self._tau = torch.as_tensor(np.asarray(grid.tau_points, float), device=dev)
+        self._tw = torch.as_tensor(np.asarray(grid.tau_weights, float), device=dev)
 
     def representation_error(self, freq):
-        return laplace_representation_error(self.grid, self.eps, self.nocc, freq,
-                                            pair_energies=self.pair_energies)
+        """max over y = d -+ freq of |y sum_k w_k e^{-y tau_k} - 1|, inf where
+        freq reaches the gap (``LinearResponse/space_time.py:908-931``)."""
+        y = torch.cat([self._d - freq, self._d + freq])
+        if float(y.min()) <= 0.0:
+            return np.inf
+        q = torch.exp(-y[:, None] * self._tau[None, :]) @ self._tw
+        return float((q * y - 1.0).abs().max())
 
     def _weights(self, freq):
         err = self.representation_error(freq)
@@ -341,9 +398,12 @@ class LaplaceRealScreening:
         return w
 
     def apply(self, freq, b):
-        """W(freq) b = b + (W - I) b."""
-        bd = to_device(b, self.proj_tau.device)
-        y = bd + self.w_minus_identity(freq) @ bd
+        """W(freq) b = [1 - chi0(freq)]^-1 b, by a solve against the
+        frequency's kept Cholesky factor (``real_screening.py:147-150``)."""
+        key = float(freq)
+        ent = self._solves.entry(
+            key, lambda: _rows_transform(self.proj_tau, self._weights(key)[0][None, :]))
+        y = _ResidueSolves.solve(ent, to_device(b, self.proj_tau.device))
         return y if isinstance(b, torch.Tensor) else y.cpu().numpy()
 
     def slope(self, freq, y):
@@ -419,13 +479,13 @@ class ExplicitRealScreening:
         naux = self.C_ov.shape[0]
         self._cap = max(2, min(2 * len(self.eps), int(cache_bytes // (8 * naux * naux))))
         self._w = OrderedDict()
+        self._solves = _ResidueSolves(self._cap)
 
     def w_minus_identity(self, freq, imaginary=False):
         key = (float(freq), bool(imaginary))
         w = self._w.get(key)
         if w is None:
-            f = frequency_factor(self.d, float(freq), imaginary, self.eta)
-            chi0 = chi0_aux([(self.C_ov, f)], 2.0, precision=self.precision)[None]
+            chi0 = self._chi0(freq, imaginary)
             dyson_batch(chi0, want_w=True, precision='fp64')
             w = self._w[key] = chi0[0]
             if len(self._w) > self._cap:
@@ -434,10 +494,16 @@ class ExplicitRealScreening:
             self._w.move_to_end(key)
         return w
 
+    def _chi0(self, freq, imaginary=False):
+        f = frequency_factor(self.d, float(freq), imaginary, self.eta)
+        return chi0_aux([(self.C_ov, f)], 2.0, precision=self.precision)[None]
+
     def apply(self, freq, b):
-        """W(freq) b = b + (W - I) b."""
-        bd = to_device(b, self.C_ov.device)
-        y = bd + self.w_minus_identity(freq) @ bd
+        """W(freq) b = [1 - chi0(freq)]^-1 b, by a solve against the
+        frequency's kept Cholesky factor (the LU inverse above the gap)."""
+        key = float(freq)
+        ent = self._solves.entry(key, lambda: self._chi0(key))
+        y = _ResidueSolves.solve(ent, to_device(b, self.C_ov.device))
         return y if isinstance(b, torch.Tensor) else y.cpu().numpy()
 
     def slope(self, freq, y):

@@ -1515,6 +1515,22 @@ int mbpt_chi0_aux(const double *C, int64_t naux, int64_t nov, int64_t ldc, const
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 
+// (1 - chi0) y = b from the Dyson step's Cholesky factor (column-major lower
+// L, as mbpt_dyson leaves it with want_w = 0): two triangular solves on the
+// nrhs right-hand sides of b (column-major n x nrhs), in place.
+int mbpt_chol_solve(const double *L, int64_t n, double *b, int nrhs, void *stream) {
+  if (n < 1 || nrhs < 1 || n > INT32_MAX) return MBPT_ERR_SHAPE;
+  cudaStream_t st = S(stream);
+  cublasHandle_t h = handles(st).blas;
+  const double one = 1.0;
+  const int ni = static_cast<int>(n);
+  for (cublasOperation_t op : {CUBLAS_OP_N, CUBLAS_OP_T})
+    if (cublasDtrsm(h, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, op, CUBLAS_DIAG_NON_UNIT, ni,
+                    nrhs, &one, L, ni, b, ni) != CUBLAS_STATUS_SUCCESS)
+      return MBPT_ERR_CUDA;
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
 struct ContractionBufs {
   double *Y = nullptr;                                        // fp64
   bf16 *w_hi = nullptr, *w_lo = nullptr, *b_hi = nullptr, *b_lo = nullptr;  // mixed

@@ -238,6 +238,22 @@ def explicit_rows(a):
             timed(f'cd: W(freq) - I {label}, chi0 + Dyson, {prec}',
                   lambda w=w, prec=prec: contour.ExplicitRealScreening(
                       C, eps, nocc, precision=prec).w_minus_identity(w))
+    del C, out
+    # whole contour solves of the HOMO and the LUMO (grid, proj(tau), the
+    # contraction of 64 frequencies, the scan with its residues), one call each
+    import time
+    states = [nocc - 1, nocc]
+    for cont, prec in (('laplace', 'fp64'), ('cd', 'mixed')):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r, z, info = contour.contour_roots(X, D, eps, nocc, states, continuation=cont,
+                                           precision=prec)
+        torch.cuda.synchronize()
+        print(json.dumps({'row': f'cd: contour_roots of HOMO and LUMO, {cont}, {prec}',
+                          'host_s': round(time.perf_counter() - t0, 3),
+                          'roots_Ha': [float(x) for x in r], 'z': [float(x) for x in z],
+                          'residues': [rec['residues'] for rec in info['states']]}),
+              flush=True)
 
 
 def chi0_aux_case(a):
