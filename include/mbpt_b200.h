@@ -357,7 +357,8 @@ int mbpt_mlp_adamw(float *params_dev, const float *grad_dev, float *m_dev, float
 /* ---- split-precision GEMM (diagnostic entry of the tensor-core engine) ---
  * C (m x n, FP32, ldc) = alpha * A B^T with A (m x k) and B (n x k) FP64,
  * each rounded to a BF16 pair and multiplied with three tcgen05 products.
- * m, n, k are padded internally to multiples of 128 / 128 / 64. */
+ * m, n, k are padded internally to multiples of 128 / 128 / 64. Extents
+ * above 2^24 are refused (MBPT_ERR_SHAPE; the sizing call returns SIZE_MAX). */
 size_t mbpt_gemm_split_workspace_bytes(int64_t m, int64_t n, int64_t k);
 int mbpt_gemm_split(const double *A_dev, const double *B_dev, int64_t m, int64_t n, int64_t k,
                     double alpha, float *C_dev, int64_t ldc, void *workspace, size_t ws_bytes,

@@ -1703,6 +1703,7 @@ int mbpt_energy_adjoint_seed(double *wmi, int64_t naux, int nfreq, const double 
 }
 
 size_t mbpt_gemm_split_tf32_workspace_bytes(int64_t m, int64_t n, int64_t k) {
+  if (!gemm_extents_ok(m, n, k)) return SIZE_MAX;
   const int64_t mp = round_up(m, 128), np = round_up(n, 128), kp = round_up(k, 32);
   Arena ar;
   ar.counting = true;
@@ -1717,7 +1718,7 @@ size_t mbpt_gemm_split_tf32_workspace_bytes(int64_t m, int64_t n, int64_t k) {
 int mbpt_gemm_split_tf32(const double *A, const double *B, int64_t m, int64_t n, int64_t k,
                          double alpha, float *C, int64_t ldc, void *ws, size_t ws_bytes,
                          int *err, void *stream) {
-  if (m < 1 || n < 1 || k < 1 || ldc < n) return MBPT_ERR_SHAPE;
+  if (!gemm_extents_ok(m, n, k) || ldc < n) return MBPT_ERR_SHAPE;
   cudaStream_t st = S(stream);
   const int64_t mp = round_up(m, 128), np = round_up(n, 128), kp = round_up(k, 32);
   Arena ar = arena(ws, ws_bytes);
@@ -1740,6 +1741,7 @@ int mbpt_gemm_split_tf32(const double *A, const double *B, int64_t m, int64_t n,
 }
 
 size_t mbpt_gemm_split_workspace_bytes(int64_t m, int64_t n, int64_t k) {
+  if (!gemm_extents_ok(m, n, k)) return SIZE_MAX;
   const int64_t mp = round_up(m, 128), np = round_up(n, 128), kp = round_up(k, 64);
   Arena ar;
   ar.counting = true;
@@ -1752,7 +1754,7 @@ size_t mbpt_gemm_split_workspace_bytes(int64_t m, int64_t n, int64_t k) {
 int mbpt_gemm_split(const double *A, const double *B, int64_t m, int64_t n, int64_t k,
                     double alpha, float *C, int64_t ldc, void *ws, size_t ws_bytes, int *err,
                     void *stream) {
-  if (m < 1 || n < 1 || k < 1 || ldc < n) return MBPT_ERR_SHAPE;
+  if (!gemm_extents_ok(m, n, k) || ldc < n) return MBPT_ERR_SHAPE;
   cudaStream_t st = S(stream);
   const int64_t mp = round_up(m, 128), np = round_up(n, 128), kp = round_up(k, 64);
   Arena ar = arena(ws, ws_bytes);

@@ -44,6 +44,15 @@ __host__ __device__ __forceinline__ int64_t round_up(int64_t x, int64_t m) {
   return (x + m - 1) / m * m;
 }
 
+// Largest matrix extent the stand-alone GEMM entry points take (2^24): with
+// every extent at most this, the padded products and their byte counts
+// (below 2^52) cannot wrap in int64_t or size_t.
+constexpr int64_t kMaxGemmExtent = int64_t(1) << 24;
+__host__ __device__ __forceinline__ bool gemm_extents_ok(int64_t m, int64_t n, int64_t k) {
+  return m >= 1 && n >= 1 && k >= 1 && m <= kMaxGemmExtent && n <= kMaxGemmExtent &&
+         k <= kMaxGemmExtent;
+}
+
 // Error word written by kernels that detect a failure on the device (a wait
 // that ran out). Zeroed by the host before a call, read back after it.
 struct DevErr {

@@ -62,6 +62,9 @@ size_t mbpt_gemm_split_static_capacity(void) { return kScratchBytes; }
 int mbpt_gemm_split_static(const double *A, const double *B, int64_t m, int64_t n, int64_t k,
                            double alpha, float *C, int64_t ldc, int *err, void *stream) {
   if (m < 1 || n < 1 || k < 1 || ldc < n) return MBPT_ERR_SHAPE;
+  // extents past 2^24 could make the byte counts below wrap; no such
+  // product fits the array anyway
+  if (!gemm_extents_ok(m, n, k)) return MBPT_ERR_WORKSPACE;
   const int64_t mp = round_up(m, 128), np = round_up(n, 128), kp = round_up(k, 64);
   const size_t a_bytes = aligned(sizeof(bf16) * mp * kp);
   const size_t b_bytes = aligned(sizeof(bf16) * np * kp);

@@ -237,14 +237,26 @@ def solve_qp_from_imaginary_axis(eps, p_state, xc_correction, z_fit, sigma_iw, g
     return (root, float(zz[0])) if with_z else root
 
 
+def _state_list(states, limit=12):
+    shown = ', '.join(str(int(s)) for s in states[:limit])
+    return shown + (f', ... ({len(states) - limit} more)' if len(states) > limit else '')
+
+
 def _report_flags(flags_h, states):
-    for s, f in zip(np.atleast_1d(states), flags_h):
-        if f & QP_FLAG_NO_ROOT:
-            warnings.warn(f'orbital {int(s)}: the quasiparticle equation has no root in '
-                          f'the widest scan window', QPNoRoot, stacklevel=3)
-        elif f & QP_FLAG_Z_OUTSIDE:
-            warnings.warn(f'orbital {int(s)}: root kept with Z outside (0, 1]',
-                          QPWeightOutside, stacklevel=3)
+    """One warning per kind for a whole solve: the count and the orbitals
+    (the first dozen named), as the reference's named flags report a
+    condition once per call rather than once per state."""
+    states = np.atleast_1d(states)
+    flags_h = np.asarray(flags_h)
+    none = states[(flags_h & QP_FLAG_NO_ROOT) != 0]
+    outside = states[((flags_h & QP_FLAG_NO_ROOT) == 0) & ((flags_h & QP_FLAG_Z_OUTSIDE) != 0)]
+    if len(none):
+        warnings.warn(f'{len(none)} of {len(states)} orbitals have no root of the '
+                      f'quasiparticle equation in the widest scan window: '
+                      f'{_state_list(none)}', QPNoRoot, stacklevel=3)
+    if len(outside):
+        warnings.warn(f'{len(outside)} of {len(states)} orbitals keep a root with Z outside '
+                      f'(0, 1]: {_state_list(outside)}', QPWeightOutside, stacklevel=3)
 
 
 class SweepResult(dict):

@@ -28,7 +28,7 @@ from .gw import gw_sweep, sigma_branch_sums
 from .space_time import _eps_host, to_device
 
 FEATURE_OFFSET = 0.1  # Ha, the two real frequencies Sigma_c is read at
-#: the network trained by `python -m mbptcode_b200.learned_warm_start --save`
+#: the network trained by `python bench_cases.py warm-start --save`
 #: (512 method-generated systems, n_orb 100-800, mixed precision)
 MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'data',
                           'qp_shift_model.npz')

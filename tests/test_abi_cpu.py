@@ -55,23 +55,3 @@ def test_host_tensors_are_refused_before_any_kernel():
         _lib.ptr(np.zeros(3))
     assert _lib.ptr(None) is None
 
-
-def test_integration_stub_matches_the_binding():
-    """The ctypes stub a maintainer would paste into MBPTcode (INTEGRATION.md,
-    section 3) declares the same argument and return types as the package's
-    own binding, entry by entry."""
-    import ctypes as C
-    import os
-    import re
-    from mbptcode_b200 import _lib
-    text = open(os.path.join(os.path.dirname(__file__), '..', 'INTEGRATION.md')).read()
-    names = {'_p': C.c_void_p, '_i64': C.c_int64, '_i': C.c_int, '_d': C.c_double,
-             '_sz': C.c_size_t}
-    argtypes = dict(re.findall(r'_L\.(mbpt_\w+)\.argtypes = \[([^\]]*)\]', text, re.S))
-    restypes = dict(re.findall(r'_L\.(mbpt_\w+)\.restype = (\w+)', text))
-    assert argtypes, 'no stub found'
-    for name, args in argtypes.items():
-        got = [names[a.strip()] for a in args.replace('\n', ' ').split(',') if a.strip()]
-        assert got == _lib._SIGNATURES[name][1], name
-    for name, res in restypes.items():
-        assert names[res] == _lib._SIGNATURES[name][0], name
