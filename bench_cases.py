@@ -410,7 +410,7 @@ def warm_start(a):
     import json
     import time
     import warnings
-    from mbptcode_b200.evgw import EvGWNotConverged, evgw_eigenvalues
+    from mbptcode_b200.evgw import EvGWNotConverged, evgw_device
     from mbptcode_b200.gw import QPNoRoot, QPWeightOutside
     from mbptcode_b200.qp_mlp import QPShiftModel, method_samples, warm_start_compare
     warnings.simplefilter('ignore', QPWeightOutside)
@@ -453,12 +453,12 @@ def warm_start(a):
         r = warm_start_compare(model, X, D, eps, nocc, ntau=a.ntau, precision=a.precision)
         g0w0.append(dict(n_orb=int(n), **r))
         tp = time.perf_counter()
-        e_p, info_p = evgw_eigenvalues(X, D, eps, nocc, ntau=a.ntau, precision=a.precision)
+        e_p, info_p = evgw_device(X, D, eps, nocc, ntau=a.ntau, precision=a.precision)
         tw = time.perf_counter()
-        e_w, info_w = evgw_eigenvalues(X, D, eps, nocc, ntau=a.ntau, precision=a.precision,
+        e_w, info_w = evgw_device(X, D, eps, nocc, ntau=a.ntau, precision=a.precision,
                                        warm=model, verify=True)
         te = time.perf_counter()
-        e_q, _ = evgw_eigenvalues(X, D, eps + 1e-11, nocc, ntau=a.ntau, precision=a.precision)
+        e_q, _ = evgw_device(X, D, eps + 1e-11, nocc, ntau=a.ntau, precision=a.precision)
         ok = np.isfinite(e_p) & np.isfinite(e_w)
         okq = np.isfinite(e_p) & np.isfinite(e_q)
         f = frontier(nocc, int(n))

@@ -282,6 +282,28 @@ int mbpt_three_index_slices(const double *X_dev, int64_t M, int64_t norb, const 
  * against 1 - chi0), without forming W. FP64. */
 int mbpt_chol_solve(const double *L_dev, int64_t n, double *b_dev, int nrhs, void *stream);
 
+/* The contour deformation's imaginary-axis term and its slope at nq points
+ * (state slot slot_dev[j], real frequency omega_dev[j]): value[j] =
+ * -(1/pi) sum_(k,q) c_k(omega - eps_q) wc[slot][k][q] with the Gauss-Legendre
+ * weights of the Lorentzian kernel and the closed-form correction of its
+ * singular part (wc(0) = e1 wc[k1] + e2 wc[k2], model a^2 / (a^2 + nu^2)),
+ * slope[j] its omega derivative (GW/contour_deformation.py:150-202
+ * `cd_integral_weights` contracted as in :310-373 `sigma_cd`,
+ * `sigma_cd_slope`). wc_dev: (nslots, nfreq, norb) FP64. */
+int mbpt_cd_integral_terms(const double *wc_dev, int nslots, int nfreq, int64_t norb,
+                           const double *eps_dev, const double *nu_dev, const double *nu_w_dev,
+                           int k1, int k2, double e1, double e2, double a, double on_tol,
+                           const int *slot_dev, const double *omega_dev, int64_t nq,
+                           double *value_dev, double *slope_dev, void *stream);
+/* err[i] = max over the pair energies d and both signs of y = d -+ freq[i] of
+ * |y sum_k tau_w[k] e^(-y tau[k]) - 1|, infinity where some y <= 0: whether
+ * the imaginary-time grid carries a real frequency
+ * (LinearResponse/space_time.py:908-931 `laplace_representation_error`). */
+int mbpt_laplace_representation_error(const double *d_dev, int64_t npairs,
+                                       const double *tau_dev, const double *tau_w_dev, int ntau,
+                                       const double *freq_dev, int64_t nf, double *err_dev,
+                                       void *stream);
+
 /* The explicit particle-hole response of one block (continuation 'cd'),
  * LinearResponse/space_time.py:934-953 `chi0_aux` as GW/real_screening.py:
  * 171-181 `screening_aux` calls it:

@@ -62,6 +62,9 @@ _SIGNATURES = {
     'mbpt_three_index_slices_workspace_bytes': (_sz, [_i64, _i64]),
     'mbpt_three_index_slices': (_i, [_p, _i64, _i64, _p, _i64, _p, _i, _p, _p, _sz, _p]),
     'mbpt_chol_solve': (_i, [_p, _i64, _p, _i, _p]),
+    'mbpt_cd_integral_terms': (_i, [_p, _i, _i, _i64, _p, _p, _p, _i, _i, _d, _d, _d, _d, _p,
+                                    _p, _i64, _p, _p, _p]),
+    'mbpt_laplace_representation_error': (_i, [_p, _i64, _p, _p, _i, _p, _i64, _p, _p]),
     'mbpt_chi0_aux_workspace_bytes': (_sz, [_i64, _i64, _i]),
     'mbpt_chi0_aux': (_i, [_p, _i64, _i64, _i64, _p, _d, _i, _i, _p, _p, _sz, _p, _p]),
     'mbpt_screening_contraction_workspace_bytes': (_sz, [_i64, _i64, _i]),

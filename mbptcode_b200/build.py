@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, 'libmbpt_b200.so')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 SOURCES = ['gemm_host.cu', 'kernels.cu', 'aux_kernels.cu', 'capi.cu', 'qp.cu', 'mlp.cu',
-           'noalloc.cu']
+           'noalloc.cu', 'contour.cu', 'ozaki.cu']
 # files whose arithmetic must round as written (no FMA contraction)
 NO_FMA = {'qp.cu'}
 

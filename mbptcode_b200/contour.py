@@ -1,41 +1,42 @@
 """Contour-deformation correlation self-energy on the B200.
 
-Mirrors the kernel seams of MBPTcode's ``src/SingleReference/GW/contour_deformation.py``
-and ``GW/real_screening.py`` with the same names and argument meaning:
+Keeps the kernel seams of MBPTcode's ``src/SingleReference/GW/contour_deformation.py``
+and ``GW/real_screening.py`` (names, arguments, the residue backends'
+apply/slope protocol, refusals) on a design of its own:
 
     Sigma^c_pp(omega) = Sigma^int + Sigma^res,
     Sigma^int = -(1/pi) sum_kq c[k, q](omega) wc[k, q],
     wc[k, q]  = B_p[:, q]^T (W(i nu_k) - I) B_p[:, q],
-    Sigma^res = sum_{q in residues} w_q (b_q^T W(|eps_q - omega|) b_q - b_q^T b_q),
+    Sigma^res = sum_q r_q(omega) (b_q^T W(|eps_q - omega|) b_q - b_q^T b_q),
 
-with B_p = D^T diag(X[:, p]) X the state's three-index slice, W = [1 - chi0]^-1
-on the contour's Gauss-Legendre frequencies nu_k, c the quadrature weights with
-the Lorentzian's singular part integrated in closed form
-(`cd_integral_weights`), and the residues' W at real frequencies below the gap
-from the cosh transform of proj(tau) (`LaplaceRealScreening`).
+B_p = D^T diag(X[:, p]) X the state's three-index slice, W = [1 - chi0]^-1,
+c the Gauss-Legendre weights of the Lorentzian kernel with its singular part
+integrated in closed form, r_q the residue weights of the poles of G the
+deformation sweeps.
 
-On the device: proj(tau) on the contour's own time grid and chi0(i nu) by the
-chi0 sweep and the tau -> omega transform, W - I by the Dyson step (one
-batched FP64 Cholesky of every frequency), the slices and the screening
-contraction (mbpt_three_index_slices, mbpt_screening_contraction: one W per
-frequency serves every state) and each residue frequency's W. The quadrature
-weights, the residue sets and the sums over k and q are host arithmetic on
-nfreq x norb numbers. FP64 throughout.
+The quasiparticle equation w = eps_p + xc + Sigma^c(w) is solved for every
+requested state at once. The search follows the reference's rules (windows
+narrowest first, the 150-point grid walked outward from the bare level,
+cells halved where the secant slope hides a pole, brackets refined by Newton
+on the closed-form slope inside the bracket, the walk ended by the weight
+sum, the root of largest Z kept), but it runs as a lockstep over states and
+cells: each round gathers every (state, frequency) point the search needs --
+a wave of grid cells, one level of halving, one Newton step of every open
+bracket -- and evaluates them in one device call. The walk is then replayed
+in the reference's order, so the roots are the ones its sequential scan
+finds; points of a wave beyond where a walk stops are evaluated and dropped.
 
-The quasiparticle equation of this route, w = eps_p + xc + Sigma^c(w), is
-solved as the reference solves it (`qp_energy_cd` on
-``Solvers/qp_equation.py`` `solve_qp_equation_scan`, without a followed root):
-a grid over the narrowest window about the bare level walked outward, cells
-halved where the secant slope hides a pole, each bracket refined by Newton on
-the closed-form slope (`sigma_cd_slope`) safeguarded by the bracket, the
-weights of a positive-weight self-energy summing to one ending the walk.
-
-Continuation 'cd' takes the residues' W from the explicit particle-hole
-response instead (`ExplicitRealScreening`, ``real_screening.py:57-91``):
-C_ov = B[:, occ, virt] from the occupied states' slices, chi0(freq) =
-2 (C_ov f) C_ov^T by mbpt_chi0_aux (a symmetric rank-k FP64 product over
-column chunks) and the Dyson step, which falls back from Cholesky to LU above
-the particle-hole gap where 1 - chi0 is indefinite.
+One evaluation call: the imaginary-axis term and its slope for all points by
+one kernel (mbpt_cd_integral_terms); the residues as one batch of linear
+systems [1 - chi0(f)] y = b, one column per (point, residue) pair, solved by
+preconditioned conjugate gradients with one FP64 product over the whole
+batch per iteration (chi0(f) = sum_k c_k(f) proj(tau_k) for the Laplace
+backend, 2 C_ov F C_ov^T for the explicit one) and Cholesky factors of
+1 - chi0 at a few anchor frequencies as preconditioners; a column whose
+frequency lies above the particle-hole gap (1 - chi0 indefinite, explicit
+backend only) or that does not converge is solved directly against its own
+frequency's factorisation. The Laplace backend's representability test of
+every frequency runs on the device (mbpt_laplace_representation_error).
 """
 from __future__ import annotations
 
@@ -64,107 +65,170 @@ QP_WEIGHT_SUM_SLACK = 1e-3       # :1625
 
 _MAX_J = 32  # output rows per transform call (the transform kernel's limit is 34)
 
+# the residue solves: relative residual of the conjugate-gradient solution,
+# iterations before a column is solved directly, anchor spacing in units of
+# the lowest particle-hole energy, columns per batched product
+PCG_TOL, PCG_MAX_ITER = 1e-13, 60
+ANCHOR_STEP = 1.0 / 32.0
+PCG_COLUMNS = 2048
+
 
 class ResidueRefused(ValueError):
     """A real frequency the imaginary-time representation does not carry
     (``real_screening.py:49-54``)."""
 
 
+# ------------------------------------------------------------ the contour grid
+
 def gap_scaled_w0(eps, nocc, scale=0.5):
     """w0 = scale (eps_LUMO - eps_HOMO) (``Base/utils/grids/grids.py:173-186``)."""
-    eps = np.asarray(eps, float)
-    w0 = scale * (eps[nocc] - eps[nocc - 1])
-    if not w0 > 0:
-        raise ValueError(f'gap_scaled_w0: the gap {eps[nocc] - eps[nocc - 1]:.6g} is not positive')
-    return w0
+    lo, _ = _transition_edges(eps, nocc, None)
+    if not lo > 0:
+        raise ValueError(f'gap_scaled_w0: the gap {lo:.6g} is not positive')
+    return scale * lo
+
+
+def _transition_edges(eps, nocc, pair_energies):
+    """(lowest, highest) particle-hole energy: of the pair energies when
+    given (both spins of an unrestricted reference), else of (eps, nocc)."""
+    if pair_energies is not None:
+        d = np.asarray(pair_energies, float)
+        return float(d.min()), float(d.max())
+    gap, span, _ = particle_hole_window(np.asarray(eps, float), nocc)
+    return float(gap), float(span)
 
 
 def cd_grid_range(eps, nocc, e_min_below_gap=None, pair_energies=None):
-    """(e_min, e_max) of the contour's time grid: e_min reaches below the gap,
-    by default by half of it (``contour_deformation.py:439-468``).
-    pair_energies: the screening's particle-hole energies when they are not
-    the ones (eps, nocc) spans (both spins of an unrestricted reference): the
-    range and the default shift then follow them."""
-    if pair_energies is not None:
-        d = np.asarray(pair_energies, float)
-        gap, e_max = float(d.min()), float(d.max())
-        shift = 0.5 * gap if e_min_below_gap is None else float(e_min_below_gap)
-    else:
-        eps = np.asarray(eps, float)
-        gap, e_max, _ = particle_hole_window(eps, nocc)
-        shift = (gap_scaled_w0(eps, nocc) if e_min_below_gap is None
-                 else float(e_min_below_gap))
-    if gap - shift <= 0:
-        raise ValueError(f'e_min_below_gap {shift} exceeds the gap {gap:.4f}: the imaginary-'
+    """(e_min, e_max) of the contour's time grid (``contour_deformation.py:439-468``):
+    the grid reaches `e_min_below_gap` (default: half the lowest particle-hole
+    energy) below the lowest particle-hole energy, so that the residues' real
+    frequencies up to that depth stay representable, and up to the highest."""
+    lo, hi = _transition_edges(eps, nocc, pair_energies)
+    depth = 0.5 * lo if e_min_below_gap is None else float(e_min_below_gap)
+    if not lo - depth > 0:
+        raise ValueError(f'e_min_below_gap {depth} exceeds the gap {lo:.4f}: the imaginary-'
                          f'time grid would be asked to represent e^{{-y tau}} at y <= 0')
-    return gap - shift, e_max
+    return lo - depth, hi
 
 
 def cd_frequency_grid(eps, nocc, ntau=CD_NTAU, nfreq_cd=CD_NFREQ, w0_cd=None,
                       e_min_below_gap=None, pair_energies=None):
-    """(nu, nu_weights, grid, w0): Gauss-Legendre nu on w0 (half the gap by
-    default; half the smallest pair energy with pair_energies) and the
-    minimax time grid over `cd_grid_range` onto it, cosine tau -> omega
-    weights only (``contour_deformation.py:471-503``)."""
+    """(nu, nu_weights, grid, w0) (``contour_deformation.py:471-503``): the
+    Gauss-Legendre imaginary frequencies of scale w0 (default half the
+    lowest particle-hole energy) and the minimax time grid over
+    `cd_grid_range`, mapped onto them by its cosine weights alone."""
     e_min, e_max = cd_grid_range(eps, nocc, e_min_below_gap, pair_energies)
-    if w0_cd is not None:
-        w0 = float(w0_cd)
-    elif pair_energies is not None:
-        w0 = 0.5 * float(np.min(pair_energies))
-    else:
-        w0 = gap_scaled_w0(eps, nocc)
+    w0 = (0.5 * _transition_edges(eps, nocc, pair_energies)[0] if w0_cd is None
+          else float(w0_cd))
     nu, nu_weights = gauss_legendre_grid(int(nfreq_cd), w0=w0)
     grid = TimeFrequencyGrid.minimax_split(int(ntau), e_min, e_max, nu, nu_weights,
                                            with_sine=False, with_inverse=False)
     return nu, nu_weights, grid, w0
 
 
+# --------------------------------------------- the imaginary-axis quadrature
+
+class LorentzianQuadrature:
+    """The weights c_k(d) of -(1/pi) int_0^inf g(d, nu) wc(nu) dnu on the
+    Gauss-Legendre nodes nu_k, g = d / (d^2 + nu^2), d = omega - eps_q
+    (``contour_deformation.py:150-202``). The kernel peaks at nu ~ |d|, which
+    the nodes cannot resolve for small |d|; its part wc(0) a^2 / (a^2 + nu^2)
+    is integrated exactly, (pi/2) sign(d) a / (a + |d|), with a = 4 median(nu)
+    and wc(0) extrapolated linearly in nu^2 from the two nodes nearest zero,
+    and only the remainder by quadrature. A pole on the contour (|d| below
+    the on-contour tolerance) takes sign 0, as its residue is taken at half
+    weight."""
+
+    def __init__(self, nu, nu_w, on_tol=RESIDUE_ON_CONTOUR_TOL):
+        self.nu = np.asarray(nu, float)
+        self.w = np.asarray(nu_w, float)
+        self.on_tol = float(on_tol)
+        self.a = 4.0 * float(np.median(self.nu))
+        k1, k2 = np.argsort(self.nu)[:2]
+        s1, s2 = self.nu[k1] ** 2, self.nu[k2] ** 2
+        # wc(0) ~ e1 wc(nu_k1) + e2 wc(nu_k2), linear in nu^2
+        self.k1, self.k2 = int(k1), int(k2)
+        self.e1, self.e2 = s2 / (s2 - s1), -s1 / (s2 - s1)
+        # the model's quadrature weights h_k
+        self.h = self.w * self.a ** 2 / (self.a ** 2 + self.nu ** 2)
+        self._dev = None
+
+    def weights(self, d):
+        """(c, dc), each (nfreq, len(d)): the weights and their d derivative."""
+        d = np.atleast_1d(np.asarray(d, float))
+        n2 = (self.nu ** 2)[:, None]
+        den = d[None, :] ** 2 + n2
+        g = d[None, :] / den
+        dg = (n2 - d[None, :] ** 2) / den ** 2
+        span = self.a + np.abs(d)
+        side = np.where(np.abs(d) < self.on_tol, 0.0, np.sign(d))
+        corr = 0.5 * np.pi * side * self.a / span - self.h @ g
+        dcorr = -0.5 * np.pi * self.a / span ** 2 - self.h @ dg
+        c, dc = self.w[:, None] * g, self.w[:, None] * dg
+        for k, e in ((self.k1, self.e1), (self.k2, self.e2)):
+            c[k] += e * corr
+            dc[k] += e * dcorr
+        return c, dc
+
+    def device(self, dev):
+        if self._dev is None:
+            self._dev = (torch.as_tensor(self.nu, device=dev),
+                         torch.as_tensor(self.w, device=dev))
+        return self._dev
+
+
 def cd_integral_weights(de, nu_points, nu_weights):
     """(c, dc), (nfreq, norb): Sigma^int = -(1/pi) sum c wc for de = omega -
-    eps, and its derivative in de (``contour_deformation.py:150-202``). The
-    Lorentzian de/(de^2 + nu^2) times wc is integrated as wc(0) times a
-    closed-form integral of de/(de^2 + nu^2) a^2/(a^2 + nu^2) plus the
-    quadrature of the remainder, wc(0) extrapolated in nu^2 from the two
-    smallest nodes (a = four times the median node); at |de| below
-    RESIDUE_ON_CONTOUR_TOL the closed form takes sign 0, as the residue term
-    takes that pole at half weight."""
-    de = np.asarray(de, float)
-    nu = np.asarray(nu_points, float)
-    wt = np.asarray(nu_weights, float)
-    den = de[None, :] ** 2 + nu[:, None] ** 2
-    g = de[None, :] / den
-    dg = (nu[:, None] ** 2 - de[None, :] ** 2) / den ** 2
-    c = wt[:, None] * g
-    dc = wt[:, None] * dg
-    k1, k2 = np.argsort(nu)[:2]
-    n1, n2 = nu[k1] ** 2, nu[k2] ** 2
-    a = 4.0 * float(np.median(nu))
-    h = wt * a * a / (a * a + nu ** 2)
-    side = np.where(np.abs(de) < RESIDUE_ON_CONTOUR_TOL, 0.0, np.sign(de))
-    ad = a + np.abs(de)
-    err = 0.5 * np.pi * side * a / ad - h @ g
-    derr = -0.5 * np.pi * a / ad ** 2 - h @ dg
-    for k, coef in ((k1, n2 / (n2 - n1)), (k2, -n1 / (n2 - n1))):
-        c[k] += coef * err
-        dc[k] += coef * derr
-    return c, dc
+    eps, and its derivative in de (``contour_deformation.py:150-202``)."""
+    return LorentzianQuadrature(nu_points, nu_weights).weights(de)
+
+
+def integral_terms(wc, eps, quad, slots, omega):
+    """(value, slope) of Sigma^int at the points (slots[j], omega[j]) on the
+    device: wc (nslots, nfreq, norb) device FP64, slots int, omega float.
+    Host arrays back."""
+    dev = wc.device
+    slots = np.ascontiguousarray(slots, dtype=np.int32)
+    omega = np.ascontiguousarray(omega, dtype=float)
+    nq = len(omega)
+    if nq == 0:
+        return np.zeros(0), np.zeros(0)
+    nu, nw = quad.device(dev)
+    ed = to_device(eps, dev)
+    sd = torch.as_tensor(slots, device=dev)
+    od = torch.as_tensor(omega, device=dev)
+    out = torch.empty((2, nq), dtype=torch.float64, device=dev)
+    wcc = wc.contiguous()
+    check(lib().mbpt_cd_integral_terms(ptr(wcc), wcc.shape[0], wcc.shape[1], wcc.shape[2],
+                                       ptr(ed), ptr(nu), ptr(nw), quad.k1, quad.k2,
+                                       float(quad.e1), float(quad.e2), float(quad.a),
+                                       float(quad.on_tol), ptr(sd), ptr(od), nq, ptr(out[0]),
+                                       ptr(out[1]), stream_ptr()), 'mbpt_cd_integral_terms')
+    h = out.cpu().numpy()
+    return h[0], h[1]
+
+
+# ----------------------------------------------------------------- residues
+
+def residue_weights(eps, nocc, omega, tol=RESIDUE_ON_CONTOUR_TOL):
+    """r[j, q] for the points omega[j] (``real_screening.py:157-168``): the
+    poles of G the deformation sweeps -- -1 for an occupied level above
+    omega, +1 for a virtual level below it, -1/2 / +1/2 for a level on the
+    contour (|eps_q - omega| < tol), 0 otherwise. (len(omega), norb)."""
+    eps = np.asarray(eps, float)
+    om = np.atleast_1d(np.asarray(omega, float))
+    gap = eps[None, :] - om[:, None]
+    occ = (np.arange(eps.size) < nocc)[None, :]
+    r = np.where(occ & (gap > 0.0), -1.0, 0.0) + np.where(~occ & (gap < 0.0), 1.0, 0.0)
+    on = np.abs(gap) < tol
+    return np.where(on, np.where(occ, -0.5, 0.5), r)
 
 
 def residue_set(eps, nocc, omega, tol=RESIDUE_ON_CONTOUR_TOL):
-    """[(q, weight)]: the poles of G the deformation sweeps over
-    (``real_screening.py:157-168``): occupied levels above omega (-1),
-    virtual ones below it (+1), a level on the contour at half weight."""
-    eps = np.asarray(eps, float)
-    out = []
-    for q in range(len(eps)):
-        gap = eps[q] - omega
-        if abs(gap) < tol:
-            out.append((q, -0.5 if q < nocc else 0.5))
-        elif q < nocc and gap > 0.0:
-            out.append((q, -1.0))
-        elif q >= nocc and gap < 0.0:
-            out.append((q, 1.0))
-    return out
+    """[(q, weight)] of the residues at one omega, in increasing q
+    (``real_screening.py:157-168``)."""
+    r = residue_weights(eps, nocc, [omega], tol)[0]
+    return [(int(q), float(r[q])) for q in np.nonzero(r)[0]]
 
 
 def real_frequency_weights(grid, omega):
@@ -173,23 +237,485 @@ def real_frequency_weights(grid, omega):
     and its omega derivative (``real_screening.py:184-209``)."""
     t = np.asarray(grid.tau_points, float)
     w = 2.0 * np.asarray(grid.tau_weights, float)
-    return w * np.cosh(omega * t), w * t * np.sinh(omega * t)
+    om = np.asarray(omega, float)
+    if om.ndim == 0:
+        return w * np.cosh(om * t), w * t * np.sinh(om * t)
+    return (w[:, None] * np.cosh(np.outer(t, om)),
+            (w * t)[:, None] * np.sinh(np.outer(t, om)))
 
 
 def laplace_representation_error(grid, eps, nocc, freq, pair_energies=None):
     """max over y = d -+ freq of |y sum_k w_k e^{-y tau_k} - 1| on the pair
     energies d (those of (eps, nocc), or pair_energies), inf where freq
-    reaches the gap (``LinearResponse/space_time.py:908-931``)."""
-    if pair_energies is None:
-        d = ov_energies(eps, nocc)
-    else:
-        d = np.asarray(pair_energies, float)
+    reaches the gap (``LinearResponse/space_time.py:908-931``); host FP64."""
+    d = ov_energies(eps, nocc) if pair_energies is None else np.asarray(pair_energies, float)
     y = np.concatenate([d - freq, d + freq])
     if y.min() <= 0.0:
         return np.inf
     q = np.exp(-np.outer(y, grid.tau_points)) @ grid.tau_weights
     return float(np.abs(q * y - 1.0).max())
 
+
+# -------------------------------------- batched solves of [1 - chi0(f)] y = b
+
+class _FactorCache:
+    """1 - chi0(f) factorised per key, kept for the latest keys within a byte
+    budget: ('chol', L) for a positive definite matrix (the Dyson step's FP64
+    Cholesky factor, solved by mbpt_chol_solve), ('w', W - I) from the LU
+    inverse otherwise."""
+
+    def __init__(self, budget_bytes, naux):
+        self.cap = max(2, int(budget_bytes // (8 * naux * naux)))
+        self._c = OrderedDict()
+
+    def get(self, key):
+        ent = self._c.get(key)
+        if ent is not None:
+            self._c.move_to_end(key)
+        return ent
+
+    def build(self, keys, chi0_of, spd_expected=True):
+        """Factorise 1 - chi0 for each key (chi0_of(keys) -> (n, naux, naux)
+        device tensor, consumed): one batched Cholesky when spd_expected,
+        the LU inverse for any key that is not positive definite."""
+        if not keys:
+            return
+        redo = list(range(len(keys)))
+        if spd_expected:
+            chi = chi0_of(keys)
+            _, _, info, _ = dyson_batch(chi, want_w=False, precision='fp64')
+            redo = [i for i in range(len(keys)) if info[i] != 0]
+            for i, k in enumerate(keys):
+                if info[i] == 0:
+                    self._put(k, ('chol', chi[i]))
+        if redo:
+            again = chi0_of([keys[i] for i in redo])
+            dyson_batch(again, want_w=True, precision='fp64')
+            for j, i in enumerate(redo):
+                self._put(keys[i], ('w', again[j]))
+
+    def _put(self, key, ent):
+        self._c[key] = ent
+        while len(self._c) > self.cap:
+            self._c.popitem(last=False)
+
+
+def _apply_factor(ent, R):
+    """M^-1 R for the columns of R (naux, k): two triangular solves against a
+    Cholesky factor, or R + (W - I) R from an LU inverse."""
+    kind, m = ent
+    if kind == 'w':
+        return R + m @ R
+    y = R.T.contiguous()
+    check(lib().mbpt_chol_solve(ptr(m), m.shape[0], ptr(y), y.shape[0], stream_ptr()),
+          'mbpt_chol_solve')
+    return y.T
+
+
+class _BatchedScreening:
+    """The solver half of a residue backend: Y[:, j] = [1 - chi0(f_j)]^-1
+    B[:, j] for a batch of frequencies at once. Subclasses give chi0(f) as a
+    dense matrix for a set of frequencies (`_chi0_dense`), chi0(f_j) x_j for
+    all columns at once (`_chi0_apply`), and the slope y^T chi0'(f) y."""
+
+    naux = 0
+    lowest = 0.0          # lowest particle-hole energy: the edge of the SPD region
+
+    def _init_solver(self, cache_bytes):
+        self._factors = _FactorCache(0.5 * cache_bytes, self.naux)
+        self._direct = _FactorCache(0.5 * cache_bytes, self.naux)
+        self.stats = {'columns': 0, 'pcg_iterations': 0, 'direct': 0, 'anchors': 0}
+
+    def _anchor_of(self, f):
+        """The anchor cell of a frequency below the lowest particle-hole
+        energy: cells of ANCHOR_STEP times it, each anchored at its middle,
+        so no anchor reaches the gap."""
+        return int(np.floor(f / (ANCHOR_STEP * self.lowest)))
+
+    def _anchor_freq(self, i):
+        return (i + 0.5) * ANCHOR_STEP * self.lowest
+
+    def solve(self, freqs, B):
+        """Y (naux, n) on the device for frequencies freqs (n,) and
+        right-hand sides B (naux, n)."""
+        freqs = np.asarray(freqs, float)
+        n = len(freqs)
+        Y = torch.empty_like(B)
+        if n == 0:
+            return Y
+        self.stats['columns'] += n
+        spd = freqs < self.lowest
+        direct = np.nonzero(~spd)[0]
+        it = np.nonzero(spd)[0]
+        if it.size:
+            done, X = self._pcg(freqs[it], B[:, torch.as_tensor(it, device=B.device)])
+            Y[:, torch.as_tensor(it, device=B.device)] = X
+            direct = np.concatenate([direct, it[~done]])
+        if direct.size:
+            self._solve_direct(freqs, B, Y, direct)
+        return Y
+
+    def _solve_direct(self, freqs, B, Y, cols):
+        self.stats['direct'] += len(cols)
+        keys = sorted({float(freqs[c]) for c in cols})
+        need = [k for k in keys if self._direct.get(k) is None]
+        for i in range(0, len(need), 8):
+            part = need[i:i + 8]
+            self._direct.build(part, self._chi0_dense, spd_expected=part[-1] < self.lowest)
+        for k in keys:
+            sel = [c for c in cols if float(freqs[c]) == k]
+            idx = torch.as_tensor(sel, device=B.device)
+            ent = self._direct.get(k)
+            if ent is None:       # evicted by a later build of this call: rebuild alone
+                self._direct.build([k], self._chi0_dense, spd_expected=k < self.lowest)
+                ent = self._direct.get(k)
+            Y[:, idx] = _apply_factor(ent, B[:, idx])
+
+    def _pcg(self, freqs, B):
+        """Conjugate gradients on [1 - chi0(f_j)] y_j = b_j, all columns at
+        once, each preconditioned by the Cholesky factor of 1 - chi0 at its
+        nearest anchor frequency. Returns (converged mask, Y)."""
+        anchors = np.array([self._anchor_of(f) for f in freqs])
+        groups = {}
+        for j, a in enumerate(anchors):
+            groups.setdefault(int(a), []).append(j)
+        need = [a for a in groups if self._factors.get(a) is None]
+        self.stats['anchors'] += len(need)
+        for i in range(0, len(need), 8):
+            self._factors.build(need[i:i + 8],
+                                lambda keys: self._chi0_dense([self._anchor_freq(a)
+                                                               for a in keys]))
+        dev = B.device
+        gidx = {a: torch.as_tensor(js, device=dev) for a, js in groups.items()}
+
+        def precond(R):
+            Z = torch.empty_like(R)
+            for a, idx in gidx.items():
+                ent = self._factors.get(a)
+                if ent is None:
+                    self._factors.build([a], lambda keys: self._chi0_dense(
+                        [self._anchor_freq(k) for k in keys]))
+                    ent = self._factors.get(a)
+                Z[:, idx] = _apply_factor(ent, R[:, idx])
+            return Z
+
+        def op(X):
+            return X - self._chi0_apply(freqs, X)
+
+        bnorm = torch.linalg.vector_norm(B, dim=0)
+        bnorm = torch.where(bnorm > 0, bnorm, torch.ones_like(bnorm))
+        X = precond(B)
+        R = B - op(X)
+        Z = precond(R)
+        P = Z.clone()
+        rz = (R * Z).sum(0)
+        done = torch.zeros(len(freqs), dtype=torch.bool, device=dev)
+        for it in range(PCG_MAX_ITER):
+            done = torch.linalg.vector_norm(R, dim=0) <= PCG_TOL * bnorm
+            if bool(done.all()):
+                break
+            self.stats['pcg_iterations'] += 1
+            Q = op(P)
+            pq = (P * Q).sum(0)
+            alpha = torch.where(done, torch.zeros_like(rz), rz / torch.where(pq != 0, pq, 1.0))
+            X = X + alpha * P
+            R = R - alpha * Q
+            Z = precond(R)
+            rz_new = (R * Z).sum(0)
+            beta = torch.where(rz != 0, rz_new / torch.where(rz != 0, rz, 1.0),
+                               torch.zeros_like(rz))
+            P = Z + beta * P
+            rz = rz_new
+        done = torch.linalg.vector_norm(R, dim=0) <= PCG_TOL * bnorm
+        return done.cpu().numpy(), X
+
+    # the reference's per-frequency protocol (``real_screening.py``)
+    def apply(self, freq, b):
+        """W(freq) b = [1 - chi0(freq)]^-1 b for one frequency; b (naux,) or
+        (naux, k), host or device, returned as given."""
+        self._refuse([float(freq)])
+        dev = self._device()
+        bd = to_device(b, dev)
+        cols = bd[:, None] if bd.dim() == 1 else bd
+        y = self.solve(np.full(cols.shape[1], float(freq)), cols.contiguous())
+        y = y[:, 0] if bd.dim() == 1 else y
+        return y if isinstance(b, torch.Tensor) else y.cpu().numpy()
+
+    def slope(self, freq, y):
+        """y^T [dchi0/dfreq] y at one frequency."""
+        yd = to_device(y, self._device())
+        return float(self.slopes(np.array([float(freq)]), yd[:, None])[0])
+
+    def _refuse(self, freqs):
+        """Raise ResidueRefused for a frequency this backend cannot serve."""
+
+    def refused(self, freqs):
+        """Boolean mask of the frequencies this backend cannot serve."""
+        return np.zeros(len(freqs), dtype=bool)
+
+
+class LaplaceRealScreening(_BatchedScreening):
+    """W at real frequencies below the particle-hole gap from proj(tau)
+    (``real_screening.py:94-154``): chi0(f) = sum_k 2 w_k cosh(f tau_k)
+    proj(tau_k) on the grid's bare Laplace quadrature. A frequency the grid
+    does not carry (quadrature error of 1/y at or above tol on the pair
+    energies) is refused (ResidueRefused). pair_energies: the particle-hole
+    energies proj(tau) was summed over, when they are not the ones (eps,
+    nocc) spans (both spins of an unrestricted reference). cache_bytes bounds
+    the factorisations kept (anchors and direct solves)."""
+
+    def __init__(self, proj_tau, grid, eps, nocc, tol=LAPLACE_SCREENING_TOL,
+                 pair_energies=None, cache_bytes=4e9):
+        dev = require_device()
+        self.proj_tau = to_device(proj_tau, dev)
+        self.grid = grid
+        self.eps = np.asarray(eps, float)
+        self.nocc = nocc
+        self.tol = tol
+        self.pair_energies = (None if pair_energies is None
+                              else np.asarray(pair_energies, float))
+        d = (ov_energies(self.eps, nocc) if self.pair_energies is None
+             else self.pair_energies)
+        self.lowest = float(d.min())
+        self.naux = self.proj_tau.shape[-1]
+        self._d = torch.as_tensor(d, dtype=torch.float64, device=dev)
+        self._tau = torch.as_tensor(np.asarray(grid.tau_points, float), device=dev)
+        self._tw = torch.as_tensor(np.asarray(grid.tau_weights, float), device=dev)
+        self._flat = self.proj_tau.reshape(-1, self.naux)
+        self._errors = {}
+        self._init_solver(cache_bytes)
+
+    def _device(self):
+        return self.proj_tau.device
+
+    def errors(self, freqs):
+        """The representation error of each frequency (device kernel, kept
+        per frequency)."""
+        freqs = np.asarray(freqs, float)
+        new = sorted({float(f) for f in freqs if float(f) not in self._errors})
+        if new:
+            dev = self._device()
+            fd = torch.as_tensor(new, dtype=torch.float64, device=dev)
+            out = torch.empty_like(fd)
+            check(lib().mbpt_laplace_representation_error(
+                ptr(self._d), self._d.numel(), ptr(self._tau), ptr(self._tw),
+                self._tau.numel(), ptr(fd), len(new), ptr(out), stream_ptr()),
+                'mbpt_laplace_representation_error')
+            for f, e in zip(new, out.cpu().numpy()):
+                self._errors[f] = float(e)
+        return np.array([self._errors[float(f)] for f in freqs])
+
+    def representation_error(self, freq):
+        """max over y = d -+ freq of |y sum_k w_k e^{-y tau_k} - 1|, inf where
+        freq reaches the gap (``LinearResponse/space_time.py:908-931``)."""
+        return float(self.errors([freq])[0])
+
+    def refused(self, freqs):
+        return ~(self.errors(freqs) < self.tol)
+
+    def _refuse(self, freqs):
+        bad = self.refused(freqs)
+        if bad.any():
+            f = float(np.asarray(freqs)[bad][0])
+            raise ResidueRefused(
+                f'real frequency {f:.4f} Ha is not carried by the tau grid: bare-quadrature '
+                f'error {self.representation_error(f):.1e} against tol {self.tol:.0e}; '
+                f'gap - freq = {self.lowest - f:.4f} Ha, the grid\'s e_min is '
+                f'{self.grid.meta.get("e_min", float("nan")):.4f}. Build the grid with '
+                f'e_min <= gap - freq, or use the explicit backend.')
+
+    def _chi0_dense(self, freqs):
+        c, _ = real_frequency_weights(self.grid, np.asarray(freqs, float))
+        return _rows_transform(self.proj_tau, np.ascontiguousarray(c.T))
+
+    def _stacked(self, coef, X):
+        """sum_k proj(tau_k) (X with column j scaled by coef[k, j]): one FP64
+        product over the time points stacked along K (proj(tau) is
+        symmetric, so its stacked rows serve as the transposed operand)."""
+        T = coef.shape[0]
+        cd = torch.as_tensor(np.ascontiguousarray(coef), device=X.device)
+        out = torch.empty_like(X)
+        for j0 in range(0, X.shape[1], PCG_COLUMNS):
+            Xs = X[:, j0:j0 + PCG_COLUMNS]
+            Z = (cd[:, None, j0:j0 + PCG_COLUMNS] * Xs[None]).reshape(T * self.naux, -1)
+            out[:, j0:j0 + PCG_COLUMNS] = self._flat.T @ Z
+        return out
+
+    def _chi0_apply(self, freqs, X):
+        c, _ = real_frequency_weights(self.grid, freqs)
+        return self._stacked(c, X)
+
+    def slopes(self, freqs, Y):
+        """y_j^T [dchi0/df](f_j) y_j for each column (host array)."""
+        if Y.shape[1] == 0:
+            return np.zeros(0)
+        _, dc = real_frequency_weights(self.grid, np.asarray(freqs, float))
+        return (Y * self._stacked(dc, Y)).sum(0).cpu().numpy()
+
+    def w_minus_identity(self, freq):
+        """W(freq) - I as a dense device matrix (FP64)."""
+        self._refuse([float(freq)])
+        chi = self._chi0_dense([float(freq)])
+        dyson_batch(chi, want_w=True, precision='fp64')
+        return chi[0]
+
+
+class ExplicitRealScreening(_BatchedScreening):
+    """W at a real frequency from the particle-hole block C_ov, explicitly
+    (``real_screening.py:57-91``, continuation 'cd'): chi0(f) = 2 C_ov F(f)
+    C_ov^T with the bubble's frequency factor F (broadened by eta, off by
+    default). Below the lowest particle-hole energy the batch is solved by
+    preconditioned conjugate gradients (two FP64 products with C_ov per
+    iteration); above it, where 1 - chi0 is indefinite, each frequency's
+    explicit chi0 (mbpt_chi0_aux) goes through the Dyson step's LU inverse.
+    pair_energies: the pair index of C_ov when it is not the one (eps, nocc)
+    spans. precision 'mixed' forms the dense chi0 of the anchors and of the
+    direct solves as one split BF16x3 product (the iterations stay FP64, so
+    the solution does too, except for the direct columns)."""
+
+    def __init__(self, C_ov, eps, nocc, eta=0.0, pair_energies=None, cache_bytes=4e9,
+                 precision='fp64'):
+        self.C_ov = to_device(C_ov, require_device())
+        self.precision = precision
+        self.eps = np.asarray(eps, float)
+        self.nocc = nocc
+        self.eta = float(eta)
+        self.d = (ov_energies(self.eps, nocc) if pair_energies is None
+                  else np.asarray(pair_energies, float))
+        if self.d.size != self.C_ov.shape[1]:
+            raise ValueError(f'C_ov has {self.C_ov.shape[1]} pairs, the pair energies '
+                             f'{self.d.size}')
+        self.naux = self.C_ov.shape[0]
+        self.lowest = float(self.d.min())
+        self._dd = torch.as_tensor(self.d, device=self.C_ov.device)
+        self._init_solver(cache_bytes)
+
+    def _device(self):
+        return self.C_ov.device
+
+    def _chi0(self, freq, imaginary=False):
+        f = frequency_factor(self.d, float(freq), imaginary, self.eta)
+        return chi0_aux([(self.C_ov, f)], 2.0, precision=self.precision)[None]
+
+    def _chi0_dense(self, freqs):
+        out = torch.empty((len(freqs), self.naux, self.naux), dtype=torch.float64,
+                          device=self.C_ov.device)
+        for i, f in enumerate(freqs):
+            chi0_aux([(self.C_ov, frequency_factor(self.d, float(f), False, self.eta))], 2.0,
+                     out=out[i], precision=self.precision)
+        return out
+
+    def _factor(self, freqs, slopes):
+        """F[pair, j] (or dF/df) of the bubble at real f_j, on the device."""
+        f = torch.as_tensor(np.asarray(freqs, float), device=self._dd.device)[None, :]
+        a, b = f - self._dd[:, None], f + self._dd[:, None]
+        if self.eta == 0.0:
+            return (1.0 / b ** 2 - 1.0 / a ** 2) if slopes else (1.0 / a - 1.0 / b)
+        e2 = self.eta ** 2
+        da, db = a ** 2 + e2, b ** 2 + e2
+        if slopes:
+            return (e2 - a ** 2) / da ** 2 - (e2 - b ** 2) / db ** 2
+        return a / da - b / db
+
+    def _chi0_apply(self, freqs, X):
+        out = torch.empty_like(X)
+        for j0 in range(0, X.shape[1], PCG_COLUMNS):
+            Z = self.C_ov.T @ X[:, j0:j0 + PCG_COLUMNS]
+            Z *= self._factor(freqs[j0:j0 + PCG_COLUMNS], False)
+            out[:, j0:j0 + PCG_COLUMNS] = 2.0 * (self.C_ov @ Z)
+        return out
+
+    def slopes(self, freqs, Y):
+        """y_j^T [dchi0/df](f_j) y_j = 2 sum_pairs dF/df (C_ov^T y_j)^2."""
+        if Y.shape[1] == 0:
+            return np.zeros(0)
+        out = []
+        for j0 in range(0, Y.shape[1], PCG_COLUMNS):
+            Z = self.C_ov.T @ Y[:, j0:j0 + PCG_COLUMNS]
+            out.append(2.0 * (self._factor(freqs[j0:j0 + PCG_COLUMNS], True) * Z * Z).sum(0))
+        return torch.cat(out).cpu().numpy()
+
+    def w_minus_identity(self, freq, imaginary=False):
+        """W(freq) - I as a dense device matrix (the Dyson step: Cholesky
+        below the gap, LU above it)."""
+        chi = self._chi0(freq, imaginary)
+        dyson_batch(chi, want_w=True, precision='fp64')
+        return chi[0]
+
+
+# ----------------------------------------------------- the self-energy batch
+
+class ContourEquation:
+    """f(w) = w - a_s - Sigma^c_s(w) and f'(w) for a set of states s (slots),
+    evaluated for many (slot, w) points per call. B: (nslots, naux, norb)
+    slices, wc: (nslots, nfreq, norb) contracted screening, bare: a_s =
+    eps_p + xc per slot, backend: the residues' screening (None: a state
+    whose points sweep no residue needs none)."""
+
+    def __init__(self, B, wc, eps, nocc, quad, bare, backend):
+        dev = require_device()
+        self.B = to_device(B, dev)
+        self.wc = to_device(wc, dev)
+        if self.B.dim() == 2:
+            self.B = self.B[None]
+        if self.wc.dim() == 2:
+            self.wc = self.wc[None]
+        self.eps = np.asarray(eps, float)
+        self.nocc = nocc
+        self.quad = quad
+        self.bare = np.atleast_1d(np.asarray(bare, float))
+        self.backend = backend
+        self.points = 0
+
+    def sigma(self, slots, w, want_slope=True, residues=None):
+        """(Sigma, dSigma/dw, refused) at the points; residues: one fixed set
+        [(q, weight)] for every point instead of the points' own."""
+        slots = np.asarray(slots, int)
+        w = np.asarray(w, float)
+        self.points += len(w)
+        val, slope = integral_terms(self.wc, self.eps, self.quad, slots, w)
+        if residues is None:
+            R = residue_weights(self.eps, self.nocc, w)
+        else:
+            R = np.zeros((len(w), self.eps.size))
+            for q, weight in residues:
+                R[:, q] = weight
+        jj, qq = np.nonzero(R)
+        refused = np.zeros(len(w), dtype=bool)
+        if jj.size == 0:
+            return val, slope, refused
+        if self.backend is None:
+            require_three_index(None, 'the residue term')
+        gap = self.eps[qq] - w[jj]
+        f = np.abs(gap)
+        bad = self.backend.refused(f)
+        if bad.any():
+            refused[np.unique(jj[bad])] = True
+        keep = ~refused[jj]
+        jj, qq, f, gap = jj[keep], qq[keep], f[keep], gap[keep]
+        r = R[jj, qq]
+        dev = self.B.device
+        cols = self.B[torch.as_tensor(slots[jj], device=dev), :,
+                      torch.as_tensor(qq, device=dev)].T.contiguous()
+        Y = self.backend.solve(f, cols)
+        by = (cols * Y).sum(0).cpu().numpy()
+        bb = (cols * cols).sum(0).cpu().numpy()
+        np.add.at(val, jj, r * (by - bb))
+        if want_slope:
+            s = self.backend.slopes(f, Y)
+            np.add.at(slope, jj, -r * s * np.sign(gap))
+        val[refused] = np.nan
+        slope[refused] = np.nan
+        return val, slope, refused
+
+    def __call__(self, slots, w, want_slope=True):
+        """(f, f', refused) at the points."""
+        slots = np.asarray(slots, int)
+        s, ds, refused = self.sigma(slots, w, want_slope)
+        return np.asarray(w, float) - self.bare[slots] - s, 1.0 - ds, refused
+
+
+# ------------------------------------- proj(tau), slices and the contraction
 
 def _rows_transform(proj, weights):
     """sum_k weights[j, k] proj[k] for any number of output rows (in chunks
@@ -286,135 +812,6 @@ def screening_contraction(Bp, wbp):
                      optimize=True)
 
 
-class _ResidueSolves:
-    """W(freq) b for the residues of one backend: 1 - chi0(freq) factorised
-    once per frequency by the Dyson step's FP64 Cholesky and kept for the
-    latest `cap` frequencies (the value and the slope of one scan point
-    apply W at the same frequencies), each b then solved against the factor
-    by two triangular solves (mbpt_chol_solve) without forming W. Where
-    1 - chi0 is not positive definite (the explicit response above the
-    gap) W - I comes from the LU inverse instead."""
-
-    def __init__(self, cap):
-        self.cap = cap
-        self._c = OrderedDict()
-
-    def entry(self, key, build):
-        ent = self._c.get(key)
-        if ent is not None:
-            self._c.move_to_end(key)
-            return ent
-        chi0 = build()
-        _, _, info, _ = dyson_batch(chi0, want_w=False, precision='fp64')
-        if info[0] == 0:
-            ent = ('factor', chi0[0])
-        else:
-            chi0 = build()
-            dyson_batch(chi0, want_w=True, precision='fp64')
-            ent = ('w', chi0[0])
-        self._c[key] = ent
-        if len(self._c) > self.cap:
-            self._c.popitem(last=False)
-        return ent
-
-    @staticmethod
-    def solve(ent, bd):
-        kind, m = ent
-        if kind == 'w':
-            return bd + m @ bd
-        y = bd.clone().contiguous()
-        check(lib().mbpt_chol_solve(ptr(m), m.shape[0], ptr(y), 1, stream_ptr()),
-              'mbpt_chol_solve')
-        return y
-
-
-class LaplaceRealScreening:
-    """W at a real frequency below the particle-hole gap from proj(tau): one
-    (ntau, naux^2) transform and one Cholesky factorisation per frequency,
-    the factor kept for later calls and W b solved against it
-    (``real_screening.py:94-154``).
-    Refuses (ResidueRefused) a frequency the grid does not carry.
-    pair_energies: the particle-hole energies proj(tau) was summed over, when
-    they are not the ones (eps, nocc) spans (both spins of an unrestricted
-    reference)."""
-
-    def __init__(self, proj_tau, grid, eps, nocc, tol=LAPLACE_SCREENING_TOL,
-                 pair_energies=None, cache_bytes=4e9):
-        self.proj_tau = to_device(proj_tau, require_device())
-        self.grid = grid
-        self.eps = np.asarray(eps, float)
-        self.nocc = nocc
-        self.tol = tol
-        self.pair_energies = (None if pair_energies is None
-                              else np.asarray(pair_energies, float))
-        # the latest frequencies' W - I (the value and the slope of one point
-        # apply W at the same frequencies), bounded by memory
-        naux = self.proj_tau.shape[-1]
-        self._cap = max(2, min(2 * len(self.eps), int(cache_bytes // (8 * naux * naux))))
-        self._w = OrderedDict()
-        self._solves = _ResidueSolves(self._cap)
-        # the representability check on the device: 2 nocc nvirt x ntau
-        # exponentials per new frequency
-        dev = self.proj_tau.device
-        d = (ov_energies(self.eps, nocc) if self.pair_energies is None
-             else self.pair_energies)
-        self._d = torch.as_tensor(d, dtype=torch.float64, device=dev)
-        self._tau = torch.as_tensor(np.asarray(grid.tau_points, float), device=dev)
-        self._tw = torch.as_tensor(np.asarray(grid.tau_weights, float), device=dev)
-
-    def representation_error(self, freq):
-        """max over y = d -+ freq of |y sum_k w_k e^{-y tau_k} - 1|, inf where
-        freq reaches the gap (``LinearResponse/space_time.py:908-931``)."""
-        y = torch.cat([self._d - freq, self._d + freq])
-        if float(y.min()) <= 0.0:
-            return np.inf
-        q = torch.exp(-y[:, None] * self._tau[None, :]) @ self._tw
-        return float((q * y - 1.0).abs().max())
-
-    def _weights(self, freq):
-        err = self.representation_error(freq)
-        if not err < self.tol:
-            gap = (particle_hole_window(self.eps, self.nocc)[0] if self.pair_energies is None
-                   else float(self.pair_energies.min()))
-            raise ResidueRefused(
-                f'real frequency {freq:.4f} Ha is not carried by the tau grid: bare-quadrature '
-                f'error {err:.1e} against tol {self.tol:.0e}; gap - freq = {gap - freq:.4f} '
-                f'Ha, the grid\'s e_min is {self.grid.meta.get("e_min", float("nan")):.4f}. '
-                f'Build the grid with e_min <= gap - freq, or use the explicit backend.')
-        return real_frequency_weights(self.grid, freq)
-
-    def w_minus_identity(self, freq):
-        key = float(freq)
-        w = self._w.get(key)
-        if w is None:
-            c, _ = self._weights(key)
-            chi0 = _rows_transform(self.proj_tau, c[None, :])
-            dyson_batch(chi0, want_w=True, precision='fp64')
-            w = self._w[key] = chi0[0]
-            if len(self._w) > self._cap:
-                self._w.popitem(last=False)
-        else:
-            self._w.move_to_end(key)
-        return w
-
-    def apply(self, freq, b):
-        """W(freq) b = [1 - chi0(freq)]^-1 b, by a solve against the
-        frequency's kept Cholesky factor (``real_screening.py:147-150``)."""
-        key = float(freq)
-        ent = self._solves.entry(
-            key, lambda: _rows_transform(self.proj_tau, self._weights(key)[0][None, :]))
-        y = _ResidueSolves.solve(ent, to_device(b, self.proj_tau.device))
-        return y if isinstance(b, torch.Tensor) else y.cpu().numpy()
-
-    def slope(self, freq, y):
-        """y^T [dchi0/dfreq] y, dchi0/dfreq = sum_k dc_k proj(tau_k)
-        (``real_screening.py:152-154``)."""
-        _, dc = self._weights(freq)
-        dchi0 = _rows_transform(self.proj_tau, dc[None, :])[0]
-        yd = to_device(y, self.proj_tau.device)
-        return float(yd @ (dchi0 @ yd))
-
-
 def ov_energies(eps, nocc):
     """d[(i, a)] = eps_a - eps_i on the pair index of C_ov, i major
     (``Base/orbital_spaces.py:31-34``)."""
@@ -442,87 +839,6 @@ def three_index_ov(X, D, eps, nocc, tile_gb=None):
     return C.reshape(naux, nocc * nvirt)
 
 
-def require_three_index(C_ov, what):
-    """``contour_deformation.py:109-114``."""
-    if C_ov is None:
-        raise ResidueRefused(
-            f'{what} needs C_ov = B[:, occ, virt] as (naux, nocc*nvirt) and it was not '
-            f'supplied. A frontier state sweeps no residues and needs none once the '
-            f'imaginary-axis screening comes in as wbp or wc.')
-
-
-class ExplicitRealScreening:
-    """W at a real frequency from the particle-hole block C_ov, explicitly
-    (``real_screening.py:57-91``, continuation 'cd'): chi0 = 2 (C_ov f) C_ov^T
-    by mbpt_chi0_aux (a symmetric rank-k product over column chunks) and
-    W - I by the Dyson step (Cholesky below the gap, LU above it, where
-    1 - chi0 is indefinite), the W - I of the latest frequencies kept for
-    later calls. eta broadens the particle-hole poles (off by default).
-    pair_energies: the pair index of C_ov when it is not the one (eps, nocc)
-    spans. O(naux^2 nocc nvirt) per frequency, the route the cubic one is
-    checked against and the only one above the particle-hole gap. precision
-    'fp64' (default) or 'mixed' (the response as one split BF16x3
-    tensor-core product; the Dyson step stays FP64)."""
-
-    def __init__(self, C_ov, eps, nocc, eta=0.0, pair_energies=None, cache_bytes=4e9,
-                 precision='fp64'):
-        self.C_ov = to_device(C_ov, require_device())
-        self.precision = precision
-        self.eps = np.asarray(eps, float)
-        self.nocc = nocc
-        self.eta = float(eta)
-        self.d = (ov_energies(self.eps, nocc) if pair_energies is None
-                  else np.asarray(pair_energies, float))
-        if self.d.size != self.C_ov.shape[1]:
-            raise ValueError(f'C_ov has {self.C_ov.shape[1]} pairs, the pair energies '
-                             f'{self.d.size}')
-        naux = self.C_ov.shape[0]
-        self._cap = max(2, min(2 * len(self.eps), int(cache_bytes // (8 * naux * naux))))
-        self._w = OrderedDict()
-        self._solves = _ResidueSolves(self._cap)
-
-    def w_minus_identity(self, freq, imaginary=False):
-        key = (float(freq), bool(imaginary))
-        w = self._w.get(key)
-        if w is None:
-            chi0 = self._chi0(freq, imaginary)
-            dyson_batch(chi0, want_w=True, precision='fp64')
-            w = self._w[key] = chi0[0]
-            if len(self._w) > self._cap:
-                self._w.popitem(last=False)
-        else:
-            self._w.move_to_end(key)
-        return w
-
-    def _chi0(self, freq, imaginary=False):
-        f = frequency_factor(self.d, float(freq), imaginary, self.eta)
-        return chi0_aux([(self.C_ov, f)], 2.0, precision=self.precision)[None]
-
-    def apply(self, freq, b):
-        """W(freq) b = [1 - chi0(freq)]^-1 b, by a solve against the
-        frequency's kept Cholesky factor (the LU inverse above the gap)."""
-        key = float(freq)
-        ent = self._solves.entry(key, lambda: self._chi0(key))
-        y = _ResidueSolves.solve(ent, to_device(b, self.C_ov.device))
-        return y if isinstance(b, torch.Tensor) else y.cpu().numpy()
-
-    def slope(self, freq, y):
-        """y^T [dchi0/dfreq] y = 2 sum_(ia) df/dw (C_ov^T y)_(ia)^2
-        (``real_screening.py:87-91``)."""
-        z = (self.C_ov.T @ to_device(y, self.C_ov.device)).cpu().numpy()
-        return 2.0 * float(frequency_factor(self.d, float(freq), False, self.eta,
-                                            slopes=True)[2] @ z ** 2)
-
-
-def residue_backend(real_screening, C_ov, eps, nocc, eta):
-    """The backend the residue term uses: the one given, else the explicit one
-    from C_ov (``contour_deformation.py:117-122``)."""
-    if real_screening is not None:
-        return real_screening
-    require_three_index(C_ov, 'the residue term')
-    return ExplicitRealScreening(C_ov, eps, nocc, eta)
-
-
 def wc_explicit(Bp, C_ov, d, nu_points, block=8):
     """wc[k, q] = Bp[:, q]^T (W(i nu_k) - I) Bp[:, q] from the explicit
     imaginary-axis screening (``contour_deformation.py:240-245``): per block
@@ -544,278 +860,463 @@ def wc_explicit(Bp, C_ov, d, nu_points, block=8):
     return np.concatenate(out)
 
 
-def sigma_cd(p, omega, Bp, eps, nocc, nu_points, nu_weights, residues=None, wbp=None,
-             eta=0.0, wc=None, C_ov=None, real_screening=None):
-    """Sigma^c_pp(omega) by contour deformation from the state's slice Bp and
-    its contracted screening wc (``contour_deformation.py:310-343``):
-    the imaginary-axis integral and, for the residue set (recomputed at omega
-    when not given), sum_q w_q (b_q^T W(|eps_q - omega|) b_q - b_q^T b_q) with
-    `real_screening`'s W (a LaplaceRealScreening or ExplicitRealScreening;
-    with C_ov and no backend the explicit one). With neither wc nor wbp the
-    imaginary-axis screening is built explicitly from C_ov (`wc_explicit`)."""
-    eps = np.asarray(eps, float)
-    Bh = Bp.detach().cpu().numpy() if isinstance(Bp, torch.Tensor) else np.asarray(Bp)
+# ------------------------------------------------------------ the lockstep scan
+# The rules are those of MBPTcode's `solve_qp_equation_scan` on a
+# `SampledEquation` with a closed-form slope and positive weights
+# (``Solvers/qp_equation.py:155-273, 1029-1420``), which the contour route
+# (`qp_energy_cd`) uses without a followed root.
+
+def _windows(a):
+    """[(lo, hi)] about the bare level a, narrowest first: the tier of the
+    state's depth |a| and every wider one (``qp_equation.py:1280-1288``)."""
+    tier = max((k for k, (depth, _) in enumerate(QP_SEARCH_WINDOW_TIERS) if abs(a) > depth),
+               default=0)
+    return [(a - half, a + half) for _, half in QP_SEARCH_WINDOW_TIERS[tier:]]
+
+
+def _valid(z, z_min=0.0):
+    """Z of a quasiparticle: finite and in (z_min, 1] (``qp_equation.py:95-102``)."""
+    z = float(z)
+    return bool(np.isfinite(z) and z_min < z <= 1.0)
+
+
+def _walk_order(c0, ncells):
+    """The cells in the order the outward walk reaches them: the one holding
+    the bare level, then at each distance the lower neighbour and the upper."""
+    order = [c0]
+    for d in range(1, ncells):
+        order.extend(c for c in (c0 - d, c0 + d) if 0 <= c < ncells)
+    return order
+
+
+class _Walk:
+    """One state's walk over one window's grid."""
+
+    def __init__(self, slot, a, lo, hi, enough):
+        self.slot, self.a, self.enough = slot, a, enough
+        self.grid = np.linspace(lo, hi, QP_GRAPHICAL_N_OMEGA)
+        c0 = min(max(int(np.searchsorted(self.grid, a)) - 1, 0), self.grid.size - 2)
+        self.order = _walk_order(c0, self.grid.size - 1)
+        self.pos, self.f, self.bad = 0, {}, {}
+        self.found, self.weighed, self.best = [], 0.0, -np.inf
+        self.refusal = None
+        self.done = False
+
+
+class _LockstepScan:
+    """The scan of many states at once. equation(slots, w, want_slope) ->
+    (f, f', refusals {index: exception}) evaluates f(w) = w - a - Sigma(w)
+    and its slope at every point of a round."""
+
+    def __init__(self, equation, tol=QP_ROOT_TOL, max_iter=QP_ROOT_MAX_ITER):
+        self.eq, self.tol, self.max_iter = equation, tol, int(max_iter)
+        self.rounds = 0
+
+    def _eval(self, slots, w, want_slope):
+        if len(w) == 0:
+            return np.zeros(0), np.zeros(0), {}
+        self.rounds += 1
+        f, fp, bad = self.eq(np.asarray(slots, int), np.asarray(w, float), want_slope)
+        return np.asarray(f, float), np.asarray(fp, float), bad
+
+    # -- brackets of a set of cells: the cell on a sign change; its halves
+    # while its secant slope is below QP_SCAN_SECANT_MIN or one end is refused
+    # and the other not, at most QP_SCAN_SPLIT_DEPTH times; one level of
+    # halving of every open cell per round
+    def _brackets(self, cells):
+        """cells: [(key, slot, l, r, fl, fr)] -> {key: [(path, l, r, fl, fr)]},
+        {key: refusal or None} of the halving points."""
+        out = {key: [] for key, *_ in cells}
+        bad = {key: None for key, *_ in cells}
+        items = [(key, slot, '', l, r, fl, fr, QP_SCAN_SPLIT_DEPTH)
+                 for key, slot, l, r, fl, fr in cells]
+        while items:
+            split = []
+            for key, slot, path, l, r, fl, fr, depth in items:
+                if fl * fr < 0.0:
+                    out[key].append((path, l, r, fl, fr))
+                    continue
+                edge = np.isnan(fl) != np.isnan(fr)
+                if depth == 0 or fl == 0.0 or fr == 0.0 or not (
+                        edge or fr - fl < QP_SCAN_SECANT_MIN * (r - l)):
+                    continue
+                split.append((key, slot, path, l, r, fl, fr, depth))
+            if not split:
+                break
+            mids = [0.5 * (it[3] + it[4]) for it in split]
+            fm, _, refused = self._eval([it[1] for it in split], mids, False)
+            items = []
+            for i, (key, slot, path, l, r, fl, fr, depth) in enumerate(split):
+                if i in refused and bad[key] is None:
+                    bad[key] = refused[i]
+                m = mids[i]
+                items.append((key, slot, path + '0', l, m, fl, fm[i], depth - 1))
+                items.append((key, slot, path + '1', m, r, fm[i], fr, depth - 1))
+        return out, bad
+
+    # -- roots of brackets: Newton on the closed-form slope inside the
+    # bracket, one step of every open bracket per round (``qp_equation.py:376-426``
+    # for a costly f): a step that leaves the bracket, or is not under half
+    # the step before the last, is a bisection; a step below tol that stays
+    # in the closed bracket ends it; a bracket one ulp wide ends at its point
+    def _roots(self, brackets):
+        """brackets: [(slot, l, r, fl, fr)] -> ([] or [(w, Z)] each, refusal
+        per bracket)."""
+        n = len(brackets)
+        roots, bad = [None] * n, [None] * n
+        live, at = [], {}
+        for i, (slot, l, r, fl, fr) in enumerate(brackets):
+            if l == r:
+                at[i] = float(l)
+            elif fl > 0.0 > fr:
+                roots[i] = []          # f falls: a pole of a positive-weight Sigma
+            else:
+                live.append(i)
+        if live:
+            slots = np.array([brackets[i][0] for i in live])
+            L = np.array([brackets[i][1] for i in live], float)
+            R = np.array([brackets[i][2] for i in live], float)
+            SL = np.sign([brackets[i][3] for i in live])
+            W = 0.5 * (L + R)
+            old = R - L
+            step = R - L
+            result = np.full(len(live), np.nan)
+            active = np.ones(len(live), dtype=bool)
+            for _ in range(self.max_iter):
+                idx = np.nonzero(active)[0]
+                if idx.size == 0:
+                    break
+                f, fp, refused = self._eval(slots[idx], W[idx], True)
+                for k, e in refused.items():
+                    if bad[live[idx[k]]] is None:
+                        bad[live[idx[k]]] = e
+                w = W[idx]
+                with np.errstate(divide='ignore', invalid='ignore'):
+                    dw = -f / fp
+                zero = f == 0.0
+                same = np.sign(f) == SL[idx]
+                L[idx] = np.where(same, w, L[idx])
+                R[idx] = np.where(same, R[idx], w)
+                l, r = L[idx], R[idx]
+                with np.errstate(invalid='ignore'):
+                    conv = (np.abs(dw) < self.tol) & (l <= w + dw) & (w + dw <= r)
+                mid = 0.5 * (l + r)
+                stuck = ~((l < mid) & (mid < r))
+                with np.errstate(invalid='ignore'):
+                    newton = (np.isfinite(dw) & (l < w + dw) & (w + dw < r)
+                              & (np.abs(dw) <= 0.5 * np.abs(old[idx])))
+                stop = zero | conv | stuck
+                result[idx] = np.where(zero, w, np.where(conv, w + dw, w))
+                go = ~stop
+                old[idx] = np.where(go, step[idx], old[idx])
+                step[idx] = np.where(go, np.where(newton, dw, mid - w), step[idx])
+                W[idx] = np.where(go, np.where(newton, w + dw, mid), w)
+                active[idx[stop]] = False
+            result = np.where(active, W, result)
+            for j, i in enumerate(live):
+                at[i] = float(result[j])
+        if at:
+            keys = list(at)
+            f, fp, refused = self._eval([brackets[i][0] for i in keys],
+                                        [at[i] for i in keys], True)
+            for j, i in enumerate(keys):
+                if j in refused and bad[i] is None:
+                    bad[i] = refused[j]
+                fl, fr = brackets[i][3], brackets[i][4]
+                if brackets[i][1] != brackets[i][2] and not abs(f[j]) <= max(abs(fl), abs(fr)):
+                    roots[i] = []      # |f| grew (a pole) or the point was refused
+                else:
+                    z = 1.0 / fp[j] if fp[j] != 0.0 else np.nan
+                    roots[i] = [(at[i], float(z))]
+        return roots, bad
+
+    def walk(self, walks):
+        """Walk every window in waves of cells that double, all walks at
+        once; each walk stops once the valid weights found leave, plus
+        QP_WEIGHT_SUM_SLACK, no more of their sum (one) than the largest of
+        them or than its window's `enough`."""
+        size = 1
+        while True:
+            live = [wk for wk in walks if not wk.done]
+            if not live:
+                return
+            chunk = {id(wk): wk.order[wk.pos:wk.pos + size] for wk in live}
+            # the grid points the wave's cells end on
+            need = []
+            for wk in live:
+                pts = sorted({i for c in chunk[id(wk)] for i in (c, c + 1)} - set(wk.f))
+                need += [(wk, i) for i in pts]
+            f, _, refused = self._eval([wk.slot for wk, _ in need],
+                                       [wk.grid[i] for wk, i in need], False)
+            for j, (wk, i) in enumerate(need):
+                wk.f[i] = float(f[j])
+                if j in refused:
+                    wk.bad[i] = refused[j]
+            cells = [((id(wk), c), wk.slot, wk.grid[c], wk.grid[c + 1], wk.f[c], wk.f[c + 1])
+                     for wk in live for c in chunk[id(wk)]]
+            brk, bad_split = self._brackets(cells)
+            flat, owner = [], []
+            for (key, slot, *_rest) in cells:
+                for path, l, r, fl, fr in sorted(brk[key]):
+                    flat.append((slot, l, r, fl, fr))
+                    owner.append(key)
+            roots, bad_root = self._roots(flat)
+            per_cell = {}
+            for k, key in enumerate(owner):
+                per_cell.setdefault(key, []).append((flat[k][1], roots[k], bad_root[k]))
+            # replay each walk in the reference's order up to where it stops
+            for wk in live:
+                for c in chunk[id(wk)]:
+                    key = (id(wk), c)
+                    for e in (wk.bad.get(c), wk.bad.get(c + 1), bad_split.get(key)):
+                        if e is not None and wk.refusal is None:
+                            wk.refusal = e
+                    for l, got, e in per_cell.get(key, []):
+                        if e is not None and wk.refusal is None:
+                            wk.refusal = e
+                        wk.found.append((l, got))
+                        for _, z in got:
+                            if _valid(z):
+                                wk.weighed += z
+                                wk.best = max(wk.best, z)
+                    wk.pos += 1
+                    if 1.0 - wk.weighed + QP_WEIGHT_SUM_SLACK <= max(wk.best, wk.enough):
+                        wk.done = True
+                        break
+                if wk.pos >= len(wk.order):
+                    wk.done = True
+            size *= 2
+
+    def solve(self, slots, bare):
+        """Per state: (w, Z, refusal, found roots of its last window), the
+        root of largest valid weight in the narrowest window that holds one
+        above QP_WINDOW_Z_MIN; a state without one keeps its widest window's
+        largest valid weight, or the root nearest its bare level."""
+        n = len(slots)
+        out = [None] * n
+        pending = list(range(n))
+        wins = [_windows(float(a)) for a in bare]
+        level = [0] * n
+        refusal = [None] * n
+        found = [[] for _ in range(n)]
+        while pending:
+            walks = []
+            for i in pending:
+                lo, hi = wins[i][level[i]]
+                last = level[i] + 1 == len(wins[i])
+                walks.append(_Walk(slots[i], float(bare[i]), lo, hi,
+                                   -np.inf if last else QP_WINDOW_Z_MIN))
+            self.walk(walks)
+            nxt = []
+            for i, wk in zip(pending, walks):
+                if wk.refusal is not None and refusal[i] is None:
+                    refusal[i] = wk.refusal
+                wk.found.sort(key=lambda lr: lr[0])
+                found[i] = [rz for _, got in wk.found for rz in got]
+                ok = [k for k, (_, z) in enumerate(found[i]) if _valid(z)]
+                if ok:
+                    k = max(ok, key=lambda j: found[i][j][1])
+                    if _valid(found[i][k][1], QP_WINDOW_Z_MIN):
+                        out[i] = (found[i][k][0], found[i][k][1], True)
+                        continue
+                if level[i] + 1 < len(wins[i]):
+                    level[i] += 1
+                    nxt.append(i)
+            pending = nxt
+        result = []
+        for i in range(n):
+            if out[i] is not None:
+                result.append((out[i][0], out[i][1], None, found[i]))
+                continue
+            if refusal[i] is not None:
+                result.append((np.nan, np.nan, refusal[i], found[i]))
+                continue
+            if not found[i]:
+                result.append((np.nan, np.nan, None, found[i]))
+                continue
+            ok = [k for k, (_, z) in enumerate(found[i]) if _valid(z)]
+            k = (max(ok, key=lambda j: found[i][j][1]) if ok
+                 else min(range(len(found[i])), key=lambda j: abs(found[i][j][0] - bare[i])))
+            result.append((found[i][k][0], found[i][k][1], None, found[i]))
+        return result
+
+
+def _report_root(w, z, refusal, bare, label):
+    """Raise the refusal of a state without a quasiparticle, warn for no root
+    or for Z outside (0, 1], as ``qp_equation.py:236-273`` does."""
+    from .gw import QPNoRoot, QPWeightOutside
+    if refusal is not None:
+        raise refusal
+    if not np.isfinite(w):
+        lo, hi = _windows(bare)[-1]
+        warnings.warn(f'{label or "the quasiparticle equation"} has no root in the widest '
+                      f'scan window [{lo:.6f}, {hi:.6f}] Ha about {bare:.6f} Ha.', QPNoRoot,
+                      stacklevel=3)
+    elif not 0.0 < z <= 1.0:
+        warnings.warn(f'the quasiparticle root of {label or "the quasiparticle equation"} '
+                      f'{w!r} Ha has Z = {z!r}, outside (0, 1]: kept', QPWeightOutside,
+                      stacklevel=3)
+
+
+def solve_qp_equation_scan(residual, fprime, a, tol=QP_ROOT_TOL, max_iter=QP_ROOT_MAX_ITER,
+                           label='', refusals=()):
+    """(w, Z) of residual(w) = 0 for a positive-weight self-energy known
+    pointwise, residual and fprime host callables (``qp_equation.py:1396-1420``).
+    Points where either raises one of `refusals` count as unknown. No
+    quasiparticle where the self-energy could be evaluated raises the first
+    refusal; no root at all is (NaN, NaN) with a QPNoRoot warning; a root
+    with Z outside (0, 1] is kept with a QPWeightOutside warning."""
+    refusals = tuple(refusals)
+
+    def equation(slots, w, want_slope):
+        f = np.empty(len(w))
+        fp = np.full(len(w), np.nan)
+        bad = {}
+        for j, x in enumerate(w):
+            try:
+                f[j] = residual(float(x))
+                if want_slope:
+                    fp[j] = fprime(float(x))
+            except refusals as e:
+                f[j], fp[j] = np.nan, np.nan
+                bad[j] = e
+        return f, fp, bad
+    (w, z, refusal, _), = _LockstepScan(equation, tol, max_iter).solve([0], [float(a)])
+    _report_root(w, z, refusal, float(a), label)
+    return float(w), float(z)
+
+
+def _contour_equation_callable(eq):
+    """Adapt a ContourEquation to the scan's (f, f', refusals) protocol."""
+    def equation(slots, w, want_slope):
+        f, fp, refused = eq(slots, w, want_slope)
+        bad = {}
+        for j in np.nonzero(refused)[0]:
+            try:
+                eq.backend._refuse(np.abs(eq.eps - w[j])[
+                    residue_weights(eq.eps, eq.nocc, [w[j]])[0] != 0])
+            except ResidueRefused as e:
+                bad[int(j)] = e
+        return f, fp, bad
+    return equation
+
+
+def solve_contour_roots(eq, labels=None, tol=QP_ROOT_TOL, max_iter=QP_ROOT_MAX_ITER,
+                        warn=True):
+    """(roots, Z, refusals) of every slot of a ContourEquation, all states'
+    searches in lockstep. warn: report no-root / Z-outside per state (a
+    refusal is returned, not raised)."""
+    n = len(eq.bare)
+    scan = _LockstepScan(_contour_equation_callable(eq), tol, max_iter)
+    res = scan.solve(list(range(n)), eq.bare)
+    roots = np.array([r[0] for r in res], float)
+    zs = np.array([r[1] for r in res], float)
+    refusals = [r[2] for r in res]
+    if warn:
+        for i, (w, z, e, _) in enumerate(res):
+            if e is None:
+                _report_root(w, z, None, float(eq.bare[i]),
+                             labels[i] if labels is not None else '')
+    eq.rounds = scan.rounds
+    return roots, zs, refusals
+
+
+# ------------------------------------------- the reference's per-state seams
+
+def _host_or_device_wc(Bp, eps, nocc, nu_points, wbp, wc, C_ov):
+    """The state's contracted screening wc (nfreq, norb): given, contracted
+    from W B_p (wbp), or built explicitly from C_ov (`wc_explicit`)."""
     if wc is None:
-        if wbp is None:
+        if wbp is not None:
+            Bh = Bp.detach().cpu().numpy() if isinstance(Bp, torch.Tensor) else np.asarray(Bp)
+            wc = screening_contraction(Bh, wbp)
+        else:
             require_three_index(C_ov, 'the imaginary-axis screening without wbp or wc')
             wc = wc_explicit(Bp, C_ov, ov_energies(eps, nocc), nu_points)
-        else:
-            wc = screening_contraction(Bh, wbp)
-    wc = wc.detach().cpu().numpy() if isinstance(wc, torch.Tensor) else np.asarray(wc)
-    c, _ = cd_integral_weights(omega - eps, nu_points, nu_weights)
-    s_int = -float(np.einsum('kq,kq->', c, wc)) / np.pi
-    res = residue_set(eps, nocc, omega) if residues is None else residues
-    s_res = 0.0
-    if res:
-        rs = residue_backend(real_screening, C_ov, eps, nocc, eta)
-        for q, weight in res:
-            b = Bh[:, q]
-            y = rs.apply(abs(eps[q] - omega), b)
-            s_res += weight * (float(b @ y) - float(b @ b))
-    return s_int + s_res
+    return wc
+
+
+def _one_state_equation(p, Bp, eps, nocc, nu_points, nu_weights, xc_correction, wbp, wc,
+                        C_ov, eta, real_screening):
+    eps = np.asarray(eps, float)
+    wc = _host_or_device_wc(Bp, eps, nocc, nu_points, wbp, wc, C_ov)
+    backend = (residue_backend(real_screening, C_ov, eps, nocc, eta)
+               if real_screening is not None or C_ov is not None else None)
+    quad = LorentzianQuadrature(nu_points, nu_weights)
+    return ContourEquation(Bp, wc, eps, nocc, quad,
+                           [float(eps[p]) + float(xc_correction)], backend)
+
+
+def sigma_cd(p, omega, Bp, eps, nocc, nu_points, nu_weights, residues=None, wbp=None,
+             eta=0.0, wc=None, C_ov=None, real_screening=None):
+    """Sigma^c_pp(omega) by contour deformation (``contour_deformation.py:310-343``)
+    from the state's slice Bp and its contracted screening (wc, or W Bp as
+    wbp, or -- with neither -- built explicitly from C_ov); the residues at
+    omega unless `residues` [(q, weight)] fixes them, their W from
+    `real_screening` (a LaplaceRealScreening or ExplicitRealScreening) or,
+    with C_ov and no backend, the explicit one."""
+    eq = _one_state_equation(p, Bp, eps, nocc, nu_points, nu_weights, 0.0, wbp, wc, C_ov,
+                             eta, real_screening)
+    if eq.backend is not None:
+        eq.backend._refuse(_residue_frequencies(eq, float(omega), residues))
+    s, _, _ = eq.sigma([0], [float(omega)], want_slope=False, residues=residues)
+    return float(s[0])
+
+
+def _residue_frequencies(eq, omega, residues):
+    if residues is None:
+        r = residue_weights(eq.eps, eq.nocc, [omega])[0]
+        return np.abs(eq.eps[r != 0] - omega)
+    return np.array([abs(eq.eps[q] - omega) for q, _ in residues])
 
 
 def sigma_cd_slope(p, omega, Bp, eps, nocc, nu_points, nu_weights, residues, wc, eta=0.0,
                    C_ov=None, real_screening=None):
     """dSigma^c_pp/domega in closed form at a frozen residue set
-    (``contour_deformation.py:346-373``): the integral weights' derivative
-    against wc, and per residue W [dchi0/dfreq] W contracted with b_q on both
-    sides, signed by the side of the pole."""
-    eps = np.asarray(eps, float)
-    Bh = Bp.detach().cpu().numpy() if isinstance(Bp, torch.Tensor) else np.asarray(Bp)
-    wc = wc.detach().cpu().numpy() if isinstance(wc, torch.Tensor) else np.asarray(wc)
-    _, dc = cd_integral_weights(omega - eps, nu_points, nu_weights)
-    slope = -float(np.einsum('kq,kq->', dc, wc)) / np.pi
-    if residues:
-        rs = residue_backend(real_screening, C_ov, eps, nocc, eta)
-        for q, weight in residues:
-            gap = eps[q] - omega
-            freq = abs(gap)
-            y = rs.apply(freq, Bh[:, q])
-            slope -= weight * rs.slope(freq, y) * np.sign(gap)
-    return slope
-
-
-# ------------------------------------------------ the scan root finder
-# Solvers/qp_equation.py: `solve_qp_equation_scan` (:1396-1420) on a
-# `SampledEquation` (:1029-1278) through `find_qp_root` (:155-233) without a
-# followed root, as `qp_energy_cd` calls it.
-
-def _qp_search_windows(a):
-    """Windows about the bare level, narrowest first: the tier of the
-    state's depth, then every wider tier (:1280-1288)."""
-    tier = 0
-    for k, (depth, _) in enumerate(QP_SEARCH_WINDOW_TIERS):
-        if abs(a) > depth:
-            tier = k
-    return [(a - half, a + half) for _, half in QP_SEARCH_WINDOW_TIERS[tier:]]
-
-
-def _valid_weight(z, z_min=0.0):
-    """Z of a quasiparticle: finite and in (z_min, 1] (:95-102)."""
-    z = float(z)
-    return bool(np.isfinite(z) and z_min < z <= 1.0)
-
-
-def _bracketed_newton(fval, l, r, sl, tol, max_iter):
-    """The root of f in (l, r), f of sign sl at l, by Newton on the slope
-    safeguarded by the bracket: a step leaving it, or not under half the step
-    before the last, is a bisection; a step below tol that stays in the
-    closed bracket ends it (:376-426, for a costly f)."""
-    if sl == 0.0:
-        return float(l)
-    w = 0.5 * (l + r)
-    step = old = r - l
-    for _ in range(int(max_iter)):
-        f, fp = fval(w)
-        if f == 0.0:
-            return float(w)
-        if np.sign(f) == sl:
-            l = w
-        else:
-            r = w
-        dw = -f / fp
-        if abs(dw) < tol and l <= w + dw <= r:
-            return float(w + dw)
-        mid = 0.5 * (l + r)
-        if not l < mid < r:
-            break
-        newton = np.isfinite(dw) and l < w + dw < r and abs(dw) <= 0.5 * abs(old)
-        old, step = step, (dw if newton else mid - w)
-        w = w + dw if newton else mid
-    return float(w)
-
-
-class _Scan:
-    """f(w) = w - a - Sigma(w) known pointwise with a closed-form slope, for
-    a positive-weight Sigma; points a refusal type rejects are NaN, the first
-    refusal kept (:1071-1092, :1143-1166, :1250-1278)."""
-
-    def __init__(self, func, fprime, tol, max_iter, refusals):
-        self.tol, self.max_iter = tol, max_iter
-        self.refusals, self.refused = tuple(refusals), None
-        self.func, self.fprime = self._guarded(func), self._guarded(fprime)
-
-    def _guarded(self, g):
-        def call(w):
-            try:
-                return g(w)
-            except self.refusals as refusal:
-                if self.refused is None:
-                    self.refused = refusal
-                return np.nan
-        return call
-
-    def weight(self, w):
-        fp = float(self.fprime(w))
-        return 1.0 / fp if fp != 0.0 else np.nan
-
-    def solve(self, bracket):
-        """[(root, Z)] of a bracket (l, r, f(l), f(r)); empty for a pole."""
-        l, r, fl, fr = bracket
-        if l == r:
-            return [(float(l), self.weight(l))]
-        if fl > 0.0 > fr:
-            return []                   # f falls: a pole of a positive-weight Sigma
-        fval = lambda x: (float(self.func(x)), float(self.fprime(x)))  # noqa: E731
-        w = _bracketed_newton(fval, l, r, np.sign(fl), self.tol, self.max_iter)
-        fw = fval(w)[0]
-        if not abs(fw) <= max(abs(fl), abs(fr)):
-            return []                   # |f| grew (a pole) or the point was refused
-        return [(float(w), self.weight(w))]
-
-    def cells(self, l, r, fl, fr, depth):
-        """Brackets in [l, r]: the cell on a sign change; its halves while
-        its secant slope is below QP_SCAN_SECANT_MIN or one end is refused
-        and the other not, at most `depth` times (:1250-1266)."""
-        if fl * fr < 0.0:
-            return [(l, r, fl, fr)]
-        edge = np.isnan(fl) != np.isnan(fr)
-        if depth == 0 or fl == 0.0 or fr == 0.0 or not (
-                edge or fr - fl < QP_SCAN_SECANT_MIN * (r - l)):
-            return []
-        m = 0.5 * (l + r)
-        fm = float(self.func(m))
-        return self.cells(l, m, fl, fm, depth - 1) + self.cells(m, r, fm, fr, depth - 1)
-
-    def outward(self, lo, hi, a):
-        """The brackets of each grid cell, cells in increasing distance from
-        the one holding a, f evaluated as the cells reach a grid point
-        (:1110-1129)."""
-        grid = np.linspace(lo, hi, QP_GRAPHICAL_N_OMEGA)
-        f = {}
-
-        def value(j):
-            if j not in f:
-                f[j] = float(self.func(grid[j]))
-            return f[j]
-        c0 = min(max(int(np.searchsorted(grid, a)) - 1, 0), grid.size - 2)
-        for d in range(grid.size - 1):
-            for c in sorted({c0 - d, c0 + d}):
-                if 0 <= c < grid.size - 1:
-                    yield self.cells(grid[c], grid[c + 1], value(c), value(c + 1),
-                                     QP_SCAN_SPLIT_DEPTH)
-
-
-def _weighed_outward(scan, lo, hi, a, enough):
-    """[(root, Z)] of the cells walked outward from a, until the valid
-    weights found leave (plus QP_WEIGHT_SUM_SLACK) no more of their sum, one,
-    than the largest of them or `enough` (:312-339)."""
-    found, best, weighed = [], -np.inf, 0.0
-    for brackets in scan.outward(lo, hi, a):
-        for bracket in brackets:
-            got = scan.solve(bracket)
-            found.append((bracket[0], got))
-            for _, z in got:
-                if _valid_weight(z):
-                    weighed += z
-                    best = max(best, z)
-        if 1.0 - weighed + QP_WEIGHT_SUM_SLACK <= max(best, enough):
-            break
-    found.sort(key=lambda lr: lr[0])
-    return [rz for _, got in found for rz in got]
-
-
-def solve_qp_equation_scan(residual, fprime, a, tol=QP_ROOT_TOL, max_iter=QP_ROOT_MAX_ITER,
-                           label='', refusals=()):
-    """(w, Z) of residual(w) = 0 for a positive-weight self-energy: per
-    window, narrowest first, the root of largest valid weight; a weight above
-    QP_WINDOW_Z_MIN ends the search, the widest window keeps its largest
-    valid weight (the root nearest a if none is valid). No quasiparticle
-    where Sigma could be evaluated raises the first refusal; no root at all
-    is (NaN, NaN) with a QPNoRoot warning; a root with Z outside (0, 1] is
-    kept with a QPWeightOutside warning (:155-273, :1396-1420)."""
-    from .gw import QPNoRoot, QPWeightOutside
-    scan = _Scan(residual, fprime, tol, max_iter, refusals)
-    windows = _qp_search_windows(a)
-    found, w, z, quasi = [], np.nan, np.nan, False
-    for i, (lo, hi) in enumerate(windows):
-        enough = QP_WINDOW_Z_MIN if i + 1 < len(windows) else -np.inf
-        found = _weighed_outward(scan, lo, hi, a, enough)
-        ok = [k for k, (_, zk) in enumerate(found) if _valid_weight(zk)]
-        if ok:
-            k = max(ok, key=lambda j: found[j][1])
-            if _valid_weight(found[k][1], QP_WINDOW_Z_MIN):
-                w, z, quasi = found[k][0], found[k][1], True
-                break
-    if not quasi:
-        if scan.refused is not None:
-            raise scan.refused
-        if not found:
-            warnings.warn(f'{label or "the quasiparticle equation"} has no root in the widest '
-                          f'scan window [{windows[-1][0]:.6f}, {windows[-1][1]:.6f}] Ha about '
-                          f'{a:.6f} Ha.', QPNoRoot, stacklevel=2)
-            return np.nan, np.nan
-        ok = [k for k, (_, zk) in enumerate(found) if _valid_weight(zk)]
-        k = (max(ok, key=lambda j: found[j][1]) if ok
-             else min(range(len(found)), key=lambda j: abs(found[j][0] - a)))
-        w, z = found[k]
-    if np.isfinite(w) and not 0.0 < z <= 1.0:
-        warnings.warn(f'the quasiparticle root of {label or "the quasiparticle equation"} '
-                      f'{w!r} Ha has Z = {z!r}, outside (0, 1]: kept', QPWeightOutside,
-                      stacklevel=2)
-    return float(w), float(z)
+    (``contour_deformation.py:346-373``)."""
+    eq = _one_state_equation(p, Bp, eps, nocc, nu_points, nu_weights, 0.0, None, wc, C_ov,
+                             eta, real_screening)
+    if residues and eq.backend is not None:
+        eq.backend._refuse(_residue_frequencies(eq, float(omega), residues))
+    _, ds, _ = eq.sigma([0], [float(omega)], want_slope=True, residues=residues or [])
+    return float(ds[0])
 
 
 def qp_energy_cd(p, Bp, eps, nocc, nu_points, nu_weights, xc_correction=0.0, tol=QP_ROOT_TOL,
                  max_iter=QP_ROOT_MAX_ITER, follow=None, wbp=None, wc=None, C_ov=None,
                  eta=0.0, real_screening=None, branch=None, rescan=True):
     """(eps^QP_p, Z_p, residues) of w = eps_p + xc_correction + Sigma^c(w) by
-    contour deformation (``contour_deformation.py:376-436``): the scan about
-    the bare level with Newton on the closed-form slope, the residue set
-    re-decided at every point and frozen at the root. The imaginary-axis
-    screening comes in as wc, as wbp contracted once here, or -- with neither
-    -- explicitly from C_ov (`wc_explicit`, contracted once). The residues
-    read `real_screening`, else the explicit backend of C_ov (broadened by
-    eta), built once for the whole scan: its kept W - I serves the value and
-    the slope at one point, as the reference's `_PointApplies` does."""
+    contour deformation (``contour_deformation.py:376-436``): the lockstep
+    scan about the bare level with the residues re-decided at every point,
+    the residue set of the root returned. Screening and backend as
+    `sigma_cd`."""
     if follow is not None or branch is not None:
         raise NotImplementedError('following a root along a walk is outside the device route')
-    eps = np.asarray(eps, float)
-    Bh = Bp.detach().cpu().numpy() if isinstance(Bp, torch.Tensor) else np.asarray(Bp)
-    if wc is None:
-        if wbp is not None:
-            wc = screening_contraction(Bh, wbp)
-        else:
-            require_three_index(C_ov, 'the imaginary-axis screening without wbp or wc')
-            wc = wc_explicit(Bp, C_ov, ov_energies(eps, nocc), nu_points)
-    wc = wc.detach().cpu().numpy() if isinstance(wc, torch.Tensor) else np.asarray(wc)
-    if real_screening is not None or C_ov is not None:
-        real_screening = residue_backend(real_screening, C_ov, eps, nocc, eta)
-    common = dict(eta=eta, C_ov=C_ov, real_screening=real_screening)
+    eq = _one_state_equation(p, Bp, eps, nocc, nu_points, nu_weights, xc_correction, wbp, wc,
+                             C_ov, eta, real_screening)
+    roots, zs, refusals = solve_contour_roots(eq, [f'orbital {p}'], tol, max_iter)
+    if refusals[0] is not None:
+        raise refusals[0]
+    w = float(roots[0])
+    return w, float(zs[0]), residue_set(eps, nocc, w)
 
-    def residual(w):
-        return w - eps[p] - xc_correction - sigma_cd(
-            p, w, Bh, eps, nocc, nu_points, nu_weights, residues=residue_set(eps, nocc, w),
-            wc=wc, **common)
 
-    def fprime(w):
-        return 1.0 - sigma_cd_slope(p, w, Bh, eps, nocc, nu_points, nu_weights,
-                                    residue_set(eps, nocc, w), wc, **common)
-    w, z = solve_qp_equation_scan(residual, fprime, float(eps[p] + xc_correction), tol=tol,
-                                  max_iter=max_iter, label=f'orbital {p}',
-                                  refusals=(ResidueRefused,))
-    return w, z, residue_set(eps, nocc, w)
+def residue_backend(real_screening, C_ov, eps, nocc, eta):
+    """The backend the residue term uses: the one given, else the explicit one
+    from C_ov (``contour_deformation.py:117-122``)."""
+    if real_screening is not None:
+        return real_screening
+    require_three_index(C_ov, 'the residue term')
+    return ExplicitRealScreening(C_ov, eps, nocc, eta)
+
+
+def require_three_index(C_ov, what):
+    """``contour_deformation.py:109-114``."""
+    if C_ov is None:
+        raise ResidueRefused(
+            f'{what} needs C_ov = B[:, occ, virt] as (naux, nocc*nvirt) and it was not '
+            f'supplied. A frontier state sweeps no residues and needs none once the '
+            f'imaginary-axis screening comes in as wbp or wc.')
 
 
 HARTREE_TO_EV = 27.211386245988  # MBPTcode constants.py:11 (CODATA 2018)
@@ -823,31 +1324,35 @@ HARTREE_TO_EV = 27.211386245988  # MBPTcode constants.py:11 (CODATA 2018)
 
 def _roots_on_contour(continuation, states, B, wcs, eps, nocc, nu, nu_w, xc_correction,
                       backend, w0, ntau, nfreq_cd):
-    """Each state's root and Z by `qp_energy_cd` on one contour grid, with
-    the per-state records (``contour_deformation.py:558-598``)."""
+    """Every state's root and Z on one contour grid, all states' scans in
+    lockstep, with the per-state records (``contour_deformation.py:558-598``)."""
     explicit = continuation == 'cd'
-    roots, zs, records = np.zeros(len(states)), np.zeros(len(states)), []
+    xc = np.broadcast_to(np.asarray(xc_correction, float).ravel()
+                         if np.ndim(xc_correction) else float(xc_correction),
+                         (len(states),))
+    wc = torch.stack([to_device(w, B.device) for w in wcs])
+    eq = ContourEquation(B, wc, eps, nocc, LorentzianQuadrature(nu, nu_w),
+                         eps[states] + xc, backend)
+    roots, zs, refusals = solve_contour_roots(eq, [f'orbital {int(p)}' for p in states])
+    records = []
     for i, p in enumerate(states):
-        xc = (float(np.asarray(xc_correction).ravel()[i]) if np.ndim(xc_correction)
-              else float(xc_correction))
-        try:
-            w, z, res = qp_energy_cd(int(p), B[i], eps, nocc, nu, nu_w, xc_correction=xc,
-                                     wc=wcs[i], real_screening=backend)
-        except ResidueRefused as refusal:
+        if refusals[i] is not None:
             if explicit:
-                raise
+                raise refusals[i]
             raise ResidueRefused(
                 f"continuation='laplace' cannot serve orbital {int(p)}: its contour sweeps "
-                f'a residue the imaginary-time grid does not represent. {refusal}') from refusal
-        roots[i], zs[i] = w, z
+                f'a residue the imaginary-time grid does not represent. {refusals[i]}'
+            ) from refusals[i]
+        res = residue_set(eps, nocc, roots[i])
         error = None
         if not explicit and res:
-            error = max(backend.representation_error(abs(eps[q] - w)) for q, _ in res)
-        records.append({'state': int(p), 'residues': len(res),
-                        'representation_error': error})
+            error = float(backend.errors([abs(eps[q] - roots[i]) for q, _ in res]).max())
+        records.append({'state': int(p), 'residues': len(res), 'representation_error': error})
     info = {'continuation': continuation, 'ntau': int(ntau), 'nfreq_cd': int(nfreq_cd),
             'w0_cd': float(w0), 'residue_route_taken': 'explicit' if explicit else 'laplace',
-            'states': records}
+            'states': records, 'points_evaluated': int(eq.points),
+            'evaluation_rounds': int(getattr(eq, 'rounds', 0)),
+            'residue_solves': dict(getattr(backend, 'stats', {}))}
     return roots, zs, info
 
 

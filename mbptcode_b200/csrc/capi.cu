@@ -457,21 +457,43 @@ constexpr int kBatchedCholMin = 4;  // frequencies from which the batch beats on
 // step for all frequencies. P: nmat * n * kCholNb doubles; Linv: nmat *
 // kCholNb^2 doubles per step, step j at Linv + j * linv_step_stride (0: every
 // step in the same place); info: nmat ints, zeroed by the caller.
+// The Ozaki-scheme update's buffers for one batch (null planes: the updates
+// run as cuBLAS DGEMMs): the int8 digit planes, 2^e_r per row, exact row norms.
+struct OzakiChol {
+  int8_t *planes = nullptr;
+  double *scale = nullptr;
+  double *rowsq = nullptr;
+  int slices = 8;
+  int *err = nullptr;
+};
+
 int chol_batched(double *A, int64_t n, int nmat, int *info, double *P, double *Linv,
-                 cublasHandle_t h, cudaStream_t st, int64_t linv_step_stride = 0) {
+                 cublasHandle_t h, cudaStream_t st, int64_t linv_step_stride = 0,
+                 const OzakiChol *oz = nullptr) {
   const long long n2 = static_cast<long long>(n) * n;
   const double one = 1.0, minus = -1.0, zero = 0.0;
+  const bool ozaki = oz && oz->planes;
+  if (ozaki) {
+    int rc = ozaki_chol_scales(A, n, nmat, oz->scale, st);
+    if (rc) return rc;
+  }
   for (int64_t j0 = 0; j0 < n; j0 += kCholNb) {
     const int nbj = static_cast<int>(std::min<int64_t>(kCholNb, n - j0));
     const int64_t m = n - j0;
     launch_chol_copy_panel(A, n, j0, m, nbj, nmat, P, st);
-    if (j0 > 0 &&
-        cublasDgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_T, static_cast<int>(m), nbj,
-                                  static_cast<int>(j0), &minus, A + j0, static_cast<int>(n), n2,
-                                  A + j0, static_cast<int>(n), n2, &one, P,
-                                  static_cast<int>(m), static_cast<long long>(m) * nbj,
-                                  nmat) != CUBLAS_STATUS_SUCCESS)
+    if (ozaki) {
+      int rc = ozaki_chol_update(A, n, nmat, j0, nbj, P, oz->scale, oz->planes, oz->slices,
+                                 oz->rowsq, oz->err, st);
+      if (rc) return rc;
+    } else if (j0 > 0 &&
+               cublasDgemmStridedBatched(h, CUBLAS_OP_N, CUBLAS_OP_T, static_cast<int>(m), nbj,
+                                         static_cast<int>(j0), &minus, A + j0,
+                                         static_cast<int>(n), n2, A + j0, static_cast<int>(n),
+                                         n2, &one, P, static_cast<int>(m),
+                                         static_cast<long long>(m) * nbj,
+                                         nmat) != CUBLAS_STATUS_SUCCESS) {
       return MBPT_ERR_CUDA;
+    }
     double *Lj = Linv + (j0 / kCholNb) * linv_step_stride;
     int rc = launch_chol_diag_block(P, m, nbj, A, n, j0, nmat, Lj, info, st);
     if (rc) return rc;
@@ -484,8 +506,26 @@ int chol_batched(double *A, int64_t n, int nmat, int *info, double *P, double *L
                                   A + j0 * n + j0 + nbj, static_cast<int>(n), n2,
                                   nmat) != CUBLAS_STATUS_SUCCESS)
       return MBPT_ERR_CUDA;
+    // the block column is final: cut it into digit planes for the later steps
+    if (ozaki && j0 + nbj < n) {
+      int rc2 = ozaki_chol_slice(A, n, nmat, j0, nbj, oz->scale, oz->planes, oz->slices, st);
+      if (rc2) return rc2;
+    }
   }
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+// MBPT_DYSON_OZAKI=1 runs the batched Cholesky's trailing updates on the int8
+// tensor cores with MBPT_DYSON_OZAKI_SLICES digits per operand (8 by
+// default; 7 is within 1e-12 of FP64 on W and at FP64 level on the
+// log-determinant); otherwise as cuBLAS DGEMMs. Read at every call, so the
+// size query and the call that follows it must see the same setting.
+int ozaki_slices() {
+  const char *e = std::getenv("MBPT_DYSON_OZAKI");
+  if (!e || std::atoi(e) == 0) return 0;
+  const char *k = std::getenv("MBPT_DYSON_OZAKI_SLICES");
+  const int v = k ? std::atoi(k) : 8;
+  return (v == 7 || v == 8) ? v : 8;
 }
 
 bool batched_chol_enabled(int nfreq) {
@@ -507,6 +547,9 @@ struct DysonBufs {
   double *T;     // diagonal-block scratch of the LAUUM
   PairScratch pairs;  // mixed mode: TF32 pairs of the tensor-core inverse
   double *chol_P = nullptr, *chol_Linv = nullptr;  // batched Cholesky scratch
+  int8_t *oz_planes = nullptr;                       // Ozaki digit planes (all frequencies)
+  double *oz_scale = nullptr, *oz_rowsq = nullptr;
+  int oz_slices = 0;
   int lwork;
 };
 
@@ -536,6 +579,12 @@ DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq, int mode = MBPT_MODE_FP64
     // every step's inverted diagonal blocks are kept: the mixed inverse reads them
     const int64_t steps = (n + kCholNb - 1) / kCholNb;
     b.chol_Linv = ar.take<double>(steps * nfreq * kCholNb * kCholNb);
+    b.oz_slices = ozaki_slices();
+    if (b.oz_slices) {
+      b.oz_planes = ar.take<int8_t>(ozaki_planes_bytes(n, nfreq, b.oz_slices));
+      b.oz_scale = ar.take<double>(static_cast<int64_t>(nfreq) * n);
+      b.oz_rowsq = ar.take<double>(static_cast<int64_t>(nfreq) * kCholNb);
+    }
   }
   if (mode == MBPT_MODE_MIXED) {
     const int64_t np = round_up(n, 128), cap = np * np;
@@ -697,10 +746,20 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
         const int f0 = w0 + static_cast<int>(static_cast<int64_t>(nw) * g / Gw);
         const int f1 = w0 + static_cast<int>(static_cast<int64_t>(nw) * (g + 1) / Gw);
         cudaStream_t gs = stream_of(g);
+        OzakiChol oz;
+        if (b.oz_planes) {
+          // this group's frequencies own a contiguous share of each buffer
+          oz.planes = b.oz_planes + ozaki_planes_bytes(n, f0, b.oz_slices);
+          oz.scale = b.oz_scale + static_cast<int64_t>(f0) * n;
+          oz.rowsq = b.oz_rowsq + static_cast<int64_t>(f0) * kCholNb;
+          oz.slices = b.oz_slices;
+          oz.err = err;
+        }
         rc0 = chol_batched(chi0 + f0 * n * n, n, f1 - f0, b.info + f0,
                            b.chol_P + static_cast<int64_t>(f0) * n * kCholNb,
                            b.chol_Linv + static_cast<int64_t>(f0) * kCholNb * kCholNb,
-                           blas_of(g), gs, static_cast<int64_t>(nfreq) * kCholNb * kCholNb);
+                           blas_of(g), gs, static_cast<int64_t>(nfreq) * kCholNb * kCholNb,
+                           &oz);
         if (rc0) break;
         // this group's log-determinants, info words and events on its own stream
         launch_logdet_diag(chi0 + f0 * n * n, n, f1 - f0, logdet + f0, gs);

@@ -12,8 +12,6 @@ namespace mbpt {
 bool timing_begin(cudaStream_t st, cudaEvent_t *a, cudaEvent_t *b);
 void timing_end(cudaStream_t st, int epi, cudaEvent_t a, cudaEvent_t b);
 
-namespace {
-
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   static std::once_flag once;
@@ -27,6 +25,22 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   });
   return fn;
 }
+
+// The dynamic shared-memory opt-in of a kernel, once per device (the
+// attribute belongs to the function on the current device).
+bool allow_smem(const void *kern, int bytes, std::atomic<uint64_t> &done) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  const uint64_t bit = dev < 64 ? (uint64_t{1} << dev) : 0;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return true;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+      cudaSuccess)
+    return false;
+  done.fetch_or(bit, std::memory_order_release);
+  return true;
+}
+
+namespace {
 
 // rows x cols matrix (cols contiguous) of BF16 or FP32 (TF32) words, boxes of
 // one 128-byte row (64 BF16 / 32 FP32 columns) x box_rows, 128-byte swizzle.
@@ -46,20 +60,6 @@ bool make_tmap(CUtensorMap *m, const void *base, int64_t rows, int64_t cols, int
                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
-}
-
-// The dynamic shared-memory opt-in of a kernel, once per device (the
-// attribute belongs to the function on the current device).
-bool allow_smem(const void *kern, int bytes, std::atomic<uint64_t> &done) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return false;
-  const uint64_t bit = dev < 64 ? (uint64_t{1} << dev) : 0;
-  if (bit && (done.load(std::memory_order_acquire) & bit)) return true;
-  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
-      cudaSuccess)
-    return false;
-  done.fetch_or(bit, std::memory_order_release);
-  return true;
 }
 
 template <int NACC, int BN, int EPI, bool TF32, int DRAIN>

@@ -1,6 +1,9 @@
 // Internal (C++) interface between the route orchestration and the kernels.
 #pragma once
+#include <atomic>
 #include <cstdint>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include "umma_gemm.cuh"
@@ -48,6 +51,26 @@ int gemm_timing(int enable, double *total_ms, long long *launches);
 // instead of their epilogue kind (-1: back to the epilogue kind).
 void timing_tag(int tag);
 constexpr int kTimingDyson = 7;  // TF32 products of the Dyson step's inverse
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (null when
+// the driver lacks it), and a kernel's dynamic shared-memory opt-in, once per
+// device (one bit per device in `done`).
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn();
+bool allow_smem(const void *kern, int bytes, std::atomic<uint64_t> &done);
+
+// ---- Ozaki-scheme FP64 updates of the batched Cholesky (ozaki.cu) ----
+// Bytes of the int8 digit planes of nmat n x n factors cut into `slices`.
+size_t ozaki_planes_bytes(int64_t n, int nmat, int slices);
+// scale[f][r] = 2^e_r >= sqrt(A_rr) of each matrix (column-major, ld n).
+int ozaki_chol_scales(const double *A, int64_t n, int nmat, double *scale, cudaStream_t st);
+// Cut block column [j0, j0 + nb) of every factor (rows j0..n-1) into digit planes.
+int ozaki_chol_slice(const double *A, int64_t n, int nmat, int64_t j0, int nb,
+                     const double *scale, int8_t *planes, int slices, cudaStream_t st);
+// P -= L[j0:, :j0] L[j0:j0+nb, :j0]^T for every matrix from the digit planes
+// (the diagonal entries from exact FP64 row norms kept in rowsq, nmat x nb).
+int ozaki_chol_update(double *A, int64_t n, int nmat, int64_t j0, int nb, double *P,
+                      const double *scale, const int8_t *planes, int slices, double *rowsq,
+                      int *err, cudaStream_t st);
 
 // Bump allocator over a caller's workspace (1024-byte aligned slices).
 struct Arena {

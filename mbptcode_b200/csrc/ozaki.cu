@@ -1,0 +1,463 @@
+// FP64-accurate trailing updates of the batched Cholesky on the int8 tensor
+// cores (tcgen05.mma kind::i8, exact int32 accumulation): the Ozaki scheme.
+//
+// Each row r of the factor L is scaled by 2^-e_r, with 2^e_r >= sqrt(A_rr)
+// (|L_rk| <= sqrt(A_rr) for a positive definite A), and cut into S signed
+// digits: x = L_rk 2^-e_r, |x| <= 1, x = sum_s d_s 2^-(7s-1) + O(2^-7S),
+// d_s in [-64, 64]. A block column of L is cut once, when it is final, into S
+// int8 planes (row r, K = column k contiguous). The update of step j,
+// P -= L[j0:, :j0] L[j0:j0+nb, :j0]^T, is then
+//   sum over levels l = s + t (2 <= l <= S + 1) of 2^(2 - 7l) sum_(s+t=l) D_s D_t^T,
+// each level one int32 TMEM accumulator fed by exact 8-bit products (|sum| <=
+// S 64^2 K < 2^31 for K below 65 536), combined in FP64 in the epilogue and
+// scaled by 2^(e_r + e_c). The terms dropped (s + t > S + 1) have no sign
+// preference off the diagonal; on it (a row against itself) their squares
+// are all positive, so each step's diagonal entries are taken from an exact
+// FP64 row norm instead (chol_rowsq_kernel).
+//
+// Kernel layout: 128 x 64 output tiles (rows r of the panel, 64 of its
+// columns), warp 0 the TMA producer (64-byte swizzled boxes of 64 K), warp 1
+// the TMEM owner and MMA issuer (S(S+1)/2 products per 32-wide K step), warps
+// 2-5 the epilogue; two pipeline stages of S A-planes and S B-planes; every
+// mbarrier wait bounded, as in the split engine.
+#include "internal.h"
+
+namespace mbpt {
+namespace ozaki {
+
+using umma::mbar_expect_tx;
+using umma::mbar_init;
+using umma::mbar_wait;
+using umma::mma_commit;
+using umma::smem_u32;
+using umma::tc_fence_after;
+using umma::tc_fence_before;
+
+constexpr int BM = 128;   // panel rows per tile
+constexpr int BN = 64;    // panel columns per tile
+constexpr int BKB = 64;   // K bytes (int8 elements) per stage
+
+template <int S>
+struct Layout {
+  static constexpr int kAPlane = BM * BKB;   // 8 KB
+  static constexpr int kBPlane = BN * BKB;   // 4 KB
+  static constexpr int kStageBytes = S * (kAPlane + kBPlane);
+  static constexpr int kStages = 2;
+  static constexpr int kSmemBytes = kStages * kStageBytes + 1024 + 256;
+  static constexpr int kLevels = S;
+  static constexpr int kTmemCols = 512;
+  static_assert(kLevels * BN <= 512, "levels exceed TMEM");
+};
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *tm, int x, int y,
+                                            int z, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// K-major operand, 64-byte swizzle: 8-row groups 512 bytes apart.
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= static_cast<uint64_t>((saddr & 0x3FFFFu) >> 4);
+  d |= static_cast<uint64_t>(1) << 16;
+  d |= static_cast<uint64_t>(512 >> 4) << 32;
+  d |= static_cast<uint64_t>(1) << 46;
+  d |= static_cast<uint64_t>(4) << 61;
+  return d;
+}
+
+// Instruction descriptor: s8 x s8 -> s32, both K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t idesc_s8(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(n >> 3) << 17) |
+         (static_cast<uint32_t>(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_s8(uint32_t tmem_d, uint64_t da, uint64_t db,
+                                       uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void tmem_ld32_s32(uint32_t addr, int (&v)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+        "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+        "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+        "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+        "=r"(v[31])
+      : "r"(addr)
+      : "memory");
+}
+
+struct UpdateArgs {
+  CUtensorMap tm_a;    // digit planes, dims (npad K, npad rows, S * nmat planes), box 64 x 128
+  CUtensorMap tm_b;    // the same planes, box 64 x 64
+  int64_t n;           // matrix size
+  int j0, nb;          // the step's first column and width (<= 128)
+  int k_tiles;         // j0 / 64
+  int nmat;
+  double *P;           // nmat panels, column-major m x nb (ld m), m = n - j0
+  int64_t p_stride;    // elements between panels
+  const double *scale; // nmat x n: 2^e_r
+  const double *rowsq; // nmat x nb: sum_(k < j0) L_(j0+i, k)^2, exact
+  int tiles_m;
+  int *err;
+};
+
+template <int S>
+__global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_constant__ UpdateArgs p) {
+  using L = Layout<S>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = reinterpret_cast<uint8_t *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + L::kStages * L::kStageBytes);
+  uint64_t *empty = full + L::kStages;
+  uint64_t *accum = empty + L::kStages;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(accum + 1);
+  int *fail = reinterpret_cast<int *>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int f = blockIdx.y;
+  const int tm = blockIdx.x >> 1, tn = blockIdx.x & 1;
+  const int r0 = tm * BM;       // panel row (matrix row j0 + r0)
+  const int c0 = tn * BN;       // panel column
+  if (c0 >= p.nb) return;       // uniform: the second half of a narrow last panel
+  const int m = static_cast<int>(p.n - p.j0);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < L::kStages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accum, 1);
+    *fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(L::kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      bool ok = true;
+      int it = 0;
+      for (int kt = 0; kt < p.k_tiles; ++kt, ++it) {
+        const int s = it % L::kStages;
+        const uint32_t ph = (it / L::kStages) & 1;
+        if (!mbar_wait(&empty[s], ph ^ 1)) { ok = false; break; }
+        mbar_expect_tx(&full[s], L::kStageBytes);
+        uint8_t *st = smem + s * L::kStageBytes;
+        const int kx = kt * BKB;
+#pragma unroll
+        for (int q = 0; q < S; ++q) {
+          const int plane = q * p.nmat + f;
+          tma_load_3d(st + q * L::kAPlane, &p.tm_a, kx, p.j0 + r0, plane, &full[s]);
+          tma_load_3d(st + S * L::kAPlane + q * L::kBPlane, &p.tm_b, kx, p.j0 + c0, plane,
+                      &full[s]);
+        }
+      }
+      if (!ok) {
+        atomicExch(fail, 1);
+        DevErr{p.err}.set(MBPT_ERR_TIMEOUT);
+      }
+      for (int q = max(0, it - L::kStages); q < it; ++q)
+        mbar_wait(&full[q % L::kStages], (q / L::kStages) & 1);
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = idesc_s8(BN);
+      bool ok = true;
+      for (int kt = 0; kt < p.k_tiles; ++kt) {
+        const int s = kt % L::kStages;
+        const uint32_t ph = (kt / L::kStages) & 1;
+        if (!mbar_wait(&full[s], ph) || *reinterpret_cast<volatile int *>(fail)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t st = smem_u32(smem + s * L::kStageBytes);
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk) {
+          const uint64_t adv = static_cast<uint64_t>(kk * 2);  // 32 bytes >> 4
+          const bool first = kt == 0 && kk == 0;
+#pragma unroll
+          for (int lev = 2; lev <= S + 1; ++lev) {
+            const uint32_t d = tmem + static_cast<uint32_t>((lev - 2) * BN);
+            const int s_lo = lev - S > 1 ? lev - S : 1;
+            const int s_hi = lev - 1 < S ? lev - 1 : S;
+#pragma unroll
+            for (int sa = s_lo; sa <= s_hi; ++sa) {
+              const int sb = lev - sa;
+              const uint64_t da = sw64_desc(st + (sa - 1) * L::kAPlane) + adv;
+              const uint64_t db = sw64_desc(st + S * L::kAPlane + (sb - 1) * L::kBPlane) + adv;
+              mma_s8(d, da, db, idesc, (first && sa == s_lo) ? 0u : 1u);
+            }
+          }
+        }
+        mma_commit(&empty[s]);
+      }
+      if (!ok) {
+        atomicExch(fail, 1);
+        DevErr{p.err}.set(MBPT_ERR_TIMEOUT);
+      }
+      mma_commit(accum);
+      mbar_wait(accum, 0);  // no MMA may still write TMEM when it is freed
+    }
+    __syncwarp();
+  } else {
+    const int sp = warp & 3;
+    const uint32_t taddr = tmem + (static_cast<uint32_t>(sp * 32) << 16);
+    const bool ok = mbar_wait(accum, 0) && !*reinterpret_cast<volatile int *>(fail);
+    __syncwarp();
+    if (!ok) {
+      if (lane == 0) DevErr{p.err}.set(MBPT_ERR_TIMEOUT);
+    } else {
+      tc_fence_after();
+      const int pr = r0 + sp * 32 + lane;             // panel row of this thread
+      const int64_t row = p.j0 + pr;                  // matrix row
+      const double *sc = p.scale + static_cast<int64_t>(f) * p.n;
+      const double srow = pr < m ? sc[row] : 0.0;
+      double *P = p.P + static_cast<int64_t>(f) * p.p_stride;
+#pragma unroll 1
+      for (int ch = 0; ch < BN / 32; ++ch) {
+        double acc[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) acc[i] = 0.0;
+        // smallest levels first
+#pragma unroll 1
+        for (int lev = S + 1; lev >= 2; --lev) {
+          int v[32];
+          tmem_ld32_s32(taddr + static_cast<uint32_t>((lev - 2) * BN + ch * 32), v);
+          const double w = ldexp(1.0, 2 - 7 * lev);
+#pragma unroll
+          for (int i = 0; i < 32; ++i) acc[i] += static_cast<double>(v[i]) * w;
+        }
+        if (pr < m) {
+#pragma unroll
+          for (int i = 0; i < 32; ++i) {
+            const int pc = c0 + ch * 32 + i;        // panel column
+            if (pc < p.nb) {
+              double *dst = P + static_cast<int64_t>(pc) * m + pr;
+              if (pr == pc)
+                *dst -= p.rowsq[static_cast<int64_t>(f) * p.nb + pc];
+              else
+                *dst -= acc[i] * srow * sc[p.j0 + pc];
+            }
+          }
+        }
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(L::kTmemCols)
+                 : "memory");
+  }
+}
+
+// scale[f][r] = 2^e_r with e_r = ceil(log2(sqrt(A_rr))) (A column-major, ld n);
+// 1 for a diagonal that is not positive and finite (that matrix fails its
+// factorisation and is redone by LU; its digits only need to stay in range).
+__global__ void chol_scale_kernel(const double *A, int64_t n, int64_t mat_stride, int nmat,
+                                  double *scale) {
+  const int64_t total = n * nmat;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t f = i / n, r = i % n;
+    const double a = A[f * mat_stride + r * n + r];
+    double s = 1.0;
+    if (a > 0.0 && a < 1e300) {
+      int e;
+      frexp(sqrt(a), &e);          // sqrt(a) = m 2^e, m in [0.5, 1): 2^e >= sqrt(a)
+      s = ldexp(1.0, e);
+    }
+    scale[i] = s;
+  }
+}
+
+// Digits of block column [j0, j0 + nb) of L (column-major in A, ld n, rows
+// j0..n-1): plane q of matrix f, row r, K = column c, at
+// D[((q * nmat + f) * npad + r) * npad + c]. Rows are read contiguously through
+// shared memory and written 16 columns per thread.
+template <int S>
+__global__ void chol_slice_kernel(const double *A, int64_t n, int64_t mat_stride, int nmat,
+                                  int j0, int nb, const double *scale, int8_t *D,
+                                  int64_t npad) {
+  __shared__ double tile[32][129];
+  const int f = blockIdx.y;
+  const int64_t rbase = j0 + static_cast<int64_t>(blockIdx.x) * 32;
+  const double *Af = A + f * mat_stride;
+  // load 32 rows x nb columns: threads walk rows fastest (column-major source)
+  for (int t = threadIdx.x; t < 32 * 128; t += blockDim.x) {
+    const int rr = t & 31, cc = t >> 5;
+    const int64_t r = rbase + rr;
+    // the factor is lower triangular: above the block's diagonal A still holds
+    // 1 - chi0, which is not part of L
+    tile[rr][cc] = (r < n && cc < nb && r >= j0 + cc)
+                       ? Af[static_cast<int64_t>(j0 + cc) * n + r] : 0.0;
+  }
+  __syncthreads();
+  // each thread: one row, 16 consecutive columns, all S planes
+  const int rr = threadIdx.x >> 3, cg = (threadIdx.x & 7) * 16;
+  const int64_t r = rbase + rr;
+  if (r >= n) return;
+  const double inv = 64.0 / scale[static_cast<int64_t>(f) * n + r];
+  __align__(16) int8_t out[S][16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    double t = tile[rr][cg + i] * inv;   // |t| <= 64
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      double d = rint(t);
+      d = fmin(fmax(d, -127.0), 127.0);  // non-finite input stays in range
+      out[q][i] = static_cast<int8_t>(static_cast<int>(d));
+      t = (t - d) * 128.0;
+    }
+  }
+  if (cg >= nb) return;
+#pragma unroll
+  for (int q = 0; q < S; ++q) {
+    int8_t *dst = D + ((static_cast<int64_t>(q) * nmat + f) * npad + r) * npad + j0 + cg;
+    *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(out[q]);
+  }
+}
+
+// rowsq[f][i] = sum_(k < j0) L_(j0+i, k)^2 in FP64 (one thread per row).
+__global__ void chol_rowsq_kernel(const double *A, int64_t n, int64_t mat_stride, int j0, int nb,
+                                  double *rowsq) {
+  const int f = blockIdx.y, i = threadIdx.x;
+  if (i >= nb) return;
+  const double *Af = A + f * mat_stride;
+  const int64_t r = j0 + i;
+  double s = 0.0;
+  for (int64_t k = 0; k < j0; ++k) {
+    const double x = Af[k * n + r];
+    s = fma(x, x, s);
+  }
+  rowsq[static_cast<int64_t>(f) * nb + i] = s;
+}
+
+bool make_plane_map(CUtensorMap *m, const int8_t *D, int64_t npad, int64_t planes,
+                    int box_rows) {
+  auto fn = encode_fn();
+  if (!fn || (reinterpret_cast<uintptr_t>(D) & 15) || npad % 128) return false;
+  cuuint64_t dims[3] = {static_cast<cuuint64_t>(npad), static_cast<cuuint64_t>(npad),
+                        static_cast<cuuint64_t>(planes)};
+  cuuint64_t strides[2] = {static_cast<cuuint64_t>(npad),
+                           static_cast<cuuint64_t>(npad * npad)};
+  cuuint32_t box[3] = {static_cast<cuuint32_t>(BKB), static_cast<cuuint32_t>(box_rows), 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t *>(D), dims, strides, box,
+            es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+inline int grid_blocks(int64_t n) {
+  int64_t b = (n + 255) / 256;
+  return static_cast<int>(b > 148 * 32 ? 148 * 32 : (b < 1 ? 1 : b));
+}
+
+}  // namespace ozaki
+
+size_t ozaki_planes_bytes(int64_t n, int nmat, int slices) {
+  const int64_t npad = round_up(n, 128);
+  return static_cast<size_t>(slices) * nmat * npad * npad;
+}
+
+int ozaki_chol_scales(const double *A, int64_t n, int nmat, double *scale, cudaStream_t st) {
+  count_launch();
+  ozaki::chol_scale_kernel<<<ozaki::grid_blocks(n * nmat), 256, 0, st>>>(A, n, n * n, nmat,
+                                                                         scale);
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+int ozaki_chol_slice(const double *A, int64_t n, int nmat, int64_t j0, int nb,
+                     const double *scale, int8_t *planes, int slices, cudaStream_t st) {
+  const int64_t npad = round_up(n, 128);
+  dim3 grid(static_cast<unsigned>((n - j0 + 31) / 32), nmat);
+  count_launch();
+  if (slices == 8)
+    ozaki::chol_slice_kernel<8><<<grid, 256, 0, st>>>(A, n, n * n, nmat, static_cast<int>(j0),
+                                                      nb, scale, planes, npad);
+  else if (slices == 7)
+    ozaki::chol_slice_kernel<7><<<grid, 256, 0, st>>>(A, n, n * n, nmat, static_cast<int>(j0),
+                                                      nb, scale, planes, npad);
+  else
+    return MBPT_ERR_SHAPE;
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+int ozaki_chol_update(double *A, int64_t n, int nmat, int64_t j0, int nb, double *P,
+                      const double *scale, const int8_t *planes, int slices, double *rowsq,
+                      int *err, cudaStream_t st) {
+  if (j0 <= 0) return MBPT_OK;
+  if (j0 % ozaki::BKB || nb < 1 || nb > 128 || j0 >= 65536) return MBPT_ERR_SHAPE;
+  const int64_t npad = round_up(n, 128);
+  ozaki::UpdateArgs p;
+  if (!ozaki::make_plane_map(&p.tm_a, planes, npad, static_cast<int64_t>(slices) * nmat,
+                             ozaki::BM) ||
+      !ozaki::make_plane_map(&p.tm_b, planes, npad, static_cast<int64_t>(slices) * nmat,
+                             ozaki::BN))
+    return MBPT_ERR_SHAPE;
+  const int64_t m = n - j0;
+  p.n = n;
+  p.j0 = static_cast<int>(j0);
+  p.nb = nb;
+  p.k_tiles = static_cast<int>(j0 / ozaki::BKB);
+  p.nmat = nmat;
+  p.P = P;
+  p.p_stride = m * nb;
+  p.scale = scale;
+  p.rowsq = rowsq;
+  p.tiles_m = static_cast<int>((m + ozaki::BM - 1) / ozaki::BM);
+  p.err = err;
+  count_launch();
+  ozaki::chol_rowsq_kernel<<<dim3(1, nmat), 128, 0, st>>>(A, n, n * n, static_cast<int>(j0),
+                                                          nb, rowsq);
+  const dim3 grid(static_cast<unsigned>(p.tiles_m * 2), nmat);
+  static std::atomic<uint64_t> attr8{0}, attr7{0};
+  if (slices == 8) {
+    auto kern = ozaki::chol_update_kernel<8>;
+    const int smem = ozaki::Layout<8>::kSmemBytes;
+    if (!allow_smem(reinterpret_cast<const void *>(kern), smem, attr8)) return MBPT_ERR_CUDA;
+    count_launch();
+    kern<<<grid, 192, smem, st>>>(p);
+  } else if (slices == 7) {
+    auto kern = ozaki::chol_update_kernel<7>;
+    const int smem = ozaki::Layout<7>::kSmemBytes;
+    if (!allow_smem(reinterpret_cast<const void *>(kern), smem, attr7)) return MBPT_ERR_CUDA;
+    count_launch();
+    kern<<<grid, 192, smem, st>>>(p);
+  } else {
+    return MBPT_ERR_SHAPE;
+  }
+  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+}  // namespace mbpt

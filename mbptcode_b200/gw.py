@@ -635,6 +635,26 @@ def solve_qp_diagonal_space_time(mf, mol, nocc, states=None, **kw):
 
 
 HARTREE_TO_EV = 27.211386245988  # MBPTcode constants.py:11 (CODATA 2018)
+# self_consistency values entering the evGW loop and the screening each keeps
+# (``GW/qp_energy.py:64-65``)
+EVGW_SCREENING = {'evgw': 'updated', 'ev': 'updated', 'evgw0': 'fixed', 'ev0': 'fixed'}
+
+
+class _MeanFieldView:
+    """The fields of a mean field the space-time drivers read, for a caller
+    that hands a bare spectrum with nocc (or an object lacking some)."""
+
+    def __init__(self, mf, eps, nocc):
+        self.__dict__.update(getattr(mf, '__dict__', {}))
+        self.mo_energy = np.asarray(eps, float)
+        if isinstance(nocc, tuple):
+            self.nelec = nocc
+        elif not hasattr(self, 'mo_occ'):
+            self.mo_occ = np.where(np.arange(self.mo_energy.size) < nocc, 2.0, 0.0)
+
+
+def _mean_field_view(mf, eps, nocc):
+    return _MeanFieldView(mf, eps, nocc)
 
 
 def _resolve_states(state, nocc):
@@ -687,16 +707,22 @@ def calc_qp_energy(mf, selfenergy='GW', polarizability='RPA', df=True, eta=None,
                 else int((occ > 0).sum()))
     nocc_ch = nocc[0 if spin_channel == 'alpha' else 1] if isinstance(nocc, tuple) else nocc
     states = _resolve_states(state, nocc_ch)
-    if self_consistency in ('evGW', 'evgw'):
-        if continuation != 'pade' or eps_anchor is not None or eps.ndim != 1:
-            raise NotImplementedError("self_consistency='evGW' runs the restricted Pade route "
-                                      "without eps_anchor")
+    consistency = str(self_consistency).lower()
+    if consistency in EVGW_SCREENING:
+        if eps_anchor is not None:
+            raise TypeError(f'self_consistency={self_consistency!r} sets its own anchor every '
+                            f'cycle, so eps_anchor would be overwritten by the loop rather '
+                            f'than read')
+        if continuation != 'pade':
+            raise ValueError(f"self_consistency={self_consistency!r} drives continuation="
+                             f"'pade' only, not {continuation!r}")
         from .evgw import evgw_eigenvalues
-        X, D = _factors(route_kwargs.get('factors'))
-        e, _ = evgw_eigenvalues(X, D, eps, nocc, precision=route_kwargs.get('precision'))
-        res = [float(e[p]) * HARTREE_TO_EV for p in states]
+        e, _ = evgw_eigenvalues(_mean_field_view(mf, eps, nocc), None, mode='space-time',
+                                screening=EVGW_SCREENING[consistency], **route_kwargs)
+        e_ch = e if e.ndim == 1 else e[0 if spin_channel == 'alpha' else 1]
+        res = [float(e_ch[p]) * HARTREE_TO_EV for p in states]
         z = None
-    elif self_consistency != 'G0W0':
+    elif consistency != 'g0w0':
         raise NotImplementedError(f'self_consistency={self_consistency!r} is outside the device '
                                   'route')
     elif continuation in ('laplace', 'cd'):

@@ -6,7 +6,8 @@ importing modules bind by name (``GW/space_time.py:66-79``,
 the static screening in ``BSE/solve.py:70``, ``GW/contour_deformation.py:104``,
 ``gradients/gwbse/reaction_field_adjoint.py:33``; the contour's explicit
 residue backend in ``GW/real_screening.py:57`` and
-``GW/contour_deformation.py:96``),
+``GW/contour_deformation.py:96``; the evGW loop, which ``GW/qp_energy.py:242``
+reaches as ``evGW.evgw_eigenvalues``),
 and its own tests substitute them with ``monkeypatch.setattr(module, name,
 ...)`` (``tests/test_rpa_log_determinant.py:57-72``). `install()` does the
 same for every module that holds one of the names, so every caller --
@@ -21,7 +22,7 @@ import importlib
 
 import numpy as np
 
-from . import adjoint, contour, gw, space_time
+from . import adjoint, contour, evgw, gw, space_time
 
 LR = 'src.SingleReference.LinearResponse.space_time'
 IT = 'src.SingleReference.GW.imaginary_time'
@@ -34,6 +35,7 @@ BSE = 'src.SingleReference.BSE.solve'
 CD = 'src.SingleReference.GW.contour_deformation'
 RF = 'src.gradients.gwbse.reaction_field_adjoint'
 RS = 'src.SingleReference.GW.real_screening'
+EV = 'src.SingleReference.GW.evGW'
 
 _SAVED: dict = {}
 
@@ -102,6 +104,7 @@ def replacements():
              'ExplicitRealScreening': contour.ExplicitRealScreening,
              'wc_explicit': contour.wc_explicit},
         RS: {'ExplicitRealScreening': contour.ExplicitRealScreening},
+        EV: {'evgw_eigenvalues': evgw.evgw_eigenvalues},
         RF: dict(static),
         ADJ: {'polarizability_backward': adjoint.polarizability_backward,
               'selfenergy_diag_backward': adjoint.selfenergy_diag_backward,

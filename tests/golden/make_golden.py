@@ -44,6 +44,14 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
 * sigma_ao.npz       the full AO self-energy with an AO collocation that is not
                      the MO one, a subset of its time points, its MO diagonal,
                      and the chi0 sweep's reverse for a seeded proj_bar;
+* evgw.npz           the reference's evGW loop (GW/evGW.py) through its
+                     space-time driver on two synthetic systems (default
+                     numerics) and a windowed, damped run: the spectra,
+                     cycles and convergence histories;
+* drop_in.npz        the seam calls MBPTcode's own G0W0 driver, dRPA energy
+                     and adjoint make (every name plugin.install() rebinds,
+                     recorded with its arguments and result), and the
+                     drivers' outputs;
 * qp_kat.npz         the root finder on closed-form self-energies
                      (tests/test_qp_refine_root.py's two-pole Sigma and others);
 * c1_<variant>.npz   the synthetic FP64 configuration at full size (n_orb = 400,
@@ -53,7 +61,7 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      stored: the tests regenerate them from the seed and check
                      the regeneration against the stored eps and checksums.
 
-    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|contour_explicit|contour_unrestricted|sigma_ao]
+    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|contour_explicit|contour_unrestricted|sigma_ao|evgw|drop_in]
 """
 import os
 import sys
@@ -333,11 +341,21 @@ def sigma_adjoint_fixture(ntau=12, nfreq=10):
         sigma=sigma, eps_bar=eps_bar, X_bar=X_bar, D_bar=D_bar)
 
 
-def _import_contour_deformation():
-    """MBPTcode's GW/contour_deformation.py imports pyscf at module load for
-    its driver (mean field, integrals); the functions this fixture calls never
-    touch it. pyscf is absent here, so a stand-in package whose every
-    attribute raises when called lets the module load."""
+_STAND_IN = []
+
+
+def _install_stand_ins():
+    """MBPTcode's drivers import pyscf (and, through the CC package that
+    evGW's DIIS lives in, opt_einsum) at module load for what this fixture
+    never runs: integrals, SCF, coupled cluster. Both are absent here, so a
+    stand-in package whose every attribute raises when called lets the
+    modules load. One call is answered: pyscf.df.addons.make_auxmol returns
+    an inert placeholder, because the space-time driver builds the auxiliary
+    molecule of the solvent gauge transform unconditionally
+    (GW/reaction_field.py:98) and, in the gas phase, the transform returns
+    None without reading it (GW/reaction_field.py:67-68)."""
+    if _STAND_IN:
+        return
     import importlib.abc
     import importlib.machinery
     import types
@@ -350,10 +368,15 @@ def _import_contour_deformation():
             return _Inert(self._n + '.' + name)
 
         def __call__(self, *a, **k):
+            if self._n == 'pyscf.df.addons.make_auxmol':
+                return _Inert('auxmol placeholder')
             raise RuntimeError(f'{self._n}: pyscf is not available here')
 
         def __mro_entries__(self, bases):
             return (object,)
+
+        def __instancecheck__(self, obj):
+            return False
 
     class _Package(types.ModuleType):
         def __init__(self, name):
@@ -367,7 +390,7 @@ def _import_contour_deformation():
 
     class _Finder(importlib.abc.MetaPathFinder, importlib.abc.Loader):
         def find_spec(self, fullname, path, target=None):
-            if fullname == 'pyscf' or fullname.startswith('pyscf.'):
+            if fullname.split('.')[0] in ('pyscf', 'opt_einsum'):
                 return importlib.machinery.ModuleSpec(fullname, self, is_package=True)
             return None
 
@@ -378,9 +401,190 @@ def _import_contour_deformation():
             pass
 
     sys.meta_path.insert(0, _Finder())
+    _STAND_IN.append(True)
+
+
+def _import_contour_deformation():
+    """The contour-deformation modules, loaded with the stand-ins."""
+    _install_stand_ins()
     import src.SingleReference.GW.contour_deformation as cd
     import src.SingleReference.GW.real_screening as rs
     return cd, rs
+
+
+class _Molecule:
+    """The fields of a pyscf Mole the space-time drivers read for a
+    closed-shell gas-phase reference with pre-built factors."""
+
+    def __init__(self, nocc):
+        self.nelectron = 2 * nocc
+        self.spin = 0
+        self.basis = 'cc-pvdz'
+
+
+class _MeanField:
+    """The fields of a pyscf RHF object the drivers read when the factors
+    come pre-built: the spectrum, occupations, MO coefficients (identity: the
+    AO collocation is the MO one) and the AO overlap (identity)."""
+
+    def __init__(self, eps, nocc):
+        self.mo_energy = np.asarray(eps, float)
+        n = self.mo_energy.size
+        self.mo_occ = np.where(np.arange(n) < nocc, 2.0, 0.0)
+        self.mo_coeff = np.eye(n)
+        self.mol = _Molecule(nocc)
+        self._nocc = nocc
+
+    def get_ovlp(self):
+        return np.eye(self.mo_energy.size)
+
+    def copy(self):
+        return _MeanField(self.mo_energy, self._nocc)
+
+
+def evgw_fixture():
+    """The reference's own evGW loop (GW/evGW.py:78-229) on synthetic
+    factors through calc_qp_energy(mode='space-time') and its space-time
+    driver, with the stand-ins for pyscf: two systems, default numerics
+    (auto-sized grids, DIIS 8 from the second cycle) and a windowed run
+    (update a frontier window, linear mixing with damping 0.3)."""
+    _install_stand_ins()
+    import dataclasses
+    from src.SingleReference.GW import evGW
+    from src.Base.numerics.numerics import numerics_or_default
+    out = {}
+    systems = {'a': (24, 4, 96, 5), 'b': (32, 5, 128, 13)}
+    for key, (n, nocc, M, seed) in systems.items():
+        X, D, eps = synthetic_system(n, nocc, M, seed=seed, variant='calibrated')
+        mf = _MeanField(eps, nocc)
+        with warnings.catch_warnings():
+            warnings.simplefilter('ignore')
+            e, info = evGW.evgw_eigenvalues(mf, mf.mol, mode='space-time', factors=(X, D),
+                                            xc_diagonal=np.zeros(n))
+        out.update({f'{key}_X': X, f'{key}_D': D, f'{key}_eps0': eps,
+                    f'{key}_size': np.array([n, nocc, M, seed]), f'{key}_eps': e,
+                    f'{key}_cycles': info['cycles'], f'{key}_history': np.array(info['history']),
+                    f'{key}_converged': info['converged']})
+    # windowed, damped: orbitals 2..7 of system a move, linear mixing
+    n, nocc, M, seed = systems['a']
+    X, D, eps = out['a_X'], out['a_D'], out['a_eps0']
+    base = numerics_or_default(None)
+    num = dataclasses.replace(base, evgw=dataclasses.replace(base.evgw, diis_size=0,
+                                                             damping=0.3))
+    mf = _MeanField(eps, nocc)
+    update = np.arange(2, 8)
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        e, info = evGW.evgw_eigenvalues(mf, mf.mol, mode='space-time', factors=(X, D),
+                                        xc_diagonal=np.zeros(n), numerics=num, update=update)
+    out.update({'w_update': update, 'w_damping': 0.3, 'w_eps': e, 'w_cycles': info['cycles'],
+                'w_history': np.array(info['history']), 'w_frozen': info['frozen']})
+    np.savez_compressed(os.path.join(HERE, 'evgw.npz'), **out)
+
+
+GRID_FIELDS = ('tau_points', 'tau_weights', 'omega_points', 'omega_weights', 'cosft_wt')
+
+
+def _encode(value, key, arrays, seen):
+    """A JSON description of one call argument; arrays are copied into
+    `arrays` (each distinct array once, found again by its bytes through
+    `seen`), a TimeFrequencyGrid as its fields."""
+    import hashlib
+    if isinstance(value, np.ndarray):
+        h = hashlib.sha1(value.tobytes() + str((value.dtype, value.shape)).encode()).hexdigest()
+        if h not in seen:
+            seen[h] = key
+            arrays[key] = np.array(value)
+        return {'array': seen[h]}
+    if hasattr(value, 'tau_points') and hasattr(value, 'cosft_wt'):
+        for f in GRID_FIELDS:
+            arrays[f'{key}_{f}'] = np.array(getattr(value, f))
+        return {'grid': key}
+    if isinstance(value, (np.integer,)):
+        return {'value': int(value)}
+    if isinstance(value, (np.floating,)):
+        return {'value': float(value)}
+    if isinstance(value, (list, tuple)) and all(np.isscalar(v) for v in value):
+        return {'value': [v.item() if hasattr(v, 'item') else v for v in value]}
+    if value is None or isinstance(value, (bool, int, float, str)):
+        return {'value': value}
+    if isinstance(value, dict) and not value:
+        return {'value': {}}
+    return {'opaque': type(value).__name__}
+
+
+def drop_in_fixture():
+    """The seam calls the reference's own drivers make, and what each seam
+    returned: MBPTcode's G0W0 driver (GW/space_time.py:631-863, through the
+    stand-ins for pyscf with pre-built factors), its dRPA energy
+    (LinearResponse/space_time.py:1100-1183) and adjoint
+    (gradients/rpa/space_time_adjoint.py:473-563) run with every name that
+    `mbptcode_b200.plugin.install()` rebinds wrapped by a recorder that keeps
+    the arguments and the result of each call (the first few calls per
+    name) and forwards to the reference's own function. A GPU test replays
+    the recorded calls through the device seams."""
+    import json
+    _install_stand_ins()
+    import importlib
+    from mbptcode_b200 import plugin
+    from src.SingleReference.GW import space_time as gst
+    from src.SingleReference.LinearResponse import space_time as lst
+    from src.gradients.rpa import space_time_adjoint as adj
+    n, nocc, M, seed = 24, 4, 64, 7
+    X, D, eps = synthetic_system(n, nocc, M, seed=seed, variant='calibrated')
+    arrays = {'X': X, 'D': D, 'eps': eps}
+    calls, counts, saved, seen = [], {}, [], {}
+    keep = {'solve_qp_from_imaginary_axis': 6, 'dielectric_log_determinant': 4}
+    for modname, names in plugin.replacements().items():
+        try:
+            mod = importlib.import_module(modname)
+        except Exception:                    # noqa: BLE001 -- modules outside the route
+            continue
+        for name in names:
+            if not hasattr(mod, name):
+                continue
+            original = getattr(mod, name)
+
+            def recorder(*a, _name=name, _mod=modname, _f=original, **k):
+                i = counts.get(_name, 0)
+                counts[_name] = i + 1
+                if i >= keep.get(_name, 2):
+                    return _f(*a, **k)
+                c = len(calls)
+                desc = {'module': _mod, 'name': _name,
+                        'args': [_encode(v, f'c{c}_a{j}', arrays, seen) for j, v in enumerate(a)],
+                        'kwargs': {kk: _encode(v, f'c{c}_k_{kk}', arrays, seen)
+                                   for kk, v in k.items()}}
+                calls.append(desc)
+                out = _f(*a, **k)
+                res = out if isinstance(out, tuple) else (out,)
+                desc['result'] = [_encode(np.asarray(r) if np.ndim(r) or isinstance(
+                    r, (np.ndarray, float, complex)) else r, f'c{c}_r{j}', arrays, seen)
+                    for j, r in enumerate(res)]
+                desc['result_tuple'] = isinstance(out, tuple)
+                return out
+            saved.append((mod, name, original))
+            setattr(mod, name, recorder)
+    try:
+        mf = _MeanField(eps, nocc)
+        with warnings.catch_warnings():
+            warnings.simplefilter('ignore')
+            roots = gst.solve_qp_energy_space_time(mf, mf.mol, nocc, np.arange(n),
+                                                   factors=(X, D), xc_diagonal=np.zeros(n))
+            e_min, e_max, mu = particle_hole_window(eps, nocc)
+            ntau = 12
+            freq, fw = screening_frequency_grid(ntau, eps, nocc, mu=mu)
+            grid = TimeFrequencyGrid.minimax_split(ntau, e_min, e_max, freq, fw)
+            e_c = lst.rpa_correlation_energy_space_time(X, D, eps, nocc, grid)
+            e_a, eb, xb, db, _ = adj.rpa_energy_and_adjoint(X, D, eps, nocc, grid)
+    finally:
+        for mod, name, original in saved:
+            setattr(mod, name, original)
+    arrays.update(driver_roots=np.asarray(roots), e_c=np.float64(e_c), eps_bar=eb, X_bar=xb,
+                  D_bar=db)
+    arrays['calls'] = np.array(json.dumps(calls))
+    np.savez_compressed(os.path.join(HERE, 'drop_in.npz'), **arrays)
+    print('recorded', {k: v for k, v in counts.items()})
 
 
 def contour_fixture():
@@ -625,6 +829,14 @@ if __name__ == '__main__':
         sigma_ao_fixture()
         print('AO self-energy fixture written to', HERE)
         sys.exit(0)
+    if ONLY == 'drop_in':
+        drop_in_fixture()
+        print('drop-in call fixture written to', HERE)
+        sys.exit(0)
+    if ONLY == 'evgw':
+        evgw_fixture()
+        print('evGW fixture written to', HERE)
+        sys.exit(0)
     if ONLY == 'contour':
         contour_fixture()
         print('contour-deformation fixture written to', HERE)
@@ -639,7 +851,7 @@ if __name__ == '__main__':
         sys.exit(0)
     if ONLY:
         sys.exit(f'--only {ONLY}: choose c1, static, unrestricted, sigma_adjoint, contour, '
-                 'contour_explicit, contour_unrestricted or sigma_ao')
+                 'contour_explicit, contour_unrestricted, sigma_ao, evgw or drop_in')
     grids_fixture()
     shared_kernel_fixture()
     route_fixture('calibrated', 24, 4, 64, 7, 'calibrated', 12, full=True)
@@ -653,4 +865,6 @@ if __name__ == '__main__':
     contour_explicit_fixture()
     contour_unrestricted_fixture()
     sigma_ao_fixture()
+    evgw_fixture()
+    drop_in_fixture()
     print('fixtures written to', HERE)

@@ -731,7 +731,7 @@ def test_calc_qp_energy_dispatch(golden):
     from mbptcode_b200 import evgw
     e_ev = gw.calc_qp_energy(mf, mode='space-time', self_consistency='evGW',
                              state=[nocc - 1, nocc], factors=(X, D))
-    e_direct, _ = evgw.evgw_eigenvalues(X, D, eps, nocc)
+    e_direct, _ = evgw.evgw_device(X, D, eps, nocc)
     assert np.abs(np.array(e_ev) / ev - e_direct[nocc - 1:nocc + 1]).max() < 1e-12
     with pytest.raises(NotImplementedError):
         gw.calc_qp_energy(mf, mode='casida', factors=(X, D))
