@@ -103,7 +103,11 @@ int mbpt_chi0_sweep(const double *X_dev, int64_t M, int64_t norb, int64_t nocc,
 /* ---- Dyson step and dielectric log-determinant ---------------------------
  * Replaces LinearResponse/space_time.py:956-968 dyson_screening (per
  * frequency, correlation=True) and :1073-1097 dielectric_log_determinant,
- * by a Cholesky factorisation of 1 - chi0 at each frequency (FP64).
+ * by a Cholesky factorisation of 1 - chi0 at each frequency (FP64). From
+ * four frequencies on, one batched factorisation of all of them; with the
+ * environment variable MBPT_DYSON_OZAKI=1 its trailing updates run on the
+ * int8 tensor cores (the Ozaki scheme, FP64-accurate), otherwise as FP64
+ * DGEMMs.
  * chi0_dev (nfreq, naux, naux): in chi0; out W - I = [1 - chi0]^-1 - 1 when
  * want_w, else the Cholesky factors.
  * logdet_dev, trace_dev (nfreq): log det(1 - chi0) and tr chi0.
@@ -120,6 +124,16 @@ size_t mbpt_dyson_workspace_bytes(int64_t naux, int nfreq, int mode);
 int mbpt_dyson(double *chi0_dev, int64_t naux, int nfreq, int want_w, int mode,
                double *logdet_dev, double *trace_dev, int *info_host, int *sign_host,
                void *workspace, size_t ws_bytes, int *err_dev, void *stream);
+/* The same step without a host wait (no synchronisation of the caller's
+ * stream): every frequency's inverse is issued from its Cholesky factor and
+ * its info word lands in info_dev (nfreq ints on the device). A nonzero word
+ * marks a frequency where 1 - chi0 is not positive definite: its W - I and
+ * log-determinant are then not valid, and the caller repeats the step (and
+ * what it fed) with mbpt_dyson, which takes such a frequency through LU. The
+ * workspace is mbpt_dyson_workspace_bytes'. */
+int mbpt_dyson_deferred(double *chi0_dev, int64_t naux, int nfreq, int want_w, int mode,
+                        double *logdet_dev, double *trace_dev, int *info_dev, void *workspace,
+                        size_t ws_bytes, int *err_dev, void *stream);
 
 /* ---- dRPA correlation energy ----------------------------------------------
  * Replaces LinearResponse/space_time.py:1100-1183

@@ -37,6 +37,7 @@ _SIGNATURES = {
                              _p, _p, _sz, _p, _p]),
     'mbpt_dyson_workspace_bytes': (_sz, [_i64, _i, _i]),
     'mbpt_dyson': (_i, [_p, _i64, _i, _i, _i, _p, _p, _p, _p, _p, _sz, _p, _p]),
+    'mbpt_dyson_deferred': (_i, [_p, _i64, _i, _i, _i, _p, _p, _p, _p, _sz, _p, _p]),
     'mbpt_rpa_energy_workspace_bytes': (_sz, [_i64, _i64, _i64, _i64, _i, _i, _i]),
     'mbpt_rpa_energy': (_i, [_p, _i64, _i64, _i64, _p, _d, _p, _i64, _p, _i, _p, _p, _i, _i,
                              _p, _p, _p, _p, _sz, _p, _p]),

@@ -690,9 +690,15 @@ DysonPipe *dyson_pipe(int nfreq) {
 // factorisations of f + 1 and f + 2. A frequency that is not positive definite
 // falls back to LU with every stream drained first. The caller's stream waits
 // for the other two at the end.
+// info_dev_out null: the host reads each frequency's info word before its
+// inverse (a positive definite frequency's W from the factor, any other by
+// LU). Non-null: no host wait; every frequency's inverse is issued from its
+// factor and the info words land in info_dev_out, where a nonzero word marks
+// a frequency whose W - I and log-determinant are not valid.
 int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, double *trace,
               int *info_host, int *sign_host, Arena &ar, cudaStream_t st,
-              int mode = MBPT_MODE_FP64, int *err = nullptr) {
+              int mode = MBPT_MODE_FP64, int *err = nullptr, int *info_dev_out = nullptr) {
+  const bool deferred = info_dev_out != nullptr;
   DysonBufs b = carve_dyson(ar, n, nfreq, mode);
   if (ar.overflow()) return MBPT_ERR_WORKSPACE;
   Handles &h = handles(st);
@@ -763,8 +769,8 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
         if (rc0) break;
         // this group's log-determinants, info words and events on its own stream
         launch_logdet_diag(chi0 + f0 * n * n, n, f1 - f0, logdet + f0, gs);
-        if (cudaMemcpyAsync(pp->info + f0, b.info + f0, sizeof(int) * (f1 - f0),
-                            cudaMemcpyDeviceToHost, gs) != cudaSuccess)
+        if (!deferred && cudaMemcpyAsync(pp->info + f0, b.info + f0, sizeof(int) * (f1 - f0),
+                                         cudaMemcpyDeviceToHost, gs) != cudaSuccess)
           rc0 = MBPT_ERR_CUDA;
         for (int f = f0; f < f1 && !rc0; ++f)
           if (cudaEventRecord(pp->ev[f], gs) != cudaSuccess) rc0 = MBPT_ERR_CUDA;
@@ -803,12 +809,12 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
   for (int f = 0; f < nfac && f < nfreq && rc == MBPT_OK; ++f) rc = factor(f);
   for (int f = 0; f < nfreq && rc == MBPT_OK; ++f) {
     if (f + nfac < nfreq && (rc = factor(f + nfac)) != MBPT_OK) break;
-    if (cudaEventSynchronize(pp->ev[f]) != cudaSuccess) {
+    if (!deferred && cudaEventSynchronize(pp->ev[f]) != cudaSuccess) {
       rc = MBPT_ERR_CUDA;
       break;
     }
-    const int inf = pp->info[f];
-    if (info_host) info_host[f] = inf;
+    const int inf = deferred ? 0 : pp->info[f];
+    if (info_host && !deferred) info_host[f] = inf;
     if (sign_host) sign_host[f] = 1;
     double *m = chi0 + f * n * n;
     if (inf == 0) {
@@ -877,6 +883,9 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
     cudaStreamWaitEvent(st, pp->join2, 0);
   }
   if (rc) return rc;
+  if (deferred && cudaMemcpyAsync(info_dev_out, b.info, sizeof(int) * nfreq,
+                                  cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return MBPT_ERR_CUDA;
   if (cudaGetLastError() != cudaSuccess) return MBPT_ERR_CUDA;
   return bad ? MBPT_ERR_NOT_SPD : MBPT_OK;
 }
@@ -1286,6 +1295,16 @@ int mbpt_dyson(double *chi0, int64_t naux, int nfreq, int want_w, int mode, doub
   Arena ar = arena(ws, ws_bytes);
   return dyson_run(chi0, naux, nfreq, want_w, logdet, trace, info_host, sign_host, ar,
                    S(stream), mode, err);
+}
+
+int mbpt_dyson_deferred(double *chi0, int64_t naux, int nfreq, int want_w, int mode,
+                        double *logdet, double *trace, int *info_dev, void *ws, size_t ws_bytes,
+                        int *err, void *stream) {
+  if (naux < 1 || nfreq < 1 || !info_dev) return MBPT_ERR_SHAPE;
+  if (mode != MBPT_MODE_FP64 && mode != MBPT_MODE_MIXED) return MBPT_ERR_UNSUPPORTED;
+  Arena ar = arena(ws, ws_bytes);
+  return dyson_run(chi0, naux, nfreq, want_w, logdet, trace, nullptr, nullptr, ar, S(stream),
+                   mode, err, info_dev);
 }
 
 size_t mbpt_rpa_energy_workspace_bytes(int64_t M, int64_t norb, int64_t nocc, int64_t naux,

@@ -305,7 +305,7 @@ def screened_tau_blocked(X, D, eps, nocc, axes, freq_block, precision=None, stre
 
 def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=None,
              eps_anchor=None, xc_diagonal=None, greedy=True, warm=None, keep=False,
-             stream=None, timings=None, freq_block=None):
+             stream=None, timings=None, freq_block=None, _deferred=True):
     """The whole space-time G0W0 sweep on device-resident (or host) inputs.
 
     Returns a SweepResult with 'roots', 'z', 'flags', 'evals' (device),
@@ -315,6 +315,11 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
     freq_block: hold chi0 for that many frequencies at a time
     (`screened_tau_blocked`; 't_chi0' then times the whole blocked build of
     W(tau) and 't_dyson' is zero); W - I is then not kept.
+
+    The Dyson step issues every frequency's inverse without reading its info
+    word (no host wait inside the sweep); the words are read with the sweep's
+    error word at its end, and a sweep that met a frequency where 1 - chi0 is
+    not positive definite is repeated with the Dyson step's LU fallback.
     """
     dev = require_device()
     # host inputs cross to the device once, here (both halves of the sweep read them)
@@ -327,8 +332,8 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
                                anchor=None if eps_anchor is None else _eps_host(eps_anchor))
     mu = axes.mu
     check_mixed_weights(precision, axes.grid.cosft_wt, axes.Ctw, axes.C, axes.S)
-    # one device error word for the sweep, read once at its end: no host sync
-    # between the stages (the Dyson step waits only for its info words)
+    # one device error word for the sweep, read once at its end with the
+    # Dyson step's info words: no host sync between the stages
     err = _Err(dev)
     ev = None
     if timings is not None:
@@ -357,7 +362,7 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
     if ev:
         ev[1].record()
     logdet, trace, info, _ = dyson_batch(chi0, want_w=True, stream=stream,
-                                         precision=precision, err=err)
+                                         precision=precision, err=err, deferred=_deferred)
     # E_c from the same factorisations: the frequency axis is a minimax quadrature
     e_c = torch.empty((), dtype=torch.float64, device=dev)
     ow = torch.as_tensor(np.asarray(axes.grid.omega_weights, float), device=dev)
@@ -370,8 +375,16 @@ def gw_sweep(X, D, eps, nocc, states=None, ntau='auto', axes=None, precision=Non
         out=None if keep else BUFFERS.take('sweep_wt', (len(axes.Ctw), naux, naux), dev))
     W_minus_I = chi0 if keep else None
     del chi0
-    return _sweep_tail(X, D, eps_h, nocc, states, axes, precision, eps_anchor, xc_diagonal,
-                       greedy, warm, keep, stream, timings, err, ev, Wt, W_minus_I, info, e_c)
+    res = _sweep_tail(X, D, eps_h, nocc, states, axes, precision, eps_anchor, xc_diagonal,
+                      greedy, warm, keep, stream, timings, err, ev, Wt, W_minus_I, info, e_c)
+    if _deferred and res['dyson_info'].any():
+        # a frequency whose 1 - chi0 is not positive definite: its W was not
+        # valid, so everything after the Dyson step is redone with its LU
+        return gw_sweep(X, D, eps_h, nocc, states=states, axes=axes, precision=precision,
+                        eps_anchor=eps_anchor, xc_diagonal=xc_diagonal, greedy=greedy,
+                        warm=warm, keep=keep, stream=stream, timings=timings,
+                        _deferred=False)
+    return res
 
 
 def _sweep_tail(X, D, eps_h, nocc, states, axes, precision, eps_anchor, xc_diagonal, greedy,
@@ -405,6 +418,8 @@ def _sweep_tail(X, D, eps_h, nocc, states, axes, precision, eps_anchor, xc_diago
         timings['dyson_frequencies'] = axes.grid.nfreq
         timings['ntau'] = axes.ntau
     err.check('gw_sweep')
+    if isinstance(info, torch.Tensor):
+        info = info.cpu().numpy()
     res = SweepResult(roots=roots, z=z, flags=flags, evals=evals, sigma=sigma, axes=axes,
                       states=states, branch=branch, dyson_info=info, e_c=e_c)
     if keep:
@@ -479,7 +494,7 @@ def gw_sweep_unrestricted(X_mos, D, spectra, noccs, states=None, ntau='auto', ax
         chi0.add_(beta).mul_(0.5)
     del beta
     logdet, trace, info, _ = dyson_batch(chi0, want_w=True, stream=stream,
-                                         precision=precision, err=err)
+                                         precision=precision, err=err, deferred=_deferred)
     e_c = torch.empty((), dtype=torch.float64, device=dev)
     ow = torch.as_tensor(np.asarray(axes.grid.omega_weights, float), device=dev)
     check(lib().mbpt_energy_sum(ptr(logdet), ptr(trace), ptr(ow), len(ow), ptr(e_c),

@@ -213,22 +213,34 @@ class NonPositiveDielectric(RuntimeWarning):
     """det(1 - chi0) is not positive at an imaginary frequency."""
 
 
-def dyson_batch(chi0, want_w=True, stream=None, precision='fp64', err=None):
+def dyson_batch(chi0, want_w=True, stream=None, precision='fp64', err=None, deferred=False):
     """In place over a device tensor (nfreq, naux, naux): chi0 -> W - I (or
     the Cholesky factors). Returns (logdet, trace, info, sign) with logdet and
     trace on the device and info/sign as host int arrays. The factorisation
     and log-determinant are FP64 in both precisions; 'mixed' forms the
-    inverse from the FP64 factor by TF32x3 tensor-core products."""
+    inverse from the FP64 factor by TF32x3 tensor-core products.
+    deferred: no host wait; info comes back as a device int32 tensor and sign
+    as None, and a nonzero info word means that frequency's results are not
+    valid (repeat without `deferred`)."""
     dev = chi0.device
     mode = _mode(precision)
     nfreq, naux = chi0.shape[0], chi0.shape[-1]
     logdet = torch.empty(nfreq, dtype=torch.float64, device=dev)
     trace = torch.empty(nfreq, dtype=torch.float64, device=dev)
-    info = np.zeros(nfreq, dtype=np.int32)
-    sign = np.ones(nfreq, dtype=np.int32)
     own = err is None
     err = _Err(dev) if own else err
     ws = WORKSPACE.get(lib().mbpt_dyson_workspace_bytes(naux, nfreq, mode), dev)
+    if deferred:
+        info_d = torch.zeros(nfreq, dtype=torch.int32, device=dev)
+        check(lib().mbpt_dyson_deferred(ptr(chi0), naux, nfreq, int(bool(want_w)), mode,
+                                        ptr(logdet), ptr(trace), ptr(info_d), ptr(ws),
+                                        ws.numel(), ptr(err.t), stream_ptr(stream)),
+              'mbpt_dyson_deferred')
+        if own:
+            err.check('mbpt_dyson_deferred')
+        return logdet, trace, info_d, None
+    info = np.zeros(nfreq, dtype=np.int32)
+    sign = np.ones(nfreq, dtype=np.int32)
     import ctypes
     rc = lib().mbpt_dyson(ptr(chi0), naux, nfreq, int(bool(want_w)), mode, ptr(logdet),
                           ptr(trace), info.ctypes.data_as(ctypes.c_void_p),

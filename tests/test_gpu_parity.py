@@ -238,6 +238,62 @@ def test_planted_nonpositive_dielectric_is_flagged():
     assert rel(W, np.linalg.inv(np.eye(n) - c) - np.eye(n)) < 1e-10
 
 
+
+def test_deferred_dyson_reports_on_the_device_and_the_sweep_repeats():
+    """The Dyson step without a host wait: the info words come back on the
+    device (the non-positive-definite frequency flagged, the others' log-
+    determinants and W - I equal to the synchronous step's), and a sweep that
+    meets such a frequency is repeated with the LU fallback, giving the same
+    result as the synchronous sweep."""
+    rng = np.random.default_rng(7)
+    n = 300
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    mats = []
+    for f in range(4):
+        lam = -rng.uniform(0.05, 3.0, n)
+        if f == 1:
+            lam[5] = 1.4
+        mats.append((Q * lam) @ Q.T)
+    c_sync = torch.as_tensor(np.stack(mats), device='cuda')
+    c_def = c_sync.clone()
+    ld_s, _, info_s, _ = st.dyson_batch(c_sync, want_w=True, precision='fp64')
+    ld_d, _, info_d, sign_d = st.dyson_batch(c_def, want_w=True, precision='fp64',
+                                             deferred=True)
+    assert isinstance(info_d, torch.Tensor) and sign_d is None
+    info_d = info_d.cpu().numpy()
+    assert list(info_d != 0) == [False, True, False, False]
+    ok = [0, 2, 3]
+    assert np.abs(ld_d.cpu().numpy()[ok] - ld_s.cpu().numpy()[ok]).max() < 1e-12
+    assert rel(c_def[ok].cpu().numpy(), c_sync[ok].cpu().numpy()) < 1e-13
+    # a sweep whose deferred step reports a failed frequency (on the imaginary
+    # axis 1 - chi0 >= I for any physical system, so the report is planted by
+    # a wrapper around the step) is repeated with the synchronous step
+    from mbptcode_b200.synthetic import synthetic_system
+    X, D, eps = synthetic_system(40, 5, 200, seed=1, variant='calibrated')
+    axes = grids.space_time_axes(eps, 5, ntau=12)
+    real, calls = gw.dyson_batch, []
+
+    def planted(chi0, *args, deferred=False, **kw):
+        calls.append(deferred)
+        out = real(chi0, *args, deferred=deferred, **kw)
+        if deferred:
+            out[2][0] = 3
+        return out
+    gw.dyson_batch = planted
+    try:
+        a = gw.gw_sweep(X, D, eps, 5, axes=axes, precision='fp64')
+    finally:
+        gw.dyson_batch = real
+    b = gw.gw_sweep(X, D, eps, 5, axes=axes, precision='fp64', _deferred=False)
+    assert calls == [True, False]
+    assert not a['dyson_info'].any()
+    ra, rb = a['roots'].cpu().numpy(), b['roots'].cpu().numpy()
+    assert np.array_equal(np.isnan(ra), np.isnan(rb))
+    fin = np.isfinite(ra)
+    assert np.abs(ra[fin] - rb[fin]).max() < 1e-12
+    assert abs(float(a['e_c']) - float(b['e_c'])) <= 1e-12 * abs(float(b['e_c']))
+
+
 @pytest.mark.parametrize('prec', ['fp64', 'mixed'])
 def test_dyson_batch_with_failed_frequency_inside(prec):
     """Four frequencies, the second not positive definite: the batched
