@@ -922,3 +922,30 @@ def qp_gradient_laplace(X, D, eps, nocc, tau, tau_w, cosft_wt, nu, nu_w, p, mu, 
     e2, X_bar, D_bar = polarizability_backward(proj_bar, X, D, eps, nocc, tau, mu)
     three_index_slice_backward(X, D, p, B_bar, X_bar, D_bar)
     return eps_bar + e2, X_bar, D_bar
+
+
+# ---------------------------------------------------------------------------
+# separable-RI fit from supplied inputs (src/Base/factorization/separable_ri.py)
+# ---------------------------------------------------------------------------
+
+def isdf_fit_products(ao, second, w, aux, FD, regularization=4e-7):
+    """separable_ri.py:664-900 with explicit arrays: the Gram matrix of the
+    product pairs and auxiliary functions, balanced by its diagonal,
+    regularised, solved by Cholesky against F D^T (separable_ri.py:1616-1653)."""
+    import scipy.linalg
+    B = ao[:, second] * w[None, :]
+    S = (ao @ ao.T) * (B @ B.T) + aux @ aux.T
+    scale = np.sqrt(np.diag(S))
+    scale[scale == 0] = 1.0
+    d = 1.0 / scale
+    G = S * d[:, None] * d[None, :]
+    G[np.diag_indices_from(G)] += regularization
+    cho = scipy.linalg.cho_factor(G, lower=True)
+    return scipy.linalg.cho_solve(cho, (FD * d[None, :]).T).T * d[None, :]
+
+
+def aux_metric_root(V, floor=1e-12):
+    """separable_ri.py:1802-1929: V^(1/2) on the eigenvalues above floor x max."""
+    w, v = np.linalg.eigh(V)
+    keep = w > floor * w.max()
+    return (v[:, keep] * np.sqrt(w[keep])) @ v[:, keep].T

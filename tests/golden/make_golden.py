@@ -52,6 +52,9 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      and adjoint make (every name plugin.install() rebinds,
                      recorded with its arguments and result), and the
                      drivers' outputs;
+* isdf.npz           the separable-RI fit from supplied collocations, pair
+                     coefficients and metric: the reference's fit_M_stable,
+                     aux_metric_sqrt and D = M^T V^1/2;
 * qp_kat.npz         the root finder on closed-form self-energies
                      (tests/test_qp_refine_root.py's two-pole Sigma and others);
 * c1_<variant>.npz   the synthetic FP64 configuration at full size (n_orb = 400,
@@ -61,7 +64,7 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      stored: the tests regenerate them from the seed and check
                      the regeneration against the stored eps and checksums.
 
-    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|contour_explicit|contour_unrestricted|sigma_ao|evgw|drop_in]
+    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|contour_explicit|contour_unrestricted|sigma_ao|evgw|drop_in|isdf]
 """
 import os
 import sys
@@ -587,6 +590,44 @@ def drop_in_fixture():
     print('recorded', {k: v for k, v in counts.items()})
 
 
+def isdf_fixture():
+    """The device half of the separable-RI factors against the reference's
+    own fit (Base/factorization/separable_ri.py, loaded with the stand-ins):
+    a seeded AO collocation on nk points, the second-factor columns and
+    angular weights of the product pairs, the auxiliary collocation, the
+    pairs' fitting coefficients F and a Coulomb metric V. The reference's
+    explicit estimator `fit_M_stable` on D = [pair columns | auxiliary
+    collocation], F = [F_pairs | I] (``build_D_F``'s layout), the metric root
+    `aux_metric_sqrt` (with a near-null direction it drops) and D = M^T V^1/2."""
+    _install_stand_ins()
+    from src.Base.factorization import separable_ri as sr
+    rng = np.random.default_rng(31)
+    nk, nao, naux = 96, 20, 40
+    second = np.array([0, 2, 3, 5, 7, 11, 13, 17])
+    w = rng.uniform(0.5, 1.5, len(second))
+    pts = rng.uniform(-2, 2, (nk, 3))
+    centres = rng.uniform(-2, 2, (nao, 3))
+    ao = np.exp(-0.7 * ((pts[:, None, :] - centres[None]) ** 2).sum(-1))
+    ao *= rng.uniform(0.5, 2.0, nao)[None, :]
+    aux_c = rng.uniform(-2, 2, (naux, 3))
+    aux = np.exp(-0.4 * ((pts[:, None, :] - aux_c[None]) ** 2).sum(-1))
+    pairs = (ao[:, :, None] * (ao[:, second] * w[None, :])[:, None, :]).reshape(nk, -1)
+    F_pairs = rng.standard_normal((naux, pairs.shape[1])) / np.sqrt(pairs.shape[1])
+    D = np.hstack([pairs, aux])
+    F = np.hstack([F_pairs, np.eye(naux)])
+    M = sr.fit_M_stable(D, F)
+    Q, _ = np.linalg.qr(rng.standard_normal((naux, naux)))
+    lam = np.exp(rng.uniform(np.log(1e-2), np.log(10.0), naux))
+    lam[3] = 1e-14 * lam.max()              # a direction in the numerical null space
+    V = (Q * lam) @ Q.T
+    V = 0.5 * (V + V.T)
+    root = sr.aux_metric_sqrt(V=V)
+    C = np.linalg.qr(rng.standard_normal((nao, nao)))[0]
+    np.savez_compressed(os.path.join(HERE, 'isdf.npz'), ao=ao, second=second, w=w, aux=aux,
+                        F_pairs=F_pairs, FD=F @ D.T, M=M, V=V, root=root, D_factor=M.T @ root,
+                        mo_coeff=C, X_mo=ao @ C)
+
+
 def contour_fixture():
     """The contour-deformation self-energy's pieces (GW/contour_deformation.py,
     GW/real_screening.py) on a small synthetic system: the contour grid
@@ -829,6 +870,10 @@ if __name__ == '__main__':
         sigma_ao_fixture()
         print('AO self-energy fixture written to', HERE)
         sys.exit(0)
+    if ONLY == 'isdf':
+        isdf_fixture()
+        print('ISDF fit fixture written to', HERE)
+        sys.exit(0)
     if ONLY == 'drop_in':
         drop_in_fixture()
         print('drop-in call fixture written to', HERE)
@@ -851,7 +896,7 @@ if __name__ == '__main__':
         sys.exit(0)
     if ONLY:
         sys.exit(f'--only {ONLY}: choose c1, static, unrestricted, sigma_adjoint, contour, '
-                 'contour_explicit, contour_unrestricted, sigma_ao, evgw or drop_in')
+                 'contour_explicit, contour_unrestricted, sigma_ao, evgw, drop_in or isdf')
     grids_fixture()
     shared_kernel_fixture()
     route_fixture('calibrated', 24, 4, 64, 7, 'calibrated', 12, full=True)
@@ -867,4 +912,5 @@ if __name__ == '__main__':
     sigma_ao_fixture()
     evgw_fixture()
     drop_in_fixture()
+    isdf_fixture()
     print('fixtures written to', HERE)

@@ -406,3 +406,14 @@ def test_contour_qp_gradient_oracle(golden):
         for a, k in ((eb, 'eps_bar'), (xb, 'X_bar'), (db, 'D_bar')):
             ref = g[k][i]
             assert np.abs(a - ref).max() <= 1e-9 * np.abs(ref).max(), (int(p), k)
+
+
+def test_isdf_fit_oracle(golden):
+    """The separable-RI fit restated in the oracle against the reference's
+    own estimator, metric root and D = M^T V^1/2 (tests/golden/isdf.npz)."""
+    g = golden('isdf')
+    M = orc.isdf_fit_products(g['ao'], g['second'], g['w'], g['aux'], g['FD'])
+    assert np.abs(M - g['M']).max() <= 1e-9 * np.abs(g['M']).max()
+    root = orc.aux_metric_root(g['V'])
+    assert np.abs(root - g['root']).max() <= 1e-12 * np.abs(g['root']).max()
+    assert np.abs(M.T @ root - g['D_factor']).max() <= 1e-9 * np.abs(g['D_factor']).max()
