@@ -407,6 +407,23 @@ int mbpt_gemm_split_tf32(const double *A_dev, const double *B_dev, int64_t m, in
                          int64_t k, double alpha, float *C_dev, int64_t ldc, void *workspace,
                          size_t ws_bytes, int *err_dev, void *stream);
 
+/* ---- FP64-accurate GEMM on the int8 tensor cores ---------------------------
+ * C (m x n, row-major, ldc) = alpha op(A) op(B) + beta C, op(A) = A (m x k,
+ * lda) or A^T (ta: A is k x m), op(B) = B (k x n, ldb) or B^T (tb: B is
+ * n x k), all FP64 row-major. The Ozaki scheme: each row of op(A) and each
+ * column of op(B) is scaled by a power of two above its largest magnitude
+ * and cut into `slices` (7 or 8) signed 7-bit digits; the digit products are
+ * exact int32 tcgen05 products, combined in FP64 (error about 2^-7S K
+ * max|row| max|column| per entry: FP64 level at 8 digits). The FP64
+ * products of the reverse sweeps (the NumPy matrix products of
+ * gradients/rpa/space_time_adjoint.py:167-218, 795-875) run on it.
+ * K is taken in passes of at most 32768. */
+size_t mbpt_dgemm_ozaki_workspace_bytes(int64_t m, int64_t n, int64_t k, int slices);
+int mbpt_dgemm_ozaki(int ta, int tb, int64_t m, int64_t n, int64_t k, double alpha,
+                     const double *A_dev, int64_t lda, const double *B_dev, int64_t ldb,
+                     double beta, double *C_dev, int64_t ldc, int slices, void *workspace,
+                     size_t ws_bytes, int *err_dev, void *stream);
+
 /* ---- split-precision GEMM without caller scratch -------------------------
  * No counterpart in MBPTcode: an addition of this library for callers that
  * cannot allocate device memory, typically hosts whose device memory is all

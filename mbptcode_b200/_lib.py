@@ -85,6 +85,9 @@ _SIGNATURES = {
     'mbpt_gemm_split': (_i, [_p, _p, _i64, _i64, _i64, _d, _p, _i64, _p, _sz, _p, _p]),
     'mbpt_gemm_split_tf32_workspace_bytes': (_sz, [_i64, _i64, _i64]),
     'mbpt_gemm_split_tf32': (_i, [_p, _p, _i64, _i64, _i64, _d, _p, _i64, _p, _sz, _p, _p]),
+    'mbpt_dgemm_ozaki_workspace_bytes': (_sz, [_i64, _i64, _i64, _i]),
+    'mbpt_dgemm_ozaki': (_i, [_i, _i, _i64, _i64, _i64, _d, _p, _i64, _p, _i64, _d, _p, _i64, _i,
+                              _p, _sz, _p, _p]),
     'mbpt_gemm_split_static_capacity': (_sz, []),
     'mbpt_gemm_split_static': (_i, [_p, _p, _i64, _i64, _i64, _d, _p, _i64, _p, _p]),
 }

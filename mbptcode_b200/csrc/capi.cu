@@ -11,6 +11,7 @@
 #include <cstring>
 #include <mutex>
 #include <algorithm>
+#include <tuple>
 #include <vector>
 
 #include "internal.h"
@@ -106,6 +107,60 @@ bool dgemm_rm(cublasHandle_t h, bool ta, bool tb, int64_t m, int64_t n, int64_t 
 }
 
 inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// The FP64 products of the reverse sweeps and of the rows beside the route
+// (the adjoints, the AO self-energy, the contour's FP64 pieces) run on the
+// int8 tensor cores by the Ozaki scheme (8 digits: FP64 level) when
+// MBPT_FP64_GEMM=ozaki, else as cuBLAS DGEMMs. The forward sweep's plain FP64
+// mode keeps native FP64 products either way. Read at every call.
+bool ozaki_fp64_enabled() {
+  const char *e = std::getenv("MBPT_FP64_GEMM");
+  return e && std::strcmp(e, "ozaki") == 0;
+}
+
+// Grow-only scratch of the Ozaki GEMM, one per (device, stream): concurrent
+// streams never share one. Growing waits for the stream's earlier work.
+void *ozaki_scratch(cudaStream_t st, size_t bytes) {
+  static std::mutex mu;
+  static std::vector<std::tuple<int, cudaStream_t, void *, size_t>> held;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> g(mu);
+  for (auto &t : held) {
+    if (std::get<0>(t) == dev && std::get<1>(t) == st) {
+      if (std::get<3>(t) >= bytes) return std::get<2>(t);
+      if (cudaStreamSynchronize(st) != cudaSuccess) return nullptr;
+      cudaFree(std::get<2>(t));
+      void *p = nullptr;
+      if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        std::get<2>(t) = nullptr;
+        std::get<3>(t) = 0;
+        return nullptr;
+      }
+      std::get<2>(t) = p;
+      std::get<3>(t) = bytes;
+      return p;
+    }
+  }
+  void *p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+  held.emplace_back(dev, st, p, bytes);
+  return p;
+}
+
+bool gemm_f64(cublasHandle_t h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
+              double alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
+              double beta, double *C, int64_t ldc) {
+  if (!ozaki_fp64_enabled())
+    return dgemm_rm(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  cudaStream_t st = nullptr;
+  if (cublasGetStream(h, &st) != CUBLAS_STATUS_SUCCESS) return false;
+  const size_t bytes = ozaki_gemm_scratch_bytes(m, n, k, 8);
+  void *ws = ozaki_scratch(st, bytes);
+  if (!ws) return false;
+  return ozaki_dgemm(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, 8, ws, bytes,
+                     nullptr, st) == MBPT_OK;
+}
 
 double *copy_weights(Arena &ar, const double *host, size_t count, cudaStream_t st) {
   double *d = ar.take<double>(count);
@@ -1067,27 +1122,27 @@ int back_run(const double *pbar, const double *X, const Dims &d, const double *e
   for (int k = 0; k < ntau; ++k) {
     // MBPTcode gradients/rpa/space_time_adjoint.py:196-217, one row tile
     launch_sym_half(pbar + k * a2, b.pb, d.naux, st);
-    if (!dgemm_rm(h, false, false, d.M, d.naux, d.naux, -2.0, D, d.naux, b.pb, d.naux, 0.0,
+    if (!gemm_f64(h, false, false, d.M, d.naux, d.naux, -2.0, D, d.naux, b.pb, d.naux, 0.0,
                   b.E, d.naux))
       return MBPT_ERR_CUDA;
     launch_scaled_branches(X, d.M, d.n, d.nocc, eps, mu, tau[k], 1.0, b.Xo_s, b.Xv_s, st);
-    if (!dgemm_rm(h, false, true, d.M, d.M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0, b.Go,
+    if (!gemm_f64(h, false, true, d.M, d.M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0, b.Go,
                   d.M) ||
-        !dgemm_rm(h, false, true, d.M, d.M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n, 0.0,
+        !gemm_f64(h, false, true, d.M, d.M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n, 0.0,
                   b.Gv, d.M))
       return MBPT_ERR_CUDA;
     launch_hadamard3(b.P, b.Go, b.Gv, d.M * d.M, st);  // Pi
-    if (!dgemm_rm(h, false, false, d.M, d.naux, d.M, 2.0, b.P, d.M, b.E, d.naux, 1.0, D_bar,
+    if (!gemm_f64(h, false, false, d.M, d.naux, d.M, 2.0, b.P, d.M, b.E, d.naux, 1.0, D_bar,
                   d.naux) ||
-        !dgemm_rm(h, false, true, d.M, d.M, d.naux, 1.0, b.E, d.naux, D, d.naux, 0.0, b.P,
+        !gemm_f64(h, false, true, d.M, d.M, d.naux, 1.0, b.E, d.naux, D, d.naux, 0.0, b.P,
                   d.M))  // Pi_bar
       return MBPT_ERR_CUDA;
     launch_hadamard3(b.T, b.P, b.Gv, d.M * d.M, st);  // Go_bar
-    if (!dgemm_rm(h, false, false, d.M, d.nocc, d.M, 1.0, b.T, d.M, X, d.n, 0.0, b.GoX,
+    if (!gemm_f64(h, false, false, d.M, d.nocc, d.M, 1.0, b.T, d.M, X, d.n, 0.0, b.GoX,
                   d.nocc))
       return MBPT_ERR_CUDA;
     launch_hadamard3(b.T, b.P, b.Go, d.M * d.M, st);  // Gv_bar
-    if (!dgemm_rm(h, false, false, d.M, d.nv, d.M, 1.0, b.T, d.M, X + d.nocc, d.n, 0.0, b.GvX,
+    if (!gemm_f64(h, false, false, d.M, d.nv, d.M, 1.0, b.T, d.M, X + d.nocc, d.n, 0.0, b.GvX,
                   d.nv))
       return MBPT_ERR_CUDA;
     launch_xbar_update(b.GoX, b.GvX, X, d.M, d.n, d.nocc, eps, mu, tau[k], X_bar, eps_bar, st);
@@ -1141,29 +1196,29 @@ int sigma_back_run(const double *X, const Dims &d, const double *eps, double mu,
     launch_scaled_branches(X, M, d.n, d.nocc, eps, mu, tau[k], 1.0, b.Xo_s, b.Xv_s, st);
     launch_sigma_back_gather(X, M, d.n, states, S, sl_bar + k * S, sg_bar + k * S, b.Xs, b.Xl,
                              b.Xg, st);
-    if (!dgemm_rm(h, false, true, M, M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0, b.Go, M) ||
-        !dgemm_rm(h, false, true, M, M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n, 0.0, b.Gv,
+    if (!gemm_f64(h, false, true, M, M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0, b.Go, M) ||
+        !gemm_f64(h, false, true, M, M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n, 0.0, b.Gv,
                   M) ||
-        !dgemm_rm(h, false, false, M, A, A, 1.0, D, A, Wk, A, 0.0, b.U, A) ||
-        !dgemm_rm(h, false, true, M, M, A, 1.0, b.U, A, D, A, 0.0, b.Zt, M) ||
-        !dgemm_rm(h, false, true, M, M, S, 1.0, b.Xl, S, b.Xs, S, 0.0, b.Al, M) ||
-        !dgemm_rm(h, false, true, M, M, S, 1.0, b.Xg, S, b.Xs, S, 0.0, b.Ag, M))
+        !gemm_f64(h, false, false, M, A, A, 1.0, D, A, Wk, A, 0.0, b.U, A) ||
+        !gemm_f64(h, false, true, M, M, A, 1.0, b.U, A, D, A, 0.0, b.Zt, M) ||
+        !gemm_f64(h, false, true, M, M, S, 1.0, b.Xl, S, b.Xs, S, 0.0, b.Al, M) ||
+        !gemm_f64(h, false, true, M, M, S, 1.0, b.Xg, S, b.Xs, S, 0.0, b.Ag, M))
       return MBPT_ERR_CUDA;
     // Go -> L = Go o Zt, Gv -> H = Gv o Zt, Zt -> Zt_bar, Al -> Go_bar, Ag -> Gv_bar
     launch_sigma_back_hadamard(b.Go, b.Gv, b.Zt, b.Al, b.Ag, M * M, st);
-    if (!dgemm_rm(h, false, false, M, S, M, 1.0, b.Go, M, b.Xl, S, 0.0, b.T1, S) ||
-        !dgemm_rm(h, false, false, M, S, M, -1.0, b.Gv, M, b.Xg, S, 1.0, b.T1, S))
+    if (!gemm_f64(h, false, false, M, S, M, 1.0, b.Go, M, b.Xl, S, 0.0, b.T1, S) ||
+        !gemm_f64(h, false, false, M, S, M, -1.0, b.Gv, M, b.Xg, S, 1.0, b.T1, S))
       return MBPT_ERR_CUDA;
     launch_scatter_cols(b.T1, M, S, states, 2.0, X_bar, d.n, st);
-    if (!dgemm_rm(h, false, false, M, d.nocc, M, 1.0, b.Al, M, X, d.n, 0.0, b.GoX, d.nocc) ||
-        !dgemm_rm(h, false, false, M, d.nv, M, 1.0, b.Ag, M, X + d.nocc, d.n, 0.0, b.GvX,
+    if (!gemm_f64(h, false, false, M, d.nocc, M, 1.0, b.Al, M, X, d.n, 0.0, b.GoX, d.nocc) ||
+        !gemm_f64(h, false, false, M, d.nv, M, 1.0, b.Ag, M, X + d.nocc, d.n, 0.0, b.GvX,
                   d.nv))
       return MBPT_ERR_CUDA;
     launch_xbar_update(b.GoX, b.GvX, X, M, d.n, d.nocc, eps, mu, tau[k], X_bar, eps_bar, st);
     // U <- Zt_bar D, then Wt_bar = D^T U and D_bar += 2 U Wt (Zt_bar and Wt symmetric)
-    if (!dgemm_rm(h, false, false, M, A, M, 1.0, b.Zt, M, D, A, 0.0, b.U, A) ||
-        !dgemm_rm(h, true, false, A, A, M, 1.0, D, A, b.U, A, 0.0, Wt_bar + k * a2, A) ||
-        !dgemm_rm(h, false, false, M, A, A, 2.0, b.U, A, Wk, A, 1.0, D_bar, A))
+    if (!gemm_f64(h, false, false, M, A, M, 1.0, b.Zt, M, D, A, 0.0, b.U, A) ||
+        !gemm_f64(h, true, false, A, A, M, 1.0, D, A, b.U, A, 0.0, Wt_bar + k * a2, A) ||
+        !gemm_f64(h, false, false, M, A, A, 2.0, b.U, A, Wk, A, 1.0, D_bar, A))
       return MBPT_ERR_CUDA;
   }
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
@@ -1183,9 +1238,9 @@ int dyson_back_run(const double *wmi, double *wbar, int64_t n, int nfreq, Arena 
     double *B = wbar + f * n * n;
     // T = B + Wm B; B <- T + T Wm
     if (cudaMemcpyAsync(T, B, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
-        !dgemm_rm(h, false, false, n, n, n, 1.0, Wm, n, B, n, 1.0, T, n) ||
+        !gemm_f64(h, false, false, n, n, n, 1.0, Wm, n, B, n, 1.0, T, n) ||
         cudaMemcpyAsync(B, T, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
-        !dgemm_rm(h, false, false, n, n, n, 1.0, T, n, Wm, n, 1.0, B, n))
+        !gemm_f64(h, false, false, n, n, n, 1.0, T, n, Wm, n, 1.0, B, n))
       return MBPT_ERR_CUDA;
   }
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
@@ -1478,22 +1533,22 @@ int mbpt_sigma_ao(const double *X_ao, int64_t M, int64_t nao, const double *mo_c
   const int64_t nv = norb - nocc, a2 = naux * naux, o2 = nao * nao;
   // the occupied/virtual split needs the MO collocation; the outer indices
   // stay AO (GW/imaginary_time.py:403-533)
-  if (!dgemm_rm(h, false, false, M, norb, nao, 1.0, X_ao, nao, mo_coeff, norb, 0.0, Xmo, norb))
+  if (!gemm_f64(h, false, false, M, norb, nao, 1.0, X_ao, nao, mo_coeff, norb, 0.0, Xmo, norb))
     return MBPT_ERR_CUDA;
   for (int k = 0; k < ntau; ++k) {
     launch_scaled_branches(Xmo, M, norb, nocc, eps, mu, tau_host[k], 1.0, Xo_s, Xv_s, st);
-    if (!dgemm_rm(h, false, true, M, M, nocc, 1.0, Xo_s, nocc, Xmo, norb, 0.0, Go, M) ||
-        !dgemm_rm(h, false, true, M, M, nv, 1.0, Xv_s, nv, Xmo + nocc, norb, 0.0, Gv, M) ||
-        !dgemm_rm(h, false, false, M, naux, naux, 1.0, D, naux, Wt + k * a2, naux, 0.0, U, naux) ||
-        !dgemm_rm(h, false, true, M, M, naux, 1.0, U, naux, D, naux, 0.0, Zt, M))
+    if (!gemm_f64(h, false, true, M, M, nocc, 1.0, Xo_s, nocc, Xmo, norb, 0.0, Go, M) ||
+        !gemm_f64(h, false, true, M, M, nv, 1.0, Xv_s, nv, Xmo + nocc, norb, 0.0, Gv, M) ||
+        !gemm_f64(h, false, false, M, naux, naux, 1.0, D, naux, Wt + k * a2, naux, 0.0, U, naux) ||
+        !gemm_f64(h, false, true, M, M, naux, 1.0, U, naux, D, naux, 0.0, Zt, M))
       return MBPT_ERR_CUDA;
     launch_hadamard(Go, Zt, M * M, st);
     launch_hadamard(Gv, Zt, M * M, st);
     // Sigma^<(tau) = X_ao^T (G_occ o Zt) X_ao, Sigma^>(tau) = -X_ao^T (G_virt o Zt) X_ao
-    if (!dgemm_rm(h, false, false, M, nao, M, 1.0, Go, M, X_ao, nao, 0.0, R, nao) ||
-        !dgemm_rm(h, true, false, nao, nao, M, 1.0, X_ao, nao, R, nao, 0.0, out + k * o2, nao) ||
-        !dgemm_rm(h, false, false, M, nao, M, 1.0, Gv, M, X_ao, nao, 0.0, R, nao) ||
-        !dgemm_rm(h, true, false, nao, nao, M, -1.0, X_ao, nao, R, nao, 0.0,
+    if (!gemm_f64(h, false, false, M, nao, M, 1.0, Go, M, X_ao, nao, 0.0, R, nao) ||
+        !gemm_f64(h, true, false, nao, nao, M, 1.0, X_ao, nao, R, nao, 0.0, out + k * o2, nao) ||
+        !gemm_f64(h, false, false, M, nao, M, 1.0, Gv, M, X_ao, nao, 0.0, R, nao) ||
+        !gemm_f64(h, true, false, nao, nao, M, -1.0, X_ao, nao, R, nao, 0.0,
                   out + (ntau + k) * o2, nao))
       return MBPT_ERR_CUDA;
   }
@@ -1518,7 +1573,7 @@ int mbpt_three_index_slices(const double *X, int64_t M, int64_t norb, const doub
     if (p < 0 || p >= norb) return MBPT_ERR_SHAPE;
     // B_p = D^T (x_p o X): LinearResponse/space_time.py:804-815
     launch_row_scaled_copy(X, M, norb, p, T, st);
-    if (!dgemm_rm(h, true, false, naux, norb, M, 1.0, D, naux, T, norb, 0.0,
+    if (!gemm_f64(h, true, false, naux, norb, M, 1.0, D, naux, T, norb, 0.0,
                   B + static_cast<int64_t>(s) * naux * norb, norb))
       return MBPT_ERR_CUDA;
   }
@@ -1676,7 +1731,7 @@ int mbpt_screening_contraction(const double *w_minus_i, int nfreq, int64_t naux,
   cublasHandle_t h = handles(st).blas;
   for (int k = 0; k < nfreq; ++k) {
     // wc[k, c] = B[:, c]^T (W - I)_k B[:, c]: GW/contour_deformation.py:229-237, 273-290
-    if (!dgemm_rm(h, false, false, naux, ncols, naux, 1.0, w_minus_i + k * naux * naux, naux,
+    if (!gemm_f64(h, false, false, naux, ncols, naux, 1.0, w_minus_i + k * naux * naux, naux,
                   B, ncols, 0.0, Y, ncols))
       return MBPT_ERR_CUDA;
     launch_rowdot(Y, ncols, B, ncols, naux, ncols, 1.0, wc + k * ncols, st);
@@ -1701,12 +1756,12 @@ int mbpt_cd_integral_backward(const double *w_minus_i, int nfreq, int64_t naux, 
     // wc[k, q] = b_q^T (W - I)_k b_q: B_bar += 2 ((W - I)_k B) diag(wc_bar[k]),
     // W_bar_k = B diag(wc_bar[k]) B^T (gradients/gwbse/qp_space_time.py:328-350)
     const double *v = wc_bar + k * norb;
-    if (!dgemm_rm(h, false, false, naux, norb, naux, 1.0, w_minus_i + k * naux * naux, naux, B,
+    if (!gemm_f64(h, false, false, naux, norb, naux, 1.0, w_minus_i + k * naux * naux, naux, B,
                   norb, 0.0, Y, norb))
       return MBPT_ERR_CUDA;
     launch_col_scale(Y, v, naux, norb, 2.0, B_bar, true, st);
     launch_col_scale(B, v, naux, norb, 1.0, T, false, st);
-    if (!dgemm_rm(h, false, true, naux, naux, norb, 1.0, T, norb, B, norb, 0.0,
+    if (!gemm_f64(h, false, true, naux, naux, norb, 1.0, T, norb, B, norb, 0.0,
                   W_bar + k * naux * naux, naux))
       return MBPT_ERR_CUDA;
   }
@@ -1729,11 +1784,11 @@ int mbpt_three_index_slice_backward(const double *X, int64_t M, int64_t norb, co
   // B_p = D^T diag(x_p) X (LinearResponse/space_time.py:804-815), its reverse
   // gradients/rpa/space_time_adjoint.py:593-624: G = D B_bar,
   // X_bar += diag(x_p) G, X_bar[:, p] += rowsum(G o X), D_bar += diag(x_p) X B_bar^T
-  if (!dgemm_rm(h, false, false, M, norb, naux, 1.0, D, naux, B_bar, norb, 0.0, G, norb))
+  if (!gemm_f64(h, false, false, M, norb, naux, 1.0, D, naux, B_bar, norb, 0.0, G, norb))
     return MBPT_ERR_CUDA;
   launch_row_dot_into_col(G, X, M, norb, X_bar, norb, p, st);
   launch_row_scale_acc(X, norb, p, G, M, norb, X_bar, st);
-  if (!dgemm_rm(h, false, true, M, naux, norb, 1.0, X, norb, B_bar, norb, 0.0, G, naux))
+  if (!gemm_f64(h, false, true, M, naux, norb, 1.0, X, norb, B_bar, norb, 0.0, G, naux))
     return MBPT_ERR_CUDA;
   launch_row_scale_acc(X, norb, p, G, M, naux, D_bar, st);
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
@@ -1778,6 +1833,21 @@ int mbpt_energy_adjoint_seed(double *wmi, int64_t naux, int nfreq, const double 
   if (naux < 1 || nfreq < 1) return MBPT_ERR_SHAPE;
   launch_chi0_bar_seed(wmi, naux, nfreq, ow_dev, S(stream));
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+size_t mbpt_dgemm_ozaki_workspace_bytes(int64_t m, int64_t n, int64_t k, int slices) {
+  if (!gemm_extents_ok(m, n, k) || (slices != 7 && slices != 8)) return SIZE_MAX;
+  return ozaki_gemm_scratch_bytes(m, n, k, slices);
+}
+
+int mbpt_dgemm_ozaki(int ta, int tb, int64_t m, int64_t n, int64_t k, double alpha,
+                     const double *A, int64_t lda, const double *B, int64_t ldb, double beta,
+                     double *C, int64_t ldc, int slices, void *ws, size_t ws_bytes, int *err,
+                     void *stream) {
+  if (!gemm_extents_ok(m, n, k) || ldc < n || lda < (ta ? m : k) || ldb < (tb ? k : n))
+    return MBPT_ERR_SHAPE;
+  return ozaki_dgemm(ta != 0, tb != 0, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, slices,
+                     ws, ws_bytes, err, S(stream));
 }
 
 size_t mbpt_gemm_split_tf32_workspace_bytes(int64_t m, int64_t n, int64_t k) {

@@ -71,6 +71,15 @@ int ozaki_chol_slice(const double *A, int64_t n, int nmat, int64_t j0, int nb,
 int ozaki_chol_update(double *A, int64_t n, int nmat, int64_t j0, int nb, double *P,
                       const double *scale, const int8_t *planes, int slices, double *rowsq,
                       int *err, cudaStream_t st);
+// C (m x n, row-major, ldc) = alpha op(A) op(B) + beta C in FP64 accuracy on
+// the int8 tensor cores (Ozaki scheme, `slices` digits per operand, 7 or 8):
+// op(A) = A (m x k, lda) or, with ta, A^T of a k x m A; op(B) = B (k x n,
+// ldb) or, with tb, B^T of an n x k B. scratch: ozaki_gemm_scratch_bytes.
+size_t ozaki_gemm_scratch_bytes(int64_t m, int64_t n, int64_t k, int slices);
+int ozaki_dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
+                const double *A, int64_t lda, const double *B, int64_t ldb, double beta,
+                double *C, int64_t ldc, int slices, void *scratch, size_t scratch_bytes,
+                int *err, cudaStream_t st);
 
 // Bump allocator over a caller's workspace (1024-byte aligned slices).
 struct Arena {

@@ -20,6 +20,8 @@
 // the TMEM owner and MMA issuer (S(S+1)/2 products per 32-wide K step), warps
 // 2-5 the epilogue; two pipeline stages of S A-planes and S B-planes; every
 // mbarrier wait bounded, as in the split engine.
+#include <algorithm>
+
 #include "internal.h"
 
 namespace mbpt {
@@ -100,22 +102,34 @@ __device__ __forceinline__ void tmem_ld32_s32(uint32_t addr, int (&v)[32]) {
       : "memory");
 }
 
+enum Epi : int {
+  EPI_CHOL = 0,  // the Cholesky panel: P -= product, column-major, exact diagonal
+  EPI_GEMM = 1,  // C = alpha product + beta C, row-major
+};
+
 struct UpdateArgs {
-  CUtensorMap tm_a;    // digit planes, dims (npad K, npad rows, S * nmat planes), box 64 x 128
-  CUtensorMap tm_b;    // the same planes, box 64 x 64
-  int64_t n;           // matrix size
-  int j0, nb;          // the step's first column and width (<= 128)
-  int k_tiles;         // j0 / 64
-  int nmat;
+  CUtensorMap tm_a;    // A digit planes (K, rows, planes), box 64 x 128
+  CUtensorMap tm_b;    // B digit planes, box 64 x 64 (the Cholesky: the same array)
+  int64_t n;           // matrix size (Cholesky)
+  int j0, nb;          // the step's first column and width (<= 128) (Cholesky)
+  int k_tiles;         // K / 64
+  int nmat;            // planes per digit level (matrices of a batch)
+  int a_row0, b_row0;  // first plane rows of the A and B operands
+  int tiles_n;         // 64-column tiles per row of tiles
   double *P;           // nmat panels, column-major m x nb (ld m), m = n - j0
   int64_t p_stride;    // elements between panels
-  const double *scale; // nmat x n: 2^e_r
+  const double *scale; // Cholesky: nmat x n, 2^e_r; GEMM: the rows of A
+  const double *scale_b;  // GEMM: the rows of B
   const double *rowsq; // nmat x nb: sum_(k < j0) L_(j0+i, k)^2, exact
+  double *C;           // GEMM output, row-major m_rows x n_cols, ld ldc
+  int64_t ldc;
+  double alpha, beta;
+  int m_rows, n_cols;
   int tiles_m;
   int *err;
 };
 
-template <int S>
+template <int S, int EPI>
 __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_constant__ UpdateArgs p) {
   using L = Layout<S>;
   extern __shared__ uint8_t smem_raw[];
@@ -129,10 +143,11 @@ __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_consta
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int f = blockIdx.y;
-  const int tm = blockIdx.x >> 1, tn = blockIdx.x & 1;
-  const int r0 = tm * BM;       // panel row (matrix row j0 + r0)
-  const int c0 = tn * BN;       // panel column
-  if (c0 >= p.nb) return;       // uniform: the second half of a narrow last panel
+  const int tm = blockIdx.x / p.tiles_n, tn = blockIdx.x % p.tiles_n;
+  const int r0 = tm * BM;       // tile row (Cholesky: matrix row j0 + r0)
+  const int c0 = tn * BN;       // tile column
+  // uniform: the second half of a narrow last panel
+  if (EPI == EPI_CHOL && c0 >= p.nb) return;
   const int m = static_cast<int>(p.n - p.j0);
 
   if (threadIdx.x == 0) {
@@ -171,8 +186,8 @@ __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_consta
 #pragma unroll
         for (int q = 0; q < S; ++q) {
           const int plane = q * p.nmat + f;
-          tma_load_3d(st + q * L::kAPlane, &p.tm_a, kx, p.j0 + r0, plane, &full[s]);
-          tma_load_3d(st + S * L::kAPlane + q * L::kBPlane, &p.tm_b, kx, p.j0 + c0, plane,
+          tma_load_3d(st + q * L::kAPlane, &p.tm_a, kx, p.a_row0 + r0, plane, &full[s]);
+          tma_load_3d(st + S * L::kAPlane + q * L::kBPlane, &p.tm_b, kx, p.b_row0 + c0, plane,
                       &full[s]);
         }
       }
@@ -234,11 +249,12 @@ __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_consta
       if (lane == 0) DevErr{p.err}.set(MBPT_ERR_TIMEOUT);
     } else {
       tc_fence_after();
-      const int pr = r0 + sp * 32 + lane;             // panel row of this thread
-      const int64_t row = p.j0 + pr;                  // matrix row
-      const double *sc = p.scale + static_cast<int64_t>(f) * p.n;
-      const double srow = pr < m ? sc[row] : 0.0;
-      double *P = p.P + static_cast<int64_t>(f) * p.p_stride;
+      const int pr = r0 + sp * 32 + lane;             // tile row of this thread
+      const bool live = EPI == EPI_CHOL ? pr < m : pr < p.m_rows;
+      const int64_t row = EPI == EPI_CHOL ? p.j0 + pr : pr;
+      const double *sc = p.scale + (EPI == EPI_CHOL ? static_cast<int64_t>(f) * p.n : 0);
+      const double srow = live ? sc[row] : 0.0;
+      double *P = EPI == EPI_CHOL ? p.P + static_cast<int64_t>(f) * p.p_stride : nullptr;
 #pragma unroll 1
       for (int ch = 0; ch < BN / 32; ++ch) {
         double acc[32];
@@ -253,7 +269,7 @@ __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_consta
 #pragma unroll
           for (int i = 0; i < 32; ++i) acc[i] += static_cast<double>(v[i]) * w;
         }
-        if (pr < m) {
+        if (EPI == EPI_CHOL && live) {
 #pragma unroll
           for (int i = 0; i < 32; ++i) {
             const int pc = c0 + ch * 32 + i;        // panel column
@@ -263,6 +279,17 @@ __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_consta
                 *dst -= p.rowsq[static_cast<int64_t>(f) * p.nb + pc];
               else
                 *dst -= acc[i] * srow * sc[p.j0 + pc];
+            }
+          }
+        } else if (EPI == EPI_GEMM && live) {
+          double *dst = p.C + static_cast<int64_t>(pr) * p.ldc;
+          const double a = p.alpha * srow;
+#pragma unroll
+          for (int i = 0; i < 32; ++i) {
+            const int col = c0 + ch * 32 + i;
+            if (col < p.n_cols) {
+              const double v = a * acc[i] * p.scale_b[col];
+              dst[col] = p.beta == 0.0 ? v : v + p.beta * dst[col];
             }
           }
         }
@@ -362,6 +389,103 @@ __global__ void chol_rowsq_kernel(const double *A, int64_t n, int64_t mat_stride
   rowsq[static_cast<int64_t>(f) * nb + i] = s;
 }
 
+// scale[i] = 2^e >= max_k |x(i, k)| of each row of an operand (1 for a row
+// of zeros or with a non-finite entry); x(i, k) = src[i ld + k], or
+// src[k ld + i] with trans.
+__global__ void row_scale_kernel(const double *src, int64_t rows, int64_t kdim, int64_t ld,
+                                 int trans, double *scale) {
+  const int lane = threadIdx.x & 31;
+  if (trans) {
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < rows;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+      double mx = 0.0;
+      for (int64_t k = 0; k < kdim; ++k) mx = fmax(mx, fabs(src[k * ld + i]));
+      int e = 0;
+      frexp(mx, &e);
+      scale[i] = (mx > 0.0 && mx < 1e300) ? ldexp(1.0, e) : 1.0;
+    }
+    return;
+  }
+  const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x >> 5) + (threadIdx.x >> 5);
+       i < rows; i += warps) {
+    double mx = 0.0;
+    for (int64_t k = lane; k < kdim; k += 32) mx = fmax(mx, fabs(src[i * ld + k]));
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) {
+      int e = 0;
+      frexp(mx, &e);
+      scale[i] = (mx > 0.0 && mx < 1e300) ? ldexp(1.0, e) : 1.0;
+    }
+  }
+}
+
+// Digit planes of an operand (rows x kdim, row scales `scale`): plane q, row
+// i, column k at planes[(q rows_pad + i) k_pad + k], zeros beyond rows and
+// kdim up to rows_pad and k_pad. One block per 32 rows x 128 columns,
+// through shared memory so that both layouts of the source are read along
+// their contiguous index.
+template <int S>
+__global__ void operand_slice_kernel(const double *src, int64_t rows, int64_t kdim, int64_t ld,
+                                     int trans, const double *scale, int8_t *planes,
+                                     int64_t rows_pad, int64_t k_pad) {
+  __shared__ double tile[32][129];
+  const int64_t i0 = static_cast<int64_t>(blockIdx.y) * 32;
+  const int64_t k0 = static_cast<int64_t>(blockIdx.x) * 128;
+  for (int t = threadIdx.x; t < 32 * 128; t += blockDim.x) {
+    int rr, kk;
+    if (trans) {
+      rr = t & 31;
+      kk = t >> 5;
+    } else {
+      rr = t >> 7;
+      kk = t & 127;
+    }
+    const int64_t i = i0 + rr, k = k0 + kk;
+    double v = 0.0;
+    if (i < rows && k < kdim) v = trans ? src[k * ld + i] : src[i * ld + k];
+    tile[rr][kk] = v;
+  }
+  __syncthreads();
+  const int rr = threadIdx.x >> 3, cg = (threadIdx.x & 7) * 16;
+  const int64_t i = i0 + rr;
+  if (i >= rows_pad) return;
+  const double inv = i < rows ? 64.0 / scale[i] : 0.0;
+  __align__(16) int8_t out[S][16];
+#pragma unroll
+  for (int c = 0; c < 16; ++c) {
+    double t = tile[rr][cg + c] * inv;     // |t| <= 64
+#pragma unroll
+    for (int q = 0; q < S; ++q) {
+      double d = rint(t);
+      d = fmin(fmax(d, -127.0), 127.0);
+      out[q][c] = static_cast<int8_t>(static_cast<int>(d));
+      t = (t - d) * 128.0;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < S; ++q) {
+    int8_t *dst = planes + (static_cast<int64_t>(q) * rows_pad + i) * k_pad + k0 + cg;
+    *reinterpret_cast<uint4 *>(dst) = *reinterpret_cast<const uint4 *>(out[q]);
+  }
+}
+
+bool make_operand_map(CUtensorMap *m, const int8_t *planes, int64_t k_pad, int64_t rows_pad,
+                      int64_t nplanes, int box_rows) {
+  auto fn = encode_fn();
+  if (!fn || (reinterpret_cast<uintptr_t>(planes) & 15) || k_pad % 128) return false;
+  cuuint64_t dims[3] = {static_cast<cuuint64_t>(k_pad), static_cast<cuuint64_t>(rows_pad),
+                        static_cast<cuuint64_t>(nplanes)};
+  cuuint64_t strides[2] = {static_cast<cuuint64_t>(k_pad),
+                           static_cast<cuuint64_t>(k_pad * rows_pad)};
+  cuuint32_t box[3] = {static_cast<cuuint32_t>(BKB), static_cast<cuuint32_t>(box_rows), 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<int8_t *>(planes), dims, strides,
+            box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 bool make_plane_map(CUtensorMap *m, const int8_t *D, int64_t npad, int64_t planes,
                     int box_rows) {
   auto fn = encode_fn();
@@ -436,6 +560,13 @@ int ozaki_chol_update(double *A, int64_t n, int nmat, int64_t j0, int nb, double
   p.scale = scale;
   p.rowsq = rowsq;
   p.tiles_m = static_cast<int>((m + ozaki::BM - 1) / ozaki::BM);
+  p.a_row0 = p.b_row0 = static_cast<int>(j0);
+  p.tiles_n = 2;
+  p.scale_b = nullptr;
+  p.C = nullptr;
+  p.ldc = 0;
+  p.alpha = p.beta = 0.0;
+  p.m_rows = p.n_cols = 0;
   p.err = err;
   count_launch();
   ozaki::chol_rowsq_kernel<<<dim3(1, nmat), 128, 0, st>>>(A, n, n * n, static_cast<int>(j0),
@@ -443,13 +574,13 @@ int ozaki_chol_update(double *A, int64_t n, int nmat, int64_t j0, int nb, double
   const dim3 grid(static_cast<unsigned>(p.tiles_m * 2), nmat);
   static std::atomic<uint64_t> attr8{0}, attr7{0};
   if (slices == 8) {
-    auto kern = ozaki::chol_update_kernel<8>;
+    auto kern = ozaki::chol_update_kernel<8, ozaki::EPI_CHOL>;
     const int smem = ozaki::Layout<8>::kSmemBytes;
     if (!allow_smem(reinterpret_cast<const void *>(kern), smem, attr8)) return MBPT_ERR_CUDA;
     count_launch();
     kern<<<grid, 192, smem, st>>>(p);
   } else if (slices == 7) {
-    auto kern = ozaki::chol_update_kernel<7>;
+    auto kern = ozaki::chol_update_kernel<7, ozaki::EPI_CHOL>;
     const int smem = ozaki::Layout<7>::kSmemBytes;
     if (!allow_smem(reinterpret_cast<const void *>(kern), smem, attr7)) return MBPT_ERR_CUDA;
     count_launch();
@@ -458,6 +589,94 @@ int ozaki_chol_update(double *A, int64_t n, int nmat, int64_t j0, int nb, double
     return MBPT_ERR_SHAPE;
   }
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+}
+
+// ---- the general FP64-accurate GEMM ------------------------------------------
+// Largest K of one product pass: S 64^2 K must stay below 2^31 (S <= 8).
+constexpr int64_t kOzakiKChunk = 32768;
+
+size_t ozaki_gemm_scratch_bytes(int64_t m, int64_t n, int64_t k, int slices) {
+  const int64_t kc = std::min<int64_t>(round_up(k, 128), kOzakiKChunk);
+  const int64_t mp = round_up(m, 128), np = round_up(n, 128);
+  return static_cast<size_t>(slices) * (mp + np) * kc + 8 * (mp + np) + 4096;
+}
+
+int ozaki_dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
+                const double *A, int64_t lda, const double *B, int64_t ldb, double beta,
+                double *C, int64_t ldc, int slices, void *scratch, size_t scratch_bytes,
+                int *err, cudaStream_t st) {
+  if (m < 1 || n < 1 || k < 1) return MBPT_ERR_SHAPE;
+  if (slices != 7 && slices != 8) return MBPT_ERR_SHAPE;
+  if (scratch_bytes < ozaki_gemm_scratch_bytes(m, n, k, slices)) return MBPT_ERR_WORKSPACE;
+  const int64_t mp = round_up(m, 128), np = round_up(n, 128);
+  static std::atomic<uint64_t> attr8{0}, attr7{0};
+  for (int64_t kb = 0; kb < k; kb += kOzakiKChunk) {
+    const int64_t kc = std::min<int64_t>(kOzakiKChunk, k - kb);
+    const int64_t kp = round_up(kc, 128);
+    uint8_t *base = static_cast<uint8_t *>(scratch);
+    int8_t *pa = reinterpret_cast<int8_t *>(base);
+    int8_t *pb = pa + static_cast<int64_t>(slices) * mp * kp;
+    double *sa = reinterpret_cast<double *>(
+        (reinterpret_cast<uintptr_t>(pb + static_cast<int64_t>(slices) * np * kp) + 255) &
+        ~static_cast<uintptr_t>(255));
+    double *sb = sa + mp;
+    // op(A) rows are K-contiguous unless ta; op(B) = B^T rows unless tb
+    const double *a0 = ta ? A + kb * lda : A + kb;
+    const double *b0 = tb ? B + kb : B + kb * ldb;
+    const int at = ta ? 1 : 0, bt = tb ? 0 : 1;
+    count_launch(2);
+    ozaki::row_scale_kernel<<<ozaki::grid_blocks(m * 32), 256, 0, st>>>(a0, m, kc, lda, at, sa);
+    ozaki::row_scale_kernel<<<ozaki::grid_blocks(n * 32), 256, 0, st>>>(b0, n, kc, ldb, bt, sb);
+    const dim3 ga(static_cast<unsigned>(kp / 128), static_cast<unsigned>(mp / 32));
+    const dim3 gb(static_cast<unsigned>(kp / 128), static_cast<unsigned>(np / 32));
+    count_launch(2);
+    if (slices == 8) {
+      ozaki::operand_slice_kernel<8><<<ga, 256, 0, st>>>(a0, m, kc, lda, at, sa, pa, mp, kp);
+      ozaki::operand_slice_kernel<8><<<gb, 256, 0, st>>>(b0, n, kc, ldb, bt, sb, pb, np, kp);
+    } else {
+      ozaki::operand_slice_kernel<7><<<ga, 256, 0, st>>>(a0, m, kc, lda, at, sa, pa, mp, kp);
+      ozaki::operand_slice_kernel<7><<<gb, 256, 0, st>>>(b0, n, kc, ldb, bt, sb, pb, np, kp);
+    }
+    ozaki::UpdateArgs p;
+    if (!ozaki::make_operand_map(&p.tm_a, pa, kp, mp, slices, ozaki::BM) ||
+        !ozaki::make_operand_map(&p.tm_b, pb, kp, np, slices, ozaki::BN))
+      return MBPT_ERR_SHAPE;
+    p.n = 0;
+    p.j0 = 0;
+    p.nb = 0;
+    p.k_tiles = static_cast<int>(kp / ozaki::BKB);
+    p.nmat = 1;
+    p.a_row0 = p.b_row0 = 0;
+    p.tiles_m = static_cast<int>(mp / ozaki::BM);
+    p.tiles_n = static_cast<int>((n + ozaki::BN - 1) / ozaki::BN);
+    p.P = nullptr;
+    p.p_stride = 0;
+    p.scale = sa;
+    p.scale_b = sb;
+    p.rowsq = nullptr;
+    p.C = C;
+    p.ldc = ldc;
+    p.alpha = alpha;
+    p.beta = kb == 0 ? beta : 1.0;
+    p.m_rows = static_cast<int>(m);
+    p.n_cols = static_cast<int>(n);
+    p.err = err;
+    const dim3 grid(static_cast<unsigned>(p.tiles_m * p.tiles_n), 1);
+    count_launch();
+    if (slices == 8) {
+      auto kern = ozaki::chol_update_kernel<8, ozaki::EPI_GEMM>;
+      const int smem = ozaki::Layout<8>::kSmemBytes;
+      if (!allow_smem(reinterpret_cast<const void *>(kern), smem, attr8)) return MBPT_ERR_CUDA;
+      kern<<<grid, 192, smem, st>>>(p);
+    } else {
+      auto kern = ozaki::chol_update_kernel<7, ozaki::EPI_GEMM>;
+      const int smem = ozaki::Layout<7>::kSmemBytes;
+      if (!allow_smem(reinterpret_cast<const void *>(kern), smem, attr7)) return MBPT_ERR_CUDA;
+      kern<<<grid, 192, smem, st>>>(p);
+    }
+    if (cudaGetLastError() != cudaSuccess) return MBPT_ERR_CUDA;
+  }
+  return MBPT_OK;
 }
 
 }  // namespace mbpt
