@@ -13,6 +13,7 @@ the learned warm start). Nothing here is imported by the package.
     python bench_cases.py chi0-aux NAUX NOV [--mixed]
     python bench_cases.py fp64-peak N
     python bench_cases.py adjoint-fd [--n 1200] [--nocc 120] [--M 7200] [--directions 32]
+    python bench_cases.py adjoint-time [--n 1200] [--nocc 120] [--M 7200]
     python bench_cases.py warm-start [--train 512] [--eval 64] [--save model.npz]
 
 tau: one tau point of the chi0 sweep and one of the self-energy sweep, mixed
@@ -391,6 +392,51 @@ def adjoint_fd(a):
         flush=True)
 
 
+
+def adjoint_time(a):
+    """E_c and dE_c/d(eps, X, D) at n_orb = 1200, N_mu = 7200, 24 points
+    (calibrated), timed with CUDA events after a warm-up call; one JSON line
+    with the FP64 products' route (MBPT_FP64_GEMM) and the self-energy
+    adjoint of 20 states beside it."""
+    import json
+    import os
+    from mbptcode_b200 import adjoint
+    n, nocc, M = a.n or 1200, a.nocc or 120, a.M or 7200
+    X, D, eps_t = synthetic_system_torch(n, nocc, M, seed=2024, variant='calibrated')
+    eps = eps_t.cpu().numpy()
+    axes = grids.space_time_axes(eps, nocc, ntau=a.ntau)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3, out
+    t_adj, out = timed(lambda: adjoint.rpa_energy_and_adjoint(X, D, eps, nocc, axes.grid,
+                                                              mu=axes.mu))
+    states20 = np.arange(nocc - 10, nocc + 10)
+    tr = grids.sigma_transforms(eps, nocc, axes.grid.tau_points, axes.grid.omega_points,
+                                axes.pade_freq, mu=axes.mu)
+
+    def sigma_adjoint():
+        sig, cache = adjoint.selfenergy_diag(X, D, eps_t, nocc, axes.grid, states20, tr,
+                                             axes.mu)
+        ones = torch.ones(sig.shape, dtype=torch.float64, device=sig.device)
+        return adjoint.selfenergy_diag_backward(ones, ones, X, D, eps_t, nocc, axes.grid,
+                                                states20, tr, axes.mu, cache)
+    t_sig, _ = timed(sigma_adjoint)
+    print(json.dumps({'case': 'adjoint-time', 'fp64_gemm': os.environ.get('MBPT_FP64_GEMM',
+                                                                          'cublas'),
+                      'n_orb': n, 'N_mu': M, 'ntau': a.ntau, 'e_c_Ha': float(out[0]),
+                      'rpa_energy_and_adjoint_s': round(t_adj, 4),
+                      'selfenergy_diag_and_adjoint_20_states_s': round(t_sig, 4),
+                      'eps_bar_norm': float(np.linalg.norm(np.asarray(
+                          out[1].cpu().numpy() if torch.is_tensor(out[1]) else out[1])))}),
+          flush=True)
+
 HARTREE_MEV = 27211.386245988
 
 
@@ -523,7 +569,7 @@ def main(argv=None):
     p = argparse.ArgumentParser(description='measurement cases beside bench.py')
     p.add_argument('case', choices=['tau', 'dyson', 'sweep', 'transform', 'qp-mlp', 'rows',
                                     'rows-cd', 'chi0-aux', 'fp64-peak', 'adjoint-fd',
-                                    'warm-start'])
+                                    'adjoint-time', 'warm-start'])
     p.add_argument('size', type=int, nargs='*', default=[])
     p.add_argument('--M', type=int, default=None)
     p.add_argument('--n', type=int, default=None)
@@ -561,6 +607,7 @@ def main(argv=None):
     run = {'tau': tau_point, 'dyson': dyson, 'sweep': sweep, 'transform': transform_case,
            'qp-mlp': qp_mlp_case, 'rows': rows, 'rows-cd': explicit_rows,
            'chi0-aux': chi0_aux_case, 'fp64-peak': fp64_peak, 'adjoint-fd': adjoint_fd,
+           'adjoint-time': adjoint_time,
            'warm-start': warm_start}[a.case]
     if a.case in ('tau', 'sweep'):
         big = a.case == 'sweep'

@@ -517,7 +517,7 @@ constexpr int kBatchedCholMin = 4;  // frequencies from which the batch beats on
 struct OzakiChol {
   int8_t *planes = nullptr;
   double *scale = nullptr;
-  double *rowsq = nullptr;
+  double *rowsq = nullptr;   // running FP64 row norms, nmat x n
   int slices = 8;
   int *err = nullptr;
 };
@@ -529,7 +529,7 @@ int chol_batched(double *A, int64_t n, int nmat, int *info, double *P, double *L
   const double one = 1.0, minus = -1.0, zero = 0.0;
   const bool ozaki = oz && oz->planes;
   if (ozaki) {
-    int rc = ozaki_chol_scales(A, n, nmat, oz->scale, st);
+    int rc = ozaki_chol_scales(A, n, nmat, oz->scale, oz->rowsq, st);
     if (rc) return rc;
   }
   for (int64_t j0 = 0; j0 < n; j0 += kCholNb) {
@@ -563,7 +563,8 @@ int chol_batched(double *A, int64_t n, int nmat, int *info, double *P, double *L
       return MBPT_ERR_CUDA;
     // the block column is final: cut it into digit planes for the later steps
     if (ozaki && j0 + nbj < n) {
-      int rc2 = ozaki_chol_slice(A, n, nmat, j0, nbj, oz->scale, oz->planes, oz->slices, st);
+      int rc2 = ozaki_chol_slice(A, n, nmat, j0, nbj, oz->scale, oz->planes, oz->slices,
+                                 oz->rowsq, st);
       if (rc2) return rc2;
     }
   }
@@ -638,7 +639,7 @@ DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq, int mode = MBPT_MODE_FP64
     if (b.oz_slices) {
       b.oz_planes = ar.take<int8_t>(ozaki_planes_bytes(n, nfreq, b.oz_slices));
       b.oz_scale = ar.take<double>(static_cast<int64_t>(nfreq) * n);
-      b.oz_rowsq = ar.take<double>(static_cast<int64_t>(nfreq) * kCholNb);
+      b.oz_rowsq = ar.take<double>(static_cast<int64_t>(nfreq) * n);
     }
   }
   if (mode == MBPT_MODE_MIXED) {
@@ -812,7 +813,7 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
           // this group's frequencies own a contiguous share of each buffer
           oz.planes = b.oz_planes + ozaki_planes_bytes(n, f0, b.oz_slices);
           oz.scale = b.oz_scale + static_cast<int64_t>(f0) * n;
-          oz.rowsq = b.oz_rowsq + static_cast<int64_t>(f0) * kCholNb;
+          oz.rowsq = b.oz_rowsq + static_cast<int64_t>(f0) * n;
           oz.slices = b.oz_slices;
           oz.err = err;
         }

@@ -61,13 +61,17 @@ bool allow_smem(const void *kern, int bytes, std::atomic<uint64_t> &done);
 // ---- Ozaki-scheme FP64 updates of the batched Cholesky (ozaki.cu) ----
 // Bytes of the int8 digit planes of nmat n x n factors cut into `slices`.
 size_t ozaki_planes_bytes(int64_t n, int nmat, int slices);
-// scale[f][r] = 2^e_r >= sqrt(A_rr) of each matrix (column-major, ld n).
-int ozaki_chol_scales(const double *A, int64_t n, int nmat, double *scale, cudaStream_t st);
-// Cut block column [j0, j0 + nb) of every factor (rows j0..n-1) into digit planes.
+// scale[f][r] = 2^e_r >= sqrt(A_rr) of each matrix (column-major, ld n);
+// the running row norms rownorm (nmat x n) start at zero.
+int ozaki_chol_scales(const double *A, int64_t n, int nmat, double *scale, double *rownorm,
+                      cudaStream_t st);
+// Cut block column [j0, j0 + nb) of every factor (rows j0..n-1) into digit
+// planes, adding its squares to the rows' running norms.
 int ozaki_chol_slice(const double *A, int64_t n, int nmat, int64_t j0, int nb,
-                     const double *scale, int8_t *planes, int slices, cudaStream_t st);
+                     const double *scale, int8_t *planes, int slices, double *rownorm,
+                     cudaStream_t st);
 // P -= L[j0:, :j0] L[j0:j0+nb, :j0]^T for every matrix from the digit planes
-// (the diagonal entries from exact FP64 row norms kept in rowsq, nmat x nb).
+// (the diagonal entries from the exact FP64 running row norms, nmat x n).
 int ozaki_chol_update(double *A, int64_t n, int nmat, int64_t j0, int nb, double *P,
                       const double *scale, const int8_t *planes, int slices, double *rowsq,
                       int *err, cudaStream_t st);

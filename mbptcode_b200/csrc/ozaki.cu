@@ -13,7 +13,7 @@
 // scaled by 2^(e_r + e_c). The terms dropped (s + t > S + 1) have no sign
 // preference off the diagonal; on it (a row against itself) their squares
 // are all positive, so each step's diagonal entries are taken from an exact
-// FP64 row norm instead (chol_rowsq_kernel).
+// FP64 row norm instead, which the slicing of each block column accumulates.
 //
 // Kernel layout: 128 x 64 output tiles (rows r of the panel, 64 of its
 // columns), warp 0 the TMA producer (64-byte swizzled boxes of 64 K), warp 1
@@ -120,7 +120,7 @@ struct UpdateArgs {
   int64_t p_stride;    // elements between panels
   const double *scale; // Cholesky: nmat x n, 2^e_r; GEMM: the rows of A
   const double *scale_b;  // GEMM: the rows of B
-  const double *rowsq; // nmat x nb: sum_(k < j0) L_(j0+i, k)^2, exact
+  const double *rowsq; // nmat x n: sum_(k < j0) L_(r, k)^2 of each row, exact
   double *C;           // GEMM output, row-major m_rows x n_cols, ld ldc
   int64_t ldc;
   double alpha, beta;
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_consta
             if (pc < p.nb) {
               double *dst = P + static_cast<int64_t>(pc) * m + pr;
               if (pr == pc)
-                *dst -= p.rowsq[static_cast<int64_t>(f) * p.nb + pc];
+                *dst -= p.rowsq[static_cast<int64_t>(f) * p.n + p.j0 + pc];
               else
                 *dst -= acc[i] * srow * sc[p.j0 + pc];
             }
@@ -334,7 +334,7 @@ __global__ void chol_scale_kernel(const double *A, int64_t n, int64_t mat_stride
 template <int S>
 __global__ void chol_slice_kernel(const double *A, int64_t n, int64_t mat_stride, int nmat,
                                   int j0, int nb, const double *scale, int8_t *D,
-                                  int64_t npad) {
+                                  int64_t npad, double *rownorm) {
   __shared__ double tile[32][129];
   const int f = blockIdx.y;
   const int64_t rbase = j0 + static_cast<int64_t>(blockIdx.x) * 32;
@@ -352,7 +352,17 @@ __global__ void chol_slice_kernel(const double *A, int64_t n, int64_t mat_stride
   // each thread: one row, 16 consecutive columns, all S planes
   const int rr = threadIdx.x >> 3, cg = (threadIdx.x & 7) * 16;
   const int64_t r = rbase + rr;
+  // the rows' running FP64 norms over the columns cut so far (the exact
+  // diagonal of the later updates), summed over the 8 threads of a row in a
+  // fixed order
+  double sq = 0.0;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) sq = fma(tile[rr][cg + i], tile[rr][cg + i], sq);
+  sq += __shfl_xor_sync(0xffffffffu, sq, 1);
+  sq += __shfl_xor_sync(0xffffffffu, sq, 2);
+  sq += __shfl_xor_sync(0xffffffffu, sq, 4);
   if (r >= n) return;
+  if (cg == 0) rownorm[static_cast<int64_t>(f) * n + r] += sq;
   const double inv = 64.0 / scale[static_cast<int64_t>(f) * n + r];
   __align__(16) int8_t out[S][16];
 #pragma unroll
@@ -374,20 +384,6 @@ __global__ void chol_slice_kernel(const double *A, int64_t n, int64_t mat_stride
   }
 }
 
-// rowsq[f][i] = sum_(k < j0) L_(j0+i, k)^2 in FP64 (one thread per row).
-__global__ void chol_rowsq_kernel(const double *A, int64_t n, int64_t mat_stride, int j0, int nb,
-                                  double *rowsq) {
-  const int f = blockIdx.y, i = threadIdx.x;
-  if (i >= nb) return;
-  const double *Af = A + f * mat_stride;
-  const int64_t r = j0 + i;
-  double s = 0.0;
-  for (int64_t k = 0; k < j0; ++k) {
-    const double x = Af[k * n + r];
-    s = fma(x, x, s);
-  }
-  rowsq[static_cast<int64_t>(f) * nb + i] = s;
-}
 
 // scale[i] = 2^e >= max_k |x(i, k)| of each row of an operand (1 for a row
 // of zeros or with a non-finite entry); x(i, k) = src[i ld + k], or
@@ -514,7 +510,10 @@ size_t ozaki_planes_bytes(int64_t n, int nmat, int slices) {
   return static_cast<size_t>(slices) * nmat * npad * npad;
 }
 
-int ozaki_chol_scales(const double *A, int64_t n, int nmat, double *scale, cudaStream_t st) {
+int ozaki_chol_scales(const double *A, int64_t n, int nmat, double *scale, double *rownorm,
+                      cudaStream_t st) {
+  if (cudaMemsetAsync(rownorm, 0, sizeof(double) * n * nmat, st) != cudaSuccess)
+    return MBPT_ERR_CUDA;
   count_launch();
   ozaki::chol_scale_kernel<<<ozaki::grid_blocks(n * nmat), 256, 0, st>>>(A, n, n * n, nmat,
                                                                          scale);
@@ -522,16 +521,17 @@ int ozaki_chol_scales(const double *A, int64_t n, int nmat, double *scale, cudaS
 }
 
 int ozaki_chol_slice(const double *A, int64_t n, int nmat, int64_t j0, int nb,
-                     const double *scale, int8_t *planes, int slices, cudaStream_t st) {
+                     const double *scale, int8_t *planes, int slices, double *rownorm,
+                     cudaStream_t st) {
   const int64_t npad = round_up(n, 128);
   dim3 grid(static_cast<unsigned>((n - j0 + 31) / 32), nmat);
   count_launch();
   if (slices == 8)
     ozaki::chol_slice_kernel<8><<<grid, 256, 0, st>>>(A, n, n * n, nmat, static_cast<int>(j0),
-                                                      nb, scale, planes, npad);
+                                                      nb, scale, planes, npad, rownorm);
   else if (slices == 7)
     ozaki::chol_slice_kernel<7><<<grid, 256, 0, st>>>(A, n, n * n, nmat, static_cast<int>(j0),
-                                                      nb, scale, planes, npad);
+                                                      nb, scale, planes, npad, rownorm);
   else
     return MBPT_ERR_SHAPE;
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
@@ -568,9 +568,6 @@ int ozaki_chol_update(double *A, int64_t n, int nmat, int64_t j0, int nb, double
   p.alpha = p.beta = 0.0;
   p.m_rows = p.n_cols = 0;
   p.err = err;
-  count_launch();
-  ozaki::chol_rowsq_kernel<<<dim3(1, nmat), 128, 0, st>>>(A, n, n * n, static_cast<int>(j0),
-                                                          nb, rowsq);
   const dim3 grid(static_cast<unsigned>(p.tiles_m * 2), nmat);
   static std::atomic<uint64_t> attr8{0}, attr7{0};
   if (slices == 8) {

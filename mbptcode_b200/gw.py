@@ -203,10 +203,12 @@ def qp_solve(sigma, pade_freq, eps_anchor, states, nocc, mu, xc=None, greedy=Tru
 
 
 def imaginary_axis_sample_points(freq_points, nocc, p, mu):
-    """z = mu -/+ i omega_p: the Pade sample points of state p, below mu for an
-    occupied state (``qp_solve.py:698-703``)."""
+    """(z_fit, query): the Pade sample points z = mu -/+ i omega_p of state p,
+    below mu for an occupied state, and the signed frequencies themselves
+    (``qp_solve.py:698-703``, whose callers unpack both)."""
     sign = -1.0 if p < nocc else 1.0
-    return mu + 1j * sign * np.asarray(freq_points, float)
+    query = sign * np.asarray(freq_points, float)
+    return mu + 1j * query, query
 
 
 def solve_qp_from_imaginary_axis(eps, p_state, xc_correction, z_fit, sigma_iw, greedy=True,

@@ -66,10 +66,15 @@ def test_ozaki_cholesky_flags_a_non_spd_frequency():
     """A frequency whose 1 - chi0 is indefinite fails its Cholesky on the
     int8 path as on the DGEMM path and is redone by LU (same W - I)."""
     n, nfreq = 256, 4
-    chi0 = _chi0_batch(n, nfreq, seed=7)
-    v = np.random.default_rng(3).standard_normal(n)
-    v /= np.linalg.norm(v)
-    chi0[2] += 1.5 * np.outer(v, v)                # an eigenvalue of chi0 above 1
+    rng = np.random.default_rng(7)
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    mats = []
+    for f in range(nfreq):
+        lam = -rng.uniform(0.05, 3.0, n)
+        if f == 2:
+            lam[5] = 1.4                           # an eigenvalue of chi0 above 1
+        mats.append((Q * lam) @ Q.T)
+    chi0 = np.stack(mats)
     ld_b, w_b, info_b = _run(chi0, ozaki=False)
     ld_o, w_o, info_o = _run(chi0, ozaki=True)
     assert info_o[2] != 0 and info_b[2] != 0

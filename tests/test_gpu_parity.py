@@ -742,7 +742,7 @@ def test_per_state_qp_solve_matches_reference_golden(golden):
     eps, nocc = g['eps'], int(g['nocc'])
     mu = float(grids.particle_hole_window(eps, nocc)[2])
     for p in range(len(eps)):
-        z_fit = gw.imaginary_axis_sample_points(g['pade'], nocc, p, mu)
+        z_fit, _ = gw.imaginary_axis_sample_points(g["pade"], nocc, p, mu)
         s_p = np.conj(g['sigma'][p]) if p < nocc else g['sigma'][p]
         root, z = gw.solve_qp_from_imaginary_axis(eps, p, 0.0, z_fit, s_p, with_z=True)
         if np.isfinite(g['roots'][p]):
