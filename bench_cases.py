@@ -14,6 +14,7 @@ the learned warm start). Nothing here is imported by the package.
     python bench_cases.py fp64-peak N
     python bench_cases.py adjoint-fd [--n 1200] [--nocc 120] [--M 7200] [--directions 32]
     python bench_cases.py adjoint-time [--n 1200] [--nocc 120] [--M 7200]
+    python bench_cases.py ozaki-gemm N
     python bench_cases.py warm-start [--train 512] [--eval 64] [--save model.npz]
 
 tau: one tau point of the chi0 sweep and one of the self-energy sweep, mixed
@@ -344,7 +345,9 @@ def adjoint_fd(a):
     random unit direction in ~5e7 parameters meets the gradient at ~1e-4 of
     its norm, so E_c's FP64 rounding (~1e-13 Ha) limits the plain h = 1e-5
     quotient to ~1e-5 relative at this size; the Richardson combination of
-    larger steps is reported beside it."""
+    larger steps is reported beside it. Each difference is given relative
+    to its direction's derivative and relative to the gradient's norm (the
+    first is large for a direction nearly orthogonal to the gradient)."""
     import json
     import time
     from mbptcode_b200 import adjoint
@@ -361,7 +364,11 @@ def adjoint_fd(a):
     torch.cuda.synchronize()
     t_adj = time.perf_counter() - t0
     g = torch.Generator(device=dev).manual_seed(a.seed + 1)
+    gnorm = float(torch.sqrt((torch.as_tensor(np.asarray(eb.cpu() if torch.is_tensor(eb) else eb),
+                                              device=dev) ** 2).sum() + (xb ** 2).sum()
+                             + (db ** 2).sum()))
     errs, rich, t_fd = [], [], time.perf_counter()
+    abs_plain, abs_rich, projections = [], [], []
     for _ in range(a.directions):
         de = torch.randn(n, generator=g, device=dev, dtype=torch.float64)
         dX = torch.randn(M, n, generator=g, device=dev, dtype=torch.float64)
@@ -377,9 +384,13 @@ def adjoint_fd(a):
 
         def central(h):
             return (energy(h) - energy(-h)) / (2 * h)
-        errs.append(abs(central(a.h) - ad) / max(abs(ad), 1e-300))
+        cp = central(a.h)
+        errs.append(abs(cp - ad) / max(abs(ad), 1e-300))
         r = (4 * central(a.h_richardson / 2) - central(a.h_richardson)) / 3
         rich.append(abs(r - ad) / max(abs(ad), 1e-300))
+        abs_plain.append(abs(cp - ad) / gnorm)
+        abs_rich.append(abs(r - ad) / gnorm)
+        projections.append(abs(ad) / gnorm)
     t_fd = time.perf_counter() - t_fd
     print(json.dumps({
         'config': {'n_orb': n, 'nocc': nocc, 'N_mu': M, 'ntau': a.ntau,
@@ -388,6 +399,10 @@ def adjoint_fd(a):
         'median_rel_diff': float(np.median(errs)),
         'richardson_h': a.h_richardson, 'richardson_max_rel_diff': max(rich),
         'richardson_median_rel_diff': float(np.median(rich)),
+        'gradient_norm': gnorm,
+        'min_projection_over_gradient_norm': float(min(projections)),
+        'max_diff_over_gradient_norm': float(max(abs_plain)),
+        'richardson_max_diff_over_gradient_norm': float(max(abs_rich)),
         'seconds_energy_and_adjoint': round(t_adj, 3), 'seconds_differences': round(t_fd, 2)}),
         flush=True)
 
@@ -436,6 +451,47 @@ def adjoint_time(a):
                       'eps_bar_norm': float(np.linalg.norm(np.asarray(
                           out[1].cpu().numpy() if torch.is_tensor(out[1]) else out[1])))}),
           flush=True)
+
+
+def ozaki_gemm_case(a):
+    """C = A B^T (N x N x N, FP64 row-major) by the int8 Ozaki GEMM
+    (mbpt_dgemm_ozaki, 8 digits) and by torch's FP64 product, three calls
+    each, CUDA-event timed; the capture case of the Ozaki kernel (one
+    launch of chol_update_kernel per call)."""
+    import json
+    from mbptcode_b200 import _lib
+    from mbptcode_b200._lib import check, lib, ptr
+    n = a.ozaki_gemm
+    g = torch.Generator(device='cuda').manual_seed(11)
+    A = torch.randn(n, n, generator=g, device='cuda', dtype=torch.float64)
+    B = torch.randn(n, n, generator=g, device='cuda', dtype=torch.float64)
+    C = torch.empty(n, n, dtype=torch.float64, device='cuda')
+    ws = torch.empty(lib().mbpt_dgemm_ozaki_workspace_bytes(n, n, n, 8), dtype=torch.uint8,
+                     device='cuda')
+
+    def oz():
+        check(lib().mbpt_dgemm_ozaki(0, 1, n, n, n, 1.0, ptr(A), n, ptr(B), n, 0.0, ptr(C), n, 8,
+                                     ptr(ws), ws.numel(), None, _lib.stream_ptr()),
+              'mbpt_dgemm_ozaki')
+
+    def best(fn):
+        ts = []
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        return min(ts)
+    t_oz = best(oz)
+    ref = A @ B.T
+    t_d = best(lambda: A @ B.T)
+    err = float((C - ref).abs().max() / ref.abs().max())
+    print(json.dumps({'case': 'ozaki-gemm', 'n': n, 'ozaki_s': round(t_oz, 5),
+                      'ozaki_fp64_tflops': round(2 * n ** 3 / t_oz / 1e12, 1),
+                      'dgemm_s': round(t_d, 5), 'dgemm_tflops': round(2 * n ** 3 / t_d / 1e12, 1),
+                      'max_err_rel': err}), flush=True)
 
 HARTREE_MEV = 27211.386245988
 
@@ -569,7 +625,7 @@ def main(argv=None):
     p = argparse.ArgumentParser(description='measurement cases beside bench.py')
     p.add_argument('case', choices=['tau', 'dyson', 'sweep', 'transform', 'qp-mlp', 'rows',
                                     'rows-cd', 'chi0-aux', 'fp64-peak', 'adjoint-fd',
-                                    'adjoint-time', 'warm-start'])
+                                    'adjoint-time', 'ozaki-gemm', 'warm-start'])
     p.add_argument('size', type=int, nargs='*', default=[])
     p.add_argument('--M', type=int, default=None)
     p.add_argument('--n', type=int, default=None)
@@ -597,7 +653,8 @@ def main(argv=None):
     p.add_argument('--save', default=None, help='write the trained network (.npz)')
     a = p.parse_args(argv)
     torch.cuda.set_device(0)
-    sized = {'dyson': 'dyson', 'transform': 'transform', 'fp64-peak': 'fp64_peak'}
+    sized = {'dyson': 'dyson', 'transform': 'transform', 'fp64-peak': 'fp64_peak',
+             'ozaki-gemm': 'ozaki_gemm'}
     if a.case in sized:
         setattr(a, sized[a.case], a.size[0])
     if a.case == 'chi0-aux':
@@ -607,7 +664,7 @@ def main(argv=None):
     run = {'tau': tau_point, 'dyson': dyson, 'sweep': sweep, 'transform': transform_case,
            'qp-mlp': qp_mlp_case, 'rows': rows, 'rows-cd': explicit_rows,
            'chi0-aux': chi0_aux_case, 'fp64-peak': fp64_peak, 'adjoint-fd': adjoint_fd,
-           'adjoint-time': adjoint_time,
+           'adjoint-time': adjoint_time, 'ozaki-gemm': ozaki_gemm_case,
            'warm-start': warm_start}[a.case]
     if a.case in ('tau', 'sweep'):
         big = a.case == 'sweep'

@@ -104,10 +104,11 @@ int mbpt_chi0_sweep(const double *X_dev, int64_t M, int64_t norb, int64_t nocc,
  * Replaces LinearResponse/space_time.py:956-968 dyson_screening (per
  * frequency, correlation=True) and :1073-1097 dielectric_log_determinant,
  * by a Cholesky factorisation of 1 - chi0 at each frequency (FP64). From
- * four frequencies on, one batched factorisation of all of them; with the
- * environment variable MBPT_DYSON_OZAKI=1 its trailing updates run on the
- * int8 tensor cores (the Ozaki scheme, FP64-accurate), otherwise as FP64
- * DGEMMs.
+ * four frequencies on, one batched factorisation of all of them, whose
+ * trailing updates run on the int8 tensor cores (the Ozaki scheme,
+ * FP64-accurate) in MBPT_MODE_MIXED and as native FP64 DGEMMs in
+ * MBPT_MODE_FP64 (the environment variable MBPT_DYSON_OZAKI=1 or =0 forces
+ * either).
  * chi0_dev (nfreq, naux, naux): in chi0; out W - I = [1 - chi0]^-1 - 1 when
  * want_w, else the Cholesky factors.
  * logdet_dev, trace_dev (nfreq): log det(1 - chi0) and tr chi0.

@@ -571,14 +571,18 @@ int chol_batched(double *A, int64_t n, int nmat, int *info, double *P, double *L
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 
-// MBPT_DYSON_OZAKI=1 runs the batched Cholesky's trailing updates on the int8
-// tensor cores with MBPT_DYSON_OZAKI_SLICES digits per operand (8 by
-// default; 7 is within 1e-12 of FP64 on W and at FP64 level on the
-// log-determinant); otherwise as cuBLAS DGEMMs. Read at every call, so the
-// size query and the call that follows it must see the same setting.
-int ozaki_slices() {
+// The batched Cholesky's trailing updates: on the int8 tensor cores (the
+// Ozaki scheme, FP64-accurate) in mixed mode, as native FP64 DGEMMs in FP64
+// mode (the plain FP64 path the mixed one is measured against).
+// MBPT_DYSON_OZAKI=1 / =0 forces either in both modes;
+// MBPT_DYSON_OZAKI_SLICES sets the digits per operand (8 by default; 7 is
+// within 1e-12 of FP64 on W and at FP64 level on the log-determinant). Read at
+// every call, so the size query and the call that follows it must see the
+// same setting.
+int ozaki_slices(int mode) {
   const char *e = std::getenv("MBPT_DYSON_OZAKI");
-  if (!e || std::atoi(e) == 0) return 0;
+  const bool on = e ? std::atoi(e) != 0 : mode == MBPT_MODE_MIXED;
+  if (!on) return 0;
   const char *k = std::getenv("MBPT_DYSON_OZAKI_SLICES");
   const int v = k ? std::atoi(k) : 8;
   return (v == 7 || v == 8) ? v : 8;
@@ -635,7 +639,7 @@ DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq, int mode = MBPT_MODE_FP64
     // every step's inverted diagonal blocks are kept: the mixed inverse reads them
     const int64_t steps = (n + kCholNb - 1) / kCholNb;
     b.chol_Linv = ar.take<double>(steps * nfreq * kCholNb * kCholNb);
-    b.oz_slices = ozaki_slices();
+    b.oz_slices = ozaki_slices(mode);
     if (b.oz_slices) {
       b.oz_planes = ar.take<int8_t>(ozaki_planes_bytes(n, nfreq, b.oz_slices));
       b.oz_scale = ar.take<double>(static_cast<int64_t>(nfreq) * n);
