@@ -114,9 +114,12 @@ __global__ void laplace_error_kernel(const double *__restrict__ d, int64_t npair
   }
   __shared__ double sw[32];
   __shared__ int sb[32];
+  // every lane takes part in every shuffle (no short-circuit around one)
   for (int o = 16; o > 0; o >>= 1) {
-    worst = fmax(worst, __shfl_down_sync(0xffffffffu, worst, o));
-    below = below || __shfl_down_sync(0xffffffffu, below ? 1 : 0, o);
+    const double w_other = __shfl_down_sync(0xffffffffu, worst, o);
+    const int b_other = __shfl_down_sync(0xffffffffu, below ? 1 : 0, o);
+    worst = fmax(worst, w_other);
+    below = below || b_other != 0;
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (lane == 0) {
