@@ -572,11 +572,12 @@ int chol_batched(double *A, int64_t n, int nmat, int *info, double *P, double *L
 }
 
 // The batched Cholesky's trailing updates: on the int8 tensor cores (the
-// Ozaki scheme, FP64-accurate) in mixed mode, as native FP64 DGEMMs in FP64
-// mode (the plain FP64 path the mixed one is measured against).
-// MBPT_DYSON_OZAKI=1 / =0 forces either in both modes;
-// MBPT_DYSON_OZAKI_SLICES sets the digits per operand (8 by default; 7 is
-// within 1e-12 of FP64 on W and at FP64 level on the log-determinant). Read at
+// Ozaki scheme) in mixed mode, as native FP64 DGEMMs in FP64 mode (the plain
+// FP64 path the mixed one is measured against). Digits per operand: 7 in
+// mixed mode (the log-determinant at FP64 level, the factor within ~1e-13;
+// W is formed from it by TF32x3 products there), 8 when forced in FP64 mode
+// (W within ~1e-14). MBPT_DYSON_OZAKI=1 / =0 forces the int8 path or the
+// DGEMMs in both modes, MBPT_DYSON_OZAKI_SLICES=7 / 8 the digits. Read at
 // every call, so the size query and the call that follows it must see the
 // same setting.
 int ozaki_slices(int mode) {
@@ -584,7 +585,7 @@ int ozaki_slices(int mode) {
   const bool on = e ? std::atoi(e) != 0 : mode == MBPT_MODE_MIXED;
   if (!on) return 0;
   const char *k = std::getenv("MBPT_DYSON_OZAKI_SLICES");
-  const int v = k ? std::atoi(k) : 8;
+  const int v = k ? std::atoi(k) : (mode == MBPT_MODE_MIXED ? 7 : 8);
   return (v == 7 || v == 8) ? v : 8;
 }
 

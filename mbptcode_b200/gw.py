@@ -496,7 +496,7 @@ def gw_sweep_unrestricted(X_mos, D, spectra, noccs, states=None, ntau='auto', ax
         chi0.add_(beta).mul_(0.5)
     del beta
     logdet, trace, info, _ = dyson_batch(chi0, want_w=True, stream=stream,
-                                         precision=precision, err=err, deferred=_deferred)
+                                         precision=precision, err=err)
     e_c = torch.empty((), dtype=torch.float64, device=dev)
     ow = torch.as_tensor(np.asarray(axes.grid.omega_weights, float), device=dev)
     check(lib().mbpt_energy_sum(ptr(logdet), ptr(trace), ptr(ow), len(ow), ptr(e_c),

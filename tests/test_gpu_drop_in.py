@@ -28,10 +28,10 @@ GRID_FIELDS = ('tau_points', 'tau_weights', 'omega_points', 'omega_weights', 'co
 # relative. The G0W0 driver sizes its grid itself (16 points here), whose
 # unregularised transform weights reach 3e8 and turn FP64 summation-order
 # differences into ~1e-7 relative on what passes through a transform (chi0,
-# W(tau), Sigma); a QP root of a state far from the gap carries the Pade
-# continuation's amplification
+# W(i w) from that chi0, W(tau), Sigma); a QP root of a state far from the
+# gap carries the Pade continuation's amplification
 TOL = {'solve_qp_from_imaginary_axis': 1e-6, 'chi0_imaginary_frequency': 1e-6,
-       '_transform_screened': 1e-6, '_sigma_mo_diagonal': 1e-6}
+       'dyson_screening': 1e-6, '_transform_screened': 1e-6, '_sigma_mo_diagonal': 1e-6}
 
 
 def _decode(desc, g):
