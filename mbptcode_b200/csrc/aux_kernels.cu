@@ -294,7 +294,7 @@ __global__ void scatter_cols_kernel(const double *__restrict__ T, int64_t M, int
 // n x n matrices (the lower factor, as cuSOLVER's lower-fill potrf leaves it;
 // the strict upper triangle is never written).
 constexpr int kCholNb = 128;
-constexpr int kCholStride = kCholNb + 2;  // (stride + 1) odd: row c of lane c in its own bank
+constexpr int kCholStride = kCholNb + 1;  // odd: a column of s read by a warp is free of bank conflicts
 
 // P_f (m x nbj, column-major, ld m) <- the block column A_f[j0:, j0:j0+nbj]
 __global__ void chol_copy_panel_kernel(const double *__restrict__ A, int64_t n, int64_t j0,
@@ -310,95 +310,213 @@ __global__ void chol_copy_panel_kernel(const double *__restrict__ A, int64_t n, 
 }
 
 // One CTA (512 threads) per matrix: the updated diagonal block (the top nbj
-// rows of P_f) is factorised in shared memory, right-looking: per column c
-// the column is scaled by 1/sqrt of its pivot (and copied to a contiguous
-// vector), then the rank-1 update of the rest runs one row per warp with the
-// lanes on consecutive columns, so the shared-memory accesses are free of
-// bank conflicts. Its lower factor goes into A_f's diagonal block (lower
-// triangle and diagonal only). The inverse X = L^-1 is formed one thread per
-// column by forward substitution, X kept transposed (column c of X in row c
-// of the strict upper triangle; the row stride makes the lanes' rows fall in
-// different banks), four independent partial sums per thread, and written to
-// Linv_f (column-major, ld kCholNb, zeros above the diagonal). A pivot that
-// is not positive records info_f = its global column + 1 (the first one
-// only), as potrf does; the factor of that matrix is then not meaningful.
+// rows of P_f, padded to 128 with the identity) is factorised and inverted in
+// shared memory, blocked by 32-column sub-blocks so that the sequential part,
+// one pivot after another, stays inside one warp:
+//  * warp 0 factorises the 32 x 32 diagonal sub-block in registers (lane r
+//    holds row r; each pivot's column is broadcast by shuffles, the chain per
+//    column is one rsqrt and one FMA) and forms its inverse X_kk by forward
+//    substitution column by column (lane c holds column c);
+//  * all warps then form the rows below it, L_ik = A_ik X_kk^T, and apply the
+//    rank-32 update of the trailing lower triangle in 4 x 4 register tiles;
+//  * after the last sub-block the off-diagonal blocks of X = L^-1 follow by
+//    block rows, X_ik = -X_ii sum_{k <= j < i} L_ij X_jk.
+// The lower factor goes into A_f's diagonal block (lower triangle and
+// diagonal only), X into Linv_f (column-major, ld kCholNb, zeros above the
+// diagonal). The diagonal is sqrt(pivot), the scaling of the column below it
+// rsqrt(pivot) (within an ulp of LAPACK's 1 / sqrt). A pivot that is not
+// positive records info_f = its global column + 1 (the first one only), as
+// potrf does; the factor of that matrix is then not meaningful.
+// Shared memory: s (128 x kCholStride: L in the strict lower triangle, the
+// off-diagonal blocks of X transposed in the upper one, X[r][c] at s[c][r]),
+// the diagonal of L and of X, the four X_kk dense (kCholXStride rows), and
+// the current panel transposed (pt, reused for the block products of the
+// inverse).
+constexpr int kCholSub = 32;
+constexpr int kCholXStride = kCholSub + 1;
+constexpr int kCholPtStride = kCholNb + 2;  // even: the 4 x 4 tiles read pairs
+constexpr int kCholSmemDoubles = kCholNb * kCholStride + 2 * kCholNb +
+                                 (kCholNb / kCholSub) * kCholSub * kCholXStride +
+                                 kCholSub * kCholPtStride;
+
 __global__ void __launch_bounds__(512) chol_diag_block_kernel(
     const double *__restrict__ P, int64_t m, int nbj, double *A, int64_t n, int64_t j0,
     double *__restrict__ Linv, int *info) {
-  extern __shared__ double sm[];
-  double *s = sm;                                  // nbj x nbj, row stride kCholStride
-  double *diag = sm + kCholNb * kCholStride;       // L_cc
-  double *xdiag = diag + kCholNb;                  // (L^-1)_cc
-  double *colc = xdiag + kCholNb;                  // the scaled column c
+  extern __shared__ __align__(16) double sm[];
+  constexpr int ST = kCholStride, XS = kCholXStride, PT = kCholPtStride, NB = kCholNb;
+  double *s = sm;
+  double *diag = s + NB * ST;                 // L_cc
+  double *xdiag = diag + NB;                  // X_cc = rsqrt(pivot)
+  double *xd = xdiag + NB;                    // X_kk dense, [k][r][c]
+  double *pt = xd + (NB / kCholSub) * kCholSub * XS;  // panel transposed, [m][i]
+  double *tb = pt;                            // the inverse's block products, [k][r][c]
   __shared__ int bad;
   const int f = blockIdx.x, tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
   const double *p = P + static_cast<int64_t>(f) * m * nbj;
   double *a = A + static_cast<int64_t>(f) * n * n;
   if (tid == 0) bad = -1;
-  // the tile, eight independent loads in flight per thread before any store
-  const int tot = nbj * nbj;
-  for (int i0 = tid; i0 < tot; i0 += 8 * blockDim.x) {
+  // the tile padded with the identity, zeros above the diagonal; eight
+  // independent loads in flight per thread before any store
+  for (int i0 = tid; i0 < NB * NB; i0 += 8 * blockDim.x) {
     double v[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int i = i0 + u * blockDim.x;
-      const int c = i / nbj, r = i % nbj;
-      v[u] = (i < tot && r >= c) ? p[static_cast<int64_t>(c) * m + r] : 0.0;
+      const int c = i / NB, r = i % NB;
+      v[u] = 0.0;
+      if (i < NB * NB && r >= c)
+        v[u] = (r < nbj && c < nbj) ? p[static_cast<int64_t>(c) * m + r] : (r == c ? 1.0 : 0.0);
     }
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int i = i0 + u * blockDim.x;
-      if (i < tot) s[(i % nbj) * kCholStride + i / nbj] = v[u];
+      if (i < NB * NB) s[(i % NB) * ST + i / NB] = v[u];
     }
   }
   __syncthreads();
-  for (int c = 0; c < nbj; ++c) {
-    // the pivot's square root and reciprocal only where they are used
-    if (tid == 0) {
-      const double d = s[c * kCholStride + c];
-      diag[c] = sqrt(d);
-      if (!(d > 0.0) && bad < 0) bad = c;
-    }
-    if (tid > c && tid < nbj) {
-      const double v = s[tid * kCholStride + c] / sqrt(s[c * kCholStride + c]);
-      s[tid * kCholStride + c] = v;
-      colc[tid] = v;
-    }
-    __syncthreads();
-    for (int r = c + 1 + warp; r < nbj; r += nwarps) {
-      const double lr = colc[r];
-      double *row = s + r * kCholStride;
-      for (int k = c + 1 + lane; k <= r; k += 32) row[k] -= lr * colc[k];
-    }
-    __syncthreads();
-  }
-  if (tid < nbj) xdiag[tid] = 1.0 / diag[tid];
-  __syncthreads();
-  // x_c = 1 / L_cc, x_r = -(sum_{c <= i < r} L_ri x_i) / L_rr, x_i (i > c) at s[c][i]
-  if (tid < nbj) {
-    const int c = tid;
-    const double *xc = s + c * kCholStride;
-    for (int r = c + 1; r < nbj; ++r) {
-      const double *lr = s + r * kCholStride;
-      double a0 = lr[c] * xdiag[c], a1 = 0.0, a2 = 0.0, a3 = 0.0;
-      int i = c + 1;
-      for (; i + 3 < r; i += 4) {
-        a0 = fma(lr[i], xc[i], a0);
-        a1 = fma(lr[i + 1], xc[i + 1], a1);
-        a2 = fma(lr[i + 2], xc[i + 2], a2);
-        a3 = fma(lr[i + 3], xc[i + 3], a3);
+  for (int k = 0; k < NB / kCholSub; ++k) {
+    const int b = k * kCholSub;
+    double *xk = xd + k * kCholSub * XS;
+    if (warp == 0) {
+      double *row = s + (b + lane) * ST + b;
+      double v[kCholSub];
+#pragma unroll
+      for (int j = 0; j < kCholSub; ++j) v[j] = row[j];
+      // right-looking in registers: entries of a lane above the diagonal
+      // are never read by another lane
+#pragma unroll
+      for (int c = 0; c < kCholSub; ++c) {
+        const double d = __shfl_sync(0xffffffffu, v[c], c);
+        const double rs = rsqrt(d);
+        if (lane == 0) {
+          xdiag[b + c] = rs;
+          diag[b + c] = sqrt(d);
+          if (!(d > 0.0) && bad < 0 && b + c < nbj) bad = b + c;
+        }
+        v[c] *= rs;
+#pragma unroll
+        for (int j = c + 1; j < kCholSub; ++j)
+          v[j] = fma(-v[c], __shfl_sync(0xffffffffu, v[c], j), v[j]);
       }
-      for (; i < r; ++i) a0 = fma(lr[i], xc[i], a0);
-      s[c * kCholStride + r] = -((a0 + a1) + (a2 + a3)) * xdiag[r];
+#pragma unroll
+      for (int j = 0; j < kCholSub; ++j)
+        if (j < lane) row[j] = v[j];
+      __syncwarp();
+      // X_kk column `lane`: x_i = (e_lane - sum_{j < i} L_ij x_j) / L_ii,
+      // the sums carried forward so that the chain per row is one FMA
+      double x[kCholSub];
+#pragma unroll
+      for (int r = 0; r < kCholSub; ++r) x[r] = r == lane ? 1.0 : 0.0;
+#pragma unroll
+      for (int i = 0; i < kCholSub; ++i) {
+        x[i] *= xdiag[b + i];
+#pragma unroll
+        for (int r = i + 1; r < kCholSub; ++r) x[r] = fma(-s[(b + r) * ST + b + i], x[i], x[r]);
+      }
+#pragma unroll
+      for (int r = 0; r < kCholSub; ++r) xk[r * XS + lane] = x[r];
     }
+    __syncthreads();
+    if (b + kCholSub >= NB) break;
+    // the rows below: L[i][b + j] = sum_q A[i][b + q] X_kk[j][q], two rows per warp pass
+    for (int i0 = b + kCholSub + 2 * warp; i0 < NB; i0 += 2 * nwarps) {
+      double *r0 = s + i0 * ST + b, *r1 = r0 + ST;
+      double acc0 = 0.0, acc1 = 0.0;
+#pragma unroll 8
+      for (int q = 0; q < kCholSub; ++q) {
+        const double x = xk[lane * XS + q];
+        acc0 = fma(r0[q], x, acc0);
+        acc1 = fma(r1[q], x, acc1);
+      }
+      __syncwarp();
+      r0[lane] = acc0;
+      r1[lane] = acc1;
+      pt[lane * PT + i0] = acc0;
+      pt[lane * PT + i0 + 1] = acc1;
+    }
+    __syncthreads();
+    // the trailing lower triangle -= panel panel^T, 4 x 4 tiles
+    const int base = b + kCholSub, nt = (NB - base) / 4;
+    for (int t = tid; t < nt * nt; t += blockDim.x) {
+      const int ti = t / nt, tj = t % nt;
+      if (ti < tj) continue;
+      const int i0 = base + 4 * ti, c0 = base + 4 * tj;
+      double acc[4][4] = {};
+#pragma unroll 4
+      for (int q = 0; q < kCholSub; ++q) {
+        const double2 a01 = *reinterpret_cast<const double2 *>(pt + q * PT + i0);
+        const double2 a23 = *reinterpret_cast<const double2 *>(pt + q * PT + i0 + 2);
+        const double2 b01 = *reinterpret_cast<const double2 *>(pt + q * PT + c0);
+        const double2 b23 = *reinterpret_cast<const double2 *>(pt + q * PT + c0 + 2);
+        const double av[4] = {a01.x, a01.y, a23.x, a23.y};
+        const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int w = 0; w < 4; ++w) acc[u][w] = fma(av[u], bv[w], acc[u][w]);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int w = 0; w < 4; ++w) s[(i0 + u) * ST + c0 + w] -= acc[u][w];
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  double *ld = Linv + static_cast<int64_t>(f) * kCholNb * kCholNb;
+  // X by block rows: T_ik = sum_{k <= j < i} L_ij X_jk, then X_ik = -X_ii T_ik;
+  // each of the 16 warps two rows (warp, warp + 16) of every block, the lanes
+  // on columns
+  for (int i = 1; i < NB / kCholSub; ++i) {
+    const double *l0 = s + (i * kCholSub + warp) * ST;
+    const double *l1 = l0 + 16 * ST;
+    for (int k = 0; k < i; ++k) {
+      double t0 = 0.0, t1 = 0.0;
+      const double *xkk = xd + k * kCholSub * XS;
+#pragma unroll 8
+      for (int q = 0; q < kCholSub; ++q) {
+        const double x = xkk[q * XS + lane];
+        t0 = fma(l0[k * kCholSub + q], x, t0);
+        t1 = fma(l1[k * kCholSub + q], x, t1);
+      }
+      for (int j = k + 1; j < i; ++j) {
+        const double *xc = s + (k * kCholSub + lane) * ST + j * kCholSub;  // X[j*32 + q][k*32 + lane]
+#pragma unroll 8
+        for (int q = 0; q < kCholSub; ++q) {
+          const double x = xc[q];
+          t0 = fma(l0[j * kCholSub + q], x, t0);
+          t1 = fma(l1[j * kCholSub + q], x, t1);
+        }
+      }
+      tb[(k * kCholSub + warp) * XS + lane] = t0;
+      tb[(k * kCholSub + warp + 16) * XS + lane] = t1;
+    }
+    __syncthreads();
+    const double *xii = xd + i * kCholSub * XS;
+    for (int k = 0; k < i; ++k) {
+      double v0 = 0.0, v1 = 0.0;
+#pragma unroll 8
+      for (int q = 0; q < kCholSub; ++q) {
+        const double tq = tb[(k * kCholSub + q) * XS + lane];
+        v0 = fma(xii[warp * XS + q], tq, v0);
+        v1 = fma(xii[(warp + 16) * XS + q], tq, v1);
+      }
+      s[(k * kCholSub + lane) * ST + i * kCholSub + warp] = -v0;
+      s[(k * kCholSub + lane) * ST + i * kCholSub + warp + 16] = -v1;
+    }
+    __syncthreads();
+  }
+  double *ld = Linv + static_cast<int64_t>(f) * NB * NB;
   for (int i = tid; i < nbj * nbj; i += blockDim.x) {
     const int c = i / nbj, r = i % nbj;
-    if (r >= c) a[(j0 + c) * n + j0 + r] = r == c ? diag[c] : s[r * kCholStride + c];
-    ld[c * kCholNb + r] = r == c ? xdiag[c] : (r > c ? s[c * kCholStride + r] : 0.0);
+    if (r >= c) a[(j0 + c) * n + j0 + r] = r == c ? diag[c] : s[r * ST + c];
+    double x = 0.0;
+    if (r == c)
+      x = xdiag[c];
+    else if (r > c)
+      x = (r / kCholSub == c / kCholSub)
+              ? xd[(r / kCholSub) * kCholSub * XS + (r % kCholSub) * XS + c % kCholSub]
+              : s[c * ST + r];
+    ld[c * NB + r] = x;
   }
   if (tid == 0 && bad >= 0 && info[f] == 0) info[f] = static_cast<int>(j0) + bad + 1;
 }
@@ -613,7 +731,7 @@ void launch_chol_copy_panel(const double *A, int64_t n, int64_t j0, int64_t m, i
 int launch_chol_diag_block(const double *P, int64_t m, int nbj, double *A, int64_t n,
                            int64_t j0, int nmat, double *Linv, int *info, cudaStream_t st) {
   if (nbj < 1 || nbj > kCholNb) return MBPT_ERR_SHAPE;
-  const size_t smem = sizeof(double) * (kCholNb * kCholStride + 3 * kCholNb);
+  const size_t smem = sizeof(double) * kCholSmemDoubles;
   if (cudaFuncSetAttribute(chol_diag_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(smem)) != cudaSuccess)
     return MBPT_ERR_CUDA;
