@@ -589,6 +589,22 @@ int ozaki_slices(int mode) {
   return (v == 7 || v == 8) ? v : 8;
 }
 
+// Mixed mode: the tensor-core inverses of that many frequencies run at once,
+// each on its own side stream with its own TF32 pair scratch (8 n_p^2 floats):
+// the recursion's deep levels are small products that leave most of the GPU
+// idle when one frequency runs alone. MBPT_DYSON_INVERSE_STREAMS (1 to 4,
+// default 4), read once per process so that the size query and the call see
+// the same count.
+constexpr int kMaxInverseStreams = 4;
+int inverse_streams() {
+  static const int v = [] {
+    const char *e = std::getenv("MBPT_DYSON_INVERSE_STREAMS");
+    const int k = e ? std::atoi(e) : kMaxInverseStreams;
+    return std::max(1, std::min(kMaxInverseStreams, k));
+  }();
+  return v;
+}
+
 bool batched_chol_enabled(int nfreq) {
   // MBPT_DYSON_BATCHED=0 keeps one cuSOLVER potrf per frequency
   static const int env = [] {
@@ -606,7 +622,8 @@ struct DysonBufs {
   double *rhs;   // n x n right-hand side of the LU inverse of a failed frequency
   double *diag;  // nfreq x n diagonals of 1 - chi0, which the factorisation overwrites
   double *T;     // diagonal-block scratch of the LAUUM
-  PairScratch pairs;  // mixed mode: TF32 pairs of the tensor-core inverse
+  PairScratch pairs[kMaxInverseStreams];  // mixed mode: one per inverse stream
+  int npairs = 0;
   double *chol_P = nullptr, *chol_Linv = nullptr;  // batched Cholesky scratch
   int8_t *oz_planes = nullptr;                       // Ozaki digit planes (all frequencies)
   double *oz_scale = nullptr, *oz_rowsq = nullptr;
@@ -649,11 +666,14 @@ DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq, int mode = MBPT_MODE_FP64
   }
   if (mode == MBPT_MODE_MIXED) {
     const int64_t np = round_up(n, 128), cap = np * np;
-    PairScratch &q = b.pairs;
-    q.np = np;
-    for (float **f : {&q.lr_hi, &q.lr_lo, &q.ic_hi, &q.ic_lo, &q.ir_hi, &q.ir_lo, &q.tt_hi,
-                      &q.tt_lo})
-      *f = ar.take<float>(cap);
+    b.npairs = std::min(inverse_streams(), std::max(1, nfreq));
+    for (int i = 0; i < b.npairs; ++i) {
+      PairScratch &q = b.pairs[i];
+      q.np = np;
+      for (float **f : {&q.lr_hi, &q.lr_lo, &q.ic_hi, &q.ic_lo, &q.ir_hi, &q.ir_lo, &q.tt_hi,
+                        &q.tt_lo})
+        *f = ar.take<float>(cap);
+    }
   }
   return b;
 }
@@ -668,6 +688,9 @@ struct DysonPipe {
   // the inverses' own cuBLAS handle (bound to `side`): the caller's handle
   // may still be running a later wave's factorisation on the caller's stream
   cublasHandle_t blas_side = nullptr;
+  // mixed mode's further inverse streams (index i + 1 of the inverse streams)
+  std::vector<cudaStream_t> isides;
+  std::vector<cudaEvent_t> ijoin;
   // second factor stream: odd frequencies factorise there with their own
   // cuSOLVER handle, so that two Cholesky factorisations (latency-bound
   // panels between DGEMM-bound updates) share the GPU
@@ -713,6 +736,14 @@ DysonPipe *dyson_pipe(int nfreq) {
               cusolverDnSetStream(p->solver2, p->fac2) == CUSOLVER_STATUS_SUCCESS &&
               cublasCreate(&p->blas2) == CUBLAS_STATUS_SUCCESS &&
               cublasSetStream(p->blas2, p->fac2) == CUBLAS_STATUS_SUCCESS;
+    for (int i = 1; p->ok && i < kMaxInverseStreams; ++i) {
+      cudaStream_t s = nullptr;
+      cudaEvent_t e = nullptr;
+      p->ok = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
+      p->isides.push_back(s);
+      p->ijoin.push_back(e);
+    }
     const char *genv = std::getenv("MBPT_DYSON_CHOL_GROUPS");
     const int g = genv ? std::atoi(genv) : 4;
     p->groups = p->nfac == 2 ? std::max(1, std::min(6, g)) : 1;
@@ -771,11 +802,17 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
   if (mode == MBPT_MODE_MIXED && want_w) {
     // the pair arrays are read as zeros wherever the recursion does not write
     // (padding, above the diagonal blocks); every frequency writes the rest
-    const size_t bytes = sizeof(float) * b.pairs.np * b.pairs.np;
-    for (float *f : {b.pairs.lr_hi, b.pairs.lr_lo, b.pairs.ic_hi, b.pairs.ic_lo, b.pairs.ir_hi,
-                     b.pairs.ir_lo, b.pairs.tt_hi, b.pairs.tt_lo})
-      if (cudaMemsetAsync(f, 0, bytes, st) != cudaSuccess) return MBPT_ERR_CUDA;
+    for (int i = 0; i < b.npairs; ++i) {
+      const PairScratch &q = b.pairs[i];
+      const size_t bytes = sizeof(float) * q.np * q.np;
+      for (float *f : {q.lr_hi, q.lr_lo, q.ic_hi, q.ic_lo, q.ir_hi, q.ir_lo, q.tt_hi, q.tt_lo})
+        if (cudaMemsetAsync(f, 0, bytes, st) != cudaSuccess) return MBPT_ERR_CUDA;
+    }
   }
+  // the inverse streams: FP64 mode's cuBLAS inverse on the side stream only
+  const int nsides = mode == MBPT_MODE_MIXED ? b.npairs : 1;
+  auto side_of = [&](int i) { return i == 0 ? pp->side : pp->isides[i - 1]; };
+  bool side_used[kMaxInverseStreams] = {};
   // many frequencies: one batched factorisation of all of them, then the
   // per-frequency loop below only reads their info words
   const bool batched = b.chol_P != nullptr;
@@ -865,7 +902,7 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
       return MBPT_ERR_CUDA;
     return MBPT_OK;
   };
-  bool bad = false, side_used = false;
+  bool bad = false;
   int rc = MBPT_OK;
   for (int f = 0; f < nfac && f < nfreq && rc == MBPT_OK; ++f) rc = factor(f);
   for (int f = 0; f < nfreq && rc == MBPT_OK; ++f) {
@@ -880,28 +917,31 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
     double *m = chi0 + f * n * n;
     if (inf == 0) {
       if (want_w) {
-        side_used = true;
-        if (cudaStreamWaitEvent(pp->side, pp->ev[f], 0) != cudaSuccess) {
+        const int si = f % nsides;
+        cudaStream_t ss = side_of(si);
+        side_used[si] = true;
+        if (cudaStreamWaitEvent(ss, pp->ev[f], 0) != cudaSuccess) {
           rc = MBPT_ERR_CUDA;
           break;
         }
         Handles hs{pp->blas_side, h.solver};
         bool full = false;
         rc = spd_inverse_from_factor(
-            hs, m, n, b.T, b.rhs, mode == MBPT_MODE_MIXED ? &b.pairs : nullptr, err, &full,
-            pp->side,
-            batched ? b.chol_Linv + static_cast<int64_t>(f) * kCholNb * kCholNb : nullptr,
+            hs, m, n, b.T, b.rhs, mode == MBPT_MODE_MIXED ? &b.pairs[si] : nullptr, err, &full,
+            ss, batched ? b.chol_Linv + static_cast<int64_t>(f) * kCholNb * kCholNb : nullptr,
             static_cast<int64_t>(nfreq) * kCholNb * kCholNb);
         if (rc) break;
-        if (!full) launch_symmetrize_minus_identity(m, n, 1, pp->side);
+        if (!full) launch_symmetrize_minus_identity(m, n, 1, ss);
       }
       continue;
     }
-    // not positive definite: drain both streams (the LU shares the scratch),
+    // not positive definite: drain every stream (the LU shares the scratch),
     // restore 1 - chi0 from its untouched triangle, then LU for log|det| (and
     // the inverse), as the reference's slogdet/inv
     bad = true;
-    if (cudaStreamSynchronize(pp->side) != cudaSuccess ||
+    for (int i = 1; i < nsides; ++i)
+      if (cudaStreamSynchronize(side_of(i)) != cudaSuccess) rc = MBPT_ERR_CUDA;
+    if (rc || cudaStreamSynchronize(pp->side) != cudaSuccess ||
         (nfac == 2 && cudaStreamSynchronize(pp->fac2) != cudaSuccess) ||
         cudaStreamSynchronize(st) != cudaSuccess) {
       rc = MBPT_ERR_CUDA;
@@ -935,9 +975,11 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
     }
     if (sign_host) sign_host[f] = sgn;
   }
-  if (side_used) {
-    cudaEventRecord(pp->join, pp->side);
-    cudaStreamWaitEvent(st, pp->join, 0);
+  for (int i = 0; i < nsides; ++i) {
+    if (!side_used[i]) continue;
+    cudaEvent_t j = i == 0 ? pp->join : pp->ijoin[i - 1];
+    cudaEventRecord(j, side_of(i));
+    cudaStreamWaitEvent(st, j, 0);
   }
   if (nfac == 2) {
     cudaEventRecord(pp->join2, pp->fac2);
