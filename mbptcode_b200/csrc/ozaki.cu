@@ -17,7 +17,8 @@
 //
 // Kernel layout: 128 x 64 output tiles (rows r of the panel, 64 of its
 // columns), warp 0 the TMA producer (64-byte swizzled boxes of 64 K), warp 1
-// the TMEM owner and MMA issuer (S(S+1)/2 products per 32-wide K step), warps
+// the TMEM owner and MMA issuer (the S(S+1)/2 products of a 32-wide K step
+// as one MMA per A plane and group of up to four B planes), warps
 // 2-5 the epilogue; two pipeline stages of S A-planes and S B-planes; every
 // mbarrier wait bounded, as in the split engine.
 #include <algorithm>
@@ -38,6 +39,7 @@ using umma::tc_fence_before;
 constexpr int BM = 128;   // panel rows per tile
 constexpr int BN = 64;    // panel columns per tile
 constexpr int BKB = 64;   // K bytes (int8 elements) per stage
+constexpr int kStackPlanes = 4;  // B planes per MMA: N = 4 x 64 = 256, the largest
 
 template <int S>
 struct Layout {
@@ -201,7 +203,6 @@ __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_consta
     __syncwarp();
   } else if (warp == 1) {
     if (lane == 0) {
-      constexpr uint32_t idesc = idesc_s8(BN);
       bool ok = true;
       for (int kt = 0; kt < p.k_tiles; ++kt) {
         const int s = kt % L::kStages;
@@ -216,17 +217,22 @@ __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_consta
         for (int kk = 0; kk < 2; ++kk) {
           const uint64_t adv = static_cast<uint64_t>(kk * 2);  // 32 bytes >> 4
           const bool first = kt == 0 && kk == 0;
+          // A plane sa against the B planes 1 .. S + 1 - sa stacked as one
+          // operand (they lie back to back, 64 rows each): product (sa, t)
+          // lands in column block sa + t - 2, its level's accumulator, so one
+          // MMA of up to 256 columns serves four levels and A is read from
+          // shared memory once per four products. Plane 1 covers every
+          // level, so its MMAs open the accumulators.
 #pragma unroll
-          for (int lev = 2; lev <= S + 1; ++lev) {
-            const uint32_t d = tmem + static_cast<uint32_t>((lev - 2) * BN);
-            const int s_lo = lev - S > 1 ? lev - S : 1;
-            const int s_hi = lev - 1 < S ? lev - 1 : S;
+          for (int sa = 1; sa <= S; ++sa) {
+            const uint64_t da = sw64_desc(st + (sa - 1) * L::kAPlane) + adv;
 #pragma unroll
-            for (int sa = s_lo; sa <= s_hi; ++sa) {
-              const int sb = lev - sa;
-              const uint64_t da = sw64_desc(st + (sa - 1) * L::kAPlane) + adv;
-              const uint64_t db = sw64_desc(st + S * L::kAPlane + (sb - 1) * L::kBPlane) + adv;
-              mma_s8(d, da, db, idesc, (first && sa == s_lo) ? 0u : 1u);
+            for (int t0 = 1; t0 <= S + 1 - sa; t0 += kStackPlanes) {
+              const int cnt = S + 1 - sa - t0 + 1 < kStackPlanes ? S + 1 - sa - t0 + 1
+                                                                  : kStackPlanes;
+              const uint32_t d = tmem + static_cast<uint32_t>((sa - 1 + t0 - 1) * BN);
+              const uint64_t db = sw64_desc(st + S * L::kAPlane + (t0 - 1) * L::kBPlane) + adv;
+              mma_s8(d, da, db, idesc_s8(cnt * BN), (first && sa == 1) ? 0u : 1u);
             }
           }
         }
