@@ -22,7 +22,24 @@
  *     the Coulomb-side products, TF32 pairs for G_occ / G_virt and for the
  *     inverse of the Dyson step. The tau <-> omega transforms, the
  *     Cholesky/log-det, the quadrature sums and the QP root search are FP64
- *     in both modes.
+ *     in both modes. MBPT_MODE_FP64_INT8 is FP64-accurate like
+ *     MBPT_MODE_FP64, with the forward sweeps' products and the Cholesky
+ *     updates of the Dyson step emulated on the int8 tensor cores (the Ozaki
+ *     scheme, 8 seven-bit digits per operand: mbpt_dgemm_ozaki); accepted
+ *     wherever MBPT_MODE_FP64 is.
+ *   - The reverse sweeps (mbpt_chi0_backward, mbpt_sigma_backward,
+ *     mbpt_dyson_backward) take the same two FP64 modes: native DGEMMs or
+ *     the emulated product, which also forms the symmetric products' upper
+ *     tiles only and the G branches' adjoints straight from its epilogue.
+ *     The FP64 products of the rows beside the route that take no mode
+ *     (mbpt_sigma_ao, mbpt_three_index_slices and its backward,
+ *     mbpt_cd_integral_backward) run on the emulated product;
+ *     MBPT_FP64_GEMM=cublas in the environment keeps cuBLAS DGEMMs there.
+ *   - The emulation's error is ~5e-15 of the operands' scale per product,
+ *     about FP64 rounding, but it changes erratically with the inputs where
+ *     rounding changes smoothly: a tau <-> omega transform whose weights
+ *     cancel at 1e8 (the 16-point grids) amplifies it ~100x more, so FP64
+ *     is the mode for such grids.
  *
  * Symbols: X (M x norb) collocation of the MO basis on the interpolation
  * points, columns [0, nocc) occupied; D (M x naux) Coulomb factor, Z = D D^T;
@@ -50,7 +67,7 @@ enum mbpt_status {
   MBPT_ERR_UNSUPPORTED = 8  /* device or option not supported */
 };
 
-enum mbpt_mode { MBPT_MODE_FP64 = 0, MBPT_MODE_MIXED = 1 };
+enum mbpt_mode { MBPT_MODE_FP64 = 0, MBPT_MODE_MIXED = 1, MBPT_MODE_FP64_INT8 = 2 };
 
 int mbpt_abi_version(void);
 const char *mbpt_status_string(int status);
@@ -255,14 +272,16 @@ int mbpt_energy_adjoint_seed(double *w_minus_i_dev, int64_t naux, int nfreq,
  * X_bar (M x norb), D_bar (M x naux) with the self-energy sweep's share and
  * writes Wt_bar_dev (ntau, naux, naux), which the Dyson and chi0 reverses
  * (mbpt_dyson_backward, mbpt_transform, mbpt_chi0_backward) take on.
- * states_dev: nstates int64 orbital indices. FP64. */
+ * states_dev: nstates int64 orbital indices. mode: MBPT_MODE_FP64 or
+ * MBPT_MODE_FP64_INT8. */
 size_t mbpt_sigma_backward_workspace_bytes(int64_t M, int64_t norb, int64_t nocc,
                                            int64_t naux, int nstates);
 int mbpt_sigma_backward(const double *X_dev, int64_t M, int64_t norb, int64_t nocc,
                         const double *eps_dev, double mu, const double *D_dev, int64_t naux,
                         const double *tau_host, int ntau, const double *Wt_dev,
                         const int64_t *states_dev, int nstates, const double *sl_bar_dev,
-                        const double *sg_bar_dev, double *eps_bar_dev, double *X_bar_dev,
+                        const double *sg_bar_dev, int mode, double *eps_bar_dev,
+                        double *X_bar_dev,
                         double *D_bar_dev, double *Wt_bar_dev, void *workspace,
                         size_t ws_bytes, int *err_dev, void *stream);
 
@@ -370,10 +389,11 @@ int mbpt_three_index_slice_backward(const double *X_dev, int64_t M, int64_t norb
 
 /* The reverse of the Dyson step W = [1 - chi0]^-1: chi0_bar_f = W_f W_bar_f W_f
  * (gradients/rpa/space_time_adjoint.py:679-685), in place over wbar_dev
- * (nfreq, naux, naux), from W - I (w_minus_i_dev, the Dyson output). FP64. */
+ * (nfreq, naux, naux), from W - I (w_minus_i_dev, the Dyson output). mode:
+ * MBPT_MODE_FP64 or MBPT_MODE_FP64_INT8. */
 size_t mbpt_dyson_backward_workspace_bytes(int64_t naux);
 int mbpt_dyson_backward(const double *w_minus_i_dev, double *wbar_dev, int64_t naux, int nfreq,
-                        void *workspace, size_t ws_bytes, void *stream);
+                        int mode, void *workspace, size_t ws_bytes, void *stream);
 
 /* ---- quasiparticle-shift network (learned warm start) --------------------
  * A 4 -> H -> H -> 1 perceptron with SiLU, FP32, parameters packed as

@@ -16,8 +16,8 @@ _PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'libmbpt_b200.s
 _LIB = None
 _LOCK = threading.Lock()
 
-MODE_FP64, MODE_MIXED = 0, 1
-MODES = {'fp64': MODE_FP64, 'mixed': MODE_MIXED}
+MODE_FP64, MODE_MIXED, MODE_FP64_INT8 = 0, 1, 2
+MODES = {'fp64': MODE_FP64, 'mixed': MODE_MIXED, 'fp64_int8': MODE_FP64_INT8}
 
 OK, ERR_SHAPE, ERR_NOT_SPD, ERR_NONFINITE, ERR_NO_ROOT, ERR_TIMEOUT, ERR_CUDA, \
     ERR_WORKSPACE, ERR_UNSUPPORTED = range(9)
@@ -56,7 +56,7 @@ _SIGNATURES = {
     'mbpt_energy_adjoint_seed': (_i, [_p, _i64, _i, _p, _p]),
     'mbpt_sigma_backward_workspace_bytes': (_sz, [_i64, _i64, _i64, _i64, _i]),
     'mbpt_sigma_backward': (_i, [_p, _i64, _i64, _i64, _p, _d, _p, _i64, _p, _i, _p, _p, _i,
-                                 _p, _p, _p, _p, _p, _p, _p, _sz, _p, _p]),
+                                 _p, _p, _i, _p, _p, _p, _p, _p, _sz, _p, _p]),
     'mbpt_sigma_ao_workspace_bytes': (_sz, [_i64, _i64, _i64, _i64, _i64]),
     'mbpt_sigma_ao': (_i, [_p, _i64, _i64, _p, _i64, _i64, _p, _d, _p, _i64, _p, _p, _i, _p,
                            _p, _sz, _p, _p]),
@@ -76,7 +76,7 @@ _SIGNATURES = {
     'mbpt_three_index_slice_backward': (_i, [_p, _i64, _i64, _p, _i64, _i64, _p, _p, _p, _p,
                                              _sz, _p]),
     'mbpt_dyson_backward_workspace_bytes': (_sz, [_i64]),
-    'mbpt_dyson_backward': (_i, [_p, _p, _i64, _i, _p, _sz, _p]),
+    'mbpt_dyson_backward': (_i, [_p, _p, _i64, _i, _i, _p, _sz, _p]),
     'mbpt_mlp_param_count': (_i, [_i]),
     'mbpt_mlp_forward': (_i, [_p, _i, _p, _i, _p, _p, _p]),
     'mbpt_mlp_backward': (_i, [_p, _i, _p, _i, _p, _p, _p, _p, _p, _p]),

@@ -29,6 +29,24 @@ from ._lib import WORKSPACE, check, host_array, lib, ptr, require_device, stream
 from .space_time import (_Err, _eps_host, _mode, chi0_sweep, dyson_batch,
                          particle_hole_window, to_device, transform)
 
+#: precision of the adjoints' sweeps (forward and reverse) where the call
+#: names none: FP64-accurate, with the products and the Cholesky updates
+#: emulated on the int8 tensor cores (8 seven-bit digits per operand), on
+#: grids whose tau <-> omega weights stay below INT8_WEIGHT_LIMIT; native FP64
+#: ('fp64') on the others. The emulation's error, ~5e-15 of the operands'
+#: scale per product, changes erratically from one tau point to the next, so
+#: weights that cancel at 1e8 (the 16-point grids of small gaps) lift it
+#: past FP64 rounding (E_c 8e-10 relative at 2.4e8, against 1e-11).
+ADJOINT_PRECISION = 'fp64_int8'
+INT8_WEIGHT_LIMIT = 1e6
+
+
+def _adjoint_precision(precision, *weights):
+    if precision is not None:
+        return precision
+    w = max((float(np.abs(np.asarray(x, float)).max()) for x in weights), default=0.0)
+    return ADJOINT_PRECISION if w <= INT8_WEIGHT_LIMIT else 'fp64'
+
 
 def chi0_backward(proj_bar, X, D, eps, nocc, tau_points, mu, precision='fp64', stream=None):
     """(eps_bar, X_bar, D_bar) device tensors for an adjoint proj_bar
@@ -66,20 +84,23 @@ def polarizability_backward(proj_bar, X, D, eps, nocc, grid, mu=None, tile_gb=No
     eps_h = _eps_host(eps)
     if mu is None:
         mu = particle_hole_window(eps_h, nocc)[2]
-    out = chi0_backward(to_device(proj_bar, dev), X, D, eps_h, nocc, grid.tau_points, mu)
+    out = chi0_backward(to_device(proj_bar, dev), X, D, eps_h, nocc, grid.tau_points, mu,
+                        precision=_adjoint_precision(None, grid.cosft_wt))
     return tuple(t if isinstance(proj_bar, torch.Tensor) else t.cpu().numpy() for t in out)
 
 
 def energy_and_adjoint_device(X, D, eps, nocc, grid, mu=None, want_grad=True,
-                              precision='fp64', stream=None):
+                              precision=None, stream=None):
     """(E_c 0-d tensor, eps_bar, X_bar, D_bar) on the device."""
+    precision = _adjoint_precision(precision, grid.cosft_wt)
     dev = require_device()
     eps_h = _eps_host(eps)
     if mu is None:
         mu = particle_hole_window(eps_h, nocc)[2]
     chi0, proj = chi0_sweep(X, D, eps_h, nocc, grid.tau_points, grid.cosft_wt, mu=mu,
                             precision=precision, want_proj=want_grad, stream=stream)
-    logdet, trace, info, _ = dyson_batch(chi0, want_w=want_grad, stream=stream)
+    logdet, trace, info, _ = dyson_batch(chi0, want_w=want_grad, stream=stream,
+                                         precision=precision)
     ow = torch.as_tensor(np.asarray(grid.omega_weights, float), device=dev)
     e_c = torch.empty((), dtype=torch.float64, device=dev)
     check(lib().mbpt_energy_sum(ptr(logdet), ptr(trace), ptr(ow), len(ow), ptr(e_c),
@@ -95,12 +116,12 @@ def energy_and_adjoint_device(X, D, eps, nocc, grid, mu=None, want_grad=True,
     proj_bar = transform(chi0, np.ascontiguousarray(np.asarray(grid.cosft_wt).T), stream)
     del chi0, proj
     eps_bar, X_bar, D_bar = chi0_backward(proj_bar, X, D, eps_h, nocc, grid.tau_points, mu,
-                                          precision='fp64', stream=stream)
+                                          precision=precision, stream=stream)
     return e_c, eps_bar, X_bar, D_bar
 
 
 def rpa_energy_and_adjoint(X, D, eps, nocc, grid, mu=None, want_grad=True, tile_gb=None,
-                           screening=None, counter_term=None, comm=None, precision='fp64'):
+                           screening=None, counter_term=None, comm=None, precision=None):
     """``space_time_adjoint.py:473-563``: (e_c, eps_bar, X_bar, D_bar,
     fold_bar) with fold_bar None (no solvent fold on the device route);
     want_grad=False returns E_c alone. Arrays come back as the inputs are
@@ -133,7 +154,7 @@ class RPAEnergy(torch.autograd.Function):
         return g * eb, g * xb, g * db, None, None, None, None
 
 
-def rpa_energy(eps, X, D=None, nocc=None, grid=None, V=None, mu=None, precision='fp64'):
+def rpa_energy(eps, X, D=None, nocc=None, grid=None, V=None, mu=None, precision=None):
     """Differentiable E_c of device tensors: give D (M x naux), or V (M x M,
     SPD) with D = chol(V) taken by torch so that V gets a gradient too."""
     if D is None:
@@ -157,7 +178,7 @@ def _back(t, like):
 
 
 def selfenergy_diag(X, D, eps, nocc, grid, states, transforms, mu, tile_gb=None, comm=None,
-                    precision='fp64'):
+                    precision=None):
     """Sigma^c_pp(i omega_out) of `states` on the grid's own tau points, and
     the cache its reverse needs (``GW/imaginary_time.py:731-768``): chi0 and
     proj(tau) in one sweep, W - I by the Dyson step, Wt(tau) = Ctw (W - I),
@@ -166,6 +187,7 @@ def selfenergy_diag(X, D, eps, nocc, grid, states, transforms, mu, tile_gb=None,
     cache's tensors stay on the device."""
     from .gw import sigma_branch_sums, sigma_frequency, w_tau_from_frequencies
     _one_rank(comm, 'selfenergy_diag')
+    precision = _adjoint_precision(precision, grid.cosft_wt, *transforms)
     dev = require_device()
     Xd, Dd = to_device(X, dev), to_device(D, dev)
     eps_h = _eps_host(eps)
@@ -181,29 +203,33 @@ def selfenergy_diag(X, D, eps, nocc, grid, states, transforms, mu, tile_gb=None,
     return _back(sigma, X), (proj, Wt, None)
 
 
-def screened_interaction_tau_backward(Wt_bar, proj_tau, grid, Ctw, tile_gb=None, comm=None):
+def screened_interaction_tau_backward(Wt_bar, proj_tau, grid, Ctw, tile_gb=None, comm=None,
+                                      precision=None):
     """proj_bar (ntau, naux, naux) for an adjoint Wt_bar on
     Wt(tau) = sum_w Ctw[tau, w] (W_w - I) (``space_time_adjoint.py:652-691``):
     chi0 rebuilt from proj(tau), W by the Dyson step, chi0_bar = W W_bar W per
-    frequency, and the two transforms turned round. FP64."""
+    frequency, and the two transforms turned round. FP64-accurate."""
     _one_rank(comm, 'screened_interaction_tau_backward')
+    precision = _adjoint_precision(precision, grid.cosft_wt, Ctw)
     dev = require_device()
     Wb, P = to_device(Wt_bar, dev), to_device(proj_tau, dev)
     cw = np.asarray(grid.cosft_wt, float)
     chi0 = transform(P, cw)
-    dyson_batch(chi0, want_w=True, precision='fp64')
+    dyson_batch(chi0, want_w=True, precision=precision)
     wbar = transform(Wb, np.ascontiguousarray(np.asarray(Ctw, float).T))
     naux, nfreq = chi0.shape[-1], chi0.shape[0]
     ws = WORKSPACE.get(lib().mbpt_dyson_backward_workspace_bytes(naux), dev)
-    check(lib().mbpt_dyson_backward(ptr(chi0), ptr(wbar), naux, nfreq, ptr(ws), ws.numel(),
-                                    stream_ptr()), 'mbpt_dyson_backward')
+    check(lib().mbpt_dyson_backward(ptr(chi0), ptr(wbar), naux, nfreq, _mode(precision),
+                                    ptr(ws), ws.numel(), stream_ptr()), 'mbpt_dyson_backward')
     proj_bar = transform(wbar, np.ascontiguousarray(cw.T))
     return _back(proj_bar, Wt_bar)
 
 
-def sigma_backward(branch_bar, X, D, eps, nocc, tau_points, states, mu, Wt):
+def sigma_backward(branch_bar, X, D, eps, nocc, tau_points, states, mu, Wt,
+                   precision=ADJOINT_PRECISION):
     """(eps_bar, X_bar, D_bar, Wt_bar) device tensors of the self-energy sweep
-    alone for branch adjoints (2, ntau, nstates) on (Sigma^<, Sigma^>)."""
+    alone for branch adjoints (2, ntau, nstates) on (Sigma^<, Sigma^>);
+    precision 'fp64' or 'fp64_int8'."""
     dev = require_device()
     Xd, Dd = to_device(X, dev), to_device(D, dev)
     eps_h = _eps_host(eps)
@@ -230,7 +256,8 @@ def sigma_backward(branch_bar, X, D, eps, nocc, tau_points, states, mu, Wt):
     err = _Err(dev)
     check(lib().mbpt_sigma_backward(ptr(Xd), M, norb, nocc, ptr(ed), float(mu), ptr(Dd), naux,
                                     tp, len(tau_h), ptr(Wc), ptr(st), S, ptr(sl), ptr(sg),
-                                    ptr(eps_bar), ptr(X_bar), ptr(D_bar), ptr(Wt_bar),
+                                    _mode(precision), ptr(eps_bar), ptr(X_bar), ptr(D_bar),
+                                    ptr(Wt_bar),
                                     ptr(ws), ws.numel(), ptr(err.t), stream_ptr()),
           'mbpt_sigma_backward')
     err.check('mbpt_sigma_backward')
@@ -258,13 +285,15 @@ def selfenergy_diag_backward(a_re, a_im, X, D, eps, nocc, grid, states, transfor
     _one_rank(comm, 'selfenergy_diag_backward')
     Ctw, C, S = transforms
     proj, Wt = cache[0], cache[1]
+    precision = _adjoint_precision(None, grid.cosft_wt, *transforms)
     eps_h = _eps_host(eps)
     bb = _branch_bar(a_re, a_im, C, S)
     e1, x1, d1, Wt_bar = sigma_backward(bb, X, D, eps_h, nocc, grid.tau_points,
-                                        np.atleast_1d(states), mu, Wt)
+                                        np.atleast_1d(states), mu, Wt, precision)
     proj_bar = screened_interaction_tau_backward(Wt_bar, to_device(proj, Wt_bar.device), grid,
-                                                 Ctw)
-    e2, x2, d2 = chi0_backward(proj_bar, X, D, eps_h, nocc, grid.tau_points, mu)
+                                                 Ctw, precision=precision)
+    e2, x2, d2 = chi0_backward(proj_bar, X, D, eps_h, nocc, grid.tau_points, mu,
+                               precision=precision)
     out = (e1 + e2, x1 + x2, d1 + d2)
     return tuple(_back(t, X) for t in out)
 

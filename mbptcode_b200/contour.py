@@ -46,7 +46,7 @@ from collections import OrderedDict
 import numpy as np
 import torch
 
-from ._lib import WORKSPACE, check, lib, ptr, require_device, stream_ptr
+from ._lib import MODES, WORKSPACE, check, lib, ptr, require_device, stream_ptr
 from .grids import TimeFrequencyGrid, gauss_legendre_grid, particle_hole_window
 from .space_time import (_eps_host, chi0_aux, chi0_sweep, dyson_batch, frequency_factor,
                          to_device, transform)
@@ -1563,8 +1563,9 @@ def qp_gradient_space_time(X, D, eps, nocc, grid, nu_points, nu_weights, p, *,
                                           ws.numel(), stream_ptr()),
           'mbpt_cd_integral_backward')
     wsd = WORKSPACE.get(lib().mbpt_dyson_backward_workspace_bytes(naux), dev)
-    check(lib().mbpt_dyson_backward(ptr(wmi), ptr(W_bar), naux, wmi.shape[0], ptr(wsd),
-                                    wsd.numel(), stream_ptr()), 'mbpt_dyson_backward')
+    check(lib().mbpt_dyson_backward(ptr(wmi), ptr(W_bar), naux, wmi.shape[0], MODES['fp64'],
+                                    ptr(wsd), wsd.numel(), stream_ptr()),
+          'mbpt_dyson_backward')
     cw_t = np.ascontiguousarray(np.asarray(grid.cosft_wt, float).T)   # (ntau, nfreq)
     proj_bar = torch.zeros_like(proj)
     for k0 in range(0, cw_t.shape[1], _MAX_J):

@@ -78,7 +78,7 @@ void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 namespace {
 
-constexpr int kAbiVersion = 1;
+constexpr int kAbiVersion = 2;
 
 struct Handles {
   cublasHandle_t blas = nullptr;
@@ -110,13 +110,20 @@ inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // The FP64 products of the reverse sweeps and of the rows beside the route
 // (the adjoints, the AO self-energy, the contour's FP64 pieces) run on the
-// int8 tensor cores by the Ozaki scheme (8 digits: FP64 level) when
-// MBPT_FP64_GEMM=ozaki, else as cuBLAS DGEMMs. The forward sweep's plain FP64
-// mode keeps native FP64 products either way. Read at every call.
+// int8 tensor cores by the Ozaki scheme (8 digits: FP64 level) unless
+// MBPT_FP64_GEMM=cublas, which keeps cuBLAS DGEMMs. The forward sweeps' plain
+// FP64 mode keeps native FP64 products; MBPT_MODE_FP64_INT8 puts them on the
+// Ozaki product too. Read at every call.
 bool ozaki_fp64_enabled() {
   const char *e = std::getenv("MBPT_FP64_GEMM");
-  return e && std::strcmp(e, "ozaki") == 0;
+  return !(e && std::strcmp(e, "cublas") == 0);
 }
+
+inline bool valid_mode(int m) {
+  return m == MBPT_MODE_FP64 || m == MBPT_MODE_MIXED || m == MBPT_MODE_FP64_INT8;
+}
+// FP64-accurate modes: native FP64 products or the Ozaki emulation of them
+inline bool fp64_mode(int m) { return m != MBPT_MODE_MIXED; }
 
 // Grow-only scratch of the Ozaki GEMM, one per (device, stream): concurrent
 // streams never share one. Growing waits for the stream's earlier work.
@@ -148,18 +155,38 @@ void *ozaki_scratch(cudaStream_t st, size_t bytes) {
   return p;
 }
 
-bool gemm_f64(cublasHandle_t h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
-              double alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
-              double beta, double *C, int64_t ldc) {
-  if (!ozaki_fp64_enabled())
-    return dgemm_rm(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+bool gemm_ozaki(cublasHandle_t h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
+                double alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
+                double beta, double *C, int64_t ldc, const OzakiEpi *epi = nullptr) {
   cudaStream_t st = nullptr;
   if (cublasGetStream(h, &st) != CUBLAS_STATUS_SUCCESS) return false;
   const size_t bytes = ozaki_gemm_scratch_bytes(m, n, k, 8);
   void *ws = ozaki_scratch(st, bytes);
   if (!ws) return false;
   return ozaki_dgemm(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, 8, ws, bytes,
-                     nullptr, st) == MBPT_OK;
+                     nullptr, st, epi) == MBPT_OK;
+}
+
+bool gemm_f64(cublasHandle_t h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
+              double alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
+              double beta, double *C, int64_t ldc) {
+  if (!ozaki_fp64_enabled())
+    return dgemm_rm(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  return gemm_ozaki(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+}
+
+// the forward sweeps' FP64 products: native in MBPT_MODE_FP64, on the Ozaki
+// product in MBPT_MODE_FP64_INT8; `sym`: the n x n product is symmetric, and
+// the Ozaki product forms its upper tiles only (the native one forms all)
+bool gemm_mode(int mode, cublasHandle_t h, bool ta, bool tb, int64_t m, int64_t n, int64_t k,
+               double alpha, const double *A, int64_t lda, const double *B, int64_t ldb,
+               double beta, double *C, int64_t ldc, bool sym = false) {
+  if (mode == MBPT_MODE_FP64_INT8) {
+    OzakiEpi e;
+    e.sym = sym;
+    return gemm_ozaki(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, &e);
+  }
+  return dgemm_rm(h, ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
 }
 
 double *copy_weights(Arena &ar, const double *host, size_t count, cudaStream_t st) {
@@ -195,7 +222,7 @@ struct Chi0Bufs {
 Chi0Bufs carve_chi0(Arena &ar, const Dims &d, int ntau, int nfreq, int mode, bool own_proj) {
   Chi0Bufs b{};
   b.w = ar.take<double>(static_cast<size_t>(nfreq) * ntau);
-  if (mode == MBPT_MODE_FP64) {
+  if (fp64_mode(mode)) {
     b.Xo_s = ar.take<double>(d.M * d.nocc);
     b.Xv_s = ar.take<double>(d.M * d.nv);
     b.Go = ar.take<double>(d.M * d.M);
@@ -226,22 +253,22 @@ int chi0_run(const double *X, const Dims &d, const double *eps, double mu, const
   if (ar.overflow()) return MBPT_ERR_WORKSPACE;
   cudaMemcpyAsync(b.w, cw, sizeof(double) * nfreq * ntau, cudaMemcpyHostToDevice, st);
   const int64_t a2 = d.naux * d.naux;
-  if (mode == MBPT_MODE_FP64) {
+  if (fp64_mode(mode)) {
     double *proj = proj_out ? proj_out : b.proj;
     cublasHandle_t h = handles(st).blas;
     for (int k = 0; k < ntau; ++k) {
       launch_scaled_branches(X, d.M, d.n, d.nocc, eps, mu, tau[k], 1.0, b.Xo_s, b.Xv_s, st);
       // G_occ = (X_o e^{e_o tau}) X_o^T, G_virt likewise (MBPTcode space_time.py:525-526)
-      if (!dgemm_rm(h, false, true, d.M, d.M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0, b.Go,
-                    d.M) ||
-          !dgemm_rm(h, false, true, d.M, d.M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n, 0.0,
-                    b.Gv, d.M))
+      if (!gemm_mode(mode, h, false, true, d.M, d.M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0,
+                     b.Go, d.M) ||
+          !gemm_mode(mode, h, false, true, d.M, d.M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n,
+                     0.0, b.Gv, d.M))
         return MBPT_ERR_CUDA;
       launch_hadamard(b.Go, b.Gv, d.M * d.M, st);
-      if (!dgemm_rm(h, false, false, d.M, d.naux, d.M, 1.0, b.Go, d.M, D, d.naux, 0.0, b.Y,
-                    d.naux) ||
-          !dgemm_rm(h, true, false, d.naux, d.naux, d.M, -2.0, D, d.naux, b.Y, d.naux, 0.0,
-                    proj + k * a2, d.naux))
+      if (!gemm_mode(mode, h, false, false, d.M, d.naux, d.M, 1.0, b.Go, d.M, D, d.naux, 0.0,
+                     b.Y, d.naux) ||
+          !gemm_mode(mode, h, true, false, d.naux, d.naux, d.M, -2.0, D, d.naux, b.Y, d.naux,
+                     0.0, proj + k * a2, d.naux, true))
         return MBPT_ERR_CUDA;
     }
     launch_transform<double>(proj, a2, d.naux, d.naux, d.naux, b.w, nfreq, ntau, chi0, a2,
@@ -582,7 +609,7 @@ int chol_batched(double *A, int64_t n, int nmat, int *info, double *P, double *L
 // same setting.
 int ozaki_slices(int mode) {
   const char *e = std::getenv("MBPT_DYSON_OZAKI");
-  const bool on = e ? std::atoi(e) != 0 : mode == MBPT_MODE_MIXED;
+  const bool on = e ? std::atoi(e) != 0 : mode != MBPT_MODE_FP64;
   if (!on) return 0;
   const char *k = std::getenv("MBPT_DYSON_OZAKI_SLICES");
   const int v = k ? std::atoi(k) : (mode == MBPT_MODE_MIXED ? 7 : 8);
@@ -1008,7 +1035,7 @@ int64_t pad_states(int nstates) { return round_up(nstates, 128); }
 
 SigmaBufs carve_sigma(Arena &ar, const Dims &d, int ntau, int nstates, int mode) {
   SigmaBufs b{};
-  if (mode == MBPT_MODE_FP64) {
+  if (fp64_mode(mode)) {
     b.U = ar.take<double>(d.M * d.naux);
     b.Zt = ar.take<double>(d.M * d.M);
     b.G = ar.take<double>(d.M * d.M);
@@ -1047,35 +1074,35 @@ int sigma_run(const double *X, const Dims &d, const double *eps, double mu, cons
   if (ar.overflow()) return MBPT_ERR_WORKSPACE;
   const int64_t a2 = d.naux * d.naux;
   const int64_t S = nstates;
-  if (mode == MBPT_MODE_FP64) {
+  if (fp64_mode(mode)) {
     cublasHandle_t h = handles(st).blas;
     launch_gather_cols_f64(X, d.M, d.n, states, S, b.Xs, st);
     for (int k = 0; k < ntau; ++k) {
       // Zt = D Wt D^T (MBPTcode imaginary_time.py:508, :513); Wt = I without Wt
-      if (Wt && !dgemm_rm(h, false, false, d.M, d.naux, d.naux, 1.0, D, d.naux, Wt + k * a2,
-                          d.naux, 0.0, b.U, d.naux))
+      if (Wt && !gemm_mode(mode, h, false, false, d.M, d.naux, d.naux, 1.0, D, d.naux,
+                           Wt + k * a2, d.naux, 0.0, b.U, d.naux))
         return MBPT_ERR_CUDA;
-      if ((Wt || k == 0) && !dgemm_rm(h, false, true, d.M, d.M, d.naux, 1.0, Wt ? b.U : D,
-                                      d.naux, D, d.naux, 0.0, b.Zt, d.M))
+      if ((Wt || k == 0) && !gemm_mode(mode, h, false, true, d.M, d.M, d.naux, 1.0,
+                                       Wt ? b.U : D, d.naux, D, d.naux, 0.0, b.Zt, d.M, true))
         return MBPT_ERR_CUDA;
       launch_scaled_branches(X, d.M, d.n, d.nocc, eps, mu, tau[k], 1.0, b.Xo_s, b.Xv_s, st);
       double *out_l = branch + static_cast<int64_t>(k) * S;
       double *out_g = branch + static_cast<int64_t>(ntau + k) * S;
       // lesser branch: G_occ o Zt contracted with X_s on both sides
-      if (!dgemm_rm(h, false, true, d.M, d.M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0, b.G,
-                    d.M))
+      if (!gemm_mode(mode, h, false, true, d.M, d.M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0,
+                     b.G, d.M))
         return MBPT_ERR_CUDA;
       launch_hadamard(b.G, b.Zt, d.M * d.M, st);
-      if (!dgemm_rm(h, false, false, d.M, S, d.M, 1.0, b.G, d.M, b.Xs, S, 0.0, b.R, S))
+      if (!gemm_mode(mode, h, false, false, d.M, S, d.M, 1.0, b.G, d.M, b.Xs, S, 0.0, b.R, S))
         return MBPT_ERR_CUDA;
       cudaMemsetAsync(out_l, 0, sizeof(double) * S, st);
       launch_rowdot(b.R, S, b.Xs, S, d.M, S, 1.0, out_l, st);
       // greater branch, with its minus sign
-      if (!dgemm_rm(h, false, true, d.M, d.M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n, 0.0,
-                    b.G, d.M))
+      if (!gemm_mode(mode, h, false, true, d.M, d.M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n,
+                     0.0, b.G, d.M))
         return MBPT_ERR_CUDA;
       launch_hadamard(b.G, b.Zt, d.M * d.M, st);
-      if (!dgemm_rm(h, false, false, d.M, S, d.M, 1.0, b.G, d.M, b.Xs, S, 0.0, b.R, S))
+      if (!gemm_mode(mode, h, false, false, d.M, S, d.M, 1.0, b.G, d.M, b.Xs, S, 0.0, b.R, S))
         return MBPT_ERR_CUDA;
       cudaMemsetAsync(out_g, 0, sizeof(double) * S, st);
       launch_rowdot(b.R, S, b.Xs, S, d.M, S, -1.0, out_g, st);
@@ -1159,7 +1186,7 @@ BackBufs carve_back(Arena &ar, const Dims &d) {
 
 int back_run(const double *pbar, const double *X, const Dims &d, const double *eps, double mu,
              const double *D, const double *tau, int ntau, double *eps_bar, double *X_bar,
-             double *D_bar, Arena &ar, cudaStream_t st) {
+             double *D_bar, Arena &ar, cudaStream_t st, int mode) {
   BackBufs b = carve_back(ar, d);
   if (ar.overflow()) return MBPT_ERR_WORKSPACE;
   cublasHandle_t h = handles(st).blas;
@@ -1170,28 +1197,44 @@ int back_run(const double *pbar, const double *X, const Dims &d, const double *e
   for (int k = 0; k < ntau; ++k) {
     // MBPTcode gradients/rpa/space_time_adjoint.py:196-217, one row tile
     launch_sym_half(pbar + k * a2, b.pb, d.naux, st);
-    if (!gemm_f64(h, false, false, d.M, d.naux, d.naux, -2.0, D, d.naux, b.pb, d.naux, 0.0,
+    if (!gemm_mode(mode, h, false, false, d.M, d.naux, d.naux, -2.0, D, d.naux, b.pb, d.naux, 0.0,
                   b.E, d.naux))
       return MBPT_ERR_CUDA;
     launch_scaled_branches(X, d.M, d.n, d.nocc, eps, mu, tau[k], 1.0, b.Xo_s, b.Xv_s, st);
-    if (!gemm_f64(h, false, true, d.M, d.M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0, b.Go,
+    if (!gemm_mode(mode, h, false, true, d.M, d.M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0, b.Go,
                   d.M) ||
-        !gemm_f64(h, false, true, d.M, d.M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n, 0.0,
+        !gemm_mode(mode, h, false, true, d.M, d.M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n, 0.0,
                   b.Gv, d.M))
       return MBPT_ERR_CUDA;
     launch_hadamard3(b.P, b.Go, b.Gv, d.M * d.M, st);  // Pi
-    if (!gemm_f64(h, false, false, d.M, d.naux, d.M, 2.0, b.P, d.M, b.E, d.naux, 1.0, D_bar,
-                  d.naux) ||
-        !gemm_f64(h, false, true, d.M, d.M, d.naux, 1.0, b.E, d.naux, D, d.naux, 0.0, b.P,
-                  d.M))  // Pi_bar
+    if (!gemm_mode(mode, h, false, false, d.M, d.naux, d.M, 2.0, b.P, d.M, b.E, d.naux, 1.0, D_bar,
+                  d.naux))
       return MBPT_ERR_CUDA;
-    launch_hadamard3(b.T, b.P, b.Gv, d.M * d.M, st);  // Go_bar
-    if (!gemm_f64(h, false, false, d.M, d.nocc, d.M, 1.0, b.T, d.M, X, d.n, 0.0, b.GoX,
-                  d.nocc))
-      return MBPT_ERR_CUDA;
-    launch_hadamard3(b.T, b.P, b.Go, d.M * d.M, st);  // Gv_bar
-    if (!gemm_f64(h, false, false, d.M, d.nv, d.M, 1.0, b.T, d.M, X + d.nocc, d.n, 0.0, b.GvX,
-                  d.nv))
+    // Pi_bar = E D^T (symmetric) and the G branches' adjoints Go_bar =
+    // Pi_bar o Gv, Gv_bar = Pi_bar o Go: on the Ozaki product both straight
+    // from its epilogue (Pi_bar never stored), else through Pi_bar
+    double *go_bar = b.P, *gv_bar = b.T;
+    if (mode == MBPT_MODE_FP64_INT8 && d.naux <= kOzakiKChunk) {
+      OzakiEpi e;
+      e.sym = true;
+      e.h1 = b.Gv;
+      e.h2 = b.Go;
+      e.c2 = gv_bar;
+      if (!gemm_ozaki(h, false, true, d.M, d.M, d.naux, 1.0, b.E, d.naux, D, d.naux, 0.0,
+                      go_bar, d.M, &e))
+        return MBPT_ERR_CUDA;
+    } else {
+      if (!dgemm_rm(h, false, true, d.M, d.M, d.naux, 1.0, b.E, d.naux, D, d.naux, 0.0, b.P,
+                    d.M))
+        return MBPT_ERR_CUDA;
+      launch_hadamard3(gv_bar, b.P, b.Go, d.M * d.M, st);
+      go_bar = b.Go;  // G_occ is not read again at this tau point
+      launch_hadamard3(go_bar, b.P, b.Gv, d.M * d.M, st);
+    }
+    if (!gemm_mode(mode, h, false, false, d.M, d.nocc, d.M, 1.0, go_bar, d.M, X, d.n, 0.0, b.GoX,
+                  d.nocc) ||
+        !gemm_mode(mode, h, false, false, d.M, d.nv, d.M, 1.0, gv_bar, d.M, X + d.nocc, d.n, 0.0,
+                  b.GvX, d.nv))
       return MBPT_ERR_CUDA;
     launch_xbar_update(b.GoX, b.GvX, X, d.M, d.n, d.nocc, eps, mu, tau[k], X_bar, eps_bar, st);
   }
@@ -1231,7 +1274,7 @@ int sigma_back_run(const double *X, const Dims &d, const double *eps, double mu,
                    const double *D, const double *tau, int ntau, const double *Wt,
                    const int64_t *states, int64_t S, const double *sl_bar,
                    const double *sg_bar, double *eps_bar, double *X_bar, double *D_bar,
-                   double *Wt_bar, Arena &ar, cudaStream_t st) {
+                   double *Wt_bar, Arena &ar, cudaStream_t st, int mode) {
   SigBackBufs b = carve_sigma_back(ar, d, S);
   if (ar.overflow()) return MBPT_ERR_WORKSPACE;
   cublasHandle_t h = handles(st).blas;
@@ -1244,29 +1287,29 @@ int sigma_back_run(const double *X, const Dims &d, const double *eps, double mu,
     launch_scaled_branches(X, M, d.n, d.nocc, eps, mu, tau[k], 1.0, b.Xo_s, b.Xv_s, st);
     launch_sigma_back_gather(X, M, d.n, states, S, sl_bar + k * S, sg_bar + k * S, b.Xs, b.Xl,
                              b.Xg, st);
-    if (!gemm_f64(h, false, true, M, M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0, b.Go, M) ||
-        !gemm_f64(h, false, true, M, M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n, 0.0, b.Gv,
+    if (!gemm_mode(mode, h, false, true, M, M, d.nocc, 1.0, b.Xo_s, d.nocc, X, d.n, 0.0, b.Go, M) ||
+        !gemm_mode(mode, h, false, true, M, M, d.nv, 1.0, b.Xv_s, d.nv, X + d.nocc, d.n, 0.0, b.Gv,
                   M) ||
-        !gemm_f64(h, false, false, M, A, A, 1.0, D, A, Wk, A, 0.0, b.U, A) ||
-        !gemm_f64(h, false, true, M, M, A, 1.0, b.U, A, D, A, 0.0, b.Zt, M) ||
-        !gemm_f64(h, false, true, M, M, S, 1.0, b.Xl, S, b.Xs, S, 0.0, b.Al, M) ||
-        !gemm_f64(h, false, true, M, M, S, 1.0, b.Xg, S, b.Xs, S, 0.0, b.Ag, M))
+        !gemm_mode(mode, h, false, false, M, A, A, 1.0, D, A, Wk, A, 0.0, b.U, A) ||
+        !gemm_mode(mode, h, false, true, M, M, A, 1.0, b.U, A, D, A, 0.0, b.Zt, M, true) ||
+        !gemm_mode(mode, h, false, true, M, M, S, 1.0, b.Xl, S, b.Xs, S, 0.0, b.Al, M) ||
+        !gemm_mode(mode, h, false, true, M, M, S, 1.0, b.Xg, S, b.Xs, S, 0.0, b.Ag, M))
       return MBPT_ERR_CUDA;
     // Go -> L = Go o Zt, Gv -> H = Gv o Zt, Zt -> Zt_bar, Al -> Go_bar, Ag -> Gv_bar
     launch_sigma_back_hadamard(b.Go, b.Gv, b.Zt, b.Al, b.Ag, M * M, st);
-    if (!gemm_f64(h, false, false, M, S, M, 1.0, b.Go, M, b.Xl, S, 0.0, b.T1, S) ||
-        !gemm_f64(h, false, false, M, S, M, -1.0, b.Gv, M, b.Xg, S, 1.0, b.T1, S))
+    if (!gemm_mode(mode, h, false, false, M, S, M, 1.0, b.Go, M, b.Xl, S, 0.0, b.T1, S) ||
+        !gemm_mode(mode, h, false, false, M, S, M, -1.0, b.Gv, M, b.Xg, S, 1.0, b.T1, S))
       return MBPT_ERR_CUDA;
     launch_scatter_cols(b.T1, M, S, states, 2.0, X_bar, d.n, st);
-    if (!gemm_f64(h, false, false, M, d.nocc, M, 1.0, b.Al, M, X, d.n, 0.0, b.GoX, d.nocc) ||
-        !gemm_f64(h, false, false, M, d.nv, M, 1.0, b.Ag, M, X + d.nocc, d.n, 0.0, b.GvX,
+    if (!gemm_mode(mode, h, false, false, M, d.nocc, M, 1.0, b.Al, M, X, d.n, 0.0, b.GoX, d.nocc) ||
+        !gemm_mode(mode, h, false, false, M, d.nv, M, 1.0, b.Ag, M, X + d.nocc, d.n, 0.0, b.GvX,
                   d.nv))
       return MBPT_ERR_CUDA;
     launch_xbar_update(b.GoX, b.GvX, X, M, d.n, d.nocc, eps, mu, tau[k], X_bar, eps_bar, st);
     // U <- Zt_bar D, then Wt_bar = D^T U and D_bar += 2 U Wt (Zt_bar and Wt symmetric)
-    if (!gemm_f64(h, false, false, M, A, M, 1.0, b.Zt, M, D, A, 0.0, b.U, A) ||
-        !gemm_f64(h, true, false, A, A, M, 1.0, D, A, b.U, A, 0.0, Wt_bar + k * a2, A) ||
-        !gemm_f64(h, false, false, M, A, A, 2.0, b.U, A, Wk, A, 1.0, D_bar, A))
+    if (!gemm_mode(mode, h, false, false, M, A, M, 1.0, b.Zt, M, D, A, 0.0, b.U, A) ||
+        !gemm_mode(mode, h, true, false, A, A, M, 1.0, D, A, b.U, A, 0.0, Wt_bar + k * a2, A) ||
+        !gemm_mode(mode, h, false, false, M, A, A, 2.0, b.U, A, Wk, A, 1.0, D_bar, A))
       return MBPT_ERR_CUDA;
   }
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
@@ -1276,7 +1319,7 @@ int sigma_back_run(const double *X, const Dims &d, const double *eps, double mu,
 // the reverse of the Dyson step W = [1 - chi0]^-1 (W symmetric), as MBPTcode
 // gradients/rpa/space_time_adjoint.py:679-685
 int dyson_back_run(const double *wmi, double *wbar, int64_t n, int nfreq, Arena &ar,
-                   cudaStream_t st) {
+                   cudaStream_t st, int mode) {
   double *T = ar.take<double>(n * n);
   if (ar.overflow()) return MBPT_ERR_WORKSPACE;
   cublasHandle_t h = handles(st).blas;
@@ -1286,9 +1329,9 @@ int dyson_back_run(const double *wmi, double *wbar, int64_t n, int nfreq, Arena 
     double *B = wbar + f * n * n;
     // T = B + Wm B; B <- T + T Wm
     if (cudaMemcpyAsync(T, B, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
-        !gemm_f64(h, false, false, n, n, n, 1.0, Wm, n, B, n, 1.0, T, n) ||
+        !gemm_mode(mode, h, false, false, n, n, n, 1.0, Wm, n, B, n, 1.0, T, n) ||
         cudaMemcpyAsync(B, T, bytes, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
-        !gemm_f64(h, false, false, n, n, n, 1.0, T, n, Wm, n, 1.0, B, n))
+        !gemm_mode(mode, h, false, false, n, n, n, 1.0, T, n, Wm, n, 1.0, B, n))
       return MBPT_ERR_CUDA;
   }
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
@@ -1378,7 +1421,7 @@ int mbpt_chi0_sweep(const double *X, int64_t M, int64_t norb, int64_t nocc, cons
                     void *ws, size_t ws_bytes, int *err, void *stream) {
   Dims d(M, norb, nocc, naux);
   if (!d.ok() || ntau < 1 || nfreq < 1 || ntau > 34 || nfreq > 34) return MBPT_ERR_SHAPE;
-  if (mode != MBPT_MODE_FP64 && mode != MBPT_MODE_MIXED) return MBPT_ERR_UNSUPPORTED;
+  if (!valid_mode(mode)) return MBPT_ERR_UNSUPPORTED;
   Arena ar = arena(ws, ws_bytes);
   return chi0_run(X, d, eps, mu, D, tau, ntau, cw, nfreq, mode, chi0, proj, ar, err, S(stream));
 }
@@ -1394,7 +1437,7 @@ int mbpt_dyson(double *chi0, int64_t naux, int nfreq, int want_w, int mode, doub
                double *trace, int *info_host, int *sign_host, void *ws, size_t ws_bytes,
                int *err, void *stream) {
   if (naux < 1 || nfreq < 1) return MBPT_ERR_SHAPE;
-  if (mode != MBPT_MODE_FP64 && mode != MBPT_MODE_MIXED) return MBPT_ERR_UNSUPPORTED;
+  if (!valid_mode(mode)) return MBPT_ERR_UNSUPPORTED;
   Arena ar = arena(ws, ws_bytes);
   return dyson_run(chi0, naux, nfreq, want_w, logdet, trace, info_host, sign_host, ar,
                    S(stream), mode, err);
@@ -1404,7 +1447,7 @@ int mbpt_dyson_deferred(double *chi0, int64_t naux, int nfreq, int want_w, int m
                         double *logdet, double *trace, int *info_dev, void *ws, size_t ws_bytes,
                         int *err, void *stream) {
   if (naux < 1 || nfreq < 1 || !info_dev) return MBPT_ERR_SHAPE;
-  if (mode != MBPT_MODE_FP64 && mode != MBPT_MODE_MIXED) return MBPT_ERR_UNSUPPORTED;
+  if (!valid_mode(mode)) return MBPT_ERR_UNSUPPORTED;
   Arena ar = arena(ws, ws_bytes);
   return dyson_run(chi0, naux, nfreq, want_w, logdet, trace, nullptr, nullptr, ar, S(stream),
                    mode, err, info_dev);
@@ -1483,7 +1526,7 @@ int mbpt_sigma_branch_sums(const double *X, int64_t M, int64_t norb, int64_t noc
                            void *ws, size_t ws_bytes, int *err, void *stream) {
   Dims d(M, norb, nocc, naux);
   if (!d.ok() || ntau < 1 || nstates < 1) return MBPT_ERR_SHAPE;
-  if (mode != MBPT_MODE_FP64 && mode != MBPT_MODE_MIXED) return MBPT_ERR_UNSUPPORTED;
+  if (!valid_mode(mode)) return MBPT_ERR_UNSUPPORTED;
   Arena ar = arena(ws, ws_bytes);
   return sigma_run(X, d, eps, mu, D, Wt, tau, ntau, states, nstates, mode, branch, ar, err,
                    S(stream));
@@ -1543,9 +1586,10 @@ int mbpt_chi0_backward(const double *pbar, const double *X, int64_t M, int64_t n
   (void)err;
   Dims d(M, norb, nocc, naux);
   if (!d.ok() || ntau < 1) return MBPT_ERR_SHAPE;
-  if (mode != MBPT_MODE_FP64) return MBPT_ERR_UNSUPPORTED;
+  if (!fp64_mode(mode)) return MBPT_ERR_UNSUPPORTED;
   Arena ar = arena(ws, ws_bytes);
-  return back_run(pbar, X, d, eps, mu, D, tau, ntau, eps_bar, X_bar, D_bar, ar, S(stream));
+  return back_run(pbar, X, d, eps, mu, D, tau, ntau, eps_bar, X_bar, D_bar, ar, S(stream),
+                  mode);
 }
 
 size_t mbpt_sigma_ao_workspace_bytes(int64_t M, int64_t nao, int64_t norb, int64_t nocc,
@@ -1630,9 +1674,10 @@ int mbpt_three_index_slices(const double *X, int64_t M, int64_t norb, const doub
 
 // The explicit particle-hole response chi0 = s (C f) C^T. FP64: columns of C
 // in chunks of kChi0AuxChunk, each chunk scaled into the workspace and folded
-// into the lower triangle by row-panel DGEMMs, the other triangle mirrored. Mixed: C f and C as zero-padded BF16 pairs, one split product
-// over the whole K on the engine's upper 128 x 256 tiles, stored as FP64 and
-// mirrored by its epilogue.
+// into the lower triangle by row-panel DGEMMs, the other triangle mirrored.
+// Mixed: C f and C as zero-padded BF16 pairs, one split product over the
+// whole K on the engine's upper 128 x 256 tiles, stored as FP64 and mirrored
+// by its epilogue.
 constexpr int64_t kChi0AuxChunk = 4096;
 constexpr int64_t kChi0AuxPanel = 1024;
 
@@ -1649,7 +1694,7 @@ int mbpt_chi0_aux(const double *C, int64_t naux, int64_t nov, int64_t ldc, const
                   size_t ws_bytes, int *err, void *stream) {
   if (naux < 1 || nov < 1 || ldc < nov || naux > INT32_MAX || ldc > INT32_MAX)
     return MBPT_ERR_SHAPE;
-  if (mode != MBPT_MODE_FP64 && mode != MBPT_MODE_MIXED) return MBPT_ERR_UNSUPPORTED;
+  if (!valid_mode(mode)) return MBPT_ERR_UNSUPPORTED;
   cudaStream_t st = S(stream);
   Arena ar = arena(ws, ws_bytes);
   if (mode == MBPT_MODE_MIXED) {
@@ -1721,7 +1766,7 @@ struct ContractionBufs {
 
 ContractionBufs carve_contraction(Arena &ar, int64_t naux, int64_t ncols, int mode) {
   ContractionBufs b;
-  if (mode == MBPT_MODE_FP64) {
+  if (fp64_mode(mode)) {
     b.Y = ar.take<double>(naux * ncols);
     return b;
   }
@@ -1747,7 +1792,7 @@ int mbpt_screening_contraction(const double *w_minus_i, int nfreq, int64_t naux,
                                const double *B, int64_t ncols, int mode, double *wc, void *ws,
                                size_t ws_bytes, int *err, void *stream) {
   if (nfreq < 1 || naux < 1 || ncols < 1) return MBPT_ERR_SHAPE;
-  if (mode != MBPT_MODE_FP64 && mode != MBPT_MODE_MIXED) return MBPT_ERR_UNSUPPORTED;
+  if (!valid_mode(mode)) return MBPT_ERR_UNSUPPORTED;
   cudaStream_t st = S(stream);
   Arena ar = arena(ws, ws_bytes);
   ContractionBufs c = carve_contraction(ar, naux, ncols, mode);
@@ -1779,8 +1824,8 @@ int mbpt_screening_contraction(const double *w_minus_i, int nfreq, int64_t naux,
   cublasHandle_t h = handles(st).blas;
   for (int k = 0; k < nfreq; ++k) {
     // wc[k, c] = B[:, c]^T (W - I)_k B[:, c]: GW/contour_deformation.py:229-237, 273-290
-    if (!gemm_f64(h, false, false, naux, ncols, naux, 1.0, w_minus_i + k * naux * naux, naux,
-                  B, ncols, 0.0, Y, ncols))
+    if (!gemm_mode(mode, h, false, false, naux, ncols, naux, 1.0, w_minus_i + k * naux * naux,
+                   naux, B, ncols, 0.0, Y, ncols))
       return MBPT_ERR_CUDA;
     launch_rowdot(Y, ncols, B, ncols, naux, ncols, 1.0, wc + k * ncols, st);
   }
@@ -1854,15 +1899,16 @@ size_t mbpt_sigma_backward_workspace_bytes(int64_t M, int64_t norb, int64_t nocc
 int mbpt_sigma_backward(const double *X, int64_t M, int64_t norb, int64_t nocc,
                         const double *eps, double mu, const double *D, int64_t naux,
                         const double *tau, int ntau, const double *Wt, const int64_t *states,
-                        int nstates, const double *sl_bar, const double *sg_bar,
+                        int nstates, const double *sl_bar, const double *sg_bar, int mode,
                         double *eps_bar, double *X_bar, double *D_bar, double *Wt_bar,
                         void *ws, size_t ws_bytes, int *err, void *stream) {
   (void)err;
   Dims d(M, norb, nocc, naux);
   if (!d.ok() || ntau < 1 || nstates < 1) return MBPT_ERR_SHAPE;
+  if (!fp64_mode(mode)) return MBPT_ERR_UNSUPPORTED;
   Arena ar = arena(ws, ws_bytes);
   return sigma_back_run(X, d, eps, mu, D, tau, ntau, Wt, states, nstates, sl_bar, sg_bar,
-                        eps_bar, X_bar, D_bar, Wt_bar, ar, S(stream));
+                        eps_bar, X_bar, D_bar, Wt_bar, ar, S(stream), mode);
 }
 
 size_t mbpt_dyson_backward_workspace_bytes(int64_t naux) {
@@ -1870,10 +1916,11 @@ size_t mbpt_dyson_backward_workspace_bytes(int64_t naux) {
 }
 
 int mbpt_dyson_backward(const double *w_minus_i, double *wbar, int64_t naux, int nfreq,
-                        void *ws, size_t ws_bytes, void *stream) {
+                        int mode, void *ws, size_t ws_bytes, void *stream) {
   if (naux < 1 || nfreq < 1) return MBPT_ERR_SHAPE;
+  if (!fp64_mode(mode)) return MBPT_ERR_UNSUPPORTED;
   Arena ar = arena(ws, ws_bytes);
-  return dyson_back_run(w_minus_i, wbar, naux, nfreq, ar, S(stream));
+  return dyson_back_run(w_minus_i, wbar, naux, nfreq, ar, S(stream), mode);
 }
 
 int mbpt_energy_adjoint_seed(double *wmi, int64_t naux, int nfreq, const double *ow_dev,

@@ -79,11 +79,23 @@ int ozaki_chol_update(double *A, int64_t n, int nmat, int64_t j0, int nb, double
 // the int8 tensor cores (Ozaki scheme, `slices` digits per operand, 7 or 8):
 // op(A) = A (m x k, lda) or, with ta, A^T of a k x m A; op(B) = B (k x n,
 // ldb) or, with tb, B^T of an n x k B. scratch: ozaki_gemm_scratch_bytes.
+// Options of the epilogue (null: a plain product):
+//   sym: the product is known to be symmetric (m == n): the tiles on and
+//        above the diagonal are formed and mirrored, the others skipped;
+//   h1 (and h2): C = (alpha op(A) op(B)) o h1 and C2 = (alpha op(A) op(B)) o h2,
+//        element-wise, h1, h2 and C2 with C's leading dimension; needs beta
+//        0 and k <= kOzakiKChunk (the product complete in one pass).
+struct OzakiEpi {
+  bool sym = false;
+  const double *h1 = nullptr, *h2 = nullptr;
+  double *c2 = nullptr;
+};
+constexpr int64_t kOzakiKChunk = 32768;
 size_t ozaki_gemm_scratch_bytes(int64_t m, int64_t n, int64_t k, int slices);
 int ozaki_dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
                 const double *A, int64_t lda, const double *B, int64_t ldb, double beta,
                 double *C, int64_t ldc, int slices, void *scratch, size_t scratch_bytes,
-                int *err, cudaStream_t st);
+                int *err, cudaStream_t st, const OzakiEpi *epi = nullptr);
 
 // Bump allocator over a caller's workspace (1024-byte aligned slices).
 struct Arena {

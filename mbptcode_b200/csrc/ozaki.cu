@@ -128,6 +128,9 @@ struct UpdateArgs {
   double alpha, beta;
   int m_rows, n_cols;
   int tiles_m;
+  int sym;             // GEMM: symmetric product, upper tiles formed and mirrored
+  const double *H1, *H2;  // GEMM: element-wise factors of C and C2 (null: none)
+  double *C2;
   int *err;
 };
 
@@ -148,8 +151,10 @@ __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_consta
   const int tm = blockIdx.x / p.tiles_n, tn = blockIdx.x % p.tiles_n;
   const int r0 = tm * BM;       // tile row (Cholesky: matrix row j0 + r0)
   const int c0 = tn * BN;       // tile column
-  // uniform: the second half of a narrow last panel
+  // uniform: the second half of a narrow last panel, a tile below the
+  // diagonal of a symmetric product
   if (EPI == EPI_CHOL && c0 >= p.nb) return;
+  if (EPI == EPI_GEMM && p.sym && c0 + BN <= r0) return;
   const int m = static_cast<int>(p.n - p.j0);
 
   if (threadIdx.x == 0) {
@@ -288,14 +293,32 @@ __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_consta
             }
           }
         } else if (EPI == EPI_GEMM && live) {
-          double *dst = p.C + static_cast<int64_t>(pr) * p.ldc;
+          const int64_t ro = static_cast<int64_t>(pr) * p.ldc;
           const double a = p.alpha * srow;
 #pragma unroll
           for (int i = 0; i < 32; ++i) {
             const int col = c0 + ch * 32 + i;
-            if (col < p.n_cols) {
+            // symmetric: the upper triangle, each entry also at its mirror
+            // (the lanes' rows are consecutive, so the mirrored stores of
+            // one column coalesce)
+            if (col < p.n_cols && (!p.sym || col >= pr)) {
               const double v = a * acc[i] * p.scale_b[col];
-              dst[col] = p.beta == 0.0 ? v : v + p.beta * dst[col];
+              const int64_t mo = static_cast<int64_t>(col) * p.ldc + pr;
+              const bool mirror = p.sym && col > pr;
+              if (p.H1) {
+                const double o1 = v * p.H1[ro + col];
+                p.C[ro + col] = o1;
+                if (mirror) p.C[mo] = o1;
+                if (p.H2) {
+                  const double o2 = v * p.H2[ro + col];
+                  p.C2[ro + col] = o2;
+                  if (mirror) p.C2[mo] = o2;
+                }
+              } else {
+                const double o = p.beta == 0.0 ? v : v + p.beta * p.C[ro + col];
+                p.C[ro + col] = o;
+                if (mirror) p.C[mo] = o;
+              }
             }
           }
         }
@@ -549,7 +572,7 @@ int ozaki_chol_update(double *A, int64_t n, int nmat, int64_t j0, int nb, double
   if (j0 <= 0) return MBPT_OK;
   if (j0 % ozaki::BKB || nb < 1 || nb > 128 || j0 >= 65536) return MBPT_ERR_SHAPE;
   const int64_t npad = round_up(n, 128);
-  ozaki::UpdateArgs p;
+  ozaki::UpdateArgs p{};
   if (!ozaki::make_plane_map(&p.tm_a, planes, npad, static_cast<int64_t>(slices) * nmat,
                              ozaki::BM) ||
       !ozaki::make_plane_map(&p.tm_b, planes, npad, static_cast<int64_t>(slices) * nmat,
@@ -596,7 +619,6 @@ int ozaki_chol_update(double *A, int64_t n, int nmat, int64_t j0, int nb, double
 
 // ---- the general FP64-accurate GEMM ------------------------------------------
 // Largest K of one product pass: S 64^2 K must stay below 2^31 (S <= 8).
-constexpr int64_t kOzakiKChunk = 32768;
 
 size_t ozaki_gemm_scratch_bytes(int64_t m, int64_t n, int64_t k, int slices) {
   const int64_t kc = std::min<int64_t>(round_up(k, 128), kOzakiKChunk);
@@ -607,9 +629,13 @@ size_t ozaki_gemm_scratch_bytes(int64_t m, int64_t n, int64_t k, int slices) {
 int ozaki_dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
                 const double *A, int64_t lda, const double *B, int64_t ldb, double beta,
                 double *C, int64_t ldc, int slices, void *scratch, size_t scratch_bytes,
-                int *err, cudaStream_t st) {
+                int *err, cudaStream_t st, const OzakiEpi *epi) {
   if (m < 1 || n < 1 || k < 1) return MBPT_ERR_SHAPE;
   if (slices != 7 && slices != 8) return MBPT_ERR_SHAPE;
+  const OzakiEpi none;
+  const OzakiEpi &x = epi ? *epi : none;
+  if (x.sym && m != n) return MBPT_ERR_SHAPE;
+  if (x.h1 && (beta != 0.0 || k > kOzakiKChunk || (x.h2 && !x.c2))) return MBPT_ERR_SHAPE;
   if (scratch_bytes < ozaki_gemm_scratch_bytes(m, n, k, slices)) return MBPT_ERR_WORKSPACE;
   const int64_t mp = round_up(m, 128), np = round_up(n, 128);
   static std::atomic<uint64_t> attr8{0}, attr7{0};
@@ -640,7 +666,7 @@ int ozaki_dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
       ozaki::operand_slice_kernel<7><<<ga, 256, 0, st>>>(a0, m, kc, lda, at, sa, pa, mp, kp);
       ozaki::operand_slice_kernel<7><<<gb, 256, 0, st>>>(b0, n, kc, ldb, bt, sb, pb, np, kp);
     }
-    ozaki::UpdateArgs p;
+    ozaki::UpdateArgs p{};
     if (!ozaki::make_operand_map(&p.tm_a, pa, kp, mp, slices, ozaki::BM) ||
         !ozaki::make_operand_map(&p.tm_b, pb, kp, np, slices, ozaki::BN))
       return MBPT_ERR_SHAPE;
@@ -663,6 +689,10 @@ int ozaki_dgemm(bool ta, bool tb, int64_t m, int64_t n, int64_t k, double alpha,
     p.beta = kb == 0 ? beta : 1.0;
     p.m_rows = static_cast<int>(m);
     p.n_cols = static_cast<int>(n);
+    p.sym = x.sym ? 1 : 0;
+    p.H1 = x.h1;
+    p.H2 = x.h1 ? x.h2 : nullptr;
+    p.C2 = x.c2;
     p.err = err;
     const dim3 grid(static_cast<unsigned>(p.tiles_m * p.tiles_n), 1);
     count_launch();

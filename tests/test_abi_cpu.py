@@ -26,7 +26,7 @@ def test_library_exports_every_declared_symbol():
 def test_host_only_queries():
     from mbptcode_b200 import _lib
     lib = _lib.lib()
-    assert lib.mbpt_abi_version() == 1
+    assert lib.mbpt_abi_version() == 2
     assert _lib.status_string(_lib.ERR_NOT_SPD).startswith('1 - chi0')
     assert lib.mbpt_mlp_param_count(64) == 64 * 64 + 7 * 64 + 1
     # workspace queries are pure host arithmetic

@@ -2,7 +2,9 @@
 golden vectors, through the C ABI (via the package's ctypes binding).
 
 Tolerances: FP64 mode agrees with the FP64 oracle to ~1e-10 relative (the
-same arithmetic in another summation order); mixed mode (split-BF16 3-term
+same arithmetic in another summation order), and so does 'fp64_int8' (the
+products emulated on the int8 tensor cores with 8 seven-bit digits, ~5e-15
+of the operands' scale per product); mixed mode (split-BF16 3-term
 products, FP32 accumulation) to 2e-5 relative on chi0-sized quantities."""
 import numpy as np
 import pytest
@@ -58,7 +60,8 @@ def test_split_gemm_matches_fp64(dev, m, n, k, kind, tol):
     assert np.abs(C.cpu().numpy() - ref).max() <= tol * scale
 
 
-@pytest.mark.parametrize('precision,tol', [('fp64', FP64_REL), ('mixed', MIXED_REL)])
+@pytest.mark.parametrize('precision,tol', [('fp64', FP64_REL), ('mixed', MIXED_REL),
+                                           ('fp64_int8', FP64_REL)])
 def test_chi0_matches_reference_golden(golden, precision, tol):
     g = golden('route_calibrated')
     X, D, eps, nocc = g['X'], g['D'], g['eps'], int(g['nocc'])
@@ -67,7 +70,8 @@ def test_chi0_matches_reference_golden(golden, precision, tol):
     assert rel(chi0, g['chi0']) < tol
 
 
-@pytest.mark.parametrize('precision,tol', [('fp64', FP64_REL), ('mixed', MIXED_REL)])
+@pytest.mark.parametrize('precision,tol', [('fp64', FP64_REL), ('mixed', MIXED_REL),
+                                           ('fp64_int8', FP64_REL)])
 def test_shared_kernel_system(golden, precision, tol):
     g = golden('shared_kernel')
     proj = st.polarizability_projected_sweep(g['X'], g['D'], g['eps'], int(g['nocc']),
@@ -157,7 +161,12 @@ def test_mixed_refuses_ill_conditioned_transforms(golden):
 
 @pytest.mark.parametrize('precision,tol,names', [
     ('fp64', 1e-11, ('calibrated', 'calibrated16', 'literal16')),
-    ('mixed', 2e-5, ('calibrated',))])
+    ('mixed', 2e-5, ('calibrated',)),
+    ('fp64_int8', 1e-11, ('calibrated',)),
+    # the int8 emulation's per-product error changes erratically from one tau
+    # point to the next, and the 16-point transforms (weights 2.4e8, 8.9e8)
+    # amplify it to ~1e-9 relative; the adjoints pick native FP64 there
+    ('fp64_int8', 1e-8, ('calibrated16', 'literal16'))])
 def test_rpa_energy_matches_reference_golden(golden, precision, tol, names):
     for name in names:
         g = golden('route_' + name)
@@ -179,14 +188,14 @@ def test_odd_sizes_against_oracle():
                                   rng.uniform(0.1, 3.0, n - nocc)]))
     axes = grids.space_time_axes(eps, nocc, ntau=12)
     ref = orc.chi0_imaginary_frequency(X, D, eps, nocc, axes.grid)
-    for precision, tol in (('fp64', FP64_REL), ('mixed', MIXED_REL)):
+    for precision, tol in (('fp64', FP64_REL), ('mixed', MIXED_REL), ('fp64_int8', FP64_REL)):
         got = st.chi0_imaginary_frequency(X, D, eps, nocc, axes.grid, precision=precision)
         assert rel(got, ref) < tol, precision
     W = np.stack([orc.dyson_screening(c, True) for c in ref])
     Wt = np.tensordot(axes.Ctw, W, axes=(1, 0))
     states = [0, 3, 4, 5, 9, 36]
     br = orc.sigma_branch_sums(X, D, Wt, eps, nocc, axes.tau_sigma, axes.mu, states)
-    for precision, tol in (('fp64', 1e-10), ('mixed', 5e-5)):
+    for precision, tol in (('fp64', 1e-10), ('mixed', 5e-5), ('fp64_int8', 1e-10)):
         got = gw.sigma_branch_sums(X, D, torch.as_tensor(Wt, device='cuda'), eps, nocc,
                                    axes.tau_sigma, states, axes.mu, precision=precision)
         assert rel(got.cpu().numpy(), br) < tol, precision
