@@ -9,6 +9,7 @@ the learned warm start). Nothing here is imported by the package.
     python bench_cases.py transform N
     python bench_cases.py qp-mlp
     python bench_cases.py rows
+    python bench_cases.py ao-sigma
     python bench_cases.py rows-cd
     python bench_cases.py chi0-aux NAUX NOV [--mixed]
     python bench_cases.py fp64-peak N
@@ -209,6 +210,44 @@ def rows(a):
           lambda: contour.sigma_cd(p, eps[p] - 0.05, B[9], eps, nocc, nu, nu_w, wc=wcs[9],
                                    real_screening=contour.LaplaceRealScreening(
                                        proj, cgrid, eps, nocc)))
+
+
+def ao_sigma(a):
+    """The full AO self-energy (self_energy_matrix_imaginary_time) at
+    n_orb = nao = 1200, N_mu = naux = 7200, 24 points, from the mixed sweep's
+    W(i omega): FP64, its int8 emulation and mixed, CUDA events after a
+    warm-up call; the mixed and emulated results against the FP64 one."""
+    import json
+    from mbptcode_b200 import gw
+    n, nocc, M = 1200, 120, 7200
+    X, D, eps_t = synthetic_system_torch(n, nocc, M, seed=2024, variant='calibrated')
+    eps = eps_t.cpu().numpy()
+    axes = grids.space_time_axes(eps, nocc, ntau=24)
+    chi0, _ = chi0_sweep(X, D, eps, nocc, axes.grid.tau_points, axes.grid.cosft_wt,
+                         mu=axes.mu, precision='mixed')
+    dyson_batch(chi0, want_w=True, precision='mixed')
+    chi0.diagonal(dim1=-2, dim2=-1).add_(1.0)          # W
+    g = torch.Generator(device='cpu').manual_seed(5)
+    mo = torch.linalg.qr(torch.randn(n, n, generator=g, dtype=torch.float64))[0].cuda()
+    X_ao = X @ mo.T                                    # X_ao mo = X
+    out = {}
+    for prec in ('fp64', 'fp64_int8', 'mixed'):
+        def run(prec=prec):
+            return gw.self_energy_matrix_imaginary_time(
+                X_ao, D, chi0, mo, eps, nocc, axes.grid.tau_points, axes.grid.omega_points,
+                axes.pade_freq, mu=axes.mu, precision=prec)
+        run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out[prec] = run()
+        e1.record()
+        torch.cuda.synchronize()
+        ref = out['fp64']
+        err = float((out[prec] - ref).abs().max() / ref.abs().max())
+        print(json.dumps({'case': 'ao-sigma', 'precision': prec, 'nao': n, 'naux': M,
+                          'ntau': 24, 's': round(e0.elapsed_time(e1) / 1e3, 4),
+                          'rel_err_vs_fp64': err}), flush=True)
 
 
 def explicit_rows(a):
@@ -624,6 +663,7 @@ def warm_start(a):
 def main(argv=None):
     p = argparse.ArgumentParser(description='measurement cases beside bench.py')
     p.add_argument('case', choices=['tau', 'dyson', 'sweep', 'transform', 'qp-mlp', 'rows',
+                                    'ao-sigma',
                                     'rows-cd', 'chi0-aux', 'fp64-peak', 'adjoint-fd',
                                     'adjoint-time', 'ozaki-gemm', 'warm-start'])
     p.add_argument('size', type=int, nargs='*', default=[])
@@ -662,6 +702,7 @@ def main(argv=None):
     if a.seed is None:
         a.seed = 0 if a.case == 'warm-start' else 2024
     run = {'tau': tau_point, 'dyson': dyson, 'sweep': sweep, 'transform': transform_case,
+           'ao-sigma': ao_sigma,
            'qp-mlp': qp_mlp_case, 'rows': rows, 'rows-cd': explicit_rows,
            'chi0-aux': chi0_aux_case, 'fp64-peak': fp64_peak, 'adjoint-fd': adjoint_fd,
            'adjoint-time': adjoint_time, 'ozaki-gemm': ozaki_gemm_case,

@@ -32,8 +32,8 @@
  *     the emulated product, which also forms the symmetric products' upper
  *     tiles only and the G branches' adjoints straight from its epilogue.
  *     The FP64 products of the rows beside the route that take no mode
- *     (mbpt_sigma_ao, mbpt_three_index_slices and its backward,
- *     mbpt_cd_integral_backward) run on the emulated product;
+ *     (mbpt_three_index_slices and its backward, mbpt_cd_integral_backward,
+ *     the MO collocation of mbpt_sigma_ao) run on the emulated product;
  *     MBPT_FP64_GEMM=cublas in the environment keeps cuBLAS DGEMMs there.
  *   - The emulation's error is ~5e-15 of the operands' scale per product,
  *     about FP64 rounding, but it changes erratically with the inputs where
@@ -291,14 +291,18 @@ int mbpt_sigma_backward(const double *X_dev, int64_t M, int64_t norb, int64_t no
  * G from the MO collocation X_ao mo_coeff (occupied/virtual split at nocc,
  * eps - mu), Zt_k = D Wt_k D^T: GW/imaginary_time.py:403-533
  * (`self_energy_matrix_imaginary_time`, before its tau -> omega fold).
- * out_dev: (2, ntau, nao, nao), lesser branch first. FP64. */
+ * out_dev: (2, ntau, nao, nao), lesser branch first, FP64. mode: FP64 (or
+ * its int8 emulation): DGEMMs and Hadamard passes; MBPT_MODE_MIXED: the
+ * split BF16 products of the self-energy sweep (U = D Wt, one pass forming
+ * G_occ o Zt and G_virt o Zt, X_ao^T H X_ao as two products, the last one
+ * stored in FP64 by its epilogue), ~1e-5 relative. */
 size_t mbpt_sigma_ao_workspace_bytes(int64_t M, int64_t nao, int64_t norb, int64_t nocc,
-                                     int64_t naux);
+                                     int64_t naux, int mode);
 int mbpt_sigma_ao(const double *X_ao_dev, int64_t M, int64_t nao, const double *mo_coeff_dev,
                   int64_t norb, int64_t nocc, const double *eps_dev, double mu,
                   const double *D_dev, int64_t naux, const double *Wt_dev,
-                  const double *tau_host, int ntau, double *out_dev, void *workspace,
-                  size_t ws_bytes, int *err_dev, void *stream);
+                  const double *tau_host, int ntau, int mode, double *out_dev,
+                  void *workspace, size_t ws_bytes, int *err_dev, void *stream);
 
 /* ---- contour deformation (GW/contour_deformation.py), FP64 ----------------
  * Three-index slices B_s = D^T diag(X[:, p_s]) X of the states p_s

@@ -57,9 +57,9 @@ _SIGNATURES = {
     'mbpt_sigma_backward_workspace_bytes': (_sz, [_i64, _i64, _i64, _i64, _i]),
     'mbpt_sigma_backward': (_i, [_p, _i64, _i64, _i64, _p, _d, _p, _i64, _p, _i, _p, _p, _i,
                                  _p, _p, _i, _p, _p, _p, _p, _p, _sz, _p, _p]),
-    'mbpt_sigma_ao_workspace_bytes': (_sz, [_i64, _i64, _i64, _i64, _i64]),
-    'mbpt_sigma_ao': (_i, [_p, _i64, _i64, _p, _i64, _i64, _p, _d, _p, _i64, _p, _p, _i, _p,
-                           _p, _sz, _p, _p]),
+    'mbpt_sigma_ao_workspace_bytes': (_sz, [_i64, _i64, _i64, _i64, _i64, _i]),
+    'mbpt_sigma_ao': (_i, [_p, _i64, _i64, _p, _i64, _i64, _p, _d, _p, _i64, _p, _p, _i, _i,
+                           _p, _p, _sz, _p, _p]),
     'mbpt_three_index_slices_workspace_bytes': (_sz, [_i64, _i64]),
     'mbpt_three_index_slices': (_i, [_p, _i64, _i64, _p, _i64, _p, _i, _p, _p, _sz, _p]),
     'mbpt_chol_solve': (_i, [_p, _i64, _p, _i, _p]),

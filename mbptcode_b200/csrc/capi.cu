@@ -1592,57 +1592,147 @@ int mbpt_chi0_backward(const double *pbar, const double *X, int64_t M, int64_t n
                   mode);
 }
 
-size_t mbpt_sigma_ao_workspace_bytes(int64_t M, int64_t nao, int64_t norb, int64_t nocc,
-                                     int64_t naux) {
-  Arena ar;
-  ar.counting = true;
-  ar.take<double>(M * norb);                 // X_mo
-  ar.take<double>(M * norb);                 // the scaled branches
-  for (int i = 0; i < 3; ++i) ar.take<double>(M * M);
-  ar.take<double>(M * naux);
-  ar.take<double>(M * nao);
-  (void)nocc;
-  return ar.used + 2048;
+// The full AO self-energy's scratch. FP64 modes: X_mo, the scaled branches,
+// G_occ, G_virt, Zt, U = D W(tau) and R; mixed: X_mo and the split (BF16
+// pair) operands of the engine's products.
+struct SigmaAoBufs {
+  double *Xmo = nullptr, *Xs = nullptr, *Go = nullptr, *Gv = nullptr, *Zt = nullptr,
+         *U = nullptr, *R = nullptr;
+  bf16 *D_hi, *D_lo, *W_hi, *W_lo, *U_hi, *U_lo, *Yo_hi, *Yo_lo, *Yv_hi, *Yv_lo, *Hl_hi,
+      *Hl_lo, *Hg_hi, *Hg_lo, *XaT_hi, *XaT_lo, *RT_hi, *RT_lo;
+};
+
+SigmaAoBufs carve_sigma_ao(Arena &ar, const Dims &d, int64_t nao, int mode) {
+  SigmaAoBufs b{};
+  const int64_t M = d.M;
+  b.Xmo = ar.take<double>(M * d.n);
+  if (fp64_mode(mode)) {
+    b.Xs = ar.take<double>(M * d.n);
+    b.Go = ar.take<double>(M * M);
+    b.Gv = ar.take<double>(M * M);
+    b.Zt = ar.take<double>(M * M);
+    b.U = ar.take<double>(M * d.naux);
+    b.R = ar.take<double>(M * nao);
+    return b;
+  }
+  const int64_t naop = round_up(nao, 128);
+  for (bf16 **q : {&b.D_hi, &b.D_lo, &b.U_hi, &b.U_lo}) *q = ar.take<bf16>(d.Mp * d.Ap);
+  for (bf16 **q : {&b.W_hi, &b.W_lo}) *q = ar.take<bf16>(d.Ap * d.Ap);
+  for (bf16 **q : {&b.Yo_hi, &b.Yo_lo}) *q = ar.take<bf16>(d.Mp * d.Ko);
+  for (bf16 **q : {&b.Yv_hi, &b.Yv_lo}) *q = ar.take<bf16>(d.Mp * d.Kv);
+  for (bf16 **q : {&b.Hl_hi, &b.Hl_lo, &b.Hg_hi, &b.Hg_lo}) *q = ar.take<bf16>(d.Mp * d.Mp);
+  for (bf16 **q : {&b.XaT_hi, &b.XaT_lo, &b.RT_hi, &b.RT_lo}) *q = ar.take<bf16>(naop * d.Mp);
+  return b;
 }
 
+size_t mbpt_sigma_ao_workspace_bytes(int64_t M, int64_t nao, int64_t norb, int64_t nocc,
+                                     int64_t naux, int mode) {
+  Dims d(M, norb, nocc, naux);
+  if (!d.ok() || nao < 1 || !valid_mode(mode)) return SIZE_MAX;
+  Arena ar;
+  ar.counting = true;
+  carve_sigma_ao(ar, d, nao, mode);
+  return ar.used + 4096;
+}
+
+// Sigma^<(tau) = X_ao^T (G_occ o Zt) X_ao and Sigma^>(tau) = -X_ao^T (G_virt o
+// Zt) X_ao per time point (GW/imaginary_time.py:403-533): the occupied/virtual
+// split needs the MO collocation, the outer indices stay AO. FP64 modes:
+// DGEMMs (or their int8 emulation) and Hadamard passes. Mixed: the engine's
+// split products, as the self-energy sweep's: U = D W(tau), then one tile pass
+// of G_occ, G_virt and Zt = U D^T whose epilogue forms H< = G_occ o Zt and
+// H> = G_virt o Zt (upper tiles, mirrored), R^T = X_ao^T H (H symmetric), and
+// X_ao^T R straight into the FP64 output by the symmetric FP64 epilogue.
 int mbpt_sigma_ao(const double *X_ao, int64_t M, int64_t nao, const double *mo_coeff,
                   int64_t norb, int64_t nocc, const double *eps, double mu, const double *D,
-                  int64_t naux, const double *Wt, const double *tau_host, int ntau, double *out,
-                  void *ws, size_t ws_bytes, int *err, void *stream) {
-  (void)err;
+                  int64_t naux, const double *Wt, const double *tau_host, int ntau, int mode,
+                  double *out, void *ws, size_t ws_bytes, int *err, void *stream) {
   Dims d(M, norb, nocc, naux);
   if (!d.ok() || nao < 1 || ntau < 1) return MBPT_ERR_SHAPE;
+  if (!valid_mode(mode)) return MBPT_ERR_UNSUPPORTED;
   cudaStream_t st = S(stream);
   Arena ar = arena(ws, ws_bytes);
-  double *Xmo = ar.take<double>(M * norb);
-  double *Xs = ar.take<double>(M * norb);
-  double *Xo_s = Xs, *Xv_s = Xs + M * nocc;
-  double *Go = ar.take<double>(M * M), *Gv = ar.take<double>(M * M), *Zt = ar.take<double>(M * M);
-  double *U = ar.take<double>(M * naux);
-  double *R = ar.take<double>(M * nao);
+  SigmaAoBufs b = carve_sigma_ao(ar, d, nao, mode);
   if (ar.overflow()) return MBPT_ERR_WORKSPACE;
   cublasHandle_t h = handles(st).blas;
   const int64_t nv = norb - nocc, a2 = naux * naux, o2 = nao * nao;
-  // the occupied/virtual split needs the MO collocation; the outer indices
-  // stay AO (GW/imaginary_time.py:403-533)
-  if (!gemm_f64(h, false, false, M, norb, nao, 1.0, X_ao, nao, mo_coeff, norb, 0.0, Xmo, norb))
+  if (!gemm_f64(h, false, false, M, norb, nao, 1.0, X_ao, nao, mo_coeff, norb, 0.0, b.Xmo,
+                norb))
     return MBPT_ERR_CUDA;
+  if (fp64_mode(mode)) {
+    double *Xo_s = b.Xs, *Xv_s = b.Xs + M * nocc;
+    for (int k = 0; k < ntau; ++k) {
+      launch_scaled_branches(b.Xmo, M, norb, nocc, eps, mu, tau_host[k], 1.0, Xo_s, Xv_s, st);
+      if (!gemm_mode(mode, h, false, true, M, M, nocc, 1.0, Xo_s, nocc, b.Xmo, norb, 0.0, b.Go,
+                     M) ||
+          !gemm_mode(mode, h, false, true, M, M, nv, 1.0, Xv_s, nv, b.Xmo + nocc, norb, 0.0,
+                     b.Gv, M) ||
+          !gemm_mode(mode, h, false, false, M, naux, naux, 1.0, D, naux, Wt + k * a2, naux,
+                     0.0, b.U, naux) ||
+          !gemm_mode(mode, h, false, true, M, M, naux, 1.0, b.U, naux, D, naux, 0.0, b.Zt, M,
+                     true))
+        return MBPT_ERR_CUDA;
+      launch_hadamard(b.Go, b.Zt, M * M, st);
+      launch_hadamard(b.Gv, b.Zt, M * M, st);
+      if (!gemm_mode(mode, h, false, false, M, nao, M, 1.0, b.Go, M, X_ao, nao, 0.0, b.R,
+                     nao) ||
+          !gemm_mode(mode, h, true, false, nao, nao, M, 1.0, X_ao, nao, b.R, nao, 0.0,
+                     out + k * o2, nao, true) ||
+          !gemm_mode(mode, h, false, false, M, nao, M, 1.0, b.Gv, M, X_ao, nao, 0.0, b.R,
+                     nao) ||
+          !gemm_mode(mode, h, true, false, nao, nao, M, -1.0, X_ao, nao, b.R, nao, 0.0,
+                     out + (ntau + k) * o2, nao, true))
+        return MBPT_ERR_CUDA;
+    }
+    return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+  }
+  const int64_t naop = round_up(nao, 128);
+  launch_split_pad<double>(D, M, naux, naux, 1.f, b.D_hi, b.D_lo, d.Ap, d.Mp, d.Ap, false, st);
+  launch_split_pad<double>(X_ao, M, nao, nao, 1.f, b.XaT_hi, b.XaT_lo, d.Mp, d.Mp, naop, true,
+                           st);
+  SplitMat Dm{b.D_hi, b.D_lo, d.Mp, d.Ap, d.Ap}, Wm{b.W_hi, b.W_lo, d.Ap, d.Ap, d.Ap};
+  SplitMat Um{b.U_hi, b.U_lo, d.Mp, d.Ap, d.Ap};
+  SplitMat Yo{b.Yo_hi, b.Yo_lo, d.Mp, d.Ko, d.Ko}, Yv{b.Yv_hi, b.Yv_lo, d.Mp, d.Kv, d.Kv};
+  SplitMat Hl{b.Hl_hi, b.Hl_lo, d.Mp, d.Mp, d.Mp}, Hg{b.Hg_hi, b.Hg_lo, d.Mp, d.Mp, d.Mp};
+  SplitMat XaT{b.XaT_hi, b.XaT_lo, naop, d.Mp, d.Mp}, RT{b.RT_hi, b.RT_lo, naop, d.Mp, d.Mp};
   for (int k = 0; k < ntau; ++k) {
-    launch_scaled_branches(Xmo, M, norb, nocc, eps, mu, tau_host[k], 1.0, Xo_s, Xv_s, st);
-    if (!gemm_f64(h, false, true, M, M, nocc, 1.0, Xo_s, nocc, Xmo, norb, 0.0, Go, M) ||
-        !gemm_f64(h, false, true, M, M, nv, 1.0, Xv_s, nv, Xmo + nocc, norb, 0.0, Gv, M) ||
-        !gemm_f64(h, false, false, M, naux, naux, 1.0, D, naux, Wt + k * a2, naux, 0.0, U, naux) ||
-        !gemm_f64(h, false, true, M, M, naux, 1.0, U, naux, D, naux, 0.0, Zt, M))
-      return MBPT_ERR_CUDA;
-    launch_hadamard(Go, Zt, M * M, st);
-    launch_hadamard(Gv, Zt, M * M, st);
-    // Sigma^<(tau) = X_ao^T (G_occ o Zt) X_ao, Sigma^>(tau) = -X_ao^T (G_virt o Zt) X_ao
-    if (!gemm_f64(h, false, false, M, nao, M, 1.0, Go, M, X_ao, nao, 0.0, R, nao) ||
-        !gemm_f64(h, true, false, nao, nao, M, 1.0, X_ao, nao, R, nao, 0.0, out + k * o2, nao) ||
-        !gemm_f64(h, false, false, M, nao, M, 1.0, Gv, M, X_ao, nao, 0.0, R, nao) ||
-        !gemm_f64(h, true, false, nao, nao, M, -1.0, X_ao, nao, R, nao, 0.0,
-                  out + (ntau + k) * o2, nao))
-      return MBPT_ERR_CUDA;
+    launch_prep_branches(b.Xmo, M, norb, nocc, eps, mu, tau_host[k], b.Yo_hi, b.Yo_lo, d.Ko,
+                         b.Yv_hi, b.Yv_lo, d.Kv, d.Mp, st);
+    launch_split_pad<double>(Wt + k * a2, naux, naux, naux, 1.f, b.W_hi, b.W_lo, d.Ap, d.Ap,
+                             d.Ap, false, st);
+    umma::EpiArgs e;
+    e.out0_hi = b.U_hi;
+    e.out0_lo = b.U_lo;
+    e.ld_out = d.Ap;
+    int rc = gemm_split(umma::EPI_SPLIT, 1, &Dm, &Wm, d.Mp, d.Ap, e, err, st);
+    if (rc) return rc;
+    e = umma::EpiArgs();
+    e.out0_hi = b.Hl_hi;
+    e.out0_lo = b.Hl_lo;
+    e.out1_hi = b.Hg_hi;
+    e.out1_lo = b.Hg_lo;
+    e.ld_out = d.Mp;
+    SplitMat A3[3] = {Yo, Yv, Um}, B3[3] = {Yo, Yv, Dm};
+    rc = gemm_split(umma::EPI_SIGMA_H, 3, A3, B3, d.Mp, d.Mp, e, err, st, umma::BAND_UPPER);
+    if (rc) return rc;
+    const SplitMat *H[2] = {&Hl, &Hg};
+    for (int br = 0; br < 2; ++br) {
+      e = umma::EpiArgs();
+      e.out0_hi = b.RT_hi;
+      e.out0_lo = b.RT_lo;
+      e.ld_out = d.Mp;
+      rc = gemm_split(umma::EPI_SPLIT, 1, &XaT, H[br], naop, d.Mp, e, err, st);
+      if (rc) return rc;
+      e = umma::EpiArgs();
+      e.outd = out + (br * static_cast<int64_t>(ntau) + k) * o2;
+      e.ld_outd = nao;
+      e.nd = static_cast<int>(nao);
+      e.shift = 0.0;
+      e.alpha = br == 0 ? 1.f : -1.f;
+      rc = gemm_split(umma::EPI_F64_SYM, 1, &XaT, &RT, naop, naop, e, err, st,
+                      umma::BAND_UPPER);
+      if (rc) return rc;
+    }
   }
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }

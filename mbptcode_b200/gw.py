@@ -51,12 +51,14 @@ def _transform_screened(Ctw, W_omega):
 def self_energy_matrix_imaginary_time(X_ao, D, W_omega, mo_coeff, eps, nocc, tau_points,
                                       omega_in, omega_out, mu=None, ranges=None,
                                       tau_indices=None, Wt_tau=None, block_memory_gb=None,
-                                      coords=None, screen_r_cut=None):
+                                      coords=None, screen_r_cut=None, precision='fp64'):
     """Full Sigma^c_{mu nu}(i omega_out) in the AO basis, (nfreq_out, nao, nao)
     complex (``imaginary_time.py:403-533``): W(tau) from W(i omega_in) (or
     Wt_tau as given), per time point the two branches X_ao^T (G o Zt) X_ao
-    with G from the MO collocation X_ao mo_coeff (mbpt_sigma_ao, FP64), then
-    Sigma = -1/2 [C (S^> + S^<) + i S (S^> - S^<)]. tau_indices: that subset's
+    with G from the MO collocation X_ao mo_coeff (mbpt_sigma_ao), then
+    Sigma = -1/2 [C (S^> + S^<) + i S (S^> - S^<)]. precision: 'fp64' (the
+    reference's arithmetic), 'fp64_int8' or 'mixed' (the self-energy sweep's
+    split BF16 products, ~1e-5 relative). tau_indices: that subset's
     contribution. block_memory_gb and coords are accepted for signature
     compatibility; distance screening (screen_r_cut) is refused. NumPy in,
     NumPy out."""
@@ -87,11 +89,12 @@ def self_energy_matrix_imaginary_time(X_ao, D, W_omega, mo_coeff, eps, nocc, tau
     norb, naux, nt = Cm.shape[1], Dd.shape[1], len(which)
     tau_h, tp = host_array(tau[which])
     br = torch.empty((2, nt, nao, nao), dtype=torch.float64, device=dev)
-    ws = WORKSPACE.get(lib().mbpt_sigma_ao_workspace_bytes(M, nao, norb, nocc, naux), dev)
+    mode = _mode(precision)
+    ws = WORKSPACE.get(lib().mbpt_sigma_ao_workspace_bytes(M, nao, norb, nocc, naux, mode), dev)
     err = _Err(dev)
     check(lib().mbpt_sigma_ao(ptr(Xa), M, nao, ptr(Cm), norb, nocc, ptr(ed), float(mu),
-                              ptr(Dd), naux, ptr(Wt), tp, nt, ptr(br), ptr(ws), ws.numel(),
-                              ptr(err.t), stream_ptr()), 'mbpt_sigma_ao')
+                              ptr(Dd), naux, ptr(Wt), tp, nt, mode, ptr(br), ptr(ws),
+                              ws.numel(), ptr(err.t), stream_ptr()), 'mbpt_sigma_ao')
     err.check('mbpt_sigma_ao')
     re = transform((br[1] + br[0]).contiguous(), np.ascontiguousarray(C[:, which]))
     im = transform((br[1] - br[0]).contiguous(), np.ascontiguousarray(S[:, which]))

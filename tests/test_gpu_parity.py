@@ -727,6 +727,11 @@ def test_ao_self_energy_and_mirrors_match_reference_golden(golden):
     assert rel(sub, g['sigma_sub']) < 1e-10
     diag = gw.sigma_ao_to_mo_diagonal(sig, mo, states=g['states'])
     assert rel(diag, g['diag']) < 1e-10
+    # the same matrix with the products on the int8 emulation (FP64 level)
+    # and on the engine's split BF16 products (mixed: ~1e-5 relative)
+    for precision, tol in (('fp64_int8', 1e-10), ('mixed', 5e-5)):
+        s_p = gw.self_energy_matrix_imaginary_time(*args, mu=mu, precision=precision)
+        assert rel(s_p, g['sigma']) < tol, precision
     axes_grid = grids.TimeFrequencyGrid.minimax_split(
         int(g['ntau']), *grids.particle_hole_window(eps, nocc)[:2], g['omega'],
         grids.screening_frequency_grid(int(g['ntau']), eps, nocc, mu=mu)[1],
@@ -854,3 +859,37 @@ def test_dyson_batched_groups_with_failed_frequency(prec):
         W_ref = np.linalg.inv(one_minus) - np.eye(n)
         err = np.abs(chi0[f].cpu().numpy() - W_ref).max()
         assert err < (1e-10 if f == 11 else tol) * max(1.0, np.abs(W_ref).max()), (f, err)
+
+
+def test_ao_self_energy_mixed_on_partial_tiles():
+    """The mixed AO self-energy (U = D W, the G o Zt tile pass, X_ao^T H X_ao
+    on the engine) against the FP64 one where no size is a multiple of 128:
+    M = 1100, nao = 300, naux = 900, 40 of 260 orbitals occupied, 6 time
+    points; both branches within 5e-5 of their scale."""
+    from mbptcode_b200._lib import MODES, WORKSPACE, check, lib, ptr, stream_ptr
+    from mbptcode_b200.space_time import _Err
+    rng = np.random.default_rng(3)
+    M, nao, norb, nocc, naux, nt = 1100, 300, 260, 40, 900, 6
+    Xa = torch.as_tensor(rng.standard_normal((M, nao)) * 0.05, device='cuda')
+    C = torch.as_tensor(np.linalg.qr(rng.standard_normal((nao, norb)))[0], device='cuda')
+    Dd = torch.as_tensor(rng.standard_normal((M, naux)) * 0.05, device='cuda')
+    A = rng.standard_normal((nt, naux, naux)) * 0.02
+    Wt = torch.as_tensor(A + A.transpose(0, 2, 1), device='cuda')
+    e = torch.as_tensor(np.sort(np.concatenate([rng.uniform(-1, -0.3, nocc),
+                                                rng.uniform(0.1, 2, norb - nocc)])),
+                        device='cuda')
+    tau = np.linspace(0.2, 3.0, nt)
+    out = {}
+    for p in ('fp64', 'mixed'):
+        m = MODES[p]
+        br = torch.empty((2, nt, nao, nao), dtype=torch.float64, device='cuda')
+        ws = WORKSPACE.get(lib().mbpt_sigma_ao_workspace_bytes(M, nao, norb, nocc, naux, m),
+                           'cuda')
+        err = _Err('cuda')
+        check(lib().mbpt_sigma_ao(ptr(Xa), M, nao, ptr(C), norb, nocc, ptr(e), -0.1, ptr(Dd),
+                                  naux, ptr(Wt), tau.ctypes.data, nt, m, ptr(br), ptr(ws),
+                                  ws.numel(), ptr(err.t), stream_ptr()), 'mbpt_sigma_ao')
+        err.check('mbpt_sigma_ao')
+        out[p] = br.cpu().numpy()
+    for b in range(2):
+        assert rel(out['mixed'][b], out['fp64'][b]) < 5e-5, b
