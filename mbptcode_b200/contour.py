@@ -903,13 +903,40 @@ class _Walk:
         self.done = False
 
 
+class _FollowWalk:
+    """One state's search, over one window's grid, for the valid root nearest
+    a root followed from a previous geometry: rings of cells outward from
+    the cell holding it, until the next ring lies farther from it than the
+    nearest root found."""
+
+    def __init__(self, slot, target, lo, hi):
+        self.slot, self.t, self.lo, self.hi = slot, float(target), lo, hi
+        self.grid = np.linspace(lo, hi, QP_GRAPHICAL_N_OMEGA)
+        self.c0 = min(max(int(np.searchsorted(self.grid, target)) - 1, 0), self.grid.size - 2)
+        self.d = 0
+        self.f, self.bad = {}, {}
+        self.solved = {}            # (l, r) of a bracket -> [(w, Z)]
+        self.best = None
+        self.refusal = None
+        self.done = False
+
+    def ring(self):
+        n = self.grid.size - 1
+        return sorted(c for c in {self.c0 - self.d, self.c0 + self.d} if 0 <= c < n)
+
+
 class _LockstepScan:
     """The scan of many states at once. equation(slots, w, want_slope) ->
     (f, f', refusals {index: exception}) evaluates f(w) = w - a - Sigma(w)
-    and its slope at every point of a round."""
+    and its slope at every point of a round. positive_weight: Sigma is a sum
+    of poles of positive weight, so a bracket where f falls holds a pole and
+    is passed over, and the valid weights of all roots sum to one, which ends
+    a window's walk early; without it every bracket of a window is solved."""
 
-    def __init__(self, equation, tol=QP_ROOT_TOL, max_iter=QP_ROOT_MAX_ITER):
+    def __init__(self, equation, tol=QP_ROOT_TOL, max_iter=QP_ROOT_MAX_ITER,
+                 positive_weight=True):
         self.eq, self.tol, self.max_iter = equation, tol, int(max_iter)
+        self.positive_weight = bool(positive_weight)
         self.rounds = 0
 
     def _eval(self, slots, w, want_slope):
@@ -968,7 +995,7 @@ class _LockstepScan:
         for i, (slot, l, r, fl, fr) in enumerate(brackets):
             if l == r:
                 at[i] = float(l)
-            elif fl > 0.0 > fr:
+            elif self.positive_weight and fl > 0.0 > fr:
                 roots[i] = []          # f falls: a pole of a positive-weight Sigma
             else:
                 live.append(i)
@@ -1080,12 +1107,152 @@ class _LockstepScan:
                                 wk.weighed += z
                                 wk.best = max(wk.best, z)
                     wk.pos += 1
-                    if 1.0 - wk.weighed + QP_WEIGHT_SUM_SLACK <= max(wk.best, wk.enough):
+                    if self.positive_weight and (
+                            1.0 - wk.weighed + QP_WEIGHT_SUM_SLACK <= max(wk.best, wk.enough)):
                         wk.done = True
                         break
                 if wk.pos >= len(wk.order):
                     wk.done = True
             size *= 2
+
+    # -- following a root: the nearest valid root to it, every state in lockstep
+    def _cells_of(self, items):
+        """items: [(walk, cell)] -> {(id(walk), cell): [(l, r, fl, fr)]} with the
+        grid points the cells end on evaluated first (kept on each walk)."""
+        need = []
+        for wk, c in items:
+            need += [(wk, i) for i in (c, c + 1) if i not in wk.f and (wk, i) not in need]
+        f, _, refused = self._eval([wk.slot for wk, _ in need], [wk.grid[i] for wk, i in need],
+                                   False)
+        for j, (wk, i) in enumerate(need):
+            wk.f[i] = float(f[j])
+            if j in refused:
+                wk.bad[i] = refused[j]
+        cells = [((id(wk), c), wk.slot, wk.grid[c], wk.grid[c + 1], wk.f[c], wk.f[c + 1])
+                 for wk, c in items]
+        brk, bad = self._brackets(cells)
+        out = {}
+        for (key, *_r), (wk, c) in zip(cells, items):
+            for e in (wk.bad.get(c), wk.bad.get(c + 1), bad.get(key)):
+                if e is not None and wk.refusal is None:
+                    wk.refusal = e
+            out[key] = [(l, r, fl, fr) for _, l, r, fl, fr in sorted(brk[key])]
+        return out
+
+    def follow_walk(self, walks):
+        """Advance every walk ring by ring until each has stopped."""
+        while True:
+            items = []
+            for wk in walks:
+                if wk.done:
+                    continue
+                cells = wk.ring()
+                if not cells:
+                    wk.done = True
+                    continue
+                near = min(max(wk.grid[c] - wk.t, wk.t - wk.grid[c + 1], 0.0) for c in cells)
+                if wk.best is not None and near > abs(wk.best[0] - wk.t):
+                    wk.done = True
+                    continue
+                items += [(wk, c) for c in cells]
+            if not items:
+                return
+            per_cell = self._cells_of(items)
+            flat, owner = [], []
+            for wk, c in items:
+                for br in per_cell[(id(wk), c)]:
+                    flat.append((wk.slot,) + br)
+                    owner.append(wk)
+            roots, bad = self._roots(flat)
+            for k, wk in enumerate(owner):
+                if bad[k] is not None and wk.refusal is None:
+                    wk.refusal = bad[k]
+                wk.solved[(flat[k][1], flat[k][2])] = roots[k]
+                for w, z in roots[k]:
+                    if _valid(z) and (wk.best is None or abs(w - wk.t) < abs(wk.best[0] - wk.t)):
+                        wk.best = (w, z)
+            for wk in {id(wk): wk for wk, _ in items}.values():
+                wk.d += 1
+
+    def _largest_beside(self, wk, a):
+        """(w, Z) of the largest valid weight of the window beside a followed
+        root below QP_WINDOW_Z_MIN: the brackets solved already as found, any
+        other solved where the weight at its secant root (1/f' there) beats
+        the largest so far; cells outward from a until the weights found
+        leave no more of their sum than that (positive weight), or all."""
+        top, weighed = wk.best, 0.0
+        for got in wk.solved.values():
+            for w, z in got:
+                if _valid(z):
+                    weighed += z
+                    if z > top[1]:
+                        top = (w, z)
+        n = wk.grid.size - 1
+        if self.positive_weight:
+            c0 = min(max(int(np.searchsorted(wk.grid, a)) - 1, 0), n - 1)
+            groups = [[c] for c in _walk_order(c0, n)]
+        else:
+            groups = [list(range(n))]
+        for cells in groups:
+            if self.positive_weight and 1.0 - weighed + QP_WEIGHT_SUM_SLACK <= top[1]:
+                break
+            per_cell = self._cells_of([(wk, c) for c in cells])
+            for c in cells:
+                for l, r, fl, fr in per_cell[(id(wk), c)]:
+                    if (l, r) in wk.solved:
+                        continue
+                    x = l if l == r else l - fl * (r - l) / (fr - fl)
+                    _, fp, _ = self._eval([wk.slot], [x], True)
+                    z = 1.0 / fp[0] if fp[0] != 0.0 else np.nan
+                    if not _valid(z) or z <= top[1]:
+                        continue
+                    got, _ = self._roots([(wk.slot, l, r, fl, fr)])
+                    wk.solved[(l, r)] = got[0]
+                    for w, zz in got[0]:
+                        if _valid(zz):
+                            weighed += zz
+                            if zz > top[1]:
+                                top = (w, zz)
+        return top
+
+    def follow(self, slots, bare, targets, rescan=True):
+        """Per state: None where no window about its bare level holds a valid
+        root near its target (``qp_equation.py:1155-1193``), else (w, Z,
+        largest, refusal): the valid root nearest the target on the narrowest
+        window that holds the target (a wider one while that root lies
+        farther from the target than the window's edge), and beside it the
+        largest valid weight of that window -- the root itself above
+        QP_WINDOW_Z_MIN, else `_largest_beside`, or () with rescan off."""
+        n = len(slots)
+        res = [None] * n
+        wins = [_windows(float(a)) for a in bare]
+
+        def holding(i, start):
+            return next((k for k in range(start, len(wins[i]))
+                         if wins[i][k][0] <= targets[i] <= wins[i][k][1]), None)
+        level = [holding(i, 0) for i in range(n)]
+        pending = [i for i in range(n) if level[i] is not None]
+        while pending:
+            walks = [_FollowWalk(slots[i], targets[i], *wins[i][level[i]]) for i in pending]
+            self.follow_walk(walks)
+            nxt = []
+            for i, wk in zip(pending, walks):
+                last = level[i] + 1 == len(wins[i])
+                t = float(targets[i])
+                if wk.best is not None and (abs(wk.best[0] - t) <= min(t - wk.lo, wk.hi - t)
+                                            or last):
+                    if _valid(wk.best[1], QP_WINDOW_Z_MIN):
+                        largest = wk.best
+                    else:
+                        largest = self._largest_beside(wk, float(bare[i])) if rescan else ()
+                    res[i] = (wk.best[0], wk.best[1], largest, wk.refusal)
+                    continue
+                k = holding(i, level[i] + 1)
+                if k is not None:
+                    level[i] = k
+                    nxt.append(i)
+            pending = nxt
+        return res
 
     def solve(self, slots, bare):
         """Per state: (w, Z, refusal, found roots of its last window), the
@@ -1158,14 +1325,84 @@ def _report_root(w, z, refusal, bare, label):
                       stacklevel=3)
 
 
-def solve_qp_equation_scan(residual, fprime, a, tol=QP_ROOT_TOL, max_iter=QP_ROOT_MAX_ITER,
-                           label='', refusals=()):
-    """(w, Z) of residual(w) = 0 for a positive-weight self-energy known
-    pointwise, residual and fprime host callables (``qp_equation.py:1396-1420``).
+def _branch_flipped(w, z, largest, followed, tol):
+    """Whether a followed root is not the largest weight here
+    (``qp_equation.py:145-152``): its branch has gone, or another root more
+    than tol away carries more weight."""
+    if followed is None:
+        return False
+    return (not followed) or (largest is not None and abs(largest[0] - w) > tol
+                              and largest[1] > z)
+
+
+def _scan_one(equation, a, follow=None, tol=QP_ROOT_TOL, max_iter=QP_ROOT_MAX_ITER, label='',
+              out=None, positive_weight=True, rescan=True):
+    """(w, Z) of one equation (the scan's protocol) about the bare level a,
+    optionally following a previous root (``qp_equation.py:155-237, 342-356``):
+    the valid root nearest it where a window holds one, else the largest
+    weight again (its branch has gone). out: a dict that receives the branch
+    ('labels', 'largest', 'followed', 'flipped', 'no_root', 'z_outside');
+    without it a warning where the largest weight has left the followed
+    root."""
+    from .gw import QPNoRoot, QPWeightOutside
+    scan = _LockstepScan(equation, tol, max_iter, positive_weight)
+    what = label or 'the quasiparticle equation'
+    largest = followed = None
+    if follow is None:
+        (w, z, refusal, _), = scan.solve([0], [float(a)])
+        _report_root(w, z, refusal, float(a), label)
+    else:
+        target = float(follow[0] if isinstance(follow, (tuple, list)) else follow)
+        got = scan.follow([0], [float(a)], [target], rescan)[0]
+        if got is not None:
+            w, z, largest, _ = got
+            largest, followed = (largest or None), True
+        else:
+            (w, z, refusal, _), = scan.solve([0], [float(a)])
+            if refusal is not None:
+                raise refusal
+            if not np.isfinite(w):
+                lo, hi = _windows(float(a))[-1]
+                warnings.warn(f'{what}: the branch followed from {target:.6f} Ha has gone and '
+                              f'no root lies in the widest scan window [{lo:.6f}, {hi:.6f}] '
+                              f'Ha about {float(a):.6f} Ha.', QPNoRoot, stacklevel=3)
+            largest, followed = (float(w), float(z)), False
+        if np.isfinite(w) and not 0.0 < z <= 1.0:
+            warnings.warn(f'the quasiparticle root of {what} {w!r} Ha has Z = {z!r}, outside '
+                          f'(0, 1]: kept', QPWeightOutside, stacklevel=3)
+    w, z = float(w), float(z)
+    flipped = _branch_flipped(w, z, largest, followed, tol)
+    if out is not None:
+        out.update(labels=None, largest=largest, followed=followed, flipped=flipped,
+                   no_root=not np.isfinite(w),
+                   z_outside=bool(np.isfinite(w) and not 0.0 < z <= 1.0))
+    elif flipped:
+        if not followed:
+            msg = (f'{what}: the branch the previous geometry kept has gone; the root of '
+                   f'largest weight is kept again, {w:.10f} Ha (Z = {z:.4f}).')
+        else:
+            msg = (f'{what}: the followed root {w:.10f} Ha has Z = {z:.4f}; the largest '
+                   f'weight is now {largest[1]:.4f} at {largest[0]:.10f} Ha; the branch is '
+                   f'kept.')
+        warnings.warn(msg, RuntimeWarning, stacklevel=3)
+    return w, z
+
+
+def solve_qp_equation_scan(residual, fprime, a, follow=None, tol=QP_ROOT_TOL,
+                           max_iter=QP_ROOT_MAX_ITER, label='', refusals=(), out=None,
+                           positive_weight=False, rescan=True):
+    """(w, Z) of residual(w) = 0 for a self-energy known pointwise,
+    residual and fprime host callables (``qp_equation.py:1396-1420``).
     Points where either raises one of `refusals` count as unknown. No
     quasiparticle where the self-energy could be evaluated raises the first
     refusal; no root at all is (NaN, NaN) with a QPNoRoot warning; a root
-    with Z outside (0, 1] is kept with a QPWeightOutside warning."""
+    with Z outside (0, 1] is kept with a QPWeightOutside warning.
+    positive_weight: Sigma a sum of poles of positive weight (a bracket
+    where f falls is a pole; the walk ends once the weights found leave no
+    more), else every bracket of a window is solved. follow, out, rescan:
+    a previous root to follow, the dict its branch goes to, and whether a
+    weak followed root's window is searched for the largest weight beside
+    it (`_scan_one`)."""
     refusals = tuple(refusals)
 
     def equation(slots, w, want_slope):
@@ -1181,9 +1418,7 @@ def solve_qp_equation_scan(residual, fprime, a, tol=QP_ROOT_TOL, max_iter=QP_ROO
                 f[j], fp[j] = np.nan, np.nan
                 bad[j] = e
         return f, fp, bad
-    (w, z, refusal, _), = _LockstepScan(equation, tol, max_iter).solve([0], [float(a)])
-    _report_root(w, z, refusal, float(a), label)
-    return float(w), float(z)
+    return _scan_one(equation, a, follow, tol, max_iter, label, out, positive_weight, rescan)
 
 
 def _contour_equation_callable(eq):
@@ -1289,16 +1524,21 @@ def qp_energy_cd(p, Bp, eps, nocc, nu_points, nu_weights, xc_correction=0.0, tol
     contour deformation (``contour_deformation.py:376-436``): the lockstep
     scan about the bare level with the residues re-decided at every point,
     the residue set of the root returned. Screening and backend as
-    `sigma_cd`."""
-    if follow is not None or branch is not None:
-        raise NotImplementedError('following a root along a walk is outside the device route')
+    `sigma_cd`. follow, branch, rescan: a walk's previous root (the root
+    nearest it is kept, whatever its weight), the dict its branch goes to,
+    and whether a weak followed root's window is searched for the largest
+    weight beside it."""
     eq = _one_state_equation(p, Bp, eps, nocc, nu_points, nu_weights, xc_correction, wbp, wc,
                              C_ov, eta, real_screening)
-    roots, zs, refusals = solve_contour_roots(eq, [f'orbital {p}'], tol, max_iter)
-    if refusals[0] is not None:
-        raise refusals[0]
-    w = float(roots[0])
-    return w, float(zs[0]), residue_set(eps, nocc, w)
+    if follow is None and branch is None:
+        roots, zs, refusals = solve_contour_roots(eq, [f'orbital {p}'], tol, max_iter)
+        if refusals[0] is not None:
+            raise refusals[0]
+        w = float(roots[0])
+        return w, float(zs[0]), residue_set(eps, nocc, w)
+    w, z = _scan_one(_contour_equation_callable(eq), eq.bare[0], follow, tol, max_iter,
+                     f'orbital {p}', branch, True, rescan)
+    return w, z, residue_set(eps, nocc, w)
 
 
 def residue_backend(real_screening, C_ov, eps, nocc, eta):
@@ -1508,6 +1748,36 @@ def _slice_backward(X, D, p, B_bar, X_bar, D_bar):
           'mbpt_three_index_slice_backward')
 
 
+def _frozen_root(w0, p):
+    """The root a reference geometry kept for orbital p: w0 a number or a
+    mapping orbital -> root; None before one is kept
+    (``gradients/gwbse/qp_space_time.py:102-114``)."""
+    if isinstance(w0, dict):
+        got = w0.get(int(p))
+        return None if got is None else float(got)
+    return None if w0 is None else float(w0)
+
+
+def _followed_branch(follow, w0, p):
+    """(w, labels) orbital p follows here: the branch `follow` (a mapping
+    orbital -> (w, labels)) names, else the frozen root by energy, else None
+    (``qp_space_time.py:137-150``)."""
+    got = follow.get(int(p)) if isinstance(follow, dict) else None
+    if got is not None:
+        w, labels = got
+        return float(w), (None if labels is None else tuple(labels))
+    root = _frozen_root(w0, p)
+    return None if root is None else (root, None)
+
+
+def _rescans_beside(z0, p):
+    """Whether a weak followed root of p has its window searched for the
+    largest weight beside it: unless the reference root's Z (z0, a mapping
+    orbital -> Z) was no quasiparticle's either (``qp_space_time.py:124-134``)."""
+    z = z0.get(int(p)) if isinstance(z0, dict) else None
+    return z is None or _valid(z, QP_WINDOW_Z_MIN)
+
+
 def qp_gradient_space_time(X, D, eps, nocc, grid, nu_points, nu_weights, p, *,
                            residue_route='laplace', mu=None, xc_correction=0.0, w0=None,
                            tol=QP_ROOT_TOL, laplace_tol=LAPLACE_SCREENING_TOL, want_grad=True,
@@ -1523,13 +1793,18 @@ def qp_gradient_space_time(X, D, eps, nocc, grid, nu_points, nu_weights, p, *,
     proj(tau)) and to eps through its weights; each residue's to the slice,
     to chi0 at its real frequency (folded onto proj(tau) by the cosh weights)
     and to eps through its frequency; then the chi0 sweep's and the slice's
-    reverses. FP64 on the device; arrays come back as X is held."""
+    reverses. FP64 on the device; arrays come back as X is held.
+    w0, follow, z0: a walk's frozen root (followed by energy), the branch
+    the last accepted geometry kept ({p: (w, labels)}), and the reference
+    roots' Z ({p: Z}, whether a weak followed root's window is rescanned);
+    route_out receives 'residue_route', 'residues', 'weights', 'roots',
+    'labels', 'branches' and 'sop_poles'."""
     if residue_route != 'laplace':
         raise NotImplementedError(f'residue_route={residue_route!r}: the device route serves '
                                   "'laplace' (the cubic residues)")
-    if any(v is not None for v in (follow, scissor, sop_poles, comm, z0, w0)):
-        raise NotImplementedError('walks, scissors, pole models and rank splits are outside '
-                                  'the device route')
+    if any(v is not None for v in (scissor, sop_poles, comm)):
+        raise NotImplementedError('scissors, pole models and rank splits are outside the '
+                                  'device route')
     dev = require_device()
     eps_h = _eps_host(eps)
     p = int(p)
@@ -1540,10 +1815,15 @@ def qp_gradient_space_time(X, D, eps, nocc, grid, nu_points, nu_weights, p, *,
     B = three_index_slices(X, D, [p])[0]
     wc = screening_contraction_device(wmi, [B])[0]
     lap = LaplaceRealScreening(proj, grid, eps_h, nocc, tol=laplace_tol)
+    followed, branch = _followed_branch(follow, w0, p), {}
     w, z, res = qp_energy_cd(p, B, eps_h, nocc, nu_points, nu_weights,
-                             xc_correction=xc_correction, tol=tol, wc=wc, real_screening=lap)
+                             xc_correction=xc_correction, tol=tol, wc=wc, real_screening=lap,
+                             follow=followed, branch=branch, rescan=_rescans_beside(z0, p))
     if route_out is not None:
-        route_out.update(residue_route='laplace', residues=res)
+        route_out.update(residue_route='laplace', residues=res, weights={p: float(z)},
+                         roots={p: float(w)}, labels={p: branch.get('labels')},
+                         branches={p: branch} if followed is not None else {},
+                         sop_poles={})
     if not want_grad:
         return w, z
     naux, norb = B.shape

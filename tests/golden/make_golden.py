@@ -57,6 +57,13 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      aux_metric_sqrt and D = M^T V^1/2;
 * qp_kat.npz         the root finder on closed-form self-energies
                      (tests/test_qp_refine_root.py's two-pole Sigma and others);
+* qp_follow.npz      the scan following a previous root (`follow`, `out`,
+                     `rescan`, `positive_weight`) on 24 seeded pole-sum
+                     self-energies: each model's poles and amplitudes, the
+                     followed points, and the root, Z and branch record the
+                     reference's `solve_qp_equation_scan` returns;
+* contour_follow.npz `qp_energy_cd` following a previous root on the system of
+                     contour.npz (Laplace residues): root, Z, branch record
 * c1_<variant>.npz   the synthetic FP64 configuration at full size (n_orb = 400,
                      nocc = 40, N_mu = 2400, 16 points, seed 400): the Sigma_c
                      diagonal, every QP root and Z, E_c, and the adjoint
@@ -64,7 +71,7 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      stored: the tests regenerate them from the seed and check
                      the regeneration against the stored eps and checksums.
 
-    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|contour_explicit|contour_unrestricted|sigma_ao|evgw|drop_in|isdf]
+    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|contour_explicit|contour_unrestricted|sigma_ao|evgw|drop_in|isdf|follow]
 """
 import os
 import sys
@@ -848,6 +855,114 @@ def qp_fixture():
     np.savez_compressed(os.path.join(HERE, 'qp_kat.npz'), **out)
 
 
+def follow_fixture(nmodels=24, seed=31):
+    """Root following on the scan (``Solvers/qp_equation.py:1396-1420``,
+    `find_qp_root` with `follow`): the reference's `solve_qp_equation_scan`
+    on seeded pole-sum self-energies Sigma(w) = sum_k A_k / (w - p_k), each
+    with its closed-form slope, unfollowed and following points beside each
+    root, between roots and outside every window, rescan on and off,
+    positive_weight on (positive amplitudes) and off (some negative), with
+    the branch record the `out` dict receives."""
+    from src.Solvers.qp_equation import solve_qp_equation_scan
+    rng = np.random.default_rng(seed)
+    models, cases = [], []
+
+    def model(a, pol, amp):
+        def f(w):
+            return w - a - float(np.sum(amp / (w - pol)))
+
+        def fp(w):
+            return 1.0 + float(np.sum(amp / (w - pol) ** 2))
+        return f, fp
+    for m in range(nmodels):
+        npol = int(rng.integers(3, 7))
+        pol = np.sort(rng.uniform(-2.0, 2.0, npol))
+        amp = np.exp(rng.uniform(np.log(1e-6), np.log(0.3), npol))
+        positive = m % 4 != 3
+        if not positive:
+            amp[int(rng.integers(npol))] *= -1.0
+        a = float(rng.uniform(-0.6, 0.6))
+        models.append((a, pol, amp, positive))
+        f, fp = model(a, pol, amp)
+        with warnings.catch_warnings():
+            warnings.simplefilter('ignore')
+            w0, _ = solve_qp_equation_scan(f, fp, a, positive_weight=positive)
+        grid = np.linspace(a - 0.5, a + 0.5, 2001)
+        vals = np.array([f(x) for x in grid])
+        roots = [0.5 * (grid[i] + grid[i + 1]) for i in range(len(grid) - 1)
+                 if vals[i] < 0.0 < vals[i + 1]]
+        targets = [None] + [r + d for r in roots[:4] for d in (0.0, 3e-3)]
+        targets += [float(rng.uniform(a - 0.4, a + 0.4)), a + 3.0]
+        for t in targets:
+            for rescan in ((True, False) if t is not None else (True,)):
+                out = {}
+                with warnings.catch_warnings():
+                    warnings.simplefilter('ignore')
+                    w, z = solve_qp_equation_scan(f, fp, a, follow=t, out=out,
+                                                  positive_weight=positive, rescan=rescan)
+                lg = out.get('largest')
+                cases.append([m, np.nan if t is None else t, float(rescan), w, z,
+                              np.nan if lg is None or not len(lg) else lg[0],
+                              np.nan if lg is None or not len(lg) else lg[1],
+                              {None: -1.0, False: 0.0, True: 1.0}[out.get('followed')],
+                              float(bool(out.get('flipped'))), float(bool(out.get('no_root'))),
+                              float(bool(out.get('z_outside')))])
+    npol_max = max(len(mm[1]) for mm in models)
+    pols = np.full((nmodels, npol_max), np.nan)
+    amps = np.zeros((nmodels, npol_max))
+    for i, (_, pol, amp, _) in enumerate(models):
+        pols[i, :len(pol)], amps[i, :len(amp)] = pol, amp
+    np.savez_compressed(os.path.join(HERE, 'qp_follow.npz'),
+                        a=np.array([mm[0] for mm in models]), poles=pols, amps=amps,
+                        positive=np.array([mm[3] for mm in models]),
+                        cases=np.array(cases, float),
+                        columns=np.array(['model', 'follow', 'rescan', 'w', 'z', 'largest_w',
+                                          'largest_z', 'followed', 'flipped', 'no_root',
+                                          'z_outside']))
+
+
+def contour_follow_fixture():
+    """`qp_energy_cd` following a previous root (``contour_deformation.py:
+    376-436`` with `follow`, `branch`, `rescan`) on the system of
+    `contour_fixture`, residues through the Laplace backend: per state, the
+    followed points the root itself, 2e-3 above it, 0.02 below it and 0.3
+    above its level, the rescan on and off; the root, Z and the branch
+    record."""
+    cd, rs = _import_contour_deformation()
+    from src.gradients.rpa.space_time_adjoint import polarizability_tau
+    from src.SingleReference.LinearResponse.space_time import three_index_slice
+    g = np.load(os.path.join(HERE, 'contour.npz'))
+    X, D, eps, nocc, mu = g['X'], g['D'], g['eps'], int(g['nocc']), float(g['mu'])
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        nu, nu_w, grid, _ = cd.cd_frequency_grid(eps, nocc)
+    proj = polarizability_tau(X, D, eps, nocc, grid, mu=mu)
+    states = g['states']
+    Bps = [three_index_slice(X, D, int(p)) for p in states]
+    wcs = cd.cd_screening_contraction_multi(proj, grid.cosft_wt, Bps)
+    cases = []
+    for i, p in enumerate(states):
+        root = float(g['roots'][i, 0])
+        for t in (root, root + 2e-3, root - 0.02, float(eps[p]) + 0.3):
+            for rescan in (True, False):
+                out = {}
+                with warnings.catch_warnings():
+                    warnings.simplefilter('ignore')
+                    w, z, res = cd.qp_energy_cd(
+                        int(p), Bps[i], eps, nocc, nu, nu_w, wc=wcs[i],
+                        real_screening=rs.LaplaceRealScreening(proj, grid, eps, nocc),
+                        follow=t, branch=out, rescan=rescan)
+                lg = out.get('largest')
+                cases.append([i, t, float(rescan), w, z,
+                              np.nan if lg is None or not len(lg) else lg[0],
+                              np.nan if lg is None or not len(lg) else lg[1],
+                              {None: -1.0, False: 0.0, True: 1.0}[out.get('followed')],
+                              float(bool(out.get('flipped'))), len(res)])
+    np.savez_compressed(os.path.join(HERE, 'contour_follow.npz'), cases=np.array(cases, float),
+                        columns=np.array(['state', 'follow', 'rescan', 'w', 'z', 'largest_w',
+                                          'largest_z', 'followed', 'flipped', 'residues']))
+
+
 if __name__ == '__main__':
     if ONLY == 'c1':
         c1_fixture('literal')
@@ -894,9 +1009,15 @@ if __name__ == '__main__':
         contour_unrestricted_fixture()
         print('unrestricted contour fixture written to', HERE)
         sys.exit(0)
+    if ONLY == 'follow':
+        follow_fixture()
+        contour_follow_fixture()
+        print('root-following fixtures written to', HERE)
+        sys.exit(0)
     if ONLY:
         sys.exit(f'--only {ONLY}: choose c1, static, unrestricted, sigma_adjoint, contour, '
-                 'contour_explicit, contour_unrestricted, sigma_ao, evgw, drop_in or isdf')
+                 'contour_explicit, contour_unrestricted, sigma_ao, evgw, drop_in, isdf or '
+                 'follow')
     grids_fixture()
     shared_kernel_fixture()
     route_fixture('calibrated', 24, 4, 64, 7, 'calibrated', 12, full=True)

@@ -831,6 +831,19 @@ def test_contour_qp_gradient_matches_reference_golden(golden):
         for a, k in ((eb, 'eps_bar'), (xb, 'X_bar'), (db, 'D_bar')):
             ref = g[k][i]
             assert np.abs(a - ref).max() <= 1e-8 * np.abs(ref).max(), (int(p), k)
+    # a walk's next geometry (here the same one): the root frozen as w0 and its
+    # branch followed from 1e-3 away; the quasiparticle branch continues, so
+    # the root, Z and gradient are the unfollowed ones
+    i, p = 1, int(g['states'][1])
+    root, zr = float(g['grad_roots'][i, 0]), float(g['grad_roots'][i, 1])
+    rec = {}
+    w, z, eb, xb, db = contour.qp_gradient_space_time(
+        g['X'], g['D'], eps, nocc, grid, nu, nu_w, p, mu=mu, w0={p: root},
+        follow={p: (root + 1e-3, None)}, z0={p: zr}, route_out=rec)
+    assert abs(w - root) < 1e-9 and abs(z - zr) < 1e-8
+    assert rec['branches'][p]['followed'] and not rec['branches'][p]['flipped']
+    assert rec['roots'][p] == w and rec['weights'][p] == z
+    assert np.abs(db - g['D_bar'][i]).max() <= 1e-8 * np.abs(g['D_bar'][i]).max()
 
 
 @pytest.mark.parametrize('prec', ['fp64', 'mixed'])
@@ -893,3 +906,36 @@ def test_ao_self_energy_mixed_on_partial_tiles():
         out[p] = br.cpu().numpy()
     for b in range(2):
         assert rel(out['mixed'][b], out['fp64'][b]) < 5e-5, b
+
+
+def test_contour_root_following_matches_reference_golden(golden):
+    """`qp_energy_cd` with a followed root (`follow`, `branch`, `rescan`) on
+    the contour system, residues by the cosh transform of proj(tau): root,
+    Z and branch record against the reference's (`contour_follow.npz`)."""
+    import warnings
+    from mbptcode_b200 import contour
+    g = golden('contour')
+    cf = golden('contour_follow')
+    col = {c: i for i, c in enumerate(cf['columns'])}
+    X, D, eps, nocc, mu = g['X'], g['D'], g['eps'], int(g['nocc']), float(g['mu'])
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        nu, nu_w, grid, _ = contour.cd_frequency_grid(eps, nocc)
+    proj = contour.polarizability_tau(X, D, eps, nocc, grid, mu=mu)
+    B = contour.three_index_slices(X, D, g['states'])
+    wcs = contour.cd_screening_contraction_multi(proj, grid.cosft_wt, list(B))
+    for row in cf['cases']:
+        i = int(row[col['state']])
+        p = int(g['states'][i])
+        out = {}
+        with warnings.catch_warnings():
+            warnings.simplefilter('ignore')
+            w, z, res = contour.qp_energy_cd(
+                p, B[i], eps, nocc, nu, nu_w, wc=wcs[i],
+                real_screening=contour.LaplaceRealScreening(proj, grid, eps, nocc),
+                follow=float(row[col['follow']]), branch=out, rescan=bool(row[col['rescan']]))
+        assert abs(w - row[col['w']]) < 1e-9 and abs(z - row[col['z']]) < 1e-8, (p, row)
+        assert {None: -1.0, False: 0.0, True: 1.0}[out['followed']] == row[col['followed']]
+        assert float(out['flipped']) == row[col['flipped']]
+        assert len(res) == int(row[col['residues']])
+        assert abs(out['largest'][0] - row[col['largest_w']]) < 1e-9

@@ -287,7 +287,8 @@ def test_contour_root_finder_on_the_oracle(golden):
         def fprime(w, p=p, B=B, wc=wc):
             return 1.0 - orc.sigma_cd_slope(p, w, B, eps, nocc, g['nu'], g['nu_w'], wc, *args)
         w, z = contour.solve_qp_equation_scan(residual, fprime, float(eps[p]),
-                                              refusals=(orc.LaplaceRefused,))
+                                              refusals=(orc.LaplaceRefused,),
+                                              positive_weight=True)
         assert abs(w - g['roots'][i, 0]) < 1e-10 and abs(z - g['roots'][i, 1]) < 1e-9, p
 
 
@@ -329,7 +330,8 @@ def test_contour_explicit_backend_oracle(golden):
         def fprime(w, p=p, i=i):
             return 1.0 - orc.sigma_cd_slope_explicit(p, w, B[i], eps, nocc, g['nu'],
                                                      g['nu_w'], g['wc'][i], C)
-        w, z = contour.solve_qp_equation_scan(residual, fprime, float(eps[p]))
+        w, z = contour.solve_qp_equation_scan(residual, fprime, float(eps[p]),
+                                              positive_weight=True)
         assert abs(w - g['roots'][i, 0]) < 1e-10 and abs(z - g['roots'][i, 1]) < 1e-9, p
 
 
@@ -374,7 +376,8 @@ def test_contour_unrestricted_oracle(golden):
                 def fprime(w, p=p, i=i, slope=slope, extra=extra):
                     return 1.0 - slope(p, w, B[i], e, n, nu, nu_w, wc, *extra, **lap)
                 roots[name] = contour.solve_qp_equation_scan(residual, fprime, float(e[p]),
-                                                             refusals=(orc.LaplaceRefused,))
+                                                             refusals=(orc.LaplaceRefused,),
+                                                             positive_weight=True)
             for name in ('laplace', 'cd'):
                 want = g[f'roots_{name}_{s}'][i]
                 w, z = roots[name]
