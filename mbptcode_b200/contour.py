@@ -1562,14 +1562,64 @@ def require_three_index(C_ov, what):
 HARTREE_TO_EV = 27.211386245988  # MBPTcode constants.py:11 (CODATA 2018)
 
 
+def _admission(eps, nocc, states, continuation, pairs=None):
+    """(start points, [(admits, reach)]) of the states: each judged at eps_p
+    moved 1 mHa toward the chemical potential by the pole model's compression
+    condition, which 'sop' enforces before anything is built
+    (``contour_deformation.py:690-703``)."""
+    from . import sum_over_poles as sop
+    starts = np.array([sop.qp_start(eps, int(p), nocc) for p in states])
+    admission = [sop.compressible(float(w), eps, nocc, pair_energies=pairs) for w in starts]
+    if continuation == 'sop':
+        for p, start, (admits, reach) in zip(states, starts, admission):
+            if not admits:
+                raise ValueError(
+                    f"continuation='sop' cannot serve orbital {int(p)}: its start point "
+                    f'{start:.4f} Ha sweeps a pole {reach:.3f} particle-hole gaps away, and '
+                    'the pole model converges only below one (beyond it single excitations '
+                    "of W matter, not their envelope); use continuation='cd'.")
+    return starts, admission
+
+
+def _sop_roots(states, wcs, eps, nocc, nu, xc, n_poles, sop_stride, pairs):
+    """Each state's root and Z on its pole model, fitted to its wc."""
+    from . import sum_over_poles as sop
+    roots, zs, poles_of = np.zeros(len(states)), np.zeros(len(states)), []
+    for i, p in enumerate(states):
+        wc = wcs[i].detach().cpu().numpy() if torch.is_tensor(wcs[i]) else np.asarray(wcs[i])
+        poles, amp = sop.sop_from_wc(wc, nu, eps, nocc, n_poles=n_poles, stride=sop_stride,
+                                     pair_energies=pairs, state=int(p))
+        roots[i], zs[i] = sop.qp_energy_sop(int(p), amp, poles, eps, nocc,
+                                            xc_correction=float(xc[i]))
+        poles_of.append(poles)
+    return roots, zs, poles_of
+
+
 def _roots_on_contour(continuation, states, B, wcs, eps, nocc, nu, nu_w, xc_correction,
-                      backend, w0, ntau, nfreq_cd):
+                      backend, w0, ntau, nfreq_cd, starts=None, admission=None, n_poles=None,
+                      sop_stride=None, pairs=None):
     """Every state's root and Z on one contour grid, all states' scans in
-    lockstep, with the per-state records (``contour_deformation.py:558-598``)."""
+    lockstep (or each on its pole model, 'sop'), with the per-state records
+    (``contour_deformation.py:558-598``)."""
     explicit = continuation == 'cd'
     xc = np.broadcast_to(np.asarray(xc_correction, float).ravel()
                          if np.ndim(xc_correction) else float(xc_correction),
                          (len(states),))
+    if starts is None:
+        starts, admission = _admission(eps, nocc, states, continuation, pairs)
+    if continuation == 'sop':
+        from . import sum_over_poles as sop
+        roots, zs, poles_of = _sop_roots(states, wcs, eps, nocc, nu, xc,
+                                         n_poles or sop.SOP_N_POLES,
+                                         sop.SOP_FIT_STRIDE if sop_stride is None else sop_stride,
+                                         pairs)
+        records = [{'state': int(p), 'qp_start': float(starts[i]), 'residues': 0,
+                    'representation_error': None, 'sop_admits': bool(admission[i][0]),
+                    'sop_reach': float(admission[i][1]), 'sop_poles': poles_of[i]}
+                   for i, p in enumerate(states)]
+        info = {'continuation': 'sop', 'ntau': int(ntau), 'nfreq_cd': int(nfreq_cd),
+                'w0_cd': float(w0), 'residue_route_taken': 'sop', 'states': records}
+        return roots, zs, info
     wc = torch.stack([to_device(w, B.device) for w in wcs])
     eq = ContourEquation(B, wc, eps, nocc, LorentzianQuadrature(nu, nu_w),
                          eps[states] + xc, backend)
@@ -1587,7 +1637,9 @@ def _roots_on_contour(continuation, states, B, wcs, eps, nocc, nu, nu_w, xc_corr
         error = None
         if not explicit and res:
             error = float(backend.errors([abs(eps[q] - roots[i]) for q, _ in res]).max())
-        records.append({'state': int(p), 'residues': len(res), 'representation_error': error})
+        records.append({'state': int(p), 'qp_start': float(starts[i]), 'residues': len(res),
+                        'representation_error': error, 'sop_admits': bool(admission[i][0]),
+                        'sop_reach': float(admission[i][1])})
     info = {'continuation': continuation, 'ntau': int(ntau), 'nfreq_cd': int(nfreq_cd),
             'w0_cd': float(w0), 'residue_route_taken': 'explicit' if explicit else 'laplace',
             'states': records, 'points_evaluated': int(eq.points),
@@ -1598,22 +1650,26 @@ def _roots_on_contour(continuation, states, B, wcs, eps, nocc, nu, nu_w, xc_corr
 
 def contour_roots(X, D, eps, nocc, states, ntau=CD_NTAU, nfreq_cd=CD_NFREQ, w0_cd=None,
                   e_min_below_gap=None, xc_correction=0.0, mu=None, continuation='laplace',
-                  precision='fp64'):
+                  precision='fp64', n_poles=None, sop_stride=None):
     """(roots in Hartree, Z, per-state records) of the states on one contour
     grid (``contour_deformation.py:558-598, 767-812``): one proj(tau) and one
     W per frequency serve every state's imaginary-axis term, each state's
     root by `qp_energy_cd`. The residues read W at real frequencies from the
     cosh transform of the same proj(tau) (continuation 'laplace', which
     refuses a state whose residues the time grid does not carry) or from the
-    explicit particle-hole response of C_ov (continuation 'cd', any state).
-    xc_correction: the static term, one per state or one for all. precision
-    'mixed' runs the screening contraction and the explicit response as
-    split tensor-core products (the Dyson steps and the Laplace residues stay
-    FP64)."""
-    if continuation not in ('laplace', 'cd'):
-        raise ValueError(f"continuation={continuation!r}: choose 'cd' or 'laplace'")
+    explicit particle-hole response of C_ov (continuation 'cd', any state);
+    'sop' models W on the imaginary axis by n_poles fitted poles instead
+    (`sum_over_poles`), Sigma closed form and no real-frequency screening,
+    and refuses the states the compression condition excludes before
+    anything is built. xc_correction: the static term, one per state or one
+    for all. precision 'mixed' runs the screening contraction and the
+    explicit response as split tensor-core products (the Dyson steps and the
+    Laplace residues stay FP64)."""
+    if continuation not in ('laplace', 'cd', 'sop'):
+        raise ValueError(f"continuation={continuation!r}: choose 'cd', 'laplace' or 'sop'")
     eps = _eps_host(eps)
     states = np.atleast_1d(np.asarray(states, int))
+    starts, admission = _admission(eps, nocc, states, continuation)
     explicit = (ExplicitRealScreening(three_index_ov(X, D, eps, nocc), eps, nocc,
                                       precision=precision)
                 if continuation == 'cd' else None)
@@ -1622,25 +1678,30 @@ def contour_roots(X, D, eps, nocc, states, ntau=CD_NTAU, nfreq_cd=CD_NFREQ, w0_c
     proj = polarizability_tau(X, D, eps, nocc, grid, mu=mu)
     B = three_index_slices(X, D, states)
     wcs = cd_screening_contraction_multi(proj, grid.cosft_wt, list(B), precision=precision)
-    backend = LaplaceRealScreening(proj, grid, eps, nocc) if explicit is None else explicit
+    backend = (explicit if explicit is not None else None if continuation == 'sop'
+               else LaplaceRealScreening(proj, grid, eps, nocc))
     del proj
     return _roots_on_contour(continuation, states, B, wcs, eps, nocc, nu, nu_w, xc_correction,
-                             backend, w0, ntau, nfreq_cd)
+                             backend, w0, ntau, nfreq_cd, starts, admission, n_poles,
+                             sop_stride)
 
 
 def contour_roots_unrestricted(X_mos, D, spectra, noccs, spin, states, ntau=CD_NTAU,
                                nfreq_cd=CD_NFREQ, w0_cd=None, e_min_below_gap=None,
-                               xc_correction=0.0, continuation='laplace', precision='fp64'):
+                               xc_correction=0.0, continuation='laplace', precision='fp64',
+                               n_poles=None, sop_stride=None):
     """`contour_roots` for one spin channel of an unrestricted reference
     (``contour_deformation.py:686-812``): both spins' pair energies side by
     side set the contour grid, proj(tau) is the spin sum (half of each spin's
     restricted sweep at its own mid-gap), the channel's slices and contraction
     read it, and the residues come from its cosh transform on those pair
     energies ('laplace') or from both spins' C_ov side by side at 1/sqrt(2),
-    so that the restricted factor 2 counts every pair once ('cd'). spin: 0
-    (alpha) or 1 (beta); states are the channel's orbitals."""
-    if continuation not in ('laplace', 'cd'):
-        raise ValueError(f"continuation={continuation!r}: choose 'cd' or 'laplace'")
+    so that the restricted factor 2 counts every pair once ('cd'), or the
+    channel's pole model with its bounds and compression test on both spins'
+    pair energies ('sop'). spin: 0 (alpha) or 1 (beta); states are the
+    channel's orbitals."""
+    if continuation not in ('laplace', 'cd', 'sop'):
+        raise ValueError(f"continuation={continuation!r}: choose 'cd', 'laplace' or 'sop'")
     if len(X_mos) != 2 or len(spectra) != 2 or len(noccs) != 2 or spin not in (0, 1):
         raise ValueError('an unrestricted contour takes two spin channels and spin 0 or 1')
     from .space_time import spin_summed
@@ -1649,6 +1710,7 @@ def contour_roots_unrestricted(X_mos, D, spectra, noccs, spin, states, ntau=CD_N
     pairs = np.concatenate([ov_energies(e, n) for e, n in zip(spectra, noccs)])
     eps, nocc = spectra[spin], noccs[spin]
     states = np.atleast_1d(np.asarray(states, int))
+    starts, admission = _admission(eps, nocc, states, continuation, pairs)
     explicit = None
     if continuation == 'cd':
         C = torch.cat([three_index_ov(X, D, e, n) for X, e, n in zip(X_mos, spectra, noccs)],
@@ -1661,11 +1723,12 @@ def contour_roots_unrestricted(X_mos, D, spectra, noccs, spin, states, ntau=CD_N
     proj = spin_summed(polarizability_tau, X_mos, D, spectra, noccs, grid)
     B = three_index_slices(X_mos[spin], D, states)
     wcs = cd_screening_contraction_multi(proj, grid.cosft_wt, list(B), precision=precision)
-    backend = (LaplaceRealScreening(proj, grid, eps, nocc, pair_energies=pairs)
-               if explicit is None else explicit)
+    backend = (explicit if explicit is not None else None if continuation == 'sop'
+               else LaplaceRealScreening(proj, grid, eps, nocc, pair_energies=pairs))
     del proj
     return _roots_on_contour(continuation, states, B, wcs, eps, nocc, nu, nu_w, xc_correction,
-                             backend, w0, ntau, nfreq_cd)
+                             backend, w0, ntau, nfreq_cd, starts, admission, n_poles,
+                             sop_stride, pairs)
 
 
 def solve_qp_energy_contour(mf, mol, nocc, states, continuation='cd', numerics=None,
@@ -1686,20 +1749,25 @@ def solve_qp_energy_contour(mf, mol, nocc, states, continuation='cd', numerics=N
     exact for any state; 'laplace' solves the same contour from the cubic
     cosh transform wherever the time grid carries the residue frequencies,
     and refuses a state by name otherwise, as the reference does. 'sop' (the
-    pole model) is outside the device route and refused. precision: as
-    `contour_roots`."""
-    if continuation not in ('cd', 'laplace'):
-        raise NotImplementedError(f"continuation={continuation!r}: the device route runs "
-                                  "'cd' (explicit residues) and 'laplace' (cubic residues)")
+    pole model: numerics.qp.n_poles poles, every numerics.qp.sop_stride-th
+    orbital's wc in the fit) refuses the states the compression condition
+    excludes. precision: as `contour_roots`."""
+    if continuation not in ('cd', 'laplace', 'sop'):
+        raise ValueError(f"solve_qp_energy_contour runs continuation='cd', 'laplace' or "
+                         f"'sop', not {continuation!r}")
     if factors is None:
         raise NotImplementedError('building the ISDF factors needs pyscf (integrals and the '
                                   'fit); pass factors=(X_mo, D)')
     eps = np.asarray(getattr(mf, 'mo_energy', mf), float)
     ntau, nfreq = CD_NTAU, CD_NFREQ
+    n_poles = sop_stride = None
     if numerics is not None:
         q = numerics.quadrature
         ntau = getattr(q, 'ntau_cd', ntau)
         nfreq = getattr(q, 'nfreq_cd', nfreq)
+        qp = getattr(numerics, 'qp', None)
+        n_poles = getattr(qp, 'n_poles', None)
+        sop_stride = getattr(qp, 'sop_stride', None)
     states = np.atleast_1d(np.asarray(states, int))
     xc = 0.0 if xc_diagonal is None else np.asarray(xc_diagonal, float)
     X, D = (factors['X_mo'], factors['D']) if isinstance(factors, dict) else factors[:2]
@@ -1725,13 +1793,13 @@ def solve_qp_energy_contour(mf, mol, nocc, states, continuation='cd', numerics=N
         roots, zs, info = contour_roots_unrestricted(
             X_mos, D, list(eps), tuple(int(n) for n in nocc), spin, states, ntau=ntau,
             nfreq_cd=nfreq, w0_cd=w0_cd, xc_correction=xc, continuation=continuation,
-            precision=precision)
+            precision=precision, n_poles=n_poles, sop_stride=sop_stride)
         return roots * HARTREE_TO_EV, zs, info
     if eps_anchor is not None:
         xc = xc + (np.asarray(eps_anchor, float)[states] - eps[states])
     roots, zs, info = contour_roots(X, D, eps, nocc, states, ntau=ntau, nfreq_cd=nfreq,
                                     w0_cd=w0_cd, xc_correction=xc, continuation=continuation,
-                                    precision=precision)
+                                    precision=precision, n_poles=n_poles, sop_stride=sop_stride)
     return roots * HARTREE_TO_EV, zs, info
 
 

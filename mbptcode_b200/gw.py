@@ -701,8 +701,8 @@ def calc_qp_energy(mf, selfenergy='GW', polarizability='RPA', df=True, eta=None,
     residues, Z from its slope), or self_consistency 'evGW'. mf: an object
     with mo_energy and mo_occ (or route_kwargs['nocc']). The reference's
     refusals are kept: GW@RPA on density fitting only, no eta, no tda; the
-    Casida and imaginary-frequency modes and the 'sop' continuation are other
-    routes and refused."""
+    Casida and imaginary-frequency modes are other routes and refused; 'sop'
+    solves the contour's pole model."""
     if mode != 'space-time':
         raise NotImplementedError(f"mode={mode!r}: the device route is mode='space-time'")
     if isinstance(selfenergy, list) or str(selfenergy).upper() != 'GW':
@@ -717,7 +717,7 @@ def calc_qp_energy(mf, selfenergy='GW', polarizability='RPA', df=True, eta=None,
     if eta is not None:
         raise ValueError("eta broadens nothing on mode='space-time'")
     continuation = 'pade' if continuation is None else continuation
-    if continuation not in ('pade', 'laplace', 'cd'):
+    if continuation not in ('pade', 'laplace', 'cd', 'sop'):
         raise NotImplementedError(f'continuation={continuation!r} is outside the device route')
     eps = np.asarray(getattr(mf, 'mo_energy', mf), float)
     nocc = route_kwargs.pop('nocc', None)
@@ -745,7 +745,7 @@ def calc_qp_energy(mf, selfenergy='GW', polarizability='RPA', df=True, eta=None,
     elif consistency != 'g0w0':
         raise NotImplementedError(f'self_consistency={self_consistency!r} is outside the device '
                                   'route')
-    elif continuation in ('laplace', 'cd'):
+    elif continuation in ('laplace', 'cd', 'sop'):
         from .contour import solve_qp_energy_contour
         ev, zs, _ = solve_qp_energy_contour(mf if eps.ndim == 2 else eps, None, nocc,
                                             np.asarray(states), continuation=continuation,

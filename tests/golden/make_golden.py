@@ -64,6 +64,10 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      reference's `solve_qp_equation_scan` returns;
 * contour_follow.npz `qp_energy_cd` following a previous root on the system of
                      contour.npz (Laplace residues): root, Z, branch record
+* sop.npz            the pole model on contour.npz's wc (fitted poles and
+                     amplitudes, Sigma, slope, roots, followed roots), the
+                     compression test, the driver's 'sop' roots, and the
+                     pole-sum root finder on seeded signed and positive sums
 * c1_<variant>.npz   the synthetic FP64 configuration at full size (n_orb = 400,
                      nocc = 40, N_mu = 2400, 16 points, seed 400): the Sigma_c
                      diagonal, every QP root and Z, E_c, and the adjoint
@@ -71,7 +75,7 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      stored: the tests regenerate them from the seed and check
                      the regeneration against the stored eps and checksums.
 
-    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|contour_explicit|contour_unrestricted|sigma_ao|evgw|drop_in|isdf|follow]
+    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|contour_explicit|contour_unrestricted|sigma_ao|evgw|drop_in|isdf|follow|sop]
 """
 import os
 import sys
@@ -963,6 +967,118 @@ def contour_follow_fixture():
                                           'largest_z', 'followed', 'flipped', 'residues']))
 
 
+def sop_fixture(nsums=40, seed=37):
+    """The pole model (GW/sum_over_poles.py) on the contour system's wc (from
+    contour.npz): per state the fitted poles and amplitudes (12 poles at the
+    default stride, 8 poles at stride 1, and 12 log-spaced unfitted),
+    Sigma and its slope at five points, the root and Z, the root followed
+    from 2e-3 away and from the neighbouring interval, with their branch
+    records, and the compression test at the start points; the reference
+    driver's per-state 'sop' roots (`_contour_roots`); and the pole-sum root
+    finder (`solve_qp_equation_poles`) on seeded sums of positive and of
+    mixed-sign weights, unfollowed and following labelled branches."""
+    cd, _ = _import_contour_deformation()
+    from src.SingleReference.GW import sum_over_poles as sp
+    from src.Solvers.qp_equation import solve_qp_equation_poles, qp_start
+    g = np.load(os.path.join(HERE, 'contour.npz'))
+    eps, nocc, nu, nu_w = g['eps'], int(g['nocc']), g['nu'], g['nu_w']
+    states, wcs = g['states'], g['wc']
+    out = {}
+    shifts = np.array([-0.05, -0.01, 0.0, 0.01, 0.05])
+    for tag, kw in (('fit12', dict()), ('fit8s1', dict(n_poles=8, stride=1)),
+                    ('log12', dict(relocate=False))):
+        poles_l, amps_l, sig, slope, roots, fol = [], [], [], [], [], []
+        for i, p in enumerate(states):
+            with warnings.catch_warnings():
+                warnings.simplefilter('ignore')
+                poles, amp = sp.sop_from_wc(wcs[i], nu, eps, nocc, **kw)
+                poles_l.append(poles)
+                amps_l.append(amp)
+                sig.append([sp.sigma_sop(eps[p] + d, amp, poles, eps, nocc, check=False)
+                            for d in shifts])
+                slope.append([sp.sigma_sop_slope(eps[p] + d, amp, poles, eps, nocc)
+                              for d in shifts])
+                br = {}
+                w, z = sp.qp_energy_sop(int(p), amp, poles, eps, nocc, branch=br)
+                roots.append([w, z])
+                lab = br['labels']
+                for follow in ((w + 2e-3, lab), (w + 2e-3, None), (w, (lab[0], None)),
+                               (w - 0.3, None)):
+                    b2 = {}
+                    w2, z2 = sp.qp_energy_sop(int(p), amp, poles, eps, nocc,
+                                              follow=follow, branch=b2)
+                    lg = b2.get('largest')
+                    fol.append([i, follow[0], -2 if follow[1] is None else
+                                (-1 if follow[1][1] is None else 0), w2, z2,
+                                np.nan if lg is None else lg[0],
+                                {None: -1.0, False: 0.0, True: 1.0}[b2.get('followed')],
+                                float(bool(b2.get('flipped')))])
+        npl = max(len(q) for q in poles_l)
+        P = np.full((len(states), npl), np.nan)
+        A = np.full((len(states), npl, len(eps)), np.nan)
+        for i in range(len(states)):
+            P[i, :len(poles_l[i])] = poles_l[i]
+            A[i, :len(poles_l[i])] = amps_l[i]
+        out.update({f'{tag}_poles': P, f'{tag}_amps': A, f'{tag}_sigma': np.array(sig),
+                    f'{tag}_slope': np.array(slope), f'{tag}_roots': np.array(roots),
+                    f'{tag}_follow': np.array(fol, float)})
+    starts = np.array([qp_start(eps, int(p), nocc) for p in states])
+    adm = [sp.compressible(float(w), eps, nocc) for w in starts]
+    out['starts'] = starts
+    out['admits'] = np.array([a[0] for a in adm])
+    out['reach'] = np.array([a[1] for a in adm])
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        r, zz, rec = cd._contour_roots('sop', states, starts, adm, list(g['B']), list(wcs),
+                                       eps, nocc, nu, nu_w, 0.0, sp.SOP_N_POLES,
+                                       sp.SOP_FIT_STRIDE, None)
+    out['driver_roots'] = np.asarray(r, float)
+    out['driver_z'] = np.asarray(zz, float)
+    rng = np.random.default_rng(seed)
+    sums, cases = [], []
+    for k in range(nsums):
+        n = int(rng.integers(4, 30))
+        pol = rng.uniform(-2.0, 2.0, n)
+        num = np.exp(rng.uniform(np.log(1e-5), np.log(0.2), n))
+        if k % 2:
+            neg = rng.random(n) < 0.3
+            num[neg] *= -rng.uniform(0.05, 1.0, int(neg.sum()))
+        if k % 5 == 4:
+            pol[1] = pol[0]                       # coinciding poles
+        a = float(rng.uniform(-0.5, 0.5))
+        sums.append((a, pol, num))
+        with warnings.catch_warnings():
+            warnings.simplefilter('ignore')
+            b = {}
+            w, z = solve_qp_equation_poles(num, pol, a, out=b)
+            lab = b.get('labels')
+            cases.append([k, np.nan, -2, w, z, np.nan, -1.0, 0.0,
+                          np.nan if lab is None or lab[0] is None else lab[0],
+                          np.nan if lab is None or lab[1] is None else lab[1]])
+            for t, labels in ((a + 0.05, None), (float(rng.uniform(-2, 2)), None),
+                              (w + 1e-3, lab)):
+                if labels is not None and not np.isfinite(w):
+                    continue
+                b2 = {}
+                w2, z2 = solve_qp_equation_poles(num, pol, a, follow=(t, labels), out=b2)
+                lg = b2.get('largest')
+                l2 = b2.get('labels')
+                cases.append([k, t, -2 if labels is None else 0, w2, z2,
+                              np.nan if lg is None else lg[0],
+                              {None: -1.0, False: 0.0, True: 1.0}[b2.get('followed')],
+                              float(bool(b2.get('flipped'))),
+                              np.nan if l2 is None or l2[0] is None else l2[0],
+                              np.nan if l2 is None or l2[1] is None else l2[1]])
+    nmax = max(len(q[1]) for q in sums)
+    SP = np.full((nsums, nmax), np.nan)
+    SN = np.zeros((nsums, nmax))
+    for k, (_, pol, num) in enumerate(sums):
+        SP[k, :len(pol)], SN[k, :len(num)] = pol, num
+    out.update(sum_a=np.array([q[0] for q in sums]), sum_poles=SP, sum_nums=SN,
+               sum_cases=np.array(cases, float), shifts=shifts)
+    np.savez_compressed(os.path.join(HERE, 'sop.npz'), **out)
+
+
 if __name__ == '__main__':
     if ONLY == 'c1':
         c1_fixture('literal')
@@ -1009,6 +1125,10 @@ if __name__ == '__main__':
         contour_unrestricted_fixture()
         print('unrestricted contour fixture written to', HERE)
         sys.exit(0)
+    if ONLY == 'sop':
+        sop_fixture()
+        print('pole-model fixture written to', HERE)
+        sys.exit(0)
     if ONLY == 'follow':
         follow_fixture()
         contour_follow_fixture()
@@ -1016,8 +1136,8 @@ if __name__ == '__main__':
         sys.exit(0)
     if ONLY:
         sys.exit(f'--only {ONLY}: choose c1, static, unrestricted, sigma_adjoint, contour, '
-                 'contour_explicit, contour_unrestricted, sigma_ao, evgw, drop_in, isdf or '
-                 'follow')
+                 'contour_explicit, contour_unrestricted, sigma_ao, evgw, drop_in, isdf, '
+                 'follow or sop')
     grids_fixture()
     shared_kernel_fixture()
     route_fixture('calibrated', 24, 4, 64, 7, 'calibrated', 12, full=True)

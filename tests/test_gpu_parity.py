@@ -590,9 +590,11 @@ def test_contour_deformation_device_matches_reference_golden(golden):
     assert np.abs(ev / contour.HARTREE_TO_EV - g['roots'][:, 0]).max() < 1e-9
     assert np.abs(zs - g['roots'][:, 1]).max() < 1e-8
     assert info['continuation'] == 'laplace' and len(info['states']) == 3
-    with pytest.raises(NotImplementedError):
-        contour.solve_qp_energy_contour(eps, None, nocc, g['states'], continuation='sop',
-                                        factors=(X, D))
+    # the pole model through the same driver: the reference driver's 'sop' roots
+    ev, zs, info = contour.solve_qp_energy_contour(eps, None, nocc, g['states'],
+                                                   continuation='sop', factors=(X, D))
+    assert np.abs(ev / contour.HARTREE_TO_EV - golden('sop')['driver_roots']).max() < 1e-8
+    assert info['continuation'] == 'sop'
 
 
 def test_contour_explicit_backend_matches_reference_golden(golden):
@@ -939,3 +941,27 @@ def test_contour_root_following_matches_reference_golden(golden):
         assert float(out['flipped']) == row[col['flipped']]
         assert len(res) == int(row[col['residues']])
         assert abs(out['largest'][0] - row[col['largest_w']]) < 1e-9
+
+
+def test_contour_pole_model_route_matches_reference_golden(golden):
+    """continuation='sop' from the factors on the device (proj(tau), the
+    slices, W on the contour's frequencies and the screening contraction),
+    each state's pole model fitted to its wc and solved in closed form,
+    against the reference driver's roots and Z (`sop.npz`); a state the
+    compression test excludes (orbital 9, reach 1.45 gaps) is refused by
+    name before anything is built."""
+    import warnings
+    from mbptcode_b200 import contour
+    g = golden('contour')
+    s = golden('sop')
+    eps, nocc, mu = g['eps'], int(g['nocc']), float(g['mu'])
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        roots, zs, info = contour.contour_roots(g['X'], g['D'], eps, nocc, g['states'],
+                                                mu=mu, continuation='sop')
+    assert np.abs(roots - s['driver_roots']).max() < 1e-8
+    assert np.abs(zs - s['driver_z']).max() < 1e-7
+    assert info['residue_route_taken'] == 'sop'
+    assert [r['sop_admits'] for r in info['states']] == list(s['admits'])
+    with pytest.raises(ValueError, match="continuation='sop' cannot serve orbital 9"):
+        contour.contour_roots(g['X'], g['D'], eps, nocc, [9], mu=mu, continuation='sop')
