@@ -1866,13 +1866,17 @@ def qp_gradient_space_time(X, D, eps, nocc, grid, nu_points, nu_weights, p, *,
     the last accepted geometry kept ({p: (w, labels)}), and the reference
     roots' Z ({p: Z}, whether a weak followed root's window is rescanned);
     route_out receives 'residue_route', 'residues', 'weights', 'roots',
-    'labels', 'branches' and 'sop_poles'."""
-    if residue_route != 'laplace':
+    'labels', 'branches' and 'sop_poles'. residue_route 'sop': the root on
+    the state's pole model (n_poles fitted to wc at sop_stride, or the
+    frozen poles sop_poles[p] of a reference geometry), differentiated at
+    fixed poles, where the amplitudes A = F^+ wc are linear in wc: the
+    adjoint on wc is Z (F^+)^T (1/D)^T and takes the integral term's chain
+    (``gradients/gwbse/sum_over_poles_adjoint.py:24-47``); no residues."""
+    if residue_route not in ('laplace', 'sop'):
         raise NotImplementedError(f'residue_route={residue_route!r}: the device route serves '
-                                  "'laplace' (the cubic residues)")
-    if any(v is not None for v in (scissor, sop_poles, comm)):
-        raise NotImplementedError('scissors, pole models and rank splits are outside the '
-                                  'device route')
+                                  "'laplace' (the cubic residues) and 'sop' (the pole model)")
+    if any(v is not None for v in (scissor, comm)):
+        raise NotImplementedError('scissors and rank splits are outside the device route')
     dev = require_device()
     eps_h = _eps_host(eps)
     p = int(p)
@@ -1882,26 +1886,48 @@ def qp_gradient_space_time(X, D, eps, nocc, grid, nu_points, nu_weights, p, *,
     wmi, _ = screening_minus_identity(proj, grid.cosft_wt)
     B = three_index_slices(X, D, [p])[0]
     wc = screening_contraction_device(wmi, [B])[0]
-    lap = LaplaceRealScreening(proj, grid, eps_h, nocc, tol=laplace_tol)
     followed, branch = _followed_branch(follow, w0, p), {}
-    w, z, res = qp_energy_cd(p, B, eps_h, nocc, nu_points, nu_weights,
-                             xc_correction=xc_correction, tol=tol, wc=wc, real_screening=lap,
-                             follow=followed, branch=branch, rescan=_rescans_beside(z0, p))
+    if residue_route == 'sop':
+        from . import sum_over_poles as sop
+        wc_h = wc.cpu().numpy()
+        frozen = None if sop_poles is None else sop_poles.get(p)
+        if frozen is None:
+            poles, amp = sop.sop_from_wc(wc_h, nu_points, eps_h, nocc,
+                                         n_poles=n_poles or sop.SOP_N_POLES,
+                                         stride=(sop.SOP_FIT_STRIDE if sop_stride is None
+                                                 else sop_stride), state=p)
+        else:
+            poles = np.asarray(frozen, float)
+            amp = sop.pole_amplitudes(wc_h, poles, nu_points)
+        w, z = sop.qp_energy_sop(p, amp, poles, eps_h, nocc, xc_correction=xc_correction,
+                                 tol=tol, follow=followed, branch=branch)
+        res = []
+    else:
+        lap = LaplaceRealScreening(proj, grid, eps_h, nocc, tol=laplace_tol)
+        w, z, res = qp_energy_cd(p, B, eps_h, nocc, nu_points, nu_weights,
+                                 xc_correction=xc_correction, tol=tol, wc=wc, real_screening=lap,
+                                 follow=followed, branch=branch, rescan=_rescans_beside(z0, p))
     if route_out is not None:
-        route_out.update(residue_route='laplace', residues=res, weights={p: float(z)},
+        route_out.update(residue_route=residue_route, residues=res, weights={p: float(z)},
                          roots={p: float(w)}, labels={p: branch.get('labels')},
                          branches={p: branch} if followed is not None else {},
-                         sop_poles={})
+                         sop_poles={p: poles} if residue_route == 'sop' else {})
     if not want_grad:
         return w, z
     naux, norb = B.shape
     eps_bar = np.zeros(norb)
     eps_bar[p] += z
-    c, dc = cd_integral_weights(w - eps_h, nu_points, nu_weights)
-    coeff = -z / np.pi
-    wc_h = wc.cpu().numpy()
-    eps_bar += -coeff * np.einsum('kq,kq->q', wc_h, dc)
-    wc_bar = torch.as_tensor(coeff * c, dtype=torch.float64, device=dev)
+    if residue_route == 'sop':
+        den = sop.denominators(w, poles, eps_h, nocc)              # (norb, M)
+        eps_bar += z * np.sum(amp.T / (den * den), axis=1)
+        wc_bar = torch.as_tensor(z * (sop.pole_pseudoinverse(nu_points, poles).T @ (1.0 / den).T),
+                                 dtype=torch.float64, device=dev)
+    else:
+        c, dc = cd_integral_weights(w - eps_h, nu_points, nu_weights)
+        coeff = -z / np.pi
+        wc_h = wc.cpu().numpy()
+        eps_bar += -coeff * np.einsum('kq,kq->q', wc_h, dc)
+        wc_bar = torch.as_tensor(coeff * c, dtype=torch.float64, device=dev)
     B_bar = torch.zeros_like(B)
     W_bar = torch.empty_like(wmi)
     ws = WORKSPACE.get(lib().mbpt_cd_integral_backward_workspace_bytes(naux, norb), dev)

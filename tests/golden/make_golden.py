@@ -1034,6 +1034,21 @@ def sop_fixture(nsums=40, seed=37):
                                        sp.SOP_FIT_STRIDE, None)
     out['driver_roots'] = np.asarray(r, float)
     out['driver_z'] = np.asarray(zz, float)
+    # the QP gradient on the pole model's route (poles fitted here, then held)
+    from src.gradients.gwbse.qp_space_time import qp_gradient_space_time
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        grid = cd.cd_frequency_grid(eps, nocc)[2]
+        grads = []
+        for p in states:
+            rec = {}
+            grads.append(qp_gradient_space_time(g['X'], g['D'], eps, nocc, grid, nu, nu_w,
+                                                int(p), residue_route='sop',
+                                                mu=float(g['mu']), route_out=rec))
+    out['grad_roots'] = np.array([[gr[0], gr[1]] for gr in grads])
+    out['grad_eps_bar'] = np.stack([gr[2] for gr in grads])
+    out['grad_X_bar'] = np.stack([gr[3] for gr in grads])
+    out['grad_D_bar'] = np.stack([gr[4] for gr in grads])
     rng = np.random.default_rng(seed)
     sums, cases = [], []
     for k in range(nsums):

@@ -965,3 +965,33 @@ def test_contour_pole_model_route_matches_reference_golden(golden):
     assert [r['sop_admits'] for r in info['states']] == list(s['admits'])
     with pytest.raises(ValueError, match="continuation='sop' cannot serve orbital 9"):
         contour.contour_roots(g['X'], g['D'], eps, nocc, [9], mu=mu, continuation='sop')
+
+
+def test_contour_pole_model_gradient_matches_reference_golden(golden):
+    """The QP energy and its gradient in (eps, X, D) on the pole model's route
+    (residue_route 'sop': poles fitted to wc, then held; the adjoint on wc
+    through the integral term's chain, no residues) against the reference's
+    qp_gradient_space_time for the three states (`sop.npz`), 1e-8 of each
+    adjoint's scale; the same with the fitted poles handed back frozen."""
+    import warnings
+    from mbptcode_b200 import contour
+    g = golden('contour')
+    s = golden('sop')
+    eps, nocc, mu = g['eps'], int(g['nocc']), float(g['mu'])
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        nu, nu_w, grid, _ = contour.cd_frequency_grid(eps, nocc)
+    for i, p in enumerate(g['states']):
+        rec = {}
+        w, z, eb, xb, db = contour.qp_gradient_space_time(
+            g['X'], g['D'], eps, nocc, grid, nu, nu_w, int(p), residue_route='sop', mu=mu,
+            route_out=rec)
+        assert abs(w - s['grad_roots'][i, 0]) < 1e-9 and abs(z - s['grad_roots'][i, 1]) < 1e-8
+        for a, k in ((eb, 'grad_eps_bar'), (xb, 'grad_X_bar'), (db, 'grad_D_bar')):
+            ref = s[k][i]
+            assert np.abs(a - ref).max() <= 1e-8 * np.abs(ref).max(), (int(p), k)
+        assert rec['residue_route'] == 'sop' and rec['residues'] == []
+        w2, z2, _, _, db2 = contour.qp_gradient_space_time(
+            g['X'], g['D'], eps, nocc, grid, nu, nu_w, int(p), residue_route='sop', mu=mu,
+            sop_poles={int(p): rec['sop_poles'][int(p)]})
+        assert w2 == w and z2 == z and np.abs(db2 - db).max() <= 1e-12 * np.abs(db).max()
