@@ -20,7 +20,7 @@ namespace umma {
 
 constexpr int BM = 128;
 constexpr int BK = 64;  // BF16 elements per 128-byte swizzle row
-constexpr int kGroupM = 8;
+constexpr int kGroupM = 16;
 
 enum Epi : int {
   EPI_SPLIT = 0,           // out0 = alpha * acc0, BF16 hi/lo
