@@ -1816,6 +1816,37 @@ def _slice_backward(X, D, p, B_bar, X_bar, D_bar):
           'mbpt_three_index_slice_backward')
 
 
+def _explicit_residue_backward(X, D, eps, nocc, pushes, X_bar, D_bar):
+    """The explicit residues' share of (eps_bar, X_bar, D_bar): each residue
+    at real frequency f puts c y y^T on chi0(f) = 2 C diag(fac) C^T, C[:, (i,a)]
+    = D^T (x_i o x_a), so C_bar = y g^T with g = 4 c fac o (C^T y) -- rank one
+    -- and the chain to (X, D) needs C^T y = X_o^T diag(D y) X_v alone:
+    D_bar += u y^T with u = rowsum(X_o o (X_v G^T)), X_bar[:, occ] +=
+    diag(D y) X_v G^T, X_bar[:, virt] += diag(D y) X_o G, and fac's slope in
+    the pair energies gives eps (``gradients/gwbse/contour_deformation_adjoint.py:
+    52-77, 149-166``, three_index_ov's reverse; C_bar never formed). X_bar and
+    D_bar are added to in place; returns the eps adjoint (host)."""
+    dev = X_bar.device
+    Xd, Dd = to_device(X, dev), to_device(D, dev)
+    Xo, Xv = Xd[:, :nocc], Xd[:, nocc:]
+    dpair = (eps[nocc:][None, :] - eps[:nocc][:, None])
+    eps_bar = np.zeros(len(eps))
+    for f, y, c in pushes:
+        Dy = Dd @ y
+        t = (Xo * Dy[:, None]).T @ Xv                        # C^T y, (nocc, nvirt)
+        fac, dfac, _ = frequency_factor(dpair, f, False, slopes=True)
+        th = t.cpu().numpy()
+        d_bar = 2.0 * c * th * th * dfac
+        eps_bar[nocc:] += d_bar.sum(axis=0)
+        eps_bar[:nocc] -= d_bar.sum(axis=1)
+        G = torch.as_tensor(4.0 * c * fac, device=dev) * t
+        XvG = Xv @ G.T                                       # (M, nocc)
+        D_bar += torch.outer((Xo * XvG).sum(dim=1), y)
+        X_bar[:, :nocc] += Dy[:, None] * XvG
+        X_bar[:, nocc:] += Dy[:, None] * (Xo @ G)
+    return eps_bar
+
+
 def _frozen_root(w0, p):
     """The root a reference geometry kept for orbital p: w0 a number or a
     mapping orbital -> root; None before one is kept
@@ -1854,8 +1885,10 @@ def qp_gradient_space_time(X, D, eps, nocc, grid, nu_points, nu_weights, p, *,
     """(eps^QP_p, Z, eps_bar, X_bar, D_bar), or (eps^QP_p, Z) with want_grad
     False: the contour-deformation QP energy of state p and its gradient in
     (eps, X, D) (``gradients/gwbse/qp_space_time.py:412-452``), residues by
-    the cosh transform of proj(tau) on `grid` (the contour's time grid, mu
-    frozen). The root is differentiated implicitly, d eps^QP = Z [d eps_p +
+    the cosh transform of proj(tau) on `grid` (residue_route 'laplace'; the
+    contour's time grid, mu frozen) or from C_ov ('explicit': each residue's
+    rank-one adjoint on chi0 taken back to (eps, X, D) through C_ov's
+    definition without forming its adjoint). The root is differentiated implicitly, d eps^QP = Z [d eps_p +
     dSigma^c(w)|_w], the residue set frozen at the root: the integral term's
     adjoint goes to the slice, to W(i nu) (then W W_bar W onto chi0 and
     proj(tau)) and to eps through its weights; each residue's to the slice,
@@ -1872,9 +1905,10 @@ def qp_gradient_space_time(X, D, eps, nocc, grid, nu_points, nu_weights, p, *,
     fixed poles, where the amplitudes A = F^+ wc are linear in wc: the
     adjoint on wc is Z (F^+)^T (1/D)^T and takes the integral term's chain
     (``gradients/gwbse/sum_over_poles_adjoint.py:24-47``); no residues."""
-    if residue_route not in ('laplace', 'sop'):
+    if residue_route not in ('laplace', 'explicit', 'sop'):
         raise NotImplementedError(f'residue_route={residue_route!r}: the device route serves '
-                                  "'laplace' (the cubic residues) and 'sop' (the pole model)")
+                                  "'laplace' (the cubic residues), 'explicit' (C_ov) and 'sop' "
+                                  '(the pole model)')
     if any(v is not None for v in (scissor, comm)):
         raise NotImplementedError('scissors and rank splits are outside the device route')
     dev = require_device()
@@ -1903,7 +1937,9 @@ def qp_gradient_space_time(X, D, eps, nocc, grid, nu_points, nu_weights, p, *,
                                  tol=tol, follow=followed, branch=branch)
         res = []
     else:
-        lap = LaplaceRealScreening(proj, grid, eps_h, nocc, tol=laplace_tol)
+        lap = (LaplaceRealScreening(proj, grid, eps_h, nocc, tol=laplace_tol)
+               if residue_route == 'laplace' else
+               ExplicitRealScreening(three_index_ov(X, D, eps_h, nocc), eps_h, nocc))
         w, z, res = qp_energy_cd(p, B, eps_h, nocc, nu_points, nu_weights,
                                  xc_correction=xc_correction, tol=tol, wc=wc, real_screening=lap,
                                  follow=followed, branch=branch, rescan=_rescans_beside(z0, p))
@@ -1946,18 +1982,23 @@ def qp_gradient_space_time(X, D, eps, nocc, grid, nu_points, nu_weights, p, *,
         transform(W_bar[k0:k0 + _MAX_J].contiguous(), np.ascontiguousarray(cw_t[:, k0:k0 + _MAX_J]),
                   out=proj_bar, accumulate=True)
     del W_bar
-    tau = np.asarray(grid.tau_points, float)
+    explicit_push = []
     for q, wt in res:
         f = abs(eps_h[q] - w)
-        cf, _ = real_frequency_weights(grid, f)
         b = B[:, q]
         y = lap.apply(f, b)
         B_bar[:, q] += (z * wt * 2.0) * (y - b)
-        proj_bar += torch.as_tensor(z * wt * cf, device=dev)[:, None, None] * torch.outer(y, y)[None]
+        if residue_route == 'laplace':
+            cf, _ = real_frequency_weights(grid, f)
+            proj_bar += (torch.as_tensor(z * wt * cf, device=dev)[:, None, None]
+                         * torch.outer(y, y)[None])
+        else:
+            explicit_push.append((f, y, z * wt))
         eps_bar[q] += z * wt * lap.slope(f, y) * np.sign(eps_h[q] - w)
-    del tau
     from .adjoint import chi0_backward
     e2, X_bar, D_bar = chi0_backward(proj_bar, X, D, eps_h, nocc, grid.tau_points, mu)
+    if explicit_push:
+        eps_bar += _explicit_residue_backward(X, D, eps_h, nocc, explicit_push, X_bar, D_bar)
     _slice_backward(X, D, p, B_bar, X_bar, D_bar)
     eps_bar = eps_bar + e2.cpu().numpy()
     if isinstance(X, torch.Tensor):

@@ -64,6 +64,8 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      reference's `solve_qp_equation_scan` returns;
 * contour_follow.npz `qp_energy_cd` following a previous root on the system of
                      contour.npz (Laplace residues): root, Z, branch record
+* contour_grad_explicit.npz  the QP gradient on the explicit residue route
+                     (residues from C_ov) for orbitals 1-4 of contour.npz's system
 * sop.npz            the pole model on contour.npz's wc (fitted poles and
                      amplitudes, Sigma, slope, roots, followed roots), the
                      compression test, the driver's 'sop' roots, and the
@@ -75,7 +77,7 @@ Each fixture stores the inputs (seeded) and the reference's outputs for them:
                      stored: the tests regenerate them from the seed and check
                      the regeneration against the stored eps and checksums.
 
-    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|contour_explicit|contour_unrestricted|sigma_ao|evgw|drop_in|isdf|follow|sop]
+    python tests/golden/make_golden.py [/root/reference] [--only c1|static|unrestricted|sigma_adjoint|contour|contour_explicit|contour_unrestricted|sigma_ao|evgw|drop_in|isdf|follow|sop|grad_explicit]
 """
 import os
 import sys
@@ -1094,6 +1096,34 @@ def sop_fixture(nsums=40, seed=37):
     np.savez_compressed(os.path.join(HERE, 'sop.npz'), **out)
 
 
+def contour_grad_explicit_fixture():
+    """The QP gradient on the explicit residue route (residue_route 'explicit':
+    residues from C_ov, their adjoint chained onto (C_ov, d) and back to
+    (eps, X, D) by three_index_ov's reverse) on the contour system, for
+    orbitals 1 to 4 (orbital 1 sweeps residues above the gap)."""
+    cd, _ = _import_contour_deformation()
+    from src.gradients.gwbse.qp_space_time import qp_gradient_space_time
+    g = np.load(os.path.join(HERE, 'contour.npz'))
+    eps, nocc, mu = g['eps'], int(g['nocc']), float(g['mu'])
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        nu, nu_w, grid, _ = cd.cd_frequency_grid(eps, nocc)
+        states = np.array([1, 2, 3, 4])
+        grads, nres = [], []
+        for p in states:
+            rec = {}
+            grads.append(qp_gradient_space_time(g['X'], g['D'], eps, nocc, grid, nu, nu_w,
+                                                int(p), residue_route='explicit', mu=mu,
+                                                route_out=rec))
+            nres.append(len(rec['residues']))
+    np.savez_compressed(os.path.join(HERE, 'contour_grad_explicit.npz'), states=states,
+                        residues=np.array(nres),
+                        roots=np.array([[gr[0], gr[1]] for gr in grads]),
+                        eps_bar=np.stack([gr[2] for gr in grads]),
+                        X_bar=np.stack([gr[3] for gr in grads]),
+                        D_bar=np.stack([gr[4] for gr in grads]))
+
+
 if __name__ == '__main__':
     if ONLY == 'c1':
         c1_fixture('literal')
@@ -1140,6 +1170,10 @@ if __name__ == '__main__':
         contour_unrestricted_fixture()
         print('unrestricted contour fixture written to', HERE)
         sys.exit(0)
+    if ONLY == 'grad_explicit':
+        contour_grad_explicit_fixture()
+        print('explicit-route gradient fixture written to', HERE)
+        sys.exit(0)
     if ONLY == 'sop':
         sop_fixture()
         print('pole-model fixture written to', HERE)
@@ -1152,7 +1186,7 @@ if __name__ == '__main__':
     if ONLY:
         sys.exit(f'--only {ONLY}: choose c1, static, unrestricted, sigma_adjoint, contour, '
                  'contour_explicit, contour_unrestricted, sigma_ao, evgw, drop_in, isdf, '
-                 'follow or sop')
+                 'follow, sop or grad_explicit')
     grids_fixture()
     shared_kernel_fixture()
     route_fixture('calibrated', 24, 4, 64, 7, 'calibrated', 12, full=True)

@@ -995,3 +995,29 @@ def test_contour_pole_model_gradient_matches_reference_golden(golden):
             g['X'], g['D'], eps, nocc, grid, nu, nu_w, int(p), residue_route='sop', mu=mu,
             sop_poles={int(p): rec['sop_poles'][int(p)]})
         assert w2 == w and z2 == z and np.abs(db2 - db).max() <= 1e-12 * np.abs(db).max()
+
+
+def test_contour_explicit_route_gradient_matches_reference_golden(golden):
+    """The QP gradient on the explicit residue route (the residues' W from
+    C_ov; their rank-one adjoint taken back to (eps, X, D) without forming
+    C_ov's adjoint) for orbitals 1-4, orbital 1 with two residues, against
+    the reference's qp_gradient_space_time (`contour_grad_explicit.npz`):
+    roots 1e-9, Z 1e-8, adjoints 1e-8 of their scale."""
+    import warnings
+    from mbptcode_b200 import contour
+    g = golden('contour')
+    e = golden('contour_grad_explicit')
+    eps, nocc, mu = g['eps'], int(g['nocc']), float(g['mu'])
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        nu, nu_w, grid, _ = contour.cd_frequency_grid(eps, nocc)
+    for i, p in enumerate(e['states']):
+        rec = {}
+        w, z, eb, xb, db = contour.qp_gradient_space_time(
+            g['X'], g['D'], eps, nocc, grid, nu, nu_w, int(p), residue_route='explicit', mu=mu,
+            route_out=rec)
+        assert len(rec['residues']) == int(e['residues'][i])
+        assert abs(w - e['roots'][i, 0]) < 1e-9 and abs(z - e['roots'][i, 1]) < 1e-8, int(p)
+        for a, k in ((eb, 'eps_bar'), (xb, 'X_bar'), (db, 'D_bar')):
+            ref = e[k][i]
+            assert np.abs(a - ref).max() <= 1e-8 * np.abs(ref).max(), (int(p), k)
