@@ -1847,6 +1847,47 @@ def _explicit_residue_backward(X, D, eps, nocc, pushes, X_bar, D_bar):
     return eps_bar
 
 
+EXPLICIT_RESIDUE_MAX_GB = 256.0   # MBPTcode src/Base/numerics/constants.py:1261
+
+
+def _gradient_route(residue_route, scissor, p, eps, nocc, w0, sop_poles, naux):
+    """(route, shift) of orbital p in the QP gradient
+    (``gradients/gwbse/qp_space_time.py:162-217``, ``GW/qp_states.py:
+    323-338``): 'sop' keeps the pole model for a state the compression test
+    admits at its start (the frozen root, else eps_p moved toward the
+    chemical potential) or that sop_poles froze onto it; a frozen scissor
+    shift (a mapping per orbital, or one number for the states the test
+    excludes) takes 'scissor'; any other falls back to 'explicit' where C_ov
+    fits in EXPLICIT_RESIDUE_MAX_GB, else 'laplace'. Other routes as asked."""
+    if residue_route != 'sop':
+        return residue_route, None
+    from . import sum_over_poles as sop
+    root = _frozen_root(w0, p)
+    start = sop.qp_start(eps, p, nocc) if root is None else root
+    shift = None
+    if scissor is not None and not isinstance(scissor, str):
+        shift = (scissor.get(int(p)) if isinstance(scissor, dict) else float(scissor))
+        shift = None if shift is None else float(shift)
+    if isinstance(scissor, dict):
+        route = 'scissor' if shift is not None else 'sop'
+    elif shift is not None and not isinstance(scissor, str) and \
+            not sop.compressible(start, eps, nocc)[0]:
+        route = 'scissor'
+    else:
+        route = 'sop'
+    if isinstance(sop_poles, dict) and sop_poles.get(int(p)) is not None:
+        admitted = True
+    elif isinstance(w0, dict) and w0.get(int(p)) is not None:
+        admitted = False
+    else:
+        admitted = sop.compressible(start, eps, nocc)[0]
+    if route == 'sop' and not admitted:
+        nvir = len(eps) - nocc
+        route = ('explicit' if naux * nocc * nvir * 8 / 1e9 <= EXPLICIT_RESIDUE_MAX_GB
+                 else 'laplace')
+    return route, shift
+
+
 def _frozen_root(w0, p):
     """The root a reference geometry kept for orbital p: w0 a number or a
     mapping orbital -> root; None before one is kept
@@ -1909,8 +1950,8 @@ def qp_gradient_space_time(X, D, eps, nocc, grid, nu_points, nu_weights, p, *,
         raise NotImplementedError(f'residue_route={residue_route!r}: the device route serves '
                                   "'laplace' (the cubic residues), 'explicit' (C_ov) and 'sop' "
                                   '(the pole model)')
-    if any(v is not None for v in (scissor, comm)):
-        raise NotImplementedError('scissors and rank splits are outside the device route')
+    if comm is not None:
+        raise NotImplementedError('rank splits are outside the one-GPU route')
     dev = require_device()
     eps_h = _eps_host(eps)
     p = int(p)
@@ -1921,6 +1962,22 @@ def qp_gradient_space_time(X, D, eps, nocc, grid, nu_points, nu_weights, p, *,
     B = three_index_slices(X, D, [p])[0]
     wc = screening_contraction_device(wmi, [B])[0]
     followed, branch = _followed_branch(follow, w0, p), {}
+    residue_route, shift = _gradient_route(residue_route, scissor, p, eps_h, nocc, w0,
+                                           sop_poles, B.shape[0])
+    if residue_route == 'scissor':
+        # a frozen shift: the root moves with eps_p alone
+        w, z = float(eps_h[p] + xc_correction + shift), 1.0
+        if route_out is not None:
+            route_out.update(residue_route='scissor', residues=[], weights={p: z},
+                             roots={p: w}, labels={p: None}, branches={}, sop_poles={})
+        if not want_grad:
+            return w, z
+        eps_bar = np.zeros(len(eps_h))
+        eps_bar[p] = z
+        if isinstance(X, torch.Tensor):
+            return (w, z, torch.as_tensor(eps_bar, device=dev),
+                    torch.zeros_like(to_device(X, dev)), torch.zeros_like(to_device(D, dev)))
+        return w, z, eps_bar, np.zeros(np.shape(X)), np.zeros(np.shape(D))
     if residue_route == 'sop':
         from . import sum_over_poles as sop
         wc_h = wc.cpu().numpy()

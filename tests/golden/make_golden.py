@@ -1116,8 +1116,26 @@ def contour_grad_explicit_fixture():
                                                 int(p), residue_route='explicit', mu=mu,
                                                 route_out=rec))
             nres.append(len(rec['residues']))
+    # the pole-model route's decisions: orbital 9 (reach 1.45 gaps) falls back
+    # to the explicit residues; a frozen scissor mapping, or a scalar where the
+    # compression test fails, shifts it; orbital 2 keeps the pole model
+    route_cases = [(9, None), (9, {9: 0.05}), (9, 0.07), (2, 0.07)]
+    route_out = []
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        for p, sc in route_cases:
+            rec = {}
+            gr = qp_gradient_space_time(g['X'], g['D'], eps, nocc, grid, nu, nu_w, p,
+                                        residue_route='sop', mu=mu, scissor=sc, route_out=rec)
+            route_out.append((rec['residue_route'], gr))
+    extra = {}
+    for j, (route, gr) in enumerate(route_out):
+        extra[f'route{j}_name'] = np.array(route)
+        extra[f'route{j}_root'] = np.array([gr[0], gr[1]])
+        extra[f'route{j}_eps_bar'] = np.asarray(gr[2])
+        extra[f'route{j}_D_bar'] = np.asarray(gr[4])
     np.savez_compressed(os.path.join(HERE, 'contour_grad_explicit.npz'), states=states,
-                        residues=np.array(nres),
+                        **extra, residues=np.array(nres),
                         roots=np.array([[gr[0], gr[1]] for gr in grads]),
                         eps_bar=np.stack([gr[2] for gr in grads]),
                         X_bar=np.stack([gr[3] for gr in grads]),

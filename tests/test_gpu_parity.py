@@ -1021,3 +1021,30 @@ def test_contour_explicit_route_gradient_matches_reference_golden(golden):
         for a, k in ((eb, 'eps_bar'), (xb, 'X_bar'), (db, 'D_bar')):
             ref = e[k][i]
             assert np.abs(a - ref).max() <= 1e-8 * np.abs(ref).max(), (int(p), k)
+
+
+def test_contour_pole_route_decisions_match_reference_golden(golden):
+    """residue_route 'sop' decides per state as the reference does: orbital 9
+    (reach 1.45 gaps) falls back to the explicit residues, a frozen scissor
+    mapping or a scalar shift where the compression test fails takes the
+    shifted root (Z = 1, no adjoint on the factors), orbital 2 keeps the pole
+    model; roots, eps_bar and D_bar against the reference's."""
+    import warnings
+    from mbptcode_b200 import contour
+    g = golden('contour')
+    e = golden('contour_grad_explicit')
+    eps, nocc, mu = g['eps'], int(g['nocc']), float(g['mu'])
+    with warnings.catch_warnings():
+        warnings.simplefilter('ignore')
+        nu, nu_w, grid, _ = contour.cd_frequency_grid(eps, nocc)
+    for j, (p, sc) in enumerate([(9, None), (9, {9: 0.05}), (9, 0.07), (2, 0.07)]):
+        rec = {}
+        w, z, eb, _, db = contour.qp_gradient_space_time(
+            g['X'], g['D'], eps, nocc, grid, nu, nu_w, p, residue_route='sop', mu=mu,
+            scissor=sc, route_out=rec)
+        assert rec['residue_route'] == str(e[f'route{j}_name']), (p, sc)
+        root = e[f'route{j}_root']
+        assert abs(w - root[0]) < 1e-9 and abs(z - root[1]) < 1e-8, (p, sc)
+        for a, k in ((eb, f'route{j}_eps_bar'), (db, f'route{j}_D_bar')):
+            ref = e[k]
+            assert np.abs(a - ref).max() <= 1e-8 * max(np.abs(ref).max(), 1e-300), (p, sc, k)
