@@ -1,6 +1,7 @@
 // Host side of the tcgen05 split GEMM engine: TMA tensor maps and launches.
 #include <cudaTypedefs.h>
 #include <atomic>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -62,10 +63,13 @@ bool make_tmap(CUtensorMap *m, const void *base, int64_t rows, int64_t cols, int
   return r == CUDA_SUCCESS;
 }
 
-template <int NACC, int BN, int EPI, bool TF32, int DRAIN>
+// CTAS = 2: clusters of two CTAs per 256 x BN tile (cta_group::2); dense K
+// (no K-band flags) only.
+template <int NACC, int BN, int EPI, bool TF32, int DRAIN, int CTAS = 1>
 int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
            const umma::EpiArgs &e, int *err, cudaStream_t st, int band = 0) {
-  using L = umma::Layout<NACC, BN, (DRAIN > 0)>;
+  using L = umma::Layout<NACC, BN, (DRAIN > 0), CTAS>;
+  if (CTAS == 2 && (band & ~umma::BAND_UPPER)) return MBPT_ERR_UNSUPPORTED;
   // the last column tile may overhang a multiple of 128 (BN = 256): its
   // B rows read as zeros and its dead columns are not stored
   if (m_rows % umma::BM || n_rows % 128 || m_rows <= 0 || n_rows <= 0) return MBPT_ERR_SHAPE;
@@ -77,28 +81,56 @@ int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
       return MBPT_ERR_SHAPE;
     if (!make_tmap(&p.tm[4 * j + 0], A[j].hi, A[j].rows, A[j].cols, A[j].ld, umma::BM, TF32) ||
         !make_tmap(&p.tm[4 * j + 1], A[j].lo, A[j].rows, A[j].cols, A[j].ld, umma::BM, TF32) ||
-        !make_tmap(&p.tm[4 * j + 2], B[j].hi, B[j].rows, B[j].cols, B[j].ld, BN, TF32) ||
-        !make_tmap(&p.tm[4 * j + 3], B[j].lo, B[j].rows, B[j].cols, B[j].ld, BN, TF32))
+        !make_tmap(&p.tm[4 * j + 2], B[j].hi, B[j].rows, B[j].cols, B[j].ld, BN / CTAS,
+                   TF32) ||
+        !make_tmap(&p.tm[4 * j + 3], B[j].lo, B[j].rows, B[j].cols, B[j].ld, BN / CTAS, TF32))
       return MBPT_ERR_SHAPE;
     p.k_tiles[j] = static_cast<int>(A[j].cols / bk);
   }
   p.tiles_m = static_cast<int>(m_rows / umma::BM);
   p.tiles_n = static_cast<int>((n_rows + BN - 1) / BN);
   p.n_valid = static_cast<int>(n_rows);
+  p.m_valid = static_cast<int>(m_rows);
   p.band = band;
   p.ngroups = 0;
   p.epi = e;
   p.err = err;
-  auto kern = umma::gemm_split_kernel<NACC, BN, EPI, TF32, DRAIN>;
+  auto kern = umma::gemm_split_kernel<NACC, BN, EPI, TF32, DRAIN, 0, CTAS>;
   static std::atomic<uint64_t> attr_set{0};  // one bit per device
   if (!allow_smem(reinterpret_cast<const void *>(kern), L::kSmemBytes, attr_set))
     return MBPT_ERR_CUDA;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   const bool timed = timing_begin(st, &ev0, &ev1);
   count_launch();
-  kern<<<p.tiles_m * p.tiles_n, 64 + BN, L::kSmemBytes, st>>>(p);
-  if (timed) timing_end(st, EPI, ev0, ev1);
-  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+  if constexpr (CTAS == 2) {
+    // a pair per 256-row unit; an odd last row tile pairs with rows past the
+    // end (zero operands, nothing stored)
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(static_cast<unsigned>(2 * ((p.tiles_m + 1) / 2) * p.tiles_n));
+    cfg.blockDim = dim3(64 + BN);
+    cfg.dynamicSmemBytes = L::kSmemBytes;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const cudaError_t rc = cudaLaunchKernelEx(&cfg, kern, p);
+    if (timed) timing_end(st, EPI, ev0, ev1);
+    return rc == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+  } else {
+    kern<<<p.tiles_m * p.tiles_n, 64 + BN, L::kSmemBytes, st>>>(p);
+    if (timed) timing_end(st, EPI, ev0, ev1);
+    return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+  }
+}
+
+// The 256-wide BF16 products run as CTA pairs unless MBPT_ENGINE_PAIRS=0.
+bool engine_pairs() {
+  const char *v = std::getenv("MBPT_ENGINE_PAIRS");
+  return !(v && v[0] == '0');
 }
 
 constexpr int kMaxGroups = 32;
@@ -142,6 +174,7 @@ int launch_grouped(const SplitMat &A, const SplitMat &B, const GemmGroup *g, int
   p.k_tiles[0] = 0;
   p.tiles_m = p.tiles_n = 0;
   p.n_valid = 1 << 30;
+  p.m_valid = 1 << 30;
   p.band = band;
   p.epi = e;
   p.err = err;
@@ -292,11 +325,19 @@ int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t 
       return launch<2, 128, EPI_HADAMARD_SPLIT, true, kDrain>(A, B, m_rows, n_rows, e, err, st,
                                                               band);
     if (!tf && nacc == 1 && epi == EPI_F32)
-      return launch<1, 256, EPI_F32, false, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
+      return engine_pairs()
+                 ? launch<1, 256, EPI_F32, false, kDrain, 2>(A, B, m_rows, n_rows, e, err, st,
+                                                            band)
+                 : launch<1, 256, EPI_F32, false, kDrain>(A, B, m_rows, n_rows, e, err, st,
+                                                         band);
     if (!tf && nacc == 3 && epi == EPI_SIGMA_H)
       return launch<3, 128, EPI_SIGMA_H, false, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
     if (!tf && nacc == 1 && epi == EPI_F64_SYM)
-      return launch<1, 256, EPI_F64_SYM, false, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
+      return engine_pairs()
+                 ? launch<1, 256, EPI_F64_SYM, false, kDrain, 2>(A, B, m_rows, n_rows, e, err,
+                                                                st, band)
+                 : launch<1, 256, EPI_F64_SYM, false, kDrain>(A, B, m_rows, n_rows, e, err, st,
+                                                             band);
     return MBPT_ERR_UNSUPPORTED;
   }
   if (band) {
@@ -328,7 +369,9 @@ int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t 
   // the non-symmetric N^3 products: 128 x 256 tiles (a quarter fewer operand
   // bytes per flop through the shared-memory ring than 128 x 128)
   if (nacc == 1 && epi == EPI_SPLIT)
-    return launch<1, 256, EPI_SPLIT, false, kDrain>(A, B, m_rows, n_rows, e, err, st);
+    return engine_pairs()
+               ? launch<1, 256, EPI_SPLIT, false, kDrain, 2>(A, B, m_rows, n_rows, e, err, st)
+               : launch<1, 256, EPI_SPLIT, false, kDrain>(A, B, m_rows, n_rows, e, err, st);
   if (nacc == 1 && epi == EPI_F32)
     return launch<1, 128, EPI_F32, false, kDrain>(A, B, m_rows, n_rows, e, err, st);
   if (nacc == 1 && epi == EPI_F32_ACC)

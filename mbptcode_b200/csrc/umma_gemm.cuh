@@ -87,6 +87,7 @@ struct Params {
   int k_tiles[NACC];
   int tiles_m, tiles_n;
   int n_valid;  // output columns to store (tiles_n * BN unless the last tile overhangs)
+  int m_valid;  // output rows to store (a CTA pair's second tile may lie past them)
   int band;  // Band flags (0: dense)
   int ngroups;
   Group grp[NGRP > 0 ? NGRP : 1];
@@ -133,6 +134,69 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity,
   }
 }
 
+// ---- CTA pairs (cluster of 2, cta_group::2) ----
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+// The shared::cluster address of this CTA's shared variable *p as held by CTA
+// `rank` of the cluster (the same offset in that CTA's shared memory).
+__device__ __forceinline__ uint32_t cluster_addr(const void *p, uint32_t rank) {
+  uint32_t a;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(p)), "r"(rank));
+  return a;
+}
+
+// Every thread of both CTAs of the cluster.
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile(
+      "barrier.cluster.arrive.release.aligned;\n\t"
+      "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t cluster_bar) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_bar)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait_cluster(uint64_t *b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait on a barrier that the other CTA of the pair also arrives on.
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t *b, uint32_t parity,
+                                                  uint64_t limit_ns = kWaitLimitNs) {
+  if (mbar_try_wait_cluster(b, parity)) return true;
+  const uint64_t t0 = global_ns();
+  while (true) {
+#pragma unroll 1
+    for (int i = 0; i < 64; ++i)
+      if (mbar_try_wait_cluster(b, parity)) return true;
+    if (global_ns() - t0 > limit_ns) return false;
+  }
+}
+
+// A tile into this CTA's shared memory whose bytes complete on a barrier of
+// either CTA of the pair (`bar` a shared::cluster address). No multicast.
+__device__ __forceinline__ void tma_load_2d_pair(void *dst, const CUtensorMap *tm, int x, int y,
+                                                 uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *tm, int x, int y,
                                             uint64_t *bar) {
   asm volatile(
@@ -161,10 +225,11 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   return d;
 }
 
-// Instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = n.
-__host__ __device__ constexpr uint32_t idesc_bf16(int n) {
+// Instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = m (128, or
+// 256 for a CTA pair), N = n.
+__host__ __device__ constexpr uint32_t idesc_bf16(int n, int m = 128) {
   return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(n >> 3) << 17) |
-         (static_cast<uint32_t>(128 >> 4) << 24);
+         (static_cast<uint32_t>(m >> 4) << 24);
 }
 
 // Instruction descriptor: TF32 x TF32 -> FP32, both K-major, M = 128, N = n.
@@ -205,6 +270,38 @@ __device__ __forceinline__ void mma3(uint32_t d, uint64_t a_hi, uint64_t a_lo, u
     mma_bf16(d, a_hi, b_lo, idesc, 1u);
     mma_bf16(d, a_lo, b_hi, idesc, 1u);
   }
+}
+
+// One MMA of a CTA pair, issued by the pair's first CTA: A's rows and B's
+// rows are split between the two CTAs' shared memory at the same offsets, and
+// each CTA's TMEM receives its own 128 rows. No output lane is disabled.
+__device__ __forceinline__ void mma_bf16_pair(uint32_t tmem_d, uint64_t da, uint64_t db,
+                                              uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, "
+      "{%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u),
+      "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma3_pair(uint32_t d, uint64_t a_hi, uint64_t a_lo,
+                                          uint64_t b_hi, uint64_t b_lo, uint32_t idesc,
+                                          uint32_t first) {
+  mma_bf16_pair(d, a_hi, b_hi, idesc, first ? 0u : 1u);
+  mma_bf16_pair(d, a_hi, b_lo, idesc, 1u);
+  mma_bf16_pair(d, a_lo, b_hi, idesc, 1u);
+}
+
+// Completion of the pair's MMAs issued so far, arriving once on the barrier
+// at `bar`'s offset in both CTAs.
+__device__ __forceinline__ void mma_commit_pair(uint64_t *bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64"
+      " [%0], %1;" ::"r"(smem_u32(bar)),
+      "h"(static_cast<uint16_t>(3))
+      : "memory");
 }
 
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
@@ -276,10 +373,12 @@ __device__ __forceinline__ float warp_column_sum(float (&v)[32], int lane) {
 }
 
 
-template <int NACC, int BN, bool DRAIN = false>
+// CTAS = 2: a CTA pair computes a 256 x BN tile, each CTA holding its 128
+// rows of A and half of B's BN rows in a stage.
+template <int NACC, int BN, bool DRAIN = false, int CTAS = 1>
 struct Layout {
   static constexpr int kABytes = BM * BK * 2;
-  static constexpr int kBBytes = BN * BK * 2;
+  static constexpr int kBBytes = BN / CTAS * BK * 2;
   static constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
   static constexpr int kStages = (kStageBytes <= 64 * 1024) ? 3 : 2;
   static constexpr int kSmemBytes = kStages * kStageBytes + 1024 + 256;
@@ -302,10 +401,22 @@ struct Layout {
 // registers while the MMAs fill the other buffer.
 // BN = 128: 6 warps (producer, MMA, 4 epilogue); BN = 256: 10 warps, the 8
 // epilogue warps covering the TMEM lane quarters twice, 128 columns each.
-template <int NACC, int BN, int EPI, bool TF32 = false, int DRAIN = 0, int NGRP = 0>
+//
+// CTAS = 2 (launched as clusters of two, BF16, dense K): the CTA pair forms a
+// 256 x BN tile with cta_group::2 MMAs issued by the first CTA. Each CTA loads
+// its own 128 rows of A and its half of B's rows, both completing on the first
+// CTA's full barrier; the commits arrive in both CTAs; the second CTA's
+// epilogue warps release drained buffers on the first CTA's barrier. Per K
+// slab a CTA then moves 64 KB instead of 96 KB for the same MMA work, and
+// three stages fit instead of two.
+template <int NACC, int BN, int EPI, bool TF32 = false, int DRAIN = 0, int NGRP = 0,
+          int CTAS = 1>
 __global__ void __launch_bounds__(64 + BN, 1)
     gemm_split_kernel(const __grid_constant__ Params<NACC, NGRP> p) {
-  using L = Layout<NACC, BN, (DRAIN > 0)>;
+  constexpr bool kPair = CTAS == 2;
+  static_assert(!kPair || (NACC == 1 && BN == 256 && !TF32 && NGRP == 0),
+                "CTA pairs: one BF16 accumulator, 256-wide tiles, single products");
+  using L = Layout<NACC, BN, (DRAIN > 0), CTAS>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
@@ -318,8 +429,12 @@ __global__ void __launch_bounds__(64 + BN, 1)
   int *fail = reinterpret_cast<int *>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // rank in the pair (0 issues the MMAs); 0 without pairs
+  const uint32_t rank = kPair ? cluster_rank() : 0u;
+  const bool leader = rank == 0;
   // this CTA's product (grouped launches) and its origins
-  int pid = blockIdx.x, tiles_m = p.tiles_m, tiles_n = p.tiles_n;
+  int pid = kPair ? static_cast<int>(blockIdx.x >> 1) : static_cast<int>(blockIdx.x);
+  int tiles_m = p.tiles_m, tiles_n = p.tiles_n;
   int a_row0 = 0, a_k0 = 0, b_row0 = 0, b_k0 = 0, grp_k_tiles = 0;
   int64_t p_off = 0, t_off = 0;
   if constexpr (NGRP > 0) {
@@ -337,17 +452,25 @@ __global__ void __launch_bounds__(64 + BN, 1)
     p_off = G.p_off;
     t_off = G.t_off;
   }
-  // grouped raster: kGroupM row tiles sweep the column tiles together (L2 reuse)
-  const int per_group = kGroupM * tiles_n;
-  const int first_m = (pid / per_group) * kGroupM;
-  const int gsize = min(tiles_m - first_m, kGroupM);
-  const int tm = first_m + (pid % per_group) % gsize;
+  // grouped raster: kGroupM row tiles sweep the column tiles together (L2
+  // reuse); a pair's unit is two row tiles, so half as many units per group
+  constexpr int kUnitsM = kPair ? kGroupM / 2 : kGroupM;
+  const int units_m = kPair ? (tiles_m + 1) / 2 : tiles_m;
+  const int per_group = kUnitsM * tiles_n;
+  const int first_m = (pid / per_group) * kUnitsM;
+  const int gsize = min(units_m - first_m, kUnitsM);
+  const int um = first_m + (pid % per_group) % gsize;
   const int tn = (pid % per_group) / gsize;
+  // the pair's first row tile; this CTA's row tile (the second CTA's may lie
+  // past the last one: it computes zeros and stores nothing)
+  const int tm_pair = kPair ? 2 * um : um;
+  const int tm = tm_pair + static_cast<int>(rank);
   const int m0 = tm * BM, n0 = tn * BN;
   constexpr int kLast = NACC - 1;
-  // uniform across the CTA, before any barrier or TMEM exists: a symmetric
-  // product skips tiles whose last 128-column block lies below the diagonal
-  if ((p.band & BAND_UPPER) && (n0 + BN) / 128 - 1 < tm) return;
+  // uniform across the CTA (and the pair), before any barrier or TMEM exists:
+  // a symmetric product skips tiles whose last 128-column block lies below
+  // the diagonal
+  if ((p.band & BAND_UPPER) && (n0 + BN) / 128 - 1 < tm_pair) return;
   // K slabs [kb, ke) of accumulator j that can hold nonzeros for this tile
   constexpr int kSlab = TF32 ? 32 : BK;
   auto k_span = [&](int j, int &kb, int &ke) {
@@ -368,21 +491,36 @@ __global__ void __launch_bounds__(64 + BN, 1)
     mbar_init(accum, 1);
     for (int b = 0; b < 2; ++b) {
       mbar_init(&dfull[b], 1);
-      mbar_init(&dempty[b], BN / 32);
+      // a pair's drained buffers are released by both CTAs' epilogue warps
+      mbar_init(&dempty[b], CTAS * BN / 32);
     }
     *fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   if (warp == 1) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                     smem_u32(tmem_slot)),
-                 "r"(L::kTmemCols)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    if constexpr (kPair) {
+      // one warp of each CTA of the pair: the same columns in both
+      asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                       smem_u32(tmem_slot)),
+                   "r"(L::kTmemCols)
+                   : "memory");
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    } else {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                       smem_u32(tmem_slot)),
+                   "r"(L::kTmemCols)
+                   : "memory");
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
   }
   tc_fence_before();
-  __syncthreads();
+  // a pair: both CTAs' barriers exist before either CTA's loads, commits or
+  // arrivals can reach them
+  if constexpr (kPair)
+    cluster_sync();
+  else
+    __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
@@ -397,30 +535,46 @@ __global__ void __launch_bounds__(64 + BN, 1)
           const int s = it % L::kStages;
           const uint32_t ph = (it / L::kStages) & 1;
           if (!mbar_wait(&empty[s], ph ^ 1)) { ok = false; break; }
-          mbar_expect_tx(&full[s], L::kStageBytes);
+          // a pair's stage completes on the first CTA's barrier with both
+          // CTAs' bytes
+          if (leader) mbar_expect_tx(&full[s], CTAS * L::kStageBytes);
           uint8_t *st = smem + s * L::kStageBytes;
           // K coordinate in elements: one 128-byte row per slab
           const int kx = kt * kSlab;
-          tma_load_2d(st, &p.tm[4 * j + 0], a_k0 + kx, a_row0 + m0, &full[s]);
-          tma_load_2d(st + L::kABytes, &p.tm[4 * j + 1], a_k0 + kx, a_row0 + m0, &full[s]);
-          tma_load_2d(st + 2 * L::kABytes, &p.tm[4 * j + 2], b_k0 + kx, b_row0 + n0, &full[s]);
-          tma_load_2d(st + 2 * L::kABytes + L::kBBytes, &p.tm[4 * j + 3], b_k0 + kx,
-                      b_row0 + n0, &full[s]);
+          if constexpr (kPair) {
+            const uint32_t bar = cluster_addr(&full[s], 0);
+            const int nb = b_row0 + n0 + static_cast<int>(rank) * (BN / 2);
+            tma_load_2d_pair(st, &p.tm[4 * j + 0], a_k0 + kx, a_row0 + m0, bar);
+            tma_load_2d_pair(st + L::kABytes, &p.tm[4 * j + 1], a_k0 + kx, a_row0 + m0, bar);
+            tma_load_2d_pair(st + 2 * L::kABytes, &p.tm[4 * j + 2], b_k0 + kx, nb, bar);
+            tma_load_2d_pair(st + 2 * L::kABytes + L::kBBytes, &p.tm[4 * j + 3], b_k0 + kx, nb,
+                             bar);
+          } else {
+            tma_load_2d(st, &p.tm[4 * j + 0], a_k0 + kx, a_row0 + m0, &full[s]);
+            tma_load_2d(st + L::kABytes, &p.tm[4 * j + 1], a_k0 + kx, a_row0 + m0, &full[s]);
+            tma_load_2d(st + 2 * L::kABytes, &p.tm[4 * j + 2], b_k0 + kx, b_row0 + n0,
+                        &full[s]);
+            tma_load_2d(st + 2 * L::kABytes + L::kBBytes, &p.tm[4 * j + 3], b_k0 + kx,
+                        b_row0 + n0, &full[s]);
+          }
         }
       }
       if (!ok) {
         atomicExch(fail, 1);
         DevErr{p.err}.set(MBPT_ERR_TIMEOUT);
       }
-      // drain: every load issued lands before the CTA may exit
-      const int issued = it;
+      // drain: every load issued lands before the CTA may exit (a pair's
+      // loads all complete on the first CTA's barriers, and the second CTA
+      // waits for the first at the closing cluster barrier)
+      const int issued = leader ? it : 0;
       for (int q = max(0, issued - L::kStages); q < issued; ++q)
         mbar_wait(&full[q % L::kStages], (q / L::kStages) & 1);
     }
     __syncwarp();
   } else if (warp == 1) {
-    if (lane == 0) {
-      constexpr uint32_t idesc = TF32 ? idesc_tf32(BN) : idesc_bf16(BN);
+    // a pair's MMAs are issued by its first CTA alone
+    if (lane == 0 && leader) {
+      constexpr uint32_t idesc = TF32 ? idesc_tf32(BN) : idesc_bf16(BN, CTAS * BM);
       int it = 0;
       bool ok = true;
       for (int j = 0; j < NACC && ok; ++j) {
@@ -435,7 +589,11 @@ __global__ void __launch_bounds__(64 + BN, 1)
           if (chunk_start) {
             const int c = q / (DRAIN > 0 ? DRAIN : 1);
             buf = c & 1;
-            if (!mbar_wait(&dempty[buf], ((c >> 1) & 1) ^ 1)) { ok = false; break; }
+            const uint32_t par = ((c >> 1) & 1) ^ 1;
+            if (!(kPair ? mbar_wait_cluster(&dempty[buf], par) : mbar_wait(&dempty[buf], par))) {
+              ok = false;
+              break;
+            }
             tc_fence_after();
             d = tmem + static_cast<uint32_t>((kLast + buf) * BN);
           }
@@ -455,19 +613,32 @@ __global__ void __launch_bounds__(64 + BN, 1)
 #pragma unroll
           for (int kk = 0; kk < 4; ++kk) {
             const uint64_t adv = static_cast<uint64_t>(kk * 2);  // 32 bytes >> 4
-            mma3<TF32>(d, a_hi + adv, a_lo + adv, b_hi + adv, b_lo + adv, idesc,
-                       (restart && kk == 0) ? 1u : 0u);
+            if constexpr (kPair)
+              mma3_pair(d, a_hi + adv, a_lo + adv, b_hi + adv, b_lo + adv, idesc,
+                        (restart && kk == 0) ? 1u : 0u);
+            else
+              mma3<TF32>(d, a_hi + adv, a_lo + adv, b_hi + adv, b_lo + adv, idesc,
+                         (restart && kk == 0) ? 1u : 0u);
           }
-          mma_commit(&empty[s]);
-          if (drained && ((q + 1) % (DRAIN > 0 ? DRAIN : 1) == 0 || kt + 1 == ke))
-            mma_commit(&dfull[buf]);
+          const bool chunk_end =
+              drained && ((q + 1) % (DRAIN > 0 ? DRAIN : 1) == 0 || kt + 1 == ke);
+          if constexpr (kPair) {
+            mma_commit_pair(&empty[s]);
+            if (chunk_end) mma_commit_pair(&dfull[buf]);
+          } else {
+            mma_commit(&empty[s]);
+            if (chunk_end) mma_commit(&dfull[buf]);
+          }
         }
       }
       if (!ok) {
         atomicExch(fail, 1);
         DevErr{p.err}.set(MBPT_ERR_TIMEOUT);
       }
-      mma_commit(accum);
+      if constexpr (kPair)
+        mma_commit_pair(accum);
+      else
+        mma_commit(accum);
       mbar_wait(accum, 0);  // no MMA may still write TMEM when it is freed
     }
     __syncwarp();
@@ -487,7 +658,9 @@ __global__ void __launch_bounds__(64 + BN, 1)
       const int nchunks = (ke - kb + DRAIN - 1) / DRAIN;
       for (int c = 0; c < nchunks; ++c) {
         const int b = c & 1;
-        if (!mbar_wait(&dfull[b], (c >> 1) & 1) || *reinterpret_cast<volatile int *>(fail)) {
+        const uint32_t par = (c >> 1) & 1;
+        if (!(kPair ? mbar_wait_cluster(&dfull[b], par) : mbar_wait(&dfull[b], par)) ||
+            *reinterpret_cast<volatile int *>(fail)) {
           ok = false;
           break;
         }
@@ -501,12 +674,17 @@ __global__ void __launch_bounds__(64 + BN, 1)
         }
         tc_fence_before();
         __syncwarp();
-        if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(
-                                        smem_u32(&dempty[b]))
-                                    : "memory");
+        if (lane == 0) {
+          if constexpr (kPair)
+            mbar_arrive_remote(cluster_addr(&dempty[b], 0));  // the MMAs' CTA
+          else
+            asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&dempty[b]))
+                         : "memory");
+        }
       }
     }
-    ok = ok && mbar_wait(accum, 0) && !*reinterpret_cast<volatile int *>(fail);
+    ok = ok && (kPair ? mbar_wait_cluster(accum, 0) : mbar_wait(accum, 0)) &&
+         !*reinterpret_cast<volatile int *>(fail);
     __syncwarp();
     if (!ok) {
       if (lane == 0) DevErr{p.err}.set(MBPT_ERR_TIMEOUT);
@@ -531,8 +709,9 @@ __global__ void __launch_bounds__(64 + BN, 1)
         }
         tmem_ld32(taddr + static_cast<uint32_t>(j * BN + cb + c), v);
       };
-      // columns past n_valid (a 256-wide tile over a 128-multiple edge) are not stored
-      const bool live = n0 + cb < p.n_valid && !(upper && tb < tm);
+      // columns past n_valid (a 256-wide tile over a 128-multiple edge) are not
+      // stored, nor the rows of a pair's second tile past m_valid
+      const bool live = n0 + cb < p.n_valid && m0 < p.m_valid && !(upper && tb < tm);
 #pragma unroll
       for (int c = 0; c < 128; c += 32) {
         if (!live) break;
@@ -649,12 +828,22 @@ __global__ void __launch_bounds__(64 + BN, 1)
   }
 
   tc_fence_before();
-  __syncthreads();
+  // a pair: neither CTA frees its TMEM (or exits, with the other's loads or
+  // arrivals still due) before both are done
+  if constexpr (kPair)
+    cluster_sync();
+  else
+    __syncthreads();
   tc_fence_after();
   if (warp == 1) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(L::kTmemCols)
-                 : "memory");
+    if constexpr (kPair)
+      asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                   "r"(L::kTmemCols)
+                   : "memory");
+    else
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                   "r"(L::kTmemCols)
+                   : "memory");
   }
 }
 

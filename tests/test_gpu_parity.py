@@ -1048,3 +1048,36 @@ def test_contour_pole_route_decisions_match_reference_golden(golden):
         for a, k in ((eb, f'route{j}_eps_bar'), (db, f'route{j}_D_bar')):
             ref = e[k]
             assert np.abs(a - ref).max() <= 1e-8 * max(np.abs(ref).max(), 1e-300), (p, sc, k)
+
+
+@pytest.mark.parametrize('M,n,nocc,naux', [(301, 37, 5, 173), (1100, 90, 12, 900)])
+def test_engine_cta_pairs_match_single_cta(M, n, nocc, naux, monkeypatch):
+    """The 256-wide BF16 products (Z = D^T Pi, proj, U = D W) as CTA pairs
+    (cta_group::2, the default) against the same products one CTA per tile
+    (MBPT_ENGINE_PAIRS=0), on row-tile counts odd and even (a pair's second
+    tile past the last row stores nothing): the same K order per element, so
+    within 1e-6 of each other, and both within the mixed tolerance of the
+    oracle."""
+    rng = np.random.default_rng(11)
+    X = rng.standard_normal((M, n)) * 0.08
+    D = rng.standard_normal((M, naux)) * 0.08
+    eps = np.sort(np.concatenate([rng.uniform(-1.2, -0.4, nocc),
+                                  rng.uniform(0.1, 3.0, n - nocc)]))
+    axes = grids.space_time_axes(eps, nocc, ntau=8)
+    ref = orc.chi0_imaginary_frequency(X, D, eps, nocc, axes.grid)
+    W = np.stack([orc.dyson_screening(c, True) for c in ref])
+    Wt = torch.as_tensor(np.tensordot(axes.Ctw, W, axes=(1, 0)), device='cuda')
+    states = [0, nocc - 1, nocc, n - 1]
+    out = {}
+    for pairs in ('1', '0'):
+        monkeypatch.setenv('MBPT_ENGINE_PAIRS', pairs)
+        chi = st.chi0_imaginary_frequency(X, D, eps, nocc, axes.grid, precision='mixed')
+        br = gw.sigma_branch_sums(X, D, Wt, eps, nocc, axes.tau_sigma, states, axes.mu,
+                                  precision='mixed').cpu().numpy()
+        out[pairs] = (chi, br)
+    assert rel(out['1'][0], out['0'][0]) < 1e-6
+    assert rel(out['1'][1], out['0'][1]) < 1e-6
+    assert rel(out['1'][0], ref) < MIXED_REL
+    br_ref = orc.sigma_branch_sums(X, D, Wt.cpu().numpy(), eps, nocc, axes.tau_sigma, axes.mu,
+                                   states)
+    assert rel(out['1'][1], br_ref) < 5e-5
