@@ -69,8 +69,8 @@ FLOPS = {
 # engine kernels at this workload, from one ncu capture of a tau point at full
 # size (python bench_cases.py tau --M 7200 --n 1200 --nocc 120
 # --states 1200, the six engine launches of one tau point)
-TRAFFIC_BYTES = {'hadamard': 314.5e6, 'split': 1943.3e6, 'f32': 1143.7e6,
-                 'sigma_hadamard': 1823.2e6, 'row_contraction': 1087.3e6}
+TRAFFIC_BYTES = {'hadamard': 314.5e6, 'split': 1956.1e6, 'f32': 1144.8e6,
+                 'sigma_hadamard': 1832.5e6, 'row_contraction': 1087.4e6}
 # algorithmic FLOPs of the Dyson step's inverse per frequency (triangular inverse
 # n^3/3 + L^-T L^-1 n^3/3, the classical SPD-inverse count), spread over launches
 # of many sizes: rated on their summed time
