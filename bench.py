@@ -61,8 +61,8 @@ SYM = (_T * (_T + 1) / 2) / (_T * _T)
 FLOPS = {
     'hadamard': SYM * 2.0 * M * M * N_ORB,              # G_occ and G_virt of one tau
     'split': 2.0 * M * M * M,                           # D^T Pi  /  D Wt
-    'f32': SYM * 2.0 * M * M * M,                       # D^T (Pi D)
-    'sigma_hadamard': SYM * (2.0 * M * M * M + 2.0 * M * M * N_ORB),   # Zt, G_occ, G_virt
+    'f32': SYM * 2.0 * M * M * M,                       # D^T (Pi D) and Zt = U D^T
+    'sigma_hadamard': SYM * 2.0 * M * M * N_ORB,        # G_occ, G_virt (o Zt)
     'row_contraction': 2.0 * 2.0 * M * M * N_ORB,       # (G o Zt) X_s, both branches
 }
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the

@@ -1027,7 +1027,7 @@ struct SigmaBufs {
   // mixed
   bf16 *D_hi, *D_lo, *W_hi, *W_lo, *U_hi, *U_lo, *Yo_hi, *Yo_lo, *Yv_hi, *Yv_lo, *Hl_hi,
       *Hl_lo, *Hg_hi, *Hg_lo, *XsT_hi, *XsT_lo;
-  float *xs;
+  float *xs, *Zf;
   double *sig;
 };
 
@@ -1062,6 +1062,7 @@ SigmaBufs carve_sigma(Arena &ar, const Dims &d, int ntau, int nstates, int mode)
     b.XsT_hi = ar.take<bf16>(Sp * d.Mp);
     b.XsT_lo = ar.take<bf16>(Sp * d.Mp);
     b.xs = ar.take<float>(d.Mp * Sp);
+    b.Zf = ar.take<float>(d.Mp * d.Mp);
     b.sig = ar.take<double>(2 * static_cast<int64_t>(ntau) * Sp);
   }
   return b;
@@ -1135,18 +1136,28 @@ int sigma_run(const double *X, const Dims &d, const double *eps, double mu, cons
         rc = gemm_split(umma::EPI_SPLIT, 1, &Dm, &Wm, d.Mp, d.Ap, e, err, st);
         if (rc) return rc;
       }
-      // one tile pass: Zt = U D^T, G_occ, G_virt -> H< = G_occ o Zt, H> = G_virt o Zt
+      // Zt = U D^T (= D W D^T, symmetric) whole in FP32: upper 256 x 256 tiles
+      // on CTA pairs, mirrored by the epilogue, its K = naux sum drained
+      e = umma::EpiArgs();
+      e.outf = b.Zf;
+      e.ld_outf = d.Mp;
+      e.alpha = 1.f;
+      rc = gemm_split(umma::EPI_F32, 1, Wt ? &Um : &Dm, &Dm, d.Mp, d.Mp, e, err, st,
+                      umma::BAND_UPPER);
+      if (rc) return rc;
+      // G_occ, G_virt (short K) -> H< = G_occ o Zt, H> = G_virt o Zt; all four
+      // symmetric: upper tiles, mirrored by the epilogue
       e = umma::EpiArgs();
       e.out0_hi = b.Hl_hi;
       e.out0_lo = b.Hl_lo;
       e.out1_hi = b.Hg_hi;
       e.out1_lo = b.Hg_lo;
       e.ld_out = d.Mp;
-      // Zt last: its K = naux sum is the long one, drained by the kernel
-      SplitMat A3[3] = {Yo, Yv, Wt ? Um : Dm}, B3[3] = {Yo, Yv, Dm};
-      // G_occ, G_virt and Zt = D W D^T are symmetric, so are H< and H>: upper
-      // tiles, mirrored by the epilogue
-      rc = gemm_split(umma::EPI_SIGMA_H, 3, A3, B3, d.Mp, d.Mp, e, err, st, umma::BAND_UPPER);
+      e.zt = b.Zf;
+      e.ld_zt = d.Mp;
+      SplitMat A2g[2] = {Yo, Yv};
+      rc = gemm_split(umma::EPI_SIGMA_HZ, 2, A2g, A2g, d.Mp, d.Mp, e, err, st,
+                      umma::BAND_UPPER);
       if (rc) return rc;
       // branch sums: sum_P X_s[P,p] (H X_s)[P,p]
       e = umma::EpiArgs();

@@ -118,11 +118,11 @@ int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const cudaError_t rc = cudaLaunchKernelEx(&cfg, kern, p);
-    if (timed) timing_end(st, EPI, ev0, ev1);
+    if (timed) timing_end(st, EPI == umma::EPI_SIGMA_HZ ? umma::EPI_SIGMA_H : EPI, ev0, ev1);
     return rc == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
   } else {
     kern<<<p.tiles_m * p.tiles_n, 64 + BN, L::kSmemBytes, st>>>(p);
-    if (timed) timing_end(st, EPI, ev0, ev1);
+    if (timed) timing_end(st, EPI == umma::EPI_SIGMA_HZ ? umma::EPI_SIGMA_H : EPI, ev0, ev1);
     return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
   }
 }
@@ -332,6 +332,13 @@ int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t 
                                                          band);
     if (!tf && nacc == 3 && epi == EPI_SIGMA_H)
       return launch<3, 128, EPI_SIGMA_H, false, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
+    // the two G products of Sigma's H (short K: not drained) against a stored Zt
+    if (!tf && nacc == 2 && epi == EPI_SIGMA_HZ)
+      return engine_pairs()
+                 ? launch<2, 256, EPI_SIGMA_HZ, false, 0, 2>(A, B, m_rows, n_rows, e, err, st,
+                                                            band)
+                 : launch<2, 256, EPI_SIGMA_HZ, false, 0>(A, B, m_rows, n_rows, e, err, st,
+                                                         band);
     if (!tf && nacc == 1 && epi == EPI_F64_SYM)
       return engine_pairs()
                  ? launch<1, 256, EPI_F64_SYM, false, kDrain, 2>(A, B, m_rows, n_rows, e, err,

@@ -32,6 +32,7 @@ enum Epi : int {
   EPI_TF32_PAIR = 6,       // alpha * acc0 as a TF32 hi/lo pair at p (and transposed at t)
   EPI_F64_SYM = 7,         // outd = alpha * acc0 - shift [row == col], FP64, rows and
                            // columns below nd, mirrored (with BAND_UPPER)
+  EPI_SIGMA_HZ = 8,        // out0 = acc0 o Zt, out1 = acc1 o Zt, Zt read (FP32) at zt
 };
 
 struct EpiArgs {
@@ -52,6 +53,9 @@ struct EpiArgs {
   int64_t ld_outd = 0;
   int nd = 0;
   double shift = 0.0;
+  // EPI_SIGMA_HZ: the FP32 factor of both products, row-major (ld_zt)
+  const float *zt = nullptr;
+  int64_t ld_zt = 0;
 };
 
 // Structure of triangular operands, for products whose rows vanish on one
@@ -414,8 +418,10 @@ template <int NACC, int BN, int EPI, bool TF32 = false, int DRAIN = 0, int NGRP 
 __global__ void __launch_bounds__(64 + BN, 1)
     gemm_split_kernel(const __grid_constant__ Params<NACC, NGRP> p) {
   constexpr bool kPair = CTAS == 2;
-  static_assert(!kPair || (NACC == 1 && BN == 256 && !TF32 && NGRP == 0),
-                "CTA pairs: one BF16 accumulator, 256-wide tiles, single products");
+  static_assert(!kPair || (BN == 256 && !TF32 && NGRP == 0 &&
+                            (NACC == 1 || (NACC == 2 && DRAIN == 0))),
+                "CTA pairs: BF16, 256-wide tiles, one accumulator or two undrained, single "
+                "products");
   using L = Layout<NACC, BN, (DRAIN > 0), CTAS>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -791,6 +797,28 @@ __global__ void __launch_bounds__(64 + BN, 1)
           // acc0 = G_occ, acc1 = G_virt, acc2 = Zt
           float z[32], v1[32];
           load(2, c, z);
+#pragma unroll
+          for (int i = 0; i < 32; ++i) v0[i] *= z[i];
+          store_split32(e.out0_hi + row * e.ld_out + col, e.out0_lo + row * e.ld_out + col, v0);
+          if (mirror)
+            store_split32_t(e.out0_hi + static_cast<int64_t>(col) * e.ld_out + row,
+                            e.out0_lo + static_cast<int64_t>(col) * e.ld_out + row, e.ld_out, v0);
+          load(1, c, v1);
+#pragma unroll
+          for (int i = 0; i < 32; ++i) v1[i] *= z[i];
+          store_split32(e.out1_hi + row * e.ld_out + col, e.out1_lo + row * e.ld_out + col, v1);
+          if (mirror)
+            store_split32_t(e.out1_hi + static_cast<int64_t>(col) * e.ld_out + row,
+                            e.out1_lo + static_cast<int64_t>(col) * e.ld_out + row, e.ld_out, v1);
+        } else if constexpr (EPI == EPI_SIGMA_HZ) {
+          // acc0 = G_occ, acc1 = G_virt; Zt (symmetric, stored whole) from memory
+          float z[32], v1[32];
+          const float4 *zs = reinterpret_cast<const float4 *>(e.zt + row * e.ld_zt + col);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const float4 t = zs[q];
+            z[4 * q] = t.x; z[4 * q + 1] = t.y; z[4 * q + 2] = t.z; z[4 * q + 3] = t.w;
+          }
 #pragma unroll
           for (int i = 0; i < 32; ++i) v0[i] *= z[i];
           store_split32(e.out0_hi + row * e.ld_out + col, e.out0_lo + row * e.ld_out + col, v0);
