@@ -387,8 +387,11 @@ int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t 
     return launch<2, 128, EPI_HADAMARD_SPLIT, false, kDrain>(A, B, m_rows, n_rows, e, err, st);
   if (nacc == 3 && epi == EPI_SIGMA_H)
     return launch<3, 128, EPI_SIGMA_H, false, kDrain>(A, B, m_rows, n_rows, e, err, st);
+  // the row contraction: two undrained accumulators, 256-wide on CTA pairs
   if (nacc == 2 && epi == EPI_ROWDOT2)
-    return launch<2, 128, EPI_ROWDOT2, false, 0>(A, B, m_rows, n_rows, e, err, st);
+    return engine_pairs()
+               ? launch<2, 256, EPI_ROWDOT2, false, 0, 2>(A, B, m_rows, n_rows, e, err, st)
+               : launch<2, 128, EPI_ROWDOT2, false, 0>(A, B, m_rows, n_rows, e, err, st);
   return MBPT_ERR_UNSUPPORTED;
 }
 

@@ -1050,14 +1050,16 @@ def test_contour_pole_route_decisions_match_reference_golden(golden):
             assert np.abs(a - ref).max() <= 1e-8 * max(np.abs(ref).max(), 1e-300), (p, sc, k)
 
 
-@pytest.mark.parametrize('M,n,nocc,naux', [(301, 37, 5, 173), (1100, 90, 12, 900)])
-def test_engine_cta_pairs_match_single_cta(M, n, nocc, naux, monkeypatch):
-    """The 256-wide BF16 products (Z = D^T Pi, proj, U = D W) as CTA pairs
-    (cta_group::2, the default) against the same products one CTA per tile
+@pytest.mark.parametrize('M,n,nocc,naux,nstates', [(301, 37, 5, 173, 4), (1100, 90, 12, 900, 4),
+                                                   (700, 400, 40, 500, 300)])
+def test_engine_cta_pairs_match_single_cta(M, n, nocc, naux, nstates, monkeypatch):
+    """The engine's 256-wide BF16 products as CTA pairs (cta_group::2, the
+    default: Z = D^T Pi, proj, U = D W, Zt = U D^T, the G products of Sigma's
+    H and the row contraction) against the same products one CTA per tile
     (MBPT_ENGINE_PAIRS=0), on row-tile counts odd and even (a pair's second
-    tile past the last row stores nothing): the same K order per element, so
-    within 1e-6 of each other, and both within the mixed tolerance of the
-    oracle."""
+    tile past the last row stores nothing) and state counts whose last
+    256-wide column tile overhangs: the same K order per element, so within
+    1e-6 of each other, and both within the mixed tolerance of the oracle."""
     rng = np.random.default_rng(11)
     X = rng.standard_normal((M, n)) * 0.08
     D = rng.standard_normal((M, naux)) * 0.08
@@ -1067,7 +1069,8 @@ def test_engine_cta_pairs_match_single_cta(M, n, nocc, naux, monkeypatch):
     ref = orc.chi0_imaginary_frequency(X, D, eps, nocc, axes.grid)
     W = np.stack([orc.dyson_screening(c, True) for c in ref])
     Wt = torch.as_tensor(np.tensordot(axes.Ctw, W, axes=(1, 0)), device='cuda')
-    states = [0, nocc - 1, nocc, n - 1]
+    # 4 states: one overhanging 256-wide column tile; 300: two, the last overhanging
+    states = [0, nocc - 1, nocc, n - 1] if nstates == 4 else list(range(nstates))
     out = {}
     for pairs in ('1', '0'):
         monkeypatch.setenv('MBPT_ENGINE_PAIRS', pairs)
