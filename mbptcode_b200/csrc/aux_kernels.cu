@@ -296,16 +296,20 @@ __global__ void scatter_cols_kernel(const double *__restrict__ T, int64_t M, int
 constexpr int kCholNb = 128;
 constexpr int kCholStride = kCholNb + 1;  // odd: a column of s read by a warp is free of bank conflicts
 
-// P_f (m x nbj, column-major, ld m) <- the block column A_f[j0:, j0:j0+nbj]
+// P_f (m x nbj, column-major, ld m) <- the block column A_f[j0:, j0:j0+nbj],
+// or of I - A_f with one_minus (the factorised matrix is then I - A_f, whose
+// entries are formed here, each read once)
 __global__ void chol_copy_panel_kernel(const double *__restrict__ A, int64_t n, int64_t j0,
-                                       int64_t m, int nbj, double *__restrict__ P) {
+                                       int64_t m, int nbj, bool one_minus,
+                                       double *__restrict__ P) {
   const double *a = A + static_cast<int64_t>(blockIdx.y) * n * n;
   double *p = P + static_cast<int64_t>(blockIdx.y) * m * nbj;
   const int64_t total = m * nbj;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t c = i / m, r = i % m;
-    p[i] = a[(j0 + c) * n + j0 + r];
+    const double v = a[(j0 + c) * n + j0 + r];
+    p[i] = one_minus ? (r == c ? 1.0 : 0.0) - v : v;
   }
 }
 
@@ -722,10 +726,10 @@ void launch_scatter_cols(const double *T, int64_t M, int64_t S, const int64_t *s
 }
 
 void launch_chol_copy_panel(const double *A, int64_t n, int64_t j0, int64_t m, int nbj,
-                            int nmat, double *P, cudaStream_t st) {
+                            int nmat, bool one_minus, double *P, cudaStream_t st) {
   dim3 grid(static_cast<unsigned>(blocks(m * nbj)), nmat);
   count_launch();
-  chol_copy_panel_kernel<<<grid, 256, 0, st>>>(A, n, j0, m, nbj, P);
+  chol_copy_panel_kernel<<<grid, 256, 0, st>>>(A, n, j0, m, nbj, one_minus, P);
 }
 
 int launch_chol_diag_block(const double *P, int64_t m, int nbj, double *A, int64_t n,

@@ -59,7 +59,7 @@ void launch_row_scale_acc(const double *a, int64_t lda, int64_t p, const double 
 void launch_row_dot_into_col(const double *G, const double *X, int64_t nr, int64_t nc,
                              double *out, int64_t ldo, int64_t p, cudaStream_t st);
 void launch_chol_copy_panel(const double *A, int64_t n, int64_t j0, int64_t m, int nbj,
-                            int nmat, double *P, cudaStream_t st);
+                            int nmat, bool one_minus, double *P, cudaStream_t st);
 int launch_chol_diag_block(const double *P, int64_t m, int nbj, double *A, int64_t n,
                            int64_t j0, int nmat, double *Linv, int *info, cudaStream_t st);
 void launch_sigma_back_gather(const double *X, int64_t M, int64_t n, const int64_t *states,
@@ -539,6 +539,9 @@ constexpr int kBatchedCholMin = 4;  // frequencies from which the batch beats on
 // step for all frequencies. P: nmat * n * kCholNb doubles; Linv: nmat *
 // kCholNb^2 doubles per step, step j at Linv + j * linv_step_stride (0: every
 // step in the same place); info: nmat ints, zeroed by the caller.
+// one_minus: A holds chi0 and the factorised matrices are I - A_f, formed
+// where each block column is first read (A's strict upper triangle keeps
+// chi0, its diagonal and lower triangle become the factor).
 // The Ozaki-scheme update's buffers for one batch (null planes: the updates
 // run as cuBLAS DGEMMs): the int8 digit planes, 2^e_r per row, exact row norms.
 struct OzakiChol {
@@ -551,18 +554,18 @@ struct OzakiChol {
 
 int chol_batched(double *A, int64_t n, int nmat, int *info, double *P, double *Linv,
                  cublasHandle_t h, cudaStream_t st, int64_t linv_step_stride = 0,
-                 const OzakiChol *oz = nullptr) {
+                 const OzakiChol *oz = nullptr, bool one_minus = false) {
   const long long n2 = static_cast<long long>(n) * n;
   const double one = 1.0, minus = -1.0, zero = 0.0;
   const bool ozaki = oz && oz->planes;
   if (ozaki) {
-    int rc = ozaki_chol_scales(A, n, nmat, oz->scale, oz->rowsq, st);
+    int rc = ozaki_chol_scales(A, n, nmat, oz->scale, oz->rowsq, one_minus, st);
     if (rc) return rc;
   }
   for (int64_t j0 = 0; j0 < n; j0 += kCholNb) {
     const int nbj = static_cast<int>(std::min<int64_t>(kCholNb, n - j0));
     const int64_t m = n - j0;
-    launch_chol_copy_panel(A, n, j0, m, nbj, nmat, P, st);
+    launch_chol_copy_panel(A, n, j0, m, nbj, nmat, one_minus, P, st);
     if (ozaki) {
       int rc = ozaki_chol_update(A, n, nmat, j0, nbj, P, oz->scale, oz->planes, oz->slices,
                                  oz->rowsq, oz->err, st);
@@ -824,7 +827,16 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
   DysonPipe *pp = dyson_pipe(nfreq);
   if (!pp) return MBPT_ERR_CUDA;
   const int ni = static_cast<int>(n);
-  launch_one_minus(chi0, n, nfreq, trace, st);
+  // many frequencies: one batched factorisation of all of them, then the
+  // per-frequency loop below only reads their info words
+  const bool batched = b.chol_P != nullptr;
+  // the batch forms 1 - chi0 where it first reads each block column (no pass
+  // of its own over the matrices); one potrf per frequency needs it whole
+  if (batched)
+    launch_trace(chi0, n, nfreq, trace, st);
+  else
+    launch_one_minus(chi0, n, nfreq, trace, st);
+  // the diagonal (of chi0 in a batch, of 1 - chi0 otherwise), for the LU fallback
   launch_diag(chi0, n, nfreq, b.diag, true, st);
   if (mode == MBPT_MODE_MIXED && want_w) {
     // the pair arrays are read as zeros wherever the recursion does not write
@@ -840,9 +852,6 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
   const int nsides = mode == MBPT_MODE_MIXED ? b.npairs : 1;
   auto side_of = [&](int i) { return i == 0 ? pp->side : pp->isides[i - 1]; };
   bool side_used[kMaxInverseStreams] = {};
-  // many frequencies: one batched factorisation of all of them, then the
-  // per-frequency loop below only reads their info words
-  const bool batched = b.chol_P != nullptr;
   if (batched) {
     if (cudaMemsetAsync(b.info, 0, sizeof(int) * nfreq, st) != cudaSuccess) return MBPT_ERR_CUDA;
     // groups of frequencies on their own streams (four by default, each of
@@ -890,7 +899,7 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
                            b.chol_P + static_cast<int64_t>(f0) * n * kCholNb,
                            b.chol_Linv + static_cast<int64_t>(f0) * kCholNb * kCholNb,
                            blas_of(g), gs, static_cast<int64_t>(nfreq) * kCholNb * kCholNb,
-                           &oz);
+                           &oz, true);
         if (rc0) break;
         // this group's log-determinants, info words and events on its own stream
         launch_logdet_diag(chi0 + f0 * n * n, n, f1 - f0, logdet + f0, gs);
@@ -976,6 +985,8 @@ int dyson_run(double *chi0, int64_t n, int nfreq, int want_w, double *logdet, do
     }
     launch_mirror_lower_to_upper(m, n, st);
     launch_diag(m, n, 1, b.diag + static_cast<int64_t>(f) * n, false, st);
+    // a batch left chi0 in the untouched triangle
+    if (batched) launch_one_minus(m, n, 1, nullptr, st);
     if (cusolverDnDgetrf(h.solver, ni, ni, m, ni, b.work, b.piv, b.info + nfreq) !=
         CUSOLVER_STATUS_SUCCESS) {
       rc = MBPT_ERR_CUDA;

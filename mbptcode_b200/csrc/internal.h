@@ -61,10 +61,10 @@ bool allow_smem(const void *kern, int bytes, std::atomic<uint64_t> &done);
 // ---- Ozaki-scheme FP64 updates of the batched Cholesky (ozaki.cu) ----
 // Bytes of the int8 digit planes of nmat n x n factors cut into `slices`.
 size_t ozaki_planes_bytes(int64_t n, int nmat, int slices);
-// scale[f][r] = 2^e_r >= sqrt(A_rr) of each matrix (column-major, ld n);
-// the running row norms rownorm (nmat x n) start at zero.
+// scale[f][r] = 2^e_r >= sqrt(A_rr) of each matrix (column-major, ld n; of
+// I - A with one_minus); the running row norms rownorm (nmat x n) start at zero.
 int ozaki_chol_scales(const double *A, int64_t n, int nmat, double *scale, double *rownorm,
-                      cudaStream_t st);
+                      bool one_minus, cudaStream_t st);
 // Cut block column [j0, j0 + nb) of every factor (rows j0..n-1) into digit
 // planes, adding its squares to the rows' running norms.
 int ozaki_chol_slice(const double *A, int64_t n, int nmat, int64_t j0, int nb,
@@ -150,7 +150,9 @@ void launch_transform_acc(const double *in, int64_t in_slice, int64_t ld_in, int
 void launch_transform_split(const double *in, int64_t in_slice, int64_t ld_in, int64_t rows,
                             int64_t cols, const double *w_dev, int J, int K, bf16 *out_hi,
                             bf16 *out_lo, int64_t out_slice, int64_t ld_out, cudaStream_t st);
+// a <- I - a per n x n slice; with trace, trace[f] = tr a first
 void launch_one_minus(double *a, int64_t n, int nmat, double *trace, cudaStream_t st);
+void launch_trace(const double *a, int64_t n, int nmat, double *trace, cudaStream_t st);
 void launch_logdet_diag(const double *L, int64_t n, int nmat, double *logdet,
                         cudaStream_t st);
 void launch_symmetrize_minus_identity(double *a, int64_t n, int nmat, cudaStream_t st);

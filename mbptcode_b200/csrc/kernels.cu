@@ -542,8 +542,12 @@ void launch_transform_split(const double *in, int64_t in_slice, int64_t ld_in, i
       in, in_slice, ld_in, rows, cols, w_dev, J, K, nullptr, out_hi, out_lo, out_slice, ld_out);
 }
 
-void launch_one_minus(double *a, int64_t n, int nmat, double *trace, cudaStream_t st) {
+void launch_trace(const double *a, int64_t n, int nmat, double *trace, cudaStream_t st) {
   count_launch(); trace_kernel<<<nmat, 256, 0, st>>>(a, n, trace);
+}
+
+void launch_one_minus(double *a, int64_t n, int nmat, double *trace, cudaStream_t st) {
+  if (trace) launch_trace(a, n, nmat, trace, st);
   dim3 grid(static_cast<unsigned>(grid_cap(n * n) / 4 + 1), nmat);
   count_launch(); one_minus_kernel<<<grid, kThreads, 0, st>>>(a, n, trace);
 }

@@ -351,12 +351,13 @@ __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_consta
 // 1 for a diagonal that is not positive and finite (that matrix fails its
 // factorisation and is redone by LU; its digits only need to stay in range).
 __global__ void chol_scale_kernel(const double *A, int64_t n, int64_t mat_stride, int nmat,
-                                  double *scale) {
+                                  bool one_minus, double *scale) {
   const int64_t total = n * nmat;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     const int64_t f = i / n, r = i % n;
-    const double a = A[f * mat_stride + r * n + r];
+    const double d = A[f * mat_stride + r * n + r];
+    const double a = one_minus ? 1.0 - d : d;  // the diagonal of I - A_f
     double s = 1.0;
     if (a > 0.0 && a < 1e300) {
       int e;
@@ -549,12 +550,12 @@ size_t ozaki_planes_bytes(int64_t n, int nmat, int slices) {
 }
 
 int ozaki_chol_scales(const double *A, int64_t n, int nmat, double *scale, double *rownorm,
-                      cudaStream_t st) {
+                      bool one_minus, cudaStream_t st) {
   if (cudaMemsetAsync(rownorm, 0, sizeof(double) * n * nmat, st) != cudaSuccess)
     return MBPT_ERR_CUDA;
   count_launch();
   ozaki::chol_scale_kernel<<<ozaki::grid_blocks(n * nmat), 256, 0, st>>>(A, n, n * n, nmat,
-                                                                         scale);
+                                                                         one_minus, scale);
   return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 
