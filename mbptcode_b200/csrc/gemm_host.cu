@@ -63,13 +63,12 @@ bool make_tmap(CUtensorMap *m, const void *base, int64_t rows, int64_t cols, int
   return r == CUDA_SUCCESS;
 }
 
-// CTAS = 2: clusters of two CTAs per 256 x BN tile (cta_group::2); dense K
-// (no K-band flags) only.
+// CTAS = 2: clusters of two CTAs per 256 x BN tile (cta_group::2); K-band
+// spans per pair.
 template <int NACC, int BN, int EPI, bool TF32, int DRAIN, int CTAS = 1>
 int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
            const umma::EpiArgs &e, int *err, cudaStream_t st, int band = 0) {
   using L = umma::Layout<NACC, BN, (DRAIN > 0), CTAS>;
-  if (CTAS == 2 && (band & ~umma::BAND_UPPER)) return MBPT_ERR_UNSUPPORTED;
   // the last column tile may overhang a multiple of 128 (BN = 256): its
   // B rows read as zeros and its dead columns are not stored
   if (m_rows % umma::BM || n_rows % 128 || m_rows <= 0 || n_rows <= 0) return MBPT_ERR_SHAPE;
@@ -359,7 +358,11 @@ int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t 
     // the symmetric FP64 store (W = L^-T L^-1): 128 x 256 tiles, which halve
     // the A reads through shared memory for the three TF32 products
     if (epi == EPI_F64_SYM && (band & BAND_UPPER))
-      return launch<1, 256, EPI_F64_SYM, true, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
+      return engine_pairs()
+                 ? launch<1, 256, EPI_F64_SYM, true, kDrain, 2>(A, B, m_rows, n_rows, e, err,
+                                                               st, band)
+                 : launch<1, 256, EPI_F64_SYM, true, kDrain>(A, B, m_rows, n_rows, e, err, st,
+                                                            band);
     if (epi == EPI_F64_SYM)
       return launch<1, 128, EPI_F64_SYM, true, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
     return launch<1, 128, EPI_F32, true, kDrain>(A, B, m_rows, n_rows, e, err, st, band);

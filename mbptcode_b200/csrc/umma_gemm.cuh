@@ -236,10 +236,11 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int n, int m = 128) {
          (static_cast<uint32_t>(m >> 4) << 24);
 }
 
-// Instruction descriptor: TF32 x TF32 -> FP32, both K-major, M = 128, N = n.
-__host__ __device__ constexpr uint32_t idesc_tf32(int n) {
+// Instruction descriptor: TF32 x TF32 -> FP32, both K-major, M = m (128, or
+// 256 for a CTA pair), N = n.
+__host__ __device__ constexpr uint32_t idesc_tf32(int n, int m = 128) {
   return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(n >> 3) << 17) |
-         (static_cast<uint32_t>(128 >> 4) << 24);
+         (static_cast<uint32_t>(m >> 4) << 24);
 }
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db,
@@ -290,12 +291,30 @@ __device__ __forceinline__ void mma_bf16_pair(uint32_t tmem_d, uint64_t da, uint
       "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
+__device__ __forceinline__ void mma_tf32_pair(uint32_t tmem_d, uint64_t da, uint64_t db,
+                                              uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, "
+      "{%5, %6, %7, %8, %9, %10, %11, %12}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u),
+      "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+template <bool TF32>
 __device__ __forceinline__ void mma3_pair(uint32_t d, uint64_t a_hi, uint64_t a_lo,
                                           uint64_t b_hi, uint64_t b_lo, uint32_t idesc,
                                           uint32_t first) {
-  mma_bf16_pair(d, a_hi, b_hi, idesc, first ? 0u : 1u);
-  mma_bf16_pair(d, a_hi, b_lo, idesc, 1u);
-  mma_bf16_pair(d, a_lo, b_hi, idesc, 1u);
+  if constexpr (TF32) {
+    mma_tf32_pair(d, a_hi, b_hi, idesc, first ? 0u : 1u);
+    mma_tf32_pair(d, a_hi, b_lo, idesc, 1u);
+    mma_tf32_pair(d, a_lo, b_hi, idesc, 1u);
+  } else {
+    mma_bf16_pair(d, a_hi, b_hi, idesc, first ? 0u : 1u);
+    mma_bf16_pair(d, a_hi, b_lo, idesc, 1u);
+    mma_bf16_pair(d, a_lo, b_hi, idesc, 1u);
+  }
 }
 
 // Completion of the pair's MMAs issued so far, arriving once on the barrier
@@ -418,10 +437,8 @@ template <int NACC, int BN, int EPI, bool TF32 = false, int DRAIN = 0, int NGRP 
 __global__ void __launch_bounds__(64 + BN, 1)
     gemm_split_kernel(const __grid_constant__ Params<NACC, NGRP> p) {
   constexpr bool kPair = CTAS == 2;
-  static_assert(!kPair || (BN == 256 && !TF32 && NGRP == 0 &&
-                            (NACC == 1 || (NACC == 2 && DRAIN == 0))),
-                "CTA pairs: BF16, 256-wide tiles, one accumulator or two undrained, single "
-                "products");
+  static_assert(!kPair || (BN == 256 && NGRP == 0 && (NACC == 1 || (NACC == 2 && DRAIN == 0))),
+                "CTA pairs: 256-wide tiles, one accumulator or two undrained, single products");
   using L = Layout<NACC, BN, (DRAIN > 0), CTAS>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -477,14 +494,16 @@ __global__ void __launch_bounds__(64 + BN, 1)
   // a symmetric product skips tiles whose last 128-column block lies below
   // the diagonal
   if ((p.band & BAND_UPPER) && (n0 + BN) / 128 - 1 < tm_pair) return;
-  // K slabs [kb, ke) of accumulator j that can hold nonzeros for this tile
+  // K slabs [kb, ke) of accumulator j that can hold nonzeros for this tile (a
+  // pair's: both CTAs run its rows' span; the slabs one CTA adds are zeros)
   constexpr int kSlab = TF32 ? 32 : BK;
+  const int m_lo = tm_pair * BM, m_hi = (tm_pair + CTAS) * BM;
   auto k_span = [&](int j, int &kb, int &ke) {
     kb = 0;
     ke = NGRP > 0 ? grp_k_tiles : p.k_tiles[j];
-    if (p.band & BAND_K_FROM_M) kb = max(kb, m0 / kSlab);
+    if (p.band & BAND_K_FROM_M) kb = max(kb, m_lo / kSlab);
     if (p.band & BAND_K_FROM_N) kb = max(kb, n0 / kSlab);
-    if (p.band & BAND_K_TO_M) ke = min(ke, (m0 + BM) / kSlab);
+    if (p.band & BAND_K_TO_M) ke = min(ke, m_hi / kSlab);
     if (p.band & BAND_K_TO_N) ke = min(ke, (n0 + BN) / kSlab);
     ke = max(ke, kb);
   };
@@ -580,7 +599,8 @@ __global__ void __launch_bounds__(64 + BN, 1)
   } else if (warp == 1) {
     // a pair's MMAs are issued by its first CTA alone
     if (lane == 0 && leader) {
-      constexpr uint32_t idesc = TF32 ? idesc_tf32(BN) : idesc_bf16(BN, CTAS * BM);
+      constexpr uint32_t idesc =
+          TF32 ? idesc_tf32(BN, CTAS * BM) : idesc_bf16(BN, CTAS * BM);
       int it = 0;
       bool ok = true;
       for (int j = 0; j < NACC && ok; ++j) {
@@ -620,8 +640,8 @@ __global__ void __launch_bounds__(64 + BN, 1)
           for (int kk = 0; kk < 4; ++kk) {
             const uint64_t adv = static_cast<uint64_t>(kk * 2);  // 32 bytes >> 4
             if constexpr (kPair)
-              mma3_pair(d, a_hi + adv, a_lo + adv, b_hi + adv, b_lo + adv, idesc,
-                        (restart && kk == 0) ? 1u : 0u);
+              mma3_pair<TF32>(d, a_hi + adv, a_lo + adv, b_hi + adv, b_lo + adv, idesc,
+                              (restart && kk == 0) ? 1u : 0u);
             else
               mma3<TF32>(d, a_hi + adv, a_lo + adv, b_hi + adv, b_lo + adv, idesc,
                          (restart && kk == 0) ? 1u : 0u);

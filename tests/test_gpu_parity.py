@@ -88,13 +88,15 @@ def test_dyson_and_transform_match_oracle(golden):
 
 
 @pytest.mark.parametrize('n', [96, 300, 1000])
-def test_dyson_inverse_both_modes(n):
+def test_dyson_inverse_both_modes(n, monkeypatch):
     """W - I from the Cholesky factor (shared-memory diagonal blocks, the
     recursive triangular inverse, L^-T L^-1) against torch's FP64 inverse:
     FP64 mode to rounding; mixed mode to 5e-6 absolute. 1 - chi0 >= I puts
     every eigenvalue of W in (0, 1], so each entry of L^-T L^-1 is a sum
     bounded by 1, which TF32 pairs (2^-22 per factor) and FP32 accumulation
-    (drained every 64 terms) reproduce to a few 2^-22."""
+    (drained every 64 terms) reproduce to a few 2^-22. The mixed L^-T L^-1
+    runs on CTA pairs with triangular K spans per pair (1, 3 and 8 row
+    tiles); one CTA per tile (MBPT_ENGINE_PAIRS=0) agrees within 1e-9."""
     g = torch.Generator(device='cpu').manual_seed(n)
     A = torch.randn(n, n // 2 + 7, generator=g, dtype=torch.float64)
     chi0 = -(A @ A.T) / n * 3.0
@@ -108,6 +110,11 @@ def test_dyson_inverse_both_modes(n):
         logdet, trace, info, _ = st.dyson_batch(c, want_w=True, precision=prec)
         assert not np.any(info)
         out[prec] = (c, logdet)
+    monkeypatch.setenv('MBPT_ENGINE_PAIRS', '0')
+    c = chi0.clone()
+    st.dyson_batch(c, want_w=True, precision='mixed')
+    monkeypatch.delenv('MBPT_ENGINE_PAIRS')
+    assert float((c - out['mixed'][0]).abs().max()) < 1e-9
     assert float((out['fp64'][0] - ref).abs().max()) < 1e-12
     err_mixed = float((out['mixed'][0] - ref).abs().max())
     print(f'n={n}: mixed max |W - W_ref| {err_mixed:.3e}')
