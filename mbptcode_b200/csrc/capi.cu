@@ -1622,6 +1622,7 @@ struct SigmaAoBufs {
          *U = nullptr, *R = nullptr;
   bf16 *D_hi, *D_lo, *W_hi, *W_lo, *U_hi, *U_lo, *Yo_hi, *Yo_lo, *Yv_hi, *Yv_lo, *Hl_hi,
       *Hl_lo, *Hg_hi, *Hg_lo, *XaT_hi, *XaT_lo, *RT_hi, *RT_lo;
+  float *Zf = nullptr;
 };
 
 SigmaAoBufs carve_sigma_ao(Arena &ar, const Dims &d, int64_t nao, int mode) {
@@ -1644,6 +1645,7 @@ SigmaAoBufs carve_sigma_ao(Arena &ar, const Dims &d, int64_t nao, int mode) {
   for (bf16 **q : {&b.Yv_hi, &b.Yv_lo}) *q = ar.take<bf16>(d.Mp * d.Kv);
   for (bf16 **q : {&b.Hl_hi, &b.Hl_lo, &b.Hg_hi, &b.Hg_lo}) *q = ar.take<bf16>(d.Mp * d.Mp);
   for (bf16 **q : {&b.XaT_hi, &b.XaT_lo, &b.RT_hi, &b.RT_lo}) *q = ar.take<bf16>(naop * d.Mp);
+  b.Zf = ar.take<float>(d.Mp * d.Mp);
   return b;
 }
 
@@ -1728,14 +1730,24 @@ int mbpt_sigma_ao(const double *X_ao, int64_t M, int64_t nao, const double *mo_c
     e.ld_out = d.Ap;
     int rc = gemm_split(umma::EPI_SPLIT, 1, &Dm, &Wm, d.Mp, d.Ap, e, err, st);
     if (rc) return rc;
+    // Zt = U D^T whole in FP32 (upper pair tiles, mirrored), then the G pass
+    // H< = G_occ o Zt, H> = G_virt o Zt, as in the diagonal sweep
+    e = umma::EpiArgs();
+    e.outf = b.Zf;
+    e.ld_outf = d.Mp;
+    e.alpha = 1.f;
+    rc = gemm_split(umma::EPI_F32, 1, &Um, &Dm, d.Mp, d.Mp, e, err, st, umma::BAND_UPPER);
+    if (rc) return rc;
     e = umma::EpiArgs();
     e.out0_hi = b.Hl_hi;
     e.out0_lo = b.Hl_lo;
     e.out1_hi = b.Hg_hi;
     e.out1_lo = b.Hg_lo;
     e.ld_out = d.Mp;
-    SplitMat A3[3] = {Yo, Yv, Um}, B3[3] = {Yo, Yv, Dm};
-    rc = gemm_split(umma::EPI_SIGMA_H, 3, A3, B3, d.Mp, d.Mp, e, err, st, umma::BAND_UPPER);
+    e.zt = b.Zf;
+    e.ld_zt = d.Mp;
+    SplitMat A2g[2] = {Yo, Yv};
+    rc = gemm_split(umma::EPI_SIGMA_HZ, 2, A2g, A2g, d.Mp, d.Mp, e, err, st, umma::BAND_UPPER);
     if (rc) return rc;
     const SplitMat *H[2] = {&Hl, &Hg};
     for (int br = 0; br < 2; ++br) {

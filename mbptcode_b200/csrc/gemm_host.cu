@@ -117,11 +117,11 @@ int launch(const SplitMat *A, const SplitMat *B, int64_t m_rows, int64_t n_rows,
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     const cudaError_t rc = cudaLaunchKernelEx(&cfg, kern, p);
-    if (timed) timing_end(st, EPI == umma::EPI_SIGMA_HZ ? umma::EPI_SIGMA_H : EPI, ev0, ev1);
+    if (timed) timing_end(st, EPI, ev0, ev1);
     return rc == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
   } else {
     kern<<<p.tiles_m * p.tiles_n, 64 + BN, L::kSmemBytes, st>>>(p);
-    if (timed) timing_end(st, EPI == umma::EPI_SIGMA_HZ ? umma::EPI_SIGMA_H : EPI, ev0, ev1);
+    if (timed) timing_end(st, EPI, ev0, ev1);
     return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
   }
 }
@@ -329,8 +329,6 @@ int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t 
                                                             band)
                  : launch<1, 256, EPI_F32, false, kDrain>(A, B, m_rows, n_rows, e, err, st,
                                                          band);
-    if (!tf && nacc == 3 && epi == EPI_SIGMA_H)
-      return launch<3, 128, EPI_SIGMA_H, false, kDrain>(A, B, m_rows, n_rows, e, err, st, band);
     // the two G products of Sigma's H (short K: not drained) against a stored Zt
     if (!tf && nacc == 2 && epi == EPI_SIGMA_HZ)
       return engine_pairs()
@@ -388,8 +386,6 @@ int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t 
     return launch<1, 128, EPI_F32_ACC, false, kDrain>(A, B, m_rows, n_rows, e, err, st);
   if (nacc == 2 && epi == EPI_HADAMARD_SPLIT)
     return launch<2, 128, EPI_HADAMARD_SPLIT, false, kDrain>(A, B, m_rows, n_rows, e, err, st);
-  if (nacc == 3 && epi == EPI_SIGMA_H)
-    return launch<3, 128, EPI_SIGMA_H, false, kDrain>(A, B, m_rows, n_rows, e, err, st);
   // the row contraction: two undrained accumulators, 256-wide on CTA pairs
   if (nacc == 2 && epi == EPI_ROWDOT2)
     return engine_pairs()

@@ -2,9 +2,10 @@
 //
 // Every product of the route's N^3 sweeps is C = A B^T with A (m x K) and
 // B (n x K) both K-contiguous, each operand held as a BF16 pair x = hi + lo.
-// One CTA owns a 128 x BN output tile and up to three accumulators in TMEM
-// (each its own (A, B, K) problem, e.g. G_occ, G_virt and Zt of the same grid
-// tile). Per 64-wide K slab it issues three tcgen05.mma per 16-wide step,
+// One CTA owns a 128 x BN output tile and one or two accumulators in TMEM
+// (each its own (A, B, K) problem, e.g. G_occ and G_virt of the same grid
+// tile); a CTA pair (cta_group::2) owns a 256 x BN tile, 128 rows each.
+// Per 64-wide K slab it issues three tcgen05.mma per 16-wide step,
 // hi*hi + hi*lo + lo*hi, all into the same FP32 accumulator (the lo*lo term,
 // 2^-18 relative, is dropped). Warp roles: warp 0 issues the TMA loads
 // (128B swizzle, no multicast), warp 1 owns TMEM and issues the MMAs, warps
@@ -26,13 +27,12 @@ enum Epi : int {
   EPI_SPLIT = 0,           // out0 = alpha * acc0, BF16 hi/lo
   EPI_F32 = 1,             // outf = alpha * acc0, FP32
   EPI_HADAMARD_SPLIT = 2,  // out0 = acc0 o acc1, BF16 hi/lo   (Pi = Go o Gv)
-  EPI_SIGMA_H = 3,         // out0 = acc0 o acc2, out1 = acc1 o acc2 (Go o Zt, Gv o Zt)
+  EPI_SIGMA_HZ = 3,        // out0 = acc0 o Zt, out1 = acc1 o Zt, Zt read (FP32) at zt
   EPI_ROWDOT2 = 4,         // sig0[c] += sum_r xs[r,c] acc0[r,c], sig1[c] -= ... acc1
   EPI_F32_ACC = 5,         // outf += alpha * acc0, FP32 read-modify-write
   EPI_TF32_PAIR = 6,       // alpha * acc0 as a TF32 hi/lo pair at p (and transposed at t)
   EPI_F64_SYM = 7,         // outd = alpha * acc0 - shift [row == col], FP64, rows and
                            // columns below nd, mirrored (with BAND_UPPER)
-  EPI_SIGMA_HZ = 8,        // out0 = acc0 o Zt, out1 = acc1 o Zt, Zt read (FP32) at zt
 };
 
 struct EpiArgs {
@@ -813,23 +813,6 @@ __global__ void __launch_bounds__(64 + BN, 1)
           if (mirror)
             store_split32_t(e.out0_hi + static_cast<int64_t>(col) * e.ld_out + row,
                             e.out0_lo + static_cast<int64_t>(col) * e.ld_out + row, e.ld_out, v0);
-        } else if constexpr (EPI == EPI_SIGMA_H) {
-          // acc0 = G_occ, acc1 = G_virt, acc2 = Zt
-          float z[32], v1[32];
-          load(2, c, z);
-#pragma unroll
-          for (int i = 0; i < 32; ++i) v0[i] *= z[i];
-          store_split32(e.out0_hi + row * e.ld_out + col, e.out0_lo + row * e.ld_out + col, v0);
-          if (mirror)
-            store_split32_t(e.out0_hi + static_cast<int64_t>(col) * e.ld_out + row,
-                            e.out0_lo + static_cast<int64_t>(col) * e.ld_out + row, e.ld_out, v0);
-          load(1, c, v1);
-#pragma unroll
-          for (int i = 0; i < 32; ++i) v1[i] *= z[i];
-          store_split32(e.out1_hi + row * e.ld_out + col, e.out1_lo + row * e.ld_out + col, v1);
-          if (mirror)
-            store_split32_t(e.out1_hi + static_cast<int64_t>(col) * e.ld_out + row,
-                            e.out1_lo + static_cast<int64_t>(col) * e.ld_out + row, e.ld_out, v1);
         } else if constexpr (EPI == EPI_SIGMA_HZ) {
           // acc0 = G_occ, acc1 = G_virt; Zt (symmetric, stored whole) from memory
           float z[32], v1[32];
