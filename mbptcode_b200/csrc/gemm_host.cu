@@ -320,9 +320,17 @@ int gemm_split(int epi, int nacc, const SplitMat *A, const SplitMat *B, int64_t 
   if (band == BAND_UPPER && !(tf && nacc == 1)) {
     // symmetric products of full K: the upper tiles, mirrored by the epilogue
     if (m_rows != n_rows) return MBPT_ERR_SHAPE;
-    if (tf && nacc == 2 && epi == EPI_HADAMARD_SPLIT)
+    if (tf && nacc == 2 && epi == EPI_HADAMARD_SPLIT) {
+      if (engine_pairs()) {
+        // 256-wide pairs: the drained (long, second) product goes first, the
+        // other reuses one of its TMEM buffers; the Hadamard is symmetric
+        const SplitMat A2[2] = {A[1], A[0]}, B2[2] = {B[1], B[0]};
+        return launch<2, 256, EPI_HADAMARD_SPLIT, true, kDrain, 2>(A2, B2, m_rows, n_rows, e,
+                                                                   err, st, band);
+      }
       return launch<2, 128, EPI_HADAMARD_SPLIT, true, kDrain>(A, B, m_rows, n_rows, e, err, st,
                                                               band);
+    }
     if (!tf && nacc == 1 && epi == EPI_F32)
       return engine_pairs()
                  ? launch<1, 256, EPI_F32, false, kDrain, 2>(A, B, m_rows, n_rows, e, err, st,

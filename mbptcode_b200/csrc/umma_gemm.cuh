@@ -405,8 +405,11 @@ struct Layout {
   static constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
   static constexpr int kStages = (kStageBytes <= 64 * 1024) ? 3 : 2;
   static constexpr int kSmemBytes = kStages * kStageBytes + 1024 + 256;
-  // a drained last accumulator takes two buffers
-  static constexpr int kCols = (NACC + (DRAIN ? 1 : 0)) * BN;
+  // a drained last accumulator takes two buffers; two 256-wide accumulators
+  // with a drain fit only as the drained one first, the other reusing one of
+  // its buffers (kDrainFirst)
+  static constexpr bool kDrainFirst = BN == 256 && NACC == 2 && DRAIN;
+  static constexpr int kCols = kDrainFirst ? 2 * BN : (NACC + (DRAIN ? 1 : 0)) * BN;
   static constexpr int kTmemCols = (kCols <= 32) ? 32 : (kCols <= 64) ? 64
                                    : (kCols <= 128) ? 128 : (kCols <= 256) ? 256 : 512;
   static_assert(kCols <= 512, "accumulators exceed TMEM");
@@ -437,8 +440,8 @@ template <int NACC, int BN, int EPI, bool TF32 = false, int DRAIN = 0, int NGRP 
 __global__ void __launch_bounds__(64 + BN, 1)
     gemm_split_kernel(const __grid_constant__ Params<NACC, NGRP> p) {
   constexpr bool kPair = CTAS == 2;
-  static_assert(!kPair || (BN == 256 && NGRP == 0 && (NACC == 1 || (NACC == 2 && DRAIN == 0))),
-                "CTA pairs: 256-wide tiles, one accumulator or two undrained, single products");
+  static_assert(!kPair || (BN == 256 && NGRP == 0 && NACC <= 2),
+                "CTA pairs: 256-wide tiles of one or two accumulators, single products");
   using L = Layout<NACC, BN, (DRAIN > 0), CTAS>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -490,6 +493,11 @@ __global__ void __launch_bounds__(64 + BN, 1)
   const int tm = tm_pair + static_cast<int>(rank);
   const int m0 = tm * BM, n0 = tn * BN;
   constexpr int kLast = NACC - 1;
+  // the drained accumulator: the last one, or the first with kDrainFirst (its
+  // chunks then go through TMEM columns [0, 2 BN) and the other accumulator
+  // takes the buffer the chunk after its last would have used)
+  constexpr bool kDrainFirst = L::kDrainFirst;
+  constexpr int kDr = kDrainFirst ? 0 : kLast;
   // uniform across the CTA (and the pair), before any barrier or TMEM exists:
   // a symmetric product skips tiles whose last 128-column block lies below
   // the diagonal
@@ -604,10 +612,26 @@ __global__ void __launch_bounds__(64 + BN, 1)
       int it = 0;
       bool ok = true;
       for (int j = 0; j < NACC && ok; ++j) {
-        const bool drained = DRAIN > 0 && j == kLast;
+        const bool drained = DRAIN > 0 && j == kDr;
         uint32_t d = tmem + static_cast<uint32_t>(j * BN);
         int buf = 0;
         int kb, ke;
+        if constexpr (kDrainFirst) {
+          if (j != kDr) {
+            // the buffer of drained chunk nch, once the epilogue has read
+            // chunk nch - 2 from it
+            k_span(kDr, kb, ke);
+            const int nch = (ke - kb + DRAIN - 1) / DRAIN;
+            const uint32_t par = ((nch >> 1) & 1) ^ 1;
+            if (!(kPair ? mbar_wait_cluster(&dempty[nch & 1], par)
+                        : mbar_wait(&dempty[nch & 1], par))) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            d = tmem + static_cast<uint32_t>((nch & 1) * BN);
+          }
+        }
         k_span(j, kb, ke);
         for (int kt = kb; kt < ke; ++kt, ++it) {
           const int q = kt - kb;  // slab index within this tile's K span
@@ -621,7 +645,7 @@ __global__ void __launch_bounds__(64 + BN, 1)
               break;
             }
             tc_fence_after();
-            d = tmem + static_cast<uint32_t>((kLast + buf) * BN);
+            d = tmem + static_cast<uint32_t>((kDr + buf) * BN);
           }
           const int s = it % L::kStages;
           const uint32_t ph = (it / L::kStages) & 1;
@@ -680,7 +704,7 @@ __global__ void __launch_bounds__(64 + BN, 1)
 #pragma unroll
       for (int i = 0; i < 128; ++i) acc[i] = 0.f;
       int kb, ke;
-      k_span(kLast, kb, ke);
+      k_span(kDr, kb, ke);
       const int nchunks = (ke - kb + DRAIN - 1) / DRAIN;
       for (int c = 0; c < nchunks; ++c) {
         const int b = c & 1;
@@ -694,7 +718,7 @@ __global__ void __launch_bounds__(64 + BN, 1)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           float t[32];
-          tmem_ld32(taddr + static_cast<uint32_t>((kLast + b) * BN + cb + 32 * q), t);
+          tmem_ld32(taddr + static_cast<uint32_t>((kDr + b) * BN + cb + 32 * q), t);
 #pragma unroll
           for (int i = 0; i < 32; ++i) acc[32 * q + i] += t[i];
         }
@@ -725,15 +749,23 @@ __global__ void __launch_bounds__(64 + BN, 1)
       const bool mirror = upper && tb > tm;
       // 32 columns starting at the warp's column c of accumulator j (the
       // drained one from registers)
+      int col_of[NACC];
+#pragma unroll
+      for (int j = 0; j < NACC; ++j) col_of[j] = j * BN;
+      if constexpr (kDrainFirst) {
+        int kb, ke;
+        k_span(kDr, kb, ke);
+        col_of[1] = (((ke - kb + DRAIN - 1) / DRAIN) & 1) * BN;
+      }
       auto load = [&](int j, int c, float (&v)[32]) {
         if constexpr (DRAIN > 0) {
-          if (j == kLast) {
+          if (j == kDr) {
 #pragma unroll
             for (int i = 0; i < 32; ++i) v[i] = acc[c + i];
             return;
           }
         }
-        tmem_ld32(taddr + static_cast<uint32_t>(j * BN + cb + c), v);
+        tmem_ld32(taddr + static_cast<uint32_t>(col_of[j] + cb + c), v);
       };
       // columns past n_valid (a 256-wide tile over a 128-multiple edge) are not
       // stored, nor the rows of a pair's second tile past m_valid
