@@ -69,8 +69,8 @@ FLOPS = {
 # engine kernels at this workload, from one ncu capture of a tau point at full
 # size (python bench_cases.py tau --M 7200 --n 1200 --nocc 120
 # --states 1200, the seven engine launches of one tau point)
-TRAFFIC_BYTES = {'hadamard': 313.3e6, 'split': 1942.4e6, 'f32': 1144.9e6,
-                 'sigma_hadamard': 591.5e6, 'row_contraction': 702.3e6}
+TRAFFIC_BYTES = {'hadamard': 362.1e6, 'split': 1955.8e6, 'f32': 1143.4e6,
+                 'sigma_hadamard': 591.7e6, 'row_contraction': 702.7e6}
 # algorithmic FLOPs of the Dyson step's inverse per frequency (triangular inverse
 # n^3/3 + L^-T L^-1 n^3/3, the classical SPD-inverse count), spread over launches
 # of many sizes: rated on their summed time
