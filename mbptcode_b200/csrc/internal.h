@@ -147,9 +147,6 @@ void launch_transform(const Tin *in, int64_t in_slice, int64_t ld_in, int64_t ro
 void launch_transform_acc(const double *in, int64_t in_slice, int64_t ld_in, int64_t rows,
                           int64_t cols, const double *w_dev, int J, int K, double *out,
                           int64_t out_slice, int64_t ld_out, cudaStream_t st);
-void launch_transform_split(const double *in, int64_t in_slice, int64_t ld_in, int64_t rows,
-                            int64_t cols, const double *w_dev, int J, int K, bf16 *out_hi,
-                            bf16 *out_lo, int64_t out_slice, int64_t ld_out, cudaStream_t st);
 // a <- I - a per n x n slice; with trace, trace[f] = tr a first
 void launch_one_minus(double *a, int64_t n, int nmat, double *trace, cudaStream_t st);
 void launch_trace(const double *a, int64_t n, int nmat, double *trace, cudaStream_t st);

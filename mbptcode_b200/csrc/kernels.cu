@@ -192,11 +192,11 @@ constexpr int kMaxJ = 34;  // largest tabulated minimax grid
 // out[j][r, c] = sum_k w[j,k] in[k][r, c] (ACC: added to out); one element
 // per thread, the J output sums in registers, so every input element is read
 // once and every output written once.
-template <typename Tin, bool SPLIT, bool ACC = false>
+template <typename Tin, bool ACC = false>
 __global__ void __launch_bounds__(256) transform_kernel(
     const Tin *__restrict__ in, int64_t in_slice, int64_t ld_in, int64_t rows, int64_t cols,
-    const double *__restrict__ w, int J, int K, double *__restrict__ out, bf16 *out_hi,
-    bf16 *out_lo, int64_t out_slice, int64_t ld_out) {
+    const double *__restrict__ w, int J, int K, double *__restrict__ out, int64_t out_slice,
+    int64_t ld_out) {
   __shared__ double ws[kMaxJ * kMaxJ];
   for (int i = threadIdx.x; i < J * K; i += blockDim.x) ws[i] = w[i];
   __syncthreads();
@@ -219,12 +219,7 @@ __global__ void __launch_bounds__(256) transform_kernel(
 #pragma unroll
     for (int j = 0; j < kMaxJ; ++j) {
       if (j < J) {
-        if constexpr (SPLIT) {
-          bf16 h, l;
-          split_bf16(static_cast<float>(acc[j]), h, l);
-          out_hi[j * out_slice + o] = h;
-          out_lo[j * out_slice + o] = l;
-        } else if constexpr (ACC) {
+        if constexpr (ACC) {
           out[j * out_slice + o] += acc[j];
         } else {
           out[j * out_slice + o] = acc[j];
@@ -518,8 +513,8 @@ void launch_transform(const Tin *in, int64_t in_slice, int64_t ld_in, int64_t ro
     }
 #undef MBPT_TRANSFORM_N
   }
-  count_launch(); transform_kernel<Tin, false><<<grid_cap(rows * cols), 256, 0, st>>>(
-      in, in_slice, ld_in, rows, cols, w_dev, J, K, out, nullptr, nullptr, out_slice, ld_out);
+  count_launch(); transform_kernel<Tin><<<grid_cap(rows * cols), 256, 0, st>>>(
+      in, in_slice, ld_in, rows, cols, w_dev, J, K, out, out_slice, ld_out);
 }
 template void launch_transform<double>(const double *, int64_t, int64_t, int64_t, int64_t,
                                        const double *, int, int, double *, int64_t, int64_t,
@@ -531,16 +526,10 @@ template void launch_transform<float>(const float *, int64_t, int64_t, int64_t, 
 void launch_transform_acc(const double *in, int64_t in_slice, int64_t ld_in, int64_t rows,
                           int64_t cols, const double *w_dev, int J, int K, double *out,
                           int64_t out_slice, int64_t ld_out, cudaStream_t st) {
-  count_launch(); transform_kernel<double, false, true><<<grid_cap(rows * cols), 256, 0, st>>>(
-      in, in_slice, ld_in, rows, cols, w_dev, J, K, out, nullptr, nullptr, out_slice, ld_out);
+  count_launch(); transform_kernel<double, true><<<grid_cap(rows * cols), 256, 0, st>>>(
+      in, in_slice, ld_in, rows, cols, w_dev, J, K, out, out_slice, ld_out);
 }
 
-void launch_transform_split(const double *in, int64_t in_slice, int64_t ld_in, int64_t rows,
-                            int64_t cols, const double *w_dev, int J, int K, bf16 *out_hi,
-                            bf16 *out_lo, int64_t out_slice, int64_t ld_out, cudaStream_t st) {
-  count_launch(); transform_kernel<double, true><<<grid_cap(rows * cols), 256, 0, st>>>(
-      in, in_slice, ld_in, rows, cols, w_dev, J, K, nullptr, out_hi, out_lo, out_slice, ld_out);
-}
 
 void launch_trace(const double *a, int64_t n, int nmat, double *trace, cudaStream_t st) {
   count_launch(); trace_kernel<<<nmat, 256, 0, st>>>(a, n, trace);
