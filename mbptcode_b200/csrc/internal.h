@@ -166,6 +166,5 @@ void launch_sigma_frequency(const double *branch, int ntau, int nstates, const d
                             const double *S, int npade, double *sigma, cudaStream_t st);
 void launch_energy_sum(const double *logdet, const double *trace, const double *w, int nfreq,
                        double *e_c, cudaStream_t st);
-void launch_fill(double *a, double v, int64_t n, cudaStream_t st);
 
 }  // namespace mbpt

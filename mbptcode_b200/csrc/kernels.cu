@@ -410,12 +410,6 @@ __global__ void energy_sum_kernel(const double *logdet, const double *trace, con
   *e_c = e / (2.0 * 3.14159265358979323846);
 }
 
-__global__ void fill_kernel(double *a, double v, int64_t n) {
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    a[i] = v;
-}
-
 inline int grid_cap(int64_t n) {
   const int b = blocks_for(n);
   return b > 148 * 32 ? 148 * 32 : b;
@@ -585,10 +579,6 @@ void launch_sigma_frequency(const double *branch, int ntau, int nstates, const d
 void launch_energy_sum(const double *logdet, const double *trace, const double *w, int nfreq,
                        double *e_c, cudaStream_t st) {
   count_launch(); energy_sum_kernel<<<1, 32, 0, st>>>(logdet, trace, w, nfreq, e_c);
-}
-
-void launch_fill(double *a, double v, int64_t n, cudaStream_t st) {
-  count_launch(); fill_kernel<<<grid_cap(n), kThreads, 0, st>>>(a, v, n);
 }
 
 }  // namespace mbpt
