@@ -134,17 +134,20 @@ bool engine_pairs() {
 
 constexpr int kMaxGroups = 32;
 
-// One grouped launch of up to kMaxGroups single-accumulator TF32 products.
-template <int EPI, int DRAIN>
+// One grouped launch of up to kMaxGroups single-accumulator TF32 products:
+// 128 x 128 tiles one CTA each, or (CTAS = 2) 256 x 256 tiles on CTA pairs,
+// whose overhang past a product's 128-multiple edges reads neighbouring rows
+// and stores nothing (each group's m_valid / n_valid).
+template <int EPI, int DRAIN, int BN = 128, int CTAS = 1>
 int launch_grouped(const SplitMat &A, const SplitMat &B, const GemmGroup *g, int ng,
                    const umma::EpiArgs &e, int *err, cudaStream_t st, int band) {
-  using L = umma::Layout<1, 128, (DRAIN > 0)>;
+  using L = umma::Layout<1, BN, (DRAIN > 0), CTAS>;
   if (!A.tf32 || !B.tf32 || ng < 1 || ng > kMaxGroups) return MBPT_ERR_SHAPE;
   umma::Params<1, kMaxGroups> p;
   if (!make_tmap(&p.tm[0], A.hi, A.rows, A.cols, A.ld, umma::BM, true) ||
       !make_tmap(&p.tm[1], A.lo, A.rows, A.cols, A.ld, umma::BM, true) ||
-      !make_tmap(&p.tm[2], B.hi, B.rows, B.cols, B.ld, 128, true) ||
-      !make_tmap(&p.tm[3], B.lo, B.rows, B.cols, B.ld, 128, true))
+      !make_tmap(&p.tm[2], B.hi, B.rows, B.cols, B.ld, BN / CTAS, true) ||
+      !make_tmap(&p.tm[3], B.lo, B.rows, B.cols, B.ld, BN / CTAS, true))
     return MBPT_ERR_SHAPE;
   int tiles = 0;
   for (int i = 0; i < ng; ++i) {
@@ -159,7 +162,9 @@ int launch_grouped(const SplitMat &A, const SplitMat &B, const GemmGroup *g, int
     umma::Group &G = p.grp[i];
     G.tile_base = tiles;
     G.tiles_m = static_cast<int>(q.m_rows / umma::BM);
-    G.tiles_n = static_cast<int>(q.n_rows / 128);
+    G.tiles_n = static_cast<int>((q.n_rows + BN - 1) / BN);
+    G.m_valid = static_cast<int>(q.m_rows);
+    G.n_valid = static_cast<int>(q.n_rows);
     G.a_row0 = static_cast<int>(q.a_row0);
     G.a_k0 = static_cast<int>(q.a_k0);
     G.b_row0 = static_cast<int>(q.b_row0);
@@ -167,7 +172,8 @@ int launch_grouped(const SplitMat &A, const SplitMat &B, const GemmGroup *g, int
     G.k_tiles = static_cast<int>(kp / 32);
     G.p_off = q.p_off;
     G.t_off = q.t_off;
-    tiles += G.tiles_m * G.tiles_n;
+    // launch units: tiles, or pairs of row tiles
+    tiles += (CTAS == 2 ? (G.tiles_m + 1) / 2 : G.tiles_m) * G.tiles_n;
   }
   p.ngroups = ng;
   p.k_tiles[0] = 0;
@@ -177,16 +183,34 @@ int launch_grouped(const SplitMat &A, const SplitMat &B, const GemmGroup *g, int
   p.band = band;
   p.epi = e;
   p.err = err;
-  auto kern = umma::gemm_split_kernel<1, 128, EPI, true, DRAIN, kMaxGroups>;
+  auto kern = umma::gemm_split_kernel<1, BN, EPI, true, DRAIN, kMaxGroups, CTAS>;
   static std::atomic<uint64_t> attr_set{0};  // one bit per device
   if (!allow_smem(reinterpret_cast<const void *>(kern), L::kSmemBytes, attr_set))
     return MBPT_ERR_CUDA;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   const bool timed = timing_begin(st, &ev0, &ev1);
   count_launch();
-  kern<<<tiles, 192, L::kSmemBytes, st>>>(p);
+  cudaError_t rc;
+  if constexpr (CTAS == 2) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(static_cast<unsigned>(2 * tiles));
+    cfg.blockDim = dim3(64 + BN);
+    cfg.dynamicSmemBytes = L::kSmemBytes;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    rc = cudaLaunchKernelEx(&cfg, kern, p);
+  } else {
+    kern<<<tiles, 64 + BN, L::kSmemBytes, st>>>(p);
+    rc = cudaGetLastError();
+  }
   if (timed) timing_end(st, EPI, ev0, ev1);
-  return cudaGetLastError() == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
+  return rc == cudaSuccess ? MBPT_OK : MBPT_ERR_CUDA;
 }
 
 }  // namespace
@@ -199,7 +223,11 @@ int gemm_split_grouped(int epi, const SplitMat &A, const SplitMat &B, const Gemm
     const int ng = std::min(kMaxGroups, ngroups - first);
     int rc = MBPT_ERR_UNSUPPORTED;
     if (epi == umma::EPI_TF32_PAIR)
-      rc = launch_grouped<umma::EPI_TF32_PAIR, kDrain>(A, B, groups + first, ng, e, err, st, band);
+      rc = engine_pairs()
+               ? launch_grouped<umma::EPI_TF32_PAIR, kDrain, 256, 2>(A, B, groups + first, ng, e,
+                                                                     err, st, band)
+               : launch_grouped<umma::EPI_TF32_PAIR, kDrain>(A, B, groups + first, ng, e, err,
+                                                             st, band);
     if (rc) return rc;
   }
   return MBPT_OK;

@@ -83,6 +83,7 @@ struct Group {
   int b_row0, b_k0;    // origin of its B block
   int k_tiles;         // K slabs from the origin
   int64_t p_off, t_off;  // element offsets of its output (and transposed output)
+  int m_valid, n_valid;  // its output rows and columns (tiles past them store nothing)
 };
 
 template <int NACC, int NGRP = 0>
@@ -440,8 +441,8 @@ template <int NACC, int BN, int EPI, bool TF32 = false, int DRAIN = 0, int NGRP 
 __global__ void __launch_bounds__(64 + BN, 1)
     gemm_split_kernel(const __grid_constant__ Params<NACC, NGRP> p) {
   constexpr bool kPair = CTAS == 2;
-  static_assert(!kPair || (BN == 256 && NGRP == 0 && NACC <= 2),
-                "CTA pairs: 256-wide tiles of one or two accumulators, single products");
+  static_assert(!kPair || (BN == 256 && (NGRP == 0 ? NACC <= 2 : NACC == 1)),
+                "CTA pairs: 256-wide tiles of one or two accumulators (one when grouped)");
   using L = Layout<NACC, BN, (DRAIN > 0), CTAS>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -462,6 +463,7 @@ __global__ void __launch_bounds__(64 + BN, 1)
   int pid = kPair ? static_cast<int>(blockIdx.x >> 1) : static_cast<int>(blockIdx.x);
   int tiles_m = p.tiles_m, tiles_n = p.tiles_n;
   int a_row0 = 0, a_k0 = 0, b_row0 = 0, b_k0 = 0, grp_k_tiles = 0;
+  int m_valid = p.m_valid, n_valid = p.n_valid;
   int64_t p_off = 0, t_off = 0;
   if constexpr (NGRP > 0) {
     int g = 0;
@@ -477,6 +479,8 @@ __global__ void __launch_bounds__(64 + BN, 1)
     grp_k_tiles = G.k_tiles;
     p_off = G.p_off;
     t_off = G.t_off;
+    m_valid = G.m_valid;
+    n_valid = G.n_valid;
   }
   // grouped raster: kGroupM row tiles sweep the column tiles together (L2
   // reuse); a pair's unit is two row tiles, so half as many units per group
@@ -769,7 +773,7 @@ __global__ void __launch_bounds__(64 + BN, 1)
       };
       // columns past n_valid (a 256-wide tile over a 128-multiple edge) are not
       // stored, nor the rows of a pair's second tile past m_valid
-      const bool live = n0 + cb < p.n_valid && m0 < p.m_valid && !(upper && tb < tm);
+      const bool live = n0 + cb < n_valid && m0 < m_valid && !(upper && tb < tm);
 #pragma unroll
       for (int c = 0; c < 128; c += 32) {
         if (!live) break;
