@@ -603,20 +603,23 @@ int chol_batched(double *A, int64_t n, int nmat, int *info, double *P, double *L
 
 // The batched Cholesky's trailing updates: on the int8 tensor cores (the
 // Ozaki scheme) in mixed mode, as native FP64 DGEMMs in FP64 mode (the plain
-// FP64 path the mixed one is measured against). Digits per operand: 7 in
-// mixed mode (the log-determinant at FP64 level, the factor within ~1e-13;
-// W is formed from it by TF32x3 products there), 8 when forced in FP64 mode
+// FP64 path the mixed one is measured against). Digits per operand: in
+// mixed mode 6 signed 8-bit digits (the log-determinant within 1e-14 of
+// LAPACK, W from the factor within ~2e-12 of its largest entry; W is formed
+// from it by TF32x3 products there), 8 when forced in FP64 mode
 // (W within ~1e-14). MBPT_DYSON_OZAKI=1 / =0 forces the int8 path or the
-// DGEMMs in both modes, MBPT_DYSON_OZAKI_SLICES=7 / 8 the digits. Read at
-// every call, so the size query and the call that follows it must see the
-// same setting.
-int ozaki_slices(int mode) {
+// DGEMMs in both modes, MBPT_DYSON_OZAKI_SLICES=6 / 7 / 8 the digits (6:
+// signed 8-bit digits, whose exact int32 level sums hold K below 22 016, so
+// larger matrices take 7). Read at every call, so the size query and the call
+// that follows it must see the same setting.
+int ozaki_slices(int mode, int64_t n) {
   const char *e = std::getenv("MBPT_DYSON_OZAKI");
   const bool on = e ? std::atoi(e) != 0 : mode != MBPT_MODE_FP64;
   if (!on) return 0;
   const char *k = std::getenv("MBPT_DYSON_OZAKI_SLICES");
-  const int v = k ? std::atoi(k) : (mode == MBPT_MODE_MIXED ? 7 : 8);
-  return (v == 7 || v == 8) ? v : 8;
+  int v = k ? std::atoi(k) : (mode == MBPT_MODE_MIXED ? 6 : 8);
+  if (v == 6 && n > kOzakiEightBitMaxK) v = 7;
+  return (v == 6 || v == 7 || v == 8) ? v : 8;
 }
 
 // Mixed mode: the tensor-core inverses of that many frequencies run at once,
@@ -687,7 +690,7 @@ DysonBufs carve_dyson(Arena &ar, int64_t n, int nfreq, int mode = MBPT_MODE_FP64
     // every step's inverted diagonal blocks are kept: the mixed inverse reads them
     const int64_t steps = (n + kCholNb - 1) / kCholNb;
     b.chol_Linv = ar.take<double>(steps * nfreq * kCholNb * kCholNb);
-    b.oz_slices = ozaki_slices(mode);
+    b.oz_slices = ozaki_slices(mode, n);
     if (b.oz_slices) {
       b.oz_planes = ar.take<int8_t>(ozaki_planes_bytes(n, nfreq, b.oz_slices));
       b.oz_scale = ar.take<double>(static_cast<int64_t>(nfreq) * n);

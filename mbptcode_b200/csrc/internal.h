@@ -59,6 +59,8 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn();
 bool allow_smem(const void *kern, int bytes, std::atomic<uint64_t> &done);
 
 // ---- Ozaki-scheme FP64 updates of the batched Cholesky (ozaki.cu) ----
+// Largest K (matrix size) of the 8-bit digit updates (slices = 6): 6 127^2 K < 2^31.
+constexpr int64_t kOzakiEightBitMaxK = 22016;
 // Bytes of the int8 digit planes of nmat n x n factors cut into `slices`.
 size_t ozaki_planes_bytes(int64_t n, int nmat, int slices);
 // scale[f][r] = 2^e_r >= sqrt(A_rr) of each matrix (column-major, ld n; of

@@ -1,6 +1,13 @@
 // FP64-accurate trailing updates of the batched Cholesky on the int8 tensor
 // cores (tcgen05.mma kind::i8, exact int32 accumulation): the Ozaki scheme.
 //
+// Digit widths: S = 7 and 8 cut signed 7-bit digits (d_s in [-64, 64], base
+// 128, as below); S = 6 cuts signed 8-bit digits of base 254 (x = L_rk / 2^e_r,
+// t = 127 x, d_1 = rint(t), then t <- 254 (t - d); d_s in [-127, 127], 47 bits
+// in all, against 49 for S = 7), whose levels 2..7 take 21 digit products per
+// K step instead of 28. Level l weighs 127^-2 254^-(l-2), exact to one
+// rounding in FP64; its int32 sums stay exact for K below 2^31 / (6 127^2).
+//
 // Each row r of the factor L is scaled by 2^-e_r, with 2^e_r >= sqrt(A_rr)
 // (|L_rk| <= sqrt(A_rr) for a positive definite A), and cut into S signed
 // digits: x = L_rk 2^-e_r, |x| <= 1, x = sum_s d_s 2^-(7s-1) + O(2^-7S),
@@ -146,6 +153,7 @@ struct UpdateArgs {
 
 template <int S, int EPI>
 __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_constant__ UpdateArgs p) {
+  static_assert(S != 6 || EPI == EPI_CHOL, "8-bit digits: the Cholesky's planes only");
   using L = Layout<S>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -287,7 +295,15 @@ __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_consta
         for (int lev = S + 1; lev >= 2; --lev) {
           int v[32];
           tmem_ld32_s32(taddr + static_cast<uint32_t>((lev - 2) * BN + ch * 32), v);
-          const double w = ldexp(1.0, 2 - 7 * lev);
+          double w;
+          if constexpr (S == 6) {
+            // 1 / (127^2 254^(lev - 2)): the power is an exact integer below 2^53
+            double pw = 16129.0;
+            for (int q = 2; q < lev; ++q) pw *= 254.0;
+            w = 1.0 / pw;
+          } else {
+            w = ldexp(1.0, 2 - 7 * lev);
+          }
 #pragma unroll
           for (int i = 0; i < 32; ++i) acc[i] += static_cast<double>(v[i]) * w;
         }
@@ -404,17 +420,19 @@ __global__ void chol_slice_kernel(const double *A, int64_t n, int64_t mat_stride
   sq += __shfl_xor_sync(0xffffffffu, sq, 4);
   if (r >= n) return;
   if (cg == 0) rownorm[static_cast<int64_t>(f) * n + r] += sq;
-  const double inv = 64.0 / scale[static_cast<int64_t>(f) * n + r];
+  // 7-bit digits: |t| <= 64, base 128; 8-bit (S = 6): |t| <= 127, base 254
+  constexpr double kTop = S == 6 ? 127.0 : 64.0, kBase = S == 6 ? 254.0 : 128.0;
+  const double inv = kTop / scale[static_cast<int64_t>(f) * n + r];
   __align__(16) int8_t out[S][16];
 #pragma unroll
   for (int i = 0; i < 16; ++i) {
-    double t = tile[rr][cg + i] * inv;   // |t| <= 64
+    double t = tile[rr][cg + i] * inv;   // |t| <= kTop
 #pragma unroll
     for (int q = 0; q < S; ++q) {
       double d = rint(t);
       d = fmin(fmax(d, -127.0), 127.0);  // non-finite input stays in range
       out[q][i] = static_cast<int8_t>(static_cast<int>(d));
-      t = (t - d) * 128.0;
+      t = (t - d) * kBase;
     }
   }
   if (cg >= nb) return;
@@ -568,6 +586,9 @@ int ozaki_chol_slice(const double *A, int64_t n, int nmat, int64_t j0, int nb,
   if (slices == 8)
     ozaki::chol_slice_kernel<8><<<grid, 256, 0, st>>>(A, n, n * n, nmat, static_cast<int>(j0),
                                                       nb, scale, planes, npad, rownorm);
+  else if (slices == 6)
+    ozaki::chol_slice_kernel<6><<<grid, 256, 0, st>>>(A, n, n * n, nmat, static_cast<int>(j0),
+                                                      nb, scale, planes, npad, rownorm);
   else if (slices == 7)
     ozaki::chol_slice_kernel<7><<<grid, 256, 0, st>>>(A, n, n * n, nmat, static_cast<int>(j0),
                                                       nb, scale, planes, npad, rownorm);
@@ -580,7 +601,9 @@ int ozaki_chol_update(double *A, int64_t n, int nmat, int64_t j0, int nb, double
                       const double *scale, const int8_t *planes, int slices, double *rowsq,
                       int *err, cudaStream_t st) {
   if (j0 <= 0) return MBPT_OK;
-  if (j0 % ozaki::BKB || nb < 1 || nb > 128 || j0 >= 65536) return MBPT_ERR_SHAPE;
+  if (j0 % ozaki::BKB || nb < 1 || nb > 128 || j0 >= 65536 ||
+      (slices == 6 && j0 > kOzakiEightBitMaxK))
+    return MBPT_ERR_SHAPE;
   const int64_t npad = round_up(n, 128);
   ozaki::UpdateArgs p{};
   if (!ozaki::make_plane_map(&p.tm_a, planes, npad, static_cast<int64_t>(slices) * nmat,
@@ -608,8 +631,14 @@ int ozaki_chol_update(double *A, int64_t n, int nmat, int64_t j0, int nb, double
   p.m_rows = p.n_cols = 0;
   p.err = err;
   const dim3 grid(static_cast<unsigned>(p.tiles_m * 2), nmat);
-  static std::atomic<uint64_t> attr8{0}, attr7{0};
-  if (slices == 8) {
+  static std::atomic<uint64_t> attr8{0}, attr7{0}, attr6{0};
+  if (slices == 6) {
+    auto kern = ozaki::chol_update_kernel<6, ozaki::EPI_CHOL>;
+    const int smem = ozaki::Layout<6>::kSmemBytes;
+    if (!allow_smem(reinterpret_cast<const void *>(kern), smem, attr6)) return MBPT_ERR_CUDA;
+    count_launch();
+    kern<<<grid, 192, smem, st>>>(p);
+  } else if (slices == 8) {
     auto kern = ozaki::chol_update_kernel<8, ozaki::EPI_CHOL>;
     const int smem = ozaki::Layout<8>::kSmemBytes;
     if (!allow_smem(reinterpret_cast<const void *>(kern), smem, attr8)) return MBPT_ERR_CUDA;
