@@ -429,8 +429,9 @@ struct Layout {
 // BN = 128: 6 warps (producer, MMA, 4 epilogue); BN = 256: 10 warps, the 8
 // epilogue warps covering the TMEM lane quarters twice, 128 columns each.
 //
-// CTAS = 2 (launched as clusters of two, BF16, dense K): the CTA pair forms a
-// 256 x BN tile with cta_group::2 MMAs issued by the first CTA. Each CTA loads
+// CTAS = 2 (launched as clusters of two; BF16 or TF32; a band's K span taken
+// per pair): the CTA pair forms a 256 x BN tile with cta_group::2 MMAs issued
+// by the first CTA. Each CTA loads
 // its own 128 rows of A and its half of B's rows, both completing on the first
 // CTA's full barrier; the commits arrive in both CTAs; the second CTA's
 // epilogue warps release drained buffers on the first CTA's barrier. Per K
