@@ -308,15 +308,30 @@ __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_consta
           for (int i = 0; i < 32; ++i) acc[i] += static_cast<double>(v[i]) * w;
         }
         if (EPI == EPI_CHOL && live) {
+          // all 32 loads first (P's column entries and the columns' scales),
+          // then the stores: one memory round trip per chunk instead of one
+          // per column, which the compiler cannot reorder across the stores
+          // (two halves of 16 columns: the registers hold acc and one half)
+          double *Prow = P + pr;   // column pc of the panel at Prow + pc m
+          // the diagonal entry from the exact running row norm
+          const int pd = pr - c0 - ch * 32;
+          const double diag = (pd >= 0 && pd < 32 && pr < p.nb)
+                                  ? p.rowsq[static_cast<int64_t>(f) * p.n + p.j0 + pr] : 0.0;
 #pragma unroll
-          for (int i = 0; i < 32; ++i) {
-            const int pc = c0 + ch * 32 + i;        // panel column
-            if (pc < p.nb) {
-              double *dst = P + static_cast<int64_t>(pc) * m + pr;
-              if (pr == pc)
-                *dst -= p.rowsq[static_cast<int64_t>(f) * p.n + p.j0 + pc];
-              else
-                *dst -= acc[i] * srow * sc[p.j0 + pc];
+          for (int h = 0; h < 32; h += 16) {
+            double old[16], scol[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const int pc = c0 + ch * 32 + h + i;  // panel column
+              old[i] = pc < p.nb ? Prow[static_cast<int64_t>(pc) * m] : 0.0;
+              scol[i] = pc < p.nb ? sc[p.j0 + pc] : 0.0;
+            }
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+              const int pc = c0 + ch * 32 + h + i;
+              if (pc < p.nb)
+                Prow[static_cast<int64_t>(pc) * m] =
+                    pr == pc ? old[i] - diag : old[i] - acc[h + i] * srow * scol[i];
             }
           }
         } else if (EPI == EPI_GEMM && live) {
