@@ -337,29 +337,44 @@ __global__ void __launch_bounds__(192, 1) chol_update_kernel(const __grid_consta
         } else if (EPI == EPI_GEMM && live) {
           const int64_t ro = static_cast<int64_t>(pr) * p.ldc;
           const double a = p.alpha * srow;
+          // eight columns at a time: their loads (column scales, factors, the
+          // old C) ahead of their stores, one memory round trip per eight
 #pragma unroll
-          for (int i = 0; i < 32; ++i) {
-            const int col = c0 + ch * 32 + i;
-            // symmetric: the upper triangle, each entry also at its mirror
-            // (the lanes' rows are consecutive, so the mirrored stores of
-            // one column coalesce)
-            if (col < p.n_cols && (!p.sym || col >= pr)) {
-              const double v = a * acc[i] * p.scale_b[col];
-              const int64_t mo = static_cast<int64_t>(col) * p.ldc + pr;
-              const bool mirror = p.sym && col > pr;
-              if (p.H1) {
-                const double o1 = v * p.H1[ro + col];
-                p.C[ro + col] = o1;
-                if (mirror) p.C[mo] = o1;
-                if (p.H2) {
-                  const double o2 = v * p.H2[ro + col];
-                  p.C2[ro + col] = o2;
-                  if (mirror) p.C2[mo] = o2;
+          for (int h = 0; h < 32; h += 8) {
+            double sb[8], f1[8], f2[8], cold[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              const int col = c0 + ch * 32 + h + i;
+              const bool in = col < p.n_cols && (!p.sym || col >= pr);
+              sb[i] = in ? p.scale_b[col] : 0.0;
+              f1[i] = in && p.H1 ? p.H1[ro + col] : 0.0;
+              f2[i] = in && p.H1 && p.H2 ? p.H2[ro + col] : 0.0;
+              cold[i] = in && !p.H1 && p.beta != 0.0 ? p.C[ro + col] : 0.0;
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              const int col = c0 + ch * 32 + h + i;
+              // symmetric: the upper triangle, each entry also at its mirror
+              // (the lanes' rows are consecutive, so the mirrored stores of
+              // one column coalesce)
+              if (col < p.n_cols && (!p.sym || col >= pr)) {
+                const double v = a * acc[h + i] * sb[i];
+                const int64_t mo = static_cast<int64_t>(col) * p.ldc + pr;
+                const bool mirror = p.sym && col > pr;
+                if (p.H1) {
+                  const double o1 = v * f1[i];
+                  p.C[ro + col] = o1;
+                  if (mirror) p.C[mo] = o1;
+                  if (p.H2) {
+                    const double o2 = v * f2[i];
+                    p.C2[ro + col] = o2;
+                    if (mirror) p.C2[mo] = o2;
+                  }
+                } else {
+                  const double o = p.beta == 0.0 ? v : v + p.beta * cold[i];
+                  p.C[ro + col] = o;
+                  if (mirror) p.C[mo] = o;
                 }
-              } else {
-                const double o = p.beta == 0.0 ? v : v + p.beta * p.C[ro + col];
-                p.C[ro + col] = o;
-                if (mirror) p.C[mo] = o;
               }
             }
           }
